@@ -1,0 +1,247 @@
+/*
+ * gz_oracle.c -- plain-C restatement of GraphZeppelin's CameoSketch ingest and Boruvka
+ * query (see gz_oracle.h for the function-by-function reference citations).
+ *
+ * TEST INFRASTRUCTURE ONLY: the parity oracle. Never linked into the product library.
+ * Single-threaded and written for clarity, not speed.
+ */
+#include "gz_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* ---- xxHash XXH3, 8-byte input path (published algorithm, xxHash 0.8.x) ---------------- */
+
+/* First 24 bytes of the XXH3 default secret (XXH3_kSecret); the 4..8-byte path reads the
+ * little-endian u64 words at offsets 8 and 16. */
+static const uint8_t kSecretHead[24] = {
+    0xb8, 0xfe, 0x6c, 0x39, 0x23, 0xa4, 0x4b, 0xbe, 0x7c, 0x01, 0x81, 0x2c,
+    0xf7, 0x21, 0xad, 0x1c, 0xde, 0xd4, 0x6d, 0xe9, 0x83, 0x90, 0x97, 0xdb};
+#define GZO_PRIME_MX2 0x9FB21C651E98DF25ULL
+
+static uint64_t read_le64(const uint8_t *p) {
+  uint64_t v = 0;
+  for (int i = 7; i >= 0; --i) v = (v << 8) | p[i];
+  return v;
+}
+static uint32_t read_le32(const uint8_t *p) {
+  return (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24);
+}
+static uint32_t bswap32(uint32_t x) {
+  return (x >> 24) | ((x >> 8) & 0xff00u) | ((x << 8) & 0xff0000u) | (x << 24);
+}
+static uint64_t rotl64(uint64_t x, int r) { return (x << r) | (x >> (64 - r)); }
+
+uint64_t gzo_xxh3_8b(uint64_t value, uint64_t seed) {
+  /* XXH3_len_4to8_64b with len == 8 */
+  uint8_t in[8];
+  for (int i = 0; i < 8; ++i) in[i] = (uint8_t)(value >> (8 * i));
+  seed ^= (uint64_t)bswap32((uint32_t)seed) << 32;
+  uint32_t input1 = read_le32(in);
+  uint32_t input2 = read_le32(in + 4);
+  uint64_t bitflip = (read_le64(kSecretHead + 8) ^ read_le64(kSecretHead + 16)) - seed;
+  uint64_t input64 = (uint64_t)input2 + ((uint64_t)input1 << 32);
+  uint64_t h = input64 ^ bitflip;
+  /* XXH3_rrmxmx(h, 8) */
+  h ^= rotl64(h, 49) ^ rotl64(h, 24);
+  h *= GZO_PRIME_MX2;
+  h ^= (h >> 35) + 8;
+  h *= GZO_PRIME_MX2;
+  return h ^ (h >> 28);
+}
+
+/* ---- sizing ------------------------------------------------------------------------------ */
+
+int gzo_params(uint32_t V, double f, uint32_t *num_columns, uint32_t *bkt_per_col) {
+  if (V < 2) return -1;
+  /* Sketch::calc_vector_length: ceil(double(V) * (V - 1) / 2), stored as vec_t */
+  uint64_t vec_len = (uint64_t)ceil((double)V * (uint32_t)(V - 1) / 2);
+  /* Sketch::calc_bkt_per_col(size_t n): ceil(log2(n)) + 1 */
+  *bkt_per_col = (uint32_t)(ceil(log2((double)vec_len)) + 1);
+  /* Sketch::calc_cc_samples with num_samples_div = 1 - log2(2 - 0.8) (CameoSketch) */
+  const double num_samples_div = 1 - log2(2 - 0.8);
+  size_t s = (size_t)ceil(f * log2((double)V) / num_samples_div);
+  *num_columns = (uint32_t)(s > 18 ? s : 18);
+  return 0;
+}
+
+uint64_t gzo_concat_pairing(uint32_t a, uint32_t b) {
+  uint32_t lo = a < b ? a : b, hi = a < b ? b : a;
+  return ((uint64_t)lo << 32) | hi;
+}
+
+/* ---- bucket helpers (include/bucket.h) ---------------------------------------------------- */
+
+static uint64_t bkt_alpha(const uint8_t *b) { return read_le64(b); }
+static uint32_t bkt_gamma(const uint8_t *b) { return read_le32(b + 8); }
+static void bkt_xor(uint8_t *b, uint64_t alpha, uint32_t gamma) {
+  for (int i = 0; i < 8; ++i) b[i] ^= (uint8_t)(alpha >> (8 * i));
+  for (int i = 0; i < 4; ++i) b[8 + i] ^= (uint8_t)(gamma >> (8 * i));
+}
+/* Bucket_Boruvka::is_good (include/bucket.h:65-67): gamma == (u32) hash(alpha, seed) */
+static int bkt_good(const uint8_t *b, uint64_t seed) {
+  return bkt_gamma(b) == (uint32_t)gzo_xxh3_8b(bkt_alpha(b), seed);
+}
+
+void gzo_sketch_update(uint8_t *sk, uint32_t C, uint32_t B, uint64_t seed, uint64_t idx) {
+  /* checksum = get_index_hash(idx, checksum_seed() == seed) truncated to vec_hash_t */
+  uint32_t checksum = (uint32_t)gzo_xxh3_8b(idx, seed);
+  /* deterministic bucket is the last one (num_buckets - 1 == C*B) */
+  bkt_xor(sk + (size_t)C * B * 12, idx, checksum);
+  for (uint32_t c = 0; c < C; ++c) {
+    /* get_index_depth(idx, column_seed(c) = seed + 5c, B): ctz(hash | 1 << B) */
+    uint64_t h = gzo_xxh3_8b(idx, seed + 5ull * c) | (1ull << B);
+    uint32_t depth = (uint32_t)__builtin_ctzll(h);
+    if (depth < B) bkt_xor(sk + ((size_t)c * B + depth) * 12, idx, checksum);
+  }
+}
+
+int gzo_apply_records(uint8_t *sketches, uint32_t V, uint32_t C, uint32_t B, uint64_t seed,
+                      const uint8_t *rec, size_t n, const uint8_t *filter) {
+  const size_t sk_bytes = ((size_t)C * B + 1) * 12;
+  int rc = 0;
+  for (size_t i = 0; i < n; ++i, rec += 9) {
+    uint32_t u = read_le32(rec + 1), v = read_le32(rec + 5);
+    if (u >= V || v >= V) { rc = GZO_BAD_VERTEX; continue; }
+    uint64_t idx = gzo_concat_pairing(u, v);
+    if (!filter || filter[u]) gzo_sketch_update(sketches + u * sk_bytes, C, B, seed, idx);
+    if (!filter || filter[v]) gzo_sketch_update(sketches + v * sk_bytes, C, B, seed, idx);
+  }
+  return rc;
+}
+
+int gzo_apply_batch(uint8_t *sketches, uint32_t V, uint32_t C, uint32_t B, uint64_t seed,
+                    uint32_t src, const uint32_t *dsts, size_t n) {
+  const size_t sk_bytes = ((size_t)C * B + 1) * 12;
+  if (src >= V) return GZO_BAD_VERTEX;
+  for (size_t i = 0; i < n; ++i) {
+    if (dsts[i] >= V) return GZO_BAD_VERTEX;
+    gzo_sketch_update(sketches + src * sk_bytes, C, B, seed, gzo_concat_pairing(src, dsts[i]));
+  }
+  return 0;
+}
+
+int gzo_sample(const uint8_t *det, const uint8_t *col, uint32_t B, uint64_t seed, uint64_t *idx) {
+  *idx = 0;
+  if (bkt_alpha(det) == 0 && bkt_gamma(det) == 0) return GZO_ZERO;
+  if (bkt_good(det, seed)) { *idx = bkt_alpha(det); return GZO_GOOD; }
+  for (uint32_t j = 0; j < B; ++j)
+    if (bkt_good(col + 12 * j, seed)) { *idx = bkt_alpha(col + 12 * j); return GZO_GOOD; }
+  return GZO_FAIL;
+}
+
+/* ---- Boruvka ------------------------------------------------------------------------------ */
+
+static uint32_t uf_find(uint32_t *p, uint32_t x) {
+  while (p[x] != x) { p[x] = p[p[x]]; x = p[x]; }
+  return x;
+}
+/* deterministic link: smaller root id wins (partition is independent of the link rule) */
+static int uf_union(uint32_t *p, uint32_t a, uint32_t b) {
+  a = uf_find(p, a); b = uf_find(p, b);
+  if (a == b) return 0;
+  if (a < b) p[b] = a; else p[a] = b;
+  return 1;
+}
+
+int gzo_boruvka(const uint8_t *sketches, uint32_t V, uint32_t C, uint32_t B, uint64_t seed,
+                uint32_t *labels, uint32_t *rounds_out, gzo_trace_rec *trace, size_t cap,
+                size_t *trace_len) {
+  const size_t sk_bytes = ((size_t)C * B + 1) * 12;
+  const size_t acc_bytes = (size_t)(B + 1) * 12; /* column buckets, then the det bucket */
+  uint32_t *parent = (uint32_t *)malloc(sizeof(uint32_t) * V);
+  uint32_t *root = (uint32_t *)malloc(sizeof(uint32_t) * V);
+  uint32_t *key = (uint32_t *)malloc(sizeof(uint32_t) * V);
+  uint8_t *acc = (uint8_t *)malloc(acc_bytes * V);
+  size_t tl = 0;
+  int rc = GZO_OK;
+  uint32_t round = 0;
+  for (uint32_t v = 0; v < V; ++v) parent[v] = v;
+  for (;;) {
+    if (round >= C) { rc = GZO_OUT_OF_SAMPLES; break; }
+    /* components fixed before this round (create_merge_instructions) */
+    for (uint32_t v = 0; v < V; ++v) root[v] = uf_find(parent, v);
+    for (uint32_t v = 0; v < V; ++v) key[v] = UINT32_MAX;
+    for (uint32_t v = 0; v < V; ++v)
+      if (key[root[v]] == UINT32_MAX) key[root[v]] = v;
+    memset(acc, 0, acc_bytes * V);
+    /* range_merge of column `round` and the deterministic bucket into each component */
+    for (uint32_t v = 0; v < V; ++v) {
+      const uint8_t *sk = sketches + v * sk_bytes;
+      uint8_t *a = acc + root[v] * acc_bytes;
+      for (size_t j = 0; j < (size_t)B * 12; ++j) a[j] ^= sk[(size_t)round * B * 12 + j];
+      for (size_t j = 0; j < 12; ++j) a[B * 12 + j] ^= sk[(size_t)C * B * 12 + j];
+    }
+    /* sample every component (iterating roots in key order gives a sorted trace) */
+    int modified = 0;
+    uint32_t n_good = 0;
+    uint64_t *good = (uint64_t *)malloc(sizeof(uint64_t) * V);
+    for (uint32_t k = 0; k < V; ++k) {
+      uint32_t r = root[k];
+      if (key[r] != k) continue; /* k is the smallest member of component r */
+      uint64_t idx;
+      uint8_t *a = acc + r * acc_bytes;
+      int res = gzo_sample(a + (size_t)B * 12, a, B, seed, &idx);
+      if (trace && tl < cap) {
+        trace[tl].round = round; trace[tl].key = k; trace[tl].result = (uint32_t)res;
+        trace[tl].pad = 0; trace[tl].idx = idx;
+      }
+      ++tl;
+      if (res == GZO_FAIL) modified = 1;
+      else if (res == GZO_GOOD) good[n_good++] = idx;
+    }
+    for (uint32_t i = 0; i < n_good; ++i) {
+      uint32_t a = (uint32_t)(good[i] >> 32), b = (uint32_t)good[i];
+      if (a >= V || b >= V) { rc = GZO_BAD_VERTEX; continue; }
+      if (uf_union(parent, a, b)) modified = 1;
+    }
+    free(good);
+    if (rc != GZO_OK) break;
+    if (!modified) break;
+    ++round;
+  }
+  for (uint32_t v = 0; v < V; ++v) root[v] = uf_find(parent, v);
+  for (uint32_t v = 0; v < V; ++v) key[v] = UINT32_MAX;
+  for (uint32_t v = 0; v < V; ++v) {
+    if (key[root[v]] == UINT32_MAX) key[root[v]] = v;
+    labels[v] = key[root[v]];
+  }
+  *rounds_out = round;
+  if (trace_len) *trace_len = tl;
+  free(parent); free(root); free(key); free(acc);
+  return rc;
+}
+
+/* ---- exact connected components over the final edge set ---------------------------------- */
+
+static int cmp_u64(const void *a, const void *b) {
+  uint64_t x = *(const uint64_t *)a, y = *(const uint64_t *)b;
+  return x < y ? -1 : x > y;
+}
+
+uint32_t gzo_exact_cc(uint32_t V, const uint8_t *rec, size_t n, uint32_t *labels) {
+  uint64_t *e = (uint64_t *)malloc(sizeof(uint64_t) * (n ? n : 1));
+  uint32_t *parent = (uint32_t *)malloc(sizeof(uint32_t) * V);
+  for (size_t i = 0; i < n; ++i) {
+    uint32_t u = read_le32(rec + 9 * i + 1), v = read_le32(rec + 9 * i + 5);
+    if (u >= V || v >= V) { free(e); free(parent); return 0; }
+    e[i] = gzo_concat_pairing(u, v);
+  }
+  qsort(e, n, sizeof(uint64_t), cmp_u64);
+  for (uint32_t v = 0; v < V; ++v) parent[v] = v;
+  for (size_t i = 0; i < n;) {
+    size_t j = i;
+    while (j < n && e[j] == e[i]) ++j;
+    if ((j - i) & 1) uf_union(parent, (uint32_t)(e[i] >> 32), (uint32_t)e[i]); /* odd => present */
+    i = j;
+  }
+  uint32_t ncc = 0;
+  for (uint32_t v = 0; v < V; ++v) {
+    uint32_t r = uf_find(parent, v);
+    labels[v] = r; /* smaller root wins in uf_union, so the root is the smallest member */
+    if (r == v) ++ncc;
+  }
+  free(e); free(parent);
+  return ncc;
+}
