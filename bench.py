@@ -1,0 +1,412 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 sketch-ingest + Boruvka connected-components path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--small]
+
+Workload (one replica per GPU): the dense planted-partition stream -- V = 2^17 vertices in 64
+planted components (sizes uniform, >= 256), intra-component edges, 10% insert-then-delete
+churn over random non-edges, ~1.4e8 packed 9-byte records (1.26 GB), one connectivity query at
+the end. A step = clear the sketches, ingest every record (device gutter + sketch update), run
+the query. `value` = updates / device time of the step with the records already in HBM;
+`e2e` = the same through the public API from pinned host memory (copies inside the timing).
+
+Under torchrun (N > 1) every rank runs an independent replica (the path is single-GPU; there is
+no data-path collective); timing is the max over ranks.
+
+`--impl reference` times the reference's own CCSketchAlg (compiled from its sources into
+oracle/_ref) on the host cores over bounded samples of the same stream.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "edge updates/sec + CC query ms on 1 B200"
+UNIT = "updates/s"
+
+FULL = dict(workload="dense_planted_v131072_c64_deg1780_churn10", num_vertices=1 << 17,
+            components=64, min_size=256, mean_degree=1780.0, churn=0.10, stream_seed=1,
+            sketch_seed=0x5EED5EED)
+SMALL = dict(workload="dense_planted_v16384_c16_deg800_churn10", num_vertices=1 << 14,
+             components=16, min_size=256, mean_degree=800.0, churn=0.10, stream_seed=1,
+             sketch_seed=0x5EED5EED)
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def gen_stream(cfg, out=None):
+    from graphzeppelin_b200 import streams as S
+    return S.planted_partition_stream_fast(cfg["num_vertices"], cfg["components"],
+                                           cfg["stream_seed"], mean_degree=cfg["mean_degree"],
+                                           min_size=cfg["min_size"],
+                                           churn_fraction=cfg["churn"], out=out)
+
+
+# ------------------------------------------------------------------------------------------------
+# clocks during the timed region
+# ------------------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons, power = [], None, set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm),
+                "power_w_max": max(power) if power else None}
+
+
+# ------------------------------------------------------------------------------------------------
+# CPU baseline: the reference's CCSketchAlg on the host cores
+# ------------------------------------------------------------------------------------------------
+def cpu_reference_run(stream, cfg, n_records: int, threads: int, timeout=600):
+    """Ingest the first n_records through oracle/_ref/gz_ref_eager (reference sources, default
+    eager-DSU build, stand-in gutter) and return its JSON (ingest_s, query_s, ...)."""
+    from oracle import oracle as O
+    if not O.have_reference():
+        try:
+            O.build()
+        except Exception:
+            pass
+    from graphzeppelin_b200 import streams as S
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "sample.gzs")
+        S.Stream(stream.num_vertices, stream.records[:n_records]).write(p)
+        if O.have_reference():
+            r = O.ref_ingest(p, cfg["sketch_seed"], 1.0, threads=threads, eager=True,
+                             timeout=timeout)
+            r["kind"] = "reference"
+            return r
+    # the compiled reference is unavailable: time the C restatement (single thread)
+    osk = O.OracleSketches(stream.num_vertices, cfg["sketch_seed"])
+    t0 = time.perf_counter()
+    osk.apply_records(stream.records[:n_records].view("u1").reshape(-1))
+    t1 = time.perf_counter()
+    rc, lab, rounds, _ = osk.boruvka(with_trace=False)
+    t2 = time.perf_counter()
+    return {"ingest_s": t1 - t0, "query_s": t2 - t1, "threads": 1, "kind": "port",
+            "updates": n_records, "rounds": rounds}
+
+
+def cpu_baseline(stream, cfg, target_s=12.0):
+    threads = os.cpu_count() or 1
+    n_total = stream.num_updates
+    cal = min(n_total, 1 << 21)
+    r = cpu_reference_run(stream, cfg, cal, threads)
+    rate = cal / max(r["ingest_s"] + r["query_s"], 1e-9)
+    n = int(min(n_total, max(cal, rate * target_s)))
+    if n > cal:
+        r = cpu_reference_run(stream, cfg, n, threads)
+    value = n / (r["ingest_s"] + r["query_s"])
+    return {"value": value, "unit": UNIT, "cores": int(r.get("threads", threads)),
+            "kind": r["kind"],
+            "sample": f"first {n} of {n_total} records of the same stream "
+                      f"(ingest {r['ingest_s']:.3f} s + query {r['query_s']:.3f} s, "
+                      f"{r.get('num_cc', '?')} components on the prefix)",
+            "ingest_updates_per_s": n / r["ingest_s"], "query_ms": r["query_s"] * 1e3}
+
+
+# ------------------------------------------------------------------------------------------------
+def roofline_terms(alg, n_records, t_launch_s, hash_peak, hbm_peak_gbs):
+    p = alg.params
+    V, C, sb = p.num_vertices, p.num_columns, p.sketch_bytes
+    entries = 2 * n_records
+    # sketch-update kernel: reads every gutter entry (8 B) once, reads + writes every touched
+    # sketch once; evaluates 1 + C hashes per endpoint update
+    bytes_alg = entries * 8 + 2 * V * sb
+    hashes = entries * (C + 1)
+    t_hbm = bytes_alg / (hbm_peak_gbs * 1e9)
+    t_int = hashes / hash_peak
+    hbm = {"achieved": bytes_alg / t_launch_s / 1e9, "peak": hbm_peak_gbs, "unit": "GB/s",
+           "frac": (bytes_alg / t_launch_s / 1e9) / hbm_peak_gbs, "bytes_per_launch": bytes_alg}
+    integer = {"achieved": hashes / t_launch_s / 1e9, "peak": hash_peak / 1e9, "unit": "Ghash/s",
+               "frac": (hashes / t_launch_s) / hash_peak, "hashes_per_launch": hashes}
+    return hbm, integer, ("int" if t_int > t_hbm else "hbm")
+
+
+def load_traffic(workload):
+    """DRAM bytes per sketch-update launch from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "sketch_update_traffic.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return d.get(workload)
+    except Exception:
+        return None
+
+
+def run_b200(args, cfg):
+    import numpy as np
+    import torch
+
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+
+    import graphzeppelin_b200 as gz
+    from graphzeppelin_b200 import cc as gzcc
+
+    t = time.time()
+    # the records live in pinned host memory (for e2e) and are copied once into HBM (for value)
+    from graphzeppelin_b200 import streams as S
+    probe, _ = gen_stream(cfg)
+    n = probe.num_updates
+    pinned = torch.empty(n * 9, dtype=torch.uint8, pin_memory=True)
+    pinned.numpy()[:] = probe.raw()
+    stream = S.Stream(cfg["num_vertices"], pinned.numpy().view(S.RECORD_DTYPE))
+    del probe
+    d_rec = pinned.cuda(non_blocking=False)
+    torch.cuda.synchronize()
+    log(f"[rank {rank}] stream: {n} records ({n * 9 / 1e9:.2f} GB) in {time.time() - t:.1f} s")
+
+    V = cfg["num_vertices"]
+    alg = gz.CCSketchAlg(V, cfg["sketch_seed"])
+    alg.set_gutter_capacity(2 * n + 1024)
+    lib_stream = torch.cuda.ExternalStream(alg.stream_handle())
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+
+    def step():
+        e0, e1, e2 = ev(), ev(), ev()
+        e0.record(lib_stream)
+        alg.clear()
+        alg.ingest_records_device(d_rec.data_ptr(), n)
+        alg.flush()
+        e1.record(lib_stream)
+        ncc = alg.num_connected_components()
+        e2.record(lib_stream)
+        return e0, e1, e2, ncc
+
+    for _ in range(args.warmup):
+        *_, ncc = step()
+    torch.cuda.synchronize()
+    if ncc != cfg["components"]:
+        raise SystemExit(f"wrong answer: {ncc} components, expected {cfg['components']}")
+
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    alg.set_profiling(True)
+    marks = []
+    tw0 = time.perf_counter()
+    for _ in range(args.steps):
+        marks.append(step())
+    torch.cuda.synchronize()
+    tw1 = time.perf_counter()
+    prof = alg.get_profile()
+    alg.set_profiling(False)
+    clocks = sampler.stop()
+    ingest_ms = [a.elapsed_time(b) for a, b, c, _ in marks]
+    query_ms = [b.elapsed_time(c) for a, b, c, _ in marks]
+    total_ms = sum(a.elapsed_time(c) for a, b, c, _ in marks)
+    if dist:
+        tt = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+    ms_per_step = total_ms / args.steps
+    value = world * n * args.steps / (total_ms / 1e3)
+
+    # end to end through the public API: pinned host records in, partition out
+    e2e_s = []
+    for i in range(max(1, min(args.steps, 3)) + 1):
+        alg.clear()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        alg.ingest_records(stream.records)
+        cc = alg.connected_components()
+        t1 = time.perf_counter()
+        if i:
+            e2e_s.append(t1 - t0)
+    assert cc.size() == cfg["components"]
+    e2e = {"value": world * n / max(e2e_s), "unit": UNIT, "h2d_bytes_per_step": n * 9,
+           "d2h_bytes_per_step": V * 4 + 4,
+           "note": "pinned host records -> gz_ingest_records (pipelined H2D) -> "
+                   "gz_connected_components -> parent array on host; wall clock, max of steps"}
+
+    line = None
+    if rank == 0:
+        hbm_peak = 6546.2
+        try:
+            with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+                hbm_peak = float(json.load(f)["hbm_gbs"])
+            peak_src = "measured (MEASURED_PEAKS.json hbm_gbs)"
+        except Exception:
+            peak_src = "fallback 6546.2 GB/s"
+        hash_peak = gzcc.measure_hash_rate(5)
+        launches = max(1, prof["sketch_update_launches"])
+        t_launch = prof["sketch_update_ms"] / launches / 1e3
+        hbm, integer, bound = roofline_terms(alg, n, t_launch, hash_peak, hbm_peak)
+        main = integer if bound == "int" else hbm
+        traffic = load_traffic(cfg["workload"])
+        roof = {"bound": bound, "achieved": main["achieved"], "peak": main["peak"],
+                "unit": main["unit"], "frac": main["frac"], "traffic": traffic,
+                "kernel": "k_sketch_update",
+                "launch_ms": t_launch * 1e3,
+                "terms": {"hbm": hbm, "int": integer},
+                "peaks": {"hbm": peak_src,
+                          "int": "measured here: gz_measure_hash_rate (register-only XXH3-8B + "
+                                 "depth ctz kernel, best of 5)"}}
+        # the whole ingest (gutter + sketch update) against the path roofline: 9 B read per
+        # record + sketch RMW, 1 + C hashes per record (one hash per edge)
+        p = alg.params
+        ing_s = statistics.mean(ingest_ms) / 1e3
+        path_bytes = 9 * n + 2 * V * p.sketch_bytes
+        path_hashes = n * (p.num_columns + 1)
+        path_t = max(path_bytes / (hbm_peak * 1e9), path_hashes / hash_peak)
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            log("[rank 0] timing the CPU reference baseline ...")
+            cpu = cpu_baseline(stream, cfg)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic (seeded planted-partition stream, C generator)",
+            "config": {"workload": cfg["workload"], "num_vertices": V, "num_updates": n,
+                       "components": cfg["components"], "num_columns": p.num_columns,
+                       "bkt_per_col": p.bkt_per_col, "sketch_bytes_total": V * p.sketch_bytes,
+                       "stream_seed": cfg["stream_seed"], "sketch_seed": cfg["sketch_seed"],
+                       "l2": "inputs larger than L2: 1.26 GB records + 1.29 GB sketches per step",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "query_ms": statistics.mean(query_ms),
+            "ingest_ms": statistics.mean(ingest_ms),
+            "ingest_updates_per_s": n / ing_s,
+            "path_roofline": {"time_ms": path_t * 1e3, "frac": path_t / ing_s,
+                              "bytes": path_bytes, "hashes": path_hashes},
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "clocks": clocks,
+            "gpu_launches": int(prof["kernel_launches"]),
+            "profile": {k: prof[k] for k in ("gutter_ms", "sketch_update_ms", "query_ms",
+                                             "sketch_update_launches", "gutter_launches")},
+            "wall_s_timed": tw1 - tw0,
+        }
+    alg.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return line
+
+
+def run_reference(args, cfg):
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    if rank != 0:
+        return None
+    stream, _ = gen_stream(cfg)
+    n_total = stream.num_updates
+    threads = os.cpu_count() or 1
+    # size one step to a few seconds of reference work
+    cal = min(n_total, 1 << 21)
+    r = cpu_reference_run(stream, cfg, cal, threads)
+    rate = cal / max(r["ingest_s"] + r["query_s"], 1e-9)
+    n = int(min(n_total, max(cal, rate * 4.0)))
+    for _ in range(args.warmup):
+        cpu_reference_run(stream, cfg, n, threads)
+    runs = [cpu_reference_run(stream, cfg, n, threads) for _ in range(args.steps)]
+    total = sum(x["ingest_s"] + x["query_s"] for x in runs)
+    value = n * args.steps / total
+    kind = runs[0]["kind"]
+    return {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+        "data": "synthetic (seeded planted-partition stream, C generator)",
+        "config": {"workload": cfg["workload"], "num_vertices": cfg["num_vertices"],
+                   "num_updates": n_total, "sample_records": n,
+                   "parallelism": f"{runs[0].get('threads', threads)} host threads"},
+        "impl": "reference",
+        "query_ms": statistics.mean(x["query_s"] for x in runs) * 1e3,
+        "ingest_updates_per_s": n / statistics.mean(x["ingest_s"] for x in runs),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": int(runs[0].get("threads", threads)),
+                         "kind": kind,
+                         "sample": f"first {n} of {n_total} records per step "
+                                   f"(reference CCSketchAlg, eager DSU, stand-in gutter)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--small", action="store_true", help="V=2^14 case (profiling)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and not args.small:
+        log("note: at least 3 warm-up steps are required for a valid number; using 3")
+        args.warmup = 3
+    cfg = SMALL if args.small else FULL
+    line = run_reference(args, cfg) if args.impl == "reference" else run_b200(args, cfg)
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,998 @@
+// gz_capi.cu -- the C ABI (include/gz_b200.h): one handle = one CCSketchAlg whose sketches live in
+// HBM, fed by a device-resident gutter and queried by device Boruvka.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/gz_b200.h"
+#include "gz_device.cuh"
+#include "gz_kernels.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string &msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define GZ_CUDA(call)                                                                    \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess)                                                               \
+      return fail(e_ == cudaErrorMemoryAllocation ? GZ_ERR_NOMEM : GZ_ERR_CUDA,          \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                   \
+  } while (0)
+
+#define GZ_TRY(expr)          \
+  do {                        \
+    int rc_ = (expr);         \
+    if (rc_ != GZ_OK) return rc_; \
+  } while (0)
+
+template <class T>
+int dev_alloc(T **p, size_t count) {
+  if (*p) return GZ_OK;
+  void *q = nullptr;
+  cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
+  if (e != cudaSuccess)
+    return fail(GZ_ERR_NOMEM, std::string("cudaMalloc(") + std::to_string(count * sizeof(T)) +
+                                  " bytes): " + cudaGetErrorString(e));
+  *p = static_cast<T *>(q);
+  return GZ_OK;
+}
+template <class T>
+void dev_free(T *&p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+template <class T>
+int host_alloc(T **p, size_t count) {
+  if (*p) return GZ_OK;
+  void *q = nullptr;
+  cudaError_t e = cudaMallocHost(&q, std::max<size_t>(count, 1) * sizeof(T));
+  if (e != cudaSuccess) return fail(GZ_ERR_NOMEM, std::string("cudaMallocHost: ") + cudaGetErrorString(e));
+  *p = static_cast<T *>(q);
+  return GZ_OK;
+}
+template <class T>
+void host_free(T *&p) {
+  if (p) cudaFreeHost(p);
+  p = nullptr;
+}
+
+// Reference sizing (include/sketch.h:62-76, :181, :188-190), evaluated with the same double
+// expressions so the results agree bit for bit.
+void reference_params(uint32_t V, double f, uint32_t &C, uint32_t &B) {
+  const uint64_t vec_len = (uint64_t)std::ceil(double(V) * (uint32_t)(V - 1) / 2);
+  B = (uint32_t)(std::ceil(std::log2((double)vec_len)) + 1);
+  const double num_samples_div = 1 - std::log2(2 - 0.8);
+  const size_t s = (size_t)std::ceil(f * std::log2((double)V) / num_samples_div);
+  C = (uint32_t)std::max<size_t>(18, s);
+}
+
+constexpr uint64_t kStageRecords = 1ull << 24;  // records per host->device pipeline chunk
+constexpr uint64_t kEntStage = 1ull << 20;      // staged apply_update_batch entries per flush
+constexpr uint64_t kMaxChunkEntries = 1ull << 31;
+constexpr int kNumPhases = 3;  // gutter, sketch update, query
+
+}  // namespace
+
+struct gz_alg {
+  std::mutex mtx;
+  int device = 0;
+  // configuration
+  uint32_t V = 0, C = 0, B = 0, nb = 0;
+  uint64_t seed = 0;
+  double sketches_factor = 1, batch_factor = 1;
+  uint64_t sketch_bytes = 0, desired_batch = 0;
+  uint32_t tile_shift = 2, ntiles = 0, threads = 1024;
+  size_t num_workers = 1;
+  // sketches + per-column hash constants
+  uint8_t *d_sk = nullptr;
+  uint64_t *d_flip = nullptr;
+  uint32_t *d_status = nullptr;  // [0] status bits, [1] work counter
+  uint32_t *h_status = nullptr;  // pinned mirror
+  // device gutter
+  uint2 *d_entries = nullptr;
+  uint64_t entry_cap = 0, entry_used = 0;
+  gz::ChunkTable chunks{};
+  int nchunks = 0;
+  uint32_t *d_tile_off = nullptr;
+  uint64_t *d_hist = nullptr, *d_scan_tmp = nullptr, *d_total = nullptr;
+  size_t hist_words = 0;
+  // host-record pipeline
+  uint8_t *d_stage[2] = {nullptr, nullptr};
+  cudaEvent_t ev_copied[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr};
+  // apply_update_batch staging
+  uint2 *h_ent[2] = {nullptr, nullptr};
+  uint2 *d_ent[2] = {nullptr, nullptr};
+  cudaEvent_t ev_ent_done[2] = {nullptr, nullptr};
+  uint64_t h_ent_n = 0;
+  int h_ent_cur = 0;
+  uint32_t *d_raw = nullptr;
+  // query state
+  gz::BoruvkaBufs bv{};
+  bool bv_alloc = false;
+  uint32_t *d_final = nullptr, *d_ncc = nullptr;
+  bool dsu_valid = true, update_locked = false, labels_on_host = false;
+  std::atomic<bool> query_running{false};
+  size_t last_rounds = 0;
+  uint32_t last_ncc = 0;
+  std::vector<uint32_t> h_labels;
+  bool trace = false;
+  // streams
+  cudaStream_t stream = nullptr, copy_stream = nullptr;
+  // profiling
+  bool prof = false;
+  struct Ev {
+    cudaEvent_t a, b;
+    int phase;
+  };
+  std::vector<Ev> prof_pending;
+  std::vector<cudaEvent_t> ev_pool;
+  gz_profile_t prof_acc{};
+  uint64_t launch_base = 0;
+
+  gz::SketchGeom sgeom() const {
+    gz::SketchGeom g;
+    g.V = V;
+    g.C = C;
+    g.B = B;
+    g.sketch_words = nb * 3;
+    g.tile_shift = tile_shift;
+    g.ntiles = ntiles;
+    return g;
+  }
+  gz::GutterGeom ggeom() const { return gz::GutterGeom{V, tile_shift, ntiles}; }
+  gz::BoruvkaGeom bgeom() const {
+    gz::BoruvkaGeom g;
+    g.V = V;
+    g.C = C;
+    g.B = B;
+    g.sketch_words = nb * 3;
+    g.flip_chk = gz::xxh3_flip(seed);
+    g.span = 64;
+    return g;
+  }
+
+  cudaEvent_t get_event() {
+    if (!ev_pool.empty()) {
+      cudaEvent_t e = ev_pool.back();
+      ev_pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+  }
+  int prof_begin() {
+    if (!prof) return -1;
+    Ev e{get_event(), get_event(), 0};
+    cudaEventRecord(e.a, stream);
+    prof_pending.push_back(e);
+    return (int)prof_pending.size() - 1;
+  }
+  void prof_end(int i, int phase) {
+    if (i < 0) return;
+    prof_pending[i].phase = phase;
+    cudaEventRecord(prof_pending[i].b, stream);
+  }
+  void prof_collect() {
+    if (prof_pending.empty()) return;
+    cudaStreamSynchronize(stream);
+    for (auto &e : prof_pending) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e.a, e.b);
+      if (e.phase == 0) {
+        prof_acc.gutter_ms += ms;
+        prof_acc.gutter_launches++;
+      } else if (e.phase == 1) {
+        prof_acc.sketch_update_ms += ms;
+        prof_acc.sketch_update_launches++;
+      } else {
+        prof_acc.query_ms += ms;
+      }
+      ev_pool.push_back(e.a);
+      ev_pool.push_back(e.b);
+    }
+    prof_pending.clear();
+  }
+};
+
+namespace {
+
+int choose_tiling(gz_alg *h, uint32_t vpt_req, uint32_t threads_req) {
+  int dev = h->device;
+  int smem_optin = 0;
+  cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (smem_optin <= 0) smem_optin = 227 * 1024;
+  const size_t budget = (size_t)smem_optin - 64;
+  const size_t flip_bytes = (size_t)(h->C + 1) * 8;
+  uint32_t shift;
+  if (vpt_req) {
+    if (vpt_req < 4 || (vpt_req & (vpt_req - 1)) || vpt_req > 64)
+      return fail(GZ_ERR_INVALID, "vertices_per_tile must be a power of two in [4, 64]");
+    shift = (uint32_t)__builtin_ctz(vpt_req);
+    if ((h->sketch_bytes << shift) + flip_bytes > budget)
+      return fail(GZ_ERR_INVALID, "vertices_per_tile does not fit in shared memory");
+  } else {
+    shift = 2;
+    const uint64_t want = std::max<uint64_t>(4, h->V / (2ull * gz::num_sms()));
+    while (shift < 6 && (1ull << (shift + 1)) <= want &&
+           (h->sketch_bytes << (shift + 1)) + flip_bytes <= budget)
+      ++shift;
+    if ((h->sketch_bytes << shift) + flip_bytes > budget)
+      return fail(GZ_ERR_INVALID, "sketch too large to stage 4 vertices in shared memory");
+  }
+  h->tile_shift = shift;
+  h->ntiles = (uint32_t)((h->V + (1u << shift) - 1) >> shift);
+  if (threads_req) {
+    if (threads_req < 64 || threads_req > 1024 || threads_req % 32)
+      return fail(GZ_ERR_INVALID, "threads_per_block must be a multiple of 32 in [64, 1024]");
+    h->threads = threads_req;
+  }
+  cudaError_t e = gz::sketch_update_prepare(h->sgeom(), h->threads);
+  if (e != cudaSuccess) return fail(GZ_ERR_CUDA, cudaGetErrorString(e));
+  return GZ_OK;
+}
+
+int init_alg(gz_alg *h, uint32_t V, uint64_t seed, double sf, double bf) {
+  if (V < 2 || V > (1u << 31)) return fail(GZ_ERR_INVALID, "num_vertices must be in [2, 2^31]");
+  GZ_CUDA(cudaGetDevice(&h->device));
+  h->V = V;
+  h->seed = seed;
+  h->sketches_factor = sf > 0 ? sf : 1;  // CCAlgConfiguration::sketches_factor
+  h->batch_factor = bf > 0 ? bf : 1;     // CCAlgConfiguration::batch_factor
+  reference_params(V, h->sketches_factor, h->C, h->B);
+  if (h->B > 63) return fail(GZ_ERR_INVALID, "bkt_per_col above 63 is not supported");
+  h->nb = h->C * h->B + 1;
+  h->sketch_bytes = (uint64_t)h->nb * gz::kBucketBytes;
+  {
+    size_t num = h->sketch_bytes / sizeof(uint32_t);
+    num *= h->batch_factor;  // same size_t *= double truncation as the reference
+    h->desired_batch = num;
+  }
+  GZ_TRY(choose_tiling(h, 0, 0));
+  GZ_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  GZ_CUDA(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+  // V rounded up to 64 so any tile size stays inside the allocation
+  const uint64_t v_pad = ((uint64_t)V + 63) & ~63ull;
+  GZ_TRY(dev_alloc(&h->d_sk, v_pad * h->sketch_bytes));
+  GZ_CUDA(cudaMemsetAsync(h->d_sk, 0, v_pad * h->sketch_bytes, h->stream));
+  std::vector<uint64_t> flip(h->C + 1);
+  for (uint32_t c = 0; c < h->C; ++c) flip[c] = gz::xxh3_flip(seed + 5ull * c);  // column_seed
+  flip[h->C] = gz::xxh3_flip(seed);                                                  // checksum_seed
+  GZ_TRY(dev_alloc(&h->d_flip, flip.size()));
+  GZ_CUDA(cudaMemcpyAsync(h->d_flip, flip.data(), flip.size() * 8, cudaMemcpyHostToDevice, h->stream));
+  GZ_TRY(dev_alloc(&h->d_status, 4));
+  GZ_CUDA(cudaMemsetAsync(h->d_status, 0, 16, h->stream));
+  GZ_TRY(host_alloc(&h->h_status, 4));
+  h->entry_cap = std::min<uint64_t>((uint64_t)V * h->desired_batch, 1ull << 29);
+  h->entry_cap = std::max<uint64_t>(h->entry_cap, 1ull << 16);
+  GZ_CUDA(cudaStreamSynchronize(h->stream));
+  return GZ_OK;
+}
+
+void destroy_alg(gz_alg *h) {
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
+  dev_free(h->d_sk);
+  dev_free(h->d_flip);
+  dev_free(h->d_status);
+  host_free(h->h_status);
+  dev_free(h->d_entries);
+  dev_free(h->d_tile_off);
+  dev_free(h->d_hist);
+  dev_free(h->d_scan_tmp);
+  dev_free(h->d_total);
+  for (int i = 0; i < 2; ++i) {
+    dev_free(h->d_stage[i]);
+    dev_free(h->d_ent[i]);
+    host_free(h->h_ent[i]);
+    if (h->ev_copied[i]) cudaEventDestroy(h->ev_copied[i]);
+    if (h->ev_free[i]) cudaEventDestroy(h->ev_free[i]);
+    if (h->ev_ent_done[i]) cudaEventDestroy(h->ev_ent_done[i]);
+  }
+  dev_free(h->d_raw);
+  auto &b = h->bv;
+  dev_free(b.parent);
+  dev_free(b.label);
+  dev_free(b.cnt);
+  dev_free(b.fill);
+  dev_free(b.minv);
+  dev_free(b.packed);
+  dev_free(b.scan_total);
+  dev_free(b.scan_tmp);
+  dev_free(b.order);
+  dev_free(b.order_comp);
+  dev_free(b.comp_start);
+  dev_free(b.comp_key);
+  dev_free(b.ncomp);
+  dev_free(b.acc);
+  dev_free(b.flags);
+  dev_free(b.forest);
+  dev_free(b.forest_n);
+  if (b.trace) cudaFree(b.trace);
+  dev_free(b.trace_n);
+  dev_free(h->d_final);
+  dev_free(h->d_ncc);
+  for (auto &e : h->prof_pending) {
+    cudaEventDestroy(e.a);
+    cudaEventDestroy(e.b);
+  }
+  for (auto e : h->ev_pool) cudaEventDestroy(e);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
+}
+
+// ---- device gutter -------------------------------------------------------------------------------
+
+int ensure_gutter(gz_alg *h) {
+  GZ_TRY(dev_alloc(&h->d_entries, h->entry_cap));
+  GZ_TRY(dev_alloc(&h->d_tile_off, (size_t)gz::kMaxChunks * (h->ntiles + 1)));
+  const size_t g2 = 2 * (size_t)gz::num_sms();
+  const size_t words = std::max<size_t>((size_t)h->ntiles * g2, h->ntiles);
+  if (h->hist_words < words) {
+    dev_free(h->d_hist);
+    dev_free(h->d_scan_tmp);
+    GZ_TRY(dev_alloc(&h->d_hist, words));
+    GZ_TRY(dev_alloc(&h->d_scan_tmp, gz::scan_tmp_words(words)));
+    h->hist_words = words;
+  }
+  GZ_TRY(dev_alloc(&h->d_total, 1));
+  return GZ_OK;
+}
+
+// Apply every buffered gutter chunk to the sketches (one sketch-update launch).
+int apply_pending(gz_alg *h) {
+  if (h->nchunks == 0) return GZ_OK;
+  const gz::SketchGeom g = h->sgeom();
+  GZ_CUDA(cudaMemsetAsync(h->d_status + 1, 0, sizeof(uint32_t), h->stream));
+  const int per_sm = std::max(1, (int)(2048 / h->threads));
+  int smem_per_sm = 0;
+  cudaDeviceGetAttribute(&smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, h->device);
+  const size_t need = gz::sketch_update_smem_bytes(g) + 1024;
+  const int by_smem = std::max(1, (int)(smem_per_sm / need));
+  const int grid = (int)std::min<uint64_t>(h->ntiles, (uint64_t)gz::num_sms() * std::min(per_sm, by_smem));
+  const int pi = h->prof_begin();
+  GZ_CUDA(gz::sketch_update(g, h->d_sk, h->d_entries, h->chunks, h->d_tile_off, h->nchunks, h->d_flip,
+                            h->d_status + 1, h->d_status, grid, h->threads, h->stream));
+  h->prof_end(pi, 1);
+  h->prof_acc.entries_applied += h->entry_used;
+  h->nchunks = 0;
+  h->entry_used = 0;
+  return GZ_OK;
+}
+
+// Counting-sort n inputs (records or entries, device memory) into a new gutter chunk.
+int gutter_chunk(gz_alg *h, int input, const void *d_in, uint64_t n) {
+  if (n == 0) return GZ_OK;
+  const uint64_t per = input == gz::kInputRecords ? 2 : 1;
+  const uint64_t max_n = std::min(h->entry_cap, kMaxChunkEntries) / per;
+  if (n > max_n) {
+    const size_t isz = input == gz::kInputRecords ? 9 : sizeof(uint2);
+    for (uint64_t off = 0; off < n; off += max_n)
+      GZ_TRY(gutter_chunk(h, input, (const uint8_t *)d_in + off * isz, std::min(max_n, n - off)));
+    return GZ_OK;
+  }
+  GZ_TRY(ensure_gutter(h));
+  if (h->entry_used + n * per > h->entry_cap || h->nchunks == gz::kMaxChunks) GZ_TRY(apply_pending(h));
+  const gz::GutterGeom gg = h->ggeom();
+  const uint64_t unit = input == gz::kInputRecords ? gz::kRecTile : 4096;
+  const int G = (int)std::max<uint64_t>(1, std::min<uint64_t>(2ull * gz::num_sms(), (n + unit - 1) / unit));
+  uint2 *out = h->d_entries + h->entry_used;
+  uint32_t *tile_off = h->d_tile_off + (size_t)h->nchunks * (h->ntiles + 1);
+  const int pi = h->prof_begin();
+  if (h->ntiles <= gz::kSmemBinsMax) {
+    const uint64_t words = (uint64_t)h->ntiles * G;
+    GZ_CUDA(gz::gutter_count_2d(input, d_in, n, gg, G, h->d_hist, h->d_status, h->stream));
+    GZ_CUDA(gz::scan_exclusive_u64(h->d_hist, words, h->d_total, h->d_scan_tmp, h->stream));
+    GZ_CUDA(gz::gutter_tile_offsets(h->d_hist, (uint32_t)G, h->ntiles, h->d_total, tile_off, h->stream));
+    GZ_CUDA(gz::gutter_scatter_2d(input, d_in, n, gg, G, h->d_hist, out, h->stream));
+  } else {
+    GZ_CUDA(cudaMemsetAsync(h->d_hist, 0, sizeof(uint64_t) * h->ntiles, h->stream));
+    GZ_CUDA(gz::gutter_count_1d(input, d_in, n, gg, G, h->d_hist, h->d_status, h->stream));
+    GZ_CUDA(gz::scan_exclusive_u64(h->d_hist, h->ntiles, h->d_total, h->d_scan_tmp, h->stream));
+    GZ_CUDA(gz::gutter_tile_offsets(h->d_hist, 1, h->ntiles, h->d_total, tile_off, h->stream));
+    GZ_CUDA(gz::gutter_scatter_1d(input, d_in, n, gg, G, h->d_hist, out, h->stream));
+  }
+  h->prof_end(pi, 0);
+  h->chunks.base[h->nchunks++] = h->entry_used;
+  h->entry_used += n * per;
+  return GZ_OK;
+}
+
+int push_staged_entries(gz_alg *h) {
+  if (h->h_ent_n == 0) return GZ_OK;
+  const int i = h->h_ent_cur;
+  GZ_TRY(dev_alloc(&h->d_ent[i], kEntStage));
+  GZ_CUDA(cudaMemcpyAsync(h->d_ent[i], h->h_ent[i], h->h_ent_n * sizeof(uint2),
+                          cudaMemcpyHostToDevice, h->stream));
+  GZ_TRY(gutter_chunk(h, gz::kInputEntries, h->d_ent[i], h->h_ent_n));
+  GZ_CUDA(cudaEventRecord(h->ev_ent_done[i], h->stream));
+  h->h_ent_n = 0;
+  h->h_ent_cur ^= 1;
+  // the next buffer may still be in flight from two pushes ago
+  GZ_CUDA(cudaEventSynchronize(h->ev_ent_done[h->h_ent_cur]));
+  return GZ_OK;
+}
+
+int stage_entry(gz_alg *h, uint32_t v, uint32_t w) {
+  if (!h->h_ent[0]) {
+    for (int i = 0; i < 2; ++i) {
+      GZ_TRY(host_alloc(&h->h_ent[i], kEntStage));
+      GZ_CUDA(cudaEventCreateWithFlags(&h->ev_ent_done[i], cudaEventDisableTiming));
+      GZ_CUDA(cudaEventRecord(h->ev_ent_done[i], h->stream));
+    }
+  }
+  h->h_ent[h->h_ent_cur][h->h_ent_n++] = make_uint2(v, w);
+  if (h->h_ent_n == kEntStage) GZ_TRY(push_staged_entries(h));
+  return GZ_OK;
+}
+
+int check_status(gz_alg *h) {
+  GZ_CUDA(cudaMemcpyAsync(h->h_status, h->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+  GZ_CUDA(cudaStreamSynchronize(h->stream));
+  const uint32_t st = h->h_status[0];
+  if (st) {
+    GZ_CUDA(cudaMemsetAsync(h->d_status, 0, sizeof(uint32_t), h->stream));
+    GZ_CUDA(cudaStreamSynchronize(h->stream));
+    if (st & gz::kStatusTimeout) return fail(GZ_ERR_TIMEOUT, "a bounded device wait timed out");
+    if (st & gz::kStatusBadVertex) return fail(GZ_ERR_BAD_VERTEX, "an update named a vertex id >= V; it was dropped");
+    if (st & gz::kStatusBadSample) return fail(GZ_ERR_BAD_SAMPLE, "a sampled edge decoded to a vertex id >= V");
+  }
+  return GZ_OK;
+}
+
+int flush_all(gz_alg *h) {
+  GZ_TRY(push_staged_entries(h));
+  GZ_TRY(apply_pending(h));
+  GZ_CUDA(cudaStreamSynchronize(h->stream));
+  return check_status(h);
+}
+
+int mark_updated(gz_alg *h) {
+  if (h->update_locked || h->query_running.load()) return fail(GZ_ERR_LOCKED, "Cannot update the algorithm: Connected components currently running");
+  h->dsu_valid = false;  // NO_EAGER_DSU form of pre_insert
+  h->labels_on_host = false;
+  return GZ_OK;
+}
+
+// ---- Boruvka ---------------------------------------------------------------------------------------
+
+int ensure_query(gz_alg *h) {
+  auto &b = h->bv;
+  const size_t V = h->V;
+  GZ_TRY(dev_alloc(&b.parent, V));
+  GZ_TRY(dev_alloc(&b.label, V));
+  GZ_TRY(dev_alloc(&b.cnt, V));
+  GZ_TRY(dev_alloc(&b.fill, V));
+  GZ_TRY(dev_alloc(&b.minv, V));
+  GZ_TRY(dev_alloc(&b.packed, V));
+  GZ_TRY(dev_alloc(&b.scan_total, 1));
+  GZ_TRY(dev_alloc(&b.scan_tmp, gz::scan_tmp_words(V)));
+  GZ_TRY(dev_alloc(&b.order, V));
+  GZ_TRY(dev_alloc(&b.order_comp, V));
+  GZ_TRY(dev_alloc(&b.comp_start, V + 1));
+  GZ_TRY(dev_alloc(&b.comp_key, V));
+  GZ_TRY(dev_alloc(&b.ncomp, 1));
+  GZ_TRY(dev_alloc(&b.acc, V * (h->B + 1) * 3));
+  GZ_TRY(dev_alloc(&b.flags, 4));
+  GZ_TRY(dev_alloc(&b.forest, V));
+  GZ_TRY(dev_alloc(&b.forest_n, 1));
+  GZ_TRY(dev_alloc(&b.trace_n, 1));
+  GZ_TRY(dev_alloc(&h->d_final, V));
+  GZ_TRY(dev_alloc(&h->d_ncc, 1));
+  b.status = h->d_status;
+  if (h->trace && !b.trace) {
+    const size_t cap = V * (size_t)(h->C + 1);
+    void *p = nullptr;
+    GZ_CUDA(cudaMalloc(&p, cap * sizeof(gz_trace_rec_t)));
+    b.trace = p;
+    b.trace_cap = (uint32_t)std::min<size_t>(cap, 0xffffffffu);
+  }
+  if (!h->trace) {
+    if (b.trace) cudaFree(b.trace);
+    b.trace = nullptr;
+    b.trace_cap = 0;
+  }
+  return GZ_OK;
+}
+
+int read_modified(gz_alg *h, bool &modified) {
+  GZ_CUDA(cudaMemcpyAsync(h->h_status + 1, h->bv.flags, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+  GZ_CUDA(cudaStreamSynchronize(h->stream));
+  modified = h->h_status[1] != 0;
+  return GZ_OK;
+}
+
+// boruvka_emulation (src/cc_sketch_alg.cpp:464-513) driven from the host, one device round per
+// iteration until a round neither FAILs nor merges.
+int run_boruvka(gz_alg *h) {
+  GZ_TRY(ensure_query(h));
+  h->update_locked = true;  // stays set if the query fails, as in the reference
+  const gz::BoruvkaGeom g = h->bgeom();
+  auto &b = h->bv;
+  const int pi = h->prof_begin();
+  GZ_CUDA(gz::boruvka_reset(g, b, h->stream));
+  GZ_CUDA(cudaMemsetAsync(b.flags, 0, sizeof(uint32_t), h->stream));
+  GZ_CUDA(gz::boruvka_round0(g, h->d_sk, b, h->stream));
+  bool modified = false;
+  GZ_TRY(read_modified(h, modified));
+  uint32_t round = 0;
+  while (modified) {
+    ++round;
+    if (round >= h->C) {
+      h->prof_end(pi, 2);
+      h->last_rounds = round;
+      return fail(GZ_ERR_OUT_OF_SAMPLES,
+                  "This sketch (seed=" + std::to_string(h->seed) + ", max samples=" +
+                      std::to_string(h->C) + ") cannot be sampled more times (cur idx=" +
+                      std::to_string(round) + ")!");
+    }
+    GZ_CUDA(cudaMemsetAsync(b.flags, 0, sizeof(uint32_t), h->stream));
+    GZ_CUDA(gz::boruvka_round(g, round, h->d_sk, b, h->trace, h->stream));
+    GZ_TRY(read_modified(h, modified));
+  }
+  GZ_CUDA(gz::boruvka_final(g, b, h->d_final, h->d_ncc, h->stream));
+  h->prof_end(pi, 2);
+  h->prof_acc.query_rounds += round + 1;
+  GZ_CUDA(cudaMemcpyAsync(h->h_status + 2, h->d_ncc, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+  GZ_TRY(check_status(h));
+  h->last_ncc = h->h_status[2];
+  h->last_rounds = round;
+  h->dsu_valid = true;
+  h->labels_on_host = false;
+  h->update_locked = false;
+  return GZ_OK;
+}
+
+// The partition: either the cached one or a fresh Boruvka. Identity when nothing was ever
+// inserted (a fresh CCSketchAlg starts with a valid, empty DSU).
+int ensure_answer(gz_alg *h) {
+  GZ_TRY(flush_all(h));
+  if (h->dsu_valid && h->d_final) return GZ_OK;
+  if (h->dsu_valid) {
+    GZ_TRY(ensure_query(h));
+    GZ_CUDA(gz::boruvka_reset(h->bgeom(), h->bv, h->stream));
+    GZ_CUDA(gz::boruvka_final(h->bgeom(), h->bv, h->d_final, h->d_ncc, h->stream));
+    GZ_CUDA(cudaMemcpyAsync(h->h_status + 2, h->d_ncc, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+    GZ_CUDA(cudaStreamSynchronize(h->stream));
+    h->last_ncc = h->h_status[2];
+    return GZ_OK;
+  }
+  h->query_running = true;
+  const int rc = run_boruvka(h);
+  h->query_running = false;
+  return rc;
+}
+
+int labels_to_host(gz_alg *h) {
+  if (h->labels_on_host) return GZ_OK;
+  h->h_labels.resize(h->V);
+  GZ_CUDA(cudaMemcpyAsync(h->h_labels.data(), h->d_final, sizeof(uint32_t) * h->V, cudaMemcpyDeviceToHost, h->stream));
+  GZ_CUDA(cudaStreamSynchronize(h->stream));
+  h->labels_on_host = true;
+  return GZ_OK;
+}
+
+struct Guard {
+  gz_alg *h;
+  std::lock_guard<std::mutex> lk;
+  explicit Guard(gz_alg *a) : h(a), lk(a->mtx) { cudaSetDevice(a->device); }
+};
+
+}  // namespace
+
+// =================================================================================================
+// C ABI
+// =================================================================================================
+extern "C" {
+
+const char *gz_version(void) { return "graphzeppelin_b200 0.1.0 (sm_100a)"; }
+
+const char *gz_status_string(int s) {
+  switch (s) {
+    case GZ_OK: return "ok";
+    case GZ_ERR_INVALID: return "invalid argument";
+    case GZ_ERR_CUDA: return "CUDA error";
+    case GZ_ERR_OUT_OF_SAMPLES: return "out of samples";
+    case GZ_ERR_LOCKED: return "updates locked";
+    case GZ_ERR_BAD_VERTEX: return "vertex id out of range";
+    case GZ_ERR_NOMEM: return "out of memory";
+    case GZ_ERR_IO: return "I/O error";
+    case GZ_ERR_TIMEOUT: return "device wait timed out";
+    case GZ_ERR_BAD_SAMPLE: return "sampled edge out of range";
+    case GZ_ERR_NO_DEVICE: return "no CUDA device";
+    default: return "unknown status";
+  }
+}
+
+const char *gz_last_error(void) { return g_last_error.c_str(); }
+
+int gz_create(uint32_t num_vertices, uint64_t seed, double sketches_factor, double batch_factor,
+              gz_alg_t **out) {
+  if (!out) return fail(GZ_ERR_INVALID, "out is null");
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(GZ_ERR_NO_DEVICE, "no CUDA device is available (this library has no CPU path)");
+  gz_alg *h = new gz_alg();
+  const int rc = init_alg(h, num_vertices, seed, sketches_factor, batch_factor);
+  if (rc != GZ_OK) {
+    destroy_alg(h);
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return GZ_OK;
+}
+
+int gz_create_from_serialized(const char *path, double batch_factor, gz_alg_t **out) {
+  if (!path || !out) return fail(GZ_ERR_INVALID, "null argument");
+  *out = nullptr;
+  FILE *f = fopen(path, "rb");
+  if (!f) return fail(GZ_ERR_IO, std::string("cannot open ") + path);
+  uint64_t seed = 0;
+  uint32_t V = 0;
+  double sf = 0;
+  if (fread(&seed, 8, 1, f) != 1 || fread(&V, 4, 1, f) != 1 || fread(&sf, 8, 1, f) != 1) {
+    fclose(f);
+    return fail(GZ_ERR_IO, "truncated header");
+  }
+  gz_alg_t *h = nullptr;
+  int rc = gz_create(V, seed, sf, batch_factor, &h);
+  if (rc != GZ_OK) {
+    fclose(f);
+    return rc;
+  }
+  std::vector<uint8_t> buf((size_t)h->sketch_bytes * V);
+  const size_t got = fread(buf.data(), 1, buf.size(), f);
+  fclose(f);
+  if (got != buf.size()) {
+    gz_destroy(h);
+    return fail(GZ_ERR_IO, "truncated sketch data");
+  }
+  cudaError_t e = cudaMemcpy(h->d_sk, buf.data(), buf.size(), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    gz_destroy(h);
+    return fail(GZ_ERR_CUDA, cudaGetErrorString(e));
+  }
+  h->dsu_valid = false;  // src/cc_sketch_alg.cpp:62-63
+  *out = h;
+  return GZ_OK;
+}
+
+int gz_destroy(gz_alg_t *h) {
+  if (!h) return GZ_OK;
+  cudaSetDevice(h->device);
+  destroy_alg(h);
+  delete h;
+  return GZ_OK;
+}
+
+int gz_get_params(const gz_alg_t *h, gz_params_t *o) {
+  if (!h || !o) return fail(GZ_ERR_INVALID, "null argument");
+  o->num_vertices = h->V;
+  o->num_columns = h->C;
+  o->bkt_per_col = h->B;
+  o->num_buckets = h->nb;
+  o->seed = h->seed;
+  o->sketch_bytes = h->sketch_bytes;
+  o->desired_updates_per_batch = h->desired_batch;
+  o->max_rounds = h->C;
+  o->sketches_factor = h->sketches_factor;
+  o->batch_factor = h->batch_factor;
+  o->vertices_per_tile = 1u << h->tile_shift;
+  o->num_tiles = h->ntiles;
+  return GZ_OK;
+}
+
+int gz_set_gutter_capacity(gz_alg_t *h, uint64_t n) {
+  if (!h || n < 2) return fail(GZ_ERR_INVALID, "capacity must be >= 2");
+  Guard g(h);
+  GZ_TRY(push_staged_entries(h));
+  GZ_TRY(apply_pending(h));
+  GZ_CUDA(cudaStreamSynchronize(h->stream));
+  dev_free(h->d_entries);
+  h->entry_cap = n;
+  return GZ_OK;
+}
+
+int gz_allocate_worker_memory(gz_alg_t *h, size_t num_workers) {
+  if (!h) return fail(GZ_ERR_INVALID, "null handle");
+  h->num_workers = std::max<size_t>(1, num_workers);
+  return GZ_OK;
+}
+
+int gz_pre_insert(gz_alg_t *h, uint32_t, uint32_t, int, int) {
+  if (!h) return fail(GZ_ERR_INVALID, "null handle");
+  Guard g(h);
+  h->dsu_valid = false;
+  h->labels_on_host = false;
+  return GZ_OK;
+}
+
+int gz_apply_update_batch(gz_alg_t *h, int, uint32_t src, const uint32_t *dsts, size_t n) {
+  if (!h || (n && !dsts)) return fail(GZ_ERR_INVALID, "null argument");
+  if (h->query_running.load()) return fail(GZ_ERR_LOCKED, "Cannot update the algorithm: Connected components currently running");
+  Guard g(h);
+  GZ_TRY(mark_updated(h));
+  if (src >= h->V) return fail(GZ_ERR_BAD_VERTEX, "src vertex id >= V");
+  for (size_t i = 0; i < n; ++i) {
+    if (dsts[i] >= h->V) return fail(GZ_ERR_BAD_VERTEX, "dst vertex id >= V");
+  }
+  for (size_t i = 0; i < n; ++i) GZ_TRY(stage_entry(h, src, dsts[i]));
+  return GZ_OK;
+}
+
+int gz_apply_raw_buckets_update(gz_alg_t *h, uint32_t src, const void *raw) {
+  if (!h || !raw) return fail(GZ_ERR_INVALID, "null argument");
+  Guard g(h);
+  if (src >= h->V) return fail(GZ_ERR_BAD_VERTEX, "src vertex id >= V");
+  h->dsu_valid = false;
+  h->labels_on_host = false;
+  GZ_TRY(dev_alloc(&h->d_raw, (size_t)h->nb * 3));
+  GZ_CUDA(cudaMemcpyAsync(h->d_raw, raw, h->sketch_bytes, cudaMemcpyHostToDevice, h->stream));
+  GZ_CUDA(gz::sketch_xor_raw(h->d_sk, h->nb * 3, src, h->d_raw, h->stream));
+  GZ_CUDA(cudaStreamSynchronize(h->stream));
+  return GZ_OK;
+}
+
+int gz_update(gz_alg_t *h, uint32_t src, uint32_t dst, int) {
+  if (!h) return fail(GZ_ERR_INVALID, "null handle");
+  if (h->query_running.load()) return fail(GZ_ERR_LOCKED, "Cannot update the algorithm: Connected components currently running");
+  Guard g(h);
+  GZ_TRY(mark_updated(h));
+  if (src >= h->V || dst >= h->V) return fail(GZ_ERR_BAD_VERTEX, "vertex id >= V");
+  GZ_TRY(stage_entry(h, src, dst));
+  GZ_TRY(stage_entry(h, dst, src));
+  return GZ_OK;
+}
+
+int gz_ingest_records_device(gz_alg_t *h, const void *d_rec, size_t n) {
+  if (!h || (n && !d_rec)) return fail(GZ_ERR_INVALID, "null argument");
+  if (h->query_running.load()) return fail(GZ_ERR_LOCKED, "Cannot update the algorithm: Connected components currently running");
+  Guard g(h);
+  GZ_TRY(mark_updated(h));
+  return gutter_chunk(h, gz::kInputRecords, d_rec, n);
+}
+
+int gz_ingest_records(gz_alg_t *h, const void *rec, size_t n) {
+  if (!h || (n && !rec)) return fail(GZ_ERR_INVALID, "null argument");
+  if (h->query_running.load()) return fail(GZ_ERR_LOCKED, "Cannot update the algorithm: Connected components currently running");
+  Guard g(h);
+  GZ_TRY(mark_updated(h));
+  if (n == 0) return GZ_OK;
+  const uint64_t chunk = std::min<uint64_t>(kStageRecords, n);
+  for (int i = 0; i < 2; ++i) {
+    if (!h->d_stage[i]) {
+      GZ_TRY(dev_alloc(&h->d_stage[i], kStageRecords * 9 + 16));
+      GZ_CUDA(cudaEventCreateWithFlags(&h->ev_copied[i], cudaEventDisableTiming));
+      GZ_CUDA(cudaEventCreateWithFlags(&h->ev_free[i], cudaEventDisableTiming));
+      GZ_CUDA(cudaEventRecord(h->ev_free[i], h->stream));
+    }
+  }
+  const uint8_t *src = static_cast<const uint8_t *>(rec);
+  int buf = 0;
+  for (uint64_t off = 0; off < n; off += chunk, buf ^= 1) {
+    const uint64_t m = std::min<uint64_t>(chunk, n - off);
+    GZ_CUDA(cudaStreamWaitEvent(h->copy_stream, h->ev_free[buf], 0));
+    GZ_CUDA(cudaMemcpyAsync(h->d_stage[buf], src + off * 9, m * 9, cudaMemcpyHostToDevice, h->copy_stream));
+    GZ_CUDA(cudaEventRecord(h->ev_copied[buf], h->copy_stream));
+    GZ_CUDA(cudaStreamWaitEvent(h->stream, h->ev_copied[buf], 0));
+    GZ_TRY(gutter_chunk(h, gz::kInputRecords, h->d_stage[buf], m));
+    GZ_CUDA(cudaEventRecord(h->ev_free[buf], h->stream));
+  }
+  // the caller's buffer may be reused once every copy has landed
+  GZ_CUDA(cudaStreamSynchronize(h->copy_stream));
+  return GZ_OK;
+}
+
+int gz_flush(gz_alg_t *h) {
+  if (!h) return fail(GZ_ERR_INVALID, "null handle");
+  Guard g(h);
+  return flush_all(h);
+}
+
+int gz_has_cached_query(const gz_alg_t *h, int code, int *out) {
+  if (!h || !out) return fail(GZ_ERR_INVALID, "null argument");
+  *out = code == GZ_CONNECTIVITY ? (h->dsu_valid ? 1 : 0) : 0;
+  return GZ_OK;
+}
+
+int gz_connected_components(gz_alg_t *h, uint32_t *parent_out, uint32_t *num_cc) {
+  if (!h) return fail(GZ_ERR_INVALID, "null handle");
+  Guard g(h);
+  GZ_TRY(ensure_answer(h));
+  if (num_cc) *num_cc = h->last_ncc;
+  if (parent_out) {
+    GZ_CUDA(cudaMemcpyAsync(parent_out, h->d_final, sizeof(uint32_t) * h->V, cudaMemcpyDeviceToHost, h->stream));
+    GZ_CUDA(cudaStreamSynchronize(h->stream));
+  }
+  return GZ_OK;
+}
+
+int gz_point_query(gz_alg_t *h, uint32_t a, uint32_t b, int *out) {
+  if (!h || !out) return fail(GZ_ERR_INVALID, "null argument");
+  Guard g(h);
+  if (a >= h->V || b >= h->V) return fail(GZ_ERR_BAD_VERTEX, "vertex id >= V");
+  GZ_TRY(ensure_answer(h));
+  GZ_TRY(labels_to_host(h));
+  *out = h->h_labels[a] == h->h_labels[b] ? 1 : 0;
+  return GZ_OK;
+}
+
+int gz_last_query_rounds(const gz_alg_t *h, size_t *out) {
+  if (!h || !out) return fail(GZ_ERR_INVALID, "null argument");
+  *out = h->last_rounds;
+  return GZ_OK;
+}
+
+int gz_spanning_forest(gz_alg_t *h, uint32_t *edges_out, size_t cap, size_t *n_edges) {
+  if (!h || !n_edges) return fail(GZ_ERR_INVALID, "null argument");
+  Guard g(h);
+  GZ_TRY(ensure_answer(h));
+  uint32_t n = 0;
+  GZ_CUDA(cudaMemcpyAsync(h->h_status + 3, h->bv.forest_n, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+  GZ_CUDA(cudaStreamSynchronize(h->stream));
+  n = std::min<uint32_t>(h->h_status[3], h->V);
+  *n_edges = n;
+  if (edges_out && cap) {
+    std::vector<uint64_t> idx(n);
+    if (n) GZ_CUDA(cudaMemcpy(idx.data(), h->bv.forest, n * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < std::min<size_t>(cap, n); ++i) {
+      edges_out[2 * i] = (uint32_t)(idx[i] >> 32);
+      edges_out[2 * i + 1] = (uint32_t)idx[i];
+    }
+  }
+  return GZ_OK;
+}
+
+int gz_dump_sketches(gz_alg_t *h, void *buf, size_t bytes) {
+  if (!h || !buf) return fail(GZ_ERR_INVALID, "null argument");
+  Guard g(h);
+  if (bytes != h->sketch_bytes * h->V) return fail(GZ_ERR_INVALID, "buffer must hold V * sketch_bytes bytes");
+  GZ_TRY(flush_all(h));
+  GZ_CUDA(cudaMemcpyAsync(buf, h->d_sk, bytes, cudaMemcpyDeviceToHost, h->stream));
+  GZ_CUDA(cudaStreamSynchronize(h->stream));
+  return GZ_OK;
+}
+
+int gz_write_binary(gz_alg_t *h, const char *path) {
+  if (!h || !path) return fail(GZ_ERR_INVALID, "null argument");
+  std::vector<uint8_t> buf((size_t)h->sketch_bytes * h->V);
+  GZ_TRY(gz_dump_sketches(h, buf.data(), buf.size()));
+  FILE *f = fopen(path, "wb");
+  if (!f) return fail(GZ_ERR_IO, std::string("cannot open ") + path);
+  const uint64_t seed = h->seed;
+  const uint32_t V = h->V;
+  const double sf = h->sketches_factor;
+  bool ok = fwrite(&seed, 8, 1, f) == 1 && fwrite(&V, 4, 1, f) == 1 && fwrite(&sf, 8, 1, f) == 1 &&
+            fwrite(buf.data(), 1, buf.size(), f) == buf.size();
+  ok = (fclose(f) == 0) && ok;
+  return ok ? GZ_OK : fail(GZ_ERR_IO, "short write");
+}
+
+int gz_set_trace(gz_alg_t *h, int enable) {
+  if (!h) return fail(GZ_ERR_INVALID, "null handle");
+  Guard g(h);
+  h->trace = enable != 0;
+  return GZ_OK;
+}
+
+int gz_get_trace(gz_alg_t *h, gz_trace_rec_t *out, size_t cap, size_t *len) {
+  if (!h || !len) return fail(GZ_ERR_INVALID, "null argument");
+  Guard g(h);
+  *len = 0;
+  if (!h->bv.trace) return GZ_OK;
+  GZ_CUDA(cudaMemcpyAsync(h->h_status + 3, h->bv.trace_n, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+  GZ_CUDA(cudaStreamSynchronize(h->stream));
+  const size_t n = std::min<size_t>(h->h_status[3], h->bv.trace_cap);
+  *len = n;
+  if (out && cap) GZ_CUDA(cudaMemcpy(out, h->bv.trace, std::min(cap, n) * sizeof(gz_trace_rec_t), cudaMemcpyDeviceToHost));
+  return GZ_OK;
+}
+
+int gz_set_profiling(gz_alg_t *h, int enable) {
+  if (!h) return fail(GZ_ERR_INVALID, "null handle");
+  Guard g(h);
+  h->prof_collect();
+  h->prof = enable != 0;
+  h->prof_acc = gz_profile_t{};
+  h->launch_base = gz::launch_count();
+  return GZ_OK;
+}
+
+int gz_get_profile(gz_alg_t *h, gz_profile_t *out) {
+  if (!h || !out) return fail(GZ_ERR_INVALID, "null argument");
+  Guard g(h);
+  h->prof_collect();
+  *out = h->prof_acc;
+  out->kernel_launches = gz::launch_count() - h->launch_base;
+  return GZ_OK;
+}
+
+int gz_clear(gz_alg_t *h) {
+  if (!h) return fail(GZ_ERR_INVALID, "null handle");
+  if (h->query_running.load()) return fail(GZ_ERR_LOCKED, "Cannot update the algorithm: Connected components currently running");
+  Guard g(h);
+  if (h->update_locked) return fail(GZ_ERR_LOCKED, "Cannot update the algorithm: Connected components currently running");
+  h->nchunks = 0;
+  h->entry_used = 0;
+  h->h_ent_n = 0;
+  const uint64_t v_pad = ((uint64_t)h->V + 63) & ~63ull;
+  GZ_CUDA(cudaMemsetAsync(h->d_sk, 0, v_pad * h->sketch_bytes, h->stream));
+  h->dsu_valid = false;
+  h->labels_on_host = false;
+  return GZ_OK;
+}
+
+int gz_measure_hash_rate(int repeats, double *hashes_per_s) {
+  if (!hashes_per_s || repeats < 1) return fail(GZ_ERR_INVALID, "bad argument");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(GZ_ERR_NO_DEVICE, "no CUDA device");
+  const int threads = 256, blocks = gz::num_sms() * 8;
+  const uint32_t iters = 4096;
+  uint64_t *out = nullptr;
+  GZ_CUDA(cudaMalloc(&out, sizeof(uint64_t) * threads * blocks));
+  cudaStream_t s = nullptr;
+  GZ_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  double best = 0;
+  gz::hash_peak(1, 16, blocks, threads, out, s);  // warm-up
+  for (int r = 0; r < repeats; ++r) {
+    cudaEventRecord(a, s);
+    gz::hash_peak(12345 + r, iters, blocks, threads, out, s);
+    cudaEventRecord(b, s);
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    const double rate = (double)threads * blocks * iters * 8 / (ms * 1e-3);
+    best = std::max(best, rate);
+  }
+  cudaError_t e = cudaGetLastError();
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaStreamDestroy(s);
+  cudaFree(out);
+  if (e != cudaSuccess) return fail(GZ_ERR_CUDA, cudaGetErrorString(e));
+  *hashes_per_s = best;
+  return GZ_OK;
+}
+
+int gz_get_stream(gz_alg_t *h, void **s) {
+  if (!h || !s) return fail(GZ_ERR_INVALID, "null argument");
+  *s = (void *)h->stream;
+  return GZ_OK;
+}
+
+int gz_set_tuning(gz_alg_t *h, uint32_t vpt, uint32_t threads) {
+  if (!h) return fail(GZ_ERR_INVALID, "null handle");
+  Guard g(h);
+  GZ_TRY(push_staged_entries(h));
+  GZ_TRY(apply_pending(h));
+  GZ_CUDA(cudaStreamSynchronize(h->stream));
+  const uint32_t old_nt = h->ntiles;
+  GZ_TRY(choose_tiling(h, vpt, threads));
+  if (h->ntiles != old_nt) {
+    dev_free(h->d_tile_off);
+    dev_free(h->d_hist);
+    dev_free(h->d_scan_tmp);
+    h->hist_words = 0;
+  }
+  return GZ_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,65 @@
+// gz_device.cuh -- device-side building blocks shared by the ingest and query kernels.
+//
+// Hashing: XXH3_64bits_withSeed of one 8-byte little-endian value (xxHash 0.8.x, path
+// XXH3_len_4to8_64b + XXH3_rrmxmx), which the reference calls through vec_hash / col_hash
+// (include/types.h:8-9) for the bucket checksum (include/bucket.h:61-63) and the per-column depth
+// (include/bucket.h:54-59). For an 8-byte input the seed only enters through one 64-bit constant
+// ("flip" below), so the host precomputes flip for the checksum seed and for every column seed
+// (seed + 5*col, include/sketch.h:175-176) and the device evaluates rrmxmx(swap32x2(idx) ^ flip).
+#pragma once
+#include <cstdint>
+
+namespace gz {
+
+// Bucket {u64 alpha; u32 gamma} packed to 12 bytes (include/bucket.h:7-12), seen as 3 words:
+// w0 = low 32 bits of alpha, w1 = high 32 bits of alpha, w2 = gamma.
+constexpr int kBucketBytes = 12;
+constexpr int kMaxBktPerCol = 64;
+
+// XXH3 default-secret words at byte offsets 8 and 16, and the rrmxmx multiplier.
+constexpr uint64_t kSecret8 = 0x1cad21f72c81017cULL;
+constexpr uint64_t kSecret16 = 0xdb979083e96dd4deULL;
+constexpr uint64_t kPrimeMx2 = 0x9FB21C651E98DF25ULL;
+
+// Seed-dependent constant of the 8-byte path: bitflip = (secret[8..16) ^ secret[16..24)) - seed',
+// seed' = seed ^ (bswap32(lo32(seed)) << 32).
+__host__ __device__ inline uint64_t xxh3_flip(uint64_t seed) {
+  uint32_t lo = (uint32_t)seed;
+  uint32_t sw = (lo >> 24) | ((lo >> 8) & 0xff00u) | ((lo << 8) & 0xff0000u) | (lo << 24);
+  uint64_t s = seed ^ ((uint64_t)sw << 32);
+  return (kSecret8 ^ kSecret16) - s;
+}
+
+__host__ __device__ inline uint64_t rrmxmx8(uint64_t h) {
+  h ^= ((h << 49) | (h >> 15)) ^ ((h << 24) | (h >> 40));
+  h *= kPrimeMx2;
+  h ^= (h >> 35) + 8;
+  h *= kPrimeMx2;
+  return h ^ (h >> 28);
+}
+
+// Hash of edge index idx = (hi << 32) | lo. The 8-byte path reads the input as two LE32 words
+// and recombines them swapped: input64 = (lo << 32) | hi.
+__host__ __device__ inline uint64_t hash_idx(uint32_t lo, uint32_t hi, uint64_t flip) {
+  return rrmxmx8((((uint64_t)lo << 32) | hi) ^ flip);
+}
+
+// Bucket_Boruvka::is_good (include/bucket.h:65-67): gamma == (u32) hash(alpha, checksum seed).
+__host__ __device__ inline bool bucket_good(uint32_t w0, uint32_t w1, uint32_t w2,
+                                            uint64_t flip_chk) {
+  return w2 == (uint32_t)hash_idx(w0, w1, flip_chk);
+}
+
+#ifdef __CUDACC__
+// depth = ctz(hash | 1 << B) (get_index_depth), B <= 64.
+__device__ __forceinline__ uint32_t depth_of(uint64_t h, uint32_t B) {
+  uint64_t x = h | (B < 64 ? (1ull << B) : 0ull);
+  return (uint32_t)(__ffsll((long long)x) - 1);
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+#endif
+
+}  // namespace gz

@@ -1,0 +1,900 @@
+// gz_kernels.cu -- sm_100a kernels of the sketch-ingest and Boruvka-query path.
+//
+//   device gutter   : 9-byte records -> per-tile endpoint entries (counting sort by vertex tile)
+//                     (replaces the GutteringSystem + driver reader threads,
+//                      include/graph_sketch_driver.h:148-179)
+//   sketch update   : per tile, sketches staged in shared memory by bulk async copies, every
+//                     entry hashed per column and XORed in with shared-memory atomics
+//                     (Sketch::update src/sketch.cpp:69-83 + apply_update_batch
+//                      src/cc_sketch_alg.cpp:106-118)
+//   Boruvka         : per-component sample, lock-free CAS union-find with path halving,
+//                     segmented XOR merge of column r (boruvka_emulation and friends,
+//                     src/cc_sketch_alg.cpp:137-513; DisjointSetUnion_MT include/dsu.h:101-174)
+//
+// All work is integer / XOR; results are bit-identical to the reference CPU build.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstdint>
+
+#include "gz_device.cuh"
+#include "gz_kernels.cuh"
+
+namespace gz {
+
+namespace {
+
+constexpr uint32_t kFull = 0xffffffffu;
+std::atomic<uint64_t> g_launches{0};  // kernel launches issued from this file
+
+// ------------------------------------------------------------------------------------------------
+// small PTX helpers (bulk async copy + mbarrier)
+// ------------------------------------------------------------------------------------------------
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Bounded wait on an mbarrier phase: gives up after limit_ns of wall time.
+__device__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity, uint64_t limit_ns) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  for (uint32_t it = 1; it < (1u << 30); ++it) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((it & 31u) == 0 && global_ns() - t0 > limit_ns) return false;
+  }
+  return false;
+}
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes,
+                                         uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(dst),
+      "l"(src), "r"(bytes), "r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ void bulk_s2g(void *dst, uint32_t src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(src),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() {
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait_read_all() {
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait_all() {
+  asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+constexpr uint32_t kBulkPiece = 32768;       // bytes per bulk copy instruction
+constexpr uint64_t kWaitLimitNs = 2000000000;  // 2 s bound on any device-side wait
+
+// ------------------------------------------------------------------------------------------------
+// record staging: coalesced 128-bit loads of a range of packed 9-byte records into shared memory
+// ------------------------------------------------------------------------------------------------
+constexpr uint32_t kRecStageBytes = kRecTile * 9 + 48;
+
+// Loads records [r, r + cnt) into s. Shared byte k mirrors global byte align16(start) + k.
+// Whole 16-byte blocks inside the range use one 128-bit load; the partial first/last block is
+// read byte by byte so no byte outside the caller's range is touched. Returns the offset of
+// record r inside s.
+__device__ __forceinline__ uint32_t stage_records(const uint8_t *base, uint64_t r, uint32_t cnt,
+                                                  uint8_t *s) {
+  const uintptr_t start = (uintptr_t)(base + r * 9);
+  const uintptr_t end = start + (uintptr_t)cnt * 9;
+  const uintptr_t a0 = start & ~(uintptr_t)15;
+  const uint32_t nvec = (uint32_t)((((end + 15) & ~(uintptr_t)15) - a0) >> 4);
+  for (uint32_t i = threadIdx.x; i < nvec; i += blockDim.x) {
+    const uintptr_t blk = a0 + ((uintptr_t)i << 4);
+    if (blk >= start && blk + 16 <= end) {
+      *reinterpret_cast<uint4 *>(s + i * 16) = __ldcs(reinterpret_cast<const uint4 *>(blk));
+    } else {
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        const uintptr_t p = blk + k;
+        if (p >= start && p < end) s[i * 16 + k] = *reinterpret_cast<const uint8_t *>(p);
+      }
+    }
+  }
+  return (uint32_t)(start - a0);
+}
+
+// src / dst of staged record i (the type byte is not needed).
+__device__ __forceinline__ void parse_record(const uint8_t *s, uint32_t shift, uint32_t i,
+                                             uint32_t &u, uint32_t &v) {
+  const uint32_t off = shift + 9 * i + 1;
+  const uint32_t *w = reinterpret_cast<const uint32_t *>(s) + (off >> 2);
+  const uint32_t sh = (off & 3) * 8;
+  u = __funnelshift_r(w[0], w[1], sh);
+  v = __funnelshift_r(w[1], w[2], sh);
+}
+
+// ------------------------------------------------------------------------------------------------
+// device gutter
+// ------------------------------------------------------------------------------------------------
+template <int INPUT, bool COUNT, bool SMEM>
+__global__ void __launch_bounds__(512)
+k_gutter(const void *__restrict__ in, uint64_t n, GutterGeom g, uint64_t *__restrict__ hist,
+         uint2 *__restrict__ entries, uint32_t *__restrict__ status) {
+  extern __shared__ __align__(16) uint8_t gsm[];
+  uint32_t *s_bin = reinterpret_cast<uint32_t *>(gsm);
+  const uint32_t nt_pad = (g.ntiles + 3) & ~3u;
+  uint8_t *s_rec = gsm + (SMEM ? nt_pad * 4 : 0);
+  const uint32_t G = gridDim.x, cta = blockIdx.x;
+  if (SMEM) {
+    for (uint32_t b = threadIdx.x; b < g.ntiles; b += blockDim.x)
+      s_bin[b] = COUNT ? 0u : (uint32_t)hist[(uint64_t)b * G + cta];
+    __syncthreads();
+  }
+  const uint64_t r0 = n * cta / G, r1 = n * (cta + 1) / G;
+  bool bad = false;
+  auto emit = [&](uint32_t v, uint32_t w) {
+    const uint32_t t = v >> g.tile_shift;
+    if (COUNT) {
+      if (SMEM) atomicAdd(&s_bin[t], 1u);
+      else atomicAdd(reinterpret_cast<unsigned long long *>(&hist[t]), 1ull);
+    } else {
+      uint64_t p;
+      if (SMEM) p = atomicAdd(&s_bin[t], 1u);
+      else p = atomicAdd(reinterpret_cast<unsigned long long *>(&hist[t]), 1ull);
+      entries[p] = make_uint2(v, w);
+    }
+  };
+  if (INPUT == kInputRecords) {
+    const uint8_t *rec = reinterpret_cast<const uint8_t *>(in);
+    for (uint64_t t = r0; t < r1; t += kRecTile) {
+      const uint32_t cnt = (uint32_t)(r1 - t < (uint64_t)kRecTile ? r1 - t : (uint64_t)kRecTile);
+      const uint32_t shift = stage_records(rec, t, cnt, s_rec);
+      __syncthreads();
+      for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
+        uint32_t u, v;
+        parse_record(s_rec, shift, i, u, v);
+        if (u >= g.V || v >= g.V) {
+          bad = true;
+          continue;
+        }
+        emit(u, v);
+        emit(v, u);
+      }
+      __syncthreads();
+    }
+  } else {
+    const uint2 *e = reinterpret_cast<const uint2 *>(in);
+    for (uint64_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+      const uint2 x = e[i];
+      if (x.x >= g.V || x.y >= g.V) {
+        bad = true;
+        continue;
+      }
+      emit(x.x, x.y);
+    }
+  }
+  if (COUNT && SMEM) {
+    __syncthreads();
+    for (uint32_t b = threadIdx.x; b < g.ntiles; b += blockDim.x)
+      hist[(uint64_t)b * G + cta] = s_bin[b];
+  }
+  if (COUNT && bad) atomicOr(status, kStatusBadVertex);
+}
+
+size_t gutter_smem(int input, GutterGeom g, bool smem) {
+  size_t s = smem ? ((g.ntiles + 3) & ~3u) * 4 : 0;
+  if (input == kInputRecords) s += kRecStageBytes;
+  return s;
+}
+
+template <int INPUT, bool COUNT, bool SMEM>
+cudaError_t launch_gutter(const void *in, uint64_t n, GutterGeom g, int G, uint64_t *hist,
+                          uint2 *entries, uint32_t *status, cudaStream_t s) {
+  const size_t smem = gutter_smem(INPUT, g, SMEM);
+  auto kern = k_gutter<INPUT, COUNT, SMEM>;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  kern<<<G, 512, smem, s>>>(in, n, g, hist, entries, status);
+  g_launches++;
+  return cudaGetLastError();
+}
+
+__global__ void k_tile_offsets(const uint64_t *scanned, uint32_t stride, uint32_t ntiles,
+                               const uint64_t *total, uint32_t *tile_off) {
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < ntiles) tile_off[b] = (uint32_t)scanned[(uint64_t)b * stride];
+  if (b == ntiles) tile_off[b] = (uint32_t)*total;
+}
+
+__global__ void k_copy_u64(const uint64_t *src, uint64_t *dst, uint64_t n) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    dst[i] = src[i];
+}
+
+// ------------------------------------------------------------------------------------------------
+// scan (exclusive, u64, in place)
+// ------------------------------------------------------------------------------------------------
+constexpr int kScanThreads = 512;
+constexpr int kScanItems = 8;
+constexpr uint64_t kScanBlock = (uint64_t)kScanThreads * kScanItems;
+
+__device__ __forceinline__ uint64_t block_exclusive(uint64_t x, uint64_t *block_total) {
+  __shared__ uint64_t ws[kScanThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint64_t inc = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint64_t y = __shfl_up_sync(kFull, inc, o);
+    if (lane >= o) inc += y;
+  }
+  if (lane == 31) ws[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    uint64_t w = lane < kScanThreads / 32 ? ws[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint64_t y = __shfl_up_sync(kFull, w, o);
+      if (lane >= o) w += y;
+    }
+    if (lane < kScanThreads / 32) ws[lane] = w;
+  }
+  __syncthreads();
+  const uint64_t before = warp ? ws[warp - 1] : 0;
+  *block_total = ws[kScanThreads / 32 - 1];
+  __syncthreads();
+  return before + inc - x;
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+k_scan_reduce(const uint64_t *__restrict__ d, uint64_t n, uint64_t *__restrict__ sums) {
+  const uint64_t base = blockIdx.x * kScanBlock + (uint64_t)threadIdx.x * kScanItems;
+  uint64_t s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k)
+    if (base + k < n) s += d[base + k];
+  uint64_t tot;
+  block_exclusive(s, &tot);
+  if (threadIdx.x == 0) sums[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+k_scan_down(uint64_t *__restrict__ d, uint64_t n, const uint64_t *__restrict__ prefix,
+            uint64_t *__restrict__ total) {
+  const uint64_t base = blockIdx.x * kScanBlock + (uint64_t)threadIdx.x * kScanItems;
+  uint64_t v[kScanItems];
+  uint64_t s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    v[k] = base + k < n ? d[base + k] : 0;
+    s += v[k];
+  }
+  uint64_t tot;
+  uint64_t run = block_exclusive(s, &tot) + (prefix ? prefix[blockIdx.x] : 0);
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    if (base + k < n) d[base + k] = run;
+    run += v[k];
+  }
+  if (total && blockIdx.x == gridDim.x - 1 && threadIdx.x == kScanThreads - 1) *total = run;
+}
+
+// ------------------------------------------------------------------------------------------------
+// sketch update
+// ------------------------------------------------------------------------------------------------
+// Folds one endpoint update (vertex v, neighbour w) into v's staged sketch: the deterministic
+// bucket always, then in each column the bucket at depth ctz(hash_c(idx) | 1 << B) when < B.
+__device__ __forceinline__ void apply_entry(uint2 e, uint32_t *s_sk, uint32_t vmask,
+                                            uint32_t sketch_words, const uint64_t *s_flip,
+                                            uint64_t flip_chk, uint32_t C, uint32_t B) {
+  const uint32_t v = e.x, w = e.y;
+  const uint32_t lo = max(v, w), hi = min(v, w);  // idx = (min << 32) | max
+  uint32_t *sk = s_sk + (v & vmask) * sketch_words;
+  const uint64_t in64 = ((uint64_t)lo << 32) | hi;
+  const uint32_t chk = (uint32_t)rrmxmx8(in64 ^ flip_chk);
+  uint32_t *det = sk + 3 * C * B;
+  atomicXor(det, lo);
+  atomicXor(det + 1, hi);
+  atomicXor(det + 2, chk);
+  for (uint32_t c = 0; c < C; ++c) {
+    const uint32_t d = depth_of(rrmxmx8(in64 ^ s_flip[c]), B);
+    if (d < B) {
+      uint32_t *bk = sk + 3 * (c * B + d);
+      atomicXor(bk, lo);
+      atomicXor(bk + 1, hi);
+      atomicXor(bk + 2, chk);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(1024, 1)
+k_sketch_update(SketchGeom g, uint8_t *__restrict__ sketches, const uint2 *__restrict__ entries,
+                ChunkTable chunks, const uint32_t *__restrict__ tile_off, int nchunks,
+                const uint64_t *__restrict__ flip, uint32_t *work_counter, uint32_t *status) {
+  extern __shared__ __align__(128) uint8_t dsm[];
+  __shared__ __align__(8) uint64_t s_bar;
+  __shared__ uint32_t s_tile, s_total;
+  const uint32_t vpt = 1u << g.tile_shift;
+  const uint32_t tile_bytes = vpt * g.sketch_words * 4;
+  uint32_t *s_sk = reinterpret_cast<uint32_t *>(dsm);
+  uint64_t *s_flip = reinterpret_cast<uint64_t *>(dsm + tile_bytes);
+  for (uint32_t i = threadIdx.x; i <= g.C; i += blockDim.x) s_flip[i] = flip[i];
+  const uint32_t bar = smem_u32(&s_bar);
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  const uint64_t flip_chk = s_flip[g.C];
+  const uint32_t stride = g.ntiles + 1;
+  uint32_t parity = 0;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const uint32_t t = atomicAdd(work_counter, 1u);
+      uint32_t total = 0;
+      if (t < g.ntiles)
+        for (int k = 0; k < nchunks; ++k)
+          total += tile_off[(uint64_t)k * stride + t + 1] - tile_off[(uint64_t)k * stride + t];
+      s_tile = t;
+      s_total = total;
+      if (t < g.ntiles && total) {
+        const uint8_t *src = sketches + (uint64_t)t * tile_bytes;
+        mbar_expect_tx(bar, tile_bytes);
+        for (uint32_t off = 0; off < tile_bytes; off += kBulkPiece)
+          bulk_g2s(smem_u32(dsm) + off, src + off, min(kBulkPiece, tile_bytes - off), bar);
+      }
+    }
+    __syncthreads();
+    const uint32_t t = s_tile;
+    if (t >= g.ntiles) break;
+    if (s_total) {
+      const bool ok = mbar_wait_bounded(bar, parity, kWaitLimitNs);
+      parity ^= 1u;
+      if (__syncthreads_or(!ok)) {
+        // the staged copy never completed: report it and leave without touching the tile
+        if (threadIdx.x == 0) {
+          atomicOr(status, kStatusTimeout);
+          mbar_wait_bounded(bar, parity ^ 1u, kWaitLimitNs);
+        }
+        return;
+      }
+      for (int k = 0; k < nchunks; ++k) {
+        const uint64_t b = chunks.base[k] + tile_off[(uint64_t)k * stride + t];
+        const uint64_t e = chunks.base[k] + tile_off[(uint64_t)k * stride + t + 1];
+        for (uint64_t i = b + threadIdx.x; i < e; i += blockDim.x)
+          apply_entry(entries[i], s_sk, vpt - 1, g.sketch_words, s_flip, flip_chk, g.C, g.B);
+      }
+      fence_proxy_async_smem();
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        uint8_t *dst = sketches + (uint64_t)t * tile_bytes;
+        for (uint32_t off = 0; off < tile_bytes; off += kBulkPiece)
+          bulk_s2g(dst + off, smem_u32(dsm) + off, min(kBulkPiece, tile_bytes - off));
+        bulk_commit();
+        bulk_wait_read_all();
+      }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) bulk_wait_all();
+}
+
+__global__ void k_sketch_xor_raw(uint32_t *sketches, uint32_t words, uint32_t v,
+                                 const uint32_t *raw) {
+  uint32_t *sk = sketches + (uint64_t)v * words;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < words; i += gridDim.x * blockDim.x)
+    sk[i] ^= raw[i];
+}
+
+// ------------------------------------------------------------------------------------------------
+// Boruvka
+// ------------------------------------------------------------------------------------------------
+struct TraceRec {
+  uint32_t round, key, result, pad;
+  uint64_t idx;
+};
+
+__device__ __forceinline__ uint32_t fmix32(uint32_t h) {
+  h ^= h >> 16;
+  h *= 0x85ebca6bu;
+  h ^= h >> 13;
+  h *= 0xc2b2ae35u;
+  h ^= h >> 16;
+  return h;
+}
+// Total order used to link roots (lower rank goes under higher): no cycles can form, the same
+// role as the random priorities of DisjointSetUnion_MT::order_edge (include/dsu.h:113-117).
+__device__ __forceinline__ uint64_t rank_of(uint32_t x) {
+  return ((uint64_t)fmix32(x) << 32) | x;
+}
+
+// find_root with path halving (include/dsu.h:145-152); loads/stores go to L2 so updates by other
+// SMs are seen.
+__device__ uint32_t dsu_find(uint32_t *parent, uint32_t x) {
+  for (;;) {
+    const uint32_t p = __ldcg(parent + x);
+    if (p == x) return x;
+    const uint32_t gp = __ldcg(parent + p);
+    if (gp == p) return p;
+    __stcg(parent + x, gp);
+    x = gp;
+  }
+}
+
+// merge with CAS (include/dsu.h:155-167). Returns true when this call linked two roots.
+__device__ bool dsu_unite(uint32_t *parent, uint32_t a, uint32_t b) {
+  for (;;) {
+    a = dsu_find(parent, a);
+    b = dsu_find(parent, b);
+    if (a == b) return false;
+    if (rank_of(a) < rank_of(b)) {
+      const uint32_t t = a;
+      a = b;
+      b = t;
+    }
+    if (atomicCAS(parent + b, b, a) == b) return true;
+  }
+}
+
+// Sketch::sample (src/sketch.cpp:94-116) on one merged column held one or two buckets per lane
+// (lane j holds bucket j and j + 32) plus the deterministic bucket (same on every lane).
+__device__ __forceinline__ int warp_sample(const uint32_t (&d)[3], const uint32_t (&a)[2][3],
+                                           uint32_t B, uint64_t flip_chk, uint64_t *idx) {
+  const int lane = threadIdx.x & 31;
+  if ((d[0] | d[1] | d[2]) == 0) {
+    *idx = 0;
+    return 1;  // ZERO
+  }
+  if (bucket_good(d[0], d[1], d[2], flip_chk)) {
+    *idx = ((uint64_t)d[1] << 32) | d[0];
+    return 0;  // GOOD
+  }
+#pragma unroll
+  for (int s = 0; s < 2; ++s) {
+    if ((uint32_t)s * 32 >= B) break;
+    const uint32_t j = s * 32 + lane;
+    const bool good = j < B && bucket_good(a[s][0], a[s][1], a[s][2], flip_chk);
+    const uint32_t m = __ballot_sync(kFull, good);
+    if (m) {
+      const int src = __ffs(m) - 1;
+      const uint32_t x0 = __shfl_sync(kFull, a[s][0], src);
+      const uint32_t x1 = __shfl_sync(kFull, a[s][1], src);
+      *idx = ((uint64_t)x1 << 32) | x0;
+      return 0;
+    }
+  }
+  *idx = 0;
+  return 2;  // FAIL
+}
+
+// sample_supernode (src/cc_sketch_alg.cpp:137-166): FAIL marks the round modified, GOOD unions
+// the sampled edge and marks modified if the partition changed.
+__device__ void handle_result(int res, uint64_t idx, uint32_t round, uint32_t key,
+                              const BoruvkaGeom &g, const BoruvkaBufs &b) {
+  if (b.trace) {
+    const uint32_t ti = atomicAdd(b.trace_n, 1u);
+    if (ti < b.trace_cap) {
+      TraceRec r;
+      r.round = round;
+      r.key = key;
+      r.result = (uint32_t)res;
+      r.pad = 0;
+      r.idx = idx;
+      reinterpret_cast<TraceRec *>(b.trace)[ti] = r;
+    }
+  }
+  if (res == 2) {
+    atomicOr(b.flags, 1u);
+  } else if (res == 0) {
+    const uint32_t x = (uint32_t)(idx >> 32), y = (uint32_t)idx;
+    if (x >= g.V || y >= g.V) {
+      atomicOr(b.status, kStatusBadSample);
+      return;
+    }
+    if (dsu_unite(b.parent, x, y)) {
+      atomicOr(b.flags, 1u);
+      const uint32_t fi = atomicAdd(b.forest_n, 1u);
+      if (fi < g.V) b.forest[fi] = idx;
+    }
+  }
+}
+
+__device__ __forceinline__ void load_bucket(const uint32_t *p, uint32_t (&x)[3]) {
+  x[0] = p[0];
+  x[1] = p[1];
+  x[2] = p[2];
+}
+
+__global__ void k_bv_reset(uint32_t V, uint32_t *parent) {
+  const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v < V) parent[v] = v;
+}
+
+// Round 0 (run_round_zero, src/cc_sketch_alg.cpp:223-244): every vertex is its own component.
+__global__ void k_bv_round0(BoruvkaGeom g, const uint32_t *__restrict__ sk_words, BoruvkaBufs b) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < g.V; v += nwarps) {
+    const uint32_t *sk = sk_words + (uint64_t)v * g.sketch_words;
+    uint32_t d[3], a[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    load_bucket(sk + 3 * g.C * g.B, d);
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+      const uint32_t j = s * 32 + lane;
+      if (j < g.B) load_bucket(sk + 3 * j, a[s]);
+    }
+    uint64_t idx;
+    const int res = warp_sample(d, a, g.B, g.flip_chk, &idx);
+    if (lane == 0) handle_result(res, idx, 0, v, g, b);
+  }
+}
+
+__global__ void k_bv_label(uint32_t V, uint32_t *parent, uint32_t *label, uint32_t *cnt,
+                           uint32_t *minv) {
+  const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= V) return;
+  const uint32_t r = dsu_find(parent, v);
+  label[v] = r;
+  atomicAdd(&cnt[r], 1u);
+  if (minv) atomicMin(&minv[r], v);
+}
+
+__global__ void k_bv_pack(uint32_t V, const uint32_t *cnt, uint64_t *packed) {
+  const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= V) return;
+  const uint32_t c = cnt[v];
+  packed[v] = (uint64_t)c | (c ? (1ull << 32) : 0ull);
+}
+
+// create_merge_instructions (src/cc_sketch_alg.cpp:382-462): group vertices by root so each
+// component's members are contiguous in `order`.
+__global__ void k_bv_group(uint32_t V, uint32_t B, uint32_t span, const uint32_t *label,
+                           const uint64_t *packed, const uint64_t *total, const uint32_t *cnt,
+                           uint32_t *fill, const uint32_t *minv, uint32_t *order,
+                           uint32_t *order_comp, uint32_t *comp_start, uint32_t *comp_key,
+                           uint32_t *ncomp, uint32_t *acc) {
+  const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= V) return;
+  const uint32_t r = label[v];
+  const uint64_t s = packed[r];
+  const uint32_t start = (uint32_t)s, c = (uint32_t)(s >> 32);
+  const uint32_t pos = start + atomicAdd(&fill[r], 1u);
+  order[pos] = v;
+  order_comp[pos] = c;
+  if (v == r) {
+    comp_start[c] = start;
+    comp_key[c] = minv ? minv[r] : r;
+    const uint32_t end = start + cnt[r];
+    if (start / span != (end - 1) / span) {
+      uint32_t *ac = acc + (uint64_t)c * (B + 1) * 3;
+      for (uint32_t i = 0; i < (B + 1) * 3; ++i) ac[i] = 0;
+    }
+  }
+  if (v == 0) {
+    const uint32_t nc = (uint32_t)(*total >> 32);
+    comp_start[nc] = V;
+    *ncomp = nc;
+  }
+}
+
+// perform_boruvka_round (src/cc_sketch_alg.cpp:246-380) for round >= 1: each warp XOR-merges
+// column `round` + the deterministic bucket over `span` consecutive grouped members; components
+// wholly inside the span are sampled right here, the rest are combined in acc.
+__global__ void k_bv_merge(BoruvkaGeom g, uint32_t round, const uint32_t *__restrict__ sk_words,
+                           BoruvkaBufs b) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t p0 = (uint64_t)w * g.span;
+  if (p0 >= g.V) return;
+  const uint32_t p1 = (uint32_t)(p0 + g.span < (uint64_t)g.V ? p0 + g.span : (uint64_t)g.V);
+  const uint32_t col = 3 * round * g.B, detw = 3 * g.C * g.B;
+  uint32_t a[2][3] = {{0, 0, 0}, {0, 0, 0}}, d[3] = {0, 0, 0};
+  uint32_t cur = b.order_comp[p0];
+  auto flush = [&](uint32_t c) {
+    const uint32_t s = b.comp_start[c], e = b.comp_start[c + 1];
+    if (s >= p0 && e <= p1) {
+      uint64_t idx;
+      const int res = warp_sample(d, a, g.B, g.flip_chk, &idx);
+      if (lane == 0) handle_result(res, idx, round, b.comp_key[c], g, b);
+    } else {
+      uint32_t *ac = b.acc + (uint64_t)c * (g.B + 1) * 3;
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const uint32_t j = q * 32 + lane;
+        if (j < g.B) {
+          atomicXor(ac + 3 * j, a[q][0]);
+          atomicXor(ac + 3 * j + 1, a[q][1]);
+          atomicXor(ac + 3 * j + 2, a[q][2]);
+        }
+      }
+      if (lane == 0) {
+        atomicXor(ac + 3 * g.B, d[0]);
+        atomicXor(ac + 3 * g.B + 1, d[1]);
+        atomicXor(ac + 3 * g.B + 2, d[2]);
+      }
+    }
+  };
+  for (uint32_t p = (uint32_t)p0; p < p1; ++p) {
+    const uint32_t c = b.order_comp[p];
+    if (c != cur) {
+      flush(cur);
+      cur = c;
+#pragma unroll
+      for (int q = 0; q < 2; ++q) a[q][0] = a[q][1] = a[q][2] = 0;
+      d[0] = d[1] = d[2] = 0;
+    }
+    const uint32_t *sk = sk_words + (uint64_t)b.order[p] * g.sketch_words;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const uint32_t j = q * 32 + lane;
+      if (j < g.B) {
+        const uint32_t *bk = sk + col + 3 * j;
+        a[q][0] ^= bk[0];
+        a[q][1] ^= bk[1];
+        a[q][2] ^= bk[2];
+      }
+    }
+    d[0] ^= sk[detw];
+    d[1] ^= sk[detw + 1];
+    d[2] ^= sk[detw + 2];
+  }
+  flush(cur);
+}
+
+__global__ void k_bv_sample_spanning(BoruvkaGeom g, uint32_t round, BoruvkaBufs b) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t nc = *b.ncomp;
+  for (uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < nc; c += nwarps) {
+    const uint32_t s = b.comp_start[c], e = b.comp_start[c + 1];
+    if (s / g.span == (e - 1) / g.span) continue;
+    const uint32_t *ac = b.acc + (uint64_t)c * (g.B + 1) * 3;
+    uint32_t a[2][3] = {{0, 0, 0}, {0, 0, 0}}, d[3];
+    d[0] = __ldcg(ac + 3 * g.B);
+    d[1] = __ldcg(ac + 3 * g.B + 1);
+    d[2] = __ldcg(ac + 3 * g.B + 2);
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const uint32_t j = q * 32 + lane;
+      if (j < g.B) {
+        a[q][0] = __ldcg(ac + 3 * j);
+        a[q][1] = __ldcg(ac + 3 * j + 1);
+        a[q][2] = __ldcg(ac + 3 * j + 2);
+      }
+    }
+    uint64_t idx;
+    const int res = warp_sample(d, a, g.B, g.flip_chk, &idx);
+    if (lane == 0) handle_result(res, idx, round, b.comp_key[c], g, b);
+  }
+}
+
+__global__ void k_bv_final(uint32_t V, uint32_t *parent, uint32_t *out, uint32_t *ncc) {
+  const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= V) return;
+  const uint32_t r = dsu_find(parent, v);
+  out[v] = r;
+  if (r == v) atomicAdd(ncc, 1u);
+}
+
+inline unsigned blocks_for(uint64_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
+
+// Eight independent hash chains per thread: each step is one 8-byte XXH3 (rrmxmx with a column
+// constant) plus the depth ctz, the per-column work of the ingest kernel, with no memory traffic.
+__global__ void k_hash_peak(uint64_t seed, uint32_t iters, uint64_t *out) {
+  const uint64_t flip = xxh3_flip(seed);
+  uint64_t x[8];
+  const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) x[k] = tid * 8 + k;
+  uint32_t acc = 0;
+  for (uint32_t i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      x[k] = rrmxmx8(x[k] ^ flip);
+      acc += depth_of(x[k], 34);
+    }
+  }
+  uint64_t r = acc;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) r ^= x[k];
+  out[tid] = r;
+}
+
+}  // namespace
+
+// ================================================================================================
+// host wrappers
+// ================================================================================================
+uint64_t launch_count() { return g_launches.load(); }
+
+cudaError_t hash_peak(uint64_t seed, uint32_t iters, int blocks, int threads, uint64_t *out,
+                      cudaStream_t s) {
+  k_hash_peak<<<blocks, threads, 0, s>>>(seed, iters, out);
+  g_launches++;
+  return cudaGetLastError();
+}
+
+int num_sms() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 1;
+  }
+  return n;
+}
+
+size_t scan_tmp_words(uint64_t n) {
+  size_t w = 0;
+  while (n > kScanBlock) {
+    n = (n + kScanBlock - 1) / kScanBlock;
+    w += n;
+  }
+  return w + 1;
+}
+
+cudaError_t scan_exclusive_u64(uint64_t *d, uint64_t n, uint64_t *total, uint64_t *tmp,
+                               cudaStream_t s) {
+  if (n == 0) return cudaMemsetAsync(total, 0, sizeof(uint64_t), s);
+  const uint64_t nb = (n + kScanBlock - 1) / kScanBlock;
+  if (nb == 1) {
+    k_scan_down<<<1, kScanThreads, 0, s>>>(d, n, nullptr, total);
+    g_launches++;
+    return cudaGetLastError();
+  }
+  uint64_t *sums = tmp;
+  k_scan_reduce<<<(unsigned)nb, kScanThreads, 0, s>>>(d, n, sums);
+  g_launches++;
+  cudaError_t e = scan_exclusive_u64(sums, nb, total, tmp + nb, s);
+  if (e != cudaSuccess) return e;
+  k_scan_down<<<(unsigned)nb, kScanThreads, 0, s>>>(d, n, sums, nullptr);
+  g_launches++;
+  return cudaGetLastError();
+}
+
+cudaError_t gutter_count_2d(int input, const void *in, uint64_t n, GutterGeom g, int G,
+                            uint64_t *hist, uint32_t *status, cudaStream_t s) {
+  return input == kInputRecords
+             ? launch_gutter<kInputRecords, true, true>(in, n, g, G, hist, nullptr, status, s)
+             : launch_gutter<kInputEntries, true, true>(in, n, g, G, hist, nullptr, status, s);
+}
+cudaError_t gutter_scatter_2d(int input, const void *in, uint64_t n, GutterGeom g, int G,
+                              const uint64_t *hist, uint2 *entries, cudaStream_t s) {
+  uint64_t *h = const_cast<uint64_t *>(hist);
+  return input == kInputRecords
+             ? launch_gutter<kInputRecords, false, true>(in, n, g, G, h, entries, nullptr, s)
+             : launch_gutter<kInputEntries, false, true>(in, n, g, G, h, entries, nullptr, s);
+}
+cudaError_t gutter_count_1d(int input, const void *in, uint64_t n, GutterGeom g, int G,
+                            uint64_t *counts, uint32_t *status, cudaStream_t s) {
+  return input == kInputRecords
+             ? launch_gutter<kInputRecords, true, false>(in, n, g, G, counts, nullptr, status, s)
+             : launch_gutter<kInputEntries, true, false>(in, n, g, G, counts, nullptr, status, s);
+}
+cudaError_t gutter_scatter_1d(int input, const void *in, uint64_t n, GutterGeom g, int G,
+                              uint64_t *cursor, uint2 *entries, cudaStream_t s) {
+  return input == kInputRecords
+             ? launch_gutter<kInputRecords, false, false>(in, n, g, G, cursor, entries, nullptr, s)
+             : launch_gutter<kInputEntries, false, false>(in, n, g, G, cursor, entries, nullptr, s);
+}
+cudaError_t gutter_tile_offsets(const uint64_t *scanned, uint32_t stride, uint32_t ntiles,
+                                const uint64_t *total, uint32_t *tile_off, cudaStream_t s) {
+  k_tile_offsets<<<blocks_for(ntiles + 1, 256), 256, 0, s>>>(scanned, stride, ntiles, total,
+                                                             tile_off);
+  g_launches++;
+  return cudaGetLastError();
+}
+cudaError_t copy_u64(const uint64_t *src, uint64_t *dst, uint64_t n, cudaStream_t s) {
+  k_copy_u64<<<(unsigned)std::min<uint64_t>(blocks_for(n, 256), 4096), 256, 0, s>>>(src, dst, n);
+  g_launches++;
+  return cudaGetLastError();
+}
+
+size_t sketch_update_smem_bytes(SketchGeom g) {
+  return ((size_t)g.sketch_words * 4 << g.tile_shift) + (size_t)(g.C + 1) * 8;
+}
+
+cudaError_t sketch_update_prepare(SketchGeom g, int /*threads*/) {
+  const size_t smem = sketch_update_smem_bytes(g);
+  return cudaFuncSetAttribute(k_sketch_update, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)smem);
+}
+
+cudaError_t sketch_update(SketchGeom g, uint8_t *sketches, const uint2 *entries,
+                          const ChunkTable &chunks, const uint32_t *tile_off, int nchunks,
+                          const uint64_t *flip, uint32_t *work_counter, uint32_t *status, int grid,
+                          int threads, cudaStream_t s) {
+  const size_t smem = sketch_update_smem_bytes(g);
+  k_sketch_update<<<grid, threads, smem, s>>>(g, sketches, entries, chunks, tile_off, nchunks, flip,
+                                              work_counter, status);
+  g_launches++;
+  return cudaGetLastError();
+}
+
+cudaError_t sketch_xor_raw(uint8_t *sketches, uint32_t words, uint32_t v, const uint32_t *raw,
+                           cudaStream_t s) {
+  k_sketch_xor_raw<<<blocks_for(words, 256), 256, 0, s>>>(reinterpret_cast<uint32_t *>(sketches),
+                                                          words, v, raw);
+  g_launches++;
+  return cudaGetLastError();
+}
+
+cudaError_t boruvka_reset(const BoruvkaGeom &g, const BoruvkaBufs &b, cudaStream_t s) {
+  k_bv_reset<<<blocks_for(g.V, 256), 256, 0, s>>>(g.V, b.parent);
+  g_launches++;
+  cudaMemsetAsync(b.forest_n, 0, sizeof(uint32_t), s);
+  if (b.trace) cudaMemsetAsync(b.trace_n, 0, sizeof(uint32_t), s);
+  return cudaGetLastError();
+}
+
+cudaError_t boruvka_round0(const BoruvkaGeom &g, const uint8_t *sketches, const BoruvkaBufs &b,
+                           cudaStream_t s) {
+  const unsigned blocks = std::min<unsigned>(blocks_for((uint64_t)g.V * 32, 256), num_sms() * 16);
+  k_bv_round0<<<blocks, 256, 0, s>>>(g, reinterpret_cast<const uint32_t *>(sketches), b);
+  g_launches++;
+  return cudaGetLastError();
+}
+
+cudaError_t boruvka_round(const BoruvkaGeom &g, uint32_t round, const uint8_t *sketches,
+                          const BoruvkaBufs &b, bool trace, cudaStream_t s) {
+  const uint32_t V = g.V;
+  cudaMemsetAsync(b.cnt, 0, sizeof(uint32_t) * V, s);
+  cudaMemsetAsync(b.fill, 0, sizeof(uint32_t) * V, s);
+  if (trace) cudaMemsetAsync(b.minv, 0xff, sizeof(uint32_t) * V, s);
+  k_bv_label<<<blocks_for(V, 256), 256, 0, s>>>(V, b.parent, b.label, b.cnt,
+                                                 trace ? b.minv : nullptr);
+  g_launches++;
+  k_bv_pack<<<blocks_for(V, 256), 256, 0, s>>>(V, b.cnt, b.packed);
+  g_launches++;
+  cudaError_t e = scan_exclusive_u64(b.packed, V, b.scan_total, b.scan_tmp, s);
+  if (e != cudaSuccess) return e;
+  k_bv_group<<<blocks_for(V, 256), 256, 0, s>>>(V, g.B, g.span, b.label, b.packed, b.scan_total,
+                                                 b.cnt, b.fill, trace ? b.minv : nullptr, b.order,
+                                                 b.order_comp, b.comp_start, b.comp_key, b.ncomp,
+                                                 b.acc);
+  g_launches++;
+  const uint64_t warps = (V + g.span - 1) / g.span;
+  k_bv_merge<<<blocks_for(warps * 32, 256), 256, 0, s>>>(
+      g, round, reinterpret_cast<const uint32_t *>(sketches), b);
+  g_launches++;
+  const unsigned sblocks = std::min<unsigned>(blocks_for((uint64_t)V * 32, 256), num_sms() * 16);
+  k_bv_sample_spanning<<<sblocks, 256, 0, s>>>(g, round, b);
+  g_launches++;
+  return cudaGetLastError();
+}
+
+cudaError_t boruvka_final(const BoruvkaGeom &g, const BoruvkaBufs &b, uint32_t *labels_out,
+                          uint32_t *ncc, cudaStream_t s) {
+  cudaMemsetAsync(ncc, 0, sizeof(uint32_t), s);
+  k_bv_final<<<blocks_for(g.V, 256), 256, 0, s>>>(g.V, b.parent, labels_out, ncc);
+  g_launches++;
+  return cudaGetLastError();
+}
+
+}  // namespace gz

@@ -1,0 +1,134 @@
+// gz_kernels.cuh -- launch interface of the sm_100a kernels (implemented in gz_kernels.cu).
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gz {
+
+// Status bits a kernel may raise in the handle's device status word.
+enum : uint32_t {
+  kStatusBadVertex = 1u << 0,
+  kStatusTimeout = 1u << 1,
+  kStatusBadSample = 1u << 2,
+};
+
+enum GutterInput : int {
+  kInputRecords = 0,  // packed 9-byte records {u8 type, u32 src, u32 dst}: 2 endpoint entries
+  kInputEntries = 1,  // uint2 {vertex, neighbour}: 1 endpoint entry
+};
+
+// Geometry shared by the gutter kernels.
+struct GutterGeom {
+  uint32_t V;
+  uint32_t tile_shift;  // tile of a vertex = v >> tile_shift (vertices_per_tile = 1 << shift)
+  uint32_t ntiles;
+};
+
+// Maximum number of gutter chunks buffered before the sketches must be updated.
+constexpr int kMaxChunks = 128;
+struct ChunkTable {
+  uint64_t base[kMaxChunks];  // first entry of the chunk in the gutter buffer
+};
+
+struct SketchGeom {
+  uint32_t V;
+  uint32_t C;                  // columns
+  uint32_t B;                  // buckets per column
+  uint32_t sketch_words;       // (C*B+1)*3 32-bit words per vertex sketch
+  uint32_t tile_shift;
+  uint32_t ntiles;
+};
+
+// Records per staging tile of the gutter kernels, and the largest tile count for which the
+// per-CTA histogram lives in shared memory.
+constexpr int kRecTile = 4096;
+constexpr uint32_t kSmemBinsMax = 12288;
+
+// ---- scan -------------------------------------------------------------------------------------
+// Exclusive prefix sum over n u64 values, in place; writes the total to *d_total. `tmp` must
+// hold scan_tmp_words(n) u64.
+size_t scan_tmp_words(uint64_t n);
+cudaError_t scan_exclusive_u64(uint64_t *d_data, uint64_t n, uint64_t *d_total, uint64_t *tmp,
+                               cudaStream_t s);
+
+// ---- device gutter ----------------------------------------------------------------------------
+// 2-D path (ntiles <= kSmemBinsMax): per-CTA histograms -> hist[tile * G + cta], scan, scatter
+// with shared-memory cursors. 1-D path: global counters.
+cudaError_t gutter_count_2d(int input, const void *d_in, uint64_t n, GutterGeom g, int G,
+                            uint64_t *hist, uint32_t *status, cudaStream_t s);
+cudaError_t gutter_scatter_2d(int input, const void *d_in, uint64_t n, GutterGeom g, int G,
+                              const uint64_t *hist_scanned, uint2 *entries, cudaStream_t s);
+cudaError_t gutter_count_1d(int input, const void *d_in, uint64_t n, GutterGeom g, int G,
+                            uint64_t *counts, uint32_t *status, cudaStream_t s);
+cudaError_t gutter_scatter_1d(int input, const void *d_in, uint64_t n, GutterGeom g, int G,
+                              uint64_t *cursor, uint2 *entries, cudaStream_t s);
+// tile_off[b] = scanned[b * stride], tile_off[ntiles] = *total  (u32, relative to chunk base)
+cudaError_t gutter_tile_offsets(const uint64_t *scanned, uint32_t stride, uint32_t ntiles,
+                                const uint64_t *total, uint32_t *tile_off, cudaStream_t s);
+// gutter_scatter_1d consumes cursors; copy scanned counts into them first.
+cudaError_t copy_u64(const uint64_t *src, uint64_t *dst, uint64_t n, cudaStream_t s);
+
+// ---- sketch update -------------------------------------------------------------------------------
+size_t sketch_update_smem_bytes(SketchGeom g);
+cudaError_t sketch_update_prepare(SketchGeom g, int threads);
+// Applies every buffered entry of `nchunks` chunks: for each tile with entries, stage its
+// sketches in shared memory with bulk async copies, XOR every entry in, write the tile back.
+cudaError_t sketch_update(SketchGeom g, uint8_t *sketches, const uint2 *entries,
+                          const ChunkTable &chunks, const uint32_t *tile_off, int nchunks,
+                          const uint64_t *flip, uint32_t *work_counter, uint32_t *status,
+                          int grid, int threads, cudaStream_t s);
+// XOR num_buckets raw buckets (device) into the sketch of vertex v.
+cudaError_t sketch_xor_raw(uint8_t *sketches, uint32_t sketch_words, uint32_t v,
+                           const uint32_t *raw, cudaStream_t s);
+
+// ---- Boruvka -----------------------------------------------------------------------------------
+struct BoruvkaBufs {
+  uint32_t *parent;      // V   DSU parents
+  uint32_t *label;       // V   root per vertex for the current round
+  uint32_t *cnt;         // V   members per root
+  uint32_t *fill;        // V   scatter cursors
+  uint32_t *minv;        // V   smallest member per root (trace keys)
+  uint64_t *packed;      // V   (cnt | has_members << 32), scanned in place
+  uint64_t *scan_total;  // 1
+  uint64_t *scan_tmp;
+  uint32_t *order;       // V   vertices grouped by component
+  uint32_t *order_comp;  // V   component index of each grouped position
+  uint32_t *comp_start;  // V+1
+  uint32_t *comp_key;    // V
+  uint32_t *ncomp;       // 1
+  uint32_t *acc;         // V * (B+1) * 3 words: merged buckets of components spanning warps
+  uint32_t *flags;       // [0] modified
+  uint64_t *forest;      // V   spanning-forest edge indices
+  uint32_t *forest_n;    // 1
+  void *trace;           // gz_trace_rec_t[trace_cap] or null
+  uint32_t *trace_n;     // 1
+  uint32_t trace_cap;
+  uint32_t *status;
+};
+
+struct BoruvkaGeom {
+  uint32_t V, C, B, sketch_words;
+  uint64_t flip_chk;
+  uint32_t span;  // members merged per warp
+};
+
+cudaError_t boruvka_reset(const BoruvkaGeom &g, const BoruvkaBufs &b, cudaStream_t s);
+cudaError_t boruvka_round0(const BoruvkaGeom &g, const uint8_t *sketches, const BoruvkaBufs &b,
+                           cudaStream_t s);
+cudaError_t boruvka_round(const BoruvkaGeom &g, uint32_t round, const uint8_t *sketches,
+                          const BoruvkaBufs &b, bool trace, cudaStream_t s);
+// parent_out[v] = root of v; *ncc = number of roots (device pointers)
+cudaError_t boruvka_final(const BoruvkaGeom &g, const BoruvkaBufs &b, uint32_t *labels_out,
+                          uint32_t *ncc, cudaStream_t s);
+
+int num_sms();
+
+// Register-only hash throughput probe: n_threads * iters * 8 hashes.
+cudaError_t hash_peak(uint64_t seed, uint32_t iters, int blocks, int threads, uint64_t *out,
+                      cudaStream_t s);
+
+// Kernel launches issued by the host wrappers of this file (monotonic, process-wide).
+uint64_t launch_count();
+
+}  // namespace gz

@@ -271,6 +271,78 @@ def chung_lu_stream(num_vertices: int, exponent: float, mean_degree: float, max_
     return Stream(V, make_records(src, dst, types))
 
 
+# ---------------------------------------------------------------------------------------------
+# fast generator (libgz_gen.so): the same planted-partition workload at benchmark scale
+# ---------------------------------------------------------------------------------------------
+
+_gen = None
+
+
+def _genlib():
+    global _gen
+    if _gen is None:
+        import ctypes
+        from . import build as _build
+        path = _build.build_gen()
+        L = ctypes.CDLL(path)
+        vp = ctypes.c_void_p
+        L.gzg_planted_edges.restype = ctypes.c_uint64
+        L.gzg_planted_edges.argtypes = [vp, vp, ctypes.c_uint32, ctypes.c_double, ctypes.c_uint64, vp]
+        L.gzg_planted_nonedges.restype = None
+        L.gzg_planted_nonedges.argtypes = [ctypes.c_uint32, vp, vp, ctypes.c_double,
+                                           ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, vp]
+        L.gzg_shuffle_stream.restype = None
+        L.gzg_shuffle_stream.argtypes = [vp, ctypes.c_uint64, vp, ctypes.c_uint64, ctypes.c_uint64, vp]
+        _gen = L
+    return _gen
+
+
+def planted_partition_stream_fast(num_vertices: int, num_components: int, seed: int, *,
+                                  p: float | None = None, mean_degree: float | None = None,
+                                  min_size: int = 1, churn_fraction: float = 0.0,
+                                  uniform_assignment: bool = False, out: np.ndarray | None = None):
+    """Planted-components stream of the same shape as planted_partition_stream, built by the
+    multithreaded C generator (counter-based randomness + Feistel shuffle): seconds for 1e8
+    records. Returns (Stream, planted component label per vertex). ``out`` may be a
+    preallocated uint8 buffer (e.g. pinned memory) of at least 9 * num_updates bytes."""
+    L = _genlib()
+    rng = np.random.default_rng(seed)
+    V, k = num_vertices, num_components
+    if uniform_assignment:
+        comp = rng.integers(0, k, V).astype(np.uint32)
+    else:
+        extra = V - k * min_size
+        cuts = np.sort(rng.integers(0, extra + 1, k - 1))
+        sizes = np.diff(np.concatenate([[0], cuts, [extra]])) + min_size
+        comp = np.repeat(np.arange(k, dtype=np.uint32), sizes)[rng.permutation(V)]
+    order = np.argsort(comp, kind="stable")
+    members = order.astype(np.uint32)
+    sizes = np.bincount(comp, minlength=k).astype(np.uint64)
+    comp_off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.uint64)
+    pos = np.empty(V, np.uint32)
+    pos[order] = (np.arange(V, dtype=np.uint64) - comp_off[comp[order]]).astype(np.uint32)
+    if p is None:
+        pairs = float((sizes * (sizes - 1) // 2).sum())
+        p = min(1.0, (mean_degree or 0) * V / 2.0 / pairs)
+    gseed = int(rng.integers(0, 2**63))
+    E = L.gzg_planted_edges(members.ctypes.data, comp_off.ctypes.data, k, p, gseed, None)
+    edges = np.empty(E, np.uint64)
+    L.gzg_planted_edges(members.ctypes.data, comp_off.ctypes.data, k, p, gseed, edges.ctypes.data)
+    nc = int(round(churn_fraction * E))
+    cand = np.empty(int(nc * 1.02) + 64, np.uint64)
+    L.gzg_planted_nonedges(V, comp.ctypes.data, pos.ctypes.data, p, gseed,
+                           int(rng.integers(0, 2**63)), cand.size, cand.ctypes.data)
+    _, first = np.unique(cand, return_index=True)
+    churn = cand[np.sort(first)][:nc]
+    n = E + 2 * churn.size
+    buf = out if out is not None else np.empty(n * 9, np.uint8)
+    assert buf.size >= n * 9
+    L.gzg_shuffle_stream(edges.ctypes.data, E, churn.ctypes.data, churn.size,
+                         int(rng.integers(0, 2**63)), buf.ctypes.data)
+    recs = buf[:n * 9].view(RECORD_DTYPE)
+    return Stream(V, recs), comp.astype(np.int64)
+
+
 def cached_stream(cache_dir: str, name: str, builder) -> Stream:
     """Build a stream once and keep it as a file under cache_dir (keyed by name)."""
     os.makedirs(cache_dir, exist_ok=True)

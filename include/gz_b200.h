@@ -1,0 +1,221 @@
+/*
+ * gz_b200.h -- C ABI of the B200-native GraphZeppelin sketch-ingest and Boruvka-query path.
+ *
+ * One opaque handle (gz_alg_t) stands for one CCSketchAlg (reference include/cc_sketch_alg.h:69)
+ * whose V vertex sketches live in the HBM of the current CUDA device. Every entry point takes
+ * plain pointers and sizes, returns a gz_status code, and never throws. Host buffers passed in
+ * are borrowed for the duration of the call only; device buffers (the *_device entry points)
+ * must stay valid until the next gz_flush / query on the same handle.
+ *
+ * Each entry point names the reference interface it replaces (file:line, paths relative to the
+ * GraphZeppelin source tree). Semantics that the reference leaves to exceptions map to codes:
+ *   OutOfSamplesException  (include/sketch.h:193-204)       -> GZ_ERR_OUT_OF_SAMPLES
+ *   UpdateLockedException  (include/cc_sketch_alg.h:25-29)  -> GZ_ERR_LOCKED
+ *
+ * Thread safety: every call on a handle takes that handle's lock, so concurrent
+ * gz_apply_update_batch calls from worker threads (the driver contract,
+ * include/graph_sketch_driver.h:49-52) are safe; they are staged and applied in bulk.
+ */
+#ifndef GZ_B200_H
+#define GZ_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define GZ_API __attribute__((visibility("default")))
+#else
+#define GZ_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct gz_alg gz_alg_t;
+
+/* Status codes. */
+enum gz_status {
+  GZ_OK = 0,
+  GZ_ERR_INVALID = 1,        /* bad argument (null handle, V < 2, size mismatch ...) */
+  GZ_ERR_CUDA = 2,           /* a CUDA runtime call failed; gz_last_error() has the text */
+  GZ_ERR_OUT_OF_SAMPLES = 3, /* Boruvka needed more rounds than the sketch has columns */
+  GZ_ERR_LOCKED = 4,         /* update while a query runs, or after a failed query */
+  GZ_ERR_BAD_VERTEX = 5,     /* an update named a vertex id >= V (the update is dropped) */
+  GZ_ERR_NOMEM = 6,          /* device or pinned host allocation failed */
+  GZ_ERR_IO = 7,             /* file could not be read or written */
+  GZ_ERR_TIMEOUT = 8,        /* a bounded device-side wait gave up (kernel returned early) */
+  GZ_ERR_BAD_SAMPLE = 9,     /* a checksum-valid sample decoded to a vertex id >= V */
+  GZ_ERR_NO_DEVICE = 10      /* no usable CUDA device (there is no CPU fallback) */
+};
+
+/* Query codes, reference enum QueryCode (include/cc_sketch_alg.h:60-63). */
+enum gz_query_code { GZ_CONNECTIVITY = 0, GZ_KSPANNINGFORESTS = 1 };
+
+/* Sample results, reference enum SampleResult (include/sketch.h:20-24). */
+enum gz_sample_result { GZ_SAMPLE_GOOD = 0, GZ_SAMPLE_ZERO = 1, GZ_SAMPLE_FAIL = 2 };
+
+/* Sizing and configuration of a handle. */
+typedef struct gz_params {
+  uint32_t num_vertices;        /* CCSketchAlg::get_num_vertices (include/cc_sketch_alg.h:255) */
+  uint32_t num_columns;         /* Sketch::get_columns == calc_cc_samples(V, f) (include/sketch.h:74-76) */
+  uint32_t bkt_per_col;         /* Sketch::calc_bkt_per_col(calc_vector_length(V)) (include/sketch.h:181) */
+  uint32_t num_buckets;         /* num_columns * bkt_per_col + 1 (src/sketch.cpp:13) */
+  uint64_t seed;                /* CCSketchAlg::get_seed (include/cc_sketch_alg.h:256) */
+  uint64_t sketch_bytes;        /* Sketch::bucket_array_bytes (include/sketch.h:117) */
+  uint64_t desired_updates_per_batch; /* include/cc_sketch_alg.h:146-150 */
+  uint64_t max_rounds;          /* CCSketchAlg::max_rounds (include/cc_sketch_alg.h:257) */
+  double sketches_factor;       /* CCAlgConfiguration::get_sketches_factor */
+  double batch_factor;          /* CCAlgConfiguration::get_batch_factor */
+  uint32_t vertices_per_tile;   /* device layout: sketches staged together in shared memory */
+  uint32_t num_tiles;
+} gz_params_t;
+
+/* One sampled component of one Boruvka round (parity tracing). key = smallest member id. */
+typedef struct gz_trace_rec {
+  uint32_t round;
+  uint32_t key;
+  uint32_t result; /* enum gz_sample_result */
+  uint32_t pad;
+  uint64_t idx;    /* sampled edge index (min << 32) | max, 0 unless GOOD */
+} gz_trace_rec_t;
+
+/* Device time spent per phase since the last reset (CUDA events on the handle's stream). */
+typedef struct gz_profile {
+  double gutter_ms;        /* record parsing + counting sort into per-tile gutters */
+  double sketch_update_ms; /* the sketch-update kernel (shared-memory XOR of every gutter entry) */
+  double query_ms;         /* Boruvka rounds, labels included */
+  uint64_t gutter_launches;
+  uint64_t sketch_update_launches;
+  uint64_t query_rounds;
+  uint64_t entries_applied; /* endpoint updates folded into sketches */
+  uint64_t kernel_launches; /* every kernel this handle launched */
+} gz_profile_t;
+
+/* ---- library ------------------------------------------------------------------------------ */
+
+GZ_API const char *gz_version(void);
+GZ_API const char *gz_status_string(int status);
+/* Text of the last error raised on the calling thread (empty if none). */
+GZ_API const char *gz_last_error(void);
+
+/* ---- construction ------------------------------------------------------------------------- */
+
+/* CCSketchAlg(num_vertices, seed, CCAlgConfiguration) -- src/cc_sketch_alg.cpp:11-28,
+ * with CCAlgConfiguration::sketches_factor / batch_factor (src/cc_alg_configuration.cpp:10-26:
+ * a factor <= 0 falls back to 1). Allocates V zeroed sketches on the current device. */
+GZ_API int gz_create(uint32_t num_vertices, uint64_t seed, double sketches_factor, double batch_factor,
+              gz_alg_t **out);
+
+/* CCSketchAlg::construct_from_serialized_data -- src/cc_sketch_alg.cpp:30-64. Reads a
+ * write_binary file (u64 seed, u32 V, f64 sketches_factor, V sketches). The DSU starts invalid. */
+GZ_API int gz_create_from_serialized(const char *path, double batch_factor, gz_alg_t **out);
+
+/* ~CCSketchAlg -- src/cc_sketch_alg.cpp:66-77. */
+GZ_API int gz_destroy(gz_alg_t *alg);
+
+GZ_API int gz_get_params(const gz_alg_t *alg, gz_params_t *out);
+
+/* Device gutter capacity in endpoint updates (default: V * desired_updates_per_batch, the
+ * reference's total gutter size). A full gutter is applied to the sketches before more
+ * updates are accepted. */
+GZ_API int gz_set_gutter_capacity(gz_alg_t *alg, uint64_t endpoint_updates);
+
+/* ---- ingest (the driver / algorithm contract, include/graph_sketch_driver.h:28-69) -------- */
+
+/* CCSketchAlg::allocate_worker_memory -- include/cc_sketch_alg.h:161-169. Host staging only:
+ * worker deltas are formed on the device, so this just records the worker count. */
+GZ_API int gz_allocate_worker_memory(gz_alg_t *alg, size_t num_workers);
+
+/* CCSketchAlg::pre_insert -- src/cc_sketch_alg.cpp:79-104 (NO_EAGER_DSU form: any update
+ * invalidates the cached query answer). */
+GZ_API int gz_pre_insert(gz_alg_t *alg, uint32_t src, uint32_t dst, int type, int thr_id);
+
+/* CCSketchAlg::apply_update_batch -- src/cc_sketch_alg.cpp:106-118: toggles edge index
+ * concat_pairing_fn(src, dsts[i]) in src's sketch only. dsts is a host array. */
+GZ_API int gz_apply_update_batch(gz_alg_t *alg, int thr_id, uint32_t src, const uint32_t *dsts,
+                          size_t n);
+
+/* CCSketchAlg::apply_raw_buckets_update -- src/cc_sketch_alg.cpp:120-123: XORs num_buckets
+ * packed 12-byte buckets (host memory, Sketch layout) into src's sketch. */
+GZ_API int gz_apply_raw_buckets_update(gz_alg_t *alg, uint32_t src, const void *raw_buckets);
+
+/* CCSketchAlg::update -- src/cc_sketch_alg.cpp:127-133: one stream update, both endpoints. */
+GZ_API int gz_update(gz_alg_t *alg, uint32_t src, uint32_t dst, int type);
+
+/* Whole-stream ingest that replaces GraphSketchDriver::process_stream_until's reader threads
+ * and the GutteringSystem (include/graph_sketch_driver.h:141-191): n_records packed 9-byte
+ * records {u8 type, u32 src, u32 dst} (reference README "Binary Stream Format") in HOST
+ * memory. Copies are pipelined against the device gutter; returns when the host buffer is no
+ * longer needed. Both endpoints of every record are updated; the type byte is not consulted
+ * (insert and delete are the same XOR toggle). */
+GZ_API int gz_ingest_records(gz_alg_t *alg, const void *records, size_t n_records);
+
+/* Same, records already in device memory of the handle's device (any byte alignment). */
+GZ_API int gz_ingest_records_device(gz_alg_t *alg, const void *d_records, size_t n_records);
+
+/* GraphSketchDriver::prep_query -- include/graph_sketch_driver.h:193-203: folds every buffered
+ * update into the sketches and synchronizes. Reports deferred device errors (BAD_VERTEX). */
+GZ_API int gz_flush(gz_alg_t *alg);
+
+/* CCSketchAlg::has_cached_query -- include/cc_sketch_alg.h:184-190. */
+GZ_API int gz_has_cached_query(const gz_alg_t *alg, int query_code, int *out);
+
+/* ---- queries ------------------------------------------------------------------------------ */
+
+/* CCSketchAlg::connected_components -- src/cc_sketch_alg.cpp:515-557, returning the
+ * ConnectedComponents payload (src/return_types.cpp:5-19): parent_out[v] = representative of
+ * v's component (may be NULL), *num_cc = number of components. Runs device Boruvka unless the
+ * cached answer is valid; flushes buffered updates first. */
+GZ_API int gz_connected_components(gz_alg_t *alg, uint32_t *parent_out, uint32_t *num_cc);
+
+/* CCSketchAlg::point_query -- src/cc_sketch_alg.cpp:570-612. */
+GZ_API int gz_point_query(gz_alg_t *alg, uint32_t a, uint32_t b, int *out);
+
+/* CCSketchAlg::last_query_rounds -- include/cc_sketch_alg.h:252. */
+GZ_API int gz_last_query_rounds(const gz_alg_t *alg, size_t *out);
+
+/* CCSketchAlg::calc_spanning_forest -- src/cc_sketch_alg.cpp:559-568: the edges whose union
+ * changed the partition during the last Boruvka (runs one if the cache is invalid).
+ * edges_out holds up to cap (src, dst) pairs with src < dst; *n_edges gets the count. */
+GZ_API int gz_spanning_forest(gz_alg_t *alg, uint32_t *edges_out, size_t cap, size_t *n_edges);
+
+/* ---- checkpoint ---------------------------------------------------------------------------- */
+
+/* CCSketchAlg::write_binary -- src/cc_sketch_alg.cpp:614-623 (byte-identical format). */
+GZ_API int gz_write_binary(gz_alg_t *alg, const char *path);
+
+/* Sketch::zero_contents (src/sketch.cpp:86-92) on every vertex sketch, discarding buffered
+ * updates: the handle holds the empty graph again (the cached answer is dropped). */
+GZ_API int gz_clear(gz_alg_t *alg);
+
+/* Copy the raw bucket bytes of all V sketches (V * sketch_bytes, reference layout) to a host
+ * buffer; buffered updates are applied first. */
+GZ_API int gz_dump_sketches(gz_alg_t *alg, void *host_buf, size_t bytes);
+
+/* ---- instrumentation ----------------------------------------------------------------------- */
+
+/* Record every sampled component of every Boruvka round (for parity checks). */
+GZ_API int gz_set_trace(gz_alg_t *alg, int enable);
+GZ_API int gz_get_trace(gz_alg_t *alg, gz_trace_rec_t *out, size_t cap, size_t *len);
+
+/* Per-phase device timings (CUDA events). enable != 0 starts a fresh accumulation. */
+GZ_API int gz_set_profiling(gz_alg_t *alg, int enable);
+GZ_API int gz_get_profile(gz_alg_t *alg, gz_profile_t *out);
+
+/* The cudaStream_t (as void*) every kernel of this handle is launched on. */
+GZ_API int gz_get_stream(gz_alg_t *alg, void **stream_out);
+
+/* Peak rate of this GPU at the ingest's hash arithmetic: a register-only kernel evaluating the
+ * 8-byte XXH3 plus the bucket-depth count-trailing-zeros, timed with CUDA events on the current
+ * device. *hashes_per_s gets the best of `repeats` launches. */
+GZ_API int gz_measure_hash_rate(int repeats, double *hashes_per_s);
+
+/* Tuning knobs of the sketch-update kernel (0 keeps the current value): vertices staged per
+ * tile (multiple of 4), threads per block. Takes effect on an empty gutter. */
+GZ_API int gz_set_tuning(gz_alg_t *alg, uint32_t vertices_per_tile, uint32_t threads_per_block);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GZ_B200_H */

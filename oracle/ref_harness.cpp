@@ -19,6 +19,8 @@
 //       loads a write_binary dump into reference Sketch objects and runs Boruvka round by round
 //       with the reference's Sketch::range_merge / Sketch::sample, logging every sampled
 //       component as {u32 round, u32 key, u32 result, u32 0, u64 idx}.
+//   params <sketches_factor> <V>...
+//       the reference's sizing functions (include/sketch.h:62-76, :181) for each V.
 #include <atomic>
 #include <chrono>
 #include <cstdio>
@@ -271,11 +273,31 @@ int run_trace(int argc, char **argv) {
   return 0;
 }
 
+// params <sketches_factor> <V>...: the reference's own sizing functions, one JSON line per V.
+int run_params(int argc, char **argv) {
+  if (argc < 4) return 2;
+  double factor = atof(argv[2]);
+  for (int i = 3; i < argc; ++i) {
+    node_id_t V = (node_id_t)strtoul(argv[i], nullptr, 10);
+    vec_t len = Sketch::calc_vector_length(V);
+    size_t samples = Sketch::calc_cc_samples(V, factor);
+    Sketch sk(len, 0, samples);
+    CCAlgConfiguration cfg;
+    cfg.sketches_factor(factor);
+    printf("{\"V\": %u, \"vector_len\": %llu, \"num_columns\": %zu, \"bkt_per_col\": %zu, "
+           "\"num_buckets\": %zu, \"sketch_bytes\": %zu}\n",
+           V, (unsigned long long)len, sk.get_columns(), Sketch::calc_bkt_per_col(len),
+           sk.get_buckets(), sk.bucket_array_bytes());
+  }
+  return 0;
+}
+
 }  // namespace
 
 int main(int argc, char **argv) {
   if (argc >= 2 && !strcmp(argv[1], "ingest")) return run_ingest(argc, argv);
   if (argc >= 2 && !strcmp(argv[1], "trace")) return run_trace(argc, argv);
+  if (argc >= 2 && !strcmp(argv[1], "params")) return run_params(argc, argv);
   fprintf(stderr,
           "usage: %s ingest <stream> <seed> <sketches_factor> <threads> <max_records|0> "
           "<dump|-> <labels|->\n       %s trace <dump> <trace_out> <labels_out>\n",

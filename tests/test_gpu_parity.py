@@ -1,0 +1,189 @@
+"""GPU path vs the golden vectors from the reference and vs the C oracle (bit-exact).
+
+Every check goes through the C ABI (libgz_b200.so) via the Python mirror of CCSketchAlg."""
+import hashlib
+import os
+
+import numpy as np
+import pytest
+
+from _golden import canonical, case_names, load_case
+
+pytestmark = pytest.mark.gpu
+
+
+def _alg(gz, V, seed, factor=1.0):
+    return gz.CCSketchAlg(V, seed, gz.CCAlgConfiguration().sketches_factor(factor))
+
+
+def _header(seed, V, factor):
+    return (np.array([seed], "<u8").tobytes() + np.array([V], "<u4").tobytes()
+            + np.array([factor], "<f8").tobytes())
+
+
+@pytest.mark.parametrize("name", case_names())
+def test_golden_case_bit_exact(gz, name, tmp_path):
+    c, st, labels, trace = load_case(name)
+    V, seed, f = c["num_vertices"], c["seed"], c["sketches_factor"]
+    alg = _alg(gz, V, seed, f)
+    alg.set_trace(True)
+    alg.ingest_records(st)
+    dump = alg.dump_sketches()
+    assert hashlib.sha256(_header(seed, V, f) + dump.tobytes()).hexdigest() == c["dump_sha256"]
+    path = str(tmp_path / "dump.bin")
+    alg.write_binary(path)
+    assert hashlib.sha256(open(path, "rb").read()).hexdigest() == c["dump_sha256"]
+    cc = alg.connected_components()
+    assert cc.size() == c["num_cc"]
+    assert (canonical(cc.parent_arr) == labels).all()
+    assert alg.last_query_rounds == c["rounds"]
+    tr = alg.get_trace()
+    assert tr.size == trace.size
+    for fld in ("round", "key", "result", "idx"):
+        assert (tr[fld] == trace[fld]).all(), fld
+
+
+@pytest.mark.parametrize("name", ["c0_v1024", "mult_v1024", "cl_v2048"])
+def test_apply_update_batch_path_equals_records_path(gz, oracle_mod, name):
+    """apply_update_batch (one endpoint per call, the driver's worker contract) must give the
+    same bytes as the record path and as the oracle's apply_batch."""
+    c, st, labels, _ = load_case(name)
+    V, seed = c["num_vertices"], c["seed"]
+    r = st.records
+    src = np.concatenate([r["src"], r["dst"]])
+    dst = np.concatenate([r["dst"], r["src"]])
+    order = np.argsort(src, kind="stable")
+    src, dst = src[order], dst[order]
+    alg = _alg(gz, V, seed)
+    osk = oracle_mod.OracleSketches(V, seed)
+    bounds = np.flatnonzero(np.diff(src)) + 1
+    batch = alg.get_desired_updates_per_batch()
+    for s_, d_ in zip(np.split(src, bounds), np.split(dst, bounds)):
+        for k in range(0, d_.size, batch):
+            alg.apply_update_batch(0, int(s_[0]), d_[k:k + batch])
+            osk.apply_batch(int(s_[0]), d_[k:k + batch])
+    assert (alg.dump_sketches() == osk.data).all()
+    cc = alg.connected_components()
+    assert (canonical(cc.parent_arr) == labels).all()
+
+
+def test_update_path_equals_oracle(gz, oracle_mod):
+    c, st, labels, _ = load_case("er_v64")
+    alg = _alg(gz, 64, c["seed"])
+    for rec in st.records:
+        alg.update(gz.GraphUpdate((int(rec["src"]), int(rec["dst"])), int(rec["type"])))
+    osk = oracle_mod.OracleSketches(64, c["seed"])
+    osk.apply_records(st.raw())
+    assert (alg.dump_sketches() == osk.data).all()
+    assert (canonical(alg.connected_components().parent_arr) == labels).all()
+
+
+@pytest.mark.parametrize("offset", [0, 1, 3, 7, 8, 12, 15])
+def test_device_ingest_any_alignment(gz, oracle_mod, offset):
+    torch = pytest.importorskip("torch")
+    c, st, labels, _ = load_case("c0_v1024")
+    raw = st.raw()
+    buf = torch.zeros(raw.size + 32, dtype=torch.uint8, device="cuda")
+    buf[offset:offset + raw.size] = torch.from_numpy(raw).cuda()
+    torch.cuda.synchronize()
+    alg = _alg(gz, 1024, c["seed"])
+    alg.ingest_records_device(buf.data_ptr() + offset, st.num_updates)
+    cc = alg.connected_components()
+    osk = oracle_mod.OracleSketches(1024, c["seed"])
+    osk.apply_records(raw)
+    assert (alg.dump_sketches() == osk.data).all()
+    assert (canonical(cc.parent_arr) == labels).all()
+
+
+@pytest.mark.parametrize("cap", [2, 1000, 4097, 65536])
+def test_small_gutter_many_chunks(gz, oracle_mod, cap):
+    """A tiny device gutter forces many partial applications; bytes must not change."""
+    c, st, labels, _ = load_case("cl_v2048")
+    alg = _alg(gz, 2048, c["seed"])
+    alg.set_gutter_capacity(cap)
+    for part in np.array_split(st.records, 7):
+        alg.ingest_records(part)
+    osk = oracle_mod.OracleSketches(2048, c["seed"])
+    osk.apply_records(st.raw())
+    assert (alg.dump_sketches() == osk.data).all()
+    assert (canonical(alg.connected_components().parent_arr) == labels).all()
+
+
+@pytest.mark.parametrize("vpt,threads", [(4, 128), (8, 256), (16, 1024), (32, 512), (64, 1024)])
+def test_tile_shapes_bit_exact(gz, oracle_mod, vpt, threads):
+    c, st, labels, _ = load_case("c0_v1024")
+    alg = _alg(gz, 1024, c["seed"])
+    alg.set_tuning(vpt, threads)
+    assert alg.params.vertices_per_tile == vpt
+    alg.ingest_records(st)
+    osk = oracle_mod.OracleSketches(1024, c["seed"])
+    osk.apply_records(st.raw())
+    assert (alg.dump_sketches() == osk.data).all()
+
+
+def test_queries_during_stream(gz, oracle_mod):
+    """TestQueryDuringStream / MTStreamWithMultipleQueries: 10 queries at stream breakpoints."""
+    c, st, _, _ = load_case("c0_v1024")
+    V, seed = 1024, c["seed"]
+    alg = _alg(gz, V, seed)
+    alg.set_trace(True)
+    driver = gz.GraphSketchDriver(alg, gz.BinaryFileStream(stream=st))
+    n = st.num_updates
+    tenth = n // 10
+    for q in range(10):
+        end = n if q == 9 else tenth * (q + 1)
+        driver.process_stream_until(end if q < 9 else gz.END_OF_STREAM)
+        driver.prep_query(gz.CONNECTIVITY)
+        cc = alg.connected_components()
+        osk = oracle_mod.OracleSketches(V, seed)
+        osk.apply_records(st.records[:end].view(np.uint8).reshape(-1))
+        rc, lab, rounds, tr = osk.boruvka()
+        assert rc == 0
+        assert (canonical(cc.parent_arr) == lab).all(), q
+        assert alg.last_query_rounds == rounds
+        got = alg.get_trace()
+        assert got.size == tr.size and (got["idx"] == tr["idx"]).all() and \
+            (got["result"] == tr["result"]).all()
+        ex_n, ex = oracle_mod.exact_cc(V, st.records[:end].view(np.uint8).reshape(-1))
+        assert cc.size() == ex_n
+    assert driver.get_total_updates() == 2 * n
+
+
+@pytest.mark.parametrize("V", [2, 3, 5, 17, 100, 301])
+def test_odd_vertex_counts(gz, oracle_mod, V):
+    from graphzeppelin_b200 import streams as S
+    st = S.erdos_renyi_stream(V, 0.3, seed=V, churn_fraction=0.5)
+    alg = _alg(gz, V, 4242 + V)
+    alg.ingest_records(st)
+    osk = oracle_mod.OracleSketches(V, 4242 + V)
+    osk.apply_records(st.raw())
+    assert (alg.dump_sketches() == osk.data).all()
+    rc, lab, rounds, _ = osk.boruvka(with_trace=False)
+    cc = alg.connected_components()
+    assert (canonical(cc.parent_arr) == lab).all()
+    assert alg.last_query_rounds == rounds
+
+
+def test_sampled_vertices_of_a_large_graph(gz, oracle_mod):
+    """V = 2^17: bytes of 48 random vertex sketches vs the oracle, partition vs exact CC."""
+    from graphzeppelin_b200 import streams as S
+    V = 1 << 17
+    st, planted = S.planted_partition_stream(V, 64, seed=17, mean_degree=40, min_size=256,
+                                             churn_fraction=0.1)
+    seed = 0xC0FFEE
+    alg = _alg(gz, V, seed)
+    alg.ingest_records(st)
+    dump = alg.dump_sketches()
+    rng = np.random.default_rng(1)
+    pick = rng.choice(V, 48, replace=False)
+    filt = np.zeros(V, np.uint8)
+    filt[pick] = 1
+    osk = oracle_mod.OracleSketches(V, seed)
+    osk.apply_records(st.raw(), vertex_filter=filt)
+    sb = osk.sketch_bytes
+    for v in pick:
+        assert (dump[v * sb:(v + 1) * sb] == osk.sketch(v)).all(), v
+    cc = alg.connected_components()
+    n, exact = oracle_mod.exact_cc(V, st.raw())
+    assert cc.size() == n == 64
+    assert (canonical(cc.parent_arr) == exact).all()
