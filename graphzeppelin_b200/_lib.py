@@ -31,7 +31,8 @@ class gz_params_t(ctypes.Structure):
                 ("seed", ctypes.c_uint64), ("sketch_bytes", ctypes.c_uint64),
                 ("desired_updates_per_batch", ctypes.c_uint64), ("max_rounds", ctypes.c_uint64),
                 ("sketches_factor", ctypes.c_double), ("batch_factor", ctypes.c_double),
-                ("vertices_per_tile", ctypes.c_uint32), ("num_tiles", ctypes.c_uint32)]
+                ("vertices_per_tile", ctypes.c_uint32), ("num_tiles", ctypes.c_uint32),
+                ("vertices_per_bin", ctypes.c_uint32), ("num_bins", ctypes.c_uint32)]
 
 
 class gz_trace_rec_t(ctypes.Structure):
@@ -81,7 +82,7 @@ SIGNATURES = [
     ("gz_set_profiling", _i, [_H, _i]),
     ("gz_get_profile", _i, [_H, ctypes.POINTER(gz_profile_t)]),
     ("gz_get_stream", _i, [_H, ctypes.POINTER(ctypes.c_void_p)]),
-    ("gz_set_tuning", _i, [_H, _u32, _u32]),
+    ("gz_set_tuning", _i, [_H, _u32, _u32, _u32]),
 ]
 
 _lib = None

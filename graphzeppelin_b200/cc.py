@@ -446,8 +446,10 @@ class CCSketchAlg:
         _check(self.lib.gz_get_stream(self._h, ctypes.byref(s)))
         return int(s.value or 0)
 
-    def set_tuning(self, vertices_per_tile: int = 0, threads_per_block: int = 0) -> None:
-        _check(self.lib.gz_set_tuning(self._h, vertices_per_tile, threads_per_block))
+    def set_tuning(self, vertices_per_tile: int = 0, threads_per_block: int = 0,
+                   tiles_per_bin: int = 0) -> None:
+        _check(self.lib.gz_set_tuning(self._h, vertices_per_tile, threads_per_block,
+                                      tiles_per_bin))
         p = _lib.gz_params_t()
         _check(self.lib.gz_get_params(self._h, ctypes.byref(p)))
         self.params = p

@@ -95,6 +95,8 @@ struct gz_alg {
   double sketches_factor = 1, batch_factor = 1;
   uint64_t sketch_bytes = 0, desired_batch = 0;
   uint32_t tile_shift = 2, ntiles = 0, threads = 1024;
+  uint32_t bin_shift = 2, nbins = 0;
+  size_t smem_optin = 227 * 1024;
   size_t num_workers = 1;
   // sketches + per-column hash constants
   uint8_t *d_sk = nullptr;
@@ -106,8 +108,9 @@ struct gz_alg {
   uint64_t entry_cap = 0, entry_used = 0;
   gz::ChunkTable chunks{};
   int nchunks = 0;
-  uint32_t *d_tile_off = nullptr;
-  uint64_t *d_hist = nullptr, *d_scan_tmp = nullptr, *d_total = nullptr;
+  uint32_t *d_bin_off = nullptr;
+  uint64_t *d_hist = nullptr, *d_scan_tmp = nullptr, *d_total = nullptr, *d_cursor = nullptr;
+  uint32_t *d_fill = nullptr;
   size_t hist_words = 0;
   // host-record pipeline
   uint8_t *d_stage[2] = {nullptr, nullptr};
@@ -150,9 +153,11 @@ struct gz_alg {
     g.sketch_words = nb * 3;
     g.tile_shift = tile_shift;
     g.ntiles = ntiles;
+    g.bin_shift = bin_shift;
+    g.nbins = nbins;
     return g;
   }
-  gz::GutterGeom ggeom() const { return gz::GutterGeom{V, tile_shift, ntiles}; }
+  gz::GutterGeom ggeom() const { return gz::GutterGeom{V, bin_shift, nbins}; }
   gz::BoruvkaGeom bgeom() const {
     gz::BoruvkaGeom g;
     g.V = V;
@@ -210,12 +215,19 @@ struct gz_alg {
 
 namespace {
 
-int choose_tiling(gz_alg *h, uint32_t vpt_req, uint32_t threads_req) {
+// Default gutter bins: the fewest tiles per bin that brings the bin count within the
+// shared-memory sort-scatter's range (each extra tile per bin costs the sketch-update kernel a
+// pass over the other tiles' entries).
+constexpr uint32_t kBinTarget = gz::kSortBinsMax;
+constexpr uint32_t kMaxTilesPerBin = 16;
+
+int choose_tiling(gz_alg *h, uint32_t vpt_req, uint32_t threads_req, uint32_t tpb_req) {
   int dev = h->device;
   int smem_optin = 0;
   cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   if (smem_optin <= 0) smem_optin = 227 * 1024;
-  const size_t budget = (size_t)smem_optin - 64;
+  h->smem_optin = (size_t)smem_optin;
+  const size_t budget = (size_t)smem_optin - 64 - gz::kQueueBytes;
   const size_t flip_bytes = (size_t)(h->C + 1) * 8;
   uint32_t shift;
   if (vpt_req) {
@@ -235,6 +247,18 @@ int choose_tiling(gz_alg *h, uint32_t vpt_req, uint32_t threads_req) {
   }
   h->tile_shift = shift;
   h->ntiles = (uint32_t)((h->V + (1u << shift) - 1) >> shift);
+  uint32_t bshift = shift;
+  if (tpb_req) {
+    if (tpb_req & (tpb_req - 1) || tpb_req > 64)
+      return fail(GZ_ERR_INVALID, "tiles_per_bin must be a power of two <= 64");
+    bshift = shift + (uint32_t)__builtin_ctz(tpb_req);
+  } else {
+    while (((h->V + (1u << bshift) - 1) >> bshift) > kBinTarget &&
+           (1u << (bshift - shift)) < kMaxTilesPerBin)
+      ++bshift;
+  }
+  h->bin_shift = bshift;
+  h->nbins = (uint32_t)((h->V + (1u << bshift) - 1) >> bshift);
   if (threads_req) {
     if (threads_req < 64 || threads_req > 1024 || threads_req % 32)
       return fail(GZ_ERR_INVALID, "threads_per_block must be a multiple of 32 in [64, 1024]");
@@ -261,7 +285,7 @@ int init_alg(gz_alg *h, uint32_t V, uint64_t seed, double sf, double bf) {
     num *= h->batch_factor;  // same size_t *= double truncation as the reference
     h->desired_batch = num;
   }
-  GZ_TRY(choose_tiling(h, 0, 0));
+  GZ_TRY(choose_tiling(h, 0, 0, 0));
   GZ_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
   GZ_CUDA(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
   // V rounded up to 64 so any tile size stays inside the allocation
@@ -290,10 +314,12 @@ void destroy_alg(gz_alg *h) {
   dev_free(h->d_status);
   host_free(h->h_status);
   dev_free(h->d_entries);
-  dev_free(h->d_tile_off);
+  dev_free(h->d_bin_off);
   dev_free(h->d_hist);
   dev_free(h->d_scan_tmp);
   dev_free(h->d_total);
+  dev_free(h->d_cursor);
+  dev_free(h->d_fill);
   for (int i = 0; i < 2; ++i) {
     dev_free(h->d_stage[i]);
     dev_free(h->d_ent[i]);
@@ -338,13 +364,16 @@ void destroy_alg(gz_alg *h) {
 
 int ensure_gutter(gz_alg *h) {
   GZ_TRY(dev_alloc(&h->d_entries, h->entry_cap));
-  GZ_TRY(dev_alloc(&h->d_tile_off, (size_t)gz::kMaxChunks * (h->ntiles + 1)));
-  const size_t g2 = 2 * (size_t)gz::num_sms();
-  const size_t words = std::max<size_t>((size_t)h->ntiles * g2, h->ntiles);
+  GZ_TRY(dev_alloc(&h->d_bin_off, (size_t)gz::kMaxChunks * (h->nbins + 1)));
+  const size_t words = h->nbins;
   if (h->hist_words < words) {
     dev_free(h->d_hist);
     dev_free(h->d_scan_tmp);
+    dev_free(h->d_cursor);
+    dev_free(h->d_fill);
     GZ_TRY(dev_alloc(&h->d_hist, words));
+    GZ_TRY(dev_alloc(&h->d_cursor, words));
+    GZ_TRY(dev_alloc(&h->d_fill, words));
     GZ_TRY(dev_alloc(&h->d_scan_tmp, gz::scan_tmp_words(words)));
     h->hist_words = words;
   }
@@ -357,14 +386,10 @@ int apply_pending(gz_alg *h) {
   if (h->nchunks == 0) return GZ_OK;
   const gz::SketchGeom g = h->sgeom();
   GZ_CUDA(cudaMemsetAsync(h->d_status + 1, 0, sizeof(uint32_t), h->stream));
-  const int per_sm = std::max(1, (int)(2048 / h->threads));
-  int smem_per_sm = 0;
-  cudaDeviceGetAttribute(&smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, h->device);
-  const size_t need = gz::sketch_update_smem_bytes(g) + 1024;
-  const int by_smem = std::max(1, (int)(smem_per_sm / need));
-  const int grid = (int)std::min<uint64_t>(h->ntiles, (uint64_t)gz::num_sms() * std::min(per_sm, by_smem));
+  const int per_sm = gz::sketch_update_ctas_per_sm(g, (int)h->threads);
+  const int grid = (int)std::min<uint64_t>(h->ntiles, (uint64_t)gz::num_sms() * per_sm);
   const int pi = h->prof_begin();
-  GZ_CUDA(gz::sketch_update(g, h->d_sk, h->d_entries, h->chunks, h->d_tile_off, h->nchunks, h->d_flip,
+  GZ_CUDA(gz::sketch_update(g, h->d_sk, h->d_entries, h->chunks, h->d_bin_off, h->nchunks, h->d_flip,
                             h->d_status + 1, h->d_status, grid, h->threads, h->stream));
   h->prof_end(pi, 1);
   h->prof_acc.entries_applied += h->entry_used;
@@ -390,20 +415,19 @@ int gutter_chunk(gz_alg *h, int input, const void *d_in, uint64_t n) {
   const uint64_t unit = input == gz::kInputRecords ? gz::kRecTile : 4096;
   const int G = (int)std::max<uint64_t>(1, std::min<uint64_t>(2ull * gz::num_sms(), (n + unit - 1) / unit));
   uint2 *out = h->d_entries + h->entry_used;
-  uint32_t *tile_off = h->d_tile_off + (size_t)h->nchunks * (h->ntiles + 1);
+  uint32_t *bin_off = h->d_bin_off + (size_t)h->nchunks * (h->nbins + 1);
   const int pi = h->prof_begin();
-  if (h->ntiles <= gz::kSmemBinsMax) {
-    const uint64_t words = (uint64_t)h->ntiles * G;
-    GZ_CUDA(gz::gutter_count_2d(input, d_in, n, gg, G, h->d_hist, h->d_status, h->stream));
-    GZ_CUDA(gz::scan_exclusive_u64(h->d_hist, words, h->d_total, h->d_scan_tmp, h->stream));
-    GZ_CUDA(gz::gutter_tile_offsets(h->d_hist, (uint32_t)G, h->ntiles, h->d_total, tile_off, h->stream));
-    GZ_CUDA(gz::gutter_scatter_2d(input, d_in, n, gg, G, h->d_hist, out, h->stream));
+  GZ_CUDA(cudaMemsetAsync(h->d_hist, 0, sizeof(uint64_t) * h->nbins, h->stream));
+  GZ_CUDA(gz::gutter_count(input, d_in, n, gg, G, h->d_hist, h->d_status, h->stream));
+  GZ_CUDA(gz::scan_exclusive_u64(h->d_hist, h->nbins, h->d_total, h->d_scan_tmp, h->stream));
+  GZ_CUDA(gz::gutter_bin_offsets(h->d_hist, 1, h->nbins, h->d_total, bin_off, h->stream));
+  const uint32_t tile = gz::sort_scatter_tile(input, gg, h->smem_optin - 1024);
+  if (tile >= 1024) {
+    GZ_CUDA(cudaMemsetAsync(h->d_fill, 0, sizeof(uint32_t) * h->nbins, h->stream));
+    GZ_CUDA(gz::gutter_sort_scatter(input, d_in, n, gg, tile, h->d_hist, h->d_fill, out, h->stream));
   } else {
-    GZ_CUDA(cudaMemsetAsync(h->d_hist, 0, sizeof(uint64_t) * h->ntiles, h->stream));
-    GZ_CUDA(gz::gutter_count_1d(input, d_in, n, gg, G, h->d_hist, h->d_status, h->stream));
-    GZ_CUDA(gz::scan_exclusive_u64(h->d_hist, h->ntiles, h->d_total, h->d_scan_tmp, h->stream));
-    GZ_CUDA(gz::gutter_tile_offsets(h->d_hist, 1, h->ntiles, h->d_total, tile_off, h->stream));
-    GZ_CUDA(gz::gutter_scatter_1d(input, d_in, n, gg, G, h->d_hist, out, h->stream));
+    GZ_CUDA(gz::copy_u64(h->d_hist, h->d_cursor, h->nbins, h->stream));
+    GZ_CUDA(gz::gutter_scatter_global(input, d_in, n, gg, G, h->d_cursor, out, h->stream));
   }
   h->prof_end(pi, 0);
   h->chunks.base[h->nchunks++] = h->entry_used;
@@ -694,6 +718,8 @@ int gz_get_params(const gz_alg_t *h, gz_params_t *o) {
   o->batch_factor = h->batch_factor;
   o->vertices_per_tile = 1u << h->tile_shift;
   o->num_tiles = h->ntiles;
+  o->vertices_per_bin = 1u << h->bin_shift;
+  o->num_bins = h->nbins;
   return GZ_OK;
 }
 
@@ -978,16 +1004,24 @@ int gz_get_stream(gz_alg_t *h, void **s) {
   return GZ_OK;
 }
 
-int gz_set_tuning(gz_alg_t *h, uint32_t vpt, uint32_t threads) {
+int gz_set_tuning(gz_alg_t *h, uint32_t vpt, uint32_t threads, uint32_t tiles_per_bin) {
   if (!h) return fail(GZ_ERR_INVALID, "null handle");
   Guard g(h);
   GZ_TRY(push_staged_entries(h));
   GZ_TRY(apply_pending(h));
   GZ_CUDA(cudaStreamSynchronize(h->stream));
-  const uint32_t old_nt = h->ntiles;
-  GZ_TRY(choose_tiling(h, vpt, threads));
-  if (h->ntiles != old_nt) {
-    dev_free(h->d_tile_off);
+  const uint32_t old_nb = h->nbins;
+  const uint32_t keep[4] = {h->tile_shift, h->ntiles, h->bin_shift, h->nbins};
+  const int rc = choose_tiling(h, vpt, threads, tiles_per_bin);
+  if (rc != GZ_OK) {
+    h->tile_shift = keep[0];
+    h->ntiles = keep[1];
+    h->bin_shift = keep[2];
+    h->nbins = keep[3];
+    return rc;
+  }
+  if (h->nbins != old_nb) {
+    dev_free(h->d_bin_off);
     dev_free(h->d_hist);
     dev_free(h->d_scan_tmp);
     h->hist_words = 0;

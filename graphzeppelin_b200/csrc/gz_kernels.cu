@@ -139,31 +139,31 @@ __device__ __forceinline__ void parse_record(const uint8_t *s, uint32_t shift, u
 // ------------------------------------------------------------------------------------------------
 // device gutter
 // ------------------------------------------------------------------------------------------------
+// Counting pass (COUNT) or global-cursor scatter (!COUNT, used only when there are too many
+// bins for the shared-memory sort). With SMEM the per-bin counts of a CTA are gathered in shared
+// memory and added to the global counts once per bin.
 template <int INPUT, bool COUNT, bool SMEM>
 __global__ void __launch_bounds__(512)
 k_gutter(const void *__restrict__ in, uint64_t n, GutterGeom g, uint64_t *__restrict__ hist,
          uint2 *__restrict__ entries, uint32_t *__restrict__ status) {
   extern __shared__ __align__(16) uint8_t gsm[];
   uint32_t *s_bin = reinterpret_cast<uint32_t *>(gsm);
-  const uint32_t nt_pad = (g.ntiles + 3) & ~3u;
+  const uint32_t nt_pad = (g.nbins + 3) & ~3u;
   uint8_t *s_rec = gsm + (SMEM ? nt_pad * 4 : 0);
   const uint32_t G = gridDim.x, cta = blockIdx.x;
   if (SMEM) {
-    for (uint32_t b = threadIdx.x; b < g.ntiles; b += blockDim.x)
-      s_bin[b] = COUNT ? 0u : (uint32_t)hist[(uint64_t)b * G + cta];
+    for (uint32_t b = threadIdx.x; b < g.nbins; b += blockDim.x) s_bin[b] = 0u;
     __syncthreads();
   }
   const uint64_t r0 = n * cta / G, r1 = n * (cta + 1) / G;
   bool bad = false;
   auto emit = [&](uint32_t v, uint32_t w) {
-    const uint32_t t = v >> g.tile_shift;
+    const uint32_t t = v >> g.bin_shift;
     if (COUNT) {
       if (SMEM) atomicAdd(&s_bin[t], 1u);
       else atomicAdd(reinterpret_cast<unsigned long long *>(&hist[t]), 1ull);
     } else {
-      uint64_t p;
-      if (SMEM) p = atomicAdd(&s_bin[t], 1u);
-      else p = atomicAdd(reinterpret_cast<unsigned long long *>(&hist[t]), 1ull);
+      const uint64_t p = atomicAdd(reinterpret_cast<unsigned long long *>(&hist[t]), 1ull);
       entries[p] = make_uint2(v, w);
     }
   };
@@ -198,14 +198,14 @@ k_gutter(const void *__restrict__ in, uint64_t n, GutterGeom g, uint64_t *__rest
   }
   if (COUNT && SMEM) {
     __syncthreads();
-    for (uint32_t b = threadIdx.x; b < g.ntiles; b += blockDim.x)
-      hist[(uint64_t)b * G + cta] = s_bin[b];
+    for (uint32_t b = threadIdx.x; b < g.nbins; b += blockDim.x)
+      if (s_bin[b]) atomicAdd(reinterpret_cast<unsigned long long *>(&hist[b]), (unsigned long long)s_bin[b]);
   }
   if (COUNT && bad) atomicOr(status, kStatusBadVertex);
 }
 
 size_t gutter_smem(int input, GutterGeom g, bool smem) {
-  size_t s = smem ? ((g.ntiles + 3) & ~3u) * 4 : 0;
+  size_t s = smem ? ((g.nbins + 3) & ~3u) * 4 : 0;
   if (input == kInputRecords) s += kRecStageBytes;
   return s;
 }
@@ -224,11 +224,123 @@ cudaError_t launch_gutter(const void *in, uint64_t n, GutterGeom g, int G, uint6
   return cudaGetLastError();
 }
 
-__global__ void k_tile_offsets(const uint64_t *scanned, uint32_t stride, uint32_t ntiles,
-                               const uint64_t *total, uint32_t *tile_off) {
+// Exclusive scan over the 1024 threads of a block (one value per thread).
+__device__ __forceinline__ uint32_t block_scan_1024(uint32_t x, uint32_t *ws /*32*/) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t inc = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(kFull, inc, o);
+    if (lane >= o) inc += y;
+  }
+  if (lane == 31) ws[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = ws[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(kFull, w, o);
+      if (lane >= o) w += y;
+    }
+    ws[lane] = w;
+  }
+  __syncthreads();
+  const uint32_t r = (warp ? ws[warp - 1] : 0) + inc - x;
+  __syncthreads();
+  return r;
+}
+
+// Sort-scatter pass: each CTA takes `rec_tile` inputs at a time, counting-sorts their endpoint
+// entries by bin in shared memory, reserves one contiguous run per bin in the bin's region of the
+// gutter (one global atomic per bin and tile), and writes the runs out, so consecutive threads
+// store to consecutive addresses. base[b] = first slot of bin b, fill[b] = slots taken so far.
+template <int INPUT>
+__global__ void __launch_bounds__(1024, 1)
+k_gutter_sort_scatter(const void *__restrict__ in, uint64_t n, GutterGeom g, uint32_t rec_tile,
+                      const uint64_t *__restrict__ base, uint32_t *__restrict__ fill,
+                      uint2 *__restrict__ entries) {
+  extern __shared__ __align__(16) uint8_t gsm[];
+  __shared__ uint32_t ws[32];
+  const uint32_t nb = g.nbins, nb4 = (nb + 3) & ~3u;
+  uint32_t *s_cur = reinterpret_cast<uint32_t *>(gsm);  // counts, then placement cursors
+  uint32_t *s_off = s_cur + nb4;                         // run start inside the tile
+  uint32_t *s_dst = s_off + nb4;                         // run start inside the gutter
+  const uint32_t ept = INPUT == kInputRecords ? 2 * rec_tile : rec_tile;
+  uint2 *s_sorted = reinterpret_cast<uint2 *>(s_dst + nb4);
+  uint8_t *s_rec = reinterpret_cast<uint8_t *>(s_sorted + ept);
+  const uint8_t *rec = reinterpret_cast<const uint8_t *>(in);
+  const uint2 *ein = reinterpret_cast<const uint2 *>(in);
+  const uint32_t per_thread = (nb + blockDim.x - 1) / blockDim.x;  // bins per thread (<= 4)
+  for (uint64_t t0 = blockIdx.x * (uint64_t)rec_tile; t0 < n; t0 += (uint64_t)gridDim.x * rec_tile) {
+    const uint32_t cnt = (uint32_t)(n - t0 < rec_tile ? n - t0 : rec_tile);
+    for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) s_cur[b] = 0u;
+    uint32_t shift = 0;
+    if (INPUT == kInputRecords) shift = stage_records(rec, t0, cnt, s_rec);
+    __syncthreads();
+    // 1. count entries per bin
+    for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
+      uint32_t u, v;
+      if (INPUT == kInputRecords) {
+        parse_record(s_rec, shift, i, u, v);
+      } else {
+        const uint2 x = ein[t0 + i];
+        u = x.x;
+        v = x.y;
+      }
+      if (u >= g.V || v >= g.V) continue;
+      atomicAdd(&s_cur[u >> g.bin_shift], 1u);
+      if (INPUT == kInputRecords) atomicAdd(&s_cur[v >> g.bin_shift], 1u);
+    }
+    __syncthreads();
+    // 2. run offsets inside the tile (bins [tid*per_thread, +per_thread) per thread)
+    uint32_t local[4] = {0, 0, 0, 0}, sum = 0;
+    for (uint32_t k = 0; k < per_thread; ++k) {
+      const uint32_t b = threadIdx.x * per_thread + k;
+      local[k] = b < nb ? s_cur[b] : 0u;
+      sum += local[k];
+    }
+    uint32_t run = block_scan_1024(sum, ws);
+    for (uint32_t k = 0; k < per_thread; ++k) {
+      const uint32_t b = threadIdx.x * per_thread + k;
+      if (b < nb) {
+        s_off[b] = run;
+        s_dst[b] = local[k] ? (uint32_t)base[b] + atomicAdd(&fill[b], local[k]) : 0u;
+        s_cur[b] = run;
+      }
+      run += local[k];
+    }
+    __syncthreads();
+    // 3. place entries in bin order
+    for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
+      uint32_t u, v;
+      if (INPUT == kInputRecords) {
+        parse_record(s_rec, shift, i, u, v);
+      } else {
+        const uint2 x = ein[t0 + i];
+        u = x.x;
+        v = x.y;
+      }
+      if (u >= g.V || v >= g.V) continue;
+      s_sorted[atomicAdd(&s_cur[u >> g.bin_shift], 1u)] = make_uint2(u, v);
+      if (INPUT == kInputRecords) s_sorted[atomicAdd(&s_cur[v >> g.bin_shift], 1u)] = make_uint2(v, u);
+    }
+    __syncthreads();
+    // 4. coalesced write-out of the runs
+    const uint32_t total = s_cur[nb - 1];
+    for (uint32_t j = threadIdx.x; j < total; j += blockDim.x) {
+      const uint2 x = s_sorted[j];
+      const uint32_t b = x.x >> g.bin_shift;
+      entries[s_dst[b] + (j - s_off[b])] = x;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void k_bin_offsets(const uint64_t *scanned, uint32_t stride, uint32_t nbins,
+                              const uint64_t *total, uint32_t *bin_off) {
   const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b < ntiles) tile_off[b] = (uint32_t)scanned[(uint64_t)b * stride];
-  if (b == ntiles) tile_off[b] = (uint32_t)*total;
+  if (b < nbins) bin_off[b] = (uint32_t)scanned[(uint64_t)b * stride];
+  if (b == nbins) bin_off[b] = (uint32_t)*total;
 }
 
 __global__ void k_copy_u64(const uint64_t *src, uint64_t *dst, uint64_t n) {
@@ -334,15 +446,17 @@ __device__ __forceinline__ void apply_entry(uint2 e, uint32_t *s_sk, uint32_t vm
 
 __global__ void __launch_bounds__(1024, 1)
 k_sketch_update(SketchGeom g, uint8_t *__restrict__ sketches, const uint2 *__restrict__ entries,
-                ChunkTable chunks, const uint32_t *__restrict__ tile_off, int nchunks,
+                ChunkTable chunks, const uint32_t *__restrict__ bin_off, int nchunks,
                 const uint64_t *__restrict__ flip, uint32_t *work_counter, uint32_t *status) {
   extern __shared__ __align__(128) uint8_t dsm[];
   __shared__ __align__(8) uint64_t s_bar;
   __shared__ uint32_t s_tile, s_total;
   const uint32_t vpt = 1u << g.tile_shift;
   const uint32_t tile_bytes = vpt * g.sketch_words * 4;
+  const uint32_t per_bin = g.bin_shift - g.tile_shift;  // log2(tiles per bin)
   uint32_t *s_sk = reinterpret_cast<uint32_t *>(dsm);
-  uint64_t *s_flip = reinterpret_cast<uint64_t *>(dsm + tile_bytes);
+  uint2 *s_queue = reinterpret_cast<uint2 *>(dsm + tile_bytes);
+  uint64_t *s_flip = reinterpret_cast<uint64_t *>(dsm + tile_bytes + kQueueBytes);
   for (uint32_t i = threadIdx.x; i <= g.C; i += blockDim.x) s_flip[i] = flip[i];
   const uint32_t bar = smem_u32(&s_bar);
   if (threadIdx.x == 0) {
@@ -351,15 +465,19 @@ k_sketch_update(SketchGeom g, uint8_t *__restrict__ sketches, const uint2 *__res
   }
   __syncthreads();
   const uint64_t flip_chk = s_flip[g.C];
-  const uint32_t stride = g.ntiles + 1;
+  const uint32_t stride = g.nbins + 1;
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  uint2 *q = s_queue + warp * 64;
   uint32_t parity = 0;
   for (;;) {
     if (threadIdx.x == 0) {
       const uint32_t t = atomicAdd(work_counter, 1u);
       uint32_t total = 0;
-      if (t < g.ntiles)
+      if (t < g.ntiles) {
+        const uint32_t bin = t >> per_bin;
         for (int k = 0; k < nchunks; ++k)
-          total += tile_off[(uint64_t)k * stride + t + 1] - tile_off[(uint64_t)k * stride + t];
+          total += bin_off[(uint64_t)k * stride + bin + 1] - bin_off[(uint64_t)k * stride + bin];
+      }
       s_tile = t;
       s_total = total;
       if (t < g.ntiles && total) {
@@ -383,11 +501,41 @@ k_sketch_update(SketchGeom g, uint8_t *__restrict__ sketches, const uint2 *__res
         }
         return;
       }
-      for (int k = 0; k < nchunks; ++k) {
-        const uint64_t b = chunks.base[k] + tile_off[(uint64_t)k * stride + t];
-        const uint64_t e = chunks.base[k] + tile_off[(uint64_t)k * stride + t + 1];
-        for (uint64_t i = b + threadIdx.x; i < e; i += blockDim.x)
-          apply_entry(entries[i], s_sk, vpt - 1, g.sketch_words, s_flip, flip_chk, g.C, g.B);
+      const uint32_t bin = t >> per_bin;
+      if (per_bin == 0) {
+        // the bin is this tile: every entry applies
+        for (int k = 0; k < nchunks; ++k) {
+          const uint64_t b = chunks.base[k] + bin_off[(uint64_t)k * stride + bin];
+          const uint64_t e = chunks.base[k] + bin_off[(uint64_t)k * stride + bin + 1];
+          for (uint64_t i = b + threadIdx.x; i < e; i += blockDim.x)
+            apply_entry(entries[i], s_sk, vpt - 1, g.sketch_words, s_flip, flip_chk, g.C, g.B);
+        }
+      } else {
+        // the bin holds several tiles: each warp ballots its 32 entries, appends this tile's to
+        // its queue, and hashes only full warps of queued entries
+        uint32_t qn = 0;
+        for (int k = 0; k < nchunks; ++k) {
+          const uint64_t b = chunks.base[k] + bin_off[(uint64_t)k * stride + bin];
+          const uint64_t e = chunks.base[k] + bin_off[(uint64_t)k * stride + bin + 1];
+          for (uint64_t i0 = b + (uint64_t)warp * 32; i0 < e; i0 += (uint64_t)nwarps * 32) {
+            const uint64_t i = i0 + lane;
+            uint2 x = make_uint2(0u, 0u);
+            if (i < e) x = entries[i];
+            const bool mine = i < e && (x.x >> g.tile_shift) == t;
+            const uint32_t m = __ballot_sync(kFull, mine);
+            if (mine) q[qn + __popc(m & ((1u << lane) - 1u))] = x;
+            qn += __popc(m);
+            __syncwarp();
+            if (qn >= 32) {
+              apply_entry(q[lane], s_sk, vpt - 1, g.sketch_words, s_flip, flip_chk, g.C, g.B);
+              __syncwarp();
+              qn -= 32;
+              if (lane < qn) q[lane] = q[32 + lane];
+              __syncwarp();
+            }
+          }
+        }
+        if (lane < qn) apply_entry(q[lane], s_sk, vpt - 1, g.sketch_words, s_flip, flip_chk, g.C, g.B);
       }
       fence_proxy_async_smem();
       __syncthreads();
@@ -778,35 +926,60 @@ cudaError_t scan_exclusive_u64(uint64_t *d, uint64_t n, uint64_t *total, uint64_
   return cudaGetLastError();
 }
 
-cudaError_t gutter_count_2d(int input, const void *in, uint64_t n, GutterGeom g, int G,
-                            uint64_t *hist, uint32_t *status, cudaStream_t s) {
-  return input == kInputRecords
-             ? launch_gutter<kInputRecords, true, true>(in, n, g, G, hist, nullptr, status, s)
-             : launch_gutter<kInputEntries, true, true>(in, n, g, G, hist, nullptr, status, s);
+cudaError_t gutter_count(int input, const void *in, uint64_t n, GutterGeom g, int G,
+                         uint64_t *counts, uint32_t *status, cudaStream_t s) {
+  const bool smem = g.nbins <= kSmemBinsMax;
+  if (input == kInputRecords)
+    return smem ? launch_gutter<kInputRecords, true, true>(in, n, g, G, counts, nullptr, status, s)
+                : launch_gutter<kInputRecords, true, false>(in, n, g, G, counts, nullptr, status, s);
+  return smem ? launch_gutter<kInputEntries, true, true>(in, n, g, G, counts, nullptr, status, s)
+              : launch_gutter<kInputEntries, true, false>(in, n, g, G, counts, nullptr, status, s);
 }
-cudaError_t gutter_scatter_2d(int input, const void *in, uint64_t n, GutterGeom g, int G,
-                              const uint64_t *hist, uint2 *entries, cudaStream_t s) {
-  uint64_t *h = const_cast<uint64_t *>(hist);
-  return input == kInputRecords
-             ? launch_gutter<kInputRecords, false, true>(in, n, g, G, h, entries, nullptr, s)
-             : launch_gutter<kInputEntries, false, true>(in, n, g, G, h, entries, nullptr, s);
-}
-cudaError_t gutter_count_1d(int input, const void *in, uint64_t n, GutterGeom g, int G,
-                            uint64_t *counts, uint32_t *status, cudaStream_t s) {
-  return input == kInputRecords
-             ? launch_gutter<kInputRecords, true, false>(in, n, g, G, counts, nullptr, status, s)
-             : launch_gutter<kInputEntries, true, false>(in, n, g, G, counts, nullptr, status, s);
-}
-cudaError_t gutter_scatter_1d(int input, const void *in, uint64_t n, GutterGeom g, int G,
-                              uint64_t *cursor, uint2 *entries, cudaStream_t s) {
+
+cudaError_t gutter_scatter_global(int input, const void *in, uint64_t n, GutterGeom g, int G,
+                                  uint64_t *cursor, uint2 *entries, cudaStream_t s) {
   return input == kInputRecords
              ? launch_gutter<kInputRecords, false, false>(in, n, g, G, cursor, entries, nullptr, s)
              : launch_gutter<kInputEntries, false, false>(in, n, g, G, cursor, entries, nullptr, s);
 }
-cudaError_t gutter_tile_offsets(const uint64_t *scanned, uint32_t stride, uint32_t ntiles,
-                                const uint64_t *total, uint32_t *tile_off, cudaStream_t s) {
-  k_tile_offsets<<<blocks_for(ntiles + 1, 256), 256, 0, s>>>(scanned, stride, ntiles, total,
-                                                             tile_off);
+
+uint32_t sort_scatter_tile(int input, GutterGeom g, size_t smem_budget) {
+  const size_t fixed = (size_t)3 * ((g.nbins + 3) & ~3u) * 4 + 64;
+  if (g.nbins > kSortBinsMax || fixed >= smem_budget) return 0;
+  const size_t per = input == kInputRecords ? 9 + 16 : 8;
+  size_t t = (smem_budget - fixed - (input == kInputRecords ? 48 : 0)) / per;
+  t = std::min<size_t>(t, input == kInputRecords ? 8192 : 16384);
+  t &= ~(size_t)127;
+  return (uint32_t)t;
+}
+
+cudaError_t gutter_sort_scatter(int input, const void *in, uint64_t n, GutterGeom g,
+                                uint32_t rec_tile, const uint64_t *base, uint32_t *fill,
+                                uint2 *entries, cudaStream_t s) {
+  const size_t nb4 = (g.nbins + 3) & ~3u;
+  const size_t smem = 3 * nb4 * 4 + (size_t)rec_tile * (input == kInputRecords ? 16 : 8) +
+                      (input == kInputRecords ? (size_t)rec_tile * 9 + 48 : 0);
+  const int G = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)num_sms(),
+                                                               (n + rec_tile - 1) / rec_tile));
+  if (input == kInputRecords) {
+    cudaError_t e = cudaFuncSetAttribute(k_gutter_sort_scatter<kInputRecords>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_gutter_sort_scatter<kInputRecords><<<G, 1024, smem, s>>>(in, n, g, rec_tile, base, fill, entries);
+  } else {
+    cudaError_t e = cudaFuncSetAttribute(k_gutter_sort_scatter<kInputEntries>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_gutter_sort_scatter<kInputEntries><<<G, 1024, smem, s>>>(in, n, g, rec_tile, base, fill, entries);
+  }
+  g_launches++;
+  return cudaGetLastError();
+}
+
+cudaError_t gutter_bin_offsets(const uint64_t *scanned, uint32_t stride, uint32_t nbins,
+                               const uint64_t *total, uint32_t *bin_off, cudaStream_t s) {
+  k_bin_offsets<<<blocks_for(nbins + 1, 256), 256, 0, s>>>(scanned, stride, nbins, total,
+                                                           bin_off);
   g_launches++;
   return cudaGetLastError();
 }
@@ -817,7 +990,7 @@ cudaError_t copy_u64(const uint64_t *src, uint64_t *dst, uint64_t n, cudaStream_
 }
 
 size_t sketch_update_smem_bytes(SketchGeom g) {
-  return ((size_t)g.sketch_words * 4 << g.tile_shift) + (size_t)(g.C + 1) * 8;
+  return ((size_t)g.sketch_words * 4 << g.tile_shift) + kQueueBytes + (size_t)(g.C + 1) * 8;
 }
 
 cudaError_t sketch_update_prepare(SketchGeom g, int /*threads*/) {
@@ -826,12 +999,20 @@ cudaError_t sketch_update_prepare(SketchGeom g, int /*threads*/) {
                               (int)smem);
 }
 
+int sketch_update_ctas_per_sm(SketchGeom g, int threads) {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sketch_update, threads,
+                                                    sketch_update_smem_bytes(g)) != cudaSuccess)
+    return 1;
+  return n > 0 ? n : 1;
+}
+
 cudaError_t sketch_update(SketchGeom g, uint8_t *sketches, const uint2 *entries,
-                          const ChunkTable &chunks, const uint32_t *tile_off, int nchunks,
+                          const ChunkTable &chunks, const uint32_t *bin_off, int nchunks,
                           const uint64_t *flip, uint32_t *work_counter, uint32_t *status, int grid,
                           int threads, cudaStream_t s) {
   const size_t smem = sketch_update_smem_bytes(g);
-  k_sketch_update<<<grid, threads, smem, s>>>(g, sketches, entries, chunks, tile_off, nchunks, flip,
+  k_sketch_update<<<grid, threads, smem, s>>>(g, sketches, entries, chunks, bin_off, nchunks, flip,
                                               work_counter, status);
   g_launches++;
   return cudaGetLastError();

@@ -18,11 +18,13 @@ enum GutterInput : int {
   kInputEntries = 1,  // uint2 {vertex, neighbour}: 1 endpoint entry
 };
 
-// Geometry shared by the gutter kernels.
+// Geometry shared by the gutter kernels. A gutter bin groups 1 << bin_shift consecutive
+// vertices; it is coarser than the shared-memory tile of the sketch-update kernel so the scatter
+// has few enough destinations for its partial lines to stay in L2.
 struct GutterGeom {
   uint32_t V;
-  uint32_t tile_shift;  // tile of a vertex = v >> tile_shift (vertices_per_tile = 1 << shift)
-  uint32_t ntiles;
+  uint32_t bin_shift;  // bin of a vertex = v >> bin_shift
+  uint32_t nbins;
 };
 
 // Maximum number of gutter chunks buffered before the sketches must be updated.
@@ -36,14 +38,18 @@ struct SketchGeom {
   uint32_t C;                  // columns
   uint32_t B;                  // buckets per column
   uint32_t sketch_words;       // (C*B+1)*3 32-bit words per vertex sketch
-  uint32_t tile_shift;
+  uint32_t tile_shift;         // vertices staged together in shared memory = 1 << tile_shift
   uint32_t ntiles;
+  uint32_t bin_shift;          // gutter bin (>= tile_shift); a bin holds 1 << (bin - tile) tiles
+  uint32_t nbins;
 };
 
-// Records per staging tile of the gutter kernels, and the largest tile count for which the
+// Records per staging tile of the gutter kernels, and the largest bin count for which the
 // per-CTA histogram lives in shared memory.
 constexpr int kRecTile = 4096;
 constexpr uint32_t kSmemBinsMax = 12288;
+// Largest bin count handled by the shared-memory sort-scatter (above it: global cursors).
+constexpr uint32_t kSortBinsMax = 4096;
 
 // ---- scan -------------------------------------------------------------------------------------
 // Exclusive prefix sum over n u64 values, in place; writes the total to *d_total. `tmp` must
@@ -53,29 +59,37 @@ cudaError_t scan_exclusive_u64(uint64_t *d_data, uint64_t n, uint64_t *d_total, 
                                cudaStream_t s);
 
 // ---- device gutter ----------------------------------------------------------------------------
-// 2-D path (ntiles <= kSmemBinsMax): per-CTA histograms -> hist[tile * G + cta], scan, scatter
-// with shared-memory cursors. 1-D path: global counters.
-cudaError_t gutter_count_2d(int input, const void *d_in, uint64_t n, GutterGeom g, int G,
-                            uint64_t *hist, uint32_t *status, cudaStream_t s);
-cudaError_t gutter_scatter_2d(int input, const void *d_in, uint64_t n, GutterGeom g, int G,
-                              const uint64_t *hist_scanned, uint2 *entries, cudaStream_t s);
-cudaError_t gutter_count_1d(int input, const void *d_in, uint64_t n, GutterGeom g, int G,
-                            uint64_t *counts, uint32_t *status, cudaStream_t s);
-cudaError_t gutter_scatter_1d(int input, const void *d_in, uint64_t n, GutterGeom g, int G,
-                              uint64_t *cursor, uint2 *entries, cudaStream_t s);
-// tile_off[b] = scanned[b * stride], tile_off[ntiles] = *total  (u32, relative to chunk base)
-cudaError_t gutter_tile_offsets(const uint64_t *scanned, uint32_t stride, uint32_t ntiles,
-                                const uint64_t *total, uint32_t *tile_off, cudaStream_t s);
+// counts[b] += endpoint entries of bin b (counts zeroed by the caller); flags bad vertex ids.
+cudaError_t gutter_count(int input, const void *d_in, uint64_t n, GutterGeom g, int G,
+                         uint64_t *counts, uint32_t *status, cudaStream_t s);
+// Inputs per tile of the shared-memory sort-scatter for this geometry (0: not applicable).
+uint32_t sort_scatter_tile(int input, GutterGeom g, size_t smem_budget);
+// Entries of bin b go to entries[base[b] + ...]; fill (nbins u32) must start at zero.
+cudaError_t gutter_sort_scatter(int input, const void *d_in, uint64_t n, GutterGeom g,
+                                uint32_t rec_tile, const uint64_t *base, uint32_t *fill,
+                                uint2 *entries, cudaStream_t s);
+// Fallback for many bins: one global atomic cursor per bin (cursor = copy of base).
+cudaError_t gutter_scatter_global(int input, const void *d_in, uint64_t n, GutterGeom g, int G,
+                                  uint64_t *cursor, uint2 *entries, cudaStream_t s);
+// bin_off[b] = scanned[b * stride], bin_off[nbins] = *total  (u32, relative to chunk base)
+cudaError_t gutter_bin_offsets(const uint64_t *scanned, uint32_t stride, uint32_t nbins,
+                               const uint64_t *total, uint32_t *bin_off, cudaStream_t s);
 // gutter_scatter_1d consumes cursors; copy scanned counts into them first.
 cudaError_t copy_u64(const uint64_t *src, uint64_t *dst, uint64_t n, cudaStream_t s);
 
 // ---- sketch update -------------------------------------------------------------------------------
+// Per-warp queues (64 entries x 32 warps) that compact the entries of a bin belonging to this
+// CTA's tile into full warps.
+constexpr size_t kQueueBytes = 64 * 8 * 32;
 size_t sketch_update_smem_bytes(SketchGeom g);
 cudaError_t sketch_update_prepare(SketchGeom g, int threads);
-// Applies every buffered entry of `nchunks` chunks: for each tile with entries, stage its
-// sketches in shared memory with bulk async copies, XOR every entry in, write the tile back.
+// CTAs of the sketch-update kernel that fit on one SM at this geometry.
+int sketch_update_ctas_per_sm(SketchGeom g, int threads);
+// Applies every buffered entry of `nchunks` chunks: for each tile whose bin has entries, stage
+// its sketches in shared memory with bulk async copies, XOR in the bin entries that belong to
+// the tile, write the tile back.
 cudaError_t sketch_update(SketchGeom g, uint8_t *sketches, const uint2 *entries,
-                          const ChunkTable &chunks, const uint32_t *tile_off, int nchunks,
+                          const ChunkTable &chunks, const uint32_t *bin_off, int nchunks,
                           const uint64_t *flip, uint32_t *work_counter, uint32_t *status,
                           int grid, int threads, cudaStream_t s);
 // XOR num_buckets raw buckets (device) into the sketch of vertex v.

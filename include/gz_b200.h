@@ -69,6 +69,8 @@ typedef struct gz_params {
   double batch_factor;          /* CCAlgConfiguration::get_batch_factor */
   uint32_t vertices_per_tile;   /* device layout: sketches staged together in shared memory */
   uint32_t num_tiles;
+  uint32_t vertices_per_bin;    /* device gutter: vertices sharing one gutter bin */
+  uint32_t num_bins;
 } gz_params_t;
 
 /* One sampled component of one Boruvka round (parity tracing). key = smallest member id. */
@@ -211,9 +213,11 @@ GZ_API int gz_get_stream(gz_alg_t *alg, void **stream_out);
  * device. *hashes_per_s gets the best of `repeats` launches. */
 GZ_API int gz_measure_hash_rate(int repeats, double *hashes_per_s);
 
-/* Tuning knobs of the sketch-update kernel (0 keeps the current value): vertices staged per
- * tile (multiple of 4), threads per block. Takes effect on an empty gutter. */
-GZ_API int gz_set_tuning(gz_alg_t *alg, uint32_t vertices_per_tile, uint32_t threads_per_block);
+/* Tuning knobs of the ingest kernels (0 picks the default): vertices staged per shared-memory
+ * tile (power of two in [4, 64]), threads per block of the sketch-update kernel, and tiles per
+ * gutter bin (power of two <= 64). Buffered updates are applied first. */
+GZ_API int gz_set_tuning(gz_alg_t *alg, uint32_t vertices_per_tile, uint32_t threads_per_block,
+                         uint32_t tiles_per_bin);
 
 #ifdef __cplusplus
 }
