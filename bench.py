@@ -71,7 +71,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -161,21 +161,27 @@ def cpu_baseline(stream, cfg, target_s=12.0):
 
 
 # ------------------------------------------------------------------------------------------------
-def roofline_terms(alg, n_records, t_launch_s, hash_peak, hbm_peak_gbs):
+def roofline_terms(alg, n_records, t_launch_s, hash_peak, hbm_peak_gbs, update_peak):
     p = alg.params
     V, C, sb = p.num_vertices, p.num_columns, p.sketch_bytes
     entries = 2 * n_records
-    # sketch-update kernel: reads every gutter entry (8 B) once, reads + writes every touched
-    # sketch once; evaluates 1 + C hashes per endpoint update
+    # sketch-update kernel (plain entries): reads every gutter entry (8 B) once, reads + writes
+    # every touched sketch once; evaluates 1 + C hashes and XORs 1 + C buckets (3 shared-memory
+    # atomics each) per endpoint update
     bytes_alg = entries * 8 + 2 * V * sb
     hashes = entries * (C + 1)
-    t_hbm = bytes_alg / (hbm_peak_gbs * 1e9)
-    t_int = hashes / hash_peak
+    updates = entries * (C + 1)
+    t = {"hbm": bytes_alg / (hbm_peak_gbs * 1e9), "int": hashes / hash_peak,
+         "smem_atomic": updates / update_peak}
     hbm = {"achieved": bytes_alg / t_launch_s / 1e9, "peak": hbm_peak_gbs, "unit": "GB/s",
            "frac": (bytes_alg / t_launch_s / 1e9) / hbm_peak_gbs, "bytes_per_launch": bytes_alg}
     integer = {"achieved": hashes / t_launch_s / 1e9, "peak": hash_peak / 1e9, "unit": "Ghash/s",
                "frac": (hashes / t_launch_s) / hash_peak, "hashes_per_launch": hashes}
-    return hbm, integer, ("int" if t_int > t_hbm else "hbm")
+    smem = {"achieved": updates / t_launch_s / 1e9, "peak": update_peak / 1e9,
+            "unit": "Gupdate/s", "frac": (updates / t_launch_s) / update_peak,
+            "bucket_updates_per_launch": updates}
+    bound = max(t, key=t.get)
+    return {"hbm": hbm, "int": integer, "smem_atomic": smem}, bound
 
 
 def load_traffic(workload):
@@ -187,6 +193,18 @@ def load_traffic(workload):
         return d.get(workload)
     except Exception:
         return None
+
+
+def combine_ranks(local_total_ms: float, records_per_rank: int, steps: int, world: int, dist=None,
+                  device=None):
+    """Whole-job result over replicas: the slowest rank's device time, every rank's records."""
+    total_ms = local_total_ms
+    if dist is not None and world > 1:
+        import torch
+        tt = torch.tensor([local_total_ms], dtype=torch.float64, device=device)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+    return total_ms, world * records_per_rank * steps / (total_ms / 1e3)
 
 
 def run_b200(args, cfg):
@@ -262,12 +280,8 @@ def run_b200(args, cfg):
     ingest_ms = [a.elapsed_time(b) for a, b, c, _ in marks]
     query_ms = [b.elapsed_time(c) for a, b, c, _ in marks]
     total_ms = sum(a.elapsed_time(c) for a, b, c, _ in marks)
-    if dist:
-        tt = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms = float(tt.item())
+    total_ms, value = combine_ranks(total_ms, n, args.steps, world, dist, device="cuda")
     ms_per_step = total_ms / args.steps
-    value = world * n * args.steps / (total_ms / 1e3)
 
     # end to end through the public API: pinned host records in, partition out
     e2e_s = []
@@ -299,25 +313,33 @@ def run_b200(args, cfg):
         except Exception:
             peak_src = "fallback 6546.2 GB/s"
         hash_peak = gzcc.measure_hash_rate(5)
+        update_peak = gzcc.measure_update_rate(5)
         launches = max(1, prof["sketch_update_launches"])
         t_launch = prof["sketch_update_ms"] / launches / 1e3
-        hbm, integer, bound = roofline_terms(alg, n, t_launch, hash_peak, hbm_peak)
-        main = integer if bound == "int" else hbm
+        terms, bound = roofline_terms(alg, n, t_launch, hash_peak, hbm_peak, update_peak)
+        main = terms[bound]
         traffic = load_traffic(cfg["workload"])
         roof = {"bound": bound, "achieved": main["achieved"], "peak": main["peak"],
                 "unit": main["unit"], "frac": main["frac"], "traffic": traffic,
                 "kernel": "k_sketch_update",
                 "launch_ms": t_launch * 1e3,
-                "terms": {"hbm": hbm, "int": integer},
+                "terms": terms,
                 "peaks": {"hbm": peak_src,
                           "int": "measured here: gz_measure_hash_rate (register-only XXH3-8B + "
-                                 "depth ctz kernel, best of 5)"}}
+                                 "depth ctz kernel, best of 5)",
+                          "smem_atomic": "measured here: gz_measure_update_rate (3 x 32-bit "
+                                         "shared atomicXor per random 12-byte bucket, 1024 "
+                                         "threads/SM, best of 5)"}}
         # the whole ingest (gutter + sketch update) against the path roofline: 9 B read per
         # record + sketch RMW, 1 + C hashes per record (one hash per edge)
         p = alg.params
         ing_s = statistics.mean(ingest_ms) / 1e3
         path_bytes = 9 * n + 2 * V * p.sketch_bytes
         path_hashes = n * (p.num_columns + 1)
+        path_updates = 2 * n * (p.num_columns + 1)
+        path_terms = {"hbm_ms": path_bytes / (hbm_peak * 1e9) * 1e3,
+                      "int_ms": path_hashes / hash_peak * 1e3,
+                      "smem_atomic_ms": path_updates / update_peak * 1e3}
         path_t = max(path_bytes / (hbm_peak * 1e9), path_hashes / hash_peak)
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
@@ -338,7 +360,11 @@ def run_b200(args, cfg):
             "ingest_ms": statistics.mean(ingest_ms),
             "ingest_updates_per_s": n / ing_s,
             "path_roofline": {"time_ms": path_t * 1e3, "frac": path_t / ing_s,
-                              "bytes": path_bytes, "hashes": path_hashes},
+                              "bytes": path_bytes, "hashes": path_hashes,
+                              "definition": "max(9 B/record + sketch RMW over HBM, one hash "
+                                            "per record per column over the hash peak)",
+                              "terms_ms": path_terms,
+                              "frac_with_smem_term": max(path_terms.values()) / 1e3 / ing_s},
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": e2e,
@@ -396,7 +422,7 @@ def run_reference(args, cfg):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--small", action="store_true", help="V=2^14 case (profiling)")

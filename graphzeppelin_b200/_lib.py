@@ -77,12 +77,13 @@ SIGNATURES = [
     ("gz_dump_sketches", _i, [_H, _P, _sz]),
     ("gz_clear", _i, [_H]),
     ("gz_measure_hash_rate", _i, [_i, ctypes.POINTER(_d)]),
+    ("gz_measure_update_rate", _i, [_i, ctypes.POINTER(_d)]),
     ("gz_set_trace", _i, [_H, _i]),
     ("gz_get_trace", _i, [_H, _P, _sz, ctypes.POINTER(_sz)]),
     ("gz_set_profiling", _i, [_H, _i]),
     ("gz_get_profile", _i, [_H, ctypes.POINTER(gz_profile_t)]),
     ("gz_get_stream", _i, [_H, ctypes.POINTER(ctypes.c_void_p)]),
-    ("gz_set_tuning", _i, [_H, _u32, _u32, _u32]),
+    ("gz_set_tuning", _i, [_H, _u32, _u32, _u32, _u32]),
 ]
 
 _lib = None

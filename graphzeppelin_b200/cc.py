@@ -447,9 +447,10 @@ class CCSketchAlg:
         return int(s.value or 0)
 
     def set_tuning(self, vertices_per_tile: int = 0, threads_per_block: int = 0,
-                   tiles_per_bin: int = 0) -> None:
+                   tiles_per_bin: int = 0, entry_form: int = 0) -> None:
+        """0 keeps defaults; entry_form 1 = plain entries, 2 = hashed entries."""
         _check(self.lib.gz_set_tuning(self._h, vertices_per_tile, threads_per_block,
-                                      tiles_per_bin))
+                                      tiles_per_bin, entry_form))
         p = _lib.gz_params_t()
         _check(self.lib.gz_get_params(self._h, ctypes.byref(p)))
         self.params = p
@@ -463,6 +464,14 @@ def measure_hash_rate(repeats: int = 5) -> float:
     lib = _lib.load()
     out = ctypes.c_double()
     _check(lib.gz_measure_hash_rate(repeats, ctypes.byref(out)))
+    return out.value
+
+
+def measure_update_rate(repeats: int = 5) -> float:
+    """Peak shared-memory 12-byte bucket XOR updates per second of the current GPU."""
+    lib = _lib.load()
+    out = ctypes.c_double()
+    _check(lib.gz_measure_update_rate(repeats, ctypes.byref(out)))
     return out.value
 
 

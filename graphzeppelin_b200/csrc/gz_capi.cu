@@ -104,8 +104,13 @@ struct gz_alg {
   uint32_t *d_status = nullptr;  // [0] status bits, [1] work counter
   uint32_t *h_status = nullptr;  // pinned mirror
   // device gutter
-  uint2 *d_entries = nullptr;
-  uint64_t entry_cap = 0, entry_used = 0;
+  uint8_t *d_gutter = nullptr;  // chunks of plain (8 B) or hashed (32 B) endpoint entries
+  uint64_t entry_cap = 0;       // capacity in endpoint updates
+  uint64_t gutter_bytes = 0, gutter_used = 0, entries_pending = 0;
+  bool hashed = false;          // records become hashed entries (each edge hashed once)
+  bool hashed_default = false;
+  uint32_t *d_hist2d = nullptr;
+  size_t hist2d_words = 0;
   gz::ChunkTable chunks{};
   int nchunks = 0;
   uint32_t *d_bin_off = nullptr;
@@ -218,7 +223,7 @@ namespace {
 // Default gutter bins: the fewest tiles per bin that brings the bin count within the
 // shared-memory sort-scatter's range (each extra tile per bin costs the sketch-update kernel a
 // pass over the other tiles' entries).
-constexpr uint32_t kBinTarget = gz::kSortBinsMax;
+constexpr uint32_t kBinTarget = 4096;  // measured best on B200 at 2^17 vertices (2 tiles per bin)
 constexpr uint32_t kMaxTilesPerBin = 16;
 
 int choose_tiling(gz_alg *h, uint32_t vpt_req, uint32_t threads_req, uint32_t tpb_req) {
@@ -252,11 +257,11 @@ int choose_tiling(gz_alg *h, uint32_t vpt_req, uint32_t threads_req, uint32_t tp
     if (tpb_req & (tpb_req - 1) || tpb_req > 64)
       return fail(GZ_ERR_INVALID, "tiles_per_bin must be a power of two <= 64");
     bshift = shift + (uint32_t)__builtin_ctz(tpb_req);
-  } else {
+  } else if (!h->hashed) {
     while (((h->V + (1u << bshift) - 1) >> bshift) > kBinTarget &&
            (1u << (bshift - shift)) < kMaxTilesPerBin)
       ++bshift;
-  }
+  }  // hashed entries are full 32-byte sectors: one bin per tile, no compaction pass needed
   h->bin_shift = bshift;
   h->nbins = (uint32_t)((h->V + (1u << bshift) - 1) >> bshift);
   if (threads_req) {
@@ -278,6 +283,8 @@ int init_alg(gz_alg *h, uint32_t V, uint64_t seed, double sf, double bf) {
   h->batch_factor = bf > 0 ? bf : 1;     // CCAlgConfiguration::batch_factor
   reference_params(V, h->sketches_factor, h->C, h->B);
   if (h->B > 63) return fail(GZ_ERR_INVALID, "bkt_per_col above 63 is not supported");
+  h->hashed_default = false;  // plain entries measured faster on B200 (see the design notes)
+  h->hashed = h->hashed_default;
   h->nb = h->C * h->B + 1;
   h->sketch_bytes = (uint64_t)h->nb * gz::kBucketBytes;
   {
@@ -313,7 +320,8 @@ void destroy_alg(gz_alg *h) {
   dev_free(h->d_flip);
   dev_free(h->d_status);
   host_free(h->h_status);
-  dev_free(h->d_entries);
+  dev_free(h->d_gutter);
+  dev_free(h->d_hist2d);
   dev_free(h->d_bin_off);
   dev_free(h->d_hist);
   dev_free(h->d_scan_tmp);
@@ -362,8 +370,15 @@ void destroy_alg(gz_alg *h) {
 
 // ---- device gutter -------------------------------------------------------------------------------
 
+uint64_t entry_bytes(const gz_alg *h, int input) {
+  return input == gz::kInputRecords && h->hashed ? 32 : 8;
+}
+
 int ensure_gutter(gz_alg *h) {
-  GZ_TRY(dev_alloc(&h->d_entries, h->entry_cap));
+  if (!h->d_gutter) {
+    h->gutter_bytes = h->entry_cap * (h->hashed ? 32 : 8);
+    GZ_TRY(dev_alloc(&h->d_gutter, h->gutter_bytes));
+  }
   GZ_TRY(dev_alloc(&h->d_bin_off, (size_t)gz::kMaxChunks * (h->nbins + 1)));
   const size_t words = h->nbins;
   if (h->hist_words < words) {
@@ -389,12 +404,13 @@ int apply_pending(gz_alg *h) {
   const int per_sm = gz::sketch_update_ctas_per_sm(g, (int)h->threads);
   const int grid = (int)std::min<uint64_t>(h->ntiles, (uint64_t)gz::num_sms() * per_sm);
   const int pi = h->prof_begin();
-  GZ_CUDA(gz::sketch_update(g, h->d_sk, h->d_entries, h->chunks, h->d_bin_off, h->nchunks, h->d_flip,
+  GZ_CUDA(gz::sketch_update(g, h->d_sk, h->d_gutter, h->chunks, h->d_bin_off, h->nchunks, h->d_flip,
                             h->d_status + 1, h->d_status, grid, h->threads, h->stream));
   h->prof_end(pi, 1);
-  h->prof_acc.entries_applied += h->entry_used;
+  h->prof_acc.entries_applied += h->entries_pending;
   h->nchunks = 0;
-  h->entry_used = 0;
+  h->gutter_used = 0;
+  h->entries_pending = 0;
   return GZ_OK;
 }
 
@@ -402,36 +418,72 @@ int apply_pending(gz_alg *h) {
 int gutter_chunk(gz_alg *h, int input, const void *d_in, uint64_t n) {
   if (n == 0) return GZ_OK;
   const uint64_t per = input == gz::kInputRecords ? 2 : 1;
-  const uint64_t max_n = std::min(h->entry_cap, kMaxChunkEntries) / per;
+  const uint64_t esz = entry_bytes(h, input);
+  GZ_TRY(ensure_gutter(h));
+  const uint64_t max_n = std::min(h->gutter_bytes / esz, kMaxChunkEntries) / per;
+  if (max_n == 0) return fail(GZ_ERR_INVALID, "gutter capacity is below one update");
   if (n > max_n) {
     const size_t isz = input == gz::kInputRecords ? 9 : sizeof(uint2);
     for (uint64_t off = 0; off < n; off += max_n)
       GZ_TRY(gutter_chunk(h, input, (const uint8_t *)d_in + off * isz, std::min(max_n, n - off)));
     return GZ_OK;
   }
-  GZ_TRY(ensure_gutter(h));
-  if (h->entry_used + n * per > h->entry_cap || h->nchunks == gz::kMaxChunks) GZ_TRY(apply_pending(h));
+  if (h->gutter_used + n * per * esz > h->gutter_bytes || h->nchunks == gz::kMaxChunks)
+    GZ_TRY(apply_pending(h));
   const gz::GutterGeom gg = h->ggeom();
   const uint64_t unit = input == gz::kInputRecords ? gz::kRecTile : 4096;
   const int G = (int)std::max<uint64_t>(1, std::min<uint64_t>(2ull * gz::num_sms(), (n + unit - 1) / unit));
-  uint2 *out = h->d_entries + h->entry_used;
+  uint8_t *out = h->d_gutter + h->gutter_used;
   uint32_t *bin_off = h->d_bin_off + (size_t)h->nchunks * (h->nbins + 1);
   const int pi = h->prof_begin();
-  GZ_CUDA(cudaMemsetAsync(h->d_hist, 0, sizeof(uint64_t) * h->nbins, h->stream));
-  GZ_CUDA(gz::gutter_count(input, d_in, n, gg, G, h->d_hist, h->d_status, h->stream));
-  GZ_CUDA(gz::scan_exclusive_u64(h->d_hist, h->nbins, h->d_total, h->d_scan_tmp, h->stream));
-  GZ_CUDA(gz::gutter_bin_offsets(h->d_hist, 1, h->nbins, h->d_total, bin_off, h->stream));
-  const uint32_t tile = gz::sort_scatter_tile(input, gg, h->smem_optin - 1024);
-  if (tile >= 1024) {
-    GZ_CUDA(cudaMemsetAsync(h->d_fill, 0, sizeof(uint32_t) * h->nbins, h->stream));
-    GZ_CUDA(gz::gutter_sort_scatter(input, d_in, n, gg, tile, h->d_hist, h->d_fill, out, h->stream));
+  if (esz == 32) {
+    // records -> hashed 32-byte entries, each record hashed once
+    const gz::HashGeom hg{h->C, h->B, h->d_flip};
+    const uint64_t n_ct = (n + gz::kCountTile - 1) / gz::kCountTile;
+    if (h->nbins <= gz::kSmemBinsMax) {
+      const size_t words = n_ct * h->nbins;
+      if (h->hist2d_words < words) {
+        dev_free(h->d_hist2d);
+        h->hist2d_words = 0;
+        GZ_TRY(dev_alloc(&h->d_hist2d, words));
+        h->hist2d_words = words;
+      }
+      GZ_CUDA(gz::gutter_count_tiles(d_in, n, gg, h->d_hist2d, h->d_status, h->stream));
+      GZ_CUDA(gz::gutter_colscan(h->d_hist2d, (uint32_t)n_ct, h->nbins, h->d_hist, h->stream));
+      GZ_CUDA(gz::scan_exclusive_u64(h->d_hist, h->nbins, h->d_total, h->d_scan_tmp, h->stream));
+      GZ_CUDA(gz::gutter_bin_offsets(h->d_hist, 1, h->nbins, h->d_total, bin_off, h->stream));
+      GZ_CUDA(gz::gutter_hash_scatter(d_in, n, gg, hg, h->d_hist2d, h->d_hist, nullptr,
+                                      reinterpret_cast<uint4 *>(out), h->stream));
+    } else {
+      GZ_CUDA(cudaMemsetAsync(h->d_hist, 0, sizeof(uint64_t) * h->nbins, h->stream));
+      GZ_CUDA(gz::gutter_count(input, d_in, n, gg, G, h->d_hist, h->d_status, h->stream));
+      GZ_CUDA(gz::scan_exclusive_u64(h->d_hist, h->nbins, h->d_total, h->d_scan_tmp, h->stream));
+      GZ_CUDA(gz::gutter_bin_offsets(h->d_hist, 1, h->nbins, h->d_total, bin_off, h->stream));
+      GZ_CUDA(gz::copy_u64(h->d_hist, h->d_cursor, h->nbins, h->stream));
+      GZ_CUDA(gz::gutter_hash_scatter(d_in, n, gg, hg, nullptr, h->d_hist, h->d_cursor,
+                                      reinterpret_cast<uint4 *>(out), h->stream));
+    }
   } else {
-    GZ_CUDA(gz::copy_u64(h->d_hist, h->d_cursor, h->nbins, h->stream));
-    GZ_CUDA(gz::gutter_scatter_global(input, d_in, n, gg, G, h->d_cursor, out, h->stream));
+    uint2 *out2 = reinterpret_cast<uint2 *>(out);
+    GZ_CUDA(cudaMemsetAsync(h->d_hist, 0, sizeof(uint64_t) * h->nbins, h->stream));
+    GZ_CUDA(gz::gutter_count(input, d_in, n, gg, G, h->d_hist, h->d_status, h->stream));
+    GZ_CUDA(gz::scan_exclusive_u64(h->d_hist, h->nbins, h->d_total, h->d_scan_tmp, h->stream));
+    GZ_CUDA(gz::gutter_bin_offsets(h->d_hist, 1, h->nbins, h->d_total, bin_off, h->stream));
+    const uint32_t tile = gz::sort_scatter_tile(input, gg, h->smem_optin - 1024);
+    if (tile >= 1024) {
+      GZ_CUDA(cudaMemsetAsync(h->d_fill, 0, sizeof(uint32_t) * h->nbins, h->stream));
+      GZ_CUDA(gz::gutter_sort_scatter(input, d_in, n, gg, tile, h->d_hist, h->d_fill, out2, h->stream));
+    } else {
+      GZ_CUDA(gz::copy_u64(h->d_hist, h->d_cursor, h->nbins, h->stream));
+      GZ_CUDA(gz::gutter_scatter_global(input, d_in, n, gg, G, h->d_cursor, out2, h->stream));
+    }
   }
   h->prof_end(pi, 0);
-  h->chunks.base[h->nchunks++] = h->entry_used;
-  h->entry_used += n * per;
+  h->chunks.base[h->nchunks] = h->gutter_used;
+  h->chunks.kind[h->nchunks] = esz == 32 ? gz::kEntryHashed : gz::kEntryPlain;
+  h->nchunks++;
+  h->gutter_used += n * per * esz;
+  h->entries_pending += n * per;
   return GZ_OK;
 }
 
@@ -729,7 +781,8 @@ int gz_set_gutter_capacity(gz_alg_t *h, uint64_t n) {
   GZ_TRY(push_staged_entries(h));
   GZ_TRY(apply_pending(h));
   GZ_CUDA(cudaStreamSynchronize(h->stream));
-  dev_free(h->d_entries);
+  dev_free(h->d_gutter);
+  dev_free(h->d_hist2d);
   h->entry_cap = n;
   return GZ_OK;
 }
@@ -954,12 +1007,47 @@ int gz_clear(gz_alg_t *h) {
   Guard g(h);
   if (h->update_locked) return fail(GZ_ERR_LOCKED, "Cannot update the algorithm: Connected components currently running");
   h->nchunks = 0;
-  h->entry_used = 0;
+  h->gutter_used = 0;
+  h->entries_pending = 0;
   h->h_ent_n = 0;
   const uint64_t v_pad = ((uint64_t)h->V + 63) & ~63ull;
   GZ_CUDA(cudaMemsetAsync(h->d_sk, 0, v_pad * h->sketch_bytes, h->stream));
   h->dsu_valid = false;
   h->labels_on_host = false;
+  return GZ_OK;
+}
+
+int gz_measure_update_rate(int repeats, double *updates_per_s) {
+  if (!updates_per_s || repeats < 1) return fail(GZ_ERR_INVALID, "bad argument");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(GZ_ERR_NO_DEVICE, "no CUDA device");
+  const int blocks = gz::num_sms();
+  const uint32_t nb = 16 * 817, iters = 4096;  // 16 sketches of 817 buckets (2^17 vertices)
+  uint32_t *out = nullptr;
+  GZ_CUDA(cudaMalloc(&out, sizeof(uint32_t) * 1024 * blocks));
+  cudaStream_t s = nullptr;
+  GZ_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  double best = 0;
+  gz::update_peak(nb, 16, blocks, out, s);  // warm-up
+  for (int r = 0; r < repeats; ++r) {
+    cudaEventRecord(a, s);
+    gz::update_peak(nb, iters, blocks, out, s);
+    cudaEventRecord(b, s);
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    best = std::max(best, (double)blocks * 1024 * iters / (ms * 1e-3));
+  }
+  cudaError_t e = cudaGetLastError();
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaStreamDestroy(s);
+  cudaFree(out);
+  if (e != cudaSuccess) return fail(GZ_ERR_CUDA, cudaGetErrorString(e));
+  *updates_per_s = best;
   return GZ_OK;
 }
 
@@ -1004,12 +1092,21 @@ int gz_get_stream(gz_alg_t *h, void **s) {
   return GZ_OK;
 }
 
-int gz_set_tuning(gz_alg_t *h, uint32_t vpt, uint32_t threads, uint32_t tiles_per_bin) {
+int gz_set_tuning(gz_alg_t *h, uint32_t vpt, uint32_t threads, uint32_t tiles_per_bin,
+                  uint32_t entry_form) {
   if (!h) return fail(GZ_ERR_INVALID, "null handle");
+  if (entry_form > 2) return fail(GZ_ERR_INVALID, "entry_form must be 0, 1 or 2");
+  if (entry_form == 2 && h->C > gz::kHashedMaxColumns)
+    return fail(GZ_ERR_INVALID, "hashed entries need at most 32 columns");
   Guard g(h);
   GZ_TRY(push_staged_entries(h));
   GZ_TRY(apply_pending(h));
   GZ_CUDA(cudaStreamSynchronize(h->stream));
+  const bool want_hashed = entry_form == 0 ? h->hashed_default : entry_form == 2;
+  if (want_hashed != h->hashed) {
+    dev_free(h->d_gutter);  // entry size changes: reallocated on the next ingest
+    h->hashed = want_hashed;
+  }
   const uint32_t old_nb = h->nbins;
   const uint32_t keep[4] = {h->tile_shift, h->ntiles, h->bin_shift, h->nbins};
   const int rc = choose_tiling(h, vpt, threads, tiles_per_bin);

@@ -26,6 +26,15 @@ namespace gz {
 namespace {
 
 constexpr uint32_t kFull = 0xffffffffu;
+
+__device__ __forceinline__ uint32_t fmix32_(uint32_t h) {  // murmur3 finaliser
+  h ^= h >> 16;
+  h *= 0x85ebca6bu;
+  h ^= h >> 13;
+  h *= 0xc2b2ae35u;
+  h ^= h >> 16;
+  return h;
+}
 std::atomic<uint64_t> g_launches{0};  // kernel launches issued from this file
 
 // ------------------------------------------------------------------------------------------------
@@ -336,6 +345,140 @@ k_gutter_sort_scatter(const void *__restrict__ in, uint64_t n, GutterGeom g, uin
   }
 }
 
+// ---- hashed gutter ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(512)
+k_count_tiles(const uint8_t *__restrict__ rec, uint64_t n, GutterGeom g, uint32_t *__restrict__ hist2d,
+              uint32_t *__restrict__ status) {
+  extern __shared__ __align__(16) uint8_t gsm[];
+  uint32_t *s_bin = reinterpret_cast<uint32_t *>(gsm);
+  uint8_t *s_rec = gsm + ((g.nbins + 3) & ~3u) * 4;
+  const uint64_t r0 = (uint64_t)blockIdx.x * kCountTile;
+  const uint64_t r1 = r0 + kCountTile < n ? r0 + kCountTile : n;
+  for (uint32_t b = threadIdx.x; b < g.nbins; b += blockDim.x) s_bin[b] = 0u;
+  bool bad = false;
+  for (uint64_t t = r0; t < r1; t += kRecTile) {
+    const uint32_t cnt = (uint32_t)(r1 - t < (uint64_t)kRecTile ? r1 - t : (uint64_t)kRecTile);
+    __syncthreads();
+    const uint32_t shift = stage_records(rec, t, cnt, s_rec);
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
+      uint32_t u, v;
+      parse_record(s_rec, shift, i, u, v);
+      if (u >= g.V || v >= g.V) {
+        bad = true;
+        continue;
+      }
+      atomicAdd(&s_bin[u >> g.bin_shift], 1u);
+      atomicAdd(&s_bin[v >> g.bin_shift], 1u);
+    }
+  }
+  __syncthreads();
+  uint32_t *row = hist2d + (uint64_t)blockIdx.x * g.nbins;
+  for (uint32_t b = threadIdx.x; b < g.nbins; b += blockDim.x) row[b] = s_bin[b];
+  if (bad) atomicOr(status, kStatusBadVertex);
+}
+
+// Column-wise exclusive scan of hist2d (count tiles x bins): a CTA owns 32 bins (one per lane,
+// so every row access is one coalesced 128-byte line) and its 16 warps split the count tiles.
+__global__ void __launch_bounds__(512)
+k_colscan(uint32_t *hist2d, uint32_t n_ct, uint32_t nbins, uint64_t *totals) {
+  __shared__ uint32_t part[16][32];
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t b = blockIdx.x * 32 + lane;
+  const uint32_t t0 = (uint32_t)((uint64_t)n_ct * warp / 16);
+  const uint32_t t1 = (uint32_t)((uint64_t)n_ct * (warp + 1) / 16);
+  uint32_t sum = 0;
+  if (b < nbins)
+    for (uint32_t t = t0; t < t1; ++t) sum += hist2d[(uint64_t)t * nbins + b];
+  part[warp][lane] = sum;
+  __syncthreads();
+  uint32_t run = 0;
+  for (uint32_t w = 0; w < warp; ++w) run += part[w][lane];
+  if (b < nbins) {
+    for (uint32_t t = t0; t < t1; ++t) {
+      uint32_t *p = hist2d + (uint64_t)t * nbins + b;
+      const uint32_t c = *p;
+      *p = run;
+      run += c;
+    }
+    if (warp == 15) totals[b] = run;
+  }
+}
+
+// Checksum and the 4-bit depth codes of every column for one edge index (hash once per record).
+__device__ __forceinline__ void hash_record(uint32_t lo, uint32_t hi, const uint64_t *s_flip,
+                                            uint32_t C, uint32_t B, uint32_t &chk,
+                                            uint32_t (&codes)[4]) {
+  const uint64_t in64 = ((uint64_t)lo << 32) | hi;
+  chk = (uint32_t)rrmxmx8(in64 ^ s_flip[C]);
+#pragma unroll
+  for (int w = 0; w < 4; ++w) {
+    uint32_t word = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const uint32_t c = w * 8 + j;
+      if (c < C) {
+        const uint32_t d = depth_of(rrmxmx8(in64 ^ s_flip[c]), B);
+        word |= min(d, kDepthEscape) << (4 * j);
+      }
+    }
+    codes[w] = word;
+  }
+}
+
+template <bool SMEM_CURSOR>
+__global__ void __launch_bounds__(512)
+k_hash_scatter(const uint8_t *__restrict__ rec, uint64_t n, GutterGeom g, HashGeom hg,
+               const uint32_t *__restrict__ hist2d, const uint64_t *__restrict__ base,
+               uint64_t *__restrict__ cursor, uint4 *__restrict__ out) {
+  extern __shared__ __align__(16) uint8_t gsm[];
+  uint64_t *s_flip = reinterpret_cast<uint64_t *>(gsm);
+  const uint32_t flip_bytes = ((hg.C + 1) * 8 + 15) & ~15u;
+  uint32_t *s_cur = reinterpret_cast<uint32_t *>(gsm + flip_bytes);
+  uint8_t *s_rec = gsm + flip_bytes + (SMEM_CURSOR ? ((g.nbins + 3) & ~3u) * 4 : 0);
+  for (uint32_t i = threadIdx.x; i <= hg.C; i += blockDim.x) s_flip[i] = hg.flip[i];
+  uint64_t r0, r1, step;
+  if (SMEM_CURSOR) {
+    r0 = (uint64_t)blockIdx.x * kCountTile;
+    r1 = r0 + kCountTile < n ? r0 + kCountTile : n;
+    step = kRecTile;
+    const uint32_t *row = hist2d + (uint64_t)blockIdx.x * g.nbins;
+    for (uint32_t b = threadIdx.x; b < g.nbins; b += blockDim.x)
+      s_cur[b] = (uint32_t)base[b] + row[b];
+  } else {
+    r0 = (uint64_t)blockIdx.x * kRecTile;
+    r1 = n;
+    step = (uint64_t)gridDim.x * kRecTile;
+  }
+  for (uint64_t t = r0; t < r1; t += step) {
+    const uint32_t cnt = (uint32_t)(r1 - t < (uint64_t)kRecTile ? r1 - t : (uint64_t)kRecTile);
+    __syncthreads();
+    const uint32_t shift = stage_records(rec, t, cnt, s_rec);
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
+      uint32_t u, v;
+      parse_record(s_rec, shift, i, u, v);
+      if (u >= g.V || v >= g.V) continue;
+      const uint32_t lo = max(u, v), hi = min(u, v);
+      uint32_t chk, codes[4];
+      hash_record(lo, hi, s_flip, hg.C, hg.B, chk, codes);
+      const uint4 tail = make_uint4(codes[0], codes[1], codes[2], codes[3]);
+      uint64_t pu, pv;
+      if (SMEM_CURSOR) {
+        pu = atomicAdd(&s_cur[u >> g.bin_shift], 1u);
+        pv = atomicAdd(&s_cur[v >> g.bin_shift], 1u);
+      } else {
+        pu = atomicAdd(reinterpret_cast<unsigned long long *>(&cursor[u >> g.bin_shift]), 1ull);
+        pv = atomicAdd(reinterpret_cast<unsigned long long *>(&cursor[v >> g.bin_shift]), 1ull);
+      }
+      out[2 * pu] = make_uint4(u, lo, hi, chk);
+      out[2 * pu + 1] = tail;
+      out[2 * pv] = make_uint4(v, lo, hi, chk);
+      out[2 * pv + 1] = tail;
+    }
+  }
+}
+
 __global__ void k_bin_offsets(const uint64_t *scanned, uint32_t stride, uint32_t nbins,
                               const uint64_t *total, uint32_t *bin_off) {
   const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -444,8 +587,56 @@ __device__ __forceinline__ void apply_entry(uint2 e, uint32_t *s_sk, uint32_t vm
   }
 }
 
+// Same for a hashed entry: the checksum and depths come with it (a depth code of 15 means
+// "15 or more" and is recomputed).
+__device__ __forceinline__ void apply_hashed(uint4 e0, uint4 e1, uint32_t *s_sk, uint32_t vmask,
+                                             uint32_t sketch_words, const uint64_t *s_flip,
+                                             uint32_t C, uint32_t B) {
+  const uint32_t v = e0.x, lo = e0.y, hi = e0.z, chk = e0.w;
+  uint32_t *sk = s_sk + (v & vmask) * sketch_words;
+  uint32_t *det = sk + 3 * C * B;
+  atomicXor(det, lo);
+  atomicXor(det + 1, hi);
+  atomicXor(det + 2, chk);
+  const uint32_t codes[4] = {e1.x, e1.y, e1.z, e1.w};
+#pragma unroll
+  for (int w = 0; w < 4; ++w) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const uint32_t c = w * 8 + j;
+      if (c < C) {
+        uint32_t d = (codes[w] >> (4 * j)) & 0xfu;
+        if (d == kDepthEscape) d = depth_of(rrmxmx8((((uint64_t)lo << 32) | hi) ^ s_flip[c]), B);
+        if (d < B) {
+          uint32_t *bk = sk + 3 * (c * B + d);
+          atomicXor(bk, lo);
+          atomicXor(bk + 1, hi);
+          atomicXor(bk + 2, chk);
+        }
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ uint32_t entry_vertex(const uint8_t *cb, int kind, uint64_t i) {
+  return kind == kEntryHashed ? reinterpret_cast<const uint4 *>(cb)[2 * i].x
+                              : reinterpret_cast<const uint2 *>(cb)[i].x;
+}
+
+__device__ __forceinline__ void apply_any(const uint8_t *cb, int kind, uint64_t i, uint32_t *s_sk,
+                                          uint32_t vmask, const SketchGeom &g,
+                                          const uint64_t *s_flip, uint64_t flip_chk) {
+  if (kind == kEntryHashed) {
+    const uint4 *E = reinterpret_cast<const uint4 *>(cb);
+    apply_hashed(E[2 * i], E[2 * i + 1], s_sk, vmask, g.sketch_words, s_flip, g.C, g.B);
+  } else {
+    apply_entry(reinterpret_cast<const uint2 *>(cb)[i], s_sk, vmask, g.sketch_words, s_flip,
+                flip_chk, g.C, g.B);
+  }
+}
+
 __global__ void __launch_bounds__(1024, 1)
-k_sketch_update(SketchGeom g, uint8_t *__restrict__ sketches, const uint2 *__restrict__ entries,
+k_sketch_update(SketchGeom g, uint8_t *__restrict__ sketches, const uint8_t *__restrict__ gutter,
                 ChunkTable chunks, const uint32_t *__restrict__ bin_off, int nchunks,
                 const uint64_t *__restrict__ flip, uint32_t *work_counter, uint32_t *status) {
   extern __shared__ __align__(128) uint8_t dsm[];
@@ -455,7 +646,7 @@ k_sketch_update(SketchGeom g, uint8_t *__restrict__ sketches, const uint2 *__res
   const uint32_t tile_bytes = vpt * g.sketch_words * 4;
   const uint32_t per_bin = g.bin_shift - g.tile_shift;  // log2(tiles per bin)
   uint32_t *s_sk = reinterpret_cast<uint32_t *>(dsm);
-  uint2 *s_queue = reinterpret_cast<uint2 *>(dsm + tile_bytes);
+  uint32_t *s_queue = reinterpret_cast<uint32_t *>(dsm + tile_bytes);
   uint64_t *s_flip = reinterpret_cast<uint64_t *>(dsm + tile_bytes + kQueueBytes);
   for (uint32_t i = threadIdx.x; i <= g.C; i += blockDim.x) s_flip[i] = flip[i];
   const uint32_t bar = smem_u32(&s_bar);
@@ -467,7 +658,7 @@ k_sketch_update(SketchGeom g, uint8_t *__restrict__ sketches, const uint2 *__res
   const uint64_t flip_chk = s_flip[g.C];
   const uint32_t stride = g.nbins + 1;
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  uint2 *q = s_queue + warp * 64;
+  uint32_t *q = s_queue + warp * 64;
   uint32_t parity = 0;
   for (;;) {
     if (threadIdx.x == 0) {
@@ -502,40 +693,37 @@ k_sketch_update(SketchGeom g, uint8_t *__restrict__ sketches, const uint2 *__res
         return;
       }
       const uint32_t bin = t >> per_bin;
-      if (per_bin == 0) {
-        // the bin is this tile: every entry applies
-        for (int k = 0; k < nchunks; ++k) {
-          const uint64_t b = chunks.base[k] + bin_off[(uint64_t)k * stride + bin];
-          const uint64_t e = chunks.base[k] + bin_off[(uint64_t)k * stride + bin + 1];
+      for (int k = 0; k < nchunks; ++k) {
+        const uint8_t *cb = gutter + chunks.base[k];
+        const int kind = chunks.kind[k];
+        const uint64_t b = bin_off[(uint64_t)k * stride + bin];
+        const uint64_t e = bin_off[(uint64_t)k * stride + bin + 1];
+        if (per_bin == 0) {
+          // the bin is this tile: every entry applies
           for (uint64_t i = b + threadIdx.x; i < e; i += blockDim.x)
-            apply_entry(entries[i], s_sk, vpt - 1, g.sketch_words, s_flip, flip_chk, g.C, g.B);
-        }
-      } else {
-        // the bin holds several tiles: each warp ballots its 32 entries, appends this tile's to
-        // its queue, and hashes only full warps of queued entries
-        uint32_t qn = 0;
-        for (int k = 0; k < nchunks; ++k) {
-          const uint64_t b = chunks.base[k] + bin_off[(uint64_t)k * stride + bin];
-          const uint64_t e = chunks.base[k] + bin_off[(uint64_t)k * stride + bin + 1];
+            apply_any(cb, kind, i, s_sk, vpt - 1, g, s_flip, flip_chk);
+        } else {
+          // the bin holds several tiles: each warp ballots 32 entries, queues the indices of
+          // this tile's, and applies only full warps of queued entries
+          uint32_t qn = 0;
           for (uint64_t i0 = b + (uint64_t)warp * 32; i0 < e; i0 += (uint64_t)nwarps * 32) {
             const uint64_t i = i0 + lane;
-            uint2 x = make_uint2(0u, 0u);
-            if (i < e) x = entries[i];
-            const bool mine = i < e && (x.x >> g.tile_shift) == t;
+            const bool mine = i < e && (entry_vertex(cb, kind, i) >> g.tile_shift) == t;
             const uint32_t m = __ballot_sync(kFull, mine);
-            if (mine) q[qn + __popc(m & ((1u << lane) - 1u))] = x;
+            if (mine) q[qn + __popc(m & ((1u << lane) - 1u))] = (uint32_t)i;
             qn += __popc(m);
             __syncwarp();
             if (qn >= 32) {
-              apply_entry(q[lane], s_sk, vpt - 1, g.sketch_words, s_flip, flip_chk, g.C, g.B);
+              apply_any(cb, kind, q[lane], s_sk, vpt - 1, g, s_flip, flip_chk);
               __syncwarp();
               qn -= 32;
               if (lane < qn) q[lane] = q[32 + lane];
               __syncwarp();
             }
           }
+          if (lane < qn) apply_any(cb, kind, q[lane], s_sk, vpt - 1, g, s_flip, flip_chk);
+          __syncwarp();
         }
-        if (lane < qn) apply_entry(q[lane], s_sk, vpt - 1, g.sketch_words, s_flip, flip_chk, g.C, g.B);
       }
       fence_proxy_async_smem();
       __syncthreads();
@@ -567,18 +755,11 @@ struct TraceRec {
   uint64_t idx;
 };
 
-__device__ __forceinline__ uint32_t fmix32(uint32_t h) {
-  h ^= h >> 16;
-  h *= 0x85ebca6bu;
-  h ^= h >> 13;
-  h *= 0xc2b2ae35u;
-  h ^= h >> 16;
-  return h;
-}
+
 // Total order used to link roots (lower rank goes under higher): no cycles can form, the same
 // role as the random priorities of DisjointSetUnion_MT::order_edge (include/dsu.h:113-117).
 __device__ __forceinline__ uint64_t rank_of(uint32_t x) {
-  return ((uint64_t)fmix32(x) << 32) | x;
+  return ((uint64_t)fmix32_(x) << 32) | x;
 }
 
 // find_root with path halving (include/dsu.h:145-152); loads/stores go to L2 so updates by other
@@ -849,6 +1030,27 @@ __global__ void k_bv_final(uint32_t V, uint32_t *parent, uint32_t *out, uint32_t
   if (r == v) atomicAdd(ncc, 1u);
 }
 
+// Shared-memory bucket-update probe: every thread XORs 96-bit updates into random 12-byte
+// buckets of a 16-vertex staged tile with three 32-bit atomicXor each -- the sketch-update
+// kernel's per-bucket operation, without hashing or global traffic.
+__global__ void __launch_bounds__(1024, 1) k_update_peak(uint32_t nb, uint32_t iters, uint32_t *out) {
+  extern __shared__ __align__(16) uint32_t usm[];
+  for (uint32_t i = threadIdx.x; i < nb * 3; i += blockDim.x) usm[i] = 0;
+  __syncthreads();
+  uint32_t seed = fmix32_(blockIdx.x * 1024u + threadIdx.x);
+  for (uint32_t it = 0; it < iters; ++it) {
+    seed = fmix32_(seed + it);
+    uint32_t *p = usm + 3 * (seed % nb);
+    atomicXor(p, seed);
+    atomicXor(p + 1, seed * 3u);
+    atomicXor(p + 2, seed ^ 0x5555u);
+  }
+  __syncthreads();
+  uint32_t x = 0;
+  for (uint32_t i = threadIdx.x; i < nb * 3; i += blockDim.x) x ^= usm[i];
+  out[blockIdx.x * 1024u + threadIdx.x] = x;
+}
+
 inline unsigned blocks_for(uint64_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
 
 // Eight independent hash chains per thread: each step is one 8-byte XXH3 (rrmxmx with a column
@@ -879,6 +1081,16 @@ __global__ void k_hash_peak(uint64_t seed, uint32_t iters, uint64_t *out) {
 // host wrappers
 // ================================================================================================
 uint64_t launch_count() { return g_launches.load(); }
+
+cudaError_t update_peak(uint32_t nb, uint32_t iters, int blocks, uint32_t *out, cudaStream_t s) {
+  const size_t smem = (size_t)nb * 12;
+  cudaError_t e = cudaFuncSetAttribute(k_update_peak, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return e;
+  k_update_peak<<<blocks, 1024, smem, s>>>(nb, iters, out);
+  g_launches++;
+  return cudaGetLastError();
+}
 
 cudaError_t hash_peak(uint64_t seed, uint32_t iters, int blocks, int threads, uint64_t *out,
                       cudaStream_t s) {
@@ -941,6 +1153,52 @@ cudaError_t gutter_scatter_global(int input, const void *in, uint64_t n, GutterG
   return input == kInputRecords
              ? launch_gutter<kInputRecords, false, false>(in, n, g, G, cursor, entries, nullptr, s)
              : launch_gutter<kInputEntries, false, false>(in, n, g, G, cursor, entries, nullptr, s);
+}
+
+cudaError_t gutter_count_tiles(const void *rec, uint64_t n, GutterGeom g, uint32_t *hist2d,
+                               uint32_t *status, cudaStream_t s) {
+  const size_t smem = ((g.nbins + 3) & ~3u) * 4 + kRecStageBytes;
+  cudaError_t e = cudaFuncSetAttribute(k_count_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return e;
+  const unsigned grid = (unsigned)((n + kCountTile - 1) / kCountTile);
+  k_count_tiles<<<grid, 512, smem, s>>>(reinterpret_cast<const uint8_t *>(rec), n, g, hist2d, status);
+  g_launches++;
+  return cudaGetLastError();
+}
+
+cudaError_t gutter_colscan(uint32_t *hist2d, uint32_t n_ct, uint32_t nbins, uint64_t *totals,
+                           cudaStream_t s) {
+  k_colscan<<<blocks_for(nbins, 32), 512, 0, s>>>(hist2d, n_ct, nbins, totals);
+  g_launches++;
+  return cudaGetLastError();
+}
+
+cudaError_t gutter_hash_scatter(const void *rec, uint64_t n, GutterGeom g, HashGeom hg,
+                                const uint32_t *hist2d, const uint64_t *base, uint64_t *cursor,
+                                uint4 *out, cudaStream_t s) {
+  const size_t flip_bytes = ((hg.C + 1) * 8 + 15) & ~15u;
+  const bool smem_cursor = hist2d != nullptr;
+  const size_t smem = flip_bytes + (smem_cursor ? ((g.nbins + 3) & ~3u) * 4 : 0) + kRecStageBytes;
+  const uint8_t *r = reinterpret_cast<const uint8_t *>(rec);
+  if (smem_cursor) {
+    cudaError_t e = cudaFuncSetAttribute(k_hash_scatter<true>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const unsigned grid = (unsigned)((n + kCountTile - 1) / kCountTile);
+    k_hash_scatter<true><<<grid, 512, smem, s>>>(r, n, g, hg, hist2d, base, cursor, out);
+  } else {
+    cudaError_t e = cudaFuncSetAttribute(k_hash_scatter<false>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hash_scatter<false>, 512, smem);
+    const uint64_t tiles = (n + kRecTile - 1) / kRecTile;
+    const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(tiles, (uint64_t)num_sms() * std::max(per_sm, 1)));
+    k_hash_scatter<false><<<grid, 512, smem, s>>>(r, n, g, hg, hist2d, base, cursor, out);
+  }
+  g_launches++;
+  return cudaGetLastError();
 }
 
 uint32_t sort_scatter_tile(int input, GutterGeom g, size_t smem_budget) {
@@ -1007,12 +1265,12 @@ int sketch_update_ctas_per_sm(SketchGeom g, int threads) {
   return n > 0 ? n : 1;
 }
 
-cudaError_t sketch_update(SketchGeom g, uint8_t *sketches, const uint2 *entries,
+cudaError_t sketch_update(SketchGeom g, uint8_t *sketches, const uint8_t *gutter,
                           const ChunkTable &chunks, const uint32_t *bin_off, int nchunks,
                           const uint64_t *flip, uint32_t *work_counter, uint32_t *status, int grid,
                           int threads, cudaStream_t s) {
   const size_t smem = sketch_update_smem_bytes(g);
-  k_sketch_update<<<grid, threads, smem, s>>>(g, sketches, entries, chunks, bin_off, nchunks, flip,
+  k_sketch_update<<<grid, threads, smem, s>>>(g, sketches, gutter, chunks, bin_off, nchunks, flip,
                                               work_counter, status);
   g_launches++;
   return cudaGetLastError();

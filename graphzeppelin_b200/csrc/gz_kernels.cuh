@@ -29,8 +29,16 @@ struct GutterGeom {
 
 // Maximum number of gutter chunks buffered before the sketches must be updated.
 constexpr int kMaxChunks = 128;
+// Entry kinds of a gutter chunk.
+enum EntryKind : uint8_t {
+  kEntryPlain = 0,   // uint2 {vertex, neighbour}: hashed by the sketch-update kernel
+  kEntryHashed = 1,  // 32 bytes {vertex, idx lo, idx hi, checksum, 4 x 8 depth codes}
+};
+constexpr uint32_t kHashedMaxColumns = 32;  // 4-bit depth codes in 128 bits
+constexpr uint32_t kDepthEscape = 15;       // code for depth >= 15: recomputed where applied
 struct ChunkTable {
-  uint64_t base[kMaxChunks];  // first entry of the chunk in the gutter buffer
+  uint64_t base[kMaxChunks];  // byte offset of the chunk in the gutter buffer
+  uint8_t kind[kMaxChunks];
 };
 
 struct SketchGeom {
@@ -49,7 +57,7 @@ struct SketchGeom {
 constexpr int kRecTile = 4096;
 constexpr uint32_t kSmemBinsMax = 12288;
 // Largest bin count handled by the shared-memory sort-scatter (above it: global cursors).
-constexpr uint32_t kSortBinsMax = 4096;
+constexpr uint32_t kSortBinsMax = 8192;
 
 // ---- scan -------------------------------------------------------------------------------------
 // Exclusive prefix sum over n u64 values, in place; writes the total to *d_total. `tmp` must
@@ -71,6 +79,25 @@ cudaError_t gutter_sort_scatter(int input, const void *d_in, uint64_t n, GutterG
 // Fallback for many bins: one global atomic cursor per bin (cursor = copy of base).
 cudaError_t gutter_scatter_global(int input, const void *d_in, uint64_t n, GutterGeom g, int G,
                                   uint64_t *cursor, uint2 *entries, cudaStream_t s);
+
+// ---- hashed gutter (records in, 32-byte entries out; every record hashed once) ---------------
+constexpr uint32_t kCountTile = 65536;  // records per count tile
+struct HashGeom {
+  uint32_t C, B;
+  const uint64_t *flip;  // C column constants, then the checksum constant
+};
+// hist2d[ct * nbins + b] = entries of bin b among the records of count tile ct
+cudaError_t gutter_count_tiles(const void *d_rec, uint64_t n, GutterGeom g, uint32_t *hist2d,
+                               uint32_t *status, cudaStream_t s);
+// per bin: hist2d column -> exclusive prefix over count tiles; totals[b] = column sum
+cudaError_t gutter_colscan(uint32_t *hist2d, uint32_t n_ct, uint32_t nbins, uint64_t *totals,
+                           cudaStream_t s);
+// Hash every record once and write its two 32-byte entries. With hist2d: positions are
+// base[b] + hist2d[ct][b] + rank inside the count tile; without: global cursors (cursor[b]
+// starts at base[b]).
+cudaError_t gutter_hash_scatter(const void *d_rec, uint64_t n, GutterGeom g, HashGeom hg,
+                                const uint32_t *hist2d, const uint64_t *base, uint64_t *cursor,
+                                uint4 *out, cudaStream_t s);
 // bin_off[b] = scanned[b * stride], bin_off[nbins] = *total  (u32, relative to chunk base)
 cudaError_t gutter_bin_offsets(const uint64_t *scanned, uint32_t stride, uint32_t nbins,
                                const uint64_t *total, uint32_t *bin_off, cudaStream_t s);
@@ -80,7 +107,7 @@ cudaError_t copy_u64(const uint64_t *src, uint64_t *dst, uint64_t n, cudaStream_
 // ---- sketch update -------------------------------------------------------------------------------
 // Per-warp queues (64 entries x 32 warps) that compact the entries of a bin belonging to this
 // CTA's tile into full warps.
-constexpr size_t kQueueBytes = 64 * 8 * 32;
+constexpr size_t kQueueBytes = 64 * 4 * 32;
 size_t sketch_update_smem_bytes(SketchGeom g);
 cudaError_t sketch_update_prepare(SketchGeom g, int threads);
 // CTAs of the sketch-update kernel that fit on one SM at this geometry.
@@ -88,7 +115,7 @@ int sketch_update_ctas_per_sm(SketchGeom g, int threads);
 // Applies every buffered entry of `nchunks` chunks: for each tile whose bin has entries, stage
 // its sketches in shared memory with bulk async copies, XOR in the bin entries that belong to
 // the tile, write the tile back.
-cudaError_t sketch_update(SketchGeom g, uint8_t *sketches, const uint2 *entries,
+cudaError_t sketch_update(SketchGeom g, uint8_t *sketches, const uint8_t *gutter,
                           const ChunkTable &chunks, const uint32_t *bin_off, int nchunks,
                           const uint64_t *flip, uint32_t *work_counter, uint32_t *status,
                           int grid, int threads, cudaStream_t s);
@@ -141,6 +168,10 @@ int num_sms();
 // Register-only hash throughput probe: n_threads * iters * 8 hashes.
 cudaError_t hash_peak(uint64_t seed, uint32_t iters, int blocks, int threads, uint64_t *out,
                       cudaStream_t s);
+
+// Shared-memory bucket-update probe: blocks x 1024 threads x iters updates of 3 atomicXor
+// each into nb staged buckets (out: blocks * 1024 words).
+cudaError_t update_peak(uint32_t nb, uint32_t iters, int blocks, uint32_t *out, cudaStream_t s);
 
 // Kernel launches issued by the host wrappers of this file (monotonic, process-wide).
 uint64_t launch_count();

@@ -213,11 +213,18 @@ GZ_API int gz_get_stream(gz_alg_t *alg, void **stream_out);
  * device. *hashes_per_s gets the best of `repeats` launches. */
 GZ_API int gz_measure_hash_rate(int repeats, double *hashes_per_s);
 
+/* Peak rate of this GPU at the sketch update's shared-memory operation: 96-bit XOR updates of
+ * random 12-byte buckets in a 157 KB staged tile with three 32-bit atomicXor each (1024 threads
+ * per SM, no hashing, no global traffic). *updates_per_s gets the best of `repeats` launches. */
+GZ_API int gz_measure_update_rate(int repeats, double *updates_per_s);
+
 /* Tuning knobs of the ingest kernels (0 picks the default): vertices staged per shared-memory
- * tile (power of two in [4, 64]), threads per block of the sketch-update kernel, and tiles per
- * gutter bin (power of two <= 64). Buffered updates are applied first. */
+ * tile (power of two in [4, 64]), threads per block of the sketch-update kernel, tiles per
+ * gutter bin (power of two <= 64), and the gutter entry form for records: 1 = plain entries
+ * (hashed per endpoint by the sketch-update kernel), 2 = hashed entries (each record hashed
+ * once in the gutter; needs at most 32 columns). Buffered updates are applied first. */
 GZ_API int gz_set_tuning(gz_alg_t *alg, uint32_t vertices_per_tile, uint32_t threads_per_block,
-                         uint32_t tiles_per_bin);
+                         uint32_t tiles_per_bin, uint32_t entry_form);
 
 #ifdef __cplusplus
 }

@@ -21,11 +21,13 @@ def _header(seed, V, factor):
             + np.array([factor], "<f8").tobytes())
 
 
+@pytest.mark.parametrize("form", [1, 2])
 @pytest.mark.parametrize("name", case_names())
-def test_golden_case_bit_exact(gz, name, tmp_path):
+def test_golden_case_bit_exact(gz, name, form, tmp_path):
     c, st, labels, trace = load_case(name)
     V, seed, f = c["num_vertices"], c["seed"], c["sketches_factor"]
     alg = _alg(gz, V, seed, f)
+    alg.set_tuning(0, 0, 0, form)
     alg.set_trace(True)
     alg.ingest_records(st)
     dump = alg.dump_sketches()
@@ -95,11 +97,13 @@ def test_device_ingest_any_alignment(gz, oracle_mod, offset):
     assert (canonical(cc.parent_arr) == labels).all()
 
 
+@pytest.mark.parametrize("form", [1, 2])
 @pytest.mark.parametrize("cap", [2, 1000, 4097, 65536])
-def test_small_gutter_many_chunks(gz, oracle_mod, cap):
+def test_small_gutter_many_chunks(gz, oracle_mod, cap, form):
     """A tiny device gutter forces many partial applications; bytes must not change."""
     c, st, labels, _ = load_case("cl_v2048")
     alg = _alg(gz, 2048, c["seed"])
+    alg.set_tuning(0, 0, 0, form)
     alg.set_gutter_capacity(cap)
     for part in np.array_split(st.records, 7):
         alg.ingest_records(part)
@@ -115,12 +119,13 @@ def test_tile_that_does_not_fit_is_rejected(gz):
         alg.set_tuning(64, 1024)  # 64 * 4332 bytes > shared memory per block
 
 
+@pytest.mark.parametrize("form", [1, 2])
 @pytest.mark.parametrize("vpt,threads,tpb", [(4, 128, 1), (8, 256, 2), (16, 1024, 8), (32, 512, 4),
                                              (32, 1024, 1), (4, 1024, 64), (16, 640, 16)])
-def test_tile_shapes_bit_exact(gz, oracle_mod, vpt, threads, tpb):
+def test_tile_shapes_bit_exact(gz, oracle_mod, vpt, threads, tpb, form):
     c, st, labels, _ = load_case("c0_v1024")
     alg = _alg(gz, 1024, c["seed"])
-    alg.set_tuning(vpt, threads, tpb)
+    alg.set_tuning(vpt, threads, tpb, form)
     assert alg.params.vertices_per_tile == vpt
     assert alg.params.vertices_per_bin == vpt * tpb
     alg.ingest_records(st)
@@ -221,3 +226,57 @@ def test_many_bins_gutter_paths(gz, oracle_mod, vpt, tpb):
     cc = alg.connected_components()
     assert cc.size() == n
     assert (canonical(cc.parent_arr) == exact).all()
+
+
+def test_records_with_more_than_32_columns_use_plain_entries(gz, oracle_mod):
+    """sketches_factor 3 gives 41 columns: records are hashed per endpoint (plain entries)."""
+    c, st, _, _ = load_case("c0_v1024")
+    alg = _alg(gz, 1024, 99, 3.0)
+    assert alg.params.num_columns == 41
+    alg.ingest_records(st)
+    osk = oracle_mod.OracleSketches(1024, 99, 3.0)
+    osk.apply_records(st.raw())
+    assert (alg.dump_sketches() == osk.data).all()
+    rc, lab, rounds, _ = osk.boruvka(with_trace=False)
+    assert (canonical(alg.connected_components().parent_arr) == lab).all()
+    assert alg.last_query_rounds == rounds
+
+
+def test_hashed_entries_with_global_cursors(gz, oracle_mod):
+    """65536 vertices at 4 per tile: 16384 bins, above the shared-memory cursor limit."""
+    from graphzeppelin_b200 import streams as S
+    V = 1 << 16
+    st = S.erdos_renyi_stream(V, 0.0002, seed=23, churn_fraction=0.1)
+    alg = _alg(gz, V, 31)
+    alg.set_tuning(4, 1024, 1, 2)
+    assert alg.params.num_bins == 16384
+    alg.ingest_records(st)
+    rng = np.random.default_rng(8)
+    pick = rng.choice(V, 64, replace=False)
+    filt = np.zeros(V, np.uint8)
+    filt[pick] = 1
+    osk = oracle_mod.OracleSketches(V, 31)
+    osk.apply_records(st.raw(), vertex_filter=filt)
+    dump = alg.dump_sketches()
+    sb = osk.sketch_bytes
+    for v in pick:
+        assert (dump[v * sb:(v + 1) * sb] == osk.sketch(v)).all(), v
+    n, exact = oracle_mod.exact_cc(V, st.raw())
+    assert (canonical(alg.connected_components().parent_arr) == exact).all()
+
+
+def test_mixed_hashed_and_plain_chunks(gz, oracle_mod):
+    """Records (hashed entries) and apply_update_batch (plain entries) buffered together."""
+    c, st, labels, _ = load_case("cl_v2048")
+    alg = _alg(gz, 2048, c["seed"])
+    alg.set_tuning(0, 0, 1, 2)
+    half = st.num_updates // 2
+    alg.ingest_records(st.records[:half])
+    rest = st.records[half:]
+    for r in rest:
+        alg.apply_update_batch(0, int(r["src"]), [int(r["dst"])])
+        alg.apply_update_batch(1, int(r["dst"]), [int(r["src"])])
+    osk = oracle_mod.OracleSketches(2048, c["seed"])
+    osk.apply_records(st.raw())
+    assert (alg.dump_sketches() == osk.data).all()
+    assert (canonical(alg.connected_components().parent_arr) == labels).all()
