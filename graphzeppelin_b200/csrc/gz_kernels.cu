@@ -1270,6 +1270,10 @@ cudaError_t sketch_update(SketchGeom g, uint8_t *sketches, const uint8_t *gutter
                           const uint64_t *flip, uint32_t *work_counter, uint32_t *status, int grid,
                           int threads, cudaStream_t s) {
   const size_t smem = sketch_update_smem_bytes(g);
+  // the limit is per function, and other handles may have set it for a smaller geometry
+  cudaError_t e = cudaFuncSetAttribute(k_sketch_update, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return e;
   k_sketch_update<<<grid, threads, smem, s>>>(g, sketches, gutter, chunks, bin_off, nchunks, flip,
                                               work_counter, status);
   g_launches++;

@@ -162,3 +162,24 @@ def test_profile_counters(gz):
     assert p["sketch_update_launches"] >= 1 and p["gutter_launches"] >= 1
     assert p["entries_applied"] == 2 * st.num_updates
     assert p["sketch_update_ms"] > 0 and p["query_ms"] > 0
+
+
+def test_handles_of_different_geometry_interleave(gz, oracle_mod):
+    """Two live handles with different sketch sizes: launches of one must not be limited by
+    the shared-memory setting made for the other."""
+    from graphzeppelin_b200 import streams as S
+    big_st = S.erdos_renyi_stream(1 << 14, 0.001, seed=41)
+    small_st = S.erdos_renyi_stream(256, 0.05, seed=42)
+    big = gz.CCSketchAlg(1 << 14, 5)
+    small = gz.CCSketchAlg(256, 6)
+    for part_b, part_s in zip(np.array_split(big_st.records, 3), np.array_split(small_st.records, 3)):
+        big.ingest_records(part_b)
+        big.flush()
+        small.ingest_records(part_s)
+        small.flush()
+    ob = oracle_mod.OracleSketches(1 << 14, 5)
+    ob.apply_records(big_st.raw())
+    os_ = oracle_mod.OracleSketches(256, 6)
+    os_.apply_records(small_st.raw())
+    assert (big.dump_sketches() == ob.data).all()
+    assert (small.dump_sketches() == os_.data).all()
