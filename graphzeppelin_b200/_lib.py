@@ -84,6 +84,7 @@ SIGNATURES = [
     ("gz_get_profile", _i, [_H, ctypes.POINTER(gz_profile_t)]),
     ("gz_get_stream", _i, [_H, ctypes.POINTER(ctypes.c_void_p)]),
     ("gz_set_tuning", _i, [_H, _u32, _u32, _u32, _u32]),
+    ("gz_ingest_records_noalloc", _i, [_P, _u32, _u64, _d, _P, _sz, _P]),
 ]
 
 _lib = None

@@ -86,6 +86,9 @@ constexpr int kNumPhases = 3;  // gutter, sketch update, query
 
 }  // namespace
 
+// Error text for entry points defined in other files of this library.
+void gz_internal_set_error(const std::string &msg) { g_last_error = msg; }
+
 struct gz_alg {
   std::mutex mtx;
   int device = 0;

@@ -195,6 +195,27 @@ GZ_API int gz_clear(gz_alg_t *alg);
  * buffer; buffered updates are applied first. */
 GZ_API int gz_dump_sketches(gz_alg_t *alg, void *host_buf, size_t bytes);
 
+/* ---- ingest without allocation ------------------------------------------------------------------
+ * No counterpart in the reference. For callers that may not allocate GPU memory: plugins inside
+ * a host framework that owns all device memory through its own pool (a library cudaMalloc would
+ * bypass its accounting), and latency-critical loops where cudaMalloc / cudaFree would
+ * synchronize the device and stall other streams. Applies n_records packed 9-byte records (device
+ * memory, any alignment) to the V sketches at d_sketches (caller-owned device memory,
+ * V * sketch_bytes in the write_binary bucket layout, updated in place) for the sketch geometry
+ * of (num_vertices, seed, sketches_factor), exactly as gz_ingest_records_device + gz_flush on a
+ * handle would, and synchronizes `stream` (a cudaStream_t, NULL for the default stream).
+ * It calls no cudaMalloc / cudaFree and no allocating library routine: its scratch is one fixed
+ * file-scope device array of about 34 MiB that every GPU loading the library holds until the
+ * process exits. Limits: at most 2,097,152 records per call and at most 4,194,304 vertices;
+ * larger calls return GZ_ERR_INVALID without touching memory. The first call on each device looks
+ * up the array's address (cudaGetSymbolAddress), so it should come before any stream capture.
+ * Every call shares the array, which keeps the previous call's contents (each call clears what
+ * must start at zero), so two calls whose GPU work overlapped would race on it: the entry point
+ * therefore serializes its callers with a lock and returns only after its GPU work is done. */
+GZ_API int gz_ingest_records_noalloc(void *d_sketches, uint32_t num_vertices, uint64_t seed,
+                                     double sketches_factor, const void *d_records,
+                                     size_t n_records, void *stream);
+
 /* ---- instrumentation ----------------------------------------------------------------------- */
 
 /* Record every sampled component of every Boruvka round (for parity checks). */
