@@ -80,6 +80,10 @@ void reference_params(uint32_t V, double f, uint32_t &C, uint32_t &B) {
 }
 
 constexpr uint64_t kStageRecords = 1ull << 24;  // records per host->device pipeline chunk
+constexpr int kStageBuffers = 4;                 // device staging buffers of the copy pipeline
+// Host-record ingest applies the gutter to the sketches whenever this many endpoint updates are
+// pending, so the sketch update of one wave runs while later records are still being copied.
+constexpr uint64_t kWaveEntries = 1ull << 26;
 constexpr uint64_t kEntStage = 1ull << 20;      // staged apply_update_batch entries per flush
 constexpr uint64_t kMaxChunkEntries = 1ull << 31;
 constexpr int kNumPhases = 3;  // gutter, sketch update, query
@@ -121,8 +125,8 @@ struct gz_alg {
   uint32_t *d_fill = nullptr;
   size_t hist_words = 0;
   // host-record pipeline
-  uint8_t *d_stage[2] = {nullptr, nullptr};
-  cudaEvent_t ev_copied[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr};
+  uint8_t *d_stage[kStageBuffers] = {};
+  cudaEvent_t ev_copied[kStageBuffers] = {}, ev_free[kStageBuffers] = {};
   // apply_update_batch staging
   uint2 *h_ent[2] = {nullptr, nullptr};
   uint2 *d_ent[2] = {nullptr, nullptr};
@@ -331,12 +335,14 @@ void destroy_alg(gz_alg *h) {
   dev_free(h->d_total);
   dev_free(h->d_cursor);
   dev_free(h->d_fill);
-  for (int i = 0; i < 2; ++i) {
+  for (int i = 0; i < kStageBuffers; ++i) {
     dev_free(h->d_stage[i]);
-    dev_free(h->d_ent[i]);
-    host_free(h->h_ent[i]);
     if (h->ev_copied[i]) cudaEventDestroy(h->ev_copied[i]);
     if (h->ev_free[i]) cudaEventDestroy(h->ev_free[i]);
+  }
+  for (int i = 0; i < 2; ++i) {
+    dev_free(h->d_ent[i]);
+    host_free(h->h_ent[i]);
     if (h->ev_ent_done[i]) cudaEventDestroy(h->ev_ent_done[i]);
   }
   dev_free(h->d_raw);
@@ -856,7 +862,8 @@ int gz_ingest_records(gz_alg_t *h, const void *rec, size_t n) {
   GZ_TRY(mark_updated(h));
   if (n == 0) return GZ_OK;
   const uint64_t chunk = std::min<uint64_t>(kStageRecords, n);
-  for (int i = 0; i < 2; ++i) {
+  const int nbuf = (int)std::min<uint64_t>(kStageBuffers, (n + chunk - 1) / chunk);
+  for (int i = 0; i < nbuf; ++i) {
     if (!h->d_stage[i]) {
       GZ_TRY(dev_alloc(&h->d_stage[i], kStageRecords * 9 + 16));
       GZ_CUDA(cudaEventCreateWithFlags(&h->ev_copied[i], cudaEventDisableTiming));
@@ -866,7 +873,7 @@ int gz_ingest_records(gz_alg_t *h, const void *rec, size_t n) {
   }
   const uint8_t *src = static_cast<const uint8_t *>(rec);
   int buf = 0;
-  for (uint64_t off = 0; off < n; off += chunk, buf ^= 1) {
+  for (uint64_t off = 0; off < n; off += chunk, buf = (buf + 1) % nbuf) {
     const uint64_t m = std::min<uint64_t>(chunk, n - off);
     GZ_CUDA(cudaStreamWaitEvent(h->copy_stream, h->ev_free[buf], 0));
     GZ_CUDA(cudaMemcpyAsync(h->d_stage[buf], src + off * 9, m * 9, cudaMemcpyHostToDevice, h->copy_stream));
@@ -874,6 +881,8 @@ int gz_ingest_records(gz_alg_t *h, const void *rec, size_t n) {
     GZ_CUDA(cudaStreamWaitEvent(h->stream, h->ev_copied[buf], 0));
     GZ_TRY(gutter_chunk(h, gz::kInputRecords, h->d_stage[buf], m));
     GZ_CUDA(cudaEventRecord(h->ev_free[buf], h->stream));
+    // fold a wave into the sketches while the copy engine keeps streaming records
+    if (h->entries_pending >= kWaveEntries && off + m < n) GZ_TRY(apply_pending(h));
   }
   // the caller's buffer may be reused once every copy has landed
   GZ_CUDA(cudaStreamSynchronize(h->copy_stream));

@@ -57,6 +57,34 @@ __device__ __forceinline__ uint32_t depth_of(uint64_t h, uint32_t B) {
   return (uint32_t)(__ffsll((long long)x) - 1);
 }
 
+// rrmxmx8 without its final xorshift, split into 32-bit halves: the final value is
+// h ^ (h >> 28), whose low word needs both halves and whose high word is only ever needed when the
+// low word is zero.
+__device__ __forceinline__ void rrmxmx8_pre(uint64_t h, uint32_t &lo, uint32_t &hi) {
+  h ^= ((h << 49) | (h >> 15)) ^ ((h << 24) | (h >> 40));
+  h *= kPrimeMx2;
+  h ^= (h >> 35) + 8;
+  h *= kPrimeMx2;
+  lo = (uint32_t)h;
+  hi = (uint32_t)(h >> 32);
+}
+// low 32 bits of rrmxmx8(h): the bucket checksum
+__device__ __forceinline__ uint32_t hash_lo32(uint64_t h) {
+  uint32_t lo, hi;
+  rrmxmx8_pre(h, lo, hi);
+  return lo ^ __funnelshift_r(lo, hi, 28);
+}
+// depth_of(rrmxmx8(h), B) for B <= 63, computing the high word only when the low word is zero.
+__device__ __forceinline__ uint32_t hash_depth(uint64_t h, uint32_t B) {
+  uint32_t lo, hi;
+  rrmxmx8_pre(h, lo, hi);
+  const uint32_t flo = lo ^ __funnelshift_r(lo, hi, 28);
+  if (B < 32) return __ffs(flo | (1u << B)) - 1;
+  if (flo) return __ffs(flo) - 1;
+  const uint32_t fhi = hi ^ (hi >> 28);
+  return 31 + __ffs(fhi | (1u << (B - 32)));
+}
+
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return (uint32_t)__cvta_generic_to_shared(p);
 }

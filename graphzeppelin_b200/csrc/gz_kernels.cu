@@ -410,7 +410,7 @@ __device__ __forceinline__ void hash_record(uint32_t lo, uint32_t hi, const uint
                                             uint32_t C, uint32_t B, uint32_t &chk,
                                             uint32_t (&codes)[4]) {
   const uint64_t in64 = ((uint64_t)lo << 32) | hi;
-  chk = (uint32_t)rrmxmx8(in64 ^ s_flip[C]);
+  chk = hash_lo32(in64 ^ s_flip[C]);
 #pragma unroll
   for (int w = 0; w < 4; ++w) {
     uint32_t word = 0;
@@ -418,7 +418,7 @@ __device__ __forceinline__ void hash_record(uint32_t lo, uint32_t hi, const uint
     for (int j = 0; j < 8; ++j) {
       const uint32_t c = w * 8 + j;
       if (c < C) {
-        const uint32_t d = depth_of(rrmxmx8(in64 ^ s_flip[c]), B);
+        const uint32_t d = hash_depth(in64 ^ s_flip[c], B);
         word |= min(d, kDepthEscape) << (4 * j);
       }
     }
@@ -571,13 +571,13 @@ __device__ __forceinline__ void apply_entry(uint2 e, uint32_t *s_sk, uint32_t vm
   const uint32_t lo = max(v, w), hi = min(v, w);  // idx = (min << 32) | max
   uint32_t *sk = s_sk + (v & vmask) * sketch_words;
   const uint64_t in64 = ((uint64_t)lo << 32) | hi;
-  const uint32_t chk = (uint32_t)rrmxmx8(in64 ^ flip_chk);
+  const uint32_t chk = hash_lo32(in64 ^ flip_chk);
   uint32_t *det = sk + 3 * C * B;
   atomicXor(det, lo);
   atomicXor(det + 1, hi);
   atomicXor(det + 2, chk);
   for (uint32_t c = 0; c < C; ++c) {
-    const uint32_t d = depth_of(rrmxmx8(in64 ^ s_flip[c]), B);
+    const uint32_t d = hash_depth(in64 ^ s_flip[c], B);
     if (d < B) {
       uint32_t *bk = sk + 3 * (c * B + d);
       atomicXor(bk, lo);
@@ -606,7 +606,7 @@ __device__ __forceinline__ void apply_hashed(uint4 e0, uint4 e1, uint32_t *s_sk,
       const uint32_t c = w * 8 + j;
       if (c < C) {
         uint32_t d = (codes[w] >> (4 * j)) & 0xfu;
-        if (d == kDepthEscape) d = depth_of(rrmxmx8((((uint64_t)lo << 32) | hi) ^ s_flip[c]), B);
+        if (d == kDepthEscape) d = hash_depth((((uint64_t)lo << 32) | hi) ^ s_flip[c], B);
         if (d < B) {
           uint32_t *bk = sk + 3 * (c * B + d);
           atomicXor(bk, lo);
@@ -618,15 +618,17 @@ __device__ __forceinline__ void apply_hashed(uint4 e0, uint4 e1, uint32_t *s_sk,
   }
 }
 
+template <bool HASHED>
 __device__ __forceinline__ uint32_t entry_vertex(const uint8_t *cb, int kind, uint64_t i) {
-  return kind == kEntryHashed ? reinterpret_cast<const uint4 *>(cb)[2 * i].x
-                              : reinterpret_cast<const uint2 *>(cb)[i].x;
+  return HASHED && kind == kEntryHashed ? reinterpret_cast<const uint4 *>(cb)[2 * i].x
+                                        : reinterpret_cast<const uint2 *>(cb)[i].x;
 }
 
+template <bool HASHED>
 __device__ __forceinline__ void apply_any(const uint8_t *cb, int kind, uint64_t i, uint32_t *s_sk,
                                           uint32_t vmask, const SketchGeom &g,
                                           const uint64_t *s_flip, uint64_t flip_chk) {
-  if (kind == kEntryHashed) {
+  if (HASHED && kind == kEntryHashed) {
     const uint4 *E = reinterpret_cast<const uint4 *>(cb);
     apply_hashed(E[2 * i], E[2 * i + 1], s_sk, vmask, g.sketch_words, s_flip, g.C, g.B);
   } else {
@@ -635,6 +637,9 @@ __device__ __forceinline__ void apply_any(const uint8_t *cb, int kind, uint64_t 
   }
 }
 
+// HASHED = some buffered chunk holds hashed entries (otherwise the plain-only variant, which
+// needs fewer registers, is launched).
+template <bool HASHED>
 __global__ void __launch_bounds__(1024, 1)
 k_sketch_update(SketchGeom g, uint8_t *__restrict__ sketches, const uint8_t *__restrict__ gutter,
                 ChunkTable chunks, const uint32_t *__restrict__ bin_off, int nchunks,
@@ -701,27 +706,27 @@ k_sketch_update(SketchGeom g, uint8_t *__restrict__ sketches, const uint8_t *__r
         if (per_bin == 0) {
           // the bin is this tile: every entry applies
           for (uint64_t i = b + threadIdx.x; i < e; i += blockDim.x)
-            apply_any(cb, kind, i, s_sk, vpt - 1, g, s_flip, flip_chk);
+            apply_any<HASHED>(cb, kind, i, s_sk, vpt - 1, g, s_flip, flip_chk);
         } else {
           // the bin holds several tiles: each warp ballots 32 entries, queues the indices of
           // this tile's, and applies only full warps of queued entries
           uint32_t qn = 0;
           for (uint64_t i0 = b + (uint64_t)warp * 32; i0 < e; i0 += (uint64_t)nwarps * 32) {
             const uint64_t i = i0 + lane;
-            const bool mine = i < e && (entry_vertex(cb, kind, i) >> g.tile_shift) == t;
+            const bool mine = i < e && (entry_vertex<HASHED>(cb, kind, i) >> g.tile_shift) == t;
             const uint32_t m = __ballot_sync(kFull, mine);
             if (mine) q[qn + __popc(m & ((1u << lane) - 1u))] = (uint32_t)i;
             qn += __popc(m);
             __syncwarp();
             if (qn >= 32) {
-              apply_any(cb, kind, q[lane], s_sk, vpt - 1, g, s_flip, flip_chk);
+              apply_any<HASHED>(cb, kind, q[lane], s_sk, vpt - 1, g, s_flip, flip_chk);
               __syncwarp();
               qn -= 32;
               if (lane < qn) q[lane] = q[32 + lane];
               __syncwarp();
             }
           }
-          if (lane < qn) apply_any(cb, kind, q[lane], s_sk, vpt - 1, g, s_flip, flip_chk);
+          if (lane < qn) apply_any<HASHED>(cb, kind, q[lane], s_sk, vpt - 1, g, s_flip, flip_chk);
           __syncwarp();
         }
       }
@@ -1054,7 +1059,8 @@ __global__ void __launch_bounds__(1024, 1) k_update_peak(uint32_t nb, uint32_t i
 inline unsigned blocks_for(uint64_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
 
 // Eight independent hash chains per thread: each step is one 8-byte XXH3 (rrmxmx with a column
-// constant) plus the depth ctz, the per-column work of the ingest kernel, with no memory traffic.
+// constant) to a bucket depth -- the per-column work of the ingest kernel -- plus one IMAD to make
+// the next input, with no memory traffic.
 __global__ void k_hash_peak(uint64_t seed, uint32_t iters, uint64_t *out) {
   const uint64_t flip = xxh3_flip(seed);
   uint64_t x[8];
@@ -1065,8 +1071,10 @@ __global__ void k_hash_peak(uint64_t seed, uint32_t iters, uint64_t *out) {
   for (uint32_t i = 0; i < iters; ++i) {
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-      x[k] = rrmxmx8(x[k] ^ flip);
-      acc += depth_of(x[k], 34);
+      // the sketch-update kernel's per-column work: one hash to a bucket depth (B = 34)
+      const uint32_t d = hash_depth(x[k] ^ flip, 34);
+      acc += d;
+      x[k] = x[k] * 0x9E3779B97F4A7C15ULL + d;
     }
   }
   uint64_t r = acc;
@@ -1253,13 +1261,16 @@ size_t sketch_update_smem_bytes(SketchGeom g) {
 
 cudaError_t sketch_update_prepare(SketchGeom g, int /*threads*/) {
   const size_t smem = sketch_update_smem_bytes(g);
-  return cudaFuncSetAttribute(k_sketch_update, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(k_sketch_update<false>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_sketch_update<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)smem);
 }
 
 int sketch_update_ctas_per_sm(SketchGeom g, int threads) {
   int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sketch_update, threads,
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sketch_update<false>, threads,
                                                     sketch_update_smem_bytes(g)) != cudaSuccess)
     return 1;
   return n > 0 ? n : 1;
@@ -1270,12 +1281,14 @@ cudaError_t sketch_update(SketchGeom g, uint8_t *sketches, const uint8_t *gutter
                           const uint64_t *flip, uint32_t *work_counter, uint32_t *status, int grid,
                           int threads, cudaStream_t s) {
   const size_t smem = sketch_update_smem_bytes(g);
+  bool hashed = false;
+  for (int k = 0; k < nchunks; ++k) hashed |= chunks.kind[k] == kEntryHashed;
+  auto kern = hashed ? k_sketch_update<true> : k_sketch_update<false>;
   // the limit is per function, and other handles may have set it for a smaller geometry
-  cudaError_t e = cudaFuncSetAttribute(k_sketch_update, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  k_sketch_update<<<grid, threads, smem, s>>>(g, sketches, gutter, chunks, bin_off, nchunks, flip,
-                                              work_counter, status);
+  kern<<<grid, threads, smem, s>>>(g, sketches, gutter, chunks, bin_off, nchunks, flip,
+                                   work_counter, status);
   g_launches++;
   return cudaGetLastError();
 }

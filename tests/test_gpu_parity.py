@@ -280,3 +280,32 @@ def test_mixed_hashed_and_plain_chunks(gz, oracle_mod):
     osk.apply_records(st.raw())
     assert (alg.dump_sketches() == osk.data).all()
     assert (canonical(alg.connected_components().parent_arr) == labels).all()
+
+
+def test_host_ingest_waves_match_device_ingest(gz, oracle_mod):
+    """4e7 host records cross a wave boundary (the gutter is folded into the sketches while later
+    records are still being copied); bytes must equal one device-resident ingest."""
+    torch = pytest.importorskip("torch")
+    from graphzeppelin_b200 import streams as S
+    V = 1 << 14
+    st, _ = S.planted_partition_stream_fast(V, 8, seed=3, mean_degree=4900, min_size=256,
+                                            churn_fraction=0.1)
+    assert st.num_updates > (1 << 25)
+    a = _alg(gz, V, 99)
+    a.set_gutter_capacity(2 * st.num_updates + 16)
+    a.ingest_records(st)
+    b = _alg(gz, V, 99)
+    b.set_gutter_capacity(2 * st.num_updates + 16)
+    d = torch.from_numpy(st.raw()).cuda()
+    b.ingest_records_device(d.data_ptr(), st.num_updates)
+    da, db = a.dump_sketches(), b.dump_sketches()
+    assert (da == db).all()
+    pick = np.random.default_rng(2).choice(V, 16, replace=False)
+    filt = np.zeros(V, np.uint8)
+    filt[pick] = 1
+    osk = oracle_mod.OracleSketches(V, 99)
+    osk.apply_records(st.raw(), vertex_filter=filt)
+    sb = osk.sketch_bytes
+    for v in pick:
+        assert (da[v * sb:(v + 1) * sb] == osk.sketch(v)).all()
+    assert a.num_connected_components() == 8
