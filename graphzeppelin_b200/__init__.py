@@ -11,6 +11,7 @@ from .cc import (CACHETREE, CONNECTIVITY, END_OF_STREAM, GUTTERTREE, KSPANNINGFO
                  GraphUpdate, GutterSystem, GZError, OutOfSamplesException, QueryCode,
                  SampleResult, SpanningForest, UpdateLockedException, UpdateType,
                  concat_pairing_fn, inv_concat_pairing_fn)
+from .batch import BatchResult, CCSketchBatch
 from .streams import RECORD_DTYPE, Stream, read_stream
 
 __all__ = [n for n in dir() if not n.startswith("_")]

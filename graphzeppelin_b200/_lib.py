@@ -85,6 +85,17 @@ SIGNATURES = [
     ("gz_get_stream", _i, [_H, ctypes.POINTER(ctypes.c_void_p)]),
     ("gz_set_tuning", _i, [_H, _u32, _u32, _u32, _u32]),
     ("gz_ingest_records_noalloc", _i, [_P, _u32, _u64, _d, _P, _sz, _P]),
+    ("gz_batch_create", _i, [_u32, _P, _P, _d, _P, ctypes.POINTER(_H)]),
+    ("gz_batch_destroy", _i, [_H]),
+    ("gz_batch_get_params", _i, [_H, _u32, ctypes.POINTER(gz_params_t)]),
+    ("gz_batch_ingest_device", _i, [_H, _P, _P]),
+    ("gz_batch_ingest", _i, [_H, _P, _P]),
+    ("gz_batch_clear", _i, [_H]),
+    ("gz_batch_connected_components", _i, [_H, _P, _P, _P, _P]),
+    ("gz_batch_dump_sketches", _i, [_H, _u32, _P, _sz]),
+    ("gz_batch_load_sketches", _i, [_H, _u32, _P, _sz]),
+    ("gz_batch_set_profiling", _i, [_H, _i]),
+    ("gz_batch_get_profile", _i, [_H, ctypes.POINTER(gz_profile_t)]),
 ]
 
 _lib = None

@@ -69,16 +69,6 @@ void host_free(T *&p) {
   p = nullptr;
 }
 
-// Reference sizing (include/sketch.h:62-76, :181, :188-190), evaluated with the same double
-// expressions so the results agree bit for bit.
-void reference_params(uint32_t V, double f, uint32_t &C, uint32_t &B) {
-  const uint64_t vec_len = (uint64_t)std::ceil(double(V) * (uint32_t)(V - 1) / 2);
-  B = (uint32_t)(std::ceil(std::log2((double)vec_len)) + 1);
-  const double num_samples_div = 1 - std::log2(2 - 0.8);
-  const size_t s = (size_t)std::ceil(f * std::log2((double)V) / num_samples_div);
-  C = (uint32_t)std::max<size_t>(18, s);
-}
-
 constexpr uint64_t kStageRecords = 1ull << 24;  // records per host->device pipeline chunk
 constexpr int kStageBuffers = 4;                 // device staging buffers of the copy pipeline
 // Host-record ingest applies the gutter to the sketches whenever this many endpoint updates are
@@ -89,6 +79,20 @@ constexpr uint64_t kMaxChunkEntries = 1ull << 31;
 constexpr int kNumPhases = 3;  // gutter, sketch update, query
 
 }  // namespace
+
+namespace gz {
+// Columns and buckets per column of one vertex sketch, CCSketchAlg's sizing
+// (src/cc_sketch_alg.cpp:16-17; include/sketch.h:62-76, :181, :188-190) evaluated with the same
+// double expressions so the results agree bit for bit: B = ceil(log2(V(V-1)/2)) + 1 buckets per
+// column, C = max(18, ceil(f * log2(V) / (1 - log2(1.2)))) columns.
+void sketch_sizing(uint32_t V, double f, uint32_t &C, uint32_t &B) {
+  const uint64_t vec_len = (uint64_t)std::ceil(double(V) * (uint32_t)(V - 1) / 2);
+  B = (uint32_t)(std::ceil(std::log2((double)vec_len)) + 1);
+  const double num_samples_div = 1 - std::log2(2 - 0.8);
+  const size_t s = (size_t)std::ceil(f * std::log2((double)V) / num_samples_div);
+  C = (uint32_t)std::max<size_t>(18, s);
+}
+}  // namespace gz
 
 // Error text for entry points defined in other files of this library.
 void gz_internal_set_error(const std::string &msg) { g_last_error = msg; }
@@ -288,7 +292,7 @@ int init_alg(gz_alg *h, uint32_t V, uint64_t seed, double sf, double bf) {
   h->seed = seed;
   h->sketches_factor = sf > 0 ? sf : 1;  // CCAlgConfiguration::sketches_factor
   h->batch_factor = bf > 0 ? bf : 1;     // CCAlgConfiguration::batch_factor
-  reference_params(V, h->sketches_factor, h->C, h->B);
+  gz::sketch_sizing(V, h->sketches_factor, h->C, h->B);
   if (h->B > 63) return fail(GZ_ERR_INVALID, "bkt_per_col above 63 is not supported");
   h->hashed_default = false;  // plain entries measured faster on B200 (see the design notes)
   h->hashed = h->hashed_default;

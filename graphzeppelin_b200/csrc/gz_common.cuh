@@ -1,0 +1,240 @@
+// gz_common.cuh -- device helpers shared by the single-graph kernels (gz_kernels.cu) and the
+// multi-graph engine (gz_batch.cu): bulk async copy + mbarrier PTX, 9-byte record staging,
+// the CAS union-find, the warp-cooperative Sketch::sample and the per-entry sketch update.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "gz_device.cuh"
+#include "gz_kernels.cuh"
+
+namespace gz {
+namespace dev {
+
+constexpr uint32_t kFull = 0xffffffffu;
+
+__device__ __forceinline__ uint32_t fmix32_(uint32_t h) {  // murmur3 finaliser
+  h ^= h >> 16;
+  h *= 0x85ebca6bu;
+  h ^= h >> 13;
+  h *= 0xc2b2ae35u;
+  h ^= h >> 16;
+  return h;
+}
+
+// ------------------------------------------------------------------------------------------------
+// small PTX helpers (bulk async copy + mbarrier)
+// ------------------------------------------------------------------------------------------------
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Bounded wait on an mbarrier phase: gives up after limit_ns of wall time.
+static __device__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity, uint64_t limit_ns) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  for (uint32_t it = 1; it < (1u << 30); ++it) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((it & 31u) == 0 && global_ns() - t0 > limit_ns) return false;
+  }
+  return false;
+}
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes,
+                                         uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(dst),
+      "l"(src), "r"(bytes), "r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ void bulk_s2g(void *dst, uint32_t src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(src),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() {
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait_read_all() {
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait_all() {
+  asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+constexpr uint32_t kBulkPiece = 32768;       // bytes per bulk copy instruction
+constexpr uint64_t kWaitLimitNs = 2000000000;  // 2 s bound on any device-side wait
+
+// ------------------------------------------------------------------------------------------------
+// record staging: coalesced 128-bit loads of a range of packed 9-byte records into shared memory
+// ------------------------------------------------------------------------------------------------
+constexpr uint32_t kRecStageBytes = kRecTile * 9 + 48;
+
+// Loads records [r, r + cnt) into s. Shared byte k mirrors global byte align16(start) + k.
+// Whole 16-byte blocks inside the range use one 128-bit load; the partial first/last block is
+// read byte by byte so no byte outside the caller's range is touched. Returns the offset of
+// record r inside s.
+__device__ __forceinline__ uint32_t stage_records(const uint8_t *base, uint64_t r, uint32_t cnt,
+                                                  uint8_t *s) {
+  const uintptr_t start = (uintptr_t)(base + r * 9);
+  const uintptr_t end = start + (uintptr_t)cnt * 9;
+  const uintptr_t a0 = start & ~(uintptr_t)15;
+  const uint32_t nvec = (uint32_t)((((end + 15) & ~(uintptr_t)15) - a0) >> 4);
+  for (uint32_t i = threadIdx.x; i < nvec; i += blockDim.x) {
+    const uintptr_t blk = a0 + ((uintptr_t)i << 4);
+    if (blk >= start && blk + 16 <= end) {
+      *reinterpret_cast<uint4 *>(s + i * 16) = __ldcs(reinterpret_cast<const uint4 *>(blk));
+    } else {
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        const uintptr_t p = blk + k;
+        if (p >= start && p < end) s[i * 16 + k] = *reinterpret_cast<const uint8_t *>(p);
+      }
+    }
+  }
+  return (uint32_t)(start - a0);
+}
+
+// src / dst of staged record i (the type byte is not needed).
+__device__ __forceinline__ void parse_record(const uint8_t *s, uint32_t shift, uint32_t i,
+                                             uint32_t &u, uint32_t &v) {
+  const uint32_t off = shift + 9 * i + 1;
+  const uint32_t *w = reinterpret_cast<const uint32_t *>(s) + (off >> 2);
+  const uint32_t sh = (off & 3) * 8;
+  u = __funnelshift_r(w[0], w[1], sh);
+  v = __funnelshift_r(w[1], w[2], sh);
+}
+
+
+// Folds one endpoint update (vertex v, neighbour w) into v's staged sketch: the deterministic
+// bucket always, then in each column the bucket at depth ctz(hash_c(idx) | 1 << B) when < B.
+__device__ __forceinline__ void apply_entry(uint2 e, uint32_t *s_sk, uint32_t vmask,
+                                            uint32_t sketch_words, const uint64_t *s_flip,
+                                            uint64_t flip_chk, uint32_t C, uint32_t B) {
+  const uint32_t v = e.x, w = e.y;
+  const uint32_t lo = max(v, w), hi = min(v, w);  // idx = (min << 32) | max
+  uint32_t *sk = s_sk + (v & vmask) * sketch_words;
+  const uint64_t in64 = ((uint64_t)lo << 32) | hi;
+  const uint32_t chk = hash_lo32(in64 ^ flip_chk);
+  uint32_t *det = sk + 3 * C * B;
+  atomicXor(det, lo);
+  atomicXor(det + 1, hi);
+  atomicXor(det + 2, chk);
+  for (uint32_t c = 0; c < C; ++c) {
+    const uint32_t d = hash_depth(in64 ^ s_flip[c], B);
+    if (d < B) {
+      uint32_t *bk = sk + 3 * (c * B + d);
+      atomicXor(bk, lo);
+      atomicXor(bk + 1, hi);
+      atomicXor(bk + 2, chk);
+    }
+  }
+}
+
+
+struct TraceRec {
+  uint32_t round, key, result, pad;
+  uint64_t idx;
+};
+
+
+// Total order used to link roots (lower rank goes under higher): no cycles can form, the same
+// role as the random priorities of DisjointSetUnion_MT::order_edge (include/dsu.h:113-117).
+__device__ __forceinline__ uint64_t rank_of(uint32_t x) {
+  return ((uint64_t)fmix32_(x) << 32) | x;
+}
+
+// find_root with path halving (include/dsu.h:145-152); loads/stores go to L2 so updates by other
+// SMs are seen.
+static __device__ uint32_t dsu_find(uint32_t *parent, uint32_t x) {
+  for (;;) {
+    const uint32_t p = __ldcg(parent + x);
+    if (p == x) return x;
+    const uint32_t gp = __ldcg(parent + p);
+    if (gp == p) return p;
+    __stcg(parent + x, gp);
+    x = gp;
+  }
+}
+
+// merge with CAS (include/dsu.h:155-167). Returns true when this call linked two roots.
+static __device__ bool dsu_unite(uint32_t *parent, uint32_t a, uint32_t b) {
+  for (;;) {
+    a = dsu_find(parent, a);
+    b = dsu_find(parent, b);
+    if (a == b) return false;
+    if (rank_of(a) < rank_of(b)) {
+      const uint32_t t = a;
+      a = b;
+      b = t;
+    }
+    if (atomicCAS(parent + b, b, a) == b) return true;
+  }
+}
+
+// Sketch::sample (src/sketch.cpp:94-116) on one merged column held one or two buckets per lane
+// (lane j holds bucket j and j + 32) plus the deterministic bucket (same on every lane).
+__device__ __forceinline__ int warp_sample(const uint32_t (&d)[3], const uint32_t (&a)[2][3],
+                                           uint32_t B, uint64_t flip_chk, uint64_t *idx) {
+  const int lane = threadIdx.x & 31;
+  if ((d[0] | d[1] | d[2]) == 0) {
+    *idx = 0;
+    return 1;  // ZERO
+  }
+  if (bucket_good(d[0], d[1], d[2], flip_chk)) {
+    *idx = ((uint64_t)d[1] << 32) | d[0];
+    return 0;  // GOOD
+  }
+#pragma unroll
+  for (int s = 0; s < 2; ++s) {
+    if ((uint32_t)s * 32 >= B) break;
+    const uint32_t j = s * 32 + lane;
+    const bool good = j < B && bucket_good(a[s][0], a[s][1], a[s][2], flip_chk);
+    const uint32_t m = __ballot_sync(kFull, good);
+    if (m) {
+      const int src = __ffs(m) - 1;
+      const uint32_t x0 = __shfl_sync(kFull, a[s][0], src);
+      const uint32_t x1 = __shfl_sync(kFull, a[s][1], src);
+      *idx = ((uint64_t)x1 << 32) | x0;
+      return 0;
+    }
+  }
+  *idx = 0;
+  return 2;  // FAIL
+}
+
+__device__ __forceinline__ void load_bucket(const uint32_t *p, uint32_t (&x)[3]) {
+  x[0] = p[0];
+  x[1] = p[1];
+  x[2] = p[2];
+}
+
+
+}  // namespace dev
+}  // namespace gz

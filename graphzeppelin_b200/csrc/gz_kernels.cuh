@@ -164,6 +164,8 @@ cudaError_t boruvka_final(const BoruvkaGeom &g, const BoruvkaBufs &b, uint32_t *
                           uint32_t *ncc, cudaStream_t s);
 
 int num_sms();
+// columns C and buckets per column B of one vertex sketch for V vertices and sketches factor f
+void sketch_sizing(uint32_t V, double f, uint32_t &C, uint32_t &B);
 
 // Register-only hash throughput probe: n_threads * iters * 8 hashes.
 cudaError_t hash_peak(uint64_t seed, uint32_t iters, int blocks, int threads, uint64_t *out,

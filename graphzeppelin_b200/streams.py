@@ -354,3 +354,31 @@ def cached_stream(cache_dir: str, name: str, builder) -> Stream:
     s.write(tmp)
     os.replace(tmp, path)
     return s
+
+
+def many_graph_streams(num_graphs: int, seed: int, *, log2_v_min: float = 8.0,
+                       log2_v_max: float = 16.0, degree_min: float = 8.0,
+                       degree_max: float = 256.0, max_components: int = 16,
+                       churn_fraction: float = 0.10):
+    """Independent planted-components streams of uneven size, one per graph: V log-uniform in
+    [2^log2_v_min, 2^log2_v_max], 1..max_components planted components, intra-component edge
+    probability set for a mean degree uniform in [degree_min, degree_max], churn as in
+    planted_partition_stream. Built by the C generator. Returns (num_vertices, sketch seeds,
+    packed records of all graphs back to back as one uint8 array, record offsets (G + 1))."""
+    rng = np.random.default_rng(seed)
+    Vs = np.exp2(rng.uniform(log2_v_min, log2_v_max, num_graphs)).astype(np.int64)
+    Vs = np.maximum(Vs, 2)
+    ks = rng.integers(1, max_components + 1, num_graphs)
+    degs = rng.uniform(degree_min, degree_max, num_graphs)
+    stream_seeds = rng.integers(0, 2**31, num_graphs)
+    sketch_seeds = rng.integers(0, 2**63, num_graphs, dtype=np.int64).astype(np.uint64)
+    parts = []
+    for V, k, d, s in zip(Vs, ks, degs, stream_seeds):
+        k = int(min(k, V))
+        st, _ = planted_partition_stream_fast(int(V), k, int(s), mean_degree=float(d),
+                                              churn_fraction=churn_fraction)
+        parts.append(st.records.view(np.uint8).reshape(-1))
+    counts = np.array([p.size // 9 for p in parts], np.uint64)
+    offsets = np.concatenate([[0], np.cumsum(counts)]).astype(np.uint64)
+    raw = np.concatenate(parts) if parts else np.zeros(0, np.uint8)
+    return Vs.astype(np.uint32), sketch_seeds, raw, offsets

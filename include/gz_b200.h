@@ -247,6 +247,46 @@ GZ_API int gz_measure_update_rate(int repeats, double *updates_per_s);
 GZ_API int gz_set_tuning(gz_alg_t *alg, uint32_t vertices_per_tile, uint32_t threads_per_block,
                          uint32_t tiles_per_bin, uint32_t entry_form);
 
+/* ---- many graphs on one GPU ------------------------------------------------------------------
+ * A gz_batch_t holds num_graphs independent CCSketchAlg instances (each its own V, seed and
+ * sketch geometry, include/cc_sketch_alg.h:69) in one device allocation. One ingest call runs one
+ * gutter pass and ONE persistent sketch-update launch over the tiles of every graph; one query
+ * runs Boruvka for all graphs at once, each round a replayed CUDA graph, each graph stopping on
+ * its own. Per graph the sketches, partition, last_query_rounds and out-of-samples outcome equal
+ * those of a gz_alg_t with the same V and seed fed the same records. */
+typedef struct gz_batch gz_batch_t;
+
+/* num_vertices[g], seeds[g]: as gz_create for graph g. vertices_per_tile may be NULL (default
+ * tiling per graph) or hold a power of two in [4, 64] (0 = default) per graph. */
+GZ_API int gz_batch_create(uint32_t num_graphs, const uint32_t *num_vertices, const uint64_t *seeds,
+                           double sketches_factor, const uint32_t *vertices_per_tile,
+                           gz_batch_t **out);
+GZ_API int gz_batch_destroy(gz_batch_t *batch);
+/* gz_get_params of graph g (batch_factor 1). */
+GZ_API int gz_batch_get_params(gz_batch_t *batch, uint32_t graph, gz_params_t *out);
+/* Applies records of every graph: graph g's packed 9-byte records {u8 type, u32 src, u32 dst}
+ * (reference README "Binary Stream Format") are d_records[offsets[g] .. offsets[g+1]) in device memory
+ * (offsets has num_graphs + 1 entries, in records). Synchronous: the records are folded into
+ * the sketches when the call returns. A vertex id >= its graph's V gives GZ_ERR_BAD_VERTEX. */
+GZ_API int gz_batch_ingest_device(gz_batch_t *batch, const void *d_records, const uint64_t *offsets);
+/* Same, records in host memory (copied to the device inside the call). */
+GZ_API int gz_batch_ingest(gz_batch_t *batch, const void *records, const uint64_t *offsets);
+/* Zeroes every graph's sketches. */
+GZ_API int gz_batch_clear(gz_batch_t *batch);
+/* connected_components (src/cc_sketch_alg.cpp:515-557) of every graph. labels_out (NULL or
+ * sum of V entries, graph-major) gets each vertex's graph-local root; num_cc, rounds and status
+ * (NULL or num_graphs entries) get each graph's component count, last_query_rounds, and
+ * GZ_OK or GZ_ERR_OUT_OF_SAMPLES. The call itself fails only on device or argument errors. */
+GZ_API int gz_batch_connected_components(gz_batch_t *batch, uint32_t *labels_out, uint32_t *num_cc,
+                                         uint32_t *rounds, int *status);
+/* Graph g's sketches, V * sketch_bytes bytes in gz_dump_sketches' layout. */
+GZ_API int gz_batch_dump_sketches(gz_batch_t *batch, uint32_t graph, void *host_buf, size_t bytes);
+/* Replaces graph g's sketches with V * sketch_bytes bytes in that layout (the sketch part of a
+ * write_binary file, as construct_from_serialized_data reads it, src/cc_sketch_alg.cpp:30-64). */
+GZ_API int gz_batch_load_sketches(gz_batch_t *batch, uint32_t graph, const void *host_buf, size_t bytes);
+GZ_API int gz_batch_set_profiling(gz_batch_t *batch, int enable);
+GZ_API int gz_batch_get_profile(gz_batch_t *batch, gz_profile_t *out);
+
 #ifdef __cplusplus
 }
 #endif
