@@ -60,11 +60,7 @@ class CCSketchBatch:
                                         _ptr(vpt) if vpt is not None else None, ctypes.byref(h)))
         self._h = h
         self.num_graphs = g
-        self.params = []
-        for i in range(g):
-            p = _lib.gz_params_t()
-            _check(self.lib.gz_batch_get_params(self._h, i, ctypes.byref(p)))
-            self.params.append(p)
+        self._refresh_params()
         self.vbase = np.concatenate([[0], np.cumsum(self.num_vertices.astype(np.int64))])
 
     def close(self):
@@ -138,6 +134,25 @@ class CCSketchBatch:
         """Replace graph g's sketches (V * sketch_bytes bytes, dump_sketches' layout)."""
         buf = np.ascontiguousarray(data, dtype=np.uint8).reshape(-1)
         _check(self.lib.gz_batch_load_sketches(self._h, g, _ptr(buf), buf.size))
+
+    def set_tuning(self, threads_per_block: int = 0, ctas_per_sm: int = 0,
+                   vertices_per_tile: Sequence[int] | None = None) -> None:
+        """Shape of the batched sketch-update launch (see gz_batch_set_tuning)."""
+        vpt = None
+        if vertices_per_tile is not None:
+            vpt = np.ascontiguousarray(vertices_per_tile, dtype=np.uint32)
+            if vpt.size != self.num_graphs:
+                raise ValueError("one vertices_per_tile entry per graph")
+        _check(self.lib.gz_batch_set_tuning(self._h, threads_per_block, ctas_per_sm,
+                                            _ptr(vpt) if vpt is not None else None))
+        self._refresh_params()
+
+    def _refresh_params(self):
+        self.params = []
+        for i in range(self.num_graphs):
+            p = _lib.gz_params_t()
+            _check(self.lib.gz_batch_get_params(self._h, i, ctypes.byref(p)))
+            self.params.append(p)
 
     def set_profiling(self, enable: bool = True) -> None:
         _check(self.lib.gz_batch_set_profiling(self._h, int(enable)))

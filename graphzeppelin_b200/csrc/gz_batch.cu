@@ -40,50 +40,120 @@ struct GraphDesc {
   uint32_t pad;
 };
 
-// index of the last base <= x in a sorted array of n bases (base[0] == 0)
-__device__ __forceinline__ uint32_t find_base(const uint32_t *base, uint32_t n, uint32_t x) {
-  uint32_t lo = 0, hi = n;
-  while (hi - lo > 1) {
-    const uint32_t mid = (lo + hi) >> 1;
-    if (base[mid] <= x) lo = mid;
-    else hi = mid;
+// ---- gutter ----------------------------------------------------------------------------------
+// The records of each graph are cut into record tiles of at most kMbRecTile records; a record
+// tile {graph, first record (lo, hi), count} belongs to one graph, so its endpoint entries land in
+// that graph's gutter bins only (at most kMbBinsMax of them).
+constexpr uint32_t kMbRecTile = 4096;
+constexpr uint32_t kMbBinsMax = 4096;
+constexpr uint32_t kMbTilesPerBinMax = 64;
+constexpr uint32_t kMbBinTarget = 4096;  // bins per graph aimed for with at most 16 tiles per bin
+
+// Counting pass: per record tile, a shared-memory histogram over the graph's bins, added to the
+// global bin counts once per non-empty bin.
+__global__ void __launch_bounds__(1024)
+k_mb_count(const uint8_t *__restrict__ rec, const uint4 *__restrict__ rtiles, uint32_t n_rt,
+           const GraphDesc *__restrict__ graphs, uint64_t *__restrict__ bins,
+           uint32_t *__restrict__ status) {
+  extern __shared__ __align__(16) uint8_t bsm[];
+  uint32_t *s_bin = reinterpret_cast<uint32_t *>(bsm);
+  uint8_t *s_rec = bsm + kMbBinsMax * 4;
+  bool bad = false;
+  for (uint32_t t = blockIdx.x; t < n_rt; t += gridDim.x) {
+    const uint4 rt = rtiles[t];
+    const GraphDesc gd = graphs[rt.x];
+    for (uint32_t b = threadIdx.x; b < gd.nbins; b += blockDim.x) s_bin[b] = 0u;
+    const uint32_t shift = stage_records(rec, ((uint64_t)rt.z << 32) | rt.y, rt.w, s_rec);
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < rt.w; i += blockDim.x) {
+      uint32_t u, v;
+      parse_record(s_rec, shift, i, u, v);
+      if (u >= gd.V || v >= gd.V) {
+        bad = true;
+        continue;
+      }
+      atomicAdd(&s_bin[u >> gd.bin_shift], 1u);
+      atomicAdd(&s_bin[v >> gd.bin_shift], 1u);
+    }
+    __syncthreads();
+    for (uint32_t b = threadIdx.x; b < gd.nbins; b += blockDim.x)
+      if (s_bin[b])
+        atomicAdd(reinterpret_cast<unsigned long long *>(bins + gd.bin_base + b),
+                  (unsigned long long)s_bin[b]);
+    __syncthreads();
   }
-  return lo;
+  if (bad) atomicOr(status, kStatusBadVertex);
 }
 
-// ---- gutter ----------------------------------------------------------------------------------
-// record tile: {graph, first record (lo, hi), count}
-template <bool COUNT>
-__global__ void __launch_bounds__(512)
-k_mb_gutter(const uint8_t *__restrict__ rec, const uint4 *__restrict__ rtiles,
-            const GraphDesc *__restrict__ graphs, uint64_t *__restrict__ bins,
-            uint2 *__restrict__ entries, uint32_t *__restrict__ status) {
+// Sort-scatter pass: per record tile, counting-sort its endpoint entries by bin in shared memory,
+// reserve one run per non-empty bin in the bin's gutter region (one global atomic per tile and
+// bin), and write the runs out with consecutive threads on consecutive addresses.
+// base[b] = first slot of global bin b (scanned counts), fill[b] = slots taken so far.
+__global__ void __launch_bounds__(1024, 1)
+k_mb_sort_scatter(const uint8_t *__restrict__ rec, const uint4 *__restrict__ rtiles, uint32_t n_rt,
+                  const GraphDesc *__restrict__ graphs, const uint64_t *__restrict__ base,
+                  uint32_t *__restrict__ fill, uint2 *__restrict__ entries) {
   extern __shared__ __align__(16) uint8_t bsm[];
-  const uint4 rt = rtiles[blockIdx.x];
-  const GraphDesc gd = graphs[rt.x];
-  const uint64_t start = ((uint64_t)rt.z << 32) | rt.y;
-  const uint32_t shift = stage_records(rec, start, rt.w, bsm);
-  __syncthreads();
-  bool bad = false;
-  for (uint32_t i = threadIdx.x; i < rt.w; i += blockDim.x) {
-    uint32_t u, v;
-    parse_record(bsm, shift, i, u, v);
-    if (u >= gd.V || v >= gd.V) {
-      bad = true;
-      continue;
+  __shared__ uint32_t ws[32];
+  uint32_t *s_cur = reinterpret_cast<uint32_t *>(bsm);  // counts, then placement cursors
+  uint32_t *s_off = s_cur + kMbBinsMax;                  // run start inside the tile
+  uint32_t *s_dst = s_off + kMbBinsMax;                  // run start inside the gutter
+  uint2 *s_sorted = reinterpret_cast<uint2 *>(s_dst + kMbBinsMax);
+  uint8_t *s_rec = reinterpret_cast<uint8_t *>(s_sorted + 2 * kMbRecTile);
+  for (uint32_t t = blockIdx.x; t < n_rt; t += gridDim.x) {
+    const uint4 rt = rtiles[t];
+    const GraphDesc gd = graphs[rt.x];
+    const uint32_t nb = gd.nbins, cnt = rt.w;
+    const uint32_t per_thread = (nb + blockDim.x - 1) / blockDim.x;  // <= 4
+    for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) s_cur[b] = 0u;
+    const uint32_t shift = stage_records(rec, ((uint64_t)rt.z << 32) | rt.y, cnt, s_rec);
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
+      uint32_t u, v;
+      parse_record(s_rec, shift, i, u, v);
+      if (u >= gd.V || v >= gd.V) continue;
+      atomicAdd(&s_cur[u >> gd.bin_shift], 1u);
+      atomicAdd(&s_cur[v >> gd.bin_shift], 1u);
     }
-    unsigned long long *bu = reinterpret_cast<unsigned long long *>(bins + gd.bin_base + (u >> gd.bin_shift));
-    unsigned long long *bv = reinterpret_cast<unsigned long long *>(bins + gd.bin_base + (v >> gd.bin_shift));
-    if (COUNT) {
-      atomicAdd(bu, 1ull);
-      atomicAdd(bv, 1ull);
-    } else {
-      entries[atomicAdd(bu, 1ull)] = make_uint2(u, v);
-      entries[atomicAdd(bv, 1ull)] = make_uint2(v, u);
+    __syncthreads();
+    uint32_t local[4] = {0, 0, 0, 0}, sum = 0;
+    for (uint32_t k = 0; k < per_thread; ++k) {
+      const uint32_t b = threadIdx.x * per_thread + k;
+      local[k] = b < nb ? s_cur[b] : 0u;
+      sum += local[k];
     }
+    uint32_t run = block_scan_1024(sum, ws);
+    for (uint32_t k = 0; k < per_thread; ++k) {
+      const uint32_t b = threadIdx.x * per_thread + k;
+      if (b < nb) {
+        const uint32_t gb = gd.bin_base + b;
+        s_off[b] = run;
+        s_dst[b] = local[k] ? (uint32_t)base[gb] + atomicAdd(&fill[gb], local[k]) : 0u;
+        s_cur[b] = run;
+      }
+      run += local[k];
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
+      uint32_t u, v;
+      parse_record(s_rec, shift, i, u, v);
+      if (u >= gd.V || v >= gd.V) continue;
+      s_sorted[atomicAdd(&s_cur[u >> gd.bin_shift], 1u)] = make_uint2(u, v);
+      s_sorted[atomicAdd(&s_cur[v >> gd.bin_shift], 1u)] = make_uint2(v, u);
+    }
+    __syncthreads();
+    const uint32_t total = s_cur[nb - 1];
+    for (uint32_t j = threadIdx.x; j < total; j += blockDim.x) {
+      const uint2 x = s_sorted[j];
+      const uint32_t b = x.x >> gd.bin_shift;
+      entries[s_dst[b] + (j - s_off[b])] = x;
+    }
+    __syncthreads();
   }
-  if (COUNT && bad) atomicOr(status, kStatusBadVertex);
 }
+
+constexpr size_t kMbCountSmem = kMbBinsMax * 4 + kMbRecTile * 9 + 48;
+constexpr size_t kMbSortSmem = 3 * kMbBinsMax * 4 + 2 * kMbRecTile * 8 + kMbRecTile * 9 + 48;
 
 __global__ void k_mb_bin_off(const uint64_t *scanned, uint64_t nbins, const uint64_t *total,
                              uint32_t *bin_off) {
@@ -93,110 +163,185 @@ __global__ void k_mb_bin_off(const uint64_t *scanned, uint64_t nbins, const uint
 }
 
 // ---- sketch update -------------------------------------------------------------------------------
-// One persistent launch over the (graph, tile) items of every graph: stage the tile with bulk
-// async copies, XOR in the entries of the tile's gutter bin that belong to it, write it back.
+// One persistent launch over the (graph, tile) items of every graph, warp-specialised: lane 0 of
+// the last warp is the producer -- it claims items from a device work counter, bulk-loads each
+// tile and its graph's hash constants into one of two buffers, and writes finished tiles back;
+// the other warps consume, XORing the tile's gutter entries into the staged buckets. Buffers
+// are handed over with mbarriers (full: tile landed; empty: every consumer thread is done), so
+// claiming, loading and writing back overlap the hashing of the other buffer and no CTA-wide
+// barrier ever waits on the producer.
+struct MbSlot {
+  uint32_t item, b, e, lt;                 // work item, entry range of its bin, tile in graph
+  uint32_t C, B, words, tile_shift, bin_shift;
+};
+
 __global__ void __launch_bounds__(1024, 1)
-k_mb_sketch_update(const GraphDesc *__restrict__ graphs, const uint32_t *__restrict__ tile_base,
-                   uint32_t G, uint32_t total_tiles, uint8_t *__restrict__ sketches,
+k_mb_sketch_update(const GraphDesc *__restrict__ graphs, const uint32_t *__restrict__ tile_graph,
+                   uint32_t total_tiles, uint8_t *__restrict__ sketches,
                    const uint2 *__restrict__ entries, const uint32_t *__restrict__ bin_off,
-                   const uint64_t *__restrict__ flip, uint32_t max_tile_bytes,
+                   const uint64_t *__restrict__ flip, uint32_t tile_stride, uint32_t flip_stride,
                    uint32_t *work_counter, uint32_t *status) {
   extern __shared__ __align__(128) uint8_t dsm[];
-  __shared__ __align__(8) uint64_t s_bar;
-  __shared__ uint32_t s_item, s_graph, s_b, s_e;
-  uint32_t *s_sk = reinterpret_cast<uint32_t *>(dsm);
-  uint32_t *s_queue = reinterpret_cast<uint32_t *>(dsm + max_tile_bytes);
-  uint64_t *s_flip = reinterpret_cast<uint64_t *>(dsm + max_tile_bytes + kQueueBytes);
-  const uint32_t bar = smem_u32(&s_bar);
+  __shared__ __align__(8) uint64_t s_full[2], s_empty[2];
+  __shared__ MbSlot s_slot[2];
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t ncw = (blockDim.x >> 5) - 1;  // consumer warps
+  const uint32_t nct = ncw * 32;               // consumer threads
+  uint8_t *s_flipb = dsm + 2 * tile_stride;    // 2 x flip_stride bytes
+  uint32_t *s_queue = reinterpret_cast<uint32_t *>(s_flipb + 2 * flip_stride);
   if (threadIdx.x == 0) {
-    mbar_init(bar, 1);
+    mbar_init(smem_u32(&s_full[0]), 1);
+    mbar_init(smem_u32(&s_full[1]), 1);
+    mbar_init(smem_u32(&s_empty[0]), nct);
+    mbar_init(smem_u32(&s_empty[1]), nct);
     mbar_fence_init();
   }
-  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  uint32_t *q = s_queue + warp * 64;
-  uint32_t parity = 0, cur_graph = 0xffffffffu;
   __syncthreads();
-  for (;;) {
-    if (threadIdx.x == 0) {
-      const uint32_t t = atomicAdd(work_counter, 1u);
-      s_item = t;
-      if (t < total_tiles) {
-        const uint32_t g = find_base(tile_base, G, t);
-        const GraphDesc gd = graphs[g];
-        const uint32_t lt = t - gd.tile_base;
-        const uint32_t bin = gd.bin_base + (lt >> (gd.bin_shift - gd.tile_shift));
-        s_graph = g;
-        s_b = bin_off[bin];
-        s_e = bin_off[bin + 1];
-        if (s_e > s_b) {
-          const uint32_t bytes = (gd.sketch_words * 4) << gd.tile_shift;
-          const uint8_t *src = sketches + gd.sk_off + (uint64_t)lt * bytes;
-          mbar_expect_tx(bar, bytes);
-          for (uint32_t off = 0; off < bytes; off += kBulkPiece)
-            bulk_g2s(smem_u32(dsm) + off, src + off, min(kBulkPiece, bytes - off), bar);
+
+  if (warp == ncw) {  // ---------------- producer ----------------
+    if (lane != 0) return;
+    // claim the next item: its slot, and where its tile and hash constants live
+    struct Claim {
+      MbSlot m;
+      const uint8_t *src;
+      const uint64_t *fsrc;
+      uint32_t bytes, fbytes;
+    };
+    auto claim = [&]() {
+      Claim c;
+      c.m.item = atomicAdd(work_counter, 1u);
+      c.m.b = c.m.e = 0;
+      c.bytes = c.fbytes = 0;
+      c.src = nullptr;
+      c.fsrc = nullptr;
+      if (c.m.item < total_tiles) {
+        const GraphDesc gd = graphs[tile_graph[c.m.item]];
+        c.m.lt = c.m.item - gd.tile_base;
+        c.m.C = gd.C;
+        c.m.B = gd.B;
+        c.m.words = gd.sketch_words;
+        c.m.tile_shift = gd.tile_shift;
+        c.m.bin_shift = gd.bin_shift;
+        const uint32_t bin = gd.bin_base + (c.m.lt >> (gd.bin_shift - gd.tile_shift));
+        c.m.b = bin_off[bin];
+        c.m.e = bin_off[bin + 1];
+        if (c.m.e > c.m.b) {
+          c.bytes = (gd.sketch_words * 4) << gd.tile_shift;
+          c.fbytes = ((gd.C + 2) & ~1u) * 8;
+          c.src = sketches + gd.sk_off + (uint64_t)c.m.lt * c.bytes;
+          c.fsrc = flip + gd.flip_off;
         }
+      }
+      return c;
+    };
+    uint8_t *pdst[2] = {nullptr, nullptr};
+    uint32_t pbytes[2] = {0, 0};
+    uint32_t issued = 0;         // bit s: a load into buffer s was issued
+    uint32_t lastk[2] = {0, 0};  // item index k of the last load into buffer s
+    uint32_t k = 0;
+    bool ok = true;
+    Claim c = claim();
+    for (;; ++k) {
+      const uint32_t s = k & 1;
+      if (k >= 2) {  // consumers must be done with tile k - 2 (same buffer) before reuse
+        if (!mbar_wait_bounded(smem_u32(&s_empty[s]), ((k - 2) >> 1) & 1, kWaitLimitNs)) {
+          ok = false;
+          break;
+        }
+        if (pbytes[s]) {
+          for (uint32_t off = 0; off < pbytes[s]; off += kBulkPiece)
+            bulk_s2g(pdst[s] + off, smem_u32(dsm + s * tile_stride) + off, min(kBulkPiece, pbytes[s] - off));
+          bulk_commit();
+          bulk_wait_read_all();
+        }
+      }
+      const uint32_t full = smem_u32(&s_full[s]);
+      s_slot[s] = c.m;
+      pbytes[s] = c.bytes;
+      pdst[s] = const_cast<uint8_t *>(c.src);
+      if (c.bytes) {
+        const uint32_t dst = smem_u32(dsm + s * tile_stride);
+        mbar_expect_tx(full, c.bytes + c.fbytes);
+        for (uint32_t off = 0; off < c.bytes; off += kBulkPiece)
+          bulk_g2s(dst + off, c.src + off, min(kBulkPiece, c.bytes - off), full);
+        bulk_g2s(smem_u32(s_flipb + s * flip_stride), c.fsrc, c.fbytes, full);
+        issued |= 1u << s;
+        lastk[s] = k;
+      } else {
+        mbar_arrive(full);  // nothing to apply, or end of work: hand the slot over at once
+      }
+      if (c.m.item >= total_tiles) break;
+      c = claim();  // the next item's lookups overlap this tile's load
+    }
+    if (ok && k >= 1) {  // write back the last tile
+      const uint32_t s = (k - 1) & 1;
+      ok = mbar_wait_bounded(smem_u32(&s_empty[s]), ((k - 1) >> 1) & 1, kWaitLimitNs);
+      if (ok && pbytes[s]) {
+        for (uint32_t off = 0; off < pbytes[s]; off += kBulkPiece)
+          bulk_s2g(pdst[s] + off, smem_u32(dsm + s * tile_stride) + off, min(kBulkPiece, pbytes[s] - off));
+        bulk_commit();
       }
     }
-    __syncthreads();
-    const uint32_t t = s_item;
-    if (t >= total_tiles) break;
-    if (s_e > s_b) {
-      const uint32_t g = s_graph;
-      const GraphDesc gd = graphs[g];
-      if (g != cur_graph) {  // this CTA's flips belong to another graph: reload
-        for (uint32_t i = threadIdx.x; i <= gd.C; i += blockDim.x) s_flip[i] = flip[gd.flip_off + i];
-        cur_graph = g;
-      }
-      const bool ok = mbar_wait_bounded(bar, parity, kWaitLimitNs);
-      parity ^= 1u;
-      if (__syncthreads_or(!ok)) {
-        if (threadIdx.x == 0) {
-          atomicOr(status, kStatusTimeout);
-          mbar_wait_bounded(bar, parity ^ 1u, kWaitLimitNs);
+    if (!ok) {
+      atomicOr(status, kStatusTimeout);
+      // every load issued must land before the CTA's shared memory goes away
+      for (uint32_t s = 0; s < 2; ++s)
+        if (issued & (1u << s)) mbar_wait_bounded(smem_u32(&s_full[s]), (lastk[s] >> 1) & 1, kWaitLimitNs);
+    }
+    bulk_wait_all();
+    return;
+  }
+
+  // ---------------- consumers ----------------
+  const uint32_t ct = threadIdx.x;  // consumer thread index (warps 0 .. ncw - 1)
+  uint32_t *q = s_queue + warp * 64;
+  for (uint32_t k = 0;; ++k) {
+    const uint32_t s = k & 1;
+    if (!mbar_wait_bounded(smem_u32(&s_full[s]), (k >> 1) & 1, kWaitLimitNs)) {
+      if (lane == 0) atomicOr(status, kStatusTimeout);
+      return;
+    }
+    const MbSlot m = s_slot[s];
+    if (m.item >= total_tiles) return;
+    if (m.e > m.b) {
+      uint32_t *s_sk = reinterpret_cast<uint32_t *>(dsm + s * tile_stride);
+      const uint64_t *s_flip = reinterpret_cast<const uint64_t *>(s_flipb + s * flip_stride);
+      const uint32_t vmask = (1u << m.tile_shift) - 1;
+      const uint64_t flip_chk = s_flip[m.C];
+      if (m.bin_shift == m.tile_shift) {
+        // every entry of the bin is this tile's; the next entry's load is in flight while the
+        // current one is hashed
+        uint32_t i = m.b + ct;
+        uint2 cur = i < m.e ? entries[i] : make_uint2(0, 0);
+        for (; i < m.e; i += nct) {
+          const uint2 e = cur;
+          if (i + nct < m.e) cur = entries[i + nct];
+          apply_entry(e, s_sk, vmask, m.words, s_flip, flip_chk, m.C, m.B);
         }
-        return;
-      }
-      const uint32_t lt = t - gd.tile_base;
-      const uint32_t vmask = (1u << gd.tile_shift) - 1;
-      const uint64_t flip_chk = s_flip[gd.C];
-      const uint32_t b = s_b, e = s_e;
-      if (gd.bin_shift == gd.tile_shift) {
-        for (uint32_t i = b + threadIdx.x; i < e; i += blockDim.x)
-          apply_entry(entries[i], s_sk, vmask, gd.sketch_words, s_flip, flip_chk, gd.C, gd.B);
       } else {
         uint32_t qn = 0;
-        for (uint32_t i0 = b + warp * 32; i0 < e; i0 += nwarps * 32) {
+        for (uint32_t i0 = m.b + warp * 32; i0 < m.e; i0 += nct) {
           const uint32_t i = i0 + lane;
-          const bool mine = i < e && (entries[i].x >> gd.tile_shift) == lt;
-          const uint32_t m = __ballot_sync(0xffffffffu, mine);
-          if (mine) q[qn + __popc(m & ((1u << lane) - 1u))] = i;
-          qn += __popc(m);
+          const bool mine = i < m.e && (entries[i].x >> m.tile_shift) == m.lt;
+          const uint32_t bal = __ballot_sync(0xffffffffu, mine);
+          if (mine) q[qn + __popc(bal & ((1u << lane) - 1u))] = i;
+          qn += __popc(bal);
           __syncwarp();
           if (qn >= 32) {
-            apply_entry(entries[q[lane]], s_sk, vmask, gd.sketch_words, s_flip, flip_chk, gd.C, gd.B);
+            apply_entry(entries[q[lane]], s_sk, vmask, m.words, s_flip, flip_chk, m.C, m.B);
             __syncwarp();
             qn -= 32;
             if (lane < qn) q[lane] = q[32 + lane];
             __syncwarp();
           }
         }
-        if (lane < qn)
-          apply_entry(entries[q[lane]], s_sk, vmask, gd.sketch_words, s_flip, flip_chk, gd.C, gd.B);
+        if (lane < qn) apply_entry(entries[q[lane]], s_sk, vmask, m.words, s_flip, flip_chk, m.C, m.B);
+        __syncwarp();
       }
-      fence_proxy_async_smem();
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        const uint32_t bytes = (gd.sketch_words * 4) << gd.tile_shift;
-        uint8_t *dst = sketches + gd.sk_off + (uint64_t)lt * bytes;
-        for (uint32_t off = 0; off < bytes; off += kBulkPiece)
-          bulk_s2g(dst + off, smem_u32(dsm) + off, min(kBulkPiece, bytes - off));
-        bulk_commit();
-        bulk_wait_read_all();
-      }
+      fence_proxy_async_smem();  // this thread's bucket writes, before the bulk write-back
     }
-    __syncthreads();
+    mbar_arrive(smem_u32(&s_empty[s]));
   }
-  if (threadIdx.x == 0) bulk_wait_all();
 }
 
 // ---- batched Boruvka -------------------------------------------------------------------------------
@@ -481,9 +626,11 @@ struct gz_batch {
   std::vector<GraphDesc> graphs;
   std::vector<uint64_t> seeds;
   uint64_t total_V = 0, total_bins = 0, total_tiles = 0, sk_bytes = 0;
-  uint32_t max_B = 0, max_C = 0, max_tile_bytes = 0, threads = 1024;
+  uint32_t max_B = 0, max_C = 0, max_tile_bytes = 0;
+  uint32_t threads = 1024, ctas_per_sm = 1;  // sketch-update CTA shape
+  std::vector<uint32_t> vpt_req;             // requested vertices per tile (0 = default)
   GraphDesc *d_graphs = nullptr;
-  uint32_t *d_tile_base = nullptr, *d_gov = nullptr;
+  uint32_t *d_tile_graph = nullptr, *d_gov = nullptr;  // graph of each global tile / vertex
   uint8_t *d_sk = nullptr;
   uint64_t *d_flip = nullptr;
   uint32_t *d_status = nullptr, *h_small = nullptr;
@@ -491,6 +638,7 @@ struct gz_batch {
   uint2 *d_entries = nullptr;
   uint64_t entry_cap = 0;
   uint64_t *d_bins = nullptr, *d_scan_tmp = nullptr, *d_total = nullptr;
+  uint32_t *d_bin_fill = nullptr;  // per-bin slots taken by the sort-scatter pass
   uint32_t *d_bin_off = nullptr;
   uint4 *d_rtiles = nullptr;
   size_t rtiles_cap = 0;
@@ -547,7 +695,7 @@ void batch_destroy(gz_batch *h) {
   if (h->round_exec) cudaGraphExecDestroy(h->round_exec);
   if (h->round_graph) cudaGraphDestroy(h->round_graph);
   mb_free(h->d_graphs);
-  mb_free(h->d_tile_base);
+  mb_free(h->d_tile_graph);
   mb_free(h->d_gov);
   mb_free(h->d_sk);
   mb_free(h->d_flip);
@@ -555,6 +703,7 @@ void batch_destroy(gz_batch *h) {
   if (h->h_small) cudaFreeHost(h->h_small);
   mb_free(h->d_entries);
   mb_free(h->d_bins);
+  mb_free(h->d_bin_fill);
   mb_free(h->d_scan_tmp);
   mb_free(h->d_total);
   mb_free(h->d_bin_off);
@@ -580,10 +729,24 @@ void batch_destroy(gz_batch *h) {
 
 // Per-graph tile/bin geometry: the single-graph default rule (tile of at most 64 vertices that
 // fits in shared memory, bins of up to 16 tiles), or an explicit vertices-per-tile.
+// Shared memory one sketch-update CTA may use when ctas_per_sm of them share an SM.
+size_t cta_smem_budget(const gz_batch *h) {
+  int optin = 0, per_sm = 0, reserved = 0;
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
+  cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, h->device);
+  cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, h->device);
+  if (optin <= 0) optin = 227 * 1024;
+  if (per_sm <= 0) per_sm = 228 * 1024;
+  const size_t share = (size_t)per_sm / h->ctas_per_sm - (size_t)std::max(reserved, 0);
+  return std::min<size_t>((size_t)optin, share);
+}
+
+// Tile and bin geometry of every graph. A requested vertices-per-tile (vpt_req[g] != 0) is
+// used as given; otherwise the largest power of two <= 64 whose tile fits the CTA's shared memory
+// (a batch has enough tiles to fill the GPU, and bigger tiles spread the shared-memory atomics
+// over more buckets).
 int layout(gz_batch *h, const std::vector<uint32_t> &vpt_req) {
-  int smem_optin = 0;
-  cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
-  if (smem_optin <= 0) smem_optin = 227 * 1024;
+  const size_t cta_smem = cta_smem_budget(h);
   uint64_t sk_off = 0, vbase = 0, bin_base = 0, tile_base = 0, flip_off = 0;
   h->max_tile_bytes = 0;
   h->max_B = h->max_C = 0;
@@ -592,7 +755,11 @@ int layout(gz_batch *h, const std::vector<uint32_t> &vpt_req) {
     h->max_C = std::max(h->max_C, gd.C);
   }
   // one launch serves every graph: its shared memory holds the largest tile and the most flips
-  const size_t budget = (size_t)smem_optin - 64 - kQueueBytes - (size_t)(h->max_C + 1) * 8;
+  const size_t queue = (size_t)(h->threads / 32) * 256;
+  // static shared memory (256), consumer queues, two padded flip arrays
+  const size_t fixed = 256 + queue + 2 * (size_t)((h->max_C + 2) & ~1u) * 8;
+  if (cta_smem <= fixed) return mb_fail(GZ_ERR_INVALID, "no shared memory left for a tile");
+  const size_t budget = ((cta_smem - fixed) / 2) & ~(size_t)127;  // two tile buffers
   for (uint32_t g = 0; g < h->G; ++g) {
     GraphDesc &gd = h->graphs[g];
     const uint64_t sketch_bytes = (uint64_t)gd.sketch_words * 4;
@@ -600,13 +767,16 @@ int layout(gz_batch *h, const std::vector<uint32_t> &vpt_req) {
     if (!vpt_req.empty() && vpt_req[g]) {
       shift = (uint32_t)__builtin_ctz(vpt_req[g]);
     } else {
-      const uint64_t want = std::max<uint64_t>(4, gd.V / (2ull * num_sms()));
-      while (shift < 6 && (1ull << (shift + 1)) <= want && (sketch_bytes << (shift + 1)) <= budget)
-        ++shift;
+      while (shift < 6 && (sketch_bytes << (shift + 1)) <= budget) ++shift;
     }
     if ((sketch_bytes << shift) > budget) return mb_fail(GZ_ERR_INVALID, "sketch too large for a tile");
     uint32_t bshift = shift;
-    while (((gd.V + (1u << bshift) - 1) >> bshift) > 4096 && (1u << (bshift - shift)) < 16) ++bshift;
+    while (((gd.V + (1u << bshift) - 1) >> bshift) > kMbBinTarget && (1u << (bshift - shift)) < 16) ++bshift;
+    while (((gd.V + (1u << bshift) - 1) >> bshift) > kMbBinsMax && (1u << (bshift - shift)) < kMbTilesPerBinMax)
+      ++bshift;
+    if (((gd.V + (1u << bshift) - 1) >> bshift) > kMbBinsMax)
+      return mb_fail(GZ_ERR_INVALID, "graph " + std::to_string(g) + " (V=" + std::to_string(gd.V) +
+                                         ") is too large for a batch: use a single-graph handle");
     gd.tile_shift = shift;
     gd.bin_shift = bshift;
     gd.ntiles = (gd.V + (1u << shift) - 1) >> shift;
@@ -621,7 +791,7 @@ int layout(gz_batch *h, const std::vector<uint32_t> &vpt_req) {
     vbase += gd.V;
     bin_base += gd.nbins;
     tile_base += gd.ntiles;
-    flip_off += gd.C + 1;
+    flip_off += (gd.C + 2) & ~1u;  // even: every graph's constants start 16-byte aligned
     h->max_tile_bytes = std::max<uint32_t>(h->max_tile_bytes, (uint32_t)(sketch_bytes << shift));
   }
   if (vbase > 0xFFFFFFF0ull || bin_base > 0xFFFFFFF0ull || tile_base > 0xFFFFFFF0ull)
@@ -633,11 +803,29 @@ int layout(gz_batch *h, const std::vector<uint32_t> &vpt_req) {
   return GZ_OK;
 }
 
+// gutter-bin arrays sized for the current layout
+int alloc_bins(gz_batch *h) {
+  mb_free(h->d_bins);
+  mb_free(h->d_bin_fill);
+  mb_free(h->d_scan_tmp);
+  mb_free(h->d_bin_off);
+  MB_TRY(mb_alloc(&h->d_bins, h->total_bins));
+  MB_TRY(mb_alloc(&h->d_bin_fill, h->total_bins));
+  MB_TRY(mb_alloc(&h->d_scan_tmp, scan_tmp_words(h->total_bins)));
+  MB_TRY(mb_alloc(&h->d_bin_off, h->total_bins + 1));
+  return GZ_OK;
+}
+
 int upload_tables(gz_batch *h) {
-  std::vector<uint32_t> tb(h->G);
-  for (uint32_t g = 0; g < h->G; ++g) tb[g] = h->graphs[g].tile_base;
+  std::vector<uint32_t> tg(h->total_tiles);
+  for (uint32_t g = 0; g < h->G; ++g) {
+    const GraphDesc &gd = h->graphs[g];
+    std::fill(tg.begin() + gd.tile_base, tg.begin() + gd.tile_base + gd.ntiles, g);
+  }
+  mb_free(h->d_tile_graph);
+  MB_TRY(mb_alloc(&h->d_tile_graph, h->total_tiles));
   MB_CUDA(cudaMemcpyAsync(h->d_graphs, h->graphs.data(), sizeof(GraphDesc) * h->G, cudaMemcpyHostToDevice, h->stream));
-  MB_CUDA(cudaMemcpyAsync(h->d_tile_base, tb.data(), sizeof(uint32_t) * h->G, cudaMemcpyHostToDevice, h->stream));
+  MB_CUDA(cudaMemcpyAsync(h->d_tile_graph, tg.data(), sizeof(uint32_t) * tg.size(), cudaMemcpyHostToDevice, h->stream));
   MB_CUDA(cudaStreamSynchronize(h->stream));
   return GZ_OK;
 }
@@ -662,8 +850,8 @@ int batch_ingest(gz_batch *h, const void *d_rec, const uint64_t *off) {
   uint64_t n_total = 0;
   for (uint32_t g = 0; g < h->G; ++g) {
     if (off[g + 1] < off[g]) return mb_fail(GZ_ERR_INVALID, "record offsets must be non-decreasing");
-    for (uint64_t s = off[g]; s < off[g + 1]; s += kRecTile) {
-      const uint32_t cnt = (uint32_t)std::min<uint64_t>(kRecTile, off[g + 1] - s);
+    for (uint64_t s = off[g]; s < off[g + 1]; s += kMbRecTile) {
+      const uint32_t cnt = (uint32_t)std::min<uint64_t>(kMbRecTile, off[g + 1] - s);
       rt.push_back(make_uint4(g, (uint32_t)s, (uint32_t)(s >> 32), cnt));
     }
     n_total += off[g + 1] - off[g];
@@ -691,32 +879,46 @@ int batch_ingest(gz_batch *h, const void *d_rec, const uint64_t *off) {
   }
   MB_CUDA(cudaMemcpyAsync(h->d_rtiles, rt.data(), sizeof(uint4) * rt.size(), cudaMemcpyHostToDevice, h->stream));
   MB_CUDA(cudaMemsetAsync(h->d_bins, 0, sizeof(uint64_t) * h->total_bins, h->stream));
-  const size_t smem = kRecTile * 9 + 48;
+  MB_CUDA(cudaMemsetAsync(h->d_bin_fill, 0, sizeof(uint32_t) * h->total_bins, h->stream));
   const uint8_t *rec = static_cast<const uint8_t *>(d_rec);
-  k_mb_gutter<true><<<(unsigned)rt.size(), 512, smem, h->stream>>>(rec, h->d_rtiles, h->d_graphs, h->d_bins,
-                                                                    nullptr, h->d_status);
-  h->launches++;
-  MB_CUDA(cudaGetLastError());
+  const uint32_t n_rt = (uint32_t)rt.size();
+  {
+    MB_CUDA(cudaFuncSetAttribute(k_mb_count, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMbCountSmem));
+    int per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mb_count, 1024, kMbCountSmem);
+    const unsigned grid = (unsigned)std::min<uint64_t>(n_rt, (uint64_t)num_sms() * std::max(per_sm, 1));
+    k_mb_count<<<grid, 1024, kMbCountSmem, h->stream>>>(rec, h->d_rtiles, n_rt, h->d_graphs, h->d_bins,
+                                                       h->d_status);
+    h->launches++;
+    MB_CUDA(cudaGetLastError());
+  }
   const uint64_t l0 = launch_count();
   MB_CUDA(scan_exclusive_u64(h->d_bins, h->total_bins, h->d_total, h->d_scan_tmp, h->stream));
   h->launches += launch_count() - l0;
   k_mb_bin_off<<<cdiv(h->total_bins + 1, 256), 256, 0, h->stream>>>(h->d_bins, h->total_bins, h->d_total,
                                                                      h->d_bin_off);
-  k_mb_gutter<false><<<(unsigned)rt.size(), 512, smem, h->stream>>>(rec, h->d_rtiles, h->d_graphs, h->d_bins,
-                                                                     h->d_entries, h->d_status);
-  h->launches += 2;
-  MB_CUDA(cudaGetLastError());
+  h->launches++;
+  {
+    MB_CUDA(cudaFuncSetAttribute(k_mb_sort_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMbSortSmem));
+    const unsigned grid = (unsigned)std::min<uint64_t>(n_rt, (uint64_t)num_sms());
+    k_mb_sort_scatter<<<grid, 1024, kMbSortSmem, h->stream>>>(rec, h->d_rtiles, n_rt, h->d_graphs, h->d_bins,
+                                                              h->d_bin_fill, h->d_entries);
+    h->launches++;
+    MB_CUDA(cudaGetLastError());
+  }
   if (h->prof) cudaEventRecord(e1, h->stream);
   // one persistent launch for every (graph, tile)
   MB_CUDA(cudaMemsetAsync(h->d_status + 1, 0, sizeof(uint32_t), h->stream));
-  const size_t ksmem = h->max_tile_bytes + kQueueBytes + (size_t)(h->max_C + 1) * 8;
+  const uint32_t tile_stride = (h->max_tile_bytes + 127) & ~127u;
+  const uint32_t flip_stride = ((h->max_C + 2) & ~1u) * 8;
+  const size_t ksmem = 2 * (size_t)tile_stride + 2 * (size_t)flip_stride + (size_t)(h->threads / 32) * 256;
   MB_CUDA(cudaFuncSetAttribute(k_mb_sketch_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ksmem));
   int per_sm = 1;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mb_sketch_update, (int)h->threads, ksmem);
   const int grid = (int)std::min<uint64_t>(h->total_tiles, (uint64_t)num_sms() * std::max(per_sm, 1));
   k_mb_sketch_update<<<grid, h->threads, ksmem, h->stream>>>(
-      h->d_graphs, h->d_tile_base, h->G, (uint32_t)h->total_tiles, h->d_sk, h->d_entries, h->d_bin_off,
-      h->d_flip, h->max_tile_bytes, h->d_status + 1, h->d_status);
+      h->d_graphs, h->d_tile_graph, (uint32_t)h->total_tiles, h->d_sk, h->d_entries, h->d_bin_off,
+      h->d_flip, tile_stride, flip_stride, h->d_status + 1, h->d_status);
   h->launches++;
   MB_CUDA(cudaGetLastError());
   if (h->prof) {
@@ -896,20 +1098,17 @@ int gz_batch_create(uint32_t num_graphs, const uint32_t *num_vertices, const uin
     if (gd.B > 63) return bail(mb_fail(GZ_ERR_INVALID, "bkt_per_col above 63 is not supported"));
     gd.sketch_words = (gd.C * gd.B + 1) * 3;
   }
-  std::vector<uint32_t> vpt;
-  if (vertices_per_tile) vpt.assign(vertices_per_tile, vertices_per_tile + num_graphs);
-  int rc = layout(h, vpt);
+  if (vertices_per_tile) h->vpt_req.assign(vertices_per_tile, vertices_per_tile + num_graphs);
+  int rc = layout(h, h->vpt_req);
   if (rc != GZ_OK) return bail(rc);
   cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) return bail(mb_fail(GZ_ERR_CUDA, cudaGetErrorString(e)));
-  if ((rc = mb_alloc(&h->d_graphs, num_graphs)) || (rc = mb_alloc(&h->d_tile_base, num_graphs)) ||
+  if ((rc = mb_alloc(&h->d_graphs, num_graphs)) ||
       (rc = mb_alloc(&h->d_gov, h->total_V)) || (rc = mb_alloc(&h->d_sk, h->sk_bytes)) ||
-      (rc = mb_alloc(&h->d_status, 4)) || (rc = mb_alloc(&h->d_bins, h->total_bins)) ||
-      (rc = mb_alloc(&h->d_scan_tmp, scan_tmp_words(h->total_bins))) || (rc = mb_alloc(&h->d_total, 1)) ||
-      (rc = mb_alloc(&h->d_bin_off, h->total_bins + 1)))
+      (rc = mb_alloc(&h->d_status, 4)) || (rc = alloc_bins(h)) || (rc = mb_alloc(&h->d_total, 1)))
     return bail(rc);
   uint64_t nflip = 0;
-  for (auto &gd : h->graphs) nflip += gd.C + 1;
+  for (auto &gd : h->graphs) nflip += (gd.C + 2) & ~1u;
   if ((rc = mb_alloc(&h->d_flip, nflip))) return bail(rc);
   std::vector<uint64_t> flip(nflip);
   std::vector<uint32_t> gov(h->total_V);
@@ -928,6 +1127,44 @@ int gz_batch_create(uint32_t num_graphs, const uint32_t *num_vertices, const uin
   if ((rc = upload_tables(h))) return bail(rc);
   *out = h;
   return GZ_OK;
+}
+
+int gz_batch_set_tuning(gz_batch_t *h, uint32_t threads_per_block, uint32_t ctas_per_sm,
+                        const uint32_t *vertices_per_tile) {
+  if (!h) return mb_fail(GZ_ERR_INVALID, "null handle");
+  const uint32_t threads = threads_per_block ? threads_per_block : 1024;
+  const uint32_t ctas = ctas_per_sm ? ctas_per_sm : 1;
+  if (threads < 64 || threads > 1024 || threads % 32)
+    return mb_fail(GZ_ERR_INVALID, "threads_per_block must be a multiple of 32 in [64, 1024]");
+  if (ctas > 4 || threads * ctas > 2048)
+    return mb_fail(GZ_ERR_INVALID, "ctas_per_sm must be in [1, 4] with threads * ctas <= 2048");
+  if (vertices_per_tile)
+    for (uint32_t g = 0; g < h->G; ++g) {
+      const uint32_t v = vertices_per_tile[g];
+      if (v && (v < 4 || v > 64 || (v & (v - 1))))
+        return mb_fail(GZ_ERR_INVALID, "vertices_per_tile must be 0 or a power of two in [4, 64]");
+    }
+  std::lock_guard<std::mutex> lk(h->mtx);
+  cudaSetDevice(h->device);
+  MB_CUDA(cudaStreamSynchronize(h->stream));
+  const uint32_t old_threads = h->threads, old_ctas = h->ctas_per_sm;
+  const std::vector<uint32_t> old_vpt = h->vpt_req;
+  h->threads = threads;
+  h->ctas_per_sm = ctas;
+  if (vertices_per_tile) h->vpt_req.assign(vertices_per_tile, vertices_per_tile + h->G);
+  else h->vpt_req.clear();
+  int rc = layout(h, h->vpt_req);
+  if (rc != GZ_OK) {  // keep the previous tuning
+    const std::string msg = gz_last_error();
+    h->threads = old_threads;
+    h->ctas_per_sm = old_ctas;
+    h->vpt_req = old_vpt;
+    layout(h, h->vpt_req);
+    gz_internal_set_error(msg);
+    return rc;
+  }
+  MB_TRY(alloc_bins(h));
+  return upload_tables(h);
 }
 
 int gz_batch_destroy(gz_batch_t *h) {

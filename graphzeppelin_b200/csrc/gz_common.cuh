@@ -36,6 +36,9 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
                : "memory");
 }
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
 __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
@@ -134,6 +137,13 @@ __device__ __forceinline__ void parse_record(const uint8_t *s, uint32_t shift, u
 
 // Folds one endpoint update (vertex v, neighbour w) into v's staged sketch: the deterministic
 // bucket always, then in each column the bucket at depth ctz(hash_c(idx) | 1 << B) when < B.
+// Columns are hashed two at a time: the two XXH3 chains are independent, which hides the
+// latency of each other's dependent integer ops.
+__device__ __forceinline__ void xor_bucket(uint32_t *bk, uint32_t lo, uint32_t hi, uint32_t chk) {
+  atomicXor(bk, lo);
+  atomicXor(bk + 1, hi);
+  atomicXor(bk + 2, chk);
+}
 __device__ __forceinline__ void apply_entry(uint2 e, uint32_t *s_sk, uint32_t vmask,
                                             uint32_t sketch_words, const uint64_t *s_flip,
                                             uint64_t flip_chk, uint32_t C, uint32_t B) {
@@ -142,19 +152,45 @@ __device__ __forceinline__ void apply_entry(uint2 e, uint32_t *s_sk, uint32_t vm
   uint32_t *sk = s_sk + (v & vmask) * sketch_words;
   const uint64_t in64 = ((uint64_t)lo << 32) | hi;
   const uint32_t chk = hash_lo32(in64 ^ flip_chk);
-  uint32_t *det = sk + 3 * C * B;
-  atomicXor(det, lo);
-  atomicXor(det + 1, hi);
-  atomicXor(det + 2, chk);
-  for (uint32_t c = 0; c < C; ++c) {
-    const uint32_t d = hash_depth(in64 ^ s_flip[c], B);
-    if (d < B) {
-      uint32_t *bk = sk + 3 * (c * B + d);
-      atomicXor(bk, lo);
-      atomicXor(bk + 1, hi);
-      atomicXor(bk + 2, chk);
-    }
+  xor_bucket(sk + 3 * C * B, lo, hi, chk);
+  uint32_t c = 0;
+  for (; c + 1 < C; c += 2) {
+    const uint32_t d0 = hash_depth(in64 ^ s_flip[c], B);
+    const uint32_t d1 = hash_depth(in64 ^ s_flip[c + 1], B);
+    if (d0 < B) xor_bucket(sk + 3 * (c * B + d0), lo, hi, chk);
+    if (d1 < B) xor_bucket(sk + 3 * ((c + 1) * B + d1), lo, hi, chk);
   }
+  if (c < C) {
+    const uint32_t d = hash_depth(in64 ^ s_flip[c], B);
+    if (d < B) xor_bucket(sk + 3 * (c * B + d), lo, hi, chk);
+  }
+}
+
+
+// Exclusive scan over the 1024 threads of a block (one value per thread).
+__device__ __forceinline__ uint32_t block_scan_1024(uint32_t x, uint32_t *ws /*32*/) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t inc = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(kFull, inc, o);
+    if (lane >= o) inc += y;
+  }
+  if (lane == 31) ws[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = ws[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(kFull, w, o);
+      if (lane >= o) w += y;
+    }
+    ws[lane] = w;
+  }
+  __syncthreads();
+  const uint32_t r = (warp ? ws[warp - 1] : 0) + inc - x;
+  __syncthreads();
+  return r;
 }
 
 

@@ -117,32 +117,6 @@ cudaError_t launch_gutter(const void *in, uint64_t n, GutterGeom g, int G, uint6
   return cudaGetLastError();
 }
 
-// Exclusive scan over the 1024 threads of a block (one value per thread).
-__device__ __forceinline__ uint32_t block_scan_1024(uint32_t x, uint32_t *ws /*32*/) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  uint32_t inc = x;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t y = __shfl_up_sync(kFull, inc, o);
-    if (lane >= o) inc += y;
-  }
-  if (lane == 31) ws[warp] = inc;
-  __syncthreads();
-  if (warp == 0) {
-    uint32_t w = ws[lane];
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(kFull, w, o);
-      if (lane >= o) w += y;
-    }
-    ws[lane] = w;
-  }
-  __syncthreads();
-  const uint32_t r = (warp ? ws[warp - 1] : 0) + inc - x;
-  __syncthreads();
-  return r;
-}
-
 // Sort-scatter pass: each CTA takes `rec_tile` inputs at a time, counting-sorts their endpoint
 // entries by bin in shared memory, reserves one contiguous run per bin in the bin's region of the
 // gutter (one global atomic per bin and tile), and writes the runs out, so consecutive threads

@@ -284,6 +284,13 @@ GZ_API int gz_batch_dump_sketches(gz_batch_t *batch, uint32_t graph, void *host_
 /* Replaces graph g's sketches with V * sketch_bytes bytes in that layout (the sketch part of a
  * write_binary file, as construct_from_serialized_data reads it, src/cc_sketch_alg.cpp:30-64). */
 GZ_API int gz_batch_load_sketches(gz_batch_t *batch, uint32_t graph, const void *host_buf, size_t bytes);
+/* Shape of the batched sketch-update launch: threads per CTA (multiple of 32 in [64, 1024]),
+ * CTAs sharing one SM (1..4, threads * CTAs <= 2048; each CTA stages its tiles in 1/ctas of the
+ * SM's shared memory, so one CTA's bulk copies overlap another's XORs), and vertices per tile per
+ * graph (NULL or 0 = the largest power of two <= 64 that fits). 0 picks the default (1024, 1).
+ * Sketch contents are kept; only the tiling changes. */
+GZ_API int gz_batch_set_tuning(gz_batch_t *batch, uint32_t threads_per_block, uint32_t ctas_per_sm,
+                               const uint32_t *vertices_per_tile);
 GZ_API int gz_batch_set_profiling(gz_batch_t *batch, int enable);
 GZ_API int gz_batch_get_profile(gz_batch_t *batch, gz_profile_t *out);
 

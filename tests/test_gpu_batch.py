@@ -118,7 +118,7 @@ def test_batch_device_records_and_tiles(gz):
     import torch
     Vs, sts = _mixed_streams()
     seeds = [9 * i + 1 for i in range(len(Vs))]
-    vpt = [4, 4, 8, 16, 32, 4, 32, 8, 64]
+    vpt = [4, 4, 8, 16, 16, 4, 16, 8, 32]
     raw = np.concatenate([s.view(np.uint8).reshape(-1) for s in sts])
     off = np.concatenate([[0], np.cumsum([len(s) for s in sts])]).astype(np.uint64)
     dev = torch.zeros(raw.size + 16, dtype=torch.uint8, device="cuda")
@@ -190,3 +190,27 @@ def test_batch_many_graphs(gz):
         for g in range(G):
             h2.update(res2.labels[g].tobytes())
         assert h.digest() == h2.digest() and (res.rounds == res2.rounds).all()
+
+
+@pytest.mark.parametrize("threads,ctas", [(512, 2), (256, 4), (1024, 1), (384, 1)])
+def test_batch_tuning_keeps_results(gz, threads, ctas):
+    """Every launch shape and tile choice gives the same bytes; retuning keeps the sketches."""
+    Vs, sts = _mixed_streams()
+    seeds = [5 * i + 2 for i in range(len(Vs))]
+    with gz.CCSketchBatch(Vs, seeds) as b:
+        half = [s[: len(s) // 2] for s in sts]
+        b.ingest(half)
+        b.set_tuning(threads, ctas)
+        b.ingest([s[len(s) // 2:] for s in sts])
+        res = b.connected_components()
+        for g, V in enumerate(Vs):
+            _check_graph(gz, b, res, g, V, seeds[g], sts[g])
+        with pytest.raises(gz.GZError):
+            b.set_tuning(1024, 3)
+
+
+def test_batch_rejects_oversized_tile(gz):
+    with gz.CCSketchBatch([1 << 16, 100], [1, 2]) as b:
+        with pytest.raises(gz.GZError):
+            b.set_tuning(1024, 1, [64, 4])
+        assert b.params[0].vertices_per_tile <= 16
