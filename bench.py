@@ -482,6 +482,13 @@ def run_many_graphs(args):
 
     # --- batched engine ---
     b = gz.CCSketchBatch(Vs, seeds)
+    tune = None
+    if not args.no_autotune:
+        t0 = time.perf_counter()
+        chosen = b.autotune(int(round(2 * n / max(1, int(Vs.sum())))))
+        hist = {int(v): int(c) for v, c in zip(*np.unique(chosen, return_counts=True))}
+        tune = {"seconds": time.perf_counter() - t0, "vertices_per_tile_hist": hist}
+        log(f"[many] autotune {tune}")
 
     def batch_step():
         b.clear()
@@ -546,6 +553,7 @@ def run_many_graphs(args):
                  "note": "pinned host records -> gz_batch_ingest -> "
                          "gz_batch_connected_components with labels; wall clock, max of 3"}
                 if e2e_ms else None),
+        "autotune": tune,
         "components_total": int(res.num_cc.sum()),
         "clocks": clocks,
         "gpu_launches": int(prof["kernel_launches"]),
@@ -565,6 +573,8 @@ def main():
     ap.add_argument("--workload", default="dense", choices=["dense", "many_graphs"],
                     help="dense: one V=2^17 graph (the headline); many_graphs: 512 uneven graphs")
     ap.add_argument("--graphs", type=int, default=0, help="graphs of the many_graphs workload")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="many_graphs: keep the default tiling instead of running the autotuner")
     ap.add_argument("--no-plain", action="store_true",
                     help="many_graphs: skip the graph-by-graph plain-path comparison")
     args = ap.parse_args()

@@ -95,6 +95,7 @@ SIGNATURES = [
     ("gz_batch_dump_sketches", _i, [_H, _u32, _P, _sz]),
     ("gz_batch_load_sketches", _i, [_H, _u32, _P, _sz]),
     ("gz_batch_set_tuning", _i, [_H, _u32, _u32, _P]),
+    ("gz_batch_autotune", _i, [_H, _u32, _P]),
     ("gz_batch_set_profiling", _i, [_H, _i]),
     ("gz_batch_get_profile", _i, [_H, ctypes.POINTER(gz_profile_t)]),
 ]

@@ -147,6 +147,13 @@ class CCSketchBatch:
                                             _ptr(vpt) if vpt is not None else None))
         self._refresh_params()
 
+    def autotune(self, records_per_vertex: int = 0) -> np.ndarray:
+        """Run the autotuner (gz_batch_autotune); returns the vertices per tile chosen per graph."""
+        out = np.zeros(self.num_graphs, np.uint32)
+        _check(self.lib.gz_batch_autotune(self._h, records_per_vertex, _ptr(out)))
+        self._refresh_params()
+        return out
+
     def _refresh_params(self):
         self.params = []
         for i in range(self.num_graphs):

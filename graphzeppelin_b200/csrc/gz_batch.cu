@@ -612,6 +612,39 @@ void mb_free(T *&p) {
   p = nullptr;
 }
 
+// ---- autotuning trials -----------------------------------------------------------------------
+__device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+
+// Trial records: record r of graph g (records off[g] .. off[g+1]) joins two distinct vertices
+// drawn uniformly from [0, nv[g]) by a counter-based hash.
+__global__ void k_trial_records(uint8_t *out, const uint64_t *off, const uint32_t *nv, uint32_t G,
+                                uint64_t seed) {
+  const uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (r >= off[G]) return;
+  uint32_t lo = 0, hi = G;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (off[mid] <= r) lo = mid;
+    else hi = mid;
+  }
+  const uint32_t n = nv[lo];
+  const uint64_t h = splitmix64(seed ^ (r * 0xD1B54A32D192ED03ull));
+  const uint32_t u = (uint32_t)(((h & 0xffffffffull) * n) >> 32);
+  uint32_t v = (uint32_t)(((h >> 32) * (n - 1)) >> 32);
+  if (v >= u) ++v;
+  uint8_t *p = out + 9 * r;
+  p[0] = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    p[1 + k] = (uint8_t)(u >> (8 * k));
+    p[5 + k] = (uint8_t)(v >> (8 * k));
+  }
+}
 
 }  // namespace
 }  // namespace gz
@@ -1269,6 +1302,115 @@ int gz_batch_set_profiling(gz_batch_t *h, int enable) {
   h->prof = enable != 0;
   h->prof_gutter_ms = h->prof_sketch_ms = h->prof_query_ms = 0;
   h->prof_rounds = 0;
+  return GZ_OK;
+}
+
+// Picks, per sketch-size class (graphs with the same columns and buckets per column), the
+// vertices per tile of the batched sketch update -- i.e. the buckets each CTA stages and the warps
+// per vertex -- and the CTA shape, by timing trial ingests on a scratch batch holding one
+// representative graph per class. The caller's sketches are not touched.
+int gz_batch_autotune(gz_batch_t *h, uint32_t records_per_vertex, uint32_t *vpt_out) {
+  if (!h) return mb_fail(GZ_ERR_INVALID, "null handle");
+  const uint32_t rpv = records_per_vertex ? records_per_vertex : 64;
+  cudaSetDevice(h->device);
+  std::vector<std::pair<uint32_t, uint32_t>> keys;  // (C, B) per class
+  std::vector<uint32_t> rep_v, cls_of(h->G);
+  for (uint32_t g = 0; g < h->G; ++g) {
+    const auto key = std::make_pair(h->graphs[g].C, h->graphs[g].B);
+    uint32_t k = 0;
+    while (k < keys.size() && keys[k] != key) ++k;
+    if (k == keys.size()) {
+      keys.push_back(key);
+      rep_v.push_back(0);
+    }
+    rep_v[k] = std::max(rep_v[k], h->graphs[g].V);
+    cls_of[g] = k;
+  }
+  const uint32_t K = (uint32_t)keys.size();
+  // scratch graphs: copies of each class's largest graph, enough (>= 16384 vertices, i.e. >= 4
+  // tiles per SM at 16 vertices per tile) that a class's trial fills the GPU like the real batch
+  std::vector<uint32_t> sv, first(K + 1, 0);
+  std::vector<uint64_t> seeds;
+  for (uint32_t k = 0; k < K; ++k) {
+    const uint32_t copies = std::max<uint32_t>(1, std::min<uint32_t>(64, (16384 + rep_v[k] - 1) / rep_v[k]));
+    first[k] = (uint32_t)sv.size();
+    for (uint32_t c = 0; c < copies; ++c) {
+      sv.push_back(rep_v[k]);
+      seeds.push_back(0x5EEDull + sv.size());
+    }
+  }
+  first[K] = (uint32_t)sv.size();
+  const uint32_t S = (uint32_t)sv.size();
+  std::vector<uint64_t> off(S + 1, 0);
+  for (uint32_t g = 0; g < S; ++g)
+    off[g + 1] = off[g] + std::min<uint64_t>(std::max<uint64_t>(1, (uint64_t)rpv * sv[g] / 2), 1ull << 22);
+  gz_batch_t *sc = nullptr;
+  MB_TRY(gz_batch_create(S, sv.data(), seeds.data(), h->factor, nullptr, &sc));
+  struct Guard {
+    gz_batch_t *b;
+    uint8_t *rec = nullptr;
+    uint64_t *off = nullptr;
+    uint32_t *nv = nullptr;
+    ~Guard() {
+      if (rec) cudaFree(rec);
+      if (off) cudaFree(off);
+      if (nv) cudaFree(nv);
+      gz_batch_destroy(b);
+    }
+  } guard{sc};
+  MB_TRY(mb_alloc(&guard.rec, off[S] * 9));
+  MB_TRY(mb_alloc(&guard.off, S + 1));
+  MB_TRY(mb_alloc(&guard.nv, S));
+  MB_CUDA(cudaMemcpyAsync(guard.off, off.data(), 8 * (S + 1), cudaMemcpyHostToDevice, sc->stream));
+  MB_CUDA(cudaMemcpyAsync(guard.nv, sv.data(), 4 * S, cudaMemcpyHostToDevice, sc->stream));
+  k_trial_records<<<cdiv(off[S], 256), 256, 0, sc->stream>>>(guard.rec, guard.off, guard.nv, S, 0xA070ull);
+  MB_CUDA(cudaGetLastError());
+  MB_CUDA(cudaStreamSynchronize(sc->stream));
+
+  struct Shape {
+    uint32_t threads, ctas;
+  };
+  const Shape shapes[] = {{1024, 1}, {768, 1}, {512, 2}};
+  double best_total = 1e300;
+  Shape best_shape = shapes[0];
+  std::vector<uint32_t> best_vpt(K, 0);
+  for (const Shape &sh : shapes) {
+    double total = 0;
+    std::vector<uint32_t> pick(K, 0);
+    bool feasible = true;
+    for (uint32_t k = 0; k < K && feasible; ++k) {
+      std::vector<uint64_t> o(S + 1);  // only class k's records
+      for (uint32_t g = 0; g <= S; ++g) o[g] = std::min(std::max(off[g], off[first[k]]), off[first[k + 1]]);
+      double best = 1e300;
+      for (uint32_t vpt = 4; vpt <= 64; vpt <<= 1) {
+        std::vector<uint32_t> vv(S, 0);
+        for (uint32_t g = first[k]; g < first[k + 1]; ++g) vv[g] = vpt;
+        if (gz_batch_set_tuning(sc, sh.threads, sh.ctas, vv.data()) != GZ_OK) continue;
+        double t = 1e300;
+        for (int rep = 0; rep < 3; ++rep) {
+          gz_batch_set_profiling(sc, 1);
+          MB_TRY(gz_batch_ingest_device(sc, guard.rec, o.data()));
+          if (rep) t = std::min(t, sc->prof_sketch_ms);
+        }
+        if (t < best) {
+          best = t;
+          pick[k] = vpt;
+        }
+      }
+      if (!pick[k]) feasible = false;
+      total += best;
+    }
+    if (feasible && total < best_total) {
+      best_total = total;
+      best_shape = sh;
+      best_vpt = pick;
+    }
+  }
+  gz_batch_set_profiling(sc, 0);
+  std::vector<uint32_t> vpt(h->G);
+  for (uint32_t g = 0; g < h->G; ++g) vpt[g] = best_vpt[cls_of[g]];
+  MB_TRY(gz_batch_set_tuning(h, best_shape.threads, best_shape.ctas, vpt.data()));
+  if (vpt_out) std::copy(vpt.begin(), vpt.end(), vpt_out);
   return GZ_OK;
 }
 

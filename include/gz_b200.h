@@ -291,6 +291,12 @@ GZ_API int gz_batch_load_sketches(gz_batch_t *batch, uint32_t graph, const void 
  * Sketch contents are kept; only the tiling changes. */
 GZ_API int gz_batch_set_tuning(gz_batch_t *batch, uint32_t threads_per_block, uint32_t ctas_per_sm,
                                const uint32_t *vertices_per_tile);
+/* Autotuner: times trial ingests (records_per_vertex random edge records per vertex, 0 = 64) on
+ * a scratch batch with one representative graph per sketch-size class (same columns and buckets
+ * per column) and applies the fastest CTA shape and per-class vertices per tile to this batch.
+ * vertices_per_tile_out (NULL or num_graphs entries) gets the choice. The sketches are kept. */
+GZ_API int gz_batch_autotune(gz_batch_t *batch, uint32_t records_per_vertex,
+                             uint32_t *vertices_per_tile_out);
 GZ_API int gz_batch_set_profiling(gz_batch_t *batch, int enable);
 GZ_API int gz_batch_get_profile(gz_batch_t *batch, gz_profile_t *out);
 

@@ -214,3 +214,27 @@ def test_batch_rejects_oversized_tile(gz):
         with pytest.raises(gz.GZError):
             b.set_tuning(1024, 1, [64, 4])
         assert b.params[0].vertices_per_tile <= 16
+
+
+def test_batch_autotune_keeps_sketches_and_results(gz):
+    """The autotuner retiles the batch (one vertices-per-tile per size class) without touching
+    the sketches; ingest after tuning still matches the single-graph path."""
+    Vs, sts = _mixed_streams()
+    seeds = [3 * i + 11 for i in range(len(Vs))]
+    with gz.CCSketchBatch(Vs, seeds) as b:
+        half = [s[: len(s) // 2] for s in sts]
+        b.ingest(half)
+        before = [b.dump_sketches(g).tobytes() for g in range(len(Vs))]
+        vpt = b.autotune(32)
+        assert all(v in (4, 8, 16, 32, 64) for v in vpt)
+        assert [b.dump_sketches(g).tobytes() for g in range(len(Vs))] == before
+        classes = {}
+        for g in range(len(Vs)):
+            p = b.params[g]
+            assert p.vertices_per_tile == vpt[g]
+            classes.setdefault((p.num_columns, p.bkt_per_col), set()).add(int(vpt[g]))
+        assert all(len(v) == 1 for v in classes.values())
+        b.ingest([s[len(s) // 2:] for s in sts])
+        res = b.connected_components()
+        for g, V in enumerate(Vs):
+            _check_graph(gz, b, res, g, V, seeds[g], sts[g])
