@@ -23,6 +23,7 @@ GZ_ERR_IO = 7
 GZ_ERR_TIMEOUT = 8
 GZ_ERR_BAD_SAMPLE = 9
 GZ_ERR_NO_DEVICE = 10
+GZ_ERR_BUDGET = 11
 
 
 class gz_params_t(ctypes.Structure):
@@ -97,6 +98,17 @@ SIGNATURES = [
     ("gz_batch_set_tuning", _i, [_H, _u32, _u32, _P]),
     ("gz_batch_autotune", _i, [_H, _u32, _P]),
     ("gz_batch_set_profiling", _i, [_H, _i]),
+    ("gz_server_tenant_bytes", _i, [_u32, _d, ctypes.POINTER(_u64)]),
+    ("gz_server_create", _i, [_u64, _u64, _d, ctypes.POINTER(_H)]),
+    ("gz_server_destroy", _i, [_H]),
+    ("gz_server_admit", _i, [_H, _u32, _u64, ctypes.POINTER(_u32)]),
+    ("gz_server_evict", _i, [_H, _u32]),
+    ("gz_server_usage", _i, [_H, ctypes.POINTER(_u64), ctypes.POINTER(_u64), ctypes.POINTER(_u32)]),
+    ("gz_server_get_params", _i, [_H, _u32, ctypes.POINTER(gz_params_t)]),
+    ("gz_server_ingest", _i, [_H, _u32, _P, _P, _P]),
+    ("gz_server_query_submit", _i, [_H, _u32, _P, ctypes.POINTER(_u64)]),
+    ("gz_server_query_wait", _i, [_H, _u64, _P, _P, _P, _P]),
+    ("gz_server_dump_sketches", _i, [_H, _u32, _P, _sz]),
     ("gz_batch_get_profile", _i, [_H, ctypes.POINTER(gz_profile_t)]),
 ]
 

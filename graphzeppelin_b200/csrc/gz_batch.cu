@@ -11,9 +11,14 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <condition_variable>
 #include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/gz_b200.h"
@@ -612,6 +617,15 @@ void mb_free(T *&p) {
   p = nullptr;
 }
 
+// graph g owns global tiles [tile_base, +ntiles) and global vertices [vbase, +V)
+__global__ void k_mb_fill_tables(const GraphDesc *graphs, uint32_t G, uint32_t *tile_graph, uint32_t *gov) {
+  for (uint32_t g = blockIdx.x; g < G; g += gridDim.x) {
+    const GraphDesc gd = graphs[g];
+    for (uint32_t i = threadIdx.x; i < gd.ntiles; i += blockDim.x) tile_graph[gd.tile_base + i] = g;
+    for (uint32_t i = threadIdx.x; i < gd.V; i += blockDim.x) gov[gd.vbase + i] = g;
+  }
+}
+
 // ---- autotuning trials -----------------------------------------------------------------------
 __device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
   x += 0x9E3779B97F4A7C15ull;
@@ -662,6 +676,11 @@ struct gz_batch {
   uint32_t max_B = 0, max_C = 0, max_tile_bytes = 0;
   uint32_t threads = 1024, ctas_per_sm = 1;  // sketch-update CTA shape
   std::vector<uint32_t> vpt_req;             // requested vertices per tile (0 = default)
+  bool own_storage = true;                   // d_sk / d_flip allocated (and freed) by this handle
+  // capacities of the device tables (grown, never shrunk)
+  uint64_t cap_graphs = 0, cap_tiles = 0, cap_V = 0, cap_bins = 0;
+  uint64_t cap_bv_V = 0, cap_bv_G = 0, cap_acc = 0;
+  gz::MBBufs captured{};  // buffers the captured Boruvka round was recorded with
   GraphDesc *d_graphs = nullptr;
   uint32_t *d_tile_graph = nullptr, *d_gov = nullptr;  // graph of each global tile / vertex
   uint8_t *d_sk = nullptr;
@@ -730,8 +749,10 @@ void batch_destroy(gz_batch *h) {
   mb_free(h->d_graphs);
   mb_free(h->d_tile_graph);
   mb_free(h->d_gov);
-  mb_free(h->d_sk);
-  mb_free(h->d_flip);
+  if (h->own_storage) {
+    mb_free(h->d_sk);
+    mb_free(h->d_flip);
+  }
   mb_free(h->d_status);
   if (h->h_small) cudaFreeHost(h->h_small);
   mb_free(h->d_entries);
@@ -774,92 +795,121 @@ size_t cta_smem_budget(const gz_batch *h) {
   return std::min<size_t>((size_t)optin, share);
 }
 
-// Tile and bin geometry of every graph. A requested vertices-per-tile (vpt_req[g] != 0) is
-// used as given; otherwise the largest power of two <= 64 whose tile fits the CTA's shared memory
-// (a batch has enough tiles to fill the GPU, and bigger tiles spread the shared-memory atomics
-// over more buckets).
-int layout(gz_batch *h, const std::vector<uint32_t> &vpt_req) {
+// Bytes of one tile buffer when the launch's graphs have at most max_C columns: two buffers, two
+// padded hash-constant arrays, the consumer warps' queues and static shared memory share the CTA.
+size_t tile_budget(const gz_batch *h, uint32_t max_C) {
   const size_t cta_smem = cta_smem_budget(h);
-  uint64_t sk_off = 0, vbase = 0, bin_base = 0, tile_base = 0, flip_off = 0;
+  const size_t fixed = 256 + (size_t)(h->threads / 32) * 256 + 2 * (size_t)((max_C + 2) & ~1u) * 8;
+  if (cta_smem <= fixed) return 0;
+  return ((cta_smem - fixed) / 2) & ~(size_t)127;
+}
+
+// Tile and bin geometry of one graph. A requested vertices-per-tile (vpt != 0) is used as given;
+// otherwise the largest power of two <= 64 whose tile fits `budget` bytes (a batch has enough
+// tiles to fill the GPU, and bigger tiles spread the shared-memory atomics over more buckets).
+int choose_tiles(GraphDesc &gd, uint32_t vpt, size_t budget) {
+  const uint64_t sketch_bytes = (uint64_t)gd.sketch_words * 4;
+  uint32_t shift = 2;
+  if (vpt) {
+    shift = (uint32_t)__builtin_ctz(vpt);
+  } else {
+    while (shift < 6 && (sketch_bytes << (shift + 1)) <= budget) ++shift;
+  }
+  if ((sketch_bytes << shift) > budget) return mb_fail(GZ_ERR_INVALID, "sketch too large for a tile");
+  uint32_t bshift = shift;
+  while (((gd.V + (1u << bshift) - 1) >> bshift) > kMbBinTarget && (1u << (bshift - shift)) < 16) ++bshift;
+  while (((gd.V + (1u << bshift) - 1) >> bshift) > kMbBinsMax && (1u << (bshift - shift)) < kMbTilesPerBinMax)
+    ++bshift;
+  if (((gd.V + (1u << bshift) - 1) >> bshift) > kMbBinsMax)
+    return mb_fail(GZ_ERR_INVALID, "a graph with V=" + std::to_string(gd.V) +
+                                       " is too large for a batch: use a single-graph handle");
+  gd.tile_shift = shift;
+  gd.bin_shift = bshift;
+  gd.ntiles = (gd.V + (1u << shift) - 1) >> shift;
+  gd.nbins = (gd.V + (1u << bshift) - 1) >> bshift;
+  return GZ_OK;
+}
+
+// Device bytes of one graph's sketches: V rounded up to 64 (any tile stays inside), 256-aligned.
+uint64_t graph_sketch_bytes(const GraphDesc &gd) {
+  const uint64_t v_pad = ((uint64_t)gd.V + 63) & ~63ull;
+  return (v_pad * gd.sketch_words * 4 + 255) & ~255ull;
+}
+
+template <class T>
+int grow(T **p, uint64_t &cap, uint64_t need) {
+  if (*p && cap >= need) return GZ_OK;
+  mb_free(*p);
+  cap = 0;
+  MB_TRY(mb_alloc(p, std::max<uint64_t>(need, 1)));
+  cap = need;
+  return GZ_OK;
+}
+
+// h->graphs hold tiling, sketch and hash-constant offsets: number their tiles, bins and vertices
+// globally, size the device tables for them and upload them.
+int finalize_graphs(gz_batch *h) {
+  uint64_t vbase = 0, bin_base = 0, tile_base = 0;
+  h->G = (uint32_t)h->graphs.size();
   h->max_tile_bytes = 0;
   h->max_B = h->max_C = 0;
-  for (const GraphDesc &gd : h->graphs) {
-    h->max_B = std::max(h->max_B, gd.B);
-    h->max_C = std::max(h->max_C, gd.C);
-  }
-  // one launch serves every graph: its shared memory holds the largest tile and the most flips
-  const size_t queue = (size_t)(h->threads / 32) * 256;
-  // static shared memory (256), consumer queues, two padded flip arrays
-  const size_t fixed = 256 + queue + 2 * (size_t)((h->max_C + 2) & ~1u) * 8;
-  if (cta_smem <= fixed) return mb_fail(GZ_ERR_INVALID, "no shared memory left for a tile");
-  const size_t budget = ((cta_smem - fixed) / 2) & ~(size_t)127;  // two tile buffers
-  for (uint32_t g = 0; g < h->G; ++g) {
-    GraphDesc &gd = h->graphs[g];
-    const uint64_t sketch_bytes = (uint64_t)gd.sketch_words * 4;
-    uint32_t shift = 2;
-    if (!vpt_req.empty() && vpt_req[g]) {
-      shift = (uint32_t)__builtin_ctz(vpt_req[g]);
-    } else {
-      while (shift < 6 && (sketch_bytes << (shift + 1)) <= budget) ++shift;
-    }
-    if ((sketch_bytes << shift) > budget) return mb_fail(GZ_ERR_INVALID, "sketch too large for a tile");
-    uint32_t bshift = shift;
-    while (((gd.V + (1u << bshift) - 1) >> bshift) > kMbBinTarget && (1u << (bshift - shift)) < 16) ++bshift;
-    while (((gd.V + (1u << bshift) - 1) >> bshift) > kMbBinsMax && (1u << (bshift - shift)) < kMbTilesPerBinMax)
-      ++bshift;
-    if (((gd.V + (1u << bshift) - 1) >> bshift) > kMbBinsMax)
-      return mb_fail(GZ_ERR_INVALID, "graph " + std::to_string(g) + " (V=" + std::to_string(gd.V) +
-                                         ") is too large for a batch: use a single-graph handle");
-    gd.tile_shift = shift;
-    gd.bin_shift = bshift;
-    gd.ntiles = (gd.V + (1u << shift) - 1) >> shift;
-    gd.nbins = (gd.V + (1u << bshift) - 1) >> bshift;
-    gd.sk_off = sk_off;
+  for (GraphDesc &gd : h->graphs) {
     gd.vbase = (uint32_t)vbase;
     gd.bin_base = (uint32_t)bin_base;
     gd.tile_base = (uint32_t)tile_base;
-    gd.flip_off = (uint32_t)flip_off;
-    const uint64_t v_pad = ((uint64_t)gd.V + 63) & ~63ull;
-    sk_off += (v_pad * sketch_bytes + 255) & ~255ull;
     vbase += gd.V;
     bin_base += gd.nbins;
     tile_base += gd.ntiles;
-    flip_off += (gd.C + 2) & ~1u;  // even: every graph's constants start 16-byte aligned
-    h->max_tile_bytes = std::max<uint32_t>(h->max_tile_bytes, (uint32_t)(sketch_bytes << shift));
+    h->max_B = std::max(h->max_B, gd.B);
+    h->max_C = std::max(h->max_C, gd.C);
+    h->max_tile_bytes = std::max<uint32_t>(h->max_tile_bytes, (gd.sketch_words * 4) << gd.tile_shift);
   }
   if (vbase > 0xFFFFFFF0ull || bin_base > 0xFFFFFFF0ull || tile_base > 0xFFFFFFF0ull)
     return mb_fail(GZ_ERR_INVALID, "batch too large for 32-bit global vertex ids");
-  h->sk_bytes = sk_off;
   h->total_V = vbase;
   h->total_bins = bin_base;
   h->total_tiles = tile_base;
-  return GZ_OK;
-}
-
-// gutter-bin arrays sized for the current layout
-int alloc_bins(gz_batch *h) {
-  mb_free(h->d_bins);
-  mb_free(h->d_bin_fill);
-  mb_free(h->d_scan_tmp);
-  mb_free(h->d_bin_off);
-  MB_TRY(mb_alloc(&h->d_bins, h->total_bins));
-  MB_TRY(mb_alloc(&h->d_bin_fill, h->total_bins));
-  MB_TRY(mb_alloc(&h->d_scan_tmp, scan_tmp_words(h->total_bins)));
-  MB_TRY(mb_alloc(&h->d_bin_off, h->total_bins + 1));
-  return GZ_OK;
-}
-
-int upload_tables(gz_batch *h) {
-  std::vector<uint32_t> tg(h->total_tiles);
-  for (uint32_t g = 0; g < h->G; ++g) {
-    const GraphDesc &gd = h->graphs[g];
-    std::fill(tg.begin() + gd.tile_base, tg.begin() + gd.tile_base + gd.ntiles, g);
+  if (h->G == 0) return GZ_OK;
+  MB_TRY(grow(&h->d_graphs, h->cap_graphs, h->G));
+  MB_TRY(grow(&h->d_tile_graph, h->cap_tiles, h->total_tiles));
+  MB_TRY(grow(&h->d_gov, h->cap_V, h->total_V));
+  if (!h->d_bins || h->cap_bins < h->total_bins) {
+    mb_free(h->d_bins);
+    mb_free(h->d_bin_fill);
+    mb_free(h->d_scan_tmp);
+    mb_free(h->d_bin_off);
+    h->cap_bins = 0;
+    MB_TRY(mb_alloc(&h->d_bins, h->total_bins));
+    MB_TRY(mb_alloc(&h->d_bin_fill, h->total_bins));
+    MB_TRY(mb_alloc(&h->d_scan_tmp, scan_tmp_words(h->total_bins)));
+    MB_TRY(mb_alloc(&h->d_bin_off, h->total_bins + 1));
+    h->cap_bins = h->total_bins;
   }
-  mb_free(h->d_tile_graph);
-  MB_TRY(mb_alloc(&h->d_tile_graph, h->total_tiles));
   MB_CUDA(cudaMemcpyAsync(h->d_graphs, h->graphs.data(), sizeof(GraphDesc) * h->G, cudaMemcpyHostToDevice, h->stream));
-  MB_CUDA(cudaMemcpyAsync(h->d_tile_graph, tg.data(), sizeof(uint32_t) * tg.size(), cudaMemcpyHostToDevice, h->stream));
-  MB_CUDA(cudaStreamSynchronize(h->stream));
+  k_mb_fill_tables<<<std::min<uint32_t>(h->G, 4096), 256, 0, h->stream>>>(h->d_graphs, h->G, h->d_tile_graph, h->d_gov);
+  h->launches++;
+  MB_CUDA(cudaGetLastError());
+  MB_CUDA(cudaStreamSynchronize(h->stream));  // the host descriptor vector may change next call
+  return GZ_OK;
+}
+
+// Layout of a batch that owns its storage: every graph's tiling, then its sketches and hash
+// constants back to back.
+int layout(gz_batch *h, const std::vector<uint32_t> &vpt_req) {
+  uint32_t max_C = 0;
+  for (const GraphDesc &gd : h->graphs) max_C = std::max(max_C, gd.C);
+  const size_t budget = tile_budget(h, max_C);
+  if (!budget) return mb_fail(GZ_ERR_INVALID, "no shared memory left for a tile");
+  uint64_t sk_off = 0, flip_off = 0;
+  for (uint32_t g = 0; g < h->graphs.size(); ++g) {
+    GraphDesc &gd = h->graphs[g];
+    MB_TRY(choose_tiles(gd, vpt_req.empty() ? 0 : vpt_req[g], budget));
+    gd.sk_off = sk_off;
+    gd.flip_off = (uint32_t)flip_off;
+    sk_off += graph_sketch_bytes(gd);
+    flip_off += (gd.C + 2) & ~1u;  // even: every graph's constants start 16-byte aligned
+  }
+  h->sk_bytes = sk_off;
   return GZ_OK;
 }
 
@@ -970,22 +1020,41 @@ int batch_ingest(gz_batch *h, const void *d_rec, const uint64_t *off) {
 }
 
 int ensure_boruvka(gz_batch *h) {
-  const size_t V = h->total_V;
-  MB_TRY(mb_alloc(&h->d_parent, V));
-  MB_TRY(mb_alloc(&h->d_label, V));
-  MB_TRY(mb_alloc(&h->d_cnt, V));
-  MB_TRY(mb_alloc(&h->d_fill, V));
-  MB_TRY(mb_alloc(&h->d_packed, V));
+  const uint64_t V = h->total_V, G = h->G;
+  if (!h->d_parent || h->cap_bv_V < V) {
+    mb_free(h->d_parent);
+    mb_free(h->d_label);
+    mb_free(h->d_cnt);
+    mb_free(h->d_fill);
+    mb_free(h->d_packed);
+    mb_free(h->d_vscan_tmp);
+    mb_free(h->d_order);
+    mb_free(h->d_comp_start);
+    h->cap_bv_V = 0;
+    MB_TRY(mb_alloc(&h->d_parent, V));
+    MB_TRY(mb_alloc(&h->d_label, V));
+    MB_TRY(mb_alloc(&h->d_cnt, V));
+    MB_TRY(mb_alloc(&h->d_fill, V));
+    MB_TRY(mb_alloc(&h->d_packed, V));
+    MB_TRY(mb_alloc(&h->d_vscan_tmp, scan_tmp_words(V)));
+    MB_TRY(mb_alloc(&h->d_order, V));
+    MB_TRY(mb_alloc(&h->d_comp_start, V + 1));
+    h->cap_bv_V = V;
+  }
+  MB_TRY(grow(&h->d_acc, h->cap_acc, V * (uint64_t)(h->max_B + 1) * 3));
+  if (!h->d_active || h->cap_bv_G < G) {
+    mb_free(h->d_active);
+    mb_free(h->d_modified);
+    mb_free(h->d_ncc);
+    h->cap_bv_G = 0;
+    MB_TRY(mb_alloc(&h->d_active, G));
+    MB_TRY(mb_alloc(&h->d_modified, G));
+    MB_TRY(mb_alloc(&h->d_ncc, G));
+    h->cap_bv_G = G;
+  }
   MB_TRY(mb_alloc(&h->d_vscan_total, 1));
-  MB_TRY(mb_alloc(&h->d_vscan_tmp, scan_tmp_words(V)));
-  MB_TRY(mb_alloc(&h->d_order, V));
-  MB_TRY(mb_alloc(&h->d_comp_start, V + 1));
   MB_TRY(mb_alloc(&h->d_ncomp, 1));
-  MB_TRY(mb_alloc(&h->d_acc, V * (size_t)(h->max_B + 1) * 3));
-  MB_TRY(mb_alloc(&h->d_active, h->G));
-  MB_TRY(mb_alloc(&h->d_modified, h->G));
   MB_TRY(mb_alloc(&h->d_round, 1));
-  MB_TRY(mb_alloc(&h->d_ncc, h->G));
   return GZ_OK;
 }
 
@@ -1029,8 +1098,15 @@ int batch_query(gz_batch *h, uint32_t *labels_out) {
   k_mb_round0<<<std::min<unsigned>(cdiv(V * 32, 256), num_sms() * 16), 256, 0, h->stream>>>(b);
   h->launches += 2;
   MB_CUDA(cudaGetLastError());
+  const MBBufs cur = h->bufs();
+  if (h->round_exec && std::memcmp(&cur, &h->captured, sizeof(MBBufs)) != 0) {
+    cudaGraphExecDestroy(h->round_exec);  // the graphs or buffers changed since the capture
+    cudaGraphDestroy(h->round_graph);
+    h->round_exec = nullptr;
+    h->round_graph = nullptr;
+  }
   if (!h->round_exec) {
-    // capture the round once: it reads the round number and the active flags from device memory
+    // capture the round: it reads the round number and the active flags from device memory
     cudaStream_t cs = nullptr;
     MB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
     MB_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
@@ -1051,6 +1127,7 @@ int batch_query(gz_batch *h, uint32_t *labels_out) {
       cudaGraphNodeType t;
       if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) h->round_kernels++;
     }
+    h->captured = cur;
   }
   uint32_t round = 0;
   for (;;) {
@@ -1136,28 +1213,24 @@ int gz_batch_create(uint32_t num_graphs, const uint32_t *num_vertices, const uin
   if (rc != GZ_OK) return bail(rc);
   cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) return bail(mb_fail(GZ_ERR_CUDA, cudaGetErrorString(e)));
-  if ((rc = mb_alloc(&h->d_graphs, num_graphs)) ||
-      (rc = mb_alloc(&h->d_gov, h->total_V)) || (rc = mb_alloc(&h->d_sk, h->sk_bytes)) ||
-      (rc = mb_alloc(&h->d_status, 4)) || (rc = alloc_bins(h)) || (rc = mb_alloc(&h->d_total, 1)))
+  if ((rc = mb_alloc(&h->d_sk, h->sk_bytes)) || (rc = mb_alloc(&h->d_status, 4)) ||
+      (rc = mb_alloc(&h->d_total, 1)))
     return bail(rc);
   uint64_t nflip = 0;
   for (auto &gd : h->graphs) nflip += (gd.C + 2) & ~1u;
   if ((rc = mb_alloc(&h->d_flip, nflip))) return bail(rc);
   std::vector<uint64_t> flip(nflip);
-  std::vector<uint32_t> gov(h->total_V);
   for (uint32_t g = 0; g < num_graphs; ++g) {
     const GraphDesc &gd = h->graphs[g];
     for (uint32_t c = 0; c < gd.C; ++c) flip[gd.flip_off + c] = xxh3_flip(seeds[g] + 5ull * c);
     flip[gd.flip_off + gd.C] = xxh3_flip(seeds[g]);
-    std::fill(gov.begin() + gd.vbase, gov.begin() + gd.vbase + gd.V, g);
   }
   if (cudaMallocHost(&h->h_small, 64) != cudaSuccess) return bail(mb_fail(GZ_ERR_NOMEM, "cudaMallocHost"));
   e = cudaMemcpyAsync(h->d_flip, flip.data(), nflip * 8, cudaMemcpyHostToDevice, h->stream);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(h->d_gov, gov.data(), gov.size() * 4, cudaMemcpyHostToDevice, h->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(h->d_sk, 0, h->sk_bytes, h->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(h->d_status, 0, 16, h->stream);
   if (e != cudaSuccess) return bail(mb_fail(GZ_ERR_CUDA, cudaGetErrorString(e)));
-  if ((rc = upload_tables(h))) return bail(rc);
+  if ((rc = finalize_graphs(h))) return bail(rc);
   *out = h;
   return GZ_OK;
 }
@@ -1196,8 +1269,7 @@ int gz_batch_set_tuning(gz_batch_t *h, uint32_t threads_per_block, uint32_t ctas
     gz_internal_set_error(msg);
     return rc;
   }
-  MB_TRY(alloc_bins(h));
-  return upload_tables(h);
+  return finalize_graphs(h);
 }
 
 int gz_batch_destroy(gz_batch_t *h) {
@@ -1422,6 +1494,492 @@ int gz_batch_get_profile(gz_batch_t *h, gz_profile_t *out) {
   out->query_ms = h->prof_query_ms;
   out->query_rounds = h->prof_rounds;
   out->kernel_launches = h->launches;
+  return GZ_OK;
+}
+
+}  // extern "C"
+
+// =================================================================================================
+// Serving: many tenants' sketches resident in one HBM arena
+// =================================================================================================
+// A tenant is one CCSketchAlg (its own V and seed) admitted against a sketch-byte budget. Each
+// ingest call applies update batches of any set of tenants with one batched gutter pass and one
+// persistent sketch-update launch (the kernels above, with the tenants' arena offsets in the
+// descriptor table). A connectivity query copies the queried tenants' sketches into a snapshot
+// pool on the query stream and runs the batched Boruvka there from a worker thread, so later
+// ingest calls proceed while it runs; the answer is that of the state at submission.
+namespace {
+
+constexpr uint32_t kServeFlipWords = 64;  // hash-constant slot per tenant (C <= 62)
+constexpr uint32_t kServeTileC = 62;      // column count the tiling budget is reserved for
+
+// First-fit allocator over [0, size) in 256-byte units.
+struct RangeAlloc {
+  std::map<uint64_t, uint64_t> free_;  // offset -> length
+  uint64_t size = 0;
+  void init(uint64_t n) {
+    size = n;
+    free_.clear();
+    if (n) free_[0] = n;
+  }
+  bool alloc(uint64_t n, uint64_t &off) {
+    n = (n + 255) & ~255ull;
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second < n) continue;
+      off = it->first;
+      const uint64_t rest = it->second - n;
+      free_.erase(it);
+      if (rest) free_[off + n] = rest;
+      return true;
+    }
+    return false;
+  }
+  void release(uint64_t off, uint64_t n) {
+    n = (n + 255) & ~255ull;
+    auto it = free_.emplace(off, n).first;
+    auto nx = std::next(it);
+    if (nx != free_.end() && it->first + it->second == nx->first) {
+      it->second += nx->second;
+      free_.erase(nx);
+    }
+    if (it != free_.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) {
+        pv->second += it->second;
+        free_.erase(it);
+      }
+    }
+  }
+};
+
+struct ServeTenant {
+  bool alive = false;
+  GraphDesc desc{};  // tiling, sketch geometry, arena offset, flip slot offset
+  uint64_t seed = 0, bytes = 0;
+  std::vector<uint64_t> flips;  // C + 1 hash constants, padded to even
+};
+
+struct QueryJob {
+  uint64_t ticket = 0;
+  std::vector<uint32_t> tenants;
+  std::vector<GraphDesc> descs;  // sk_off into the snapshot pool, flip_off into `flips`
+  std::vector<uint64_t> flips;
+  std::vector<std::pair<uint64_t, uint64_t>> snaps;  // snapshot regions to release
+  bool done = false;
+  int rc = GZ_OK;
+  std::string err;
+  std::vector<uint32_t> labels, ncc, rounds;
+  std::vector<int> status;
+};
+
+}  // namespace
+
+struct gz_server {
+  std::mutex mtx;  // tenant registry and ingest
+  int device = 0;
+  double factor = 1;
+  uint64_t budget = 0, used = 0;
+  uint8_t *arena = nullptr;
+  RangeAlloc arena_alloc;
+  uint64_t *d_flip = nullptr;  // kServeFlipWords per slot
+  uint32_t slot_cap = 0;
+  std::vector<uint32_t> free_slots;
+  std::vector<ServeTenant> tenants;
+  uint32_t alive = 0;
+  gz_batch ingest;  // engine over the arena
+  gz_batch query;   // engine over the snapshot pool
+  uint64_t *d_qflip = nullptr;
+  uint64_t qflip_cap = 0;
+  uint8_t *d_rec = nullptr;
+  uint64_t rec_cap = 0;
+  // snapshots and the query worker
+  uint8_t *snap = nullptr;
+  RangeAlloc snap_alloc;
+  std::mutex qmtx;
+  std::condition_variable qcv, done_cv;
+  std::deque<QueryJob *> queue;
+  std::map<uint64_t, QueryJob *> jobs;
+  uint64_t next_ticket = 1;
+  bool stop = false;
+  std::thread worker;
+  cudaEvent_t snap_done = nullptr;
+};
+
+namespace {
+
+int serve_run_job(gz_server *s, QueryJob *j) {
+  gz_batch *q = &s->query;
+  MB_TRY(grow(&s->d_qflip, s->qflip_cap, j->flips.size()));
+  q->d_flip = s->d_qflip;
+  MB_CUDA(cudaMemcpyAsync(s->d_qflip, j->flips.data(), 8 * j->flips.size(), cudaMemcpyHostToDevice, q->stream));
+  q->graphs = j->descs;
+  MB_TRY(finalize_graphs(q));
+  j->labels.resize(q->total_V);
+  MB_TRY(batch_query(q, j->labels.data()));
+  j->ncc = q->ncc;
+  j->rounds = q->rounds;
+  j->status.assign(q->status.begin(), q->status.end());
+  return GZ_OK;
+}
+
+void serve_worker(gz_server *s) {
+  cudaSetDevice(s->device);
+  for (;;) {
+    QueryJob *j = nullptr;
+    {
+      std::unique_lock<std::mutex> lk(s->qmtx);
+      s->qcv.wait(lk, [&] { return s->stop || !s->queue.empty(); });
+      if (s->queue.empty()) return;
+      j = s->queue.front();
+      s->queue.pop_front();
+    }
+    j->rc = serve_run_job(s, j);
+    if (j->rc != GZ_OK) j->err = gz_last_error();
+    {
+      std::lock_guard<std::mutex> lk(s->qmtx);
+      for (auto &r : j->snaps) s->snap_alloc.release(r.first, r.second);
+      j->done = true;
+    }
+    s->done_cv.notify_all();
+  }
+}
+
+void serve_destroy(gz_server *s) {
+  {
+    std::lock_guard<std::mutex> lk(s->qmtx);
+    s->stop = true;
+  }
+  s->qcv.notify_all();
+  if (s->worker.joinable()) s->worker.join();
+  for (auto &kv : s->jobs) delete kv.second;
+  s->jobs.clear();
+  s->ingest.d_sk = nullptr;
+  s->query.d_sk = nullptr;
+  batch_destroy(&s->ingest);
+  batch_destroy(&s->query);
+  if (s->snap_done) cudaEventDestroy(s->snap_done);
+  mb_free(s->arena);
+  mb_free(s->snap);
+  mb_free(s->d_flip);
+  mb_free(s->d_qflip);
+  mb_free(s->d_rec);
+}
+
+int serve_engine_init(gz_server *s, gz_batch *e, uint8_t *storage) {
+  e->device = s->device;
+  e->factor = s->factor;
+  e->own_storage = false;
+  e->d_sk = storage;
+  MB_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+  MB_TRY(mb_alloc(&e->d_status, 4));
+  MB_TRY(mb_alloc(&e->d_total, 1));
+  MB_CUDA(cudaMemsetAsync(e->d_status, 0, 16, e->stream));
+  if (cudaMallocHost(&e->h_small, 64) != cudaSuccess) return mb_fail(GZ_ERR_NOMEM, "cudaMallocHost");
+  return GZ_OK;
+}
+
+int serve_check_tenants(gz_server *s, uint32_t n, const uint32_t *ids) {
+  std::vector<uint32_t> seen(ids, ids + n);
+  std::sort(seen.begin(), seen.end());
+  for (uint32_t i = 0; i < n; ++i) {
+    if (ids[i] >= s->tenants.size() || !s->tenants[ids[i]].alive)
+      return mb_fail(GZ_ERR_INVALID, "tenant " + std::to_string(ids[i]) + " is not admitted");
+    if (i && seen[i] == seen[i - 1]) return mb_fail(GZ_ERR_INVALID, "a tenant is listed twice");
+  }
+  return GZ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gz_server_tenant_bytes(uint32_t num_vertices, double sketches_factor, uint64_t *bytes) {
+  if (!bytes || num_vertices < 2) return mb_fail(GZ_ERR_INVALID, "bad argument");
+  GraphDesc gd{};
+  gd.V = num_vertices;
+  sketch_sizing(num_vertices, sketches_factor > 0 ? sketches_factor : 1, gd.C, gd.B);
+  gd.sketch_words = (gd.C * gd.B + 1) * 3;
+  *bytes = graph_sketch_bytes(gd);
+  return GZ_OK;
+}
+
+int gz_server_create(uint64_t budget_bytes, uint64_t snapshot_bytes, double sketches_factor,
+                     gz_server_t **out) {
+  if (!out || budget_bytes < 256 || snapshot_bytes < 256) return mb_fail(GZ_ERR_INVALID, "bad argument");
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return mb_fail(GZ_ERR_NO_DEVICE, "no CUDA device");
+  gz_server *s = new gz_server();
+  auto bail = [&](int rc) {
+    serve_destroy(s);
+    delete s;
+    return rc;
+  };
+  cudaGetDevice(&s->device);
+  s->factor = sketches_factor > 0 ? sketches_factor : 1;
+  s->budget = (budget_bytes + 255) & ~255ull;
+  int rc;
+  if ((rc = mb_alloc(&s->arena, s->budget)) || (rc = mb_alloc(&s->snap, (snapshot_bytes + 255) & ~255ull)))
+    return bail(rc);
+  s->arena_alloc.init(s->budget);
+  s->snap_alloc.init((snapshot_bytes + 255) & ~255ull);
+  if ((rc = serve_engine_init(s, &s->ingest, s->arena)) || (rc = serve_engine_init(s, &s->query, s->snap)))
+    return bail(rc);
+  if (cudaEventCreateWithFlags(&s->snap_done, cudaEventDisableTiming) != cudaSuccess)
+    return bail(mb_fail(GZ_ERR_CUDA, "cudaEventCreate"));
+  s->worker = std::thread(serve_worker, s);
+  *out = s;
+  return GZ_OK;
+}
+
+int gz_server_destroy(gz_server_t *s) {
+  if (!s) return GZ_OK;
+  cudaSetDevice(s->device);
+  serve_destroy(s);
+  delete s;
+  return GZ_OK;
+}
+
+int gz_server_admit(gz_server_t *s, uint32_t num_vertices, uint64_t seed, uint32_t *tenant_out) {
+  if (!s || !tenant_out) return mb_fail(GZ_ERR_INVALID, "null argument");
+  if (num_vertices < 2 || num_vertices > (1u << 31)) return mb_fail(GZ_ERR_INVALID, "a tenant needs 2 <= V <= 2^31");
+  std::lock_guard<std::mutex> lk(s->mtx);
+  cudaSetDevice(s->device);
+  ServeTenant t;
+  GraphDesc &gd = t.desc;
+  gd.V = num_vertices;
+  sketch_sizing(num_vertices, s->factor, gd.C, gd.B);
+  if (gd.B > 63 || gd.C > kServeTileC) return mb_fail(GZ_ERR_INVALID, "sketch geometry not supported by the server");
+  gd.sketch_words = (gd.C * gd.B + 1) * 3;
+  const size_t budget = tile_budget(&s->ingest, kServeTileC);
+  MB_TRY(choose_tiles(gd, 0, budget));
+  t.bytes = graph_sketch_bytes(gd);
+  uint64_t off = 0;
+  if (s->used + t.bytes > s->budget || !s->arena_alloc.alloc(t.bytes, off))
+    return mb_fail(GZ_ERR_BUDGET, "sketch-byte budget exhausted: " + std::to_string(t.bytes) + " more bytes needed, " +
+                                      std::to_string(s->budget - s->used) + " free");
+  gd.sk_off = off;
+  uint32_t slot;
+  if (!s->free_slots.empty()) {
+    slot = s->free_slots.back();
+    s->free_slots.pop_back();
+  } else {
+    slot = s->slot_cap;
+    if (slot >= (1u << 20)) {
+      s->arena_alloc.release(off, t.bytes);
+      return mb_fail(GZ_ERR_INVALID, "too many tenants");
+    }
+    const uint32_t cap = std::max<uint32_t>(64, s->slot_cap * 2);
+    uint64_t *nf = nullptr;
+    if (cudaMalloc(&nf, (size_t)cap * kServeFlipWords * 8) != cudaSuccess) {
+      s->arena_alloc.release(off, t.bytes);
+      return mb_fail(GZ_ERR_NOMEM, "cudaMalloc of hash constants");
+    }
+    if (s->d_flip) {
+      cudaMemcpyAsync(nf, s->d_flip, (size_t)s->slot_cap * kServeFlipWords * 8, cudaMemcpyDeviceToDevice, s->ingest.stream);
+      cudaStreamSynchronize(s->ingest.stream);
+      cudaFree(s->d_flip);
+    }
+    s->d_flip = nf;
+    for (uint32_t k = cap; k-- > s->slot_cap + 1;) s->free_slots.push_back(k);
+    s->slot_cap = cap;
+  }
+  gd.flip_off = slot * kServeFlipWords;
+  t.seed = seed;
+  t.flips.assign((gd.C + 2) & ~1u, 0);
+  for (uint32_t c = 0; c < gd.C; ++c) t.flips[c] = xxh3_flip(seed + 5ull * c);
+  t.flips[gd.C] = xxh3_flip(seed);
+  t.alive = true;
+  MB_CUDA(cudaMemcpyAsync(s->d_flip + gd.flip_off, t.flips.data(), 8 * t.flips.size(), cudaMemcpyHostToDevice,
+                          s->ingest.stream));
+  MB_CUDA(cudaMemsetAsync(s->arena + off, 0, t.bytes, s->ingest.stream));
+  MB_CUDA(cudaStreamSynchronize(s->ingest.stream));
+  s->used += t.bytes;
+  uint32_t id = (uint32_t)s->tenants.size();
+  s->tenants.push_back(std::move(t));
+  s->alive++;
+  *tenant_out = id;
+  return GZ_OK;
+}
+
+int gz_server_evict(gz_server_t *s, uint32_t tenant) {
+  if (!s) return mb_fail(GZ_ERR_INVALID, "null handle");
+  std::lock_guard<std::mutex> lk(s->mtx);
+  cudaSetDevice(s->device);
+  MB_TRY(serve_check_tenants(s, 1, &tenant));
+  ServeTenant &t = s->tenants[tenant];
+  // queries already submitted read their snapshots, not the arena
+  MB_CUDA(cudaStreamSynchronize(s->ingest.stream));
+  s->arena_alloc.release(t.desc.sk_off, t.bytes);
+  s->free_slots.push_back(t.desc.flip_off / kServeFlipWords);
+  s->used -= t.bytes;
+  t.alive = false;
+  t.flips.clear();
+  t.flips.shrink_to_fit();
+  s->alive--;
+  return GZ_OK;
+}
+
+int gz_server_usage(gz_server_t *s, uint64_t *used, uint64_t *budget, uint32_t *tenants) {
+  if (!s) return mb_fail(GZ_ERR_INVALID, "null handle");
+  std::lock_guard<std::mutex> lk(s->mtx);
+  if (used) *used = s->used;
+  if (budget) *budget = s->budget;
+  if (tenants) *tenants = s->alive;
+  return GZ_OK;
+}
+
+int gz_server_get_params(gz_server_t *s, uint32_t tenant, gz_params_t *o) {
+  if (!s || !o) return mb_fail(GZ_ERR_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(s->mtx);
+  MB_TRY(serve_check_tenants(s, 1, &tenant));
+  const GraphDesc &gd = s->tenants[tenant].desc;
+  std::memset(o, 0, sizeof(*o));
+  o->num_vertices = gd.V;
+  o->num_columns = gd.C;
+  o->bkt_per_col = gd.B;
+  o->num_buckets = gd.C * gd.B + 1;
+  o->seed = s->tenants[tenant].seed;
+  o->sketch_bytes = (uint64_t)gd.sketch_words * 4;
+  o->max_rounds = gd.C;
+  o->sketches_factor = s->factor;
+  o->batch_factor = 1;
+  o->vertices_per_tile = 1u << gd.tile_shift;
+  o->num_tiles = gd.ntiles;
+  o->vertices_per_bin = 1u << gd.bin_shift;
+  o->num_bins = gd.nbins;
+  return GZ_OK;
+}
+
+// Applies update batches: tenant ids[i]'s packed 9-byte records are records[offsets[i] ..
+// offsets[i+1]) in host memory. Synchronous.
+int gz_server_ingest(gz_server_t *s, uint32_t n, const uint32_t *ids, const void *records,
+                     const uint64_t *offsets) {
+  if (!s || (n && (!ids || !offsets))) return mb_fail(GZ_ERR_INVALID, "null argument");
+  if (n == 0) return GZ_OK;
+  std::lock_guard<std::mutex> lk(s->mtx);
+  cudaSetDevice(s->device);
+  MB_TRY(serve_check_tenants(s, n, ids));
+  const uint64_t nrec = offsets[n] - offsets[0];
+  if (nrec == 0) return GZ_OK;
+  if (!records) return mb_fail(GZ_ERR_INVALID, "null records");
+  gz_batch *e = &s->ingest;
+  e->graphs.resize(n);
+  for (uint32_t i = 0; i < n; ++i) e->graphs[i] = s->tenants[ids[i]].desc;
+  e->d_flip = s->d_flip;
+  MB_TRY(finalize_graphs(e));
+  MB_TRY(grow(&s->d_rec, s->rec_cap, nrec * 9));
+  MB_CUDA(cudaMemcpyAsync(s->d_rec, static_cast<const uint8_t *>(records) + offsets[0] * 9, nrec * 9,
+                          cudaMemcpyHostToDevice, e->stream));
+  std::vector<uint64_t> rel(n + 1);
+  for (uint32_t i = 0; i <= n; ++i) rel[i] = offsets[i] - offsets[0];
+  return batch_ingest(e, s->d_rec, rel.data());
+}
+
+// Snapshots the listed tenants' sketches (ordered after every earlier ingest call, before every
+// later one) and queues their connected-components query; *ticket identifies it.
+int gz_server_query_submit(gz_server_t *s, uint32_t n, const uint32_t *ids, uint64_t *ticket) {
+  if (!s || !ids || !ticket || n == 0) return mb_fail(GZ_ERR_INVALID, "bad argument");
+  std::lock_guard<std::mutex> lk(s->mtx);
+  cudaSetDevice(s->device);
+  MB_TRY(serve_check_tenants(s, n, ids));
+  QueryJob *j = new QueryJob();
+  j->tenants.assign(ids, ids + n);
+  uint64_t need = 0;
+  for (uint32_t i = 0; i < n; ++i) need += (s->tenants[ids[i]].bytes + 255) & ~255ull;
+  if (need > s->snap_alloc.size) {
+    delete j;
+    return mb_fail(GZ_ERR_INVALID, "the snapshot pool is smaller than this query's tenants");
+  }
+  {
+    // wait for snapshot space (the worker releases it as queries finish)
+    std::unique_lock<std::mutex> ql(s->qmtx);
+    for (;;) {
+      std::vector<std::pair<uint64_t, uint64_t>> got;
+      bool ok = true;
+      for (uint32_t i = 0; i < n && ok; ++i) {
+        uint64_t off;
+        if (s->snap_alloc.alloc(s->tenants[ids[i]].bytes, off)) got.emplace_back(off, s->tenants[ids[i]].bytes);
+        else ok = false;
+      }
+      if (ok) {
+        j->snaps = std::move(got);
+        break;
+      }
+      for (auto &r : got) s->snap_alloc.release(r.first, r.second);
+      if (s->queue.empty() && std::all_of(s->jobs.begin(), s->jobs.end(), [](auto &kv) { return kv.second->done; })) {
+        delete j;
+        return mb_fail(GZ_ERR_NOMEM, "snapshot pool fragmented");
+      }
+      s->done_cv.wait(ql);
+    }
+  }
+  // copies on the query stream after all ingest work so far; later ingest work waits for them
+  cudaEvent_t ev;
+  MB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  MB_CUDA(cudaEventRecord(ev, s->ingest.stream));
+  MB_CUDA(cudaStreamWaitEvent(s->query.stream, ev, 0));
+  cudaEventDestroy(ev);
+  uint64_t flip_off = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    const ServeTenant &t = s->tenants[ids[i]];
+    GraphDesc gd = t.desc;
+    MB_CUDA(cudaMemcpyAsync(s->snap + j->snaps[i].first, s->arena + t.desc.sk_off, t.bytes, cudaMemcpyDeviceToDevice,
+                            s->query.stream));
+    gd.sk_off = j->snaps[i].first;
+    gd.flip_off = (uint32_t)flip_off;
+    j->flips.insert(j->flips.end(), t.flips.begin(), t.flips.end());
+    flip_off += t.flips.size();
+    j->descs.push_back(gd);
+  }
+  MB_CUDA(cudaEventRecord(s->snap_done, s->query.stream));
+  MB_CUDA(cudaStreamWaitEvent(s->ingest.stream, s->snap_done, 0));
+  {
+    std::lock_guard<std::mutex> ql(s->qmtx);
+    j->ticket = s->next_ticket++;
+    s->jobs[j->ticket] = j;
+    s->queue.push_back(j);
+    *ticket = j->ticket;
+  }
+  s->qcv.notify_all();
+  return GZ_OK;
+}
+
+// Waits for a submitted query. labels_out (NULL or the sum of the tenants' V, in submission
+// order) gets each vertex's tenant-local root; num_cc, rounds and status (NULL or one per tenant)
+// as gz_batch_connected_components.
+int gz_server_query_wait(gz_server_t *s, uint64_t ticket, uint32_t *labels_out, uint32_t *num_cc,
+                         uint32_t *rounds, int *status) {
+  if (!s) return mb_fail(GZ_ERR_INVALID, "null handle");
+  QueryJob *j = nullptr;
+  {
+    std::unique_lock<std::mutex> ql(s->qmtx);
+    auto it = s->jobs.find(ticket);
+    if (it == s->jobs.end()) return mb_fail(GZ_ERR_INVALID, "unknown ticket");
+    j = it->second;
+    s->done_cv.wait(ql, [&] { return j->done; });
+    s->jobs.erase(it);
+  }
+  std::unique_ptr<QueryJob> owned(j);
+  if (j->rc != GZ_OK) return mb_fail(j->rc, j->err);
+  if (labels_out) std::copy(j->labels.begin(), j->labels.end(), labels_out);
+  for (size_t i = 0; i < j->tenants.size(); ++i) {
+    if (num_cc) num_cc[i] = j->ncc[i];
+    if (rounds) rounds[i] = j->rounds[i];
+    if (status) status[i] = j->status[i];
+  }
+  return GZ_OK;
+}
+
+int gz_server_dump_sketches(gz_server_t *s, uint32_t tenant, void *host_buf, size_t bytes) {
+  if (!s || !host_buf) return mb_fail(GZ_ERR_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(s->mtx);
+  cudaSetDevice(s->device);
+  MB_TRY(serve_check_tenants(s, 1, &tenant));
+  const GraphDesc &gd = s->tenants[tenant].desc;
+  if (bytes != (uint64_t)gd.V * gd.sketch_words * 4) return mb_fail(GZ_ERR_INVALID, "buffer must hold V * sketch_bytes");
+  MB_CUDA(cudaMemcpyAsync(host_buf, s->arena + gd.sk_off, bytes, cudaMemcpyDeviceToHost, s->ingest.stream));
+  MB_CUDA(cudaStreamSynchronize(s->ingest.stream));
   return GZ_OK;
 }
 

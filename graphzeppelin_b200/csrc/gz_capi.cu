@@ -130,6 +130,7 @@ struct gz_alg {
   size_t hist_words = 0;
   // host-record pipeline
   uint8_t *d_stage[kStageBuffers] = {};
+  uint64_t stage_cap = 0;  // records each staging buffer holds
   cudaEvent_t ev_copied[kStageBuffers] = {}, ev_free[kStageBuffers] = {};
   // apply_update_batch staging
   uint2 *h_ent[2] = {nullptr, nullptr};
@@ -702,6 +703,7 @@ const char *gz_status_string(int s) {
     case GZ_ERR_TIMEOUT: return "device wait timed out";
     case GZ_ERR_BAD_SAMPLE: return "sampled edge out of range";
     case GZ_ERR_NO_DEVICE: return "no CUDA device";
+    case GZ_ERR_BUDGET: return "sketch-byte budget exhausted";
     default: return "unknown status";
   }
 }
@@ -867,9 +869,21 @@ int gz_ingest_records(gz_alg_t *h, const void *rec, size_t n) {
   if (n == 0) return GZ_OK;
   const uint64_t chunk = std::min<uint64_t>(kStageRecords, n);
   const int nbuf = (int)std::min<uint64_t>(kStageBuffers, (n + chunk - 1) / chunk);
+  if (chunk > h->stage_cap) {
+    // staging buffers are sized for the largest chunk seen (small update batches stay small)
+    GZ_CUDA(cudaStreamSynchronize(h->stream));
+    GZ_CUDA(cudaStreamSynchronize(h->copy_stream));
+    for (int i = 0; i < kStageBuffers; ++i) {
+      dev_free(h->d_stage[i]);
+      if (h->ev_copied[i]) cudaEventDestroy(h->ev_copied[i]);
+      if (h->ev_free[i]) cudaEventDestroy(h->ev_free[i]);
+      h->ev_copied[i] = h->ev_free[i] = nullptr;
+    }
+    h->stage_cap = std::min<uint64_t>(kStageRecords, std::max<uint64_t>(chunk, 1ull << 16));
+  }
   for (int i = 0; i < nbuf; ++i) {
     if (!h->d_stage[i]) {
-      GZ_TRY(dev_alloc(&h->d_stage[i], kStageRecords * 9 + 16));
+      GZ_TRY(dev_alloc(&h->d_stage[i], h->stage_cap * 9 + 16));
       GZ_CUDA(cudaEventCreateWithFlags(&h->ev_copied[i], cudaEventDisableTiming));
       GZ_CUDA(cudaEventCreateWithFlags(&h->ev_free[i], cudaEventDisableTiming));
       GZ_CUDA(cudaEventRecord(h->ev_free[i], h->stream));

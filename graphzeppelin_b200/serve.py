@@ -1,0 +1,501 @@
+"""Serving many tenants' connectivity sketches on one GPU.
+
+A tenant is one CCSketchAlg (include/cc_sketch_alg.h:69) with its own vertex count and seed.
+``SketchServer`` wraps the gz_server_* entry points: tenants are admitted while their sketch bytes
+fit a device budget, update batches of many tenants are applied by one batched ingest, and
+connectivity queries run on a device snapshot while later ingests proceed.
+
+``serving_trace`` builds a seeded request trace (tenant arrivals and per-tenant requests on
+Poisson processes; update batches with deletions of live edges; connectivity and point queries),
+and ``replay`` runs a trace against either the batched server or the plain path -- one
+CCSketchAlg per tenant, each request handled on its own -- recording throughput, query latency,
+admissions and every answer, so the two can be compared answer for answer.
+"""
+from __future__ import annotations
+
+import ctypes
+import hashlib
+import time
+from collections import deque
+from dataclasses import dataclass, field
+from typing import Dict, List, Sequence
+
+import numpy as np
+
+from . import _lib
+from .cc import CCSketchAlg, GZError, _as_raw, _check, _ptr
+from .streams import RECORD_DTYPE
+
+UPDATE, CONNECTIVITY_QUERY, POINT_QUERY = 0, 1, 2
+
+
+class BudgetExhausted(GZError):
+    """The server's sketch-byte budget has no room for the tenant (GZ_ERR_BUDGET)."""
+
+
+def _check_srv(rc: int):
+    if rc == _lib.GZ_ERR_BUDGET:
+        raise BudgetExhausted(rc, _lib.last_error())
+    _check(rc)
+
+
+def tenant_bytes(num_vertices: int, sketches_factor: float = 1.0) -> int:
+    """Device bytes one tenant's sketches take from a server budget."""
+    lib = _lib.load()
+    out = ctypes.c_uint64()
+    _check(lib.gz_server_tenant_bytes(num_vertices, sketches_factor, ctypes.byref(out)))
+    return int(out.value)
+
+
+class SketchServer:
+    def __init__(self, budget_bytes: int, snapshot_bytes: int, sketches_factor: float = 1.0):
+        self.lib = _lib.load()
+        h = ctypes.c_void_p()
+        _check(self.lib.gz_server_create(int(budget_bytes), int(snapshot_bytes), sketches_factor,
+                                         ctypes.byref(h)))
+        self._h = h
+        self.num_vertices: Dict[int, int] = {}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.gz_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def admit(self, num_vertices: int, seed: int) -> int:
+        t = ctypes.c_uint32()
+        _check_srv(self.lib.gz_server_admit(self._h, num_vertices, int(seed) & (2**64 - 1),
+                                            ctypes.byref(t)))
+        self.num_vertices[t.value] = int(num_vertices)
+        return int(t.value)
+
+    def evict(self, tenant: int) -> None:
+        _check(self.lib.gz_server_evict(self._h, tenant))
+        self.num_vertices.pop(tenant, None)
+
+    def usage(self):
+        used, budget, n = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint32()
+        _check(self.lib.gz_server_usage(self._h, ctypes.byref(used), ctypes.byref(budget),
+                                        ctypes.byref(n)))
+        return int(used.value), int(budget.value), int(n.value)
+
+    def params(self, tenant: int):
+        p = _lib.gz_params_t()
+        _check(self.lib.gz_server_get_params(self._h, tenant, ctypes.byref(p)))
+        return p
+
+    def ingest(self, tenants: Sequence[int], raws: Sequence[np.ndarray]) -> None:
+        """Apply one update batch per listed tenant (each a packed 9-byte record buffer)."""
+        if not tenants:
+            return
+        ids = np.ascontiguousarray(tenants, dtype=np.uint32)
+        raws = [_as_raw(r) for r in raws]
+        off = np.zeros(len(raws) + 1, np.uint64)
+        off[1:] = np.cumsum([r.size // 9 for r in raws])
+        buf = np.concatenate(raws)
+        _check(self.lib.gz_server_ingest(self._h, ids.size, _ptr(ids),
+                                         _ptr(buf) if buf.size else None, _ptr(off)))
+
+    def query_submit(self, tenants: Sequence[int]) -> int:
+        ids = np.ascontiguousarray(tenants, dtype=np.uint32)
+        t = ctypes.c_uint64()
+        _check(self.lib.gz_server_query_submit(self._h, ids.size, _ptr(ids), ctypes.byref(t)))
+        return int(t.value)
+
+    def query_wait(self, ticket: int, tenants: Sequence[int]):
+        """Per tenant (labels, num_cc, rounds, status) of a submitted query."""
+        sizes = [self.num_vertices[t] for t in tenants]
+        labels = np.empty(sum(sizes), np.uint32)
+        ncc = np.zeros(len(tenants), np.uint32)
+        rounds = np.zeros(len(tenants), np.uint32)
+        status = np.zeros(len(tenants), np.int32)
+        _check(self.lib.gz_server_query_wait(self._h, ticket, _ptr(labels), _ptr(ncc),
+                                             _ptr(rounds), _ptr(status)))
+        out, o = [], 0
+        for i, n in enumerate(sizes):
+            out.append((labels[o:o + n], int(ncc[i]), int(rounds[i]), int(status[i])))
+            o += n
+        return out
+
+    def connected_components(self, tenants: Sequence[int]):
+        return self.query_wait(self.query_submit(tenants), tenants)
+
+    def dump_sketches(self, tenant: int) -> np.ndarray:
+        p = self.params(tenant)
+        buf = np.empty(p.sketch_bytes * p.num_vertices, np.uint8)
+        _check(self.lib.gz_server_dump_sketches(self._h, tenant, _ptr(buf), buf.size))
+        return buf
+
+
+# ------------------------------------------------------------------------------------------------
+# request trace
+# ------------------------------------------------------------------------------------------------
+@dataclass
+class ServingTrace:
+    num_vertices: np.ndarray   # (T,) per tenant
+    seeds: np.ndarray          # (T,) sketch seed per tenant
+    time: np.ndarray           # (N,) arrival time of each request, seconds, non-decreasing
+    tenant: np.ndarray         # (N,)
+    kind: np.ndarray           # (N,) UPDATE / CONNECTIVITY_QUERY / POINT_QUERY
+    rec_off: np.ndarray        # (N + 1,) record range of each request in raw (empty for queries)
+    raw: np.ndarray            # packed 9-byte records of every update batch, in request order
+    point: np.ndarray          # (N, 2) endpoints of point queries
+    last_request: np.ndarray   # (T,) index of each tenant's last request
+
+    @property
+    def num_updates(self) -> int:
+        return int(self.rec_off[-1])
+
+    def records(self, i: int) -> np.ndarray:
+        return self.raw[9 * int(self.rec_off[i]):9 * int(self.rec_off[i + 1])]
+
+
+def _chung_lu_endpoints(rng, V: int, n: int, a: float) -> np.ndarray:
+    """n vertex draws with P(i) proportional to (i + 1)^-a (inverse of the continuous CDF)."""
+    u = rng.random(n)
+    b = 1.0 - a
+    z = ((V + 1.0) ** b - 1.0) / b
+    x = (u * z * b + 1.0) ** (1.0 / b) - 1.0
+    return np.minimum(x.astype(np.int64), V - 1).astype(np.uint32)
+
+
+def serving_trace(num_tenants: int = 2000, seed: int = 7, *, log2_v_min: float = 10.0,
+                  log2_v_max: float = 18.0, exponent: float = 2.3,
+                  requests_per_tenant: float = 6.0, batch_min: int = 1024,
+                  batch_max: int = 65536, delete_fraction: float = 0.2,
+                  mix=(0.90, 0.08, 0.02), tenant_rate: float = 100.0,
+                  request_rate: float = 4.0) -> ServingTrace:
+    """Seeded serving trace. Tenants arrive as a Poisson process (tenant_rate per second), each
+    with V log-uniform in [2^log2_v_min, 2^log2_v_max] and 1 + Poisson(requests_per_tenant - 1)
+    requests arriving as a Poisson process (request_rate per second) after it. The first request
+    is an update batch; the rest are update batches / connectivity queries / point queries with
+    probabilities `mix`. An update batch has U[batch_min, batch_max] records: (1 -
+    delete_fraction) of them insert an edge whose endpoints are drawn from the tenant's Chung-Lu
+    weights (i + 1)^(-1/(exponent - 1)), the rest delete live edges of the tenant. Each tenant's
+    requests follow its own stream in order."""
+    rng = np.random.default_rng(seed)
+    T = num_tenants
+    Vs = np.exp2(rng.uniform(log2_v_min, log2_v_max, T)).astype(np.int64).clip(2, None)
+    seeds = rng.integers(0, 2**63, T, dtype=np.int64).astype(np.uint64)
+    arrive = np.cumsum(rng.exponential(1.0 / tenant_rate, T))
+    a = 1.0 / (exponent - 1.0)
+    times, tenants, kinds, counts, points, parts = [], [], [], [], [], []
+    for t in range(T):
+        V = int(Vs[t])
+        R = 1 + int(rng.poisson(max(requests_per_tenant - 1.0, 0.0)))
+        k = rng.choice(3, R, p=mix)
+        k[0] = UPDATE
+        ts = arrive[t] + np.cumsum(rng.exponential(1.0 / request_rate, R))
+        tr = np.random.default_rng([seed, t])
+        eu = np.zeros(0, np.uint32)
+        ev = np.zeros(0, np.uint32)
+        alive = np.zeros(0, bool)
+        for r in range(R):
+            pu = pv = 0
+            cnt = 0
+            if k[r] == UPDATE:
+                n = int(tr.integers(batch_min, batch_max + 1))
+                n_alive = int(alive.sum())
+                nd = min(int(round(delete_fraction * n)), n_alive)
+                ni = n - nd
+                u = _chung_lu_endpoints(tr, V, ni, a)
+                v = _chung_lu_endpoints(tr, V, ni, a)
+                keep = u != v
+                u, v = u[keep], v[keep]
+                recs_i = np.empty(u.size, RECORD_DTYPE)
+                recs_i["type"], recs_i["src"], recs_i["dst"] = 0, u, v
+                if nd:
+                    live_idx = np.flatnonzero(alive)
+                    pick = tr.choice(live_idx, nd, replace=False)
+                    alive[pick] = False
+                    recs_d = np.empty(nd, RECORD_DTYPE)
+                    recs_d["type"], recs_d["src"], recs_d["dst"] = 1, eu[pick], ev[pick]
+                else:
+                    recs_d = np.empty(0, RECORD_DTYPE)
+                eu = np.concatenate([eu, u])
+                ev = np.concatenate([ev, v])
+                alive = np.concatenate([alive, np.ones(u.size, bool)])
+                recs = np.concatenate([recs_i, recs_d])
+                recs = recs[tr.permutation(recs.size)]
+                parts.append(recs.view(np.uint8).reshape(-1))
+                cnt = recs.size
+            elif k[r] == POINT_QUERY:
+                pu, pv = (int(x) for x in tr.integers(0, V, 2))
+            times.append(ts[r])
+            tenants.append(t)
+            kinds.append(int(k[r]))
+            counts.append(cnt)
+            points.append((pu, pv))
+    order = np.argsort(np.asarray(times), kind="stable")
+    times = np.asarray(times)[order]
+    tenants = np.asarray(tenants, np.int64)[order]
+    kinds = np.asarray(kinds, np.int8)[order]
+    counts = np.asarray(counts, np.int64)
+    points = np.asarray(points, np.uint32).reshape(-1, 2)[order]
+    # records in request order
+    part_of = np.full(len(counts), -1, np.int64)
+    part_of[np.flatnonzero(counts)] = np.arange(int((counts > 0).sum()))
+    ordered = [parts[part_of[i]] for i in order if part_of[i] >= 0]
+    raw = np.concatenate(ordered) if ordered else np.zeros(0, np.uint8)
+    rec_off = np.zeros(len(order) + 1, np.int64)
+    rec_off[1:] = np.cumsum(counts[order])
+    last = np.zeros(T, np.int64)
+    last[tenants] = np.arange(len(order))  # the last write per tenant wins: its last request
+    return ServingTrace(Vs.astype(np.uint32), seeds, times, tenants, kinds, rec_off, raw,
+                        points, last)
+
+
+# ------------------------------------------------------------------------------------------------
+# replay
+# ------------------------------------------------------------------------------------------------
+@dataclass
+class ServingResult:
+    mode: str
+    seconds: float = 0.0
+    updates: int = 0
+    latencies_ms: List[float] = field(default_factory=list)  # one per query, request order
+    answers: Dict[int, tuple] = field(default_factory=dict)  # request index -> answer
+    admitted: int = 0
+    max_resident: int = 0
+    max_used_bytes: int = 0
+    ticks: int = 0
+    gpu_queries: int = 0
+    rejected: int = 0
+
+    def summary(self) -> dict:
+        lat = np.asarray(self.latencies_ms) if self.latencies_ms else np.zeros(1)
+        return {"mode": self.mode, "seconds": self.seconds, "updates": self.updates,
+                "updates_per_s": self.updates / max(self.seconds, 1e-9),
+                "queries": len(self.latencies_ms),
+                "query_p50_ms": float(np.percentile(lat, 50)),
+                "query_p99_ms": float(np.percentile(lat, 99)),
+                "admitted_tenants": self.admitted, "max_resident_tenants": self.max_resident,
+                "max_used_bytes": self.max_used_bytes, "ticks": self.ticks,
+                "gpu_query_batches": self.gpu_queries, "rejected_tenants": self.rejected}
+
+
+def _cc_answer(labels: np.ndarray, ncc: int) -> tuple:
+    p = labels.astype(np.int64)
+    mn = np.full(p.size, np.iinfo(np.int64).max)
+    np.minimum.at(mn, p, np.arange(p.size))
+    canon = mn[p].astype(np.uint32)
+    return (ncc, hashlib.sha1(canon.tobytes()).hexdigest())
+
+
+def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes: int = 0,
+           time_scale: float = 1.0, sketches_factor: float = 1.0,
+           max_tick_updates: int = 1 << 24) -> ServingResult:
+    """Serve every request of `trace`. mode "batched": the gz_server path (continuous batching:
+    each tick applies the arrived update batches of all admitted tenants in one ingest and
+    submits their queries to the snapshot worker; answers are collected one tick later).
+    mode "plain": one CCSketchAlg per tenant, every request handled on its own in arrival order.
+    Requests are released at trace time / time_scale after the start; tenants are admitted in
+    arrival order while their sketch bytes fit the budget and leave after their last request."""
+    res = ServingResult(mode)
+    N = trace.time.size
+    T = trace.num_vertices.size
+    cost = {}
+    pending: Dict[int, deque] = {}
+    waiting: deque = deque()
+    resident = set()
+    state = {}          # plain: CCSketchAlg; batched: server tenant id
+    used = [0]
+    served = np.zeros(T, np.int64)      # requests answered per tenant
+    total = np.bincount(trace.tenant, minlength=T)
+    server = None
+    if mode == "batched":
+        snap = snapshot_bytes or max(budget_bytes // 4, 1 << 26)
+        server = SketchServer(budget_bytes, snap, sketches_factor)
+    cache = {}          # batched: tenant -> (labels, ncc, version it answers for)
+    version = np.zeros(T, np.int64)  # update batches applied per tenant
+    inflight = None     # batched: (ticket, tenants, [(req, t)], versions)
+    t0 = time.perf_counter()
+    nxt = 0
+
+    def now_trace():
+        return (time.perf_counter() - t0) * time_scale
+
+    def finish(i, t, answer):
+        res.answers[i] = answer
+        if trace.kind[i] != UPDATE:
+            res.latencies_ms.append((time.perf_counter() - t0 - trace.time[i] / time_scale) * 1e3)
+        served[t] += 1
+        if served[t] == total[t]:
+            depart(t)
+
+    def depart(t):
+        resident.discard(t)
+        used[0] -= cost[t]
+        if mode == "batched":
+            server.evict(state.pop(t))
+            cache.pop(t, None)
+        else:
+            state.pop(t).close()
+
+    def admit():
+        while waiting:
+            t = waiting[0]
+            c = cost.setdefault(t, tenant_bytes(int(trace.num_vertices[t]), sketches_factor))
+            if c > budget_bytes:  # can never fit: refused, its requests are dropped
+                waiting.popleft()
+                res.rejected += 1
+                dropped = pending.pop(t, deque())
+                served[t] = total[t]
+                for i in dropped:
+                    res.answers[i] = ("rejected",)
+                continue
+            if used[0] + c > budget_bytes:
+                return
+            if mode == "batched":
+                try:
+                    state[t] = server.admit(int(trace.num_vertices[t]), int(trace.seeds[t]))
+                except BudgetExhausted:
+                    return
+            else:
+                a = CCSketchAlg(int(trace.num_vertices[t]), int(trace.seeds[t]))
+                a.set_gutter_capacity(1 << 18)
+                state[t] = a
+            waiting.popleft()
+            used[0] += c
+            resident.add(t)
+            res.admitted += 1
+            res.max_resident = max(res.max_resident, len(resident))
+            res.max_used_bytes = max(res.max_used_bytes, used[0])
+
+    def collect_inflight():
+        nonlocal inflight
+        if inflight is None:
+            return
+        ticket, tens, reqs, vers = inflight
+        inflight = None
+        out = server.query_wait(ticket, [state[t] for t in tens])
+        got = {}
+        for t, (lab, ncc, rounds, status), v in zip(tens, out, vers):
+            got[t] = (lab.copy(), ncc, v)
+            cache[t] = got[t]
+        for i, t in reqs:
+            lab, ncc, _ = got[t]
+            finish(i, t, _answer(i, lab, ncc))
+
+    def _answer(i, lab, ncc):
+        if trace.kind[i] == CONNECTIVITY_QUERY:
+            return _cc_answer(lab, ncc)
+        u, v = trace.point[i]
+        return (bool(lab[u] == lab[v]),)
+
+    try:
+        while True:
+            tnow = now_trace()
+            while nxt < N and trace.time[nxt] <= tnow:
+                t = int(trace.tenant[nxt])
+                if t not in pending:
+                    pending[t] = deque()
+                    waiting.append(t)
+                pending[t].append(nxt)
+                nxt += 1
+            admit()
+            if mode == "plain":
+                # oldest released request of a resident tenant first
+                best = None
+                for t in resident:
+                    q = pending.get(t)
+                    if q and (best is None or q[0] < best[0]):
+                        best = (q[0], t)
+                if best is None:
+                    if nxt >= N and not resident and not waiting:
+                        break
+                    if nxt < N:
+                        time.sleep(max(0.0, min(0.002, (trace.time[nxt] - tnow) / time_scale)))
+                    continue
+                i, t = best
+                pending[t].popleft()
+                a = state[t]
+                if trace.kind[i] == UPDATE:
+                    a.ingest_records(trace.records(i))
+                    res.updates += int(trace.rec_off[i + 1] - trace.rec_off[i])
+                    finish(i, t, ())
+                elif trace.kind[i] == CONNECTIVITY_QUERY:
+                    cc = a.connected_components()
+                    finish(i, t, _cc_answer(cc.parent_arr, cc.size()))
+                else:
+                    u, v = trace.point[i]
+                    finish(i, t, (bool(a.point_query(int(u), int(v))),))
+                continue
+            # batched: one tick
+            ing_t, ing_raw, ing_req = [], [], []
+            qreq = []
+            budget_left = max_tick_updates
+            for t in sorted(resident, key=lambda x: pending[x][0] if pending.get(x) else N):
+                q = pending.get(t)
+                if not q or (inflight is not None and t in inflight[1]):
+                    continue
+                parts = []
+                while q and budget_left > 0:
+                    i = q[0]
+                    if trace.kind[i] == UPDATE:
+                        parts.append(trace.records(i))
+                        budget_left -= int(trace.rec_off[i + 1] - trace.rec_off[i])
+                        ing_req.append((i, t))
+                        q.popleft()
+                    else:
+                        qreq.append((i, t))
+                        q.popleft()
+                        break
+                if parts:
+                    ing_t.append(state[t])
+                    ing_raw.append(np.concatenate(parts))
+                    version[t] += 1
+            if not ing_t and not qreq and inflight is None:
+                if nxt >= N and not resident and not waiting:
+                    break
+                if nxt < N:
+                    time.sleep(max(0.0, min(0.002, (trace.time[nxt] - tnow) / time_scale)))
+                continue
+            res.ticks += 1
+            if ing_t:
+                server.ingest(ing_t, ing_raw)
+                for i, t in ing_req:
+                    res.updates += int(trace.rec_off[i + 1] - trace.rec_off[i])
+                    finish(i, t, ())
+            # queries: cached answers at once, the rest on a device snapshot
+            fresh = []
+            for i, t in qreq:
+                c = cache.get(t)
+                if c is not None and c[2] == version[t]:  # nothing applied since: cached answer
+                    finish(i, t, _answer(i, c[0], c[1]))
+                else:
+                    fresh.append((i, t))
+            prev = inflight
+            inflight = None
+            if fresh:
+                tens = sorted({t for _, t in fresh})
+                ticket = server.query_submit([state[t] for t in tens])
+                res.gpu_queries += 1
+                new = (ticket, tens, fresh, [int(version[t]) for t in tens])
+            else:
+                new = None
+            if prev is not None:
+                inflight = prev
+                collect_inflight()
+            inflight = new
+    finally:
+        if inflight is not None:
+            collect_inflight()
+        res.seconds = time.perf_counter() - t0
+        for t in list(state):
+            if mode == "plain":
+                state.pop(t).close()
+        if server is not None:
+            server.close()
+    return res

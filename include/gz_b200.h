@@ -46,7 +46,8 @@ enum gz_status {
   GZ_ERR_IO = 7,             /* file could not be read or written */
   GZ_ERR_TIMEOUT = 8,        /* a bounded device-side wait gave up (kernel returned early) */
   GZ_ERR_BAD_SAMPLE = 9,     /* a checksum-valid sample decoded to a vertex id >= V */
-  GZ_ERR_NO_DEVICE = 10      /* no usable CUDA device (there is no CPU fallback) */
+  GZ_ERR_NO_DEVICE = 10,     /* no usable CUDA device (there is no CPU fallback) */
+  GZ_ERR_BUDGET = 11         /* a server's sketch-byte budget has no room for this tenant */
 };
 
 /* Query codes, reference enum QueryCode (include/cc_sketch_alg.h:60-63). */
@@ -298,6 +299,44 @@ GZ_API int gz_batch_set_tuning(gz_batch_t *batch, uint32_t threads_per_block, ui
 GZ_API int gz_batch_autotune(gz_batch_t *batch, uint32_t records_per_vertex,
                              uint32_t *vertices_per_tile_out);
 GZ_API int gz_batch_set_profiling(gz_batch_t *batch, int enable);
+
+/* ---- serving: many tenants resident in one HBM budget ------------------------------------------
+ * A gz_server_t keeps the sketches of many tenants (each one CCSketchAlg with its own V and
+ * seed) in one device arena of budget_bytes, admitting a tenant only while its sketch bytes
+ * (V x columns x buckets x 12 B, rounded) fit. gz_server_ingest applies update batches of any set
+ * of tenants with one batched gutter pass and one persistent sketch-update launch.
+ * gz_server_query_submit snapshots the queried tenants' sketches (after every earlier ingest
+ * call, before every later one) into a pool of snapshot_bytes and runs their batched Boruvka on
+ * a second stream from a worker thread, so ingest calls made meanwhile proceed; the answer is
+ * the connected_components (src/cc_sketch_alg.cpp:515-557) of each tenant at submission. */
+typedef struct gz_server gz_server_t;
+
+/* Device bytes one tenant of num_vertices takes from the budget. */
+GZ_API int gz_server_tenant_bytes(uint32_t num_vertices, double sketches_factor, uint64_t *bytes);
+GZ_API int gz_server_create(uint64_t budget_bytes, uint64_t snapshot_bytes, double sketches_factor,
+                            gz_server_t **out);
+GZ_API int gz_server_destroy(gz_server_t *server);
+/* Admits a tenant with zeroed sketches; GZ_ERR_BUDGET when the budget has no room for it. */
+GZ_API int gz_server_admit(gz_server_t *server, uint32_t num_vertices, uint64_t seed,
+                           uint32_t *tenant_out);
+/* Frees a tenant's sketches (queries already submitted for it still complete). */
+GZ_API int gz_server_evict(gz_server_t *server, uint32_t tenant);
+GZ_API int gz_server_usage(gz_server_t *server, uint64_t *used_bytes, uint64_t *budget_bytes,
+                           uint32_t *tenants);
+GZ_API int gz_server_get_params(gz_server_t *server, uint32_t tenant, gz_params_t *out);
+/* Tenant tenants[i]'s packed 9-byte records are records[offsets[i] .. offsets[i+1]) in host
+ * memory (offsets: n + 1 entries; each tenant at most once per call). Synchronous. */
+GZ_API int gz_server_ingest(gz_server_t *server, uint32_t n, const uint32_t *tenants,
+                            const void *records, const uint64_t *offsets);
+GZ_API int gz_server_query_submit(gz_server_t *server, uint32_t n, const uint32_t *tenants,
+                                  uint64_t *ticket);
+/* Waits for a submitted query: labels_out (NULL or the sum of the tenants' V, in submission
+ * order) gets each vertex's tenant-local root; num_cc, rounds, status (NULL or n entries) as
+ * gz_batch_connected_components. */
+GZ_API int gz_server_query_wait(gz_server_t *server, uint64_t ticket, uint32_t *labels_out,
+                                uint32_t *num_cc, uint32_t *rounds, int *status);
+GZ_API int gz_server_dump_sketches(gz_server_t *server, uint32_t tenant, void *host_buf,
+                                   size_t bytes);
 GZ_API int gz_batch_get_profile(gz_batch_t *batch, gz_profile_t *out);
 
 #ifdef __cplusplus
