@@ -561,6 +561,77 @@ def run_many_graphs(args):
     return line
 
 
+SERVING = dict(workload="serving_t2000_v2e10-2e18_chunglu2.3_budget120GB", num_tenants=2000,
+               trace_seed=7, budget_bytes=120 * 10**9, snapshot_bytes=40 * 10**9)
+
+
+def run_serving(args):
+    """Serving loop: a seeded trace of tenants (V log-uniform 2^10..2^18, Chung-Lu endpoints,
+    exponent 2.3) whose requests are update batches of 1k-64k records (20% deletions of live
+    edges), connectivity queries and point queries, served by the batched server (continuous
+    batching, snapshot queries) and by the plain per-tenant CCSketchAlg path, both admitting
+    tenants against a 120 GB sketch budget. Each arm runs the trace twice: paced (requests
+    released at their arrival times, compressed by --time-scale) for query latency, and saturated
+    (every request released at once) for throughput."""
+    import numpy as np
+    import torch
+
+    from graphzeppelin_b200 import serve as SV
+
+    torch.cuda.set_device(0)
+    T = args.tenants or SERVING["num_tenants"]
+    t = time.time()
+    tr = SV.serving_trace(T, SERVING["trace_seed"])
+    log(f"[serving] {T} tenants, {tr.time.size} requests, {tr.num_updates} updates "
+        f"({tr.raw.size / 1e9:.2f} GB) over {tr.time[-1]:.1f} s of trace in {time.time() - t:.1f} s")
+    budget = SERVING["budget_bytes"]
+    kw = dict(snapshot_bytes=SERVING["snapshot_bytes"])
+    arms = {}
+    sampler = ClockSampler(0)
+    sampler.start()
+    for mode in ("batched", "plain"):
+        if mode == "plain" and args.no_plain:
+            continue
+        paced = SV.replay(tr, mode, budget, time_scale=args.time_scale, **kw)
+        sat = SV.replay(tr, mode, budget, time_scale=1e12, **kw)
+        arms[mode] = {"paced": paced, "saturated": sat}
+        log(f"[serving] {mode}: paced {paced.summary()}; saturated {sat.summary()}")
+        torch.cuda.empty_cache()
+    clocks = sampler.stop()
+    b = arms["batched"]
+    equal = None
+    if "plain" in arms:
+        equal = (b["paced"].answers == arms["plain"]["paced"].answers ==
+                 b["saturated"].answers == arms["plain"]["saturated"].answers)
+    else:
+        equal = b["paced"].answers == b["saturated"].answers
+    if equal is False:
+        raise SystemExit("batched and plain serving answers differ")
+    sat = b["saturated"].summary()
+    paced = b["paced"].summary()
+    line = {
+        "metric": "edge updates/sec + p50/p99 query ms, serving on 1 B200",
+        "value": sat["updates_per_s"], "unit": UNIT, "n_gpus": 1, "steps": 1, "warmup": 0,
+        "ms_per_step": sat["seconds"] * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u64",
+        "data": "synthetic (seeded serving trace: Poisson arrivals, Chung-Lu update batches)",
+        "config": {"workload": SERVING["workload"] if T == 2000 else f"serving_t{T}",
+                   "tenants": T, "requests": int(tr.time.size), "updates": tr.num_updates,
+                   "budget_bytes": budget, "snapshot_bytes": SERVING["snapshot_bytes"],
+                   "trace_seconds": float(tr.time[-1]), "time_scale": args.time_scale},
+        "timing": "wall clock of the replay loop (host + GPU), from the first release to the "
+                  "last answer",
+        "batched": {"saturated": sat, "paced": paced},
+        "plain_per_tenant": ({"saturated": arms["plain"]["saturated"].summary(),
+                              "paced": arms["plain"]["paced"].summary()} if "plain" in arms else None),
+        "answers_equal": equal,
+        "query_p50_ms": paced["query_p50_ms"], "query_p99_ms": paced["query_p99_ms"],
+        "admitted_tenants": paced["admitted_tenants"],
+        "clocks": clocks,
+    }
+    return line
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -570,13 +641,17 @@ def main():
     ap.add_argument("--small", action="store_true", help="V=2^14 case (profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="dense", choices=["dense", "many_graphs"],
-                    help="dense: one V=2^17 graph (the headline); many_graphs: 512 uneven graphs")
+    ap.add_argument("--workload", default="dense", choices=["dense", "many_graphs", "serving"],
+                    help="dense: one V=2^17 graph (the headline); many_graphs: 512 uneven graphs; "
+                         "serving: 2000 tenants behind a 120 GB sketch budget")
     ap.add_argument("--graphs", type=int, default=0, help="graphs of the many_graphs workload")
+    ap.add_argument("--tenants", type=int, default=0, help="tenants of the serving workload")
+    ap.add_argument("--time-scale", type=float, default=4.0,
+                    help="serving: trace seconds per wall second in the paced replay")
     ap.add_argument("--no-autotune", action="store_true",
                     help="many_graphs: keep the default tiling instead of running the autotuner")
     ap.add_argument("--no-plain", action="store_true",
-                    help="many_graphs: skip the graph-by-graph plain-path comparison")
+                    help="many_graphs / serving: skip the plain-path comparison")
     args = ap.parse_args()
     if args.warmup < 3 and not args.small:
         log("note: at least 3 warm-up steps are required for a valid number; using 3")
@@ -584,6 +659,8 @@ def main():
     cfg = SMALL if args.small else FULL
     if args.workload == "many_graphs":
         line = run_many_graphs(args)
+    elif args.workload == "serving":
+        line = run_serving(args)
     else:
         line = run_reference(args, cfg) if args.impl == "reference" else run_b200(args, cfg)
     if line is not None:

@@ -314,12 +314,14 @@ def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes:
     served = np.zeros(T, np.int64)      # requests answered per tenant
     total = np.bincount(trace.tenant, minlength=T)
     server = None
+    snap_job_bytes = 0
     if mode == "batched":
         snap = snapshot_bytes or max(budget_bytes // 4, 1 << 26)
         server = SketchServer(budget_bytes, snap, sketches_factor)
+        snap_job_bytes = snap // 2  # two query jobs fit the snapshot pool at once
     cache = {}          # batched: tenant -> (labels, ncc, version it answers for)
     version = np.zeros(T, np.int64)  # update batches applied per tenant
-    inflight = None     # batched: (ticket, tenants, [(req, t)], versions)
+    inflight = []       # batched: jobs of the previous tick, (ticket, tenants, [(req, t)], versions)
     t0 = time.perf_counter()
     nxt = 0
 
@@ -373,20 +375,16 @@ def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes:
             res.max_resident = max(res.max_resident, len(resident))
             res.max_used_bytes = max(res.max_used_bytes, used[0])
 
-    def collect_inflight():
-        nonlocal inflight
-        if inflight is None:
-            return
-        ticket, tens, reqs, vers = inflight
-        inflight = None
-        out = server.query_wait(ticket, [state[t] for t in tens])
-        got = {}
-        for t, (lab, ncc, rounds, status), v in zip(tens, out, vers):
-            got[t] = (lab.copy(), ncc, v)
-            cache[t] = got[t]
-        for i, t in reqs:
-            lab, ncc, _ = got[t]
-            finish(i, t, _answer(i, lab, ncc))
+    def collect(jobs):
+        for ticket, tens, reqs, vers in jobs:
+            out = server.query_wait(ticket, [state[t] for t in tens])
+            got = {}
+            for t, (lab, ncc, rounds, status), v in zip(tens, out, vers):
+                got[t] = (lab.copy(), ncc, v)
+                cache[t] = got[t]
+            for i, t in reqs:
+                lab, ncc, _ = got[t]
+                finish(i, t, _answer(i, lab, ncc))
 
     def _answer(i, lab, ncc):
         if trace.kind[i] == CONNECTIVITY_QUERY:
@@ -436,9 +434,10 @@ def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes:
             ing_t, ing_raw, ing_req = [], [], []
             qreq = []
             budget_left = max_tick_updates
+            busy = {t for job in inflight for t in job[1]}
             for t in sorted(resident, key=lambda x: pending[x][0] if pending.get(x) else N):
                 q = pending.get(t)
-                if not q or (inflight is not None and t in inflight[1]):
+                if not q or t in busy:
                     continue
                 parts = []
                 while q and budget_left > 0:
@@ -456,7 +455,7 @@ def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes:
                     ing_t.append(state[t])
                     ing_raw.append(np.concatenate(parts))
                     version[t] += 1
-            if not ing_t and not qreq and inflight is None:
+            if not ing_t and not qreq and not inflight:
                 if nxt >= N and not resident and not waiting:
                     break
                 if nxt < N:
@@ -476,22 +475,30 @@ def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes:
                     finish(i, t, _answer(i, c[0], c[1]))
                 else:
                     fresh.append((i, t))
-            prev = inflight
-            inflight = None
+            prev, inflight = inflight, []
+            new = []
             if fresh:
-                tens = sorted({t for _, t in fresh})
-                ticket = server.query_submit([state[t] for t in tens])
-                res.gpu_queries += 1
-                new = (ticket, tens, fresh, [int(version[t]) for t in tens])
-            else:
-                new = None
-            if prev is not None:
-                inflight = prev
-                collect_inflight()
+                # jobs of at most half the snapshot pool, so one runs while the next is copied
+                groups, cur, cur_bytes = [], [], 0
+                for t in sorted({t for _, t in fresh}):
+                    if cur and cur_bytes + cost[t] > snap_job_bytes:
+                        groups.append(cur)
+                        cur, cur_bytes = [], 0
+                    cur.append(t)
+                    cur_bytes += cost[t]
+                groups.append(cur)
+                for tens in groups:
+                    members = set(tens)
+                    ticket = server.query_submit([state[t] for t in tens])
+                    res.gpu_queries += 1
+                    new.append((ticket, tens, [(i, t) for i, t in fresh if t in members],
+                                [int(version[t]) for t in tens]))
+            collect(prev)
             inflight = new
     finally:
-        if inflight is not None:
-            collect_inflight()
+        if inflight:
+            jobs, inflight = inflight, []
+            collect(jobs)
         res.seconds = time.perf_counter() - t0
         for t in list(state):
             if mode == "plain":
