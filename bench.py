@@ -584,6 +584,10 @@ def run_serving(args):
     tr = SV.serving_trace(T, SERVING["trace_seed"])
     log(f"[serving] {T} tenants, {tr.time.size} requests, {tr.num_updates} updates "
         f"({tr.raw.size / 1e9:.2f} GB) over {tr.time[-1]:.1f} s of trace in {time.time() - t:.1f} s")
+    # the request payloads live in pinned host memory, as a server's receive buffers would
+    pinned = torch.empty(tr.raw.size, dtype=torch.uint8, pin_memory=True)
+    pinned.numpy()[:] = tr.raw
+    tr.raw = pinned.numpy()
     budget = SERVING["budget_bytes"]
     kw = dict(snapshot_bytes=SERVING["snapshot_bytes"])
     arms = {}

@@ -96,6 +96,7 @@ SIGNATURES = [
     ("gz_batch_dump_sketches", _i, [_H, _u32, _P, _sz]),
     ("gz_batch_load_sketches", _i, [_H, _u32, _P, _sz]),
     ("gz_batch_set_tuning", _i, [_H, _u32, _u32, _P]),
+    ("gz_batch_set_route", _i, [_H, _d]),
     ("gz_batch_autotune", _i, [_H, _u32, _P]),
     ("gz_batch_set_profiling", _i, [_H, _i]),
     ("gz_server_tenant_bytes", _i, [_u32, _d, ctypes.POINTER(_u64)]),
@@ -104,8 +105,10 @@ SIGNATURES = [
     ("gz_server_admit", _i, [_H, _u32, _u64, ctypes.POINTER(_u32)]),
     ("gz_server_evict", _i, [_H, _u32]),
     ("gz_server_usage", _i, [_H, ctypes.POINTER(_u64), ctypes.POINTER(_u64), ctypes.POINTER(_u32)]),
+    ("gz_server_set_route", _i, [_H, _d]),
     ("gz_server_get_params", _i, [_H, _u32, ctypes.POINTER(gz_params_t)]),
     ("gz_server_ingest", _i, [_H, _u32, _P, _P, _P]),
+    ("gz_server_ingest_segments", _i, [_H, _u32, _P, _P, _P]),
     ("gz_server_query_submit", _i, [_H, _u32, _P, ctypes.POINTER(_u64)]),
     ("gz_server_query_wait", _i, [_H, _u64, _P, _P, _P, _P]),
     ("gz_server_dump_sketches", _i, [_H, _u32, _P, _sz]),

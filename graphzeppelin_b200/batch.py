@@ -147,6 +147,10 @@ class CCSketchBatch:
                                             _ptr(vpt) if vpt is not None else None))
         self._refresh_params()
 
+    def set_route(self, sparse_factor: float) -> None:
+        """Per-call routing between in-place and staged ingest (gz_batch_set_route)."""
+        _check(self.lib.gz_batch_set_route(self._h, float(sparse_factor)))
+
     def autotune(self, records_per_vertex: int = 0) -> np.ndarray:
         """Run the autotuner (gz_batch_autotune); returns the vertices per tile chosen per graph."""
         out = np.zeros(self.num_graphs, np.uint32)

@@ -42,7 +42,7 @@ struct GraphDesc {
   uint32_t tile_base; // first global tile
   uint32_t flip_off;  // first of the graph's C + 1 hash constants
   uint32_t nbins, ntiles;
-  uint32_t pad;
+  uint32_t direct_max;  // tiles with fewer entries are updated in place in HBM, unstaged
 };
 
 // ---- gutter ----------------------------------------------------------------------------------
@@ -167,6 +167,79 @@ __global__ void k_mb_bin_off(const uint64_t *scanned, uint64_t nbins, const uint
   if (b == nbins) bin_off[b] = (uint32_t)*total;
 }
 
+// ---- sparse route: records applied in place ---------------------------------------------------
+// For a graph whose call brings too few records to pay for the gutter and tile staging, each
+// record is hashed once (checksum and C depths, shared by both endpoints) and XORed into both
+// endpoints' sketches in HBM with global atomics. A self-loop XORs one sketch twice: no change,
+// as in the gutter path.
+constexpr uint32_t kMbFlipMax = 64;
+
+__global__ void __launch_bounds__(512)
+k_mb_direct(const uint8_t *__restrict__ rec, const uint4 *__restrict__ rtiles, uint32_t n_rt,
+            const GraphDesc *__restrict__ graphs, uint8_t *__restrict__ sketches,
+            const uint64_t *__restrict__ flip, uint32_t *__restrict__ status) {
+  extern __shared__ __align__(16) uint8_t dsm[];
+  uint64_t *s_flip = reinterpret_cast<uint64_t *>(dsm);
+  uint8_t *s_rec = dsm + kMbFlipMax * 8;
+  bool bad = false;
+  for (uint32_t t = blockIdx.x; t < n_rt; t += gridDim.x) {
+    const uint4 rt = rtiles[t];
+    const GraphDesc gd = graphs[rt.x];
+    for (uint32_t i = threadIdx.x; i <= gd.C; i += blockDim.x) s_flip[i] = flip[gd.flip_off + i];
+    const uint32_t shift = stage_records(rec, ((uint64_t)rt.z << 32) | rt.y, rt.w, s_rec);
+    __syncthreads();
+    uint32_t *gsk = reinterpret_cast<uint32_t *>(sketches + gd.sk_off);
+    const uint64_t flip_chk = s_flip[gd.C];
+    for (uint32_t i = threadIdx.x; i < rt.w; i += blockDim.x) {
+      uint32_t u, v;
+      parse_record(s_rec, shift, i, u, v);
+      if (u >= gd.V || v >= gd.V) {
+        bad = true;
+        continue;
+      }
+      if (u == v) continue;
+      const uint32_t lo = max(u, v), hi = min(u, v);
+      const uint64_t in64 = ((uint64_t)lo << 32) | hi;
+      const uint32_t chk = hash_lo32(in64 ^ flip_chk);
+      uint32_t *su = gsk + (uint64_t)u * gd.sketch_words;
+      uint32_t *sv = gsk + (uint64_t)v * gd.sketch_words;
+      const uint32_t det = 3 * gd.C * gd.B;
+      xor_bucket(su + det, lo, hi, chk);
+      xor_bucket(sv + det, lo, hi, chk);
+      for (uint32_t c = 0; c < gd.C; ++c) {
+        const uint32_t d = hash_depth(in64 ^ s_flip[c], gd.B);
+        if (d < gd.B) {
+          const uint32_t o = 3 * (c * gd.B + d);
+          xor_bucket(su + o, lo, hi, chk);
+          xor_bucket(sv + o, lo, hi, chk);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (bad) atomicOr(status, kStatusBadVertex);
+}
+
+constexpr size_t kMbDirectSmem = kMbFlipMax * 8 + kMbRecTile * 9 + 48;
+
+// Work list of the tile kernel: the global tiles whose gutter bin holds entries.
+__global__ void k_mb_worklist(const GraphDesc *__restrict__ graphs, const uint32_t *__restrict__ tile_graph,
+                              uint32_t total_tiles, const uint32_t *__restrict__ bin_off,
+                              uint32_t *__restrict__ list, uint32_t *__restrict__ count) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  bool take = false;
+  if (t < total_tiles) {
+    const GraphDesc gd = graphs[tile_graph[t]];
+    const uint32_t bin = gd.bin_base + ((t - gd.tile_base) >> (gd.bin_shift - gd.tile_shift));
+    take = bin_off[bin + 1] > bin_off[bin];
+  }
+  const uint32_t m = __ballot_sync(kFull, take);
+  uint32_t base = 0;
+  if ((threadIdx.x & 31) == 0 && m) base = atomicAdd(count, (uint32_t)__popc(m));
+  base = __shfl_sync(kFull, base, 0);
+  if (take) list[base + __popc(m & ((1u << (threadIdx.x & 31)) - 1u))] = t;
+}
+
 // ---- sketch update -------------------------------------------------------------------------------
 // One persistent launch over the (graph, tile) items of every graph, warp-specialised: lane 0 of
 // the last warp is the producer -- it claims items from a device work counter, bulk-loads each
@@ -178,11 +251,14 @@ __global__ void k_mb_bin_off(const uint64_t *scanned, uint64_t nbins, const uint
 struct MbSlot {
   uint32_t item, b, e, lt;                 // work item, entry range of its bin, tile in graph
   uint32_t C, B, words, tile_shift, bin_shift;
+  uint32_t direct;                         // apply in place in HBM (no staged tile)
+  uint64_t sk_off;                         // the graph's sketches
 };
 
 __global__ void __launch_bounds__(1024, 1)
 k_mb_sketch_update(const GraphDesc *__restrict__ graphs, const uint32_t *__restrict__ tile_graph,
-                   uint32_t total_tiles, uint8_t *__restrict__ sketches,
+                   const uint32_t *__restrict__ worklist, const uint32_t *__restrict__ worklist_len,
+                   uint8_t *__restrict__ sketches,
                    const uint2 *__restrict__ entries, const uint32_t *__restrict__ bin_off,
                    const uint64_t *__restrict__ flip, uint32_t tile_stride, uint32_t flip_stride,
                    uint32_t *work_counter, uint32_t *status) {
@@ -191,6 +267,7 @@ k_mb_sketch_update(const GraphDesc *__restrict__ graphs, const uint32_t *__restr
   __shared__ MbSlot s_slot[2];
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t ncw = (blockDim.x >> 5) - 1;  // consumer warps
+  const uint32_t total_tiles = *worklist_len;  // items; item k is global tile worklist[k]
   const uint32_t nct = ncw * 32;               // consumer threads
   uint8_t *s_flipb = dsm + 2 * tile_stride;    // 2 x flip_stride bytes
   uint32_t *s_queue = reinterpret_cast<uint32_t *>(s_flipb + 2 * flip_stride);
@@ -220,8 +297,9 @@ k_mb_sketch_update(const GraphDesc *__restrict__ graphs, const uint32_t *__restr
       c.src = nullptr;
       c.fsrc = nullptr;
       if (c.m.item < total_tiles) {
-        const GraphDesc gd = graphs[tile_graph[c.m.item]];
-        c.m.lt = c.m.item - gd.tile_base;
+        const uint32_t tile = worklist[c.m.item];
+        const GraphDesc gd = graphs[tile_graph[tile]];
+        c.m.lt = tile - gd.tile_base;
         c.m.C = gd.C;
         c.m.B = gd.B;
         c.m.words = gd.sketch_words;
@@ -230,11 +308,16 @@ k_mb_sketch_update(const GraphDesc *__restrict__ graphs, const uint32_t *__restr
         const uint32_t bin = gd.bin_base + (c.m.lt >> (gd.bin_shift - gd.tile_shift));
         c.m.b = bin_off[bin];
         c.m.e = bin_off[bin + 1];
+        c.m.sk_off = gd.sk_off;
+        // a bin shared by several tiles is staged (its entries are filtered per tile)
+        c.m.direct = gd.bin_shift == gd.tile_shift && c.m.e - c.m.b < gd.direct_max;
         if (c.m.e > c.m.b) {
-          c.bytes = (gd.sketch_words * 4) << gd.tile_shift;
           c.fbytes = ((gd.C + 2) & ~1u) * 8;
-          c.src = sketches + gd.sk_off + (uint64_t)c.m.lt * c.bytes;
           c.fsrc = flip + gd.flip_off;
+          if (!c.m.direct) {
+            c.bytes = (gd.sketch_words * 4) << gd.tile_shift;
+            c.src = sketches + gd.sk_off + (uint64_t)c.m.lt * c.bytes;
+          }
         }
       }
       return c;
@@ -264,7 +347,7 @@ k_mb_sketch_update(const GraphDesc *__restrict__ graphs, const uint32_t *__restr
       s_slot[s] = c.m;
       pbytes[s] = c.bytes;
       pdst[s] = const_cast<uint8_t *>(c.src);
-      if (c.bytes) {
+      if (c.fbytes) {  // entries to apply: the hash constants, and the tile unless in place
         const uint32_t dst = smem_u32(dsm + s * tile_stride);
         mbar_expect_tx(full, c.bytes + c.fbytes);
         for (uint32_t off = 0; off < c.bytes; off += kBulkPiece)
@@ -313,7 +396,11 @@ k_mb_sketch_update(const GraphDesc *__restrict__ graphs, const uint32_t *__restr
       const uint64_t *s_flip = reinterpret_cast<const uint64_t *>(s_flipb + s * flip_stride);
       const uint32_t vmask = (1u << m.tile_shift) - 1;
       const uint64_t flip_chk = s_flip[m.C];
-      if (m.bin_shift == m.tile_shift) {
+      if (m.direct) {
+        uint32_t *gsk = reinterpret_cast<uint32_t *>(sketches + m.sk_off);
+        for (uint32_t i = m.b + ct; i < m.e; i += nct)
+          apply_entry_global(entries[i], gsk, m.words, s_flip, flip_chk, m.C, m.B);
+      } else if (m.bin_shift == m.tile_shift) {
         // every entry of the bin is this tile's; the next entry's load is in flight while the
         // current one is hashed
         uint32_t i = m.b + ct;
@@ -677,6 +764,9 @@ struct gz_batch {
   uint32_t threads = 1024, ctas_per_sm = 1;  // sketch-update CTA shape
   std::vector<uint32_t> vpt_req;             // requested vertices per tile (0 = default)
   bool own_storage = true;                   // d_sk / d_flip allocated (and freed) by this handle
+  double sparse_factor = 1.0;                // scales the sparse-route threshold (0 = never)
+  uint32_t *d_worklist = nullptr, *d_wl_len = nullptr;
+  uint64_t cap_worklist = 0;
   // capacities of the device tables (grown, never shrunk)
   uint64_t cap_graphs = 0, cap_tiles = 0, cap_V = 0, cap_bins = 0;
   uint64_t cap_bv_V = 0, cap_bv_G = 0, cap_acc = 0;
@@ -764,6 +854,8 @@ void batch_destroy(gz_batch *h) {
   mb_free(h->d_bin_off);
   mb_free(h->d_rtiles);
   mb_free(h->d_rec);
+  mb_free(h->d_worklist);
+  mb_free(h->d_wl_len);
   mb_free(h->d_parent);
   mb_free(h->d_label);
   mb_free(h->d_cnt);
@@ -828,6 +920,9 @@ int choose_tiles(GraphDesc &gd, uint32_t vpt, size_t budget) {
   gd.bin_shift = bshift;
   gd.ntiles = (gd.V + (1u << shift) - 1) >> shift;
   gd.nbins = (gd.V + (1u << bshift) - 1) >> bshift;
+  // Staging a tile moves 2 x tile bytes over HBM; updating in place moves about one 32-byte
+  // sector read and written per bucket, C + 1 buckets per entry: in place wins below this.
+  gd.direct_max = (uint32_t)((sketch_bytes << shift) / (32ull * (gd.C + 1)));
   return GZ_OK;
 }
 
@@ -928,32 +1023,35 @@ int batch_flush_status(gz_batch *h) {
   return GZ_OK;
 }
 
+// Whether graph gd takes n records of one call in place (sparse route): staging its touched
+// tiles moves about 2 x V x sketch bytes over HBM plus the gutter's bytes, updating in place
+// about 2 (C + 1) bucket sectors of 64 B read + written per record.
+bool route_sparse(const gz_batch *h, const GraphDesc &gd, uint64_t n) {
+  const double staged = 2.0 * gd.V * (gd.sketch_words * 4.0) + 50.0 * n;
+  const double in_place = 128.0 * (gd.C + 1) * (double)n;
+  return in_place < staged * h->sparse_factor;
+}
+
 // records of graph g are d_rec[off[g] .. off[g+1]) (9-byte records)
 int batch_ingest(gz_batch *h, const void *d_rec, const uint64_t *off) {
-  std::vector<uint4> rt;
-  uint64_t n_total = 0;
+  std::vector<uint4> rt_dense, rt_sparse;
+  uint64_t n_dense = 0;
   for (uint32_t g = 0; g < h->G; ++g) {
     if (off[g + 1] < off[g]) return mb_fail(GZ_ERR_INVALID, "record offsets must be non-decreasing");
+    const uint64_t n = off[g + 1] - off[g];
+    if (!n) continue;
+    const bool sparse = route_sparse(h, h->graphs[g], n);
+    auto &rt = sparse ? rt_sparse : rt_dense;
     for (uint64_t s = off[g]; s < off[g + 1]; s += kMbRecTile) {
       const uint32_t cnt = (uint32_t)std::min<uint64_t>(kMbRecTile, off[g + 1] - s);
       rt.push_back(make_uint4(g, (uint32_t)s, (uint32_t)(s >> 32), cnt));
     }
-    n_total += off[g + 1] - off[g];
+    if (!sparse) n_dense += n;
   }
-  if (rt.empty()) return GZ_OK;
-  if (2 * n_total >= 0xFFFFFFF0ull) return mb_fail(GZ_ERR_INVALID, "more than 2^31 records in one batch ingest");
-  if (h->entry_cap < 2 * n_total) {
-    mb_free(h->d_entries);
-    h->entry_cap = 0;
-    MB_TRY(mb_alloc(&h->d_entries, 2 * n_total));
-    h->entry_cap = 2 * n_total;
-  }
-  if (h->rtiles_cap < rt.size()) {
-    mb_free(h->d_rtiles);
-    h->rtiles_cap = 0;
-    MB_TRY(mb_alloc(&h->d_rtiles, rt.size()));
-    h->rtiles_cap = rt.size();
-  }
+  if (rt_dense.empty() && rt_sparse.empty()) return GZ_OK;
+  if (2 * n_dense >= 0xFFFFFFF0ull) return mb_fail(GZ_ERR_INVALID, "more than 2^31 records in one batch ingest");
+  const size_t n_rt = rt_dense.size() + rt_sparse.size();
+  MB_TRY(grow(&h->d_rtiles, h->rtiles_cap, n_rt));
   cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
   if (h->prof) {
     cudaEventCreate(&e0);
@@ -961,50 +1059,73 @@ int batch_ingest(gz_batch *h, const void *d_rec, const uint64_t *off) {
     cudaEventCreate(&e2);
     cudaEventRecord(e0, h->stream);
   }
-  MB_CUDA(cudaMemcpyAsync(h->d_rtiles, rt.data(), sizeof(uint4) * rt.size(), cudaMemcpyHostToDevice, h->stream));
-  MB_CUDA(cudaMemsetAsync(h->d_bins, 0, sizeof(uint64_t) * h->total_bins, h->stream));
-  MB_CUDA(cudaMemsetAsync(h->d_bin_fill, 0, sizeof(uint32_t) * h->total_bins, h->stream));
+  rt_dense.insert(rt_dense.end(), rt_sparse.begin(), rt_sparse.end());
+  MB_CUDA(cudaMemcpyAsync(h->d_rtiles, rt_dense.data(), sizeof(uint4) * n_rt, cudaMemcpyHostToDevice, h->stream));
+  const uint32_t n_rt_dense = (uint32_t)(n_rt - rt_sparse.size());
   const uint8_t *rec = static_cast<const uint8_t *>(d_rec);
-  const uint32_t n_rt = (uint32_t)rt.size();
-  {
-    MB_CUDA(cudaFuncSetAttribute(k_mb_count, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMbCountSmem));
-    int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mb_count, 1024, kMbCountSmem);
-    const unsigned grid = (unsigned)std::min<uint64_t>(n_rt, (uint64_t)num_sms() * std::max(per_sm, 1));
-    k_mb_count<<<grid, 1024, kMbCountSmem, h->stream>>>(rec, h->d_rtiles, n_rt, h->d_graphs, h->d_bins,
-                                                       h->d_status);
+  if (n_rt_dense) {
+    MB_TRY(grow(&h->d_entries, h->entry_cap, 2 * n_dense));
+    MB_TRY(grow(&h->d_worklist, h->cap_worklist, h->total_tiles));
+    MB_TRY(mb_alloc(&h->d_wl_len, 1));
+    MB_CUDA(cudaMemsetAsync(h->d_bins, 0, sizeof(uint64_t) * h->total_bins, h->stream));
+    MB_CUDA(cudaMemsetAsync(h->d_bin_fill, 0, sizeof(uint32_t) * h->total_bins, h->stream));
+    MB_CUDA(cudaMemsetAsync(h->d_wl_len, 0, sizeof(uint32_t), h->stream));
+    {
+      MB_CUDA(cudaFuncSetAttribute(k_mb_count, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMbCountSmem));
+      int per_sm = 1;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mb_count, 1024, kMbCountSmem);
+      const unsigned grid = (unsigned)std::min<uint64_t>(n_rt_dense, (uint64_t)num_sms() * std::max(per_sm, 1));
+      k_mb_count<<<grid, 1024, kMbCountSmem, h->stream>>>(rec, h->d_rtiles, n_rt_dense, h->d_graphs, h->d_bins,
+                                                         h->d_status);
+      h->launches++;
+      MB_CUDA(cudaGetLastError());
+    }
+    const uint64_t l0 = launch_count();
+    MB_CUDA(scan_exclusive_u64(h->d_bins, h->total_bins, h->d_total, h->d_scan_tmp, h->stream));
+    h->launches += launch_count() - l0;
+    k_mb_bin_off<<<cdiv(h->total_bins + 1, 256), 256, 0, h->stream>>>(h->d_bins, h->total_bins, h->d_total,
+                                                                       h->d_bin_off);
     h->launches++;
-    MB_CUDA(cudaGetLastError());
-  }
-  const uint64_t l0 = launch_count();
-  MB_CUDA(scan_exclusive_u64(h->d_bins, h->total_bins, h->d_total, h->d_scan_tmp, h->stream));
-  h->launches += launch_count() - l0;
-  k_mb_bin_off<<<cdiv(h->total_bins + 1, 256), 256, 0, h->stream>>>(h->d_bins, h->total_bins, h->d_total,
-                                                                     h->d_bin_off);
-  h->launches++;
-  {
-    MB_CUDA(cudaFuncSetAttribute(k_mb_sort_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMbSortSmem));
-    const unsigned grid = (unsigned)std::min<uint64_t>(n_rt, (uint64_t)num_sms());
-    k_mb_sort_scatter<<<grid, 1024, kMbSortSmem, h->stream>>>(rec, h->d_rtiles, n_rt, h->d_graphs, h->d_bins,
-                                                              h->d_bin_fill, h->d_entries);
+    {
+      MB_CUDA(cudaFuncSetAttribute(k_mb_sort_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMbSortSmem));
+      const unsigned grid = (unsigned)std::min<uint64_t>(n_rt_dense, (uint64_t)num_sms());
+      k_mb_sort_scatter<<<grid, 1024, kMbSortSmem, h->stream>>>(rec, h->d_rtiles, n_rt_dense, h->d_graphs,
+                                                                h->d_bins, h->d_bin_fill, h->d_entries);
+      h->launches++;
+      MB_CUDA(cudaGetLastError());
+    }
+    k_mb_worklist<<<cdiv(h->total_tiles, 256), 256, 0, h->stream>>>(
+        h->d_graphs, h->d_tile_graph, (uint32_t)h->total_tiles, h->d_bin_off, h->d_worklist, h->d_wl_len);
     h->launches++;
     MB_CUDA(cudaGetLastError());
   }
   if (h->prof) cudaEventRecord(e1, h->stream);
-  // one persistent launch for every (graph, tile)
-  MB_CUDA(cudaMemsetAsync(h->d_status + 1, 0, sizeof(uint32_t), h->stream));
-  const uint32_t tile_stride = (h->max_tile_bytes + 127) & ~127u;
-  const uint32_t flip_stride = ((h->max_C + 2) & ~1u) * 8;
-  const size_t ksmem = 2 * (size_t)tile_stride + 2 * (size_t)flip_stride + (size_t)(h->threads / 32) * 256;
-  MB_CUDA(cudaFuncSetAttribute(k_mb_sketch_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ksmem));
-  int per_sm = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mb_sketch_update, (int)h->threads, ksmem);
-  const int grid = (int)std::min<uint64_t>(h->total_tiles, (uint64_t)num_sms() * std::max(per_sm, 1));
-  k_mb_sketch_update<<<grid, h->threads, ksmem, h->stream>>>(
-      h->d_graphs, h->d_tile_graph, (uint32_t)h->total_tiles, h->d_sk, h->d_entries, h->d_bin_off,
-      h->d_flip, tile_stride, flip_stride, h->d_status + 1, h->d_status);
-  h->launches++;
-  MB_CUDA(cudaGetLastError());
+  if (n_rt_dense) {
+    // one persistent launch over every non-empty tile
+    MB_CUDA(cudaMemsetAsync(h->d_status + 1, 0, sizeof(uint32_t), h->stream));
+    const uint32_t tile_stride = (h->max_tile_bytes + 127) & ~127u;
+    const uint32_t flip_stride = ((h->max_C + 2) & ~1u) * 8;
+    const size_t ksmem = 2 * (size_t)tile_stride + 2 * (size_t)flip_stride + (size_t)(h->threads / 32) * 256;
+    MB_CUDA(cudaFuncSetAttribute(k_mb_sketch_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ksmem));
+    int per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mb_sketch_update, (int)h->threads, ksmem);
+    const int grid = (int)std::min<uint64_t>(h->total_tiles, (uint64_t)num_sms() * std::max(per_sm, 1));
+    k_mb_sketch_update<<<grid, h->threads, ksmem, h->stream>>>(
+        h->d_graphs, h->d_tile_graph, h->d_worklist, h->d_wl_len, h->d_sk, h->d_entries, h->d_bin_off,
+        h->d_flip, tile_stride, flip_stride, h->d_status + 1, h->d_status);
+    h->launches++;
+    MB_CUDA(cudaGetLastError());
+  }
+  if (!rt_sparse.empty()) {
+    MB_CUDA(cudaFuncSetAttribute(k_mb_direct, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMbDirectSmem));
+    int per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mb_direct, 512, kMbDirectSmem);
+    const unsigned grid = (unsigned)std::min<uint64_t>(rt_sparse.size(), (uint64_t)num_sms() * std::max(per_sm, 1));
+    k_mb_direct<<<grid, 512, kMbDirectSmem, h->stream>>>(rec, h->d_rtiles + n_rt_dense, (uint32_t)rt_sparse.size(),
+                                                         h->d_graphs, h->d_sk, h->d_flip, h->d_status);
+    h->launches++;
+    MB_CUDA(cudaGetLastError());
+  }
   if (h->prof) {
     cudaEventRecord(e2, h->stream);
     cudaEventSynchronize(e2);
@@ -1284,6 +1405,13 @@ int gz_batch_set_tuning(gz_batch_t *h, uint32_t threads_per_block, uint32_t ctas
     return rc;
   }
   return finalize_graphs(h);
+}
+
+int gz_batch_set_route(gz_batch_t *h, double sparse_factor) {
+  if (!h || !(sparse_factor >= 0)) return mb_fail(GZ_ERR_INVALID, "bad argument");
+  std::lock_guard<std::mutex> lk(h->mtx);
+  h->sparse_factor = sparse_factor;
+  return GZ_OK;
 }
 
 int gz_batch_destroy(gz_batch_t *h) {
@@ -1804,10 +1932,12 @@ int gz_server_admit(gz_server_t *s, uint32_t num_vertices, uint64_t seed, uint32
   for (uint32_t c = 0; c < gd.C; ++c) t.flips[c] = xxh3_flip(seed + 5ull * c);
   t.flips[gd.C] = xxh3_flip(seed);
   t.alive = true;
+  // pageable source: the call returns once the bytes are staged, so t may move afterwards
   MB_CUDA(cudaMemcpyAsync(s->d_flip + gd.flip_off, t.flips.data(), 8 * t.flips.size(), cudaMemcpyHostToDevice,
                           s->ingest.stream));
+  // zeroed on the ingest stream: ordered before every later ingest of this tenant, and after
+  // every snapshot copy of the range's previous owner (the ingest stream waits for those)
   MB_CUDA(cudaMemsetAsync(s->arena + off, 0, t.bytes, s->ingest.stream));
-  MB_CUDA(cudaStreamSynchronize(s->ingest.stream));
   s->used += t.bytes;
   uint32_t id = (uint32_t)s->tenants.size();
   s->tenants.push_back(std::move(t));
@@ -1822,8 +1952,8 @@ int gz_server_evict(gz_server_t *s, uint32_t tenant) {
   cudaSetDevice(s->device);
   MB_TRY(serve_check_tenants(s, 1, &tenant));
   ServeTenant &t = s->tenants[tenant];
-  // queries already submitted read their snapshots, not the arena
-  MB_CUDA(cudaStreamSynchronize(s->ingest.stream));
+  // queries already submitted read their snapshots, whose copies the ingest stream waits for
+  // before any later work on the range (a new tenant's zeroing included)
   s->arena_alloc.release(t.desc.sk_off, t.bytes);
   s->free_slots.push_back(t.desc.flip_off / kServeFlipWords);
   s->used -= t.bytes;
@@ -1831,6 +1961,13 @@ int gz_server_evict(gz_server_t *s, uint32_t tenant) {
   t.flips.clear();
   t.flips.shrink_to_fit();
   s->alive--;
+  return GZ_OK;
+}
+
+int gz_server_set_route(gz_server_t *s, double sparse_factor) {
+  if (!s || !(sparse_factor >= 0)) return mb_fail(GZ_ERR_INVALID, "bad argument");
+  std::lock_guard<std::mutex> lk(s->mtx);
+  s->ingest.sparse_factor = sparse_factor;
   return GZ_OK;
 }
 
@@ -1888,6 +2025,43 @@ int gz_server_ingest(gz_server_t *s, uint32_t n, const uint32_t *ids, const void
   std::vector<uint64_t> rel(n + 1);
   for (uint32_t i = 0; i <= n; ++i) rel[i] = offsets[i] - offsets[0];
   return batch_ingest(e, s->d_rec, rel.data());
+}
+
+// Applies update batches given as segments: segment k holds counts[k] packed records at host
+// address ptrs[k] for tenant tenants[k]; the segments of one tenant must be consecutive. Each
+// segment is one copy into the device staging buffer (pinned sources copy at full link speed).
+int gz_server_ingest_segments(gz_server_t *s, uint32_t nseg, const uint32_t *tenants,
+                              const void *const *ptrs, const uint64_t *counts) {
+  if (!s || (nseg && (!tenants || !ptrs || !counts))) return mb_fail(GZ_ERR_INVALID, "null argument");
+  if (nseg == 0) return GZ_OK;
+  std::lock_guard<std::mutex> lk(s->mtx);
+  cudaSetDevice(s->device);
+  std::vector<uint32_t> ids;
+  std::vector<uint64_t> off(1, 0);
+  for (uint32_t k = 0; k < nseg; ++k) {
+    if (ids.empty() || ids.back() != tenants[k]) {
+      ids.push_back(tenants[k]);
+      off.push_back(off.back());
+    }
+    off.back() += counts[k];
+  }
+  MB_TRY(serve_check_tenants(s, (uint32_t)ids.size(), ids.data()));
+  const uint64_t nrec = off.back();
+  if (nrec == 0) return GZ_OK;
+  gz_batch *e = &s->ingest;
+  e->graphs.resize(ids.size());
+  for (size_t i = 0; i < ids.size(); ++i) e->graphs[i] = s->tenants[ids[i]].desc;
+  e->d_flip = s->d_flip;
+  MB_TRY(finalize_graphs(e));
+  MB_TRY(grow(&s->d_rec, s->rec_cap, nrec * 9));
+  uint64_t pos = 0;
+  for (uint32_t k = 0; k < nseg; ++k) {
+    if (!counts[k]) continue;
+    if (!ptrs[k]) return mb_fail(GZ_ERR_INVALID, "null segment");
+    MB_CUDA(cudaMemcpyAsync(s->d_rec + pos * 9, ptrs[k], counts[k] * 9, cudaMemcpyHostToDevice, e->stream));
+    pos += counts[k];
+  }
+  return batch_ingest(e, s->d_rec, off.data());
 }
 
 // Snapshots the listed tenants' sketches (ordered after every earlier ingest call, before every

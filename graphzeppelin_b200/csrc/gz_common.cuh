@@ -194,6 +194,31 @@ __device__ __forceinline__ uint32_t block_scan_1024(uint32_t x, uint32_t *ws /*3
 }
 
 
+// apply_entry on an unstaged sketch in global memory: the bucket XORs are global atomics (used
+// when a tile has too few entries to pay for staging it). gsk = the graph's first sketch.
+__device__ __forceinline__ void apply_entry_global(uint2 e, uint32_t *gsk, uint32_t sketch_words,
+                                                   const uint64_t *s_flip, uint64_t flip_chk,
+                                                   uint32_t C, uint32_t B) {
+  const uint32_t v = e.x, w = e.y;
+  const uint32_t lo = max(v, w), hi = min(v, w);
+  uint32_t *sk = gsk + (uint64_t)v * sketch_words;
+  const uint64_t in64 = ((uint64_t)lo << 32) | hi;
+  const uint32_t chk = hash_lo32(in64 ^ flip_chk);
+  xor_bucket(sk + 3 * C * B, lo, hi, chk);
+  uint32_t c = 0;
+  for (; c + 1 < C; c += 2) {
+    const uint32_t d0 = hash_depth(in64 ^ s_flip[c], B);
+    const uint32_t d1 = hash_depth(in64 ^ s_flip[c + 1], B);
+    if (d0 < B) xor_bucket(sk + 3 * (c * B + d0), lo, hi, chk);
+    if (d1 < B) xor_bucket(sk + 3 * ((c + 1) * B + d1), lo, hi, chk);
+  }
+  if (c < C) {
+    const uint32_t d = hash_depth(in64 ^ s_flip[c], B);
+    if (d < B) xor_bucket(sk + 3 * (c * B + d), lo, hi, chk);
+  }
+}
+
+
 struct TraceRec {
   uint32_t round, key, result, pad;
   uint64_t idx;

@@ -84,6 +84,10 @@ class SketchServer:
         _check(self.lib.gz_server_evict(self._h, tenant))
         self.num_vertices.pop(tenant, None)
 
+    def set_route(self, sparse_factor: float) -> None:
+        """Per-call routing between in-place and staged ingest (gz_server_set_route)."""
+        _check(self.lib.gz_server_set_route(self._h, float(sparse_factor)))
+
     def usage(self):
         used, budget, n = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint32()
         _check(self.lib.gz_server_usage(self._h, ctypes.byref(used), ctypes.byref(budget),
@@ -106,6 +110,19 @@ class SketchServer:
         buf = np.concatenate(raws)
         _check(self.lib.gz_server_ingest(self._h, ids.size, _ptr(ids),
                                          _ptr(buf) if buf.size else None, _ptr(off)))
+
+    def ingest_segments(self, tenants: Sequence[int], segments: Sequence[np.ndarray]) -> None:
+        """Apply update batches given as segments (tenants[k]'s records in segments[k]; a
+        tenant's segments consecutive). Each segment is copied to the device once, straight
+        from its memory (pinned memory copies fastest)."""
+        if not tenants:
+            return
+        segs = [_as_raw(r) for r in segments]
+        ids = np.ascontiguousarray(tenants, dtype=np.uint32)
+        ptrs = (ctypes.c_void_p * len(segs))(*[r.ctypes.data if r.size else None for r in segs])
+        counts = np.array([r.size // 9 for r in segs], np.uint64)
+        _check(self.lib.gz_server_ingest_segments(self._h, ids.size, _ptr(ids), ptrs, _ptr(counts)))
+        del segs
 
     def query_submit(self, tenants: Sequence[int]) -> int:
         ids = np.ascontiguousarray(tenants, dtype=np.uint32)
@@ -272,6 +289,10 @@ class ServingResult:
     ticks: int = 0
     gpu_queries: int = 0
     rejected: int = 0
+    phase_s: Dict[str, float] = field(default_factory=dict)  # wall seconds per loop phase
+
+    def _add(self, phase: str, t0: float) -> None:
+        self.phase_s[phase] = self.phase_s.get(phase, 0.0) + time.perf_counter() - t0
 
     def summary(self) -> dict:
         lat = np.asarray(self.latencies_ms) if self.latencies_ms else np.zeros(1)
@@ -282,7 +303,8 @@ class ServingResult:
                 "query_p99_ms": float(np.percentile(lat, 99)),
                 "admitted_tenants": self.admitted, "max_resident_tenants": self.max_resident,
                 "max_used_bytes": self.max_used_bytes, "ticks": self.ticks,
-                "gpu_query_batches": self.gpu_queries, "rejected_tenants": self.rejected}
+                "gpu_query_batches": self.gpu_queries, "rejected_tenants": self.rejected,
+                "phase_s": {k: round(v, 4) for k, v in self.phase_s.items()}}
 
 
 def _cc_answer(labels: np.ndarray, ncc: int) -> tuple:
@@ -295,7 +317,7 @@ def _cc_answer(labels: np.ndarray, ncc: int) -> tuple:
 
 def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes: int = 0,
            time_scale: float = 1.0, sketches_factor: float = 1.0,
-           max_tick_updates: int = 1 << 24) -> ServingResult:
+           max_tick_updates: int = 1 << 24, route: float | None = None) -> ServingResult:
     """Serve every request of `trace`. mode "batched": the gz_server path (continuous batching:
     each tick applies the arrived update batches of all admitted tenants in one ingest and
     submits their queries to the snapshot worker; answers are collected one tick later).
@@ -318,6 +340,8 @@ def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes:
     if mode == "batched":
         snap = snapshot_bytes or max(budget_bytes // 4, 1 << 26)
         server = SketchServer(budget_bytes, snap, sketches_factor)
+        if route is not None:
+            server.set_route(route)
         snap_job_bytes = snap // 2  # two query jobs fit the snapshot pool at once
     cache = {}          # batched: tenant -> (labels, ncc, version it answers for)
     version = np.zeros(T, np.int64)  # update batches applied per tenant
@@ -337,6 +361,7 @@ def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes:
             depart(t)
 
     def depart(t):
+        ts = time.perf_counter()
         resident.discard(t)
         used[0] -= cost[t]
         if mode == "batched":
@@ -344,6 +369,7 @@ def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes:
             cache.pop(t, None)
         else:
             state.pop(t).close()
+        res._add("evict", ts)
 
     def admit():
         while waiting:
@@ -359,6 +385,7 @@ def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes:
                 continue
             if used[0] + c > budget_bytes:
                 return
+            ts = time.perf_counter()
             if mode == "batched":
                 try:
                     state[t] = server.admit(int(trace.num_vertices[t]), int(trace.seeds[t]))
@@ -368,6 +395,7 @@ def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes:
                 a = CCSketchAlg(int(trace.num_vertices[t]), int(trace.seeds[t]))
                 a.set_gutter_capacity(1 << 18)
                 state[t] = a
+            res._add("admit", ts)
             waiting.popleft()
             used[0] += c
             resident.add(t)
@@ -377,7 +405,9 @@ def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes:
 
     def collect(jobs):
         for ticket, tens, reqs, vers in jobs:
+            ts = time.perf_counter()
             out = server.query_wait(ticket, [state[t] for t in tens])
+            res._add("query_wait", ts)
             got = {}
             for t, (lab, ncc, rounds, status), v in zip(tens, out, vers):
                 got[t] = (lab.copy(), ncc, v)
@@ -419,19 +449,22 @@ def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes:
                 i, t = best
                 pending[t].popleft()
                 a = state[t]
+                ts = time.perf_counter()
                 if trace.kind[i] == UPDATE:
                     a.ingest_records(trace.records(i))
+                    res._add("ingest", ts)
                     res.updates += int(trace.rec_off[i + 1] - trace.rec_off[i])
                     finish(i, t, ())
                 elif trace.kind[i] == CONNECTIVITY_QUERY:
                     cc = a.connected_components()
+                    res._add("query", ts)
                     finish(i, t, _cc_answer(cc.parent_arr, cc.size()))
                 else:
                     u, v = trace.point[i]
                     finish(i, t, (bool(a.point_query(int(u), int(v))),))
                 continue
             # batched: one tick
-            ing_t, ing_raw, ing_req = [], [], []
+            ing_t, ing_seg, ing_req = [], [], []
             qreq = []
             budget_left = max_tick_updates
             busy = {t for job in inflight for t in job[1]}
@@ -439,11 +472,13 @@ def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes:
                 q = pending.get(t)
                 if not q or t in busy:
                     continue
-                parts = []
+                nparts = 0
                 while q and budget_left > 0:
                     i = q[0]
                     if trace.kind[i] == UPDATE:
-                        parts.append(trace.records(i))
+                        ing_t.append(state[t])
+                        ing_seg.append(trace.records(i))
+                        nparts += 1
                         budget_left -= int(trace.rec_off[i + 1] - trace.rec_off[i])
                         ing_req.append((i, t))
                         q.popleft()
@@ -451,9 +486,7 @@ def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes:
                         qreq.append((i, t))
                         q.popleft()
                         break
-                if parts:
-                    ing_t.append(state[t])
-                    ing_raw.append(np.concatenate(parts))
+                if nparts:
                     version[t] += 1
             if not ing_t and not qreq and not inflight:
                 if nxt >= N and not resident and not waiting:
@@ -463,7 +496,9 @@ def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes:
                 continue
             res.ticks += 1
             if ing_t:
-                server.ingest(ing_t, ing_raw)
+                ts = time.perf_counter()
+                server.ingest_segments(ing_t, ing_seg)
+                res._add("ingest", ts)
                 for i, t in ing_req:
                     res.updates += int(trace.rec_off[i + 1] - trace.rec_off[i])
                     finish(i, t, ())
@@ -489,7 +524,9 @@ def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes:
                 groups.append(cur)
                 for tens in groups:
                     members = set(tens)
+                    ts = time.perf_counter()
                     ticket = server.query_submit([state[t] for t in tens])
+                    res._add("query_submit", ts)
                     res.gpu_queries += 1
                     new.append((ticket, tens, [(i, t) for i, t in fresh if t in members],
                                 [int(version[t]) for t in tens]))

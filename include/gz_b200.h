@@ -292,6 +292,13 @@ GZ_API int gz_batch_load_sketches(gz_batch_t *batch, uint32_t graph, const void 
  * Sketch contents are kept; only the tiling changes. */
 GZ_API int gz_batch_set_tuning(gz_batch_t *batch, uint32_t threads_per_block, uint32_t ctas_per_sm,
                                const uint32_t *vertices_per_tile);
+/* Routing of each ingest call, per graph: a graph whose call brings few records for its size
+ * (the in-place cost estimate, 2 (C + 1) bucket sectors per record, below sparse_factor times
+ * the staged cost, its sketches read and written once plus the gutter's bytes) skips the
+ * gutter: each record is hashed once and XORed into both endpoints' sketches in HBM. The rest
+ * are guttered and applied tile by tile in shared memory. 0 = always staged, 1 = the default,
+ * a huge value = always in place. */
+GZ_API int gz_batch_set_route(gz_batch_t *batch, double sparse_factor);
 /* Autotuner: times trial ingests (records_per_vertex random edge records per vertex, 0 = 64) on
  * a scratch batch with one representative graph per sketch-size class (same columns and buckets
  * per column) and applies the fastest CTA shape and per-class vertices per tile to this batch.
@@ -323,11 +330,19 @@ GZ_API int gz_server_admit(gz_server_t *server, uint32_t num_vertices, uint64_t 
 GZ_API int gz_server_evict(gz_server_t *server, uint32_t tenant);
 GZ_API int gz_server_usage(gz_server_t *server, uint64_t *used_bytes, uint64_t *budget_bytes,
                            uint32_t *tenants);
+/* gz_batch_set_route for the server's ingest calls. */
+GZ_API int gz_server_set_route(gz_server_t *server, double sparse_factor);
 GZ_API int gz_server_get_params(gz_server_t *server, uint32_t tenant, gz_params_t *out);
 /* Tenant tenants[i]'s packed 9-byte records are records[offsets[i] .. offsets[i+1]) in host
  * memory (offsets: n + 1 entries; each tenant at most once per call). Synchronous. */
 GZ_API int gz_server_ingest(gz_server_t *server, uint32_t n, const uint32_t *tenants,
                             const void *records, const uint64_t *offsets);
+/* Same as gz_server_ingest with the records given as segments: segment k is counts[k] records
+ * at host address ptrs[k] for tenant tenants[k] (a tenant's segments consecutive). Each segment
+ * is copied once, straight to the device (no host-side gathering). */
+GZ_API int gz_server_ingest_segments(gz_server_t *server, uint32_t num_segments,
+                                     const uint32_t *tenants, const void *const *ptrs,
+                                     const uint64_t *counts);
 GZ_API int gz_server_query_submit(gz_server_t *server, uint32_t n, const uint32_t *tenants,
                                   uint64_t *ticket);
 /* Waits for a submitted query: labels_out (NULL or the sum of the tenants' V, in submission

@@ -238,3 +238,36 @@ def test_batch_autotune_keeps_sketches_and_results(gz):
         res = b.connected_components()
         for g, V in enumerate(Vs):
             _check_graph(gz, b, res, g, V, seeds[g], sts[g])
+
+
+def test_batch_sparse_ingest_in_place_and_staged(gz):
+    """Calls with only a few entries per tile update sketches in place in HBM; calls with many
+    stage tiles in shared memory; the two mix within a launch and across calls."""
+    from graphzeppelin_b200 import streams as S
+    Vs = [4096, 1000, 300, 20000]
+    seeds = [21, 22, 23, 24]
+    full = [S.erdos_renyi_stream(V, min(1.0, 40.0 / V), seed=V).records for V in Vs]
+    with gz.CCSketchBatch(Vs, seeds) as b:
+        # sparse calls: a few hundred records per graph, then one dense call with the rest
+        cuts = [np.linspace(0, len(r) // 4, 6).astype(int) for r in full]
+        for k in range(5):
+            b.ingest([r[c[k]:c[k + 1]] for r, c in zip(full, cuts)])
+        b.ingest([r[c[-1]:] for r, c in zip(full, cuts)])
+        res = b.connected_components()
+        for g, V in enumerate(Vs):
+            _check_graph(gz, b, res, g, V, seeds[g], full[g])
+
+
+@pytest.mark.parametrize("route", [0.0, 1.0, 1e30])
+def test_batch_routes_agree(gz, route):
+    """Always staged, the cost model's choice, and always in place give the same bytes."""
+    Vs, sts = _mixed_streams()
+    seeds = [13 * i + 5 for i in range(len(Vs))]
+    with gz.CCSketchBatch(Vs, seeds) as b:
+        b.set_route(route)
+        parts = [np.array_split(s, 4) for s in sts]
+        for k in range(4):
+            b.ingest([p[k] for p in parts])
+        res = b.connected_components()
+        for g, V in enumerate(Vs):
+            _check_graph(gz, b, res, g, V, seeds[g], sts[g])
