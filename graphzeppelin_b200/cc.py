@@ -446,6 +446,11 @@ class CCSketchAlg:
         _check(self.lib.gz_get_stream(self._h, ctypes.byref(s)))
         return int(s.value or 0)
 
+    def set_eager_dsu(self, enable: bool = True) -> None:
+        """The reference's default eager DSU (gz_set_eager_dsu): pre_insert keeps a union-find
+        and spanning forest on the host so queries stay cached until a forest edge changes."""
+        _check(self.lib.gz_set_eager_dsu(self._h, int(enable)))
+
     def set_tuning(self, vertices_per_tile: int = 0, threads_per_block: int = 0,
                    tiles_per_bin: int = 0, entry_form: int = 0) -> None:
         """0 keeps defaults; entry_form 1 = plain entries, 2 = hashed entries."""

@@ -9,6 +9,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <unordered_set>
 #include <vector>
 
 #include "../../include/gz_b200.h"
@@ -144,6 +145,12 @@ struct gz_alg {
   bool bv_alloc = false;
   uint32_t *d_final = nullptr, *d_ncc = nullptr;
   bool dsu_valid = true, update_locked = false, labels_on_host = false;
+  // eager DSU (the reference's default build, src/cc_sketch_alg.cpp:87-102): a host union-find
+  // and the spanning-forest edge set, kept while dsu_valid; host_answer = it holds merges the
+  // device answer (d_final) lacks
+  bool eager = false, host_answer = false, boruvka_ran = false;
+  std::vector<uint32_t> hdsu;
+  std::unordered_set<uint64_t> hforest;
   std::atomic<bool> query_running{false};
   size_t last_rounds = 0;
   uint32_t last_ncc = 0;
@@ -550,10 +557,70 @@ int flush_all(gz_alg *h) {
   return check_status(h);
 }
 
-int mark_updated(gz_alg *h) {
+int check_unlocked(gz_alg *h) {
   if (h->update_locked || h->query_running.load()) return fail(GZ_ERR_LOCKED, "Cannot update the algorithm: Connected components currently running");
-  h->dsu_valid = false;  // NO_EAGER_DSU form of pre_insert
+  return GZ_OK;
+}
+
+// The cached answer is lost: the NO_EAGER_DSU form of pre_insert, and every update path whose
+// updates the eager DSU cannot see.
+void invalidate_answer(gz_alg *h) {
+  h->dsu_valid = false;
+  h->host_answer = false;
   h->labels_on_host = false;
+}
+
+int mark_updated(gz_alg *h) {
+  GZ_TRY(check_unlocked(h));
+  invalidate_answer(h);
+  return GZ_OK;
+}
+
+uint32_t host_find(std::vector<uint32_t> &p, uint32_t x) {
+  while (p[x] != x) {
+    p[x] = p[p[x]];
+    x = p[x];
+  }
+  return x;
+}
+
+// CCSketchAlg::pre_insert (src/cc_sketch_alg.cpp:79-104) for one update (u, v).
+void pre_insert_one(gz_alg *h, uint32_t u, uint32_t v) {
+  if (!h->dsu_valid) return;
+  if (!h->eager || u >= h->V || v >= h->V) {
+    invalidate_answer(h);
+    return;
+  }
+  const uint32_t a = std::min(u, v), b = std::max(u, v);
+  const uint64_t key = ((uint64_t)a << 32) | b;
+  const uint32_t ra = host_find(h->hdsu, a), rb = host_find(h->hdsu, b);
+  if (ra != rb) {  // new connectivity: merge, and the edge joins the spanning forest
+    h->hdsu[std::max(ra, rb)] = std::min(ra, rb);
+    h->hforest.insert(key);
+    h->host_answer = true;
+    h->labels_on_host = false;
+  } else if (h->hforest.count(key)) {  // one of the forest's edges changed
+    invalidate_answer(h);
+  }
+}
+
+// Seed the eager DSU from the device answer (labels and Boruvka's spanning forest).
+int eager_from_device(gz_alg *h, bool have_forest) {
+  h->hdsu.resize(h->V);
+  GZ_CUDA(cudaMemcpyAsync(h->hdsu.data(), h->d_final, sizeof(uint32_t) * h->V, cudaMemcpyDeviceToHost, h->stream));
+  uint32_t n = 0;
+  std::vector<uint64_t> idx;
+  if (have_forest) {
+    GZ_CUDA(cudaMemcpyAsync(h->h_status + 3, h->bv.forest_n, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+    GZ_CUDA(cudaStreamSynchronize(h->stream));
+    n = std::min<uint32_t>(h->h_status[3], h->V);
+    idx.resize(n);
+    if (n) GZ_CUDA(cudaMemcpyAsync(idx.data(), h->bv.forest, n * sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
+  }
+  GZ_CUDA(cudaStreamSynchronize(h->stream));
+  h->hforest.clear();
+  h->hforest.insert(idx.begin(), idx.end());
+  h->host_answer = false;
   return GZ_OK;
 }
 
@@ -643,6 +710,8 @@ int run_boruvka(gz_alg *h) {
   h->dsu_valid = true;
   h->labels_on_host = false;
   h->update_locked = false;
+  h->boruvka_ran = true;
+  if (h->eager) GZ_TRY(eager_from_device(h, true));
   return GZ_OK;
 }
 
@@ -650,6 +719,22 @@ int run_boruvka(gz_alg *h) {
 // inserted (a fresh CCSketchAlg starts with a valid, empty DSU).
 int ensure_answer(gz_alg *h) {
   GZ_TRY(flush_all(h));
+  if (h->dsu_valid && h->host_answer) {
+    // the eager DSU's partition: labels computed here, copied to the device answer
+    GZ_TRY(ensure_query(h));
+    h->h_labels.resize(h->V);
+    uint32_t ncc = 0;
+    for (uint32_t v = 0; v < h->V; ++v) {
+      h->h_labels[v] = host_find(h->hdsu, v);
+      ncc += h->h_labels[v] == v;
+    }
+    GZ_CUDA(cudaMemcpyAsync(h->d_final, h->h_labels.data(), sizeof(uint32_t) * h->V, cudaMemcpyHostToDevice, h->stream));
+    GZ_CUDA(cudaStreamSynchronize(h->stream));
+    h->last_ncc = ncc;
+    h->labels_on_host = true;
+    h->host_answer = false;
+    return GZ_OK;
+  }
   if (h->dsu_valid && h->d_final) return GZ_OK;
   if (h->dsu_valid) {
     GZ_TRY(ensure_query(h));
@@ -808,19 +893,37 @@ int gz_allocate_worker_memory(gz_alg_t *h, size_t num_workers) {
   return GZ_OK;
 }
 
-int gz_pre_insert(gz_alg_t *h, uint32_t, uint32_t, int, int) {
+int gz_pre_insert(gz_alg_t *h, uint32_t src, uint32_t dst, int, int) {
   if (!h) return fail(GZ_ERR_INVALID, "null handle");
   Guard g(h);
-  h->dsu_valid = false;
-  h->labels_on_host = false;
+  pre_insert_one(h, src, dst);
   return GZ_OK;
+}
+
+int gz_set_eager_dsu(gz_alg_t *h, int enable) {
+  if (!h) return fail(GZ_ERR_INVALID, "null handle");
+  Guard g(h);
+  if ((enable != 0) == h->eager) return GZ_OK;
+  h->eager = enable != 0;
+  h->host_answer = false;
+  h->hforest.clear();
+  if (!h->eager || !h->dsu_valid) {
+    h->hdsu.clear();
+    return GZ_OK;
+  }
+  // a valid answer exists: start the eager DSU from it
+  GZ_TRY(ensure_answer(h));
+  return eager_from_device(h, h->boruvka_ran);
 }
 
 int gz_apply_update_batch(gz_alg_t *h, int, uint32_t src, const uint32_t *dsts, size_t n) {
   if (!h || (n && !dsts)) return fail(GZ_ERR_INVALID, "null argument");
   if (h->query_running.load()) return fail(GZ_ERR_LOCKED, "Cannot update the algorithm: Connected components currently running");
   Guard g(h);
-  GZ_TRY(mark_updated(h));
+  // the reference leaves the DSU to pre_insert, which the driver calls for every update; without
+  // the eager DSU the cached answer is dropped here as well
+  GZ_TRY(check_unlocked(h));
+  if (!h->eager) invalidate_answer(h);
   if (src >= h->V) return fail(GZ_ERR_BAD_VERTEX, "src vertex id >= V");
   for (size_t i = 0; i < n; ++i) {
     if (dsts[i] >= h->V) return fail(GZ_ERR_BAD_VERTEX, "dst vertex id >= V");
@@ -833,8 +936,7 @@ int gz_apply_raw_buckets_update(gz_alg_t *h, uint32_t src, const void *raw) {
   if (!h || !raw) return fail(GZ_ERR_INVALID, "null argument");
   Guard g(h);
   if (src >= h->V) return fail(GZ_ERR_BAD_VERTEX, "src vertex id >= V");
-  h->dsu_valid = false;
-  h->labels_on_host = false;
+  invalidate_answer(h);
   GZ_TRY(dev_alloc(&h->d_raw, (size_t)h->nb * 3));
   GZ_CUDA(cudaMemcpyAsync(h->d_raw, raw, h->sketch_bytes, cudaMemcpyHostToDevice, h->stream));
   GZ_CUDA(gz::sketch_xor_raw(h->d_sk, h->nb * 3, src, h->d_raw, h->stream));
@@ -846,7 +948,8 @@ int gz_update(gz_alg_t *h, uint32_t src, uint32_t dst, int) {
   if (!h) return fail(GZ_ERR_INVALID, "null handle");
   if (h->query_running.load()) return fail(GZ_ERR_LOCKED, "Cannot update the algorithm: Connected components currently running");
   Guard g(h);
-  GZ_TRY(mark_updated(h));
+  GZ_TRY(check_unlocked(h));
+  pre_insert_one(h, src, dst);  // CCSketchAlg::update calls pre_insert first
   if (src >= h->V || dst >= h->V) return fail(GZ_ERR_BAD_VERTEX, "vertex id >= V");
   GZ_TRY(stage_entry(h, src, dst));
   GZ_TRY(stage_entry(h, dst, src));
@@ -865,7 +968,19 @@ int gz_ingest_records(gz_alg_t *h, const void *rec, size_t n) {
   if (!h || (n && !rec)) return fail(GZ_ERR_INVALID, "null argument");
   if (h->query_running.load()) return fail(GZ_ERR_LOCKED, "Cannot update the algorithm: Connected components currently running");
   Guard g(h);
-  GZ_TRY(mark_updated(h));
+  GZ_TRY(check_unlocked(h));
+  if (h->eager) {
+    // the driver's per-update pre_insert, in stream order, until the DSU is invalidated
+    const uint8_t *r = static_cast<const uint8_t *>(rec);
+    for (size_t i = 0; i < n && h->dsu_valid; ++i) {
+      uint32_t u, v;
+      std::memcpy(&u, r + 9 * i + 1, 4);
+      std::memcpy(&v, r + 9 * i + 5, 4);
+      pre_insert_one(h, u, v);
+    }
+  } else {
+    invalidate_answer(h);
+  }
   if (n == 0) return GZ_OK;
   const uint64_t chunk = std::min<uint64_t>(kStageRecords, n);
   const int nbuf = (int)std::min<uint64_t>(kStageBuffers, (n + chunk - 1) / chunk);
@@ -951,6 +1066,16 @@ int gz_spanning_forest(gz_alg_t *h, uint32_t *edges_out, size_t cap, size_t *n_e
   if (!h || !n_edges) return fail(GZ_ERR_INVALID, "null argument");
   Guard g(h);
   GZ_TRY(ensure_answer(h));
+  if (h->eager) {  // Boruvka's forest plus the edges the eager DSU merged since
+    std::vector<uint64_t> idx(h->hforest.begin(), h->hforest.end());
+    std::sort(idx.begin(), idx.end());
+    *n_edges = idx.size();
+    for (size_t i = 0; edges_out && i < std::min(cap, idx.size()); ++i) {
+      edges_out[2 * i] = (uint32_t)(idx[i] >> 32);
+      edges_out[2 * i + 1] = (uint32_t)idx[i];
+    }
+    return GZ_OK;
+  }
   uint32_t n = 0;
   GZ_CUDA(cudaMemcpyAsync(h->h_status + 3, h->bv.forest_n, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
   GZ_CUDA(cudaStreamSynchronize(h->stream));
@@ -1042,8 +1167,14 @@ int gz_clear(gz_alg_t *h) {
   h->h_ent_n = 0;
   const uint64_t v_pad = ((uint64_t)h->V + 63) & ~63ull;
   GZ_CUDA(cudaMemsetAsync(h->d_sk, 0, v_pad * h->sketch_bytes, h->stream));
-  h->dsu_valid = false;
-  h->labels_on_host = false;
+  invalidate_answer(h);
+  if (h->eager) {  // empty sketches: the eager DSU restarts from singletons, as at construction
+    h->hdsu.resize(h->V);
+    for (uint32_t v = 0; v < h->V; ++v) h->hdsu[v] = v;
+    h->hforest.clear();
+    h->dsu_valid = true;
+    h->host_answer = true;
+  }
   return GZ_OK;
 }
 

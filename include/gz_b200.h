@@ -134,6 +134,16 @@ GZ_API int gz_allocate_worker_memory(gz_alg_t *alg, size_t num_workers);
  * invalidates the cached query answer). */
 GZ_API int gz_pre_insert(gz_alg_t *alg, uint32_t src, uint32_t dst, int type, int thr_id);
 
+/* Eager DSU, the reference's default build (without -DNO_EAGER_DSU): when enabled, gz_pre_insert,
+ * gz_update and gz_ingest_records run CCSketchAlg::pre_insert (src/cc_sketch_alg.cpp:87-102) on
+ * each update in order -- an update joining two components merges them and records a
+ * spanning-forest edge; an update to a recorded forest edge invalidates the DSU -- so that while
+ * the DSU stays valid, gz_has_cached_query is true and queries are answered from it without
+ * Boruvka. Updates this cannot see (gz_ingest_records_device, gz_apply_raw_buckets_update)
+ * invalidate it. Off by default (the NO_EAGER_DSU behaviour: every update invalidates the
+ * cached answer). */
+GZ_API int gz_set_eager_dsu(gz_alg_t *alg, int enable);
+
 /* CCSketchAlg::apply_update_batch -- src/cc_sketch_alg.cpp:106-118: toggles edge index
  * concat_pairing_fn(src, dsts[i]) in src's sketch only. dsts is a host array. */
 GZ_API int gz_apply_update_batch(gz_alg_t *alg, int thr_id, uint32_t src, const uint32_t *dsts,

@@ -245,3 +245,38 @@ uint32_t gzo_exact_cc(uint32_t V, const uint8_t *rec, size_t n, uint32_t *labels
   free(e); free(parent);
   return ncc;
 }
+
+/* Eager DSU, CCSketchAlg::pre_insert of the default build (src/cc_sketch_alg.cpp:87-102), run
+ * over the records in stream order from a valid DSU of singletons. The forest-edge set is an
+ * open-addressing table of (min << 32 | max) keys (a forest has at most V - 1 edges). */
+size_t gzo_eager_dsu(uint32_t V, const uint8_t *rec, size_t n, uint32_t *labels) {
+  uint32_t *parent = (uint32_t *)malloc(sizeof(uint32_t) * V);
+  size_t cap = 16;
+  while (cap < 2 * (size_t)V) cap <<= 1;
+  uint64_t *set = (uint64_t *)calloc(cap, sizeof(uint64_t)); /* 0 = empty (idx 0 is (0,0): a self-loop, never a forest edge) */
+  for (uint32_t v = 0; v < V; ++v) parent[v] = v;
+  size_t pos = n;
+  for (size_t i = 0; i < n; ++i) {
+    uint32_t u = read_le32(rec + 9 * i + 1), v = read_le32(rec + 9 * i + 5);
+    if (u >= V || v >= V) { free(parent); free(set); return (size_t)-1; }
+    uint32_t a = u < v ? u : v, b = u < v ? v : u;
+    uint64_t key = ((uint64_t)a << 32) | b;
+    size_t h = (size_t)((key * 0x9E3779B97F4A7C15ull) >> 20) & (cap - 1);
+    if (uf_union(parent, a, b)) {
+      while (set[h] && set[h] != key) h = (h + 1) & (cap - 1);
+      set[h] = key;
+    } else {
+      int found = 0;
+      while (set[h]) {
+        if (set[h] == key) { found = 1; break; }
+        h = (h + 1) & (cap - 1);
+      }
+      if (found) { pos = i; break; }
+    }
+  }
+  if (pos == n && labels)
+    for (uint32_t v = 0; v < V; ++v) labels[v] = uf_find(parent, v);
+  free(parent);
+  free(set);
+  return pos;
+}

@@ -96,6 +96,14 @@ int gzo_boruvka(const uint8_t *sketches, uint32_t V, uint32_t C, uint32_t B, uin
  * Returns the number of components, or 0 on a bad vertex id. */
 uint32_t gzo_exact_cc(uint32_t V, const uint8_t *records, size_t n_records, uint32_t *labels_out);
 
+/* Eager DSU of the default build: CCSketchAlg::pre_insert (src/cc_sketch_alg.cpp:87-102) over
+ * the records in stream order, from a valid DSU of singletons. An update joining two sets merges
+ * them and records (min, max) as a spanning-forest edge; an update whose endpoints are already
+ * joined invalidates the DSU iff (min, max) is a recorded forest edge. Returns the index of the
+ * invalidating record, or n_records if the DSU stays valid (then labels_out[v] = smallest member
+ * of v's set); (size_t)-1 on a bad vertex id. */
+size_t gzo_eager_dsu(uint32_t V, const uint8_t *records, size_t n_records, uint32_t *labels_out);
+
 #ifdef __cplusplus
 }
 #endif

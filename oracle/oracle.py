@@ -67,6 +67,8 @@ def lib():
                                   ctypes.POINTER(ctypes.c_size_t)]
         L.gzo_exact_cc.restype = ctypes.c_uint32
         L.gzo_exact_cc.argtypes = [ctypes.c_uint32, u8p, ctypes.c_size_t, u32p]
+        L.gzo_eager_dsu.restype = ctypes.c_size_t
+        L.gzo_eager_dsu.argtypes = [ctypes.c_uint32, u8p, ctypes.c_size_t, u32p]
         _lib = L
     return _lib
 
@@ -139,6 +141,18 @@ def exact_cc(num_vertices: int, raw: np.ndarray):
     n = lib().gzo_exact_cc(num_vertices, _p(raw, ctypes.c_uint8), raw.size // 9,
                            _p(labels, ctypes.c_uint32))
     return int(n), labels
+
+
+def eager_dsu(num_vertices: int, raw: np.ndarray):
+    """The default build's eager DSU over a record stream from singletons: (index of the record
+    that invalidated it or None, labels = smallest member id when still valid)."""
+    raw = np.ascontiguousarray(raw, np.uint8)
+    labels = np.zeros(num_vertices, np.uint32)
+    n = raw.size // 9
+    pos = lib().gzo_eager_dsu(num_vertices, _p(raw, ctypes.c_uint8), n, _p(labels, ctypes.c_uint32))
+    if pos == ctypes.c_size_t(-1).value:
+        raise ValueError("record names a vertex >= V")
+    return (None, labels) if pos == n else (int(pos), None)
 
 
 # ---- the compiled reference (oracle/_ref) --------------------------------------------------

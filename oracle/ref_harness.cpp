@@ -173,6 +173,7 @@ int run_ingest(int argc, char **argv) {
     for (auto &x : th) x.join();
   }
   double t1 = now_s();
+  const int cached = alg.has_cached_query(CONNECTIVITY) ? 1 : 0;  // before the query
   // ---- timed query ----
   ConnectedComponents cc = alg.connected_components();
   double t2 = now_s();
@@ -194,9 +195,10 @@ int run_ingest(int argc, char **argv) {
   const int eager = 1;
 #endif
   printf("{\"V\": %u, \"updates\": %llu, \"threads\": %d, \"eager_dsu\": %d, \"batch\": %zu, "
-         "\"ingest_s\": %.6f, \"query_s\": %.6f, \"num_cc\": %u, \"rounds\": %zu}\n",
+         "\"ingest_s\": %.6f, \"query_s\": %.6f, \"num_cc\": %u, \"rounds\": %zu, "
+         "\"cached_before_query\": %d}\n",
          V, (unsigned long long)s.n, threads, eager, batch, t1 - t0, t2 - t1, (unsigned)cc.size(),
-         alg.last_query_rounds);
+         alg.last_query_rounds, cached);
   return 0;
 }
 
