@@ -2159,6 +2159,66 @@ int gz_server_query_wait(gz_server_t *s, uint64_t ticket, uint32_t *labels_out, 
   return GZ_OK;
 }
 
+// CCSketchAlg::write_binary (src/cc_sketch_alg.cpp:614-623) of one tenant: u64 seed, u32 V,
+// f64 sketches_factor, then the V sketches.
+int gz_server_write_binary(gz_server_t *s, uint32_t tenant, const char *path) {
+  if (!s || !path) return mb_fail(GZ_ERR_INVALID, "null argument");
+  std::vector<uint8_t> buf;
+  uint64_t seed;
+  uint32_t V;
+  {
+    std::lock_guard<std::mutex> lk(s->mtx);
+    MB_TRY(serve_check_tenants(s, 1, &tenant));
+    const ServeTenant &t = s->tenants[tenant];
+    seed = t.seed;
+    V = t.desc.V;
+    buf.resize((size_t)V * t.desc.sketch_words * 4);
+  }
+  MB_TRY(gz_server_dump_sketches(s, tenant, buf.data(), buf.size()));
+  FILE *f = fopen(path, "wb");
+  if (!f) return mb_fail(GZ_ERR_IO, std::string("cannot open ") + path);
+  const double sf = s->factor;
+  const bool ok = fwrite(&seed, 8, 1, f) == 1 && fwrite(&V, 4, 1, f) == 1 && fwrite(&sf, 8, 1, f) == 1 &&
+                  fwrite(buf.data(), 1, buf.size(), f) == buf.size();
+  if (fclose(f) != 0 || !ok) return mb_fail(GZ_ERR_IO, std::string("cannot write ") + path);
+  return GZ_OK;
+}
+
+// Re-admission from a write_binary file (construct_from_serialized_data,
+// src/cc_sketch_alg.cpp:30-64): the tenant gets the file's V, seed and sketches; the file's
+// sketches_factor must be the server's.
+int gz_server_admit_serialized(gz_server_t *s, const char *path, uint32_t *tenant_out) {
+  if (!s || !path || !tenant_out) return mb_fail(GZ_ERR_INVALID, "null argument");
+  FILE *f = fopen(path, "rb");
+  if (!f) return mb_fail(GZ_ERR_IO, std::string("cannot open ") + path);
+  uint64_t seed = 0;
+  uint32_t V = 0;
+  double sf = 0;
+  if (fread(&seed, 8, 1, f) != 1 || fread(&V, 4, 1, f) != 1 || fread(&sf, 8, 1, f) != 1) {
+    fclose(f);
+    return mb_fail(GZ_ERR_IO, "truncated header");
+  }
+  if ((sf > 0 ? sf : 1.0) != s->factor) {
+    fclose(f);
+    return mb_fail(GZ_ERR_INVALID, "the file's sketches_factor differs from the server's");
+  }
+  uint32_t C, B;
+  sketch_sizing(V, s->factor, C, B);
+  std::vector<uint8_t> buf((size_t)V * (C * B + 1) * 12);
+  const size_t got = fread(buf.data(), 1, buf.size(), f);
+  fclose(f);
+  if (got != buf.size()) return mb_fail(GZ_ERR_IO, "truncated sketch data");
+  uint32_t id;
+  MB_TRY(gz_server_admit(s, V, seed, &id));
+  std::lock_guard<std::mutex> lk(s->mtx);
+  cudaSetDevice(s->device);
+  MB_CUDA(cudaMemcpyAsync(s->arena + s->tenants[id].desc.sk_off, buf.data(), buf.size(), cudaMemcpyHostToDevice,
+                          s->ingest.stream));
+  MB_CUDA(cudaStreamSynchronize(s->ingest.stream));
+  *tenant_out = id;
+  return GZ_OK;
+}
+
 int gz_server_dump_sketches(gz_server_t *s, uint32_t tenant, void *host_buf, size_t bytes) {
   if (!s || !host_buf) return mb_fail(GZ_ERR_INVALID, "null argument");
   std::lock_guard<std::mutex> lk(s->mtx);

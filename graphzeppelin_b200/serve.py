@@ -148,6 +148,17 @@ class SketchServer:
     def connected_components(self, tenants: Sequence[int]):
         return self.query_wait(self.query_submit(tenants), tenants)
 
+    def write_binary(self, tenant: int, path: str) -> None:
+        """Checkpoint a tenant in CCSketchAlg::write_binary's format."""
+        _check(self.lib.gz_server_write_binary(self._h, tenant, path.encode()))
+
+    def admit_serialized(self, path: str) -> int:
+        """Admit a tenant from a write_binary file (its V, seed and sketches)."""
+        t = ctypes.c_uint32()
+        _check_srv(self.lib.gz_server_admit_serialized(self._h, path.encode(), ctypes.byref(t)))
+        self.num_vertices[t.value] = int(self.params(t.value).num_vertices)
+        return int(t.value)
+
     def dump_sketches(self, tenant: int) -> np.ndarray:
         p = self.params(tenant)
         buf = np.empty(p.sketch_bytes * p.num_vertices, np.uint8)

@@ -362,6 +362,12 @@ GZ_API int gz_server_query_wait(gz_server_t *server, uint64_t ticket, uint32_t *
                                 uint32_t *num_cc, uint32_t *rounds, int *status);
 GZ_API int gz_server_dump_sketches(gz_server_t *server, uint32_t tenant, void *host_buf,
                                    size_t bytes);
+/* Checkpoint of one tenant in CCSketchAlg::write_binary's format (src/cc_sketch_alg.cpp:614-623),
+ * and admission of a tenant from such a file (construct_from_serialized_data,
+ * src/cc_sketch_alg.cpp:30-64; the file's sketches_factor must be the server's): eviction and
+ * re-admission without replaying the stream. */
+GZ_API int gz_server_write_binary(gz_server_t *server, uint32_t tenant, const char *path);
+GZ_API int gz_server_admit_serialized(gz_server_t *server, const char *path, uint32_t *tenant_out);
 GZ_API int gz_batch_get_profile(gz_batch_t *batch, gz_profile_t *out);
 
 #ifdef __cplusplus

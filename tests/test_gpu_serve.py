@@ -136,3 +136,32 @@ def test_serving_replay_batched_equals_plain_and_alone(gz, oracle_mod):
         osk = oracle_mod.OracleSketches(int(tr.num_vertices[t]), int(tr.seeds[t]))
         osk.apply_records(raw)
         assert srv.dump_sketches(sid).tobytes() == osk.data.tobytes()
+
+
+def test_server_checkpoint_and_readmission(gz, tmp_path):
+    """A tenant checkpointed by the server, evicted and re-admitted keeps its sketches and
+    answers; files move both ways between the server and CCSketchAlg."""
+    from graphzeppelin_b200.serve import SketchServer
+    from graphzeppelin_b200 import streams as S
+    st, _ = S.planted_partition_stream(1500, 4, 8, mean_degree=7, churn_fraction=0.1)
+    recs = st.records
+    with SketchServer(1 << 28, 1 << 27) as srv:
+        t = srv.admit(1500, 77)
+        srv.ingest([t], [recs[: len(recs) // 2]])
+        before = srv.dump_sketches(t).tobytes()
+        p = str(tmp_path / "tenant.bin")
+        srv.write_binary(t, p)
+        srv.evict(t)
+        t2 = srv.admit_serialized(p)
+        assert srv.dump_sketches(t2).tobytes() == before
+        srv.ingest([t2], [recs[len(recs) // 2:]])
+        lab, ncc, rounds, _ = srv.connected_components([t2])[0]
+        a = gz.CCSketchAlg.construct_from_serialized_data(p)
+        a.ingest_records(recs[len(recs) // 2:])
+        cc = a.connected_components()
+        assert ncc == cc.size() and (lab == cc.parent_arr).all() and rounds == a.last_query_rounds
+        q = str(tmp_path / "alg.bin")
+        a.write_binary(q)
+        t3 = srv.admit_serialized(q)
+        assert srv.dump_sketches(t3).tobytes() == srv.dump_sketches(t2).tobytes()
+        a.close()
