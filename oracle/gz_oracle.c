@@ -53,6 +53,20 @@ uint64_t gzo_xxh3_8b(uint64_t value, uint64_t seed) {
 
 /* ---- sizing ------------------------------------------------------------------------------ */
 
+int gzo_params_alg(uint32_t V, double f, int cube, uint32_t *num_samples, uint32_t *cols_per_sample,
+                   uint32_t *bkt_per_col) {
+  if (V < 2) return -1;
+  uint64_t vec_len = (uint64_t)ceil((double)V * (uint32_t)(V - 1) / 2);
+  *bkt_per_col = (uint32_t)(ceil(log2((double)vec_len)) + 1);
+  /* include/sketch.h:183-190: CubeSketch (L0_SAMPLING) takes 7 columns per sample and
+   * num_samples_div = log2(3) - 1; CameoSketch 1 column and 1 - log2(2 - 0.8) */
+  const double num_samples_div = cube ? log2(3) - 1 : 1 - log2(2 - 0.8);
+  size_t s = (size_t)ceil(f * log2((double)V) / num_samples_div);
+  *num_samples = (uint32_t)(s > 18 ? s : 18);
+  *cols_per_sample = cube ? 7 : 1;
+  return 0;
+}
+
 int gzo_params(uint32_t V, double f, uint32_t *num_columns, uint32_t *bkt_per_col) {
   if (V < 2) return -1;
   /* Sketch::calc_vector_length: ceil(double(V) * (V - 1) / 2), stored as vec_t */
@@ -84,6 +98,19 @@ static int bkt_good(const uint8_t *b, uint64_t seed) {
   return bkt_gamma(b) == (uint32_t)gzo_xxh3_8b(bkt_alpha(b), seed);
 }
 
+/* Sketch::update of the CubeSketch build (src/sketch.cpp:50-67): the deterministic bucket, then
+ * in every column all buckets of depth 0..d (d < B). */
+void gzo_sketch_update_cube(uint8_t *sk, uint32_t C, uint32_t B, uint64_t seed, uint64_t idx) {
+  uint32_t checksum = (uint32_t)gzo_xxh3_8b(idx, seed);
+  bkt_xor(sk + (size_t)C * B * 12, idx, checksum);
+  for (uint32_t c = 0; c < C; ++c) {
+    uint64_t h = gzo_xxh3_8b(idx, seed + 5ull * c) | (1ull << B);
+    uint32_t depth = (uint32_t)__builtin_ctzll(h);
+    if (depth < B)
+      for (uint32_t j = 0; j <= depth; ++j) bkt_xor(sk + ((size_t)c * B + j) * 12, idx, checksum);
+  }
+}
+
 void gzo_sketch_update(uint8_t *sk, uint32_t C, uint32_t B, uint64_t seed, uint64_t idx) {
   /* checksum = get_index_hash(idx, checksum_seed() == seed) truncated to vec_hash_t */
   uint32_t checksum = (uint32_t)gzo_xxh3_8b(idx, seed);
@@ -97,18 +124,25 @@ void gzo_sketch_update(uint8_t *sk, uint32_t C, uint32_t B, uint64_t seed, uint6
   }
 }
 
-int gzo_apply_records(uint8_t *sketches, uint32_t V, uint32_t C, uint32_t B, uint64_t seed,
-                      const uint8_t *rec, size_t n, const uint8_t *filter) {
+int gzo_apply_records_alg(uint8_t *sketches, uint32_t V, uint32_t C, uint32_t B, uint64_t seed,
+                          const uint8_t *rec, size_t n, const uint8_t *filter, int cube) {
   const size_t sk_bytes = ((size_t)C * B + 1) * 12;
+  void (*upd)(uint8_t *, uint32_t, uint32_t, uint64_t, uint64_t) =
+      cube ? gzo_sketch_update_cube : gzo_sketch_update;
   int rc = 0;
   for (size_t i = 0; i < n; ++i, rec += 9) {
     uint32_t u = read_le32(rec + 1), v = read_le32(rec + 5);
     if (u >= V || v >= V) { rc = GZO_BAD_VERTEX; continue; }
     uint64_t idx = gzo_concat_pairing(u, v);
-    if (!filter || filter[u]) gzo_sketch_update(sketches + u * sk_bytes, C, B, seed, idx);
-    if (!filter || filter[v]) gzo_sketch_update(sketches + v * sk_bytes, C, B, seed, idx);
+    if (!filter || filter[u]) upd(sketches + u * sk_bytes, C, B, seed, idx);
+    if (!filter || filter[v]) upd(sketches + v * sk_bytes, C, B, seed, idx);
   }
   return rc;
+}
+
+int gzo_apply_records(uint8_t *sketches, uint32_t V, uint32_t C, uint32_t B, uint64_t seed,
+                      const uint8_t *rec, size_t n, const uint8_t *filter) {
+  return gzo_apply_records_alg(sketches, V, C, B, seed, rec, n, filter, 0);
 }
 
 int gzo_apply_batch(uint8_t *sketches, uint32_t V, uint32_t C, uint32_t B, uint64_t seed,
@@ -120,6 +154,17 @@ int gzo_apply_batch(uint8_t *sketches, uint32_t V, uint32_t C, uint32_t B, uint6
     gzo_sketch_update(sketches + src * sk_bytes, C, B, seed, gzo_concat_pairing(src, dsts[i]));
   }
   return 0;
+}
+
+/* Sketch::sample (src/sketch.cpp:94-116) over cps consecutive columns of B buckets. */
+static int sample_cols(const uint8_t *det, const uint8_t *col, uint32_t cps, uint32_t B, uint64_t seed,
+                       uint64_t *idx) {
+  *idx = 0;
+  if (bkt_alpha(det) == 0 && bkt_gamma(det) == 0) return GZO_ZERO;
+  if (bkt_good(det, seed)) { *idx = bkt_alpha(det); return GZO_GOOD; }
+  for (uint32_t j = 0; j < cps * B; ++j)
+    if (bkt_good(col + 12 * j, seed)) { *idx = bkt_alpha(col + 12 * j); return GZO_GOOD; }
+  return GZO_FAIL;
 }
 
 int gzo_sample(const uint8_t *det, const uint8_t *col, uint32_t B, uint64_t seed, uint64_t *idx) {
@@ -145,11 +190,12 @@ static int uf_union(uint32_t *p, uint32_t a, uint32_t b) {
   return 1;
 }
 
-int gzo_boruvka(const uint8_t *sketches, uint32_t V, uint32_t C, uint32_t B, uint64_t seed,
-                uint32_t *labels, uint32_t *rounds_out, gzo_trace_rec *trace, size_t cap,
-                size_t *trace_len) {
+int gzo_boruvka_alg(const uint8_t *sketches, uint32_t V, uint32_t C, uint32_t B, uint32_t cps,
+                    uint64_t seed, uint32_t *labels, uint32_t *rounds_out, gzo_trace_rec *trace,
+                    size_t cap, size_t *trace_len) {
   const size_t sk_bytes = ((size_t)C * B + 1) * 12;
-  const size_t acc_bytes = (size_t)(B + 1) * 12; /* column buckets, then the det bucket */
+  const size_t acc_bytes = (size_t)(cps * B + 1) * 12; /* the round's columns, then the det bucket */
+  const uint32_t num_samples = C / cps;
   uint32_t *parent = (uint32_t *)malloc(sizeof(uint32_t) * V);
   uint32_t *root = (uint32_t *)malloc(sizeof(uint32_t) * V);
   uint32_t *key = (uint32_t *)malloc(sizeof(uint32_t) * V);
@@ -159,19 +205,19 @@ int gzo_boruvka(const uint8_t *sketches, uint32_t V, uint32_t C, uint32_t B, uin
   uint32_t round = 0;
   for (uint32_t v = 0; v < V; ++v) parent[v] = v;
   for (;;) {
-    if (round >= C) { rc = GZO_OUT_OF_SAMPLES; break; }
+    if (round >= num_samples) { rc = GZO_OUT_OF_SAMPLES; break; }
     /* components fixed before this round (create_merge_instructions) */
     for (uint32_t v = 0; v < V; ++v) root[v] = uf_find(parent, v);
     for (uint32_t v = 0; v < V; ++v) key[v] = UINT32_MAX;
     for (uint32_t v = 0; v < V; ++v)
       if (key[root[v]] == UINT32_MAX) key[root[v]] = v;
     memset(acc, 0, acc_bytes * V);
-    /* range_merge of column `round` and the deterministic bucket into each component */
+    /* range_merge of sample `round` (columns round*cps .. +cps) and the deterministic bucket */
     for (uint32_t v = 0; v < V; ++v) {
       const uint8_t *sk = sketches + v * sk_bytes;
       uint8_t *a = acc + root[v] * acc_bytes;
-      for (size_t j = 0; j < (size_t)B * 12; ++j) a[j] ^= sk[(size_t)round * B * 12 + j];
-      for (size_t j = 0; j < 12; ++j) a[B * 12 + j] ^= sk[(size_t)C * B * 12 + j];
+      for (size_t j = 0; j < (size_t)cps * B * 12; ++j) a[j] ^= sk[(size_t)round * cps * B * 12 + j];
+      for (size_t j = 0; j < 12; ++j) a[(size_t)cps * B * 12 + j] ^= sk[(size_t)C * B * 12 + j];
     }
     /* sample every component (iterating roots in key order gives a sorted trace) */
     int modified = 0;
@@ -182,7 +228,7 @@ int gzo_boruvka(const uint8_t *sketches, uint32_t V, uint32_t C, uint32_t B, uin
       if (key[r] != k) continue; /* k is the smallest member of component r */
       uint64_t idx;
       uint8_t *a = acc + r * acc_bytes;
-      int res = gzo_sample(a + (size_t)B * 12, a, B, seed, &idx);
+      int res = sample_cols(a + (size_t)cps * B * 12, a, cps, B, seed, &idx);
       if (trace && tl < cap) {
         trace[tl].round = round; trace[tl].key = k; trace[tl].result = (uint32_t)res;
         trace[tl].pad = 0; trace[tl].idx = idx;
@@ -211,6 +257,12 @@ int gzo_boruvka(const uint8_t *sketches, uint32_t V, uint32_t C, uint32_t B, uin
   if (trace_len) *trace_len = tl;
   free(parent); free(root); free(key); free(acc);
   return rc;
+}
+
+int gzo_boruvka(const uint8_t *sketches, uint32_t V, uint32_t C, uint32_t B, uint64_t seed,
+                uint32_t *labels, uint32_t *rounds_out, gzo_trace_rec *trace, size_t cap,
+                size_t *trace_len) {
+  return gzo_boruvka_alg(sketches, V, C, B, 1, seed, labels, rounds_out, trace, cap, trace_len);
 }
 
 /* ---- exact connected components over the final edge set ---------------------------------- */

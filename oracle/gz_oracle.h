@@ -90,6 +90,20 @@ int gzo_boruvka(const uint8_t *sketches, uint32_t V, uint32_t C, uint32_t B, uin
                 uint32_t *labels_out, uint32_t *rounds_out, gzo_trace_rec *trace,
                 size_t trace_cap, size_t *trace_len);
 
+/* CubeSketch (the reference built with -DL0_SAMPLING): sizing (include/sketch.h:183-190:
+ * 7 columns per sample, num_samples_div = log2(3) - 1; cube = 0 gives CameoSketch), the update
+ * (src/sketch.cpp:50-67: every depth 0..d of each column), and Boruvka whose round r merges and
+ * scans the cps columns of sample r (src/sketch.cpp:94-116, 156-179). */
+int gzo_params_alg(uint32_t num_vertices, double sketches_factor, int cube, uint32_t *num_samples,
+                   uint32_t *cols_per_sample, uint32_t *bkt_per_col);
+void gzo_sketch_update_cube(uint8_t *sketch, uint32_t C, uint32_t B, uint64_t seed, uint64_t idx);
+int gzo_apply_records_alg(uint8_t *sketches, uint32_t V, uint32_t C, uint32_t B, uint64_t seed,
+                          const uint8_t *records, size_t n_records, const uint8_t *vertex_filter,
+                          int cube);
+int gzo_boruvka_alg(const uint8_t *sketches, uint32_t V, uint32_t C, uint32_t B, uint32_t cps,
+                    uint64_t seed, uint32_t *labels_out, uint32_t *rounds_out, gzo_trace_rec *trace,
+                    size_t trace_cap, size_t *trace_len);
+
 /* Ground truth: exact union-find over the final edge set of a record stream (edges toggled an
  * odd number of times), the role GraphVerifier's Kruskal plays in the reference
  * (test/util/graph_verifier.cpp). labels_out[v] = smallest vertex id of v's component.

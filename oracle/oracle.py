@@ -21,6 +21,7 @@ LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF_DIR = os.path.join(HERE, "_ref")
 REF_NOEAGER = os.path.join(REF_DIR, "gz_ref_noeager")
 REF_EAGER = os.path.join(REF_DIR, "gz_ref_eager")
+REF_CUBE = os.path.join(REF_DIR, "gz_ref_cube")  # -DL0_SAMPLING -DNO_EAGER_DSU
 
 GOOD, ZERO, FAIL = 0, 1, 2
 TRACE_DTYPE = np.dtype([("round", "<u4"), ("key", "<u4"), ("result", "<u4"), ("pad", "<u4"),
@@ -67,6 +68,15 @@ def lib():
                                   ctypes.POINTER(ctypes.c_size_t)]
         L.gzo_exact_cc.restype = ctypes.c_uint32
         L.gzo_exact_cc.argtypes = [ctypes.c_uint32, u8p, ctypes.c_size_t, u32p]
+        L.gzo_params_alg.restype = ctypes.c_int
+        L.gzo_params_alg.argtypes = [ctypes.c_uint32, ctypes.c_double, ctypes.c_int, u32p, u32p, u32p]
+        L.gzo_apply_records_alg.restype = ctypes.c_int
+        L.gzo_apply_records_alg.argtypes = [u8p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                            ctypes.c_uint64, u8p, ctypes.c_size_t, u8p, ctypes.c_int]
+        L.gzo_boruvka_alg.restype = ctypes.c_int
+        L.gzo_boruvka_alg.argtypes = [u8p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                      ctypes.c_uint32, ctypes.c_uint64, u32p, u32p, ctypes.c_void_p,
+                                      ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
         L.gzo_eager_dsu.restype = ctypes.c_size_t
         L.gzo_eager_dsu.argtypes = [ctypes.c_uint32, u8p, ctypes.c_size_t, u32p]
         _lib = L
@@ -81,6 +91,15 @@ def xxh3_8b(value: int, seed: int) -> int:
     return int(lib().gzo_xxh3_8b(value & (2**64 - 1), seed & (2**64 - 1)))
 
 
+def params_alg(num_vertices: int, sketches_factor: float = 1.0, cube: bool = False):
+    """(num_samples, cols_per_sample, bkt_per_col) of CameoSketch or CubeSketch."""
+    s, c, b = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+    if lib().gzo_params_alg(num_vertices, sketches_factor, int(cube), ctypes.byref(s), ctypes.byref(c),
+                            ctypes.byref(b)):
+        raise ValueError("num_vertices must be >= 2")
+    return s.value, c.value, b.value
+
+
 def params(num_vertices: int, sketches_factor: float = 1.0):
     """(num_columns, bkt_per_col, num_buckets, sketch_bytes) of CCSketchAlg(V, .., f)."""
     c, b = ctypes.c_uint32(), ctypes.c_uint32()
@@ -93,9 +112,13 @@ def params(num_vertices: int, sketches_factor: float = 1.0):
 class OracleSketches:
     """V sketches in the reference byte layout, updated by the C restatement."""
 
-    def __init__(self, num_vertices: int, seed: int, sketches_factor: float = 1.0):
-        self.V, self.seed, self.factor = num_vertices, seed, sketches_factor
-        self.C, self.B, self.nb, self.sketch_bytes = params(num_vertices, sketches_factor)
+    def __init__(self, num_vertices: int, seed: int, sketches_factor: float = 1.0,
+                 cube: bool = False):
+        self.V, self.seed, self.factor, self.cube = num_vertices, seed, sketches_factor, cube
+        samples, self.cps, self.B = params_alg(num_vertices, sketches_factor, cube)
+        self.C = samples * self.cps
+        self.nb = self.C * self.B + 1
+        self.sketch_bytes = self.nb * 12
         self.data = np.zeros(num_vertices * self.sketch_bytes, np.uint8)
 
     def apply_records(self, raw: np.ndarray, vertex_filter: np.ndarray | None = None) -> int:
@@ -104,8 +127,9 @@ class OracleSketches:
         if vertex_filter is not None:
             vertex_filter = np.ascontiguousarray(vertex_filter, np.uint8)
             filt = _p(vertex_filter, ctypes.c_uint8)
-        return lib().gzo_apply_records(_p(self.data, ctypes.c_uint8), self.V, self.C, self.B,
-                                       self.seed, _p(raw, ctypes.c_uint8), raw.size // 9, filt)
+        return lib().gzo_apply_records_alg(_p(self.data, ctypes.c_uint8), self.V, self.C, self.B,
+                                           self.seed, _p(raw, ctypes.c_uint8), raw.size // 9, filt,
+                                           int(self.cube))
 
     def apply_batch(self, src: int, dsts) -> int:
         d = np.ascontiguousarray(dsts, np.uint32)
@@ -122,9 +146,9 @@ class OracleSketches:
         cap = self.V * (self.C + 1) if with_trace else 0
         trace = np.zeros(cap, TRACE_DTYPE)
         tl = ctypes.c_size_t()
-        rc = lib().gzo_boruvka(_p(self.data, ctypes.c_uint8), self.V, self.C, self.B, self.seed,
-                               _p(labels, ctypes.c_uint32), ctypes.byref(rounds),
-                               trace.ctypes.data if with_trace else None, cap, ctypes.byref(tl))
+        rc = lib().gzo_boruvka_alg(_p(self.data, ctypes.c_uint8), self.V, self.C, self.B, self.cps,
+                                   self.seed, _p(labels, ctypes.c_uint32), ctypes.byref(rounds),
+                                   trace.ctypes.data if with_trace else None, cap, ctypes.byref(tl))
         return rc, labels, rounds.value, trace[:min(tl.value, cap)]
 
     def dump_bytes(self) -> bytes:
@@ -161,21 +185,26 @@ def have_reference() -> bool:
     return os.path.exists(REF_NOEAGER) and os.path.exists(REF_EAGER)
 
 
+def have_cube_reference() -> bool:
+    return os.path.exists(REF_CUBE)
+
+
 def ref_ingest(stream_path: str, seed: int, sketches_factor: float = 1.0, threads: int = 1,
                eager: bool = False, max_records: int = 0, dump_path: str | None = None,
-               labels_path: str | None = None, timeout: float | None = None) -> dict:
-    exe = REF_EAGER if eager else REF_NOEAGER
+               labels_path: str | None = None, timeout: float | None = None,
+               cube: bool = False) -> dict:
+    exe = REF_CUBE if cube else (REF_EAGER if eager else REF_NOEAGER)
     out = subprocess.run([exe, "ingest", stream_path, str(seed), repr(float(sketches_factor)),
                           str(threads), str(max_records), dump_path or "-", labels_path or "-"],
                          check=True, capture_output=True, text=True, timeout=timeout)
     return json.loads(out.stdout.strip().splitlines()[-1])
 
 
-def ref_trace(dump_path: str):
+def ref_trace(dump_path: str, cube: bool = False):
     """Boruvka trace from the reference's own Sketch code: (info, labels, trace)."""
     with tempfile.TemporaryDirectory() as td:
         tp, lp = os.path.join(td, "trace.bin"), os.path.join(td, "labels.bin")
-        out = subprocess.run([REF_NOEAGER, "trace", dump_path, tp, lp], check=True,
+        out = subprocess.run([REF_CUBE if cube else REF_NOEAGER, "trace", dump_path, tp, lp], check=True,
                              capture_output=True, text=True)
         info = json.loads(out.stdout.strip().splitlines()[-1])
         return info, np.fromfile(lp, np.uint32), np.fromfile(tp, TRACE_DTYPE)
