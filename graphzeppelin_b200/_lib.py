@@ -24,6 +24,8 @@ GZ_ERR_TIMEOUT = 8
 GZ_ERR_BAD_SAMPLE = 9
 GZ_ERR_NO_DEVICE = 10
 GZ_ERR_BUDGET = 11
+GZ_CAMEO_SKETCH = 0
+GZ_CUBE_SKETCH = 1
 
 
 class gz_params_t(ctypes.Structure):
@@ -33,7 +35,9 @@ class gz_params_t(ctypes.Structure):
                 ("desired_updates_per_batch", ctypes.c_uint64), ("max_rounds", ctypes.c_uint64),
                 ("sketches_factor", ctypes.c_double), ("batch_factor", ctypes.c_double),
                 ("vertices_per_tile", ctypes.c_uint32), ("num_tiles", ctypes.c_uint32),
-                ("vertices_per_bin", ctypes.c_uint32), ("num_bins", ctypes.c_uint32)]
+                ("vertices_per_bin", ctypes.c_uint32), ("num_bins", ctypes.c_uint32),
+                ("cols_per_sample", ctypes.c_uint32), ("sketch_algorithm", ctypes.c_uint32),
+                ("in_place", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
 
 class gz_trace_rec_t(ctypes.Structure):
@@ -58,6 +62,8 @@ SIGNATURES = [
     ("gz_last_error", ctypes.c_char_p, []),
     ("gz_create", _i, [_u32, _u64, _d, _d, ctypes.POINTER(_H)]),
     ("gz_create_from_serialized", _i, [ctypes.c_char_p, _d, ctypes.POINTER(_H)]),
+    ("gz_create_ex", _i, [_u32, _u64, _d, _d, _i, ctypes.POINTER(_H)]),
+    ("gz_create_from_serialized_ex", _i, [ctypes.c_char_p, _d, _i, ctypes.POINTER(_H)]),
     ("gz_destroy", _i, [_H]),
     ("gz_get_params", _i, [_H, ctypes.POINTER(gz_params_t)]),
     ("gz_set_gutter_capacity", _i, [_H, _u64]),

@@ -269,15 +269,20 @@ class CCSketchAlg:
     run device Boruvka. The cached-query behaviour is that of the reference built with
     NO_EAGER_DSU: any update invalidates it."""
 
+    SKETCH_ALGORITHMS = {"cameo": _lib.GZ_CAMEO_SKETCH, "cube": _lib.GZ_CUBE_SKETCH}
+
     def __init__(self, num_vertices: int, seed: int, config: CCAlgConfiguration | None = None,
-                 _handle=None):
+                 _handle=None, sketch_algorithm: str = "cameo"):
+        """sketch_algorithm: "cameo" (CameoSketch, the reference's default build) or "cube"
+        (CubeSketch, the reference built with -DL0_SAMPLING)."""
         self.lib = _lib.load()
         self.config = config or CCAlgConfiguration()
         if _handle is None:
             h = ctypes.c_void_p()
-            _check(self.lib.gz_create(num_vertices, seed & (2**64 - 1),
-                                      self.config.get_sketches_factor(),
-                                      self.config.get_batch_factor(), ctypes.byref(h)))
+            _check(self.lib.gz_create_ex(num_vertices, seed & (2**64 - 1),
+                                         self.config.get_sketches_factor(),
+                                         self.config.get_batch_factor(),
+                                         self.SKETCH_ALGORITHMS[sketch_algorithm], ctypes.byref(h)))
             _handle = h
         self._h = _handle
         p = _lib.gz_params_t()
@@ -288,13 +293,15 @@ class CCSketchAlg:
     # -- construction / teardown ---------------------------------------------------------------
     @classmethod
     def construct_from_serialized_data(cls, input_file: str,
-                                       config: CCAlgConfiguration | None = None) -> "CCSketchAlg":
+                                       config: CCAlgConfiguration | None = None,
+                                       sketch_algorithm: str = "cameo") -> "CCSketchAlg":
         """src/cc_sketch_alg.cpp:30-43 (the file's sketches_factor replaces the config's)."""
         lib = _lib.load()
         config = config or CCAlgConfiguration()
         h = ctypes.c_void_p()
-        _check(lib.gz_create_from_serialized(input_file.encode(), config.get_batch_factor(),
-                                             ctypes.byref(h)))
+        _check(lib.gz_create_from_serialized_ex(input_file.encode(), config.get_batch_factor(),
+                                                cls.SKETCH_ALGORITHMS[sketch_algorithm],
+                                                ctypes.byref(h)))
         obj = cls.__new__(cls)
         p = _lib.gz_params_t()
         _check(lib.gz_get_params(h, ctypes.byref(p)))

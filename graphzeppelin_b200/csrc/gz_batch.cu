@@ -1439,6 +1439,7 @@ int gz_batch_get_params(gz_batch_t *h, uint32_t graph, gz_params_t *o) {
   o->num_tiles = gd.ntiles;
   o->vertices_per_bin = 1u << gd.bin_shift;
   o->num_bins = gd.nbins;
+  o->cols_per_sample = 1;
   return GZ_OK;
 }
 
@@ -1999,6 +2000,7 @@ int gz_server_get_params(gz_server_t *s, uint32_t tenant, gz_params_t *o) {
   o->num_tiles = gd.ntiles;
   o->vertices_per_bin = 1u << gd.bin_shift;
   o->num_bins = gd.nbins;
+  o->cols_per_sample = 1;
   return GZ_OK;
 }
 

@@ -86,6 +86,22 @@ namespace gz {
 // (src/cc_sketch_alg.cpp:16-17; include/sketch.h:62-76, :181, :188-190) evaluated with the same
 // double expressions so the results agree bit for bit: B = ceil(log2(V(V-1)/2)) + 1 buckets per
 // column, C = max(18, ceil(f * log2(V) / (1 - log2(1.2)))) columns.
+// CubeSketch (the reference built with -DL0_SAMPLING, include/sketch.h:183-190) takes 7 columns per
+// sample and num_samples_div = log2(3) - 1; CameoSketch 1 column.
+void sketch_sizing_alg(uint32_t V, double f, bool cube, uint32_t &samples, uint32_t &cps, uint32_t &B) {
+  if (!cube) {
+    sketch_sizing(V, f, samples, B);
+    cps = 1;
+    return;
+  }
+  const uint64_t vec_len = (uint64_t)std::ceil(double(V) * (uint32_t)(V - 1) / 2);
+  B = (uint32_t)(std::ceil(std::log2((double)vec_len)) + 1);
+  const double num_samples_div = std::log2(3) - 1;
+  const size_t s = (size_t)std::ceil(f * std::log2((double)V) / num_samples_div);
+  samples = (uint32_t)std::max<size_t>(18, s);
+  cps = 7;
+}
+
 void sketch_sizing(uint32_t V, double f, uint32_t &C, uint32_t &B) {
   const uint64_t vec_len = (uint64_t)std::ceil(double(V) * (uint32_t)(V - 1) / 2);
   B = (uint32_t)(std::ceil(std::log2((double)vec_len)) + 1);
@@ -103,6 +119,10 @@ struct gz_alg {
   int device = 0;
   // configuration
   uint32_t V = 0, C = 0, B = 0, nb = 0;
+  // CubeSketch (L0_SAMPLING) or CameoSketch: samples of cps columns each (C = samples * cps)
+  bool cube = false;
+  uint32_t samples = 0, cps = 1;
+  bool in_place = false;  // sketches too large to stage 4 in shared memory: updated in HBM
   uint64_t seed = 0;
   double sketches_factor = 1, batch_factor = 1;
   uint64_t sketch_bytes = 0, desired_batch = 0;
@@ -179,6 +199,7 @@ struct gz_alg {
     g.ntiles = ntiles;
     g.bin_shift = bin_shift;
     g.nbins = nbins;
+    g.cube = cube ? 1 : 0;
     return g;
   }
   gz::GutterGeom ggeom() const { return gz::GutterGeom{V, bin_shift, nbins}; }
@@ -190,6 +211,7 @@ struct gz_alg {
     g.sketch_words = nb * 3;
     g.flip_chk = gz::xxh3_flip(seed);
     g.span = 64;
+    g.cps = cps;
     return g;
   }
 
@@ -266,8 +288,12 @@ int choose_tiling(gz_alg *h, uint32_t vpt_req, uint32_t threads_req, uint32_t tp
     while (shift < 6 && (1ull << (shift + 1)) <= want &&
            (h->sketch_bytes << (shift + 1)) + flip_bytes <= budget)
       ++shift;
-    if ((h->sketch_bytes << shift) + flip_bytes > budget)
-      return fail(GZ_ERR_INVALID, "sketch too large to stage 4 vertices in shared memory");
+    if ((h->sketch_bytes << shift) + flip_bytes > budget) {
+      // not even 4 vertex sketches fit a tile (CubeSketch at large V): updates go straight to
+      // HBM, hashed once per record (apply_in_place)
+      h->in_place = true;
+      shift = 2;
+    }
   }
   h->tile_shift = shift;
   h->ntiles = (uint32_t)((h->V + (1u << shift) - 1) >> shift);
@@ -288,19 +314,22 @@ int choose_tiling(gz_alg *h, uint32_t vpt_req, uint32_t threads_req, uint32_t tp
       return fail(GZ_ERR_INVALID, "threads_per_block must be a multiple of 32 in [64, 1024]");
     h->threads = threads_req;
   }
+  if (h->in_place) return GZ_OK;
   cudaError_t e = gz::sketch_update_prepare(h->sgeom(), h->threads);
   if (e != cudaSuccess) return fail(GZ_ERR_CUDA, cudaGetErrorString(e));
   return GZ_OK;
 }
 
-int init_alg(gz_alg *h, uint32_t V, uint64_t seed, double sf, double bf) {
+int init_alg(gz_alg *h, uint32_t V, uint64_t seed, double sf, double bf, bool cube) {
   if (V < 2 || V > (1u << 31)) return fail(GZ_ERR_INVALID, "num_vertices must be in [2, 2^31]");
   GZ_CUDA(cudaGetDevice(&h->device));
   h->V = V;
   h->seed = seed;
   h->sketches_factor = sf > 0 ? sf : 1;  // CCAlgConfiguration::sketches_factor
   h->batch_factor = bf > 0 ? bf : 1;     // CCAlgConfiguration::batch_factor
-  gz::sketch_sizing(V, h->sketches_factor, h->C, h->B);
+  h->cube = cube;
+  gz::sketch_sizing_alg(V, h->sketches_factor, cube, h->samples, h->cps, h->B);
+  h->C = h->samples * h->cps;
   if (h->B > 63) return fail(GZ_ERR_INVALID, "bkt_per_col above 63 is not supported");
   h->hashed_default = false;  // plain entries measured faster on B200 (see the design notes)
   h->hashed = h->hashed_default;
@@ -438,6 +467,12 @@ int apply_pending(gz_alg *h) {
 // Counting-sort n inputs (records or entries, device memory) into a new gutter chunk.
 int gutter_chunk(gz_alg *h, int input, const void *d_in, uint64_t n) {
   if (n == 0) return GZ_OK;
+  if (h->in_place) {
+    const int pi = h->prof_begin();
+    GZ_CUDA(gz::apply_in_place(input, d_in, n, h->sgeom(), h->d_sk, h->d_flip, h->d_status, h->stream));
+    h->prof_end(pi, 1);
+    return GZ_OK;
+  }
   const uint64_t per = input == gz::kInputRecords ? 2 : 1;
   const uint64_t esz = entry_bytes(h, input);
   GZ_TRY(ensure_gutter(h));
@@ -642,7 +677,7 @@ int ensure_query(gz_alg *h) {
   GZ_TRY(dev_alloc(&b.comp_start, V + 1));
   GZ_TRY(dev_alloc(&b.comp_key, V));
   GZ_TRY(dev_alloc(&b.ncomp, 1));
-  GZ_TRY(dev_alloc(&b.acc, V * (h->B + 1) * 3));
+  GZ_TRY(dev_alloc(&b.acc, V * (h->cps * h->B + 1) * 3));
   GZ_TRY(dev_alloc(&b.flags, 4));
   GZ_TRY(dev_alloc(&b.forest, V));
   GZ_TRY(dev_alloc(&b.forest_n, 1));
@@ -688,12 +723,12 @@ int run_boruvka(gz_alg *h) {
   uint32_t round = 0;
   while (modified) {
     ++round;
-    if (round >= h->C) {
+    if (round >= h->samples) {
       h->prof_end(pi, 2);
       h->last_rounds = round;
       return fail(GZ_ERR_OUT_OF_SAMPLES,
                   "This sketch (seed=" + std::to_string(h->seed) + ", max samples=" +
-                      std::to_string(h->C) + ") cannot be sampled more times (cur idx=" +
+                      std::to_string(h->samples) + ") cannot be sampled more times (cur idx=" +
                       std::to_string(round) + ")!");
     }
     GZ_CUDA(cudaMemsetAsync(b.flags, 0, sizeof(uint32_t), h->stream));
@@ -797,13 +832,21 @@ const char *gz_last_error(void) { return g_last_error.c_str(); }
 
 int gz_create(uint32_t num_vertices, uint64_t seed, double sketches_factor, double batch_factor,
               gz_alg_t **out) {
+  return gz_create_ex(num_vertices, seed, sketches_factor, batch_factor, GZ_CAMEO_SKETCH, out);
+}
+
+int gz_create_ex(uint32_t num_vertices, uint64_t seed, double sketches_factor, double batch_factor,
+                 int sketch_algorithm, gz_alg_t **out) {
   if (!out) return fail(GZ_ERR_INVALID, "out is null");
+  if (sketch_algorithm != GZ_CAMEO_SKETCH && sketch_algorithm != GZ_CUBE_SKETCH)
+    return fail(GZ_ERR_INVALID, "sketch_algorithm must be GZ_CAMEO_SKETCH or GZ_CUBE_SKETCH");
   *out = nullptr;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return fail(GZ_ERR_NO_DEVICE, "no CUDA device is available (this library has no CPU path)");
   gz_alg *h = new gz_alg();
-  const int rc = init_alg(h, num_vertices, seed, sketches_factor, batch_factor);
+  const int rc = init_alg(h, num_vertices, seed, sketches_factor, batch_factor,
+                          sketch_algorithm == GZ_CUBE_SKETCH);
   if (rc != GZ_OK) {
     destroy_alg(h);
     delete h;
@@ -814,6 +857,11 @@ int gz_create(uint32_t num_vertices, uint64_t seed, double sketches_factor, doub
 }
 
 int gz_create_from_serialized(const char *path, double batch_factor, gz_alg_t **out) {
+  return gz_create_from_serialized_ex(path, batch_factor, GZ_CAMEO_SKETCH, out);
+}
+
+int gz_create_from_serialized_ex(const char *path, double batch_factor, int sketch_algorithm,
+                                 gz_alg_t **out) {
   if (!path || !out) return fail(GZ_ERR_INVALID, "null argument");
   *out = nullptr;
   FILE *f = fopen(path, "rb");
@@ -826,7 +874,7 @@ int gz_create_from_serialized(const char *path, double batch_factor, gz_alg_t **
     return fail(GZ_ERR_IO, "truncated header");
   }
   gz_alg_t *h = nullptr;
-  int rc = gz_create(V, seed, sf, batch_factor, &h);
+  int rc = gz_create_ex(V, seed, sf, batch_factor, sketch_algorithm, &h);
   if (rc != GZ_OK) {
     fclose(f);
     return rc;
@@ -865,13 +913,16 @@ int gz_get_params(const gz_alg_t *h, gz_params_t *o) {
   o->seed = h->seed;
   o->sketch_bytes = h->sketch_bytes;
   o->desired_updates_per_batch = h->desired_batch;
-  o->max_rounds = h->C;
+  o->max_rounds = h->samples;
   o->sketches_factor = h->sketches_factor;
   o->batch_factor = h->batch_factor;
   o->vertices_per_tile = 1u << h->tile_shift;
   o->num_tiles = h->ntiles;
   o->vertices_per_bin = 1u << h->bin_shift;
   o->num_bins = h->nbins;
+  o->cols_per_sample = h->cps;
+  o->sketch_algorithm = h->cube ? GZ_CUBE_SKETCH : GZ_CAMEO_SKETCH;
+  o->in_place = h->in_place ? 1 : 0;
   return GZ_OK;
 }
 
@@ -1257,8 +1308,10 @@ int gz_set_tuning(gz_alg_t *h, uint32_t vpt, uint32_t threads, uint32_t tiles_pe
                   uint32_t entry_form) {
   if (!h) return fail(GZ_ERR_INVALID, "null handle");
   if (entry_form > 2) return fail(GZ_ERR_INVALID, "entry_form must be 0, 1 or 2");
-  if (entry_form == 2 && h->C > gz::kHashedMaxColumns)
-    return fail(GZ_ERR_INVALID, "hashed entries need at most 32 columns");
+  if (entry_form == 2 && (h->C > gz::kHashedMaxColumns || h->cube))
+    return fail(GZ_ERR_INVALID, "hashed entries need CameoSketch with at most 32 columns");
+  if (h->in_place && (vpt || threads || tiles_per_bin || entry_form == 2))
+    return fail(GZ_ERR_INVALID, "this handle updates its sketches in place: there are no tiles to tune");
   Guard g(h);
   GZ_TRY(push_staged_entries(h));
   GZ_TRY(apply_pending(h));

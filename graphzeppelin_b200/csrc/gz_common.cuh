@@ -219,6 +219,85 @@ __device__ __forceinline__ void apply_entry_global(uint2 e, uint32_t *gsk, uint3
 }
 
 
+// CubeSketch update (src/sketch.cpp:50-67, the reference built with -DL0_SAMPLING): the
+// deterministic bucket, then in each column every bucket of depth 0..d when d < B.
+__device__ __forceinline__ void apply_entry_cube(uint2 e, uint32_t *sk_base, uint32_t vmask,
+                                                 uint32_t sketch_words, const uint64_t *s_flip,
+                                                 uint64_t flip_chk, uint32_t C, uint32_t B) {
+  const uint32_t v = e.x, w = e.y;
+  const uint32_t lo = max(v, w), hi = min(v, w);
+  uint32_t *sk = sk_base + (uint64_t)(v & vmask) * sketch_words;
+  const uint64_t in64 = ((uint64_t)lo << 32) | hi;
+  const uint32_t chk = hash_lo32(in64 ^ flip_chk);
+  xor_bucket(sk + 3 * C * B, lo, hi, chk);
+  for (uint32_t c = 0; c < C; ++c) {
+    const uint32_t d = hash_depth(in64 ^ s_flip[c], B);
+    if (d < B)
+      for (uint32_t j = 0; j <= d; ++j) xor_bucket(sk + 3 * (c * B + j), lo, hi, chk);
+  }
+}
+
+// One update (u, v) XORed in place (global memory) into the sketch su of u and, when sv is not
+// null, into the sketch sv of v; hashed once, since the checksum and each column's depth are
+// the same for both endpoints. CUBE selects the CubeSketch rule (depths 0..d) over
+// CameoSketch's (depth d).
+template <bool CUBE>
+__device__ __forceinline__ void xor_update_in_place(uint32_t *su, uint32_t *sv, uint32_t u, uint32_t v,
+                                                    const uint64_t *s_flip, uint64_t flip_chk,
+                                                    uint32_t C, uint32_t B) {
+  const uint32_t lo = max(u, v), hi = min(u, v);
+  const uint64_t in64 = ((uint64_t)lo << 32) | hi;
+  const uint32_t chk = hash_lo32(in64 ^ flip_chk);
+  xor_bucket(su + 3 * C * B, lo, hi, chk);
+  if (sv) xor_bucket(sv + 3 * C * B, lo, hi, chk);
+  for (uint32_t c = 0; c < C; ++c) {
+    const uint32_t d = hash_depth(in64 ^ s_flip[c], B);
+    if (d < B) {
+      for (uint32_t j = CUBE ? 0 : d; j <= d; ++j) {
+        xor_bucket(su + 3 * (c * B + j), lo, hi, chk);
+        if (sv) xor_bucket(sv + 3 * (c * B + j), lo, hi, chk);
+      }
+    }
+  }
+}
+
+// warp_sample over NC columns merged in registers (lane j holds buckets j and j + 32 of each
+// column): the deterministic bucket, then columns 0..NC-1 in order, depths 0..B-1 in each --
+// Sketch::sample's scan over a sample's columns (src/sketch.cpp:94-116).
+template <int NC>
+__device__ __forceinline__ int warp_sample_cols(const uint32_t (&d)[3], const uint32_t (&a)[NC][2][3],
+                                                uint32_t B, uint64_t flip_chk, uint64_t *idx) {
+  const int lane = threadIdx.x & 31;
+  if ((d[0] | d[1] | d[2]) == 0) {
+    *idx = 0;
+    return 1;  // ZERO
+  }
+  if (bucket_good(d[0], d[1], d[2], flip_chk)) {
+    *idx = ((uint64_t)d[1] << 32) | d[0];
+    return 0;  // GOOD
+  }
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+      if ((uint32_t)s * 32 >= B) break;
+      const uint32_t j = s * 32 + lane;
+      const bool good = j < B && bucket_good(a[c][s][0], a[c][s][1], a[c][s][2], flip_chk);
+      const uint32_t m = __ballot_sync(kFull, good);
+      if (m) {
+        const int src = __ffs(m) - 1;
+        const uint32_t x0 = __shfl_sync(kFull, a[c][s][0], src);
+        const uint32_t x1 = __shfl_sync(kFull, a[c][s][1], src);
+        *idx = ((uint64_t)x1 << 32) | x0;
+        return 0;
+      }
+    }
+  }
+  *idx = 0;
+  return 2;  // FAIL
+}
+
+
 struct TraceRec {
   uint32_t round, key, result, pad;
   uint64_t idx;

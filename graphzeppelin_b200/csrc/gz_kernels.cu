@@ -464,6 +464,9 @@ __device__ __forceinline__ void apply_any(const uint8_t *cb, int kind, uint64_t 
   if (HASHED && kind == kEntryHashed) {
     const uint4 *E = reinterpret_cast<const uint4 *>(cb);
     apply_hashed(E[2 * i], E[2 * i + 1], s_sk, vmask, g.sketch_words, s_flip, g.C, g.B);
+  } else if (g.cube) {
+    apply_entry_cube(reinterpret_cast<const uint2 *>(cb)[i], s_sk, vmask, g.sketch_words, s_flip,
+                     flip_chk, g.C, g.B);
   } else {
     apply_entry(reinterpret_cast<const uint2 *>(cb)[i], s_sk, vmask, g.sketch_words, s_flip,
                 flip_chk, g.C, g.B);
@@ -578,6 +581,53 @@ k_sketch_update(SketchGeom g, uint8_t *__restrict__ sketches, const uint8_t *__r
   if (threadIdx.x == 0) bulk_wait_all();
 }
 
+template <int INPUT, bool CUBE>
+__global__ void __launch_bounds__(512)
+k_in_place(const void *__restrict__ in, uint64_t n, SketchGeom g, uint32_t *__restrict__ sk_words,
+           const uint64_t *__restrict__ flip, uint32_t *__restrict__ status) {
+  extern __shared__ __align__(16) uint8_t ism[];
+  uint64_t *s_flip = reinterpret_cast<uint64_t *>(ism);
+  for (uint32_t i = threadIdx.x; i <= g.C; i += blockDim.x) s_flip[i] = flip[i];
+  __syncthreads();
+  const uint64_t flip_chk = s_flip[g.C];
+  bool bad = false;
+  if (INPUT == kInputRecords) {
+    uint8_t *s_rec = ism + (((size_t)g.C + 2) & ~(size_t)1) * 8;
+    const uint8_t *rec = reinterpret_cast<const uint8_t *>(in);
+    for (uint64_t t = (uint64_t)blockIdx.x * kRecTile; t < n; t += (uint64_t)gridDim.x * kRecTile) {
+      const uint32_t cnt = (uint32_t)(n - t < (uint64_t)kRecTile ? n - t : (uint64_t)kRecTile);
+      const uint32_t shift = stage_records(rec, t, cnt, s_rec);
+      __syncthreads();
+      for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
+        uint32_t u, v;
+        parse_record(s_rec, shift, i, u, v);
+        if (u >= g.V || v >= g.V) {
+          bad = true;
+          continue;
+        }
+        if (u == v) continue;  // both endpoint updates land in one sketch and cancel
+        xor_update_in_place<CUBE>(sk_words + (uint64_t)u * g.sketch_words,
+                                  sk_words + (uint64_t)v * g.sketch_words, u, v, s_flip, flip_chk,
+                                  g.C, g.B);
+      }
+      __syncthreads();
+    }
+  } else {
+    const uint2 *e = reinterpret_cast<const uint2 *>(in);
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+      const uint2 x = e[i];
+      if (x.x >= g.V || x.y >= g.V) {
+        bad = true;
+        continue;
+      }
+      xor_update_in_place<CUBE>(sk_words + (uint64_t)x.x * g.sketch_words, nullptr, x.x, x.y, s_flip,
+                                flip_chk, g.C, g.B);
+    }
+  }
+  if (bad) atomicOr(status, kStatusBadVertex);
+}
+
 __global__ void k_sketch_xor_raw(uint32_t *sketches, uint32_t words, uint32_t v,
                                  const uint32_t *raw) {
   uint32_t *sk = sketches + (uint64_t)v * words;
@@ -626,20 +676,26 @@ __global__ void k_bv_reset(uint32_t V, uint32_t *parent) {
 }
 
 // Round 0 (run_round_zero, src/cc_sketch_alg.cpp:223-244): every vertex is its own component.
+// Round 0 (run_round_zero, src/cc_sketch_alg.cpp:223-244): every vertex sketch samples its
+// sample 0 -- columns 0..CPS-1 and the deterministic bucket -- one warp per vertex.
+template <int CPS>
 __global__ void k_bv_round0(BoruvkaGeom g, const uint32_t *__restrict__ sk_words, BoruvkaBufs b) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < g.V; v += nwarps) {
     const uint32_t *sk = sk_words + (uint64_t)v * g.sketch_words;
-    uint32_t d[3], a[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    uint32_t d[3], a[CPS][2][3];
     load_bucket(sk + 3 * g.C * g.B, d);
 #pragma unroll
-    for (int s = 0; s < 2; ++s) {
-      const uint32_t j = s * 32 + lane;
-      if (j < g.B) load_bucket(sk + 3 * j, a[s]);
-    }
+    for (int c = 0; c < CPS; ++c)
+#pragma unroll
+      for (int s = 0; s < 2; ++s) {
+        const uint32_t j = s * 32 + lane;
+        a[c][s][0] = a[c][s][1] = a[c][s][2] = 0;
+        if (j < g.B) load_bucket(sk + 3 * (c * g.B + j), a[c][s]);
+      }
     uint64_t idx;
-    const int res = warp_sample(d, a, g.B, g.flip_chk, &idx);
+    const int res = warp_sample_cols<CPS>(d, a, g.B, g.flip_chk, &idx);
     if (lane == 0) handle_result(res, idx, 0, v, g, b);
   }
 }
@@ -663,7 +719,7 @@ __global__ void k_bv_pack(uint32_t V, const uint32_t *cnt, uint64_t *packed) {
 
 // create_merge_instructions (src/cc_sketch_alg.cpp:382-462): group vertices by root so each
 // component's members are contiguous in `order`.
-__global__ void k_bv_group(uint32_t V, uint32_t B, uint32_t span, const uint32_t *label,
+__global__ void k_bv_group(uint32_t V, uint32_t acc_words, uint32_t span, const uint32_t *label,
                            const uint64_t *packed, const uint64_t *total, const uint32_t *cnt,
                            uint32_t *fill, const uint32_t *minv, uint32_t *order,
                            uint32_t *order_comp, uint32_t *comp_start, uint32_t *comp_key,
@@ -681,8 +737,8 @@ __global__ void k_bv_group(uint32_t V, uint32_t B, uint32_t span, const uint32_t
     comp_key[c] = minv ? minv[r] : r;
     const uint32_t end = start + cnt[r];
     if (start / span != (end - 1) / span) {
-      uint32_t *ac = acc + (uint64_t)c * (B + 1) * 3;
-      for (uint32_t i = 0; i < (B + 1) * 3; ++i) ac[i] = 0;
+      uint32_t *ac = acc + (uint64_t)c * acc_words;
+      for (uint32_t i = 0; i < acc_words; ++i) ac[i] = 0;
     }
   }
   if (v == 0) {
@@ -693,8 +749,10 @@ __global__ void k_bv_group(uint32_t V, uint32_t B, uint32_t span, const uint32_t
 }
 
 // perform_boruvka_round (src/cc_sketch_alg.cpp:246-380) for round >= 1: each warp XOR-merges
-// column `round` + the deterministic bucket over `span` consecutive grouped members; components
-// wholly inside the span are sampled right here, the rest are combined in acc.
+// sample `round` (columns round*CPS .. +CPS) + the deterministic bucket over `span` consecutive
+// grouped members; components wholly inside the span are sampled right here, the rest are
+// combined in acc (per component: CPS*B column buckets, then the deterministic one).
+template <int CPS>
 __global__ void k_bv_merge(BoruvkaGeom g, uint32_t round, const uint32_t *__restrict__ sk_words,
                            BoruvkaBufs b) {
   const uint32_t lane = threadIdx.x & 31;
@@ -702,53 +760,65 @@ __global__ void k_bv_merge(BoruvkaGeom g, uint32_t round, const uint32_t *__rest
   const uint64_t p0 = (uint64_t)w * g.span;
   if (p0 >= g.V) return;
   const uint32_t p1 = (uint32_t)(p0 + g.span < (uint64_t)g.V ? p0 + g.span : (uint64_t)g.V);
-  const uint32_t col = 3 * round * g.B, detw = 3 * g.C * g.B;
-  uint32_t a[2][3] = {{0, 0, 0}, {0, 0, 0}}, d[3] = {0, 0, 0};
+  const uint32_t col = 3 * round * CPS * g.B, detw = 3 * g.C * g.B;
+  const uint32_t acc_words = (CPS * g.B + 1) * 3;
+  uint32_t a[CPS][2][3], d[3] = {0, 0, 0};
+#pragma unroll
+  for (int c = 0; c < CPS; ++c)
+#pragma unroll
+    for (int q = 0; q < 2; ++q) a[c][q][0] = a[c][q][1] = a[c][q][2] = 0;
   uint32_t cur = b.order_comp[p0];
-  auto flush = [&](uint32_t c) {
-    const uint32_t s = b.comp_start[c], e = b.comp_start[c + 1];
+  auto flush = [&](uint32_t comp) {
+    const uint32_t s = b.comp_start[comp], e = b.comp_start[comp + 1];
     if (s >= p0 && e <= p1) {
       uint64_t idx;
-      const int res = warp_sample(d, a, g.B, g.flip_chk, &idx);
-      if (lane == 0) handle_result(res, idx, round, b.comp_key[c], g, b);
+      const int res = warp_sample_cols<CPS>(d, a, g.B, g.flip_chk, &idx);
+      if (lane == 0) handle_result(res, idx, round, b.comp_key[comp], g, b);
     } else {
-      uint32_t *ac = b.acc + (uint64_t)c * (g.B + 1) * 3;
+      uint32_t *ac = b.acc + (uint64_t)comp * acc_words;
 #pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        const uint32_t j = q * 32 + lane;
-        if (j < g.B) {
-          atomicXor(ac + 3 * j, a[q][0]);
-          atomicXor(ac + 3 * j + 1, a[q][1]);
-          atomicXor(ac + 3 * j + 2, a[q][2]);
+      for (int c = 0; c < CPS; ++c)
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          const uint32_t j = q * 32 + lane;
+          if (j < g.B) {
+            uint32_t *bk = ac + 3 * (c * g.B + j);
+            atomicXor(bk, a[c][q][0]);
+            atomicXor(bk + 1, a[c][q][1]);
+            atomicXor(bk + 2, a[c][q][2]);
+          }
         }
-      }
       if (lane == 0) {
-        atomicXor(ac + 3 * g.B, d[0]);
-        atomicXor(ac + 3 * g.B + 1, d[1]);
-        atomicXor(ac + 3 * g.B + 2, d[2]);
+        atomicXor(ac + 3 * CPS * g.B, d[0]);
+        atomicXor(ac + 3 * CPS * g.B + 1, d[1]);
+        atomicXor(ac + 3 * CPS * g.B + 2, d[2]);
       }
     }
   };
   for (uint32_t p = (uint32_t)p0; p < p1; ++p) {
-    const uint32_t c = b.order_comp[p];
-    if (c != cur) {
+    const uint32_t comp = b.order_comp[p];
+    if (comp != cur) {
       flush(cur);
-      cur = c;
+      cur = comp;
 #pragma unroll
-      for (int q = 0; q < 2; ++q) a[q][0] = a[q][1] = a[q][2] = 0;
+      for (int c = 0; c < CPS; ++c)
+#pragma unroll
+        for (int q = 0; q < 2; ++q) a[c][q][0] = a[c][q][1] = a[c][q][2] = 0;
       d[0] = d[1] = d[2] = 0;
     }
     const uint32_t *sk = sk_words + (uint64_t)b.order[p] * g.sketch_words;
 #pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      const uint32_t j = q * 32 + lane;
-      if (j < g.B) {
-        const uint32_t *bk = sk + col + 3 * j;
-        a[q][0] ^= bk[0];
-        a[q][1] ^= bk[1];
-        a[q][2] ^= bk[2];
+    for (int c = 0; c < CPS; ++c)
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const uint32_t j = q * 32 + lane;
+        if (j < g.B) {
+          const uint32_t *bk = sk + col + 3 * (c * g.B + j);
+          a[c][q][0] ^= bk[0];
+          a[c][q][1] ^= bk[1];
+          a[c][q][2] ^= bk[2];
+        }
       }
-    }
     d[0] ^= sk[detw];
     d[1] ^= sk[detw + 1];
     d[2] ^= sk[detw + 2];
@@ -756,30 +826,36 @@ __global__ void k_bv_merge(BoruvkaGeom g, uint32_t round, const uint32_t *__rest
   flush(cur);
 }
 
+template <int CPS>
 __global__ void k_bv_sample_spanning(BoruvkaGeom g, uint32_t round, BoruvkaBufs b) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   const uint32_t nc = *b.ncomp;
-  for (uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < nc; c += nwarps) {
-    const uint32_t s = b.comp_start[c], e = b.comp_start[c + 1];
+  const uint32_t acc_words = (CPS * g.B + 1) * 3;
+  for (uint32_t comp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; comp < nc; comp += nwarps) {
+    const uint32_t s = b.comp_start[comp], e = b.comp_start[comp + 1];
     if (s / g.span == (e - 1) / g.span) continue;
-    const uint32_t *ac = b.acc + (uint64_t)c * (g.B + 1) * 3;
-    uint32_t a[2][3] = {{0, 0, 0}, {0, 0, 0}}, d[3];
-    d[0] = __ldcg(ac + 3 * g.B);
-    d[1] = __ldcg(ac + 3 * g.B + 1);
-    d[2] = __ldcg(ac + 3 * g.B + 2);
+    const uint32_t *ac = b.acc + (uint64_t)comp * acc_words;
+    uint32_t a[CPS][2][3], d[3];
+    d[0] = __ldcg(ac + 3 * CPS * g.B);
+    d[1] = __ldcg(ac + 3 * CPS * g.B + 1);
+    d[2] = __ldcg(ac + 3 * CPS * g.B + 2);
 #pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      const uint32_t j = q * 32 + lane;
-      if (j < g.B) {
-        a[q][0] = __ldcg(ac + 3 * j);
-        a[q][1] = __ldcg(ac + 3 * j + 1);
-        a[q][2] = __ldcg(ac + 3 * j + 2);
+    for (int c = 0; c < CPS; ++c)
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const uint32_t j = q * 32 + lane;
+        a[c][q][0] = a[c][q][1] = a[c][q][2] = 0;
+        if (j < g.B) {
+          const uint32_t *bk = ac + 3 * (c * g.B + j);
+          a[c][q][0] = __ldcg(bk);
+          a[c][q][1] = __ldcg(bk + 1);
+          a[c][q][2] = __ldcg(bk + 2);
+        }
       }
-    }
     uint64_t idx;
-    const int res = warp_sample(d, a, g.B, g.flip_chk, &idx);
-    if (lane == 0) handle_result(res, idx, round, b.comp_key[c], g, b);
+    const int res = warp_sample_cols<CPS>(d, a, g.B, g.flip_chk, &idx);
+    if (lane == 0) handle_result(res, idx, round, b.comp_key[comp], g, b);
   }
 }
 
@@ -1049,6 +1125,28 @@ cudaError_t sketch_update(SketchGeom g, uint8_t *sketches, const uint8_t *gutter
   return cudaGetLastError();
 }
 
+cudaError_t apply_in_place(int input, const void *in, uint64_t n, SketchGeom g, uint8_t *sketches,
+                           const uint64_t *flip, uint32_t *status, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  const size_t flip_bytes = (((size_t)g.C + 2) & ~(size_t)1) * 8;
+  const size_t smem = flip_bytes + (input == kInputRecords ? kRecStageBytes : 0);
+  const uint64_t units = input == kInputRecords ? (n + kRecTile - 1) / kRecTile : (n + 511) / 512;
+  const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(units, (uint64_t)num_sms() * 4));
+  uint32_t *sk = reinterpret_cast<uint32_t *>(sketches);
+  auto launch = [&](auto kern) -> cudaError_t {
+    if (smem > 48 * 1024) {
+      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+    }
+    kern<<<grid, 512, smem, s>>>(in, n, g, sk, flip, status);
+    g_launches++;
+    return cudaGetLastError();
+  };
+  if (input == kInputRecords)
+    return g.cube ? launch(k_in_place<kInputRecords, true>) : launch(k_in_place<kInputRecords, false>);
+  return g.cube ? launch(k_in_place<kInputEntries, true>) : launch(k_in_place<kInputEntries, false>);
+}
+
 cudaError_t sketch_xor_raw(uint8_t *sketches, uint32_t words, uint32_t v, const uint32_t *raw,
                            cudaStream_t s) {
   k_sketch_xor_raw<<<blocks_for(words, 256), 256, 0, s>>>(reinterpret_cast<uint32_t *>(sketches),
@@ -1068,7 +1166,10 @@ cudaError_t boruvka_reset(const BoruvkaGeom &g, const BoruvkaBufs &b, cudaStream
 cudaError_t boruvka_round0(const BoruvkaGeom &g, const uint8_t *sketches, const BoruvkaBufs &b,
                            cudaStream_t s) {
   const unsigned blocks = std::min<unsigned>(blocks_for((uint64_t)g.V * 32, 256), num_sms() * 16);
-  k_bv_round0<<<blocks, 256, 0, s>>>(g, reinterpret_cast<const uint32_t *>(sketches), b);
+  const uint32_t *sk = reinterpret_cast<const uint32_t *>(sketches);
+  if (g.cps == 1) k_bv_round0<1><<<blocks, 256, 0, s>>>(g, sk, b);
+  else if (g.cps == 7) k_bv_round0<7><<<blocks, 256, 0, s>>>(g, sk, b);
+  else return cudaErrorInvalidValue;
   g_launches++;
   return cudaGetLastError();
 }
@@ -1086,17 +1187,20 @@ cudaError_t boruvka_round(const BoruvkaGeom &g, uint32_t round, const uint8_t *s
   g_launches++;
   cudaError_t e = scan_exclusive_u64(b.packed, V, b.scan_total, b.scan_tmp, s);
   if (e != cudaSuccess) return e;
-  k_bv_group<<<blocks_for(V, 256), 256, 0, s>>>(V, g.B, g.span, b.label, b.packed, b.scan_total,
+  if (g.cps != 1 && g.cps != 7) return cudaErrorInvalidValue;
+  k_bv_group<<<blocks_for(V, 256), 256, 0, s>>>(V, (g.cps * g.B + 1) * 3, g.span, b.label, b.packed, b.scan_total,
                                                  b.cnt, b.fill, trace ? b.minv : nullptr, b.order,
                                                  b.order_comp, b.comp_start, b.comp_key, b.ncomp,
                                                  b.acc);
   g_launches++;
   const uint64_t warps = (V + g.span - 1) / g.span;
-  k_bv_merge<<<blocks_for(warps * 32, 256), 256, 0, s>>>(
-      g, round, reinterpret_cast<const uint32_t *>(sketches), b);
-  g_launches++;
+  const uint32_t *sk = reinterpret_cast<const uint32_t *>(sketches);
   const unsigned sblocks = std::min<unsigned>(blocks_for((uint64_t)V * 32, 256), num_sms() * 16);
-  k_bv_sample_spanning<<<sblocks, 256, 0, s>>>(g, round, b);
+  if (g.cps == 1) k_bv_merge<1><<<blocks_for(warps * 32, 256), 256, 0, s>>>(g, round, sk, b);
+  else k_bv_merge<7><<<blocks_for(warps * 32, 256), 256, 0, s>>>(g, round, sk, b);
+  g_launches++;
+  if (g.cps == 1) k_bv_sample_spanning<1><<<sblocks, 256, 0, s>>>(g, round, b);
+  else k_bv_sample_spanning<7><<<sblocks, 256, 0, s>>>(g, round, b);
   g_launches++;
   return cudaGetLastError();
 }

@@ -50,6 +50,7 @@ struct SketchGeom {
   uint32_t ntiles;
   uint32_t bin_shift;          // gutter bin (>= tile_shift); a bin holds 1 << (bin - tile) tiles
   uint32_t nbins;
+  uint32_t cube = 0;           // CubeSketch update rule (every depth 0..d) instead of CameoSketch
 };
 
 // Records per staging tile of the gutter kernels, and the largest bin count for which the
@@ -120,6 +121,11 @@ cudaError_t sketch_update(SketchGeom g, uint8_t *sketches, const uint8_t *gutter
                           const uint64_t *flip, uint32_t *work_counter, uint32_t *status,
                           int grid, int threads, cudaStream_t s);
 // XOR num_buckets raw buckets (device) into the sketch of vertex v.
+// Updates applied in place in HBM, without staging (sketches too large for a shared-memory tile
+// of 4 vertices): records are hashed once and XORed into both endpoints' sketches, entries
+// {vertex, neighbour} into their vertex's sketch.
+cudaError_t apply_in_place(int input, const void *d_in, uint64_t n, SketchGeom g, uint8_t *sketches,
+                           const uint64_t *flip, uint32_t *status, cudaStream_t s);
 cudaError_t sketch_xor_raw(uint8_t *sketches, uint32_t sketch_words, uint32_t v,
                            const uint32_t *raw, cudaStream_t s);
 
@@ -151,7 +157,8 @@ struct BoruvkaBufs {
 struct BoruvkaGeom {
   uint32_t V, C, B, sketch_words;
   uint64_t flip_chk;
-  uint32_t span;  // members merged per warp
+  uint32_t span;     // members merged per warp
+  uint32_t cps = 1;  // columns per sample: round r merges and scans columns r*cps .. r*cps+cps-1
 };
 
 cudaError_t boruvka_reset(const BoruvkaGeom &g, const BoruvkaBufs &b, cudaStream_t s);
@@ -166,6 +173,8 @@ cudaError_t boruvka_final(const BoruvkaGeom &g, const BoruvkaBufs &b, uint32_t *
 int num_sms();
 // columns C and buckets per column B of one vertex sketch for V vertices and sketches factor f
 void sketch_sizing(uint32_t V, double f, uint32_t &C, uint32_t &B);
+// samples, columns per sample and B of CameoSketch (cube = false: C = samples) or CubeSketch
+void sketch_sizing_alg(uint32_t V, double f, bool cube, uint32_t &samples, uint32_t &cps, uint32_t &B);
 
 // Register-only hash throughput probe: n_threads * iters * 8 hashes.
 cudaError_t hash_peak(uint64_t seed, uint32_t iters, int blocks, int threads, uint64_t *out,

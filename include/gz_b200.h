@@ -53,6 +53,11 @@ enum gz_status {
 /* Query codes, reference enum QueryCode (include/cc_sketch_alg.h:60-63). */
 enum gz_query_code { GZ_CONNECTIVITY = 0, GZ_KSPANNINGFORESTS = 1 };
 
+/* Sketch algorithm: CameoSketch (the reference's default build) or CubeSketch (the reference
+ * built with -DL0_SAMPLING: 7 columns per sample, every depth 0..d updated, include/sketch.h:183-190,
+ * src/sketch.cpp:50-67). */
+enum gz_sketch_algorithm { GZ_CAMEO_SKETCH = 0, GZ_CUBE_SKETCH = 1 };
+
 /* Sample results, reference enum SampleResult (include/sketch.h:20-24). */
 enum gz_sample_result { GZ_SAMPLE_GOOD = 0, GZ_SAMPLE_ZERO = 1, GZ_SAMPLE_FAIL = 2 };
 
@@ -72,6 +77,10 @@ typedef struct gz_params {
   uint32_t num_tiles;
   uint32_t vertices_per_bin;    /* device gutter: vertices sharing one gutter bin */
   uint32_t num_bins;
+  uint32_t cols_per_sample;     /* Sketch::cols_per_sample: 1 (CameoSketch) or 7 (CubeSketch) */
+  uint32_t sketch_algorithm;    /* enum gz_sketch_algorithm */
+  uint32_t in_place;            /* 1: sketches too large to stage in shared memory are updated in HBM */
+  uint32_t reserved;
 } gz_params_t;
 
 /* One sampled component of one Boruvka round (parity tracing). key = smallest member id. */
@@ -110,9 +119,19 @@ GZ_API const char *gz_last_error(void);
 GZ_API int gz_create(uint32_t num_vertices, uint64_t seed, double sketches_factor, double batch_factor,
               gz_alg_t **out);
 
+/* gz_create with the sketch algorithm chosen at run time (the reference chooses it when it is
+ * compiled): GZ_CAMEO_SKETCH or GZ_CUBE_SKETCH. num_columns is then samples x cols_per_sample,
+ * and a query can run max_rounds = samples rounds. */
+GZ_API int gz_create_ex(uint32_t num_vertices, uint64_t seed, double sketches_factor,
+                        double batch_factor, int sketch_algorithm, gz_alg_t **out);
+
 /* CCSketchAlg::construct_from_serialized_data -- src/cc_sketch_alg.cpp:30-64. Reads a
  * write_binary file (u64 seed, u32 V, f64 sketches_factor, V sketches). The DSU starts invalid. */
 GZ_API int gz_create_from_serialized(const char *path, double batch_factor, gz_alg_t **out);
+/* Same, for a file written by a handle of the given sketch algorithm (the file format does not
+ * record it). */
+GZ_API int gz_create_from_serialized_ex(const char *path, double batch_factor, int sketch_algorithm,
+                                        gz_alg_t **out);
 
 /* ~CCSketchAlg -- src/cc_sketch_alg.cpp:66-77. */
 GZ_API int gz_destroy(gz_alg_t *alg);
