@@ -636,6 +636,125 @@ def run_serving(args):
     return line
 
 
+POWERLAW = dict(workload="powerlaw_v1048576_chunglu2.1_deg200_max16384_q10", num_vertices=1 << 20,
+                exponent=2.1, mean_degree=200.0, max_degree=1 << 14, stream_seed=2, queries=10,
+                sketch_seed=0x9E37)
+
+
+def run_powerlaw(args):
+    """Power-law graph with interleaved queries: a Chung-Lu stream (V = 2^20, exponent 2.1, mean
+    degree 200 after a 2^14 degree cap; shuffled inserts, deletes of 15% of them, re-inserts of
+    half of those) ingested in 10 segments with a connectivity query after each. Arm
+    "snapshot": each query runs on a device snapshot (gz_query_submit) while the next segment is
+    ingested. Arm "blocking": each query (gz_connected_components) stops ingest until it ends.
+    A step = clear + the whole stream with its 10 queries."""
+    import numpy as np
+    import torch
+
+    import graphzeppelin_b200 as gz
+    from graphzeppelin_b200 import streams as S
+
+    torch.cuda.set_device(0)
+    cfg = POWERLAW
+    V, Q = cfg["num_vertices"], cfg["queries"]
+    t = time.time()
+    probe = S.chung_lu_stream_fast(V, cfg["exponent"], cfg["mean_degree"], cfg["max_degree"],
+                                   cfg["stream_seed"])
+    n = probe.num_updates
+    pinned = torch.empty(n * 9, dtype=torch.uint8, pin_memory=True)
+    pinned.numpy()[:] = probe.raw()
+    del probe
+    host = pinned.numpy().view(S.RECORD_DTYPE)
+    d_rec = pinned.cuda()
+    torch.cuda.synchronize()
+    log(f"[powerlaw] {n} records ({n * 9 / 1e9:.2f} GB) in {time.time() - t:.1f} s")
+    cuts = np.linspace(0, n, Q + 1).astype(np.int64)
+    alg = gz.CCSketchAlg(V, cfg["sketch_seed"])
+    alg.set_gutter_capacity(2 * int(cuts[1] - cuts[0]) + 1024)
+    base = d_rec.data_ptr()
+
+    def step_snapshot(from_host=False):
+        alg.clear()
+        answers, tickets = [], []
+        for k in range(Q):
+            if from_host:
+                alg.ingest_records(host[cuts[k]:cuts[k + 1]])
+            else:
+                alg.ingest_records_device(base + 9 * int(cuts[k]), int(cuts[k + 1] - cuts[k]))
+            tickets.append(alg.query_submit())
+            if k:
+                answers.append(alg.query_wait(tickets[k - 1])[0].size())
+        answers.append(alg.query_wait(tickets[-1])[0].size())
+        return answers
+
+    def step_blocking():
+        alg.clear()
+        answers = []
+        for k in range(Q):
+            alg.ingest_records_device(base + 9 * int(cuts[k]), int(cuts[k + 1] - cuts[k]))
+            answers.append(alg.num_connected_components())
+        return answers
+
+    def timed(fn, steps):
+        out, ms = None, []
+        for _ in range(steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            out = fn()
+            torch.cuda.synchronize()
+            ms.append((time.perf_counter() - t0) * 1e3)
+        return out, ms
+
+    for _ in range(args.warmup):
+        a_snap = step_snapshot()
+        a_block = step_blocking()
+    if a_snap != a_block:
+        raise SystemExit(f"snapshot and blocking answers differ: {a_snap} vs {a_block}")
+    sampler = ClockSampler(0)
+    sampler.start()
+    alg.set_profiling(True)
+    a_snap, snap_ms = timed(step_snapshot, args.steps)
+    prof = alg.get_profile()
+    alg.set_profiling(True)  # resets the counters: the blocking arm's queries are timed here
+    a_block, block_ms = timed(step_blocking, args.steps)
+    prof_block = alg.get_profile()
+    alg.set_profiling(False)
+    clocks = sampler.stop()
+    assert a_snap == a_block
+    e2e_ms = []
+    if not args.no_e2e:
+        a_host, e2e_ms = timed(lambda: step_snapshot(from_host=True), max(1, min(args.steps, 3)))
+        assert a_host == a_snap
+    p = alg.params
+    alg.close()
+    ms = statistics.mean(snap_ms)
+    return {
+        "metric": "edge updates/sec with interleaved CC queries on 1 B200", "value": n / (ms / 1e3),
+        "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+        "data": "synthetic (seeded Chung-Lu stream, C generator)",
+        "config": {"workload": cfg["workload"], "num_vertices": V, "num_updates": n, "queries": Q,
+                   "num_columns": p.num_columns, "bkt_per_col": p.bkt_per_col,
+                   "sketch_bytes_total": V * p.sketch_bytes,
+                   "l2": "inputs larger than L2 (1.2 GB of records, 14 GB of sketches)"},
+        "timing": "wall clock between device synchronisations, whole stream with its queries",
+        "snapshot_queries": {"ms_per_step": ms, "updates_per_s": n / (ms / 1e3),
+                             "ingest_ms_per_step": (prof["gutter_ms"] + prof["sketch_update_ms"]) / args.steps},
+        "blocking_queries": {"ms_per_step": statistics.mean(block_ms),
+                             "updates_per_s": n / (statistics.mean(block_ms) / 1e3),
+                             "query_ms": prof_block["query_ms"] / (args.steps * Q),
+                             "ingest_ms_per_step": (prof_block["gutter_ms"] + prof_block["sketch_update_ms"]) / args.steps},
+        "query_ms": prof_block["query_ms"] / (args.steps * Q),
+        "components_at_each_query": a_snap,
+        "e2e": ({"value": n / (max(e2e_ms) / 1e3), "unit": UNIT, "h2d_bytes_per_step": n * 9,
+                 "d2h_bytes_per_step": Q * V * 4,
+                 "note": "pinned host records -> gz_ingest_records in 10 segments, snapshot query "
+                         "after each (labels to host); wall clock, max of steps"} if e2e_ms else None),
+        "clocks": clocks,
+        "gpu_launches": int(prof["kernel_launches"]),
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -645,9 +764,11 @@ def main():
     ap.add_argument("--small", action="store_true", help="V=2^14 case (profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="dense", choices=["dense", "many_graphs", "serving"],
+    ap.add_argument("--workload", default="dense",
+                    choices=["dense", "many_graphs", "serving", "powerlaw"],
                     help="dense: one V=2^17 graph (the headline); many_graphs: 512 uneven graphs; "
-                         "serving: 2000 tenants behind a 120 GB sketch budget")
+                         "serving: 2000 tenants behind a 120 GB sketch budget; powerlaw: V=2^20 "
+                         "Chung-Lu stream with 10 interleaved queries")
     ap.add_argument("--graphs", type=int, default=0, help="graphs of the many_graphs workload")
     ap.add_argument("--tenants", type=int, default=0, help="tenants of the serving workload")
     ap.add_argument("--time-scale", type=float, default=4.0,
@@ -665,6 +786,8 @@ def main():
         line = run_many_graphs(args)
     elif args.workload == "serving":
         line = run_serving(args)
+    elif args.workload == "powerlaw":
+        line = run_powerlaw(args)
     else:
         line = run_reference(args, cfg) if args.impl == "reference" else run_b200(args, cfg)
     if line is not None:

@@ -76,6 +76,8 @@ SIGNATURES = [
     ("gz_ingest_records_device", _i, [_H, _P, _sz]),
     ("gz_flush", _i, [_H]),
     ("gz_has_cached_query", _i, [_H, _i, ctypes.POINTER(_i)]),
+    ("gz_query_submit", _i, [_H, ctypes.POINTER(_u64)]),
+    ("gz_query_wait", _i, [_H, _u64, _P, ctypes.POINTER(_u32), ctypes.POINTER(_sz)]),
     ("gz_connected_components", _i, [_H, _P, ctypes.POINTER(_u32)]),
     ("gz_point_query", _i, [_H, _u32, _u32, ctypes.POINTER(_i)]),
     ("gz_last_query_rounds", _i, [_H, ctypes.POINTER(_sz)]),

@@ -383,6 +383,21 @@ class CCSketchAlg:
         self.cc_alg_end = time.perf_counter()
         return ConnectedComponents(parent, n.value)
 
+    def query_submit(self) -> int:
+        """Snapshot the sketches (after every update so far) and start their connectivity query
+        on the device; updates made afterwards proceed meanwhile. Returns a ticket."""
+        t = ctypes.c_uint64()
+        _check(self.lib.gz_query_submit(self._h, ctypes.byref(t)))
+        return int(t.value)
+
+    def query_wait(self, ticket: int):
+        """(ConnectedComponents, rounds) of the state at the ticket's submission."""
+        parent = np.empty(self.params.num_vertices, np.uint32)
+        n = ctypes.c_uint32()
+        r = ctypes.c_size_t()
+        _check(self.lib.gz_query_wait(self._h, ticket, _ptr(parent), ctypes.byref(n), ctypes.byref(r)))
+        return ConnectedComponents(parent, n.value), int(r.value)
+
     def num_connected_components(self) -> int:
         n = ctypes.c_uint32()
         _check(self.lib.gz_connected_components(self._h, None, ctypes.byref(n)))

@@ -8,7 +8,10 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <condition_variable>
+#include <map>
 #include <string>
+#include <thread>
 #include <unordered_set>
 #include <vector>
 
@@ -171,6 +174,27 @@ struct gz_alg {
   bool eager = false, host_answer = false, boruvka_ran = false;
   std::vector<uint32_t> hdsu;
   std::unordered_set<uint64_t> hforest;
+  // snapshot queries (gz_query_submit / gz_query_wait): a copy of the sketches taken at
+  // submission, queried by a worker thread on its own stream and buffers while ingest goes on
+  struct SnapResult {
+    int rc = GZ_OK;
+    std::string err;
+    uint32_t ncc = 0, rounds = 0;
+    std::vector<uint32_t> labels;
+  };
+  struct Snap {
+    uint8_t *d_sk = nullptr;
+    gz::BoruvkaBufs bv{};
+    uint32_t *d_final = nullptr, *d_ncc = nullptr, *d_status = nullptr, *h_pin = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t before = nullptr, copied = nullptr;
+    std::thread worker;
+    std::mutex m;
+    std::condition_variable cv;
+    bool stop = false, queued = false, running = false;
+    uint64_t next_ticket = 1, job = 0;
+    std::map<uint64_t, SnapResult> results;
+  } snap;
   std::atomic<bool> query_running{false};
   size_t last_rounds = 0;
   uint32_t last_ncc = 0;
@@ -361,7 +385,10 @@ int init_alg(gz_alg *h, uint32_t V, uint64_t seed, double sf, double bf, bool cu
   return GZ_OK;
 }
 
+void snap_shutdown(gz_alg *h);
+
 void destroy_alg(gz_alg *h) {
+  snap_shutdown(h);
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
   dev_free(h->d_sk);
@@ -661,9 +688,8 @@ int eager_from_device(gz_alg *h, bool have_forest) {
 
 // ---- Boruvka ---------------------------------------------------------------------------------------
 
-int ensure_query(gz_alg *h) {
-  auto &b = h->bv;
-  const size_t V = h->V;
+// Boruvka buffers for V vertices; acc_words per component spanning warps
+int alloc_bv(gz::BoruvkaBufs &b, size_t V, size_t acc_words, uint32_t *status) {
   GZ_TRY(dev_alloc(&b.parent, V));
   GZ_TRY(dev_alloc(&b.label, V));
   GZ_TRY(dev_alloc(&b.cnt, V));
@@ -677,14 +703,168 @@ int ensure_query(gz_alg *h) {
   GZ_TRY(dev_alloc(&b.comp_start, V + 1));
   GZ_TRY(dev_alloc(&b.comp_key, V));
   GZ_TRY(dev_alloc(&b.ncomp, 1));
-  GZ_TRY(dev_alloc(&b.acc, V * (h->cps * h->B + 1) * 3));
+  GZ_TRY(dev_alloc(&b.acc, V * acc_words));
   GZ_TRY(dev_alloc(&b.flags, 4));
   GZ_TRY(dev_alloc(&b.forest, V));
   GZ_TRY(dev_alloc(&b.forest_n, 1));
   GZ_TRY(dev_alloc(&b.trace_n, 1));
+  b.status = status;
+  return GZ_OK;
+}
+
+void free_bv(gz::BoruvkaBufs &b) {
+  dev_free(b.parent);
+  dev_free(b.label);
+  dev_free(b.cnt);
+  dev_free(b.fill);
+  dev_free(b.minv);
+  dev_free(b.packed);
+  dev_free(b.scan_total);
+  dev_free(b.scan_tmp);
+  dev_free(b.order);
+  dev_free(b.order_comp);
+  dev_free(b.comp_start);
+  dev_free(b.comp_key);
+  dev_free(b.ncomp);
+  dev_free(b.acc);
+  dev_free(b.flags);
+  dev_free(b.forest);
+  dev_free(b.forest_n);
+  dev_free(b.trace_n);
+}
+
+// boruvka_emulation (src/cc_sketch_alg.cpp:464-513) on the sketches at sk with buffers b on
+// stream s, driven from the host one device round at a time until a round neither FAILs nor
+// merges; pin is a pinned 4-word host mirror. GZ_ERR_OUT_OF_SAMPLES when round `samples` is
+// reached (rounds_out = that round).
+int boruvka_core(const gz::BoruvkaGeom &g, uint32_t samples, const uint8_t *sk, gz::BoruvkaBufs &b,
+                 uint32_t *d_final, uint32_t *d_ncc, uint32_t *pin, bool trace, cudaStream_t s,
+                 uint32_t &rounds_out, uint32_t &ncc_out) {
+  auto modified = [&](bool &m) -> int {
+    GZ_CUDA(cudaMemcpyAsync(pin + 1, b.flags, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    GZ_CUDA(cudaStreamSynchronize(s));
+    m = pin[1] != 0;
+    return GZ_OK;
+  };
+  GZ_CUDA(gz::boruvka_reset(g, b, s));
+  GZ_CUDA(cudaMemsetAsync(b.flags, 0, sizeof(uint32_t), s));
+  GZ_CUDA(gz::boruvka_round0(g, sk, b, s));
+  bool mod = false;
+  GZ_TRY(modified(mod));
+  uint32_t round = 0;
+  while (mod) {
+    ++round;
+    if (round >= samples) {
+      rounds_out = round;
+      return GZ_ERR_OUT_OF_SAMPLES;
+    }
+    GZ_CUDA(cudaMemsetAsync(b.flags, 0, sizeof(uint32_t), s));
+    GZ_CUDA(gz::boruvka_round(g, round, sk, b, trace, s));
+    GZ_TRY(modified(mod));
+  }
+  GZ_CUDA(gz::boruvka_final(g, b, d_final, d_ncc, s));
+  GZ_CUDA(cudaMemcpyAsync(pin + 2, d_ncc, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  GZ_CUDA(cudaStreamSynchronize(s));
+  ncc_out = pin[2];
+  rounds_out = round;
+  return GZ_OK;
+}
+
+// ---- snapshot queries ---------------------------------------------------------------------------
+void snap_worker(gz_alg *h) {
+  cudaSetDevice(h->device);
+  auto &S = h->snap;
+  for (;;) {
+    uint64_t t;
+    {
+      std::unique_lock<std::mutex> lk(S.m);
+      S.cv.wait(lk, [&] { return S.stop || S.queued; });
+      if (!S.queued) return;
+      S.queued = false;
+      S.running = true;
+      t = S.job;
+    }
+    gz_alg::SnapResult r;
+    r.rc = boruvka_core(h->bgeom(), h->samples, S.d_sk, S.bv, S.d_final, S.d_ncc, S.h_pin, false, S.stream,
+                        r.rounds, r.ncc);
+    if (r.rc == GZ_ERR_OUT_OF_SAMPLES) {
+      r.err = "This sketch (seed=" + std::to_string(h->seed) + ", max samples=" + std::to_string(h->samples) +
+              ") cannot be sampled more times (cur idx=" + std::to_string(r.rounds) + ")!";
+    } else if (r.rc == GZ_OK) {
+      r.labels.resize(h->V);
+      cudaError_t e = cudaMemcpyAsync(r.labels.data(), S.d_final, sizeof(uint32_t) * h->V,
+                                      cudaMemcpyDeviceToHost, S.stream);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(S.h_pin, S.d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, S.stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(S.stream);
+      if (e != cudaSuccess) {
+        r.rc = GZ_ERR_CUDA;
+        r.err = cudaGetErrorString(e);
+      } else if (S.h_pin[0]) {
+        r.rc = (S.h_pin[0] & gz::kStatusTimeout) ? GZ_ERR_TIMEOUT : GZ_ERR_BAD_SAMPLE;
+        r.err = "the snapshot query's device status reported an error";
+        cudaMemsetAsync(S.d_status, 0, sizeof(uint32_t), S.stream);
+        cudaStreamSynchronize(S.stream);
+      }
+    } else {
+      r.err = gz_last_error();
+    }
+    {
+      std::lock_guard<std::mutex> lk(S.m);
+      S.results[t] = std::move(r);
+      S.running = false;
+    }
+    S.cv.notify_all();
+  }
+}
+
+int snap_ensure(gz_alg *h) {
+  auto &S = h->snap;
+  if (S.worker.joinable()) return GZ_OK;
+  GZ_TRY(dev_alloc(&S.d_sk, (size_t)h->V * h->sketch_bytes));
+  GZ_TRY(dev_alloc(&S.d_status, 4));
+  GZ_TRY(alloc_bv(S.bv, h->V, (size_t)(h->cps * h->B + 1) * 3, S.d_status));
+  GZ_TRY(dev_alloc(&S.d_final, h->V));
+  GZ_TRY(dev_alloc(&S.d_ncc, 1));
+  GZ_TRY(host_alloc(&S.h_pin, 4));
+  GZ_CUDA(cudaStreamCreateWithFlags(&S.stream, cudaStreamNonBlocking));
+  GZ_CUDA(cudaEventCreateWithFlags(&S.before, cudaEventDisableTiming));
+  GZ_CUDA(cudaEventCreateWithFlags(&S.copied, cudaEventDisableTiming));
+  GZ_CUDA(cudaMemsetAsync(S.d_status, 0, 16, S.stream));
+  GZ_CUDA(cudaStreamSynchronize(S.stream));
+  S.worker = std::thread(snap_worker, h);
+  return GZ_OK;
+}
+
+void snap_shutdown(gz_alg *h) {
+  auto &S = h->snap;
+  if (S.worker.joinable()) {
+    {
+      std::lock_guard<std::mutex> lk(S.m);
+      S.stop = true;
+    }
+    S.cv.notify_all();
+    S.worker.join();
+  }
+  if (S.stream) cudaStreamSynchronize(S.stream);
+  dev_free(S.d_sk);
+  free_bv(S.bv);
+  dev_free(S.d_final);
+  dev_free(S.d_ncc);
+  dev_free(S.d_status);
+  host_free(S.h_pin);
+  if (S.before) cudaEventDestroy(S.before);
+  if (S.copied) cudaEventDestroy(S.copied);
+  if (S.stream) cudaStreamDestroy(S.stream);
+  S.before = S.copied = nullptr;
+  S.stream = nullptr;
+}
+
+int ensure_query(gz_alg *h) {
+  auto &b = h->bv;
+  const size_t V = h->V;
+  GZ_TRY(alloc_bv(b, V, (size_t)(h->cps * h->B + 1) * 3, h->d_status));
   GZ_TRY(dev_alloc(&h->d_final, V));
   GZ_TRY(dev_alloc(&h->d_ncc, 1));
-  b.status = h->d_status;
   if (h->trace && !b.trace) {
     const size_t cap = V * (size_t)(h->C + 1);
     void *p = nullptr;
@@ -700,47 +880,28 @@ int ensure_query(gz_alg *h) {
   return GZ_OK;
 }
 
-int read_modified(gz_alg *h, bool &modified) {
-  GZ_CUDA(cudaMemcpyAsync(h->h_status + 1, h->bv.flags, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
-  GZ_CUDA(cudaStreamSynchronize(h->stream));
-  modified = h->h_status[1] != 0;
-  return GZ_OK;
-}
-
 // boruvka_emulation (src/cc_sketch_alg.cpp:464-513) driven from the host, one device round per
 // iteration until a round neither FAILs nor merges.
 int run_boruvka(gz_alg *h) {
   GZ_TRY(ensure_query(h));
   h->update_locked = true;  // stays set if the query fails, as in the reference
   const gz::BoruvkaGeom g = h->bgeom();
-  auto &b = h->bv;
   const int pi = h->prof_begin();
-  GZ_CUDA(gz::boruvka_reset(g, b, h->stream));
-  GZ_CUDA(cudaMemsetAsync(b.flags, 0, sizeof(uint32_t), h->stream));
-  GZ_CUDA(gz::boruvka_round0(g, h->d_sk, b, h->stream));
-  bool modified = false;
-  GZ_TRY(read_modified(h, modified));
-  uint32_t round = 0;
-  while (modified) {
-    ++round;
-    if (round >= h->samples) {
-      h->prof_end(pi, 2);
-      h->last_rounds = round;
-      return fail(GZ_ERR_OUT_OF_SAMPLES,
-                  "This sketch (seed=" + std::to_string(h->seed) + ", max samples=" +
-                      std::to_string(h->samples) + ") cannot be sampled more times (cur idx=" +
-                      std::to_string(round) + ")!");
-    }
-    GZ_CUDA(cudaMemsetAsync(b.flags, 0, sizeof(uint32_t), h->stream));
-    GZ_CUDA(gz::boruvka_round(g, round, h->d_sk, b, h->trace, h->stream));
-    GZ_TRY(read_modified(h, modified));
-  }
-  GZ_CUDA(gz::boruvka_final(g, b, h->d_final, h->d_ncc, h->stream));
+  uint32_t round = 0, ncc = 0;
+  const int rc = boruvka_core(g, h->samples, h->d_sk, h->bv, h->d_final, h->d_ncc, h->h_status, h->trace,
+                              h->stream, round, ncc);
   h->prof_end(pi, 2);
+  if (rc == GZ_ERR_OUT_OF_SAMPLES) {
+    h->last_rounds = round;
+    return fail(GZ_ERR_OUT_OF_SAMPLES,
+                "This sketch (seed=" + std::to_string(h->seed) + ", max samples=" +
+                    std::to_string(h->samples) + ") cannot be sampled more times (cur idx=" +
+                    std::to_string(round) + ")!");
+  }
+  GZ_TRY(rc);
   h->prof_acc.query_rounds += round + 1;
-  GZ_CUDA(cudaMemcpyAsync(h->h_status + 2, h->d_ncc, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
   GZ_TRY(check_status(h));
-  h->last_ncc = h->h_status[2];
+  h->last_ncc = ncc;
   h->last_rounds = round;
   h->dsu_valid = true;
   h->labels_on_host = false;
@@ -1077,6 +1238,52 @@ int gz_flush(gz_alg_t *h) {
   if (!h) return fail(GZ_ERR_INVALID, "null handle");
   Guard g(h);
   return flush_all(h);
+}
+
+int gz_query_submit(gz_alg_t *h, uint64_t *ticket) {
+  if (!h || !ticket) return fail(GZ_ERR_INVALID, "null argument");
+  Guard g(h);
+  GZ_TRY(flush_all(h));  // every update so far is in the sketches
+  auto &S = h->snap;
+  {
+    // one snapshot at a time: the previous query must be done with the copy
+    std::unique_lock<std::mutex> lk(S.m);
+    S.cv.wait(lk, [&] { return !S.queued && !S.running; });
+  }
+  GZ_TRY(snap_ensure(h));
+  // the copy follows all sketch work so far; later sketch work waits for the copy
+  GZ_CUDA(cudaEventRecord(S.before, h->stream));
+  GZ_CUDA(cudaStreamWaitEvent(S.stream, S.before, 0));
+  GZ_CUDA(cudaMemcpyAsync(S.d_sk, h->d_sk, (size_t)h->V * h->sketch_bytes, cudaMemcpyDeviceToDevice, S.stream));
+  GZ_CUDA(cudaEventRecord(S.copied, S.stream));
+  GZ_CUDA(cudaStreamWaitEvent(h->stream, S.copied, 0));
+  {
+    std::lock_guard<std::mutex> lk(S.m);
+    S.job = S.next_ticket++;
+    S.queued = true;
+    *ticket = S.job;
+  }
+  S.cv.notify_all();
+  return GZ_OK;
+}
+
+int gz_query_wait(gz_alg_t *h, uint64_t ticket, uint32_t *parent_out, uint32_t *num_cc, size_t *rounds) {
+  if (!h) return fail(GZ_ERR_INVALID, "null handle");
+  auto &S = h->snap;
+  gz_alg::SnapResult r;
+  {
+    std::unique_lock<std::mutex> lk(S.m);
+    const bool pending = S.job == ticket && (S.queued || S.running);
+    if (!pending && !S.results.count(ticket)) return fail(GZ_ERR_INVALID, "unknown or already collected ticket");
+    S.cv.wait(lk, [&] { return S.results.count(ticket) > 0; });
+    r = std::move(S.results[ticket]);
+    S.results.erase(ticket);
+  }
+  if (rounds) *rounds = r.rounds;
+  if (r.rc != GZ_OK) return fail(r.rc, r.err);
+  if (num_cc) *num_cc = r.ncc;
+  if (parent_out) std::copy(r.labels.begin(), r.labels.end(), parent_out);
+  return GZ_OK;
 }
 
 int gz_has_cached_query(const gz_alg_t *h, int code, int *out) {

@@ -207,3 +207,68 @@ GZG_API void gzg_shuffle_stream(const uint64_t *edges, uint64_t E, const uint64_
     memcpy(r + 5, &b, 4);
   }
 }
+
+/* ---- Chung-Lu power-law streams ----------------------------------------------------------- */
+
+/* vertex drawn with probability proportional to its weight: cdf holds the normalised cumulative
+ * weights (cdf[V-1] == 1); ids relabels weight ranks to vertex ids */
+static inline uint32_t cl_draw(const double *cdf, const uint32_t *ids, uint32_t V, uint64_t r) {
+  const double x = (double)(r >> 11) * 0x1.0p-53;
+  uint32_t lo = 0, hi = V - 1;
+  while (lo < hi) {
+    const uint32_t mid = lo + (hi - lo) / 2;
+    if (cdf[mid] > x) hi = mid;
+    else lo = mid + 1;
+  }
+  return ids[lo];
+}
+
+/* edge i of the stream: endpoints drawn independently from the weights, a repeat of the first
+ * endpoint redrawn (up to 16 times, then its neighbour id) so there are no self-loops */
+static inline void cl_edge(const double *cdf, const uint32_t *ids, uint32_t V, uint64_t seed,
+                           uint64_t i, uint32_t *u, uint32_t *v) {
+  *u = cl_draw(cdf, ids, V, rnd(seed, 101, i));
+  uint32_t w = cl_draw(cdf, ids, V, rnd(seed, 102, i));
+  for (uint32_t t = 0; w == *u && t < 16; ++t) w = cl_draw(cdf, ids, V, rnd(seed, 103 + t, i));
+  if (w == *u) w = (*u + 1) % V;
+  *v = w;
+}
+
+static inline void put_record(uint8_t *p, uint8_t type, uint32_t u, uint32_t v) {
+  p[0] = type;
+  memcpy(p + 1, &u, 4);
+  memcpy(p + 5, &v, 4);
+}
+
+/*
+ * A Chung-Lu stream of m edge inserts (i.i.d. weighted endpoints, so already in random order),
+ * then deletions of nd = floor(del_frac * m) of them, then re-inserts of nr = floor(rein_frac * nd)
+ * of the deleted ones, each phase in its own pseudo-random order. Writes m + nd + nr packed
+ * 9-byte records to out (NULL: count only) and returns that number. An insert that repeats an
+ * earlier edge toggles it, as any repeated update does.
+ */
+GZG_API uint64_t gzg_chung_lu_stream(const double *cdf, const uint32_t *ids, uint32_t V, uint64_t m,
+                                     double del_frac, double rein_frac, uint64_t seed, uint8_t *out) {
+  const uint64_t nd = (uint64_t)floor(del_frac * (double)m);
+  const uint64_t nr = (uint64_t)floor(rein_frac * (double)nd);
+  if (!out) return m + nd + nr;
+  const perm_t Pd = perm_make(nd ? nd : 1, seed ^ 0xDE1E7Eull);
+  const perm_t Pr = perm_make(nr ? nr : 1, seed ^ 0x4E1A5Eull);
+#pragma omp parallel for schedule(static, 65536)
+  for (uint64_t i = 0; i < m + nd + nr; ++i) {
+    uint64_t e;
+    uint8_t type = 0;
+    if (i < m) {
+      e = i;
+    } else if (i < m + nd) {
+      e = perm_fwd(&Pd, i - m); /* a deleted edge is one of the first nd inserted */
+      type = 1;
+    } else {
+      e = perm_fwd(&Pr, i - m - nd); /* a re-inserted edge is one of the first nr deleted */
+    }
+    uint32_t u, v;
+    cl_edge(cdf, ids, V, seed, e, &u, &v);
+    put_record(out + 9 * i, type, u, v);
+  }
+  return m + nd + nr;
+}

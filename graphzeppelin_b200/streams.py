@@ -291,6 +291,9 @@ def _genlib():
         L.gzg_planted_nonedges.restype = None
         L.gzg_planted_nonedges.argtypes = [ctypes.c_uint32, vp, vp, ctypes.c_double,
                                            ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, vp]
+        L.gzg_chung_lu_stream.restype = ctypes.c_uint64
+        L.gzg_chung_lu_stream.argtypes = [vp, vp, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_double,
+                                          ctypes.c_double, ctypes.c_uint64, vp]
         L.gzg_shuffle_stream.restype = None
         L.gzg_shuffle_stream.argtypes = [vp, ctypes.c_uint64, vp, ctypes.c_uint64, ctypes.c_uint64, vp]
         _gen = L
@@ -382,3 +385,36 @@ def many_graph_streams(num_graphs: int, seed: int, *, log2_v_min: float = 8.0,
     offsets = np.concatenate([[0], np.cumsum(counts)]).astype(np.uint64)
     raw = np.concatenate(parts) if parts else np.zeros(0, np.uint8)
     return Vs.astype(np.uint32), sketch_seeds, raw, offsets
+
+
+def chung_lu_stream_fast(num_vertices: int, exponent: float, mean_degree: float, max_degree: int,
+                         seed: int, delete_fraction: float = 0.15, reinsert_fraction: float = 0.5,
+                         out: np.ndarray | None = None) -> Stream:
+    """Chung-Lu power-law stream from the multithreaded C generator: vertex weights
+    (rank)^(-1/(exponent-1)) scaled to mean_degree and capped at max_degree (vertex ids a seeded
+    permutation of the ranks), V * mean_degree / 2 inserts of weight-drawn endpoint pairs, then
+    deletes of a delete_fraction of them, then re-inserts of a reinsert_fraction of those.
+    Repeated pairs toggle, like any repeated update. ``out``: optional preallocated uint8 buffer."""
+    L = _genlib()
+    rng = np.random.default_rng(seed)
+    V = num_vertices
+    w = np.arange(1, V + 1, dtype=np.float64) ** (-1.0 / (exponent - 1.0))
+    for _ in range(100):  # scale so that the mean degree after the cap is mean_degree
+        f = mean_degree * V / np.minimum(w, max_degree).sum()
+        w *= f
+        if abs(f - 1.0) < 1e-12:
+            break
+    w = np.minimum(w, max_degree)
+    m = int(w.sum() / 2)
+    cdf = np.cumsum(w)
+    cdf /= cdf[-1]
+    cdf[-1] = 1.0
+    ids = rng.permutation(V).astype(np.uint32)
+    gseed = int(rng.integers(0, 2**63))
+    n = L.gzg_chung_lu_stream(cdf.ctypes.data, ids.ctypes.data, V, m, delete_fraction,
+                              reinsert_fraction, gseed, None)
+    buf = out if out is not None else np.empty(n * 9, np.uint8)
+    assert buf.size >= n * 9
+    L.gzg_chung_lu_stream(cdf.ctypes.data, ids.ctypes.data, V, m, delete_fraction,
+                          reinsert_fraction, gseed, buf.ctypes.data)
+    return Stream(V, buf[:n * 9].view(RECORD_DTYPE))
