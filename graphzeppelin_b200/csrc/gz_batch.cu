@@ -444,7 +444,7 @@ struct MBBufs {
   const uint64_t *flip;
   uint32_t *parent, *label, *cnt, *fill;
   uint64_t *packed, *scan_total;
-  uint32_t *order, *comp_start, *ncomp, *acc;
+  uint32_t *order, *order_comp, *comp_start, *ncomp, *acc;
   uint32_t *active, *modified;  // per graph
   const uint32_t *round;        // current round (device)
   uint32_t *status;
@@ -487,33 +487,93 @@ __device__ __forceinline__ const uint32_t *mb_sketch(const MBBufs &b, const Grap
          (uint64_t)(v - gd.vbase) * gd.sketch_words;
 }
 
-__global__ void k_mb_round0(MBBufs b) {
+// Per-lane view of one vertex's graph for the query kernels: where its sketch lives and the
+// sizes of its sample regions. Each lane loads the descriptor of its own vertex; a warp then
+// hands them round with shuffles, one vertex at a time.
+struct MbVert {
+  const uint32_t *sk;  // the vertex's sketch (words)
+  uint32_t g, B, det;  // graph, buckets per column, word offset of the deterministic bucket
+  uint64_t chk;        // the graph's checksum flip
+};
+__device__ __forceinline__ MbVert mb_vert(const MBBufs &b, uint32_t v) {
+  MbVert m;
+  m.g = b.gov[v];
+  const GraphDesc gd = b.graphs[m.g];
+  m.sk = mb_sketch(b, gd, v);
+  m.B = gd.B;
+  m.det = 3 * gd.C * gd.B;
+  m.chk = b.flip[gd.flip_off + gd.C];
+  return m;
+}
+__device__ __forceinline__ MbVert mb_vert_shfl(const MbVert &m, uint32_t src) {
+  MbVert o;
+  o.sk = reinterpret_cast<const uint32_t *>(__shfl_sync(kFull, reinterpret_cast<unsigned long long>(m.sk), src));
+  o.g = __shfl_sync(kFull, m.g, src);
+  o.B = __shfl_sync(kFull, m.B, src);
+  o.det = __shfl_sync(kFull, m.det, src);
+  o.chk = __shfl_sync(kFull, (unsigned long long)m.chk, src);
+  return o;
+}
+
+constexpr int kMbKB = 4;  // vertices whose loads a warp keeps in flight together
+constexpr size_t kMbStageBytes = 8 * sizeof(uint32_t) * Region<1>::kStage;
+
+// Round 0 for every active graph: a warp takes 32 consecutive global vertices (run_round_zero,
+// src/cc_sketch_alg.cpp:223-244), batches their loads, samples each in word space, and the 32
+// lanes then apply their vertex's result together.
+__global__ void __launch_bounds__(256, 3) k_mb_round0(MBBufs b) {
+  constexpr int NW = Region<1>::kNW;
+  extern __shared__ uint32_t mb_stage[];
   const uint32_t lane = threadIdx.x & 31;
+  uint32_t *st = mb_stage + (threadIdx.x >> 5) * Region<1>::kStage;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < b.total_V; v += nwarps) {
-    const uint32_t g = b.gov[v];
-    if (!b.active[g]) continue;
-    const GraphDesc gd = b.graphs[g];
-    const uint32_t *sk = mb_sketch(b, gd, v);
-    uint32_t d[3], a[2][3] = {{0, 0, 0}, {0, 0, 0}};
-    load_bucket(sk + 3 * gd.C * gd.B, d);
-#pragma unroll
-    for (int s = 0; s < 2; ++s) {
-      const uint32_t j = s * 32 + lane;
-      if (j < gd.B) load_bucket(sk + 3 * j, a[s]);
+  for (uint32_t base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; base < b.total_V;
+       base += nwarps * 32) {
+    const uint32_t n = b.total_V - base < 32 ? b.total_V - base : 32;
+    MbVert me{};
+    bool my_act = false;
+    if (lane < n) {
+      me = mb_vert(b, base + lane);
+      my_act = b.active[me.g] != 0;
     }
-    uint64_t idx;
-    const int res = warp_sample(d, a, gd.B, b.flip[gd.flip_off + gd.C], &idx);
-    if (lane == 0) mb_handle(res, idx, g, gd, b);
+    const uint32_t act = __ballot_sync(kFull, my_act);
+    int my_res = 1;
+    uint64_t my_idx = 0;
+    for (uint32_t i = 0; i < n; i += kMbKB) {
+      uint32_t x[kMbKB][NW], dw[kMbKB];
+      MbVert m[kMbKB];
+#pragma unroll
+      for (int k = 0; k < kMbKB; ++k) {
+        if (i + k >= n) break;
+        m[k] = mb_vert_shfl(me, i + k);
+        if (act >> (i + k) & 1) region_load(m[k].sk, m[k].sk + m[k].det, 3 * m[k].B, lane, x[k], dw[k]);
+      }
+#pragma unroll
+      for (int k = 0; k < kMbKB; ++k) {
+        if (i + k >= n) break;
+        if (!(act >> (i + k) & 1)) continue;
+        uint64_t idx;
+        const int res = warp_sample_region<1>(x[k], dw[k], 3 * m[k].B, m[k].B, m[k].chk, st, &idx);
+        if (lane == i + k) {
+          my_res = res;
+          my_idx = idx;
+        }
+      }
+    }
+    if (my_act) mb_handle(my_res, my_idx, me.g, b.graphs[me.g], b);
   }
 }
 
-__global__ void k_mb_label(MBBufs b) {
+// Roots and members per root of the active graphs' vertices (one atomic per root per warp).
+__global__ void __launch_bounds__(256) k_mb_label(MBBufs b) {
   const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-  if (v >= b.total_V || !b.active[b.gov[v]]) return;
+  const bool ok = v < b.total_V && b.active[b.gov[v]];
+  const uint32_t act = __ballot_sync(kFull, ok);
+  if (!ok) return;
   const uint32_t r = dsu_find(b.parent, v);
   b.label[v] = r;
-  atomicAdd(&b.cnt[r], 1u);
+  const uint32_t peers = __match_any_sync(act, r);
+  if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&b.cnt[r], (uint32_t)__popc(peers));
 }
 
 __global__ void k_mb_pack(MBBufs b) {
@@ -523,18 +583,23 @@ __global__ void k_mb_pack(MBBufs b) {
   b.packed[v] = (uint64_t)c | (c ? (1ull << 32) : 0ull);
 }
 
-__global__ void k_mb_group(MBBufs b) {
+__global__ void __launch_bounds__(256) k_mb_group(MBBufs b) {
+  __shared__ uint32_t stage[8][32];
   const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
   if (v == 0) {
     const uint32_t nc = (uint32_t)(*b.scan_total >> 32), members = (uint32_t)*b.scan_total;
     b.comp_start[nc] = members;
     *b.ncomp = nc;
   }
-  if (v >= b.total_V || !b.active[b.gov[v]]) return;
+  const bool ok = v < b.total_V && b.active[b.gov[v]];
+  const uint32_t act = __ballot_sync(kFull, ok);
+  if (!ok) return;
   const uint32_t r = b.label[v];
   const uint64_t s = b.packed[r];
   const uint32_t start = (uint32_t)s, c = (uint32_t)(s >> 32);
-  b.order[start + atomicAdd(&b.fill[r], 1u)] = v;
+  const uint32_t pos = start + warp_agg_inc(b.fill, r, act, stage[threadIdx.x >> 5]);
+  b.order[pos] = v;
+  b.order_comp[pos] = c;
   if (v == r) {
     b.comp_start[c] = start;
     const uint32_t end = start + b.cnt[r];
@@ -545,19 +610,15 @@ __global__ void k_mb_group(MBBufs b) {
   }
 }
 
-// component index of grouped position p (comp_start is sorted)
-__device__ __forceinline__ uint32_t comp_of(const MBBufs &b, uint32_t nc, uint32_t p) {
-  uint32_t lo = 0, hi = nc;
-  while (hi - lo > 1) {
-    const uint32_t mid = (lo + hi) >> 1;
-    if (b.comp_start[mid] <= p) lo = mid;
-    else hi = mid;
-  }
-  return lo;
-}
-
-__global__ void k_mb_merge(MBBufs b) {
+// Round >= 1 merge (perform_boruvka_round, src/cc_sketch_alg.cpp:246-380) over the grouped
+// members of every active graph: `span` members per warp, kMbKB members' loads in flight,
+// column `round` of each graph XORed in word space; in-span components are sampled here (the
+// results applied 32 at a time by the lanes), the others combined in acc.
+__global__ void __launch_bounds__(256, 2) k_mb_merge(MBBufs b) {
+  constexpr int NW = Region<1>::kNW;
+  extern __shared__ uint32_t mb_stage[];
   const uint32_t lane = threadIdx.x & 31;
+  uint32_t *st = mb_stage + (threadIdx.x >> 5) * Region<1>::kStage;
   const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nc = *b.ncomp;
   const uint32_t members = b.comp_start[nc];
@@ -565,63 +626,78 @@ __global__ void k_mb_merge(MBBufs b) {
   if (p0 >= members) return;
   const uint32_t p1 = (p0 + b.span < members) ? (uint32_t)(p0 + b.span) : members;
   const uint32_t round = *b.round;
-  uint32_t a[2][3] = {{0, 0, 0}, {0, 0, 0}}, d[3] = {0, 0, 0};
-  uint32_t cur = comp_of(b, nc, (uint32_t)p0);
-  uint32_t next_start = b.comp_start[cur + 1];
-  uint32_t g = b.gov[b.order[p0]];
-  GraphDesc gd = b.graphs[g];
+  uint32_t acc[NW], dacc = 0;
+#pragma unroll
+  for (int k = 0; k < NW; ++k) acc[k] = 0;
+  uint32_t cur = 0xffffffffu;
+  MbVert cm{};  // a member of the current component (its graph's geometry)
+  int my_res = 1;
+  uint64_t my_idx = 0;
+  uint32_t my_g = 0, nres = 0;
+  auto apply = [&]() {
+    if (lane < nres) mb_handle(my_res, my_idx, my_g, b.graphs[my_g], b);
+    __syncwarp();
+    nres = 0;
+  };
   auto flush = [&]() {
     const uint32_t s = b.comp_start[cur], e = b.comp_start[cur + 1];
+    const uint32_t W = 3 * cm.B;
     if (s >= p0 && e <= p1) {
       uint64_t idx;
-      const int res = warp_sample(d, a, gd.B, b.flip[gd.flip_off + gd.C], &idx);
-      if (lane == 0) mb_handle(res, idx, g, gd, b);
+      const int res = warp_sample_region<1>(acc, dacc, W, cm.B, cm.chk, st, &idx);
+      if (lane == nres) {
+        my_res = res;
+        my_idx = idx;
+        my_g = cm.g;
+      }
+      if (++nres == 32) apply();
     } else {
       uint32_t *ac = b.acc + (uint64_t)cur * b.acc_words;
 #pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        const uint32_t j = q * 32 + lane;
-        if (j < gd.B) {
-          atomicXor(ac + 3 * j, a[q][0]);
-          atomicXor(ac + 3 * j + 1, a[q][1]);
-          atomicXor(ac + 3 * j + 2, a[q][2]);
-        }
+      for (int k = 0; k < NW; ++k) {
+        const uint32_t wi = k * 32 + lane;
+        if (wi < W && acc[k]) atomicXor(ac + wi, acc[k]);
       }
-      if (lane == 0) {
-        atomicXor(ac + 3 * gd.B, d[0]);
-        atomicXor(ac + 3 * gd.B + 1, d[1]);
-        atomicXor(ac + 3 * gd.B + 2, d[2]);
-      }
+      if (lane < 3 && dacc) atomicXor(ac + W + lane, dacc);
     }
   };
-  for (uint32_t p = (uint32_t)p0; p < p1; ++p) {
-    if (p == next_start) {
-      flush();
-      ++cur;
-      next_start = b.comp_start[cur + 1];
-      g = b.gov[b.order[p]];
-      gd = b.graphs[g];
-#pragma unroll
-      for (int q = 0; q < 2; ++q) a[q][0] = a[q][1] = a[q][2] = 0;
-      d[0] = d[1] = d[2] = 0;
+  for (uint32_t cb = (uint32_t)p0; cb < p1; cb += 32) {
+    const uint32_t n = p1 - cb < 32 ? p1 - cb : 32;
+    MbVert me{};
+    uint32_t my_c = 0;
+    if (lane < n) {
+      me = mb_vert(b, b.order[cb + lane]);
+      my_c = b.order_comp[cb + lane];
     }
-    const uint32_t *sk = mb_sketch(b, gd, b.order[p]);
-    const uint32_t col = 3 * round * gd.B, detw = 3 * gd.C * gd.B;
+    for (uint32_t i = 0; i < n; i += kMbKB) {
+      uint32_t x[kMbKB][NW], dw[kMbKB];
+      MbVert m[kMbKB];
 #pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      const uint32_t j = q * 32 + lane;
-      if (j < gd.B) {
-        const uint32_t *bk = sk + col + 3 * j;
-        a[q][0] ^= bk[0];
-        a[q][1] ^= bk[1];
-        a[q][2] ^= bk[2];
+      for (int k = 0; k < kMbKB; ++k) {
+        if (i + k >= n) break;
+        m[k] = mb_vert_shfl(me, i + k);
+        region_load(m[k].sk + 3 * round * m[k].B, m[k].sk + m[k].det, 3 * m[k].B, lane, x[k], dw[k]);
+      }
+#pragma unroll
+      for (int k = 0; k < kMbKB; ++k) {
+        if (i + k >= n) break;
+        const uint32_t c = __shfl_sync(kFull, my_c, i + k);
+        if (c != cur) {
+          if (cur != 0xffffffffu) flush();
+          cur = c;
+          cm = m[k];
+#pragma unroll
+          for (int q = 0; q < NW; ++q) acc[q] = 0;
+          dacc = 0;
+        }
+#pragma unroll
+        for (int q = 0; q < NW; ++q) acc[q] ^= x[k][q];
+        dacc ^= dw[k];
       }
     }
-    d[0] ^= sk[detw];
-    d[1] ^= sk[detw + 1];
-    d[2] ^= sk[detw + 2];
   }
   flush();
+  apply();
 }
 
 __global__ void k_mb_sample_spanning(MBBufs b) {
@@ -790,7 +866,7 @@ struct gz_batch {
   // Boruvka
   uint32_t *d_parent = nullptr, *d_label = nullptr, *d_cnt = nullptr, *d_fill = nullptr;
   uint64_t *d_packed = nullptr, *d_vscan_total = nullptr, *d_vscan_tmp = nullptr;
-  uint32_t *d_order = nullptr, *d_comp_start = nullptr, *d_ncomp = nullptr, *d_acc = nullptr;
+  uint32_t *d_order = nullptr, *d_order_comp = nullptr, *d_comp_start = nullptr, *d_ncomp = nullptr, *d_acc = nullptr;
   uint32_t *d_active = nullptr, *d_modified = nullptr, *d_round = nullptr, *d_ncc = nullptr;
   cudaGraphExec_t round_exec = nullptr;
   cudaGraph_t round_graph = nullptr;
@@ -815,6 +891,7 @@ struct gz_batch {
     b.packed = d_packed;
     b.scan_total = d_vscan_total;
     b.order = d_order;
+    b.order_comp = d_order_comp;
     b.comp_start = d_comp_start;
     b.ncomp = d_ncomp;
     b.acc = d_acc;
@@ -824,7 +901,7 @@ struct gz_batch {
     b.status = d_status;
     b.total_V = (uint32_t)total_V;
     b.acc_words = (max_B + 1) * 3;
-    b.span = 64;
+    b.span = total_V >= (1u << 19) ? 128 : 64;
     return b;
   }
 };
@@ -864,6 +941,7 @@ void batch_destroy(gz_batch *h) {
   mb_free(h->d_vscan_total);
   mb_free(h->d_vscan_tmp);
   mb_free(h->d_order);
+  mb_free(h->d_order_comp);
   mb_free(h->d_comp_start);
   mb_free(h->d_ncomp);
   mb_free(h->d_acc);
@@ -1151,6 +1229,7 @@ int ensure_boruvka(gz_batch *h) {
     mb_free(h->d_packed);
     mb_free(h->d_vscan_tmp);
     mb_free(h->d_order);
+    mb_free(h->d_order_comp);
     mb_free(h->d_comp_start);
     h->cap_bv_V = 0;
     MB_TRY(mb_alloc(&h->d_parent, V));
@@ -1160,6 +1239,7 @@ int ensure_boruvka(gz_batch *h) {
     MB_TRY(mb_alloc(&h->d_packed, V));
     MB_TRY(mb_alloc(&h->d_vscan_tmp, scan_tmp_words(V)));
     MB_TRY(mb_alloc(&h->d_order, V));
+    MB_TRY(mb_alloc(&h->d_order_comp, V));
     MB_TRY(mb_alloc(&h->d_comp_start, V + 1));
     h->cap_bv_V = V;
   }
@@ -1192,7 +1272,7 @@ int enqueue_round(gz_batch *h, cudaStream_t s) {
   MB_CUDA(scan_exclusive_u64(h->d_packed, V, h->d_vscan_total, h->d_vscan_tmp, s));
   k_mb_group<<<cdiv(V, 256), 256, 0, s>>>(b);
   const uint64_t warps = (V + b.span - 1) / b.span;
-  k_mb_merge<<<cdiv(warps * 32, 256), 256, 0, s>>>(b);
+  k_mb_merge<<<cdiv(warps * 32, 256), 256, kMbStageBytes, s>>>(b);
   k_mb_sample_spanning<<<std::min<unsigned>(cdiv(V * 32, 256), num_sms() * 16), 256, 0, s>>>(b);
   MB_CUDA(cudaGetLastError());
   return GZ_OK;
@@ -1217,7 +1297,7 @@ int batch_query(gz_batch *h, uint32_t *labels_out) {
   k_mb_reset<<<cdiv(V, 256), 256, 0, h->stream>>>((uint32_t)V, h->d_parent);
   MB_CUDA(cudaMemcpyAsync(h->d_active, active.data(), sizeof(uint32_t) * G, cudaMemcpyHostToDevice, h->stream));
   MB_CUDA(cudaMemsetAsync(h->d_modified, 0, sizeof(uint32_t) * G, h->stream));
-  k_mb_round0<<<std::min<unsigned>(cdiv(V * 32, 256), num_sms() * 16), 256, 0, h->stream>>>(b);
+  k_mb_round0<<<std::min<unsigned>(cdiv(V, 256), num_sms() * 8), 256, kMbStageBytes, h->stream>>>(b);
   h->launches += 2;
   MB_CUDA(cudaGetLastError());
   // The round runs as a captured CUDA graph once the same graphs and buffers come back (a batch

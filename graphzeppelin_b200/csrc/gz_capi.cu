@@ -234,7 +234,7 @@ struct gz_alg {
     g.B = B;
     g.sketch_words = nb * 3;
     g.flip_chk = gz::xxh3_flip(seed);
-    g.span = 64;
+    g.span = V >= (1u << 19) ? 128 : 64;  // fewer warps (and acc atomics) per round at large V
     g.cps = cps;
     return g;
   }

@@ -298,6 +298,100 @@ __device__ __forceinline__ int warp_sample_cols(const uint32_t (&d)[3], const ui
 }
 
 
+// ---- sample regions in word space --------------------------------------------------------------
+// The columns of one sample (CPS consecutive columns, column-major) are one contiguous run of
+// W = 3 * CPS * B words, and merging sketches is a plain XOR of those words. The query kernels
+// therefore load, XOR and combine a region as W words spread over the warp (lane l holds words
+// l, l + 32, ...; fully coalesced), plus the deterministic bucket's 3 words on lanes 0..2, and
+// go to bucket order only to sample, through a per-warp shared-memory stage.
+template <int CPS>
+struct Region {
+  static constexpr int kNW = (3 * CPS * 64 + 31) / 32;  // word slots per lane (B <= 64)
+  static constexpr int kStage = 3 * CPS * 64 + 4;        // per-warp stage words
+};
+
+// Load region words [0, W) at src and the deterministic bucket at det into x / dw.
+template <int NW>
+__device__ __forceinline__ void region_load(const uint32_t *__restrict__ src,
+                                            const uint32_t *__restrict__ det, uint32_t W,
+                                            uint32_t lane, uint32_t (&x)[NW], uint32_t &dw) {
+#pragma unroll
+  for (int k = 0; k < NW; ++k) {
+    const uint32_t w = k * 32 + lane;
+    x[k] = w < W ? src[w] : 0u;
+  }
+  dw = lane < 3 ? det[lane] : 0u;
+}
+
+// Sketch::sample (src/sketch.cpp:94-116) of a region held in word space: the deterministic
+// bucket first, then columns 0..CPS-1, depths 0..B-1 in each, the first good bucket wins.
+// s is this warp's stage (Region<CPS>::kStage words). Returns 0 GOOD / 1 ZERO / 2 FAIL.
+template <int CPS, int NW>
+__device__ __forceinline__ int warp_sample_region(const uint32_t (&x)[NW], uint32_t dw,
+                                                  uint32_t W, uint32_t B, uint64_t flip_chk,
+                                                  uint32_t *s, uint64_t *idx) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t d0 = __shfl_sync(kFull, dw, 0), d1 = __shfl_sync(kFull, dw, 1),
+                 d2 = __shfl_sync(kFull, dw, 2);
+  if ((d0 | d1 | d2) == 0) {
+    *idx = 0;
+    return 1;  // ZERO
+  }
+  if (bucket_good(d0, d1, d2, flip_chk)) {
+    *idx = ((uint64_t)d1 << 32) | d0;
+    return 0;  // GOOD
+  }
+  __syncwarp();
+#pragma unroll
+  for (int k = 0; k < NW; ++k) {
+    const uint32_t w = k * 32 + lane;
+    if (w < W) s[w] = x[k];
+  }
+  __syncwarp();
+  int res = 2;
+  *idx = 0;
+#pragma unroll
+  for (int c = 0; c < CPS && res == 2; ++c) {
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      if ((uint32_t)q * 32 >= B || res != 2) break;
+      const uint32_t j = q * 32 + lane;
+      uint32_t a0 = 0, a1 = 0, a2 = 0;
+      if (j < B) {
+        const uint32_t *bk = s + 3 * (c * B + j);
+        a0 = bk[0];
+        a1 = bk[1];
+        a2 = bk[2];
+      }
+      const bool good = j < B && bucket_good(a0, a1, a2, flip_chk);
+      const uint32_t m = __ballot_sync(kFull, good);
+      if (m) {
+        const int src = __ffs(m) - 1;
+        const uint32_t x0 = __shfl_sync(kFull, a0, src);
+        const uint32_t x1 = __shfl_sync(kFull, a1, src);
+        *idx = ((uint64_t)x1 << 32) | x0;
+        res = 0;
+      }
+    }
+  }
+  return res;
+}
+
+// Warp-aggregated counter add: lanes in `active` holding the same key add one each to ctr[key]
+// with one atomic per distinct key; returns this lane's slot (old value + rank among its key's
+// lanes). stage is a 32-word per-warp shared array used to hand the base to the key's lanes.
+__device__ __forceinline__ uint32_t warp_agg_inc(uint32_t *ctr, uint32_t key, uint32_t active,
+                                                 uint32_t *stage) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t peers = __match_any_sync(active, key);
+  const uint32_t leader = __ffs(peers) - 1;
+  if (lane == leader) stage[lane] = atomicAdd(ctr + key, (uint32_t)__popc(peers));
+  __syncwarp(active);
+  const uint32_t base = stage[leader];
+  __syncwarp(active);
+  return base + __popc(peers & ((1u << lane) - 1u));
+}
+
 struct TraceRec {
   uint32_t round, key, result, pad;
   uint64_t idx;

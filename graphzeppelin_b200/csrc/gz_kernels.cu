@@ -675,39 +675,65 @@ __global__ void k_bv_reset(uint32_t V, uint32_t *parent) {
   if (v < V) parent[v] = v;
 }
 
-// Round 0 (run_round_zero, src/cc_sketch_alg.cpp:223-244): every vertex is its own component.
 // Round 0 (run_round_zero, src/cc_sketch_alg.cpp:223-244): every vertex sketch samples its
-// sample 0 -- columns 0..CPS-1 and the deterministic bucket -- one warp per vertex.
-template <int CPS>
-__global__ void k_bv_round0(BoruvkaGeom g, const uint32_t *__restrict__ sk_words, BoruvkaBufs b) {
+// sample 0 -- columns 0..CPS-1 and the deterministic bucket. A warp takes 32 consecutive
+// vertices, loads them KB at a time (all loads of a batch in flight together) and samples each
+// through its shared-memory stage; lane i keeps vertex i's result, and the 32 results are then
+// applied by the 32 lanes at once, so the union-find chains of one warp overlap.
+template <int CPS, int KB>
+__global__ void __launch_bounds__(256, CPS == 1 ? 3 : 1) k_bv_round0(BoruvkaGeom g, const uint32_t *__restrict__ sk_words,
+                                                   BoruvkaBufs b) {
+  constexpr int NW = Region<CPS>::kNW;
+  extern __shared__ uint32_t bv_stage[];
   const uint32_t lane = threadIdx.x & 31;
+  uint32_t *st = bv_stage + (threadIdx.x >> 5) * Region<CPS>::kStage;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < g.V; v += nwarps) {
-    const uint32_t *sk = sk_words + (uint64_t)v * g.sketch_words;
-    uint32_t d[3], a[CPS][2][3];
-    load_bucket(sk + 3 * g.C * g.B, d);
+  const uint32_t W = 3 * CPS * g.B, detw = 3 * g.C * g.B;
+  for (uint32_t base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; base < g.V;
+       base += nwarps * 32) {
+    const uint32_t n = g.V - base < 32 ? g.V - base : 32;
+    int my_res = 1;
+    uint64_t my_idx = 0;
+    for (uint32_t i = 0; i < n; i += KB) {
+      uint32_t x[KB][NW], dw[KB];
 #pragma unroll
-    for (int c = 0; c < CPS; ++c)
+      for (int k = 0; k < KB; ++k)
+        if (i + k < n) {
+          const uint32_t *sk = sk_words + (uint64_t)(base + i + k) * g.sketch_words;
+          region_load(sk, sk + detw, W, lane, x[k], dw[k]);
+        }
 #pragma unroll
-      for (int s = 0; s < 2; ++s) {
-        const uint32_t j = s * 32 + lane;
-        a[c][s][0] = a[c][s][1] = a[c][s][2] = 0;
-        if (j < g.B) load_bucket(sk + 3 * (c * g.B + j), a[c][s]);
-      }
-    uint64_t idx;
-    const int res = warp_sample_cols<CPS>(d, a, g.B, g.flip_chk, &idx);
-    if (lane == 0) handle_result(res, idx, 0, v, g, b);
+      for (int k = 0; k < KB; ++k)
+        if (i + k < n) {
+          uint64_t idx;
+          const int res = warp_sample_region<CPS>(x[k], dw[k], W, g.B, g.flip_chk, st, &idx);
+          if (lane == i + k) {
+            my_res = res;
+            my_idx = idx;
+          }
+        }
+    }
+    if (lane < n) handle_result(my_res, my_idx, 0, base + lane, g, b);
   }
 }
 
-__global__ void k_bv_label(uint32_t V, uint32_t *parent, uint32_t *label, uint32_t *cnt,
-                           uint32_t *minv) {
+// Root of every vertex and members per root; lanes of a warp that share a root add to its
+// counter with one atomic (a giant component would otherwise serialise V atomics on one word).
+// minv (trace keys) gets the smallest member: lanes hold consecutive vertices, so the lowest
+// lane of each root group.
+__global__ void __launch_bounds__(256) k_bv_label(uint32_t V, uint32_t *parent, uint32_t *label,
+                                                  uint32_t *cnt, uint32_t *minv) {
   const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t active = __ballot_sync(kFull, v < V);
   if (v >= V) return;
   const uint32_t r = dsu_find(parent, v);
   label[v] = r;
-  atomicAdd(&cnt[r], 1u);
-  if (minv) atomicMin(&minv[r], v);
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t peers = __match_any_sync(active, r);
+  if (lane == __ffs(peers) - 1) {
+    atomicAdd(&cnt[r], (uint32_t)__popc(peers));
+    if (minv) atomicMin(&minv[r], v);
+  }
 }
 
 __global__ void k_bv_pack(uint32_t V, const uint32_t *cnt, uint64_t *packed) {
@@ -718,18 +744,22 @@ __global__ void k_bv_pack(uint32_t V, const uint32_t *cnt, uint64_t *packed) {
 }
 
 // create_merge_instructions (src/cc_sketch_alg.cpp:382-462): group vertices by root so each
-// component's members are contiguous in `order`.
-__global__ void k_bv_group(uint32_t V, uint32_t acc_words, uint32_t span, const uint32_t *label,
-                           const uint64_t *packed, const uint64_t *total, const uint32_t *cnt,
-                           uint32_t *fill, const uint32_t *minv, uint32_t *order,
-                           uint32_t *order_comp, uint32_t *comp_start, uint32_t *comp_key,
-                           uint32_t *ncomp, uint32_t *acc) {
+// component's members are contiguous in `order` (slots taken with warp-aggregated atomics).
+__global__ void __launch_bounds__(256) k_bv_group(uint32_t V, uint32_t acc_words, uint32_t span,
+                                                  const uint32_t *label, const uint64_t *packed,
+                                                  const uint64_t *total, const uint32_t *cnt,
+                                                  uint32_t *fill, const uint32_t *minv,
+                                                  uint32_t *order, uint32_t *order_comp,
+                                                  uint32_t *comp_start, uint32_t *comp_key,
+                                                  uint32_t *ncomp, uint32_t *acc) {
+  __shared__ uint32_t stage[8][32];
   const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t active = __ballot_sync(kFull, v < V);
   if (v >= V) return;
   const uint32_t r = label[v];
   const uint64_t s = packed[r];
   const uint32_t start = (uint32_t)s, c = (uint32_t)(s >> 32);
-  const uint32_t pos = start + atomicAdd(&fill[r], 1u);
+  const uint32_t pos = start + warp_agg_inc(fill, r, active, stage[threadIdx.x >> 5]);
   order[pos] = v;
   order_comp[pos] = c;
   if (v == r) {
@@ -749,81 +779,89 @@ __global__ void k_bv_group(uint32_t V, uint32_t acc_words, uint32_t span, const 
 }
 
 // perform_boruvka_round (src/cc_sketch_alg.cpp:246-380) for round >= 1: each warp XOR-merges
-// sample `round` (columns round*CPS .. +CPS) + the deterministic bucket over `span` consecutive
-// grouped members; components wholly inside the span are sampled right here, the rest are
-// combined in acc (per component: CPS*B column buckets, then the deterministic one).
-template <int CPS>
-__global__ void k_bv_merge(BoruvkaGeom g, uint32_t round, const uint32_t *__restrict__ sk_words,
-                           BoruvkaBufs b) {
+// sample `round` (columns round*CPS .. +CPS, one contiguous word run) + the deterministic bucket
+// over `span` consecutive grouped members, KB members' loads in flight at a time; components
+// wholly inside the span are sampled right here, the rest are combined in acc (per component:
+// CPS*B column buckets, then the deterministic one) with one coalesced atomicXor per word.
+template <int CPS, int KB>
+__global__ void __launch_bounds__(256, CPS == 1 ? 3 : 1) k_bv_merge(BoruvkaGeom g, uint32_t round,
+                                                  const uint32_t *__restrict__ sk_words, BoruvkaBufs b) {
+  constexpr int NW = Region<CPS>::kNW;
+  extern __shared__ uint32_t bv_stage[];
   const uint32_t lane = threadIdx.x & 31;
+  uint32_t *st = bv_stage + (threadIdx.x >> 5) * Region<CPS>::kStage;
   const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint64_t p0 = (uint64_t)w * g.span;
   if (p0 >= g.V) return;
   const uint32_t p1 = (uint32_t)(p0 + g.span < (uint64_t)g.V ? p0 + g.span : (uint64_t)g.V);
   const uint32_t col = 3 * round * CPS * g.B, detw = 3 * g.C * g.B;
-  const uint32_t acc_words = (CPS * g.B + 1) * 3;
-  uint32_t a[CPS][2][3], d[3] = {0, 0, 0};
+  const uint32_t W = 3 * CPS * g.B;
+  uint32_t acc[NW], dacc = 0;
 #pragma unroll
-  for (int c = 0; c < CPS; ++c)
-#pragma unroll
-    for (int q = 0; q < 2; ++q) a[c][q][0] = a[c][q][1] = a[c][q][2] = 0;
+  for (int k = 0; k < NW; ++k) acc[k] = 0;
   uint32_t cur = b.order_comp[p0];
+  // results of components sampled here: lane j holds the j-th, applied 32 at a time
+  int my_res = 1;
+  uint64_t my_idx = 0;
+  uint32_t my_key = 0, nres = 0;
+  auto apply = [&]() {
+    if (lane < nres) handle_result(my_res, my_idx, round, my_key, g, b);
+    __syncwarp();
+    nres = 0;
+  };
   auto flush = [&](uint32_t comp) {
     const uint32_t s = b.comp_start[comp], e = b.comp_start[comp + 1];
     if (s >= p0 && e <= p1) {
       uint64_t idx;
-      const int res = warp_sample_cols<CPS>(d, a, g.B, g.flip_chk, &idx);
-      if (lane == 0) handle_result(res, idx, round, b.comp_key[comp], g, b);
-    } else {
-      uint32_t *ac = b.acc + (uint64_t)comp * acc_words;
-#pragma unroll
-      for (int c = 0; c < CPS; ++c)
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-          const uint32_t j = q * 32 + lane;
-          if (j < g.B) {
-            uint32_t *bk = ac + 3 * (c * g.B + j);
-            atomicXor(bk, a[c][q][0]);
-            atomicXor(bk + 1, a[c][q][1]);
-            atomicXor(bk + 2, a[c][q][2]);
-          }
-        }
-      if (lane == 0) {
-        atomicXor(ac + 3 * CPS * g.B, d[0]);
-        atomicXor(ac + 3 * CPS * g.B + 1, d[1]);
-        atomicXor(ac + 3 * CPS * g.B + 2, d[2]);
+      const int res = warp_sample_region<CPS>(acc, dacc, W, g.B, g.flip_chk, st, &idx);
+      if (lane == nres) {
+        my_res = res;
+        my_idx = idx;
+        my_key = b.comp_key[comp];
       }
+      if (++nres == 32) apply();
+    } else {
+      uint32_t *ac = b.acc + (uint64_t)comp * (W + 3);
+#pragma unroll
+      for (int k = 0; k < NW; ++k) {
+        const uint32_t wi = k * 32 + lane;
+        if (wi < W && acc[k]) atomicXor(ac + wi, acc[k]);
+      }
+      if (lane < 3 && dacc) atomicXor(ac + W + lane, dacc);
     }
   };
-  for (uint32_t p = (uint32_t)p0; p < p1; ++p) {
-    const uint32_t comp = b.order_comp[p];
-    if (comp != cur) {
-      flush(cur);
-      cur = comp;
+  for (uint32_t cb = (uint32_t)p0; cb < p1; cb += 32) {
+    const uint32_t n = p1 - cb < 32 ? p1 - cb : 32;
+    const uint32_t my_v = lane < n ? b.order[cb + lane] : 0u;
+    const uint32_t my_c = lane < n ? b.order_comp[cb + lane] : 0u;
+    for (uint32_t i = 0; i < n; i += KB) {
+      uint32_t x[KB][NW], dw[KB];
 #pragma unroll
-      for (int c = 0; c < CPS; ++c)
-#pragma unroll
-        for (int q = 0; q < 2; ++q) a[c][q][0] = a[c][q][1] = a[c][q][2] = 0;
-      d[0] = d[1] = d[2] = 0;
-    }
-    const uint32_t *sk = sk_words + (uint64_t)b.order[p] * g.sketch_words;
-#pragma unroll
-    for (int c = 0; c < CPS; ++c)
-#pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        const uint32_t j = q * 32 + lane;
-        if (j < g.B) {
-          const uint32_t *bk = sk + col + 3 * (c * g.B + j);
-          a[c][q][0] ^= bk[0];
-          a[c][q][1] ^= bk[1];
-          a[c][q][2] ^= bk[2];
+      for (int k = 0; k < KB; ++k)
+        if (i + k < n) {
+          const uint32_t v = __shfl_sync(kFull, my_v, i + k);
+          const uint32_t *sk = sk_words + (uint64_t)v * g.sketch_words;
+          region_load(sk + col, sk + detw, W, lane, x[k], dw[k]);
         }
-      }
-    d[0] ^= sk[detw];
-    d[1] ^= sk[detw + 1];
-    d[2] ^= sk[detw + 2];
+#pragma unroll
+      for (int k = 0; k < KB; ++k)
+        if (i + k < n) {
+          const uint32_t c = __shfl_sync(kFull, my_c, i + k);
+          if (c != cur) {
+            flush(cur);
+            cur = c;
+#pragma unroll
+            for (int q = 0; q < NW; ++q) acc[q] = 0;
+            dacc = 0;
+          }
+#pragma unroll
+          for (int q = 0; q < NW; ++q) acc[q] ^= x[k][q];
+          dacc ^= dw[k];
+        }
+    }
   }
   flush(cur);
+  apply();
 }
 
 template <int CPS>
@@ -1155,6 +1193,11 @@ cudaError_t sketch_xor_raw(uint8_t *sketches, uint32_t words, uint32_t v, const 
   return cudaGetLastError();
 }
 
+// per-block stage of the round-0 and merge kernels: 8 warps x Region<CPS>::kStage words
+size_t bv_stage_bytes(int cps) {
+  return 8 * sizeof(uint32_t) * (cps == 1 ? dev::Region<1>::kStage : dev::Region<7>::kStage);
+}
+
 cudaError_t boruvka_reset(const BoruvkaGeom &g, const BoruvkaBufs &b, cudaStream_t s) {
   k_bv_reset<<<blocks_for(g.V, 256), 256, 0, s>>>(g.V, b.parent);
   g_launches++;
@@ -1165,10 +1208,11 @@ cudaError_t boruvka_reset(const BoruvkaGeom &g, const BoruvkaBufs &b, cudaStream
 
 cudaError_t boruvka_round0(const BoruvkaGeom &g, const uint8_t *sketches, const BoruvkaBufs &b,
                            cudaStream_t s) {
-  const unsigned blocks = std::min<unsigned>(blocks_for((uint64_t)g.V * 32, 256), num_sms() * 16);
+  // one warp per 32 vertices, 8 warps per block, grid-stride beyond 8 blocks per SM
+  const unsigned blocks = std::min<unsigned>(blocks_for((uint64_t)g.V, 256), num_sms() * 8);
   const uint32_t *sk = reinterpret_cast<const uint32_t *>(sketches);
-  if (g.cps == 1) k_bv_round0<1><<<blocks, 256, 0, s>>>(g, sk, b);
-  else if (g.cps == 7) k_bv_round0<7><<<blocks, 256, 0, s>>>(g, sk, b);
+  if (g.cps == 1) k_bv_round0<1, 4><<<blocks, 256, bv_stage_bytes(1), s>>>(g, sk, b);
+  else if (g.cps == 7) k_bv_round0<7, 1><<<blocks, 256, bv_stage_bytes(7), s>>>(g, sk, b);
   else return cudaErrorInvalidValue;
   g_launches++;
   return cudaGetLastError();
@@ -1196,8 +1240,8 @@ cudaError_t boruvka_round(const BoruvkaGeom &g, uint32_t round, const uint8_t *s
   const uint64_t warps = (V + g.span - 1) / g.span;
   const uint32_t *sk = reinterpret_cast<const uint32_t *>(sketches);
   const unsigned sblocks = std::min<unsigned>(blocks_for((uint64_t)V * 32, 256), num_sms() * 16);
-  if (g.cps == 1) k_bv_merge<1><<<blocks_for(warps * 32, 256), 256, 0, s>>>(g, round, sk, b);
-  else k_bv_merge<7><<<blocks_for(warps * 32, 256), 256, 0, s>>>(g, round, sk, b);
+  if (g.cps == 1) k_bv_merge<1, 4><<<blocks_for(warps * 32, 256), 256, bv_stage_bytes(1), s>>>(g, round, sk, b);
+  else k_bv_merge<7, 1><<<blocks_for(warps * 32, 256), 256, bv_stage_bytes(7), s>>>(g, round, sk, b);
   g_launches++;
   if (g.cps == 1) k_bv_sample_spanning<1><<<sblocks, 256, 0, s>>>(g, round, b);
   else k_bv_sample_spanning<7><<<sblocks, 256, 0, s>>>(g, round, b);
