@@ -482,6 +482,11 @@ class CCSketchAlg:
         _check(self.lib.gz_get_params(self._h, ctypes.byref(p)))
         self.params = p
 
+    def set_direct_factor(self, factor: float) -> None:
+        """Sparse tiles below factor x the staging break-even go in place (gz_set_direct_factor);
+        0 always stages."""
+        _check(self.lib.gz_set_direct_factor(self._h, float(factor)))
+
     def set_gutter_capacity(self, endpoint_updates: int) -> None:
         _check(self.lib.gz_set_gutter_capacity(self._h, endpoint_updates))
 

@@ -482,7 +482,7 @@ k_sketch_update(SketchGeom g, uint8_t *__restrict__ sketches, const uint8_t *__r
                 const uint64_t *__restrict__ flip, uint32_t *work_counter, uint32_t *status) {
   extern __shared__ __align__(128) uint8_t dsm[];
   __shared__ __align__(8) uint64_t s_bar;
-  __shared__ uint32_t s_tile, s_total;
+  __shared__ uint32_t s_tile, s_total, s_direct;
   const uint32_t vpt = 1u << g.tile_shift;
   const uint32_t tile_bytes = vpt * g.sketch_words * 4;
   const uint32_t per_bin = g.bin_shift - g.tile_shift;  // log2(tiles per bin)
@@ -510,9 +510,12 @@ k_sketch_update(SketchGeom g, uint8_t *__restrict__ sketches, const uint8_t *__r
         for (int k = 0; k < nchunks; ++k)
           total += bin_off[(uint64_t)k * stride + bin + 1] - bin_off[(uint64_t)k * stride + bin];
       }
+      // a tile with too few entries to pay for staging its sketches is updated in place in HBM
+      const bool direct = !HASHED && per_bin == 0 && total < g.direct_max;
       s_tile = t;
       s_total = total;
-      if (t < g.ntiles && total) {
+      s_direct = direct;
+      if (t < g.ntiles && total && !direct) {
         const uint8_t *src = sketches + (uint64_t)t * tile_bytes;
         mbar_expect_tx(bar, tile_bytes);
         for (uint32_t off = 0; off < tile_bytes; off += kBulkPiece)
@@ -522,7 +525,16 @@ k_sketch_update(SketchGeom g, uint8_t *__restrict__ sketches, const uint8_t *__r
     __syncthreads();
     const uint32_t t = s_tile;
     if (t >= g.ntiles) break;
-    if (s_total) {
+    if (s_total && s_direct) {
+      uint32_t *gsk = reinterpret_cast<uint32_t *>(sketches);
+      for (int k = 0; k < nchunks; ++k) {
+        const uint2 *E = reinterpret_cast<const uint2 *>(gutter + chunks.base[k]);
+        const uint64_t b = bin_off[(uint64_t)k * stride + t];
+        const uint64_t e = bin_off[(uint64_t)k * stride + t + 1];
+        for (uint64_t i = b + threadIdx.x; i < e; i += blockDim.x)
+          apply_entry_global(E[i], gsk, g.sketch_words, s_flip, flip_chk, g.C, g.B);
+      }
+    } else if (s_total) {
       const bool ok = mbar_wait_bounded(bar, parity, kWaitLimitNs);
       parity ^= 1u;
       if (__syncthreads_or(!ok)) {

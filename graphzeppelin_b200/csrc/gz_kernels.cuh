@@ -51,6 +51,8 @@ struct SketchGeom {
   uint32_t bin_shift;          // gutter bin (>= tile_shift); a bin holds 1 << (bin - tile) tiles
   uint32_t nbins;
   uint32_t cube = 0;           // CubeSketch update rule (every depth 0..d) instead of CameoSketch
+  uint32_t direct_max = 0;     // one tile per bin only: a tile with fewer plain entries than this
+                               // is updated in place in HBM (global atomics) instead of staged
 };
 
 // Records per staging tile of the gutter kernels, and the largest bin count for which the

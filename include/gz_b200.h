@@ -288,6 +288,11 @@ GZ_API int gz_measure_update_rate(int repeats, double *updates_per_s);
  * once in the gutter; needs at most 32 columns). Buffered updates are applied first. */
 GZ_API int gz_set_tuning(gz_alg_t *alg, uint32_t vertices_per_tile, uint32_t threads_per_block,
                          uint32_t tiles_per_bin, uint32_t entry_form);
+/* Route of sparse tiles (one tile per gutter bin, plain CameoSketch entries): a tile holding
+ * fewer entries than factor x (its sketch bytes / (32 (columns + 1))) -- the break-even of
+ * staging it in shared memory against updating its buckets in HBM -- is updated in place with
+ * global atomics. 0 = always staged, 1 = the default. Same role as gz_batch_set_route. */
+GZ_API int gz_set_direct_factor(gz_alg_t *alg, double factor);
 
 /* ---- many graphs on one GPU ------------------------------------------------------------------
  * A gz_batch_t holds num_graphs independent CCSketchAlg instances (each its own V, seed and

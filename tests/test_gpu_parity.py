@@ -134,6 +134,30 @@ def test_tile_shapes_bit_exact(gz, oracle_mod, vpt, threads, tpb, form):
     assert (alg.dump_sketches() == osk.data).all()
 
 
+@pytest.mark.parametrize("factor", [0.0, 1.0, 1e9])
+@pytest.mark.parametrize("vpt", [4, 16])
+def test_direct_route_bit_exact(gz, oracle_mod, vpt, factor):
+    """Sparse tiles updated in place in HBM (global atomics) instead of staged: 0 stages every
+    tile, 1e9 sends every tile in place, 1 mixes the two by entry count. Bytes must not move."""
+    c, st, labels, _ = load_case("c0_v1024")
+    alg = _alg(gz, 1024, c["seed"])
+    alg.set_tuning(vpt, 1024, 1)
+    alg.set_direct_factor(factor)
+    half = st.num_updates // 2
+    rec = st.records
+    alg.ingest_records(rec[:half])
+    alg.flush()
+    alg.ingest_records(rec[half:half + 500])  # a sparse launch: most tiles get few entries
+    alg.flush()
+    alg.ingest_records(rec[half + 500:])
+    osk = oracle_mod.OracleSketches(1024, c["seed"])
+    osk.apply_records(st.raw())
+    assert (alg.dump_sketches() == osk.data).all()
+    cc = alg.connected_components()
+    assert cc.size() == c["num_cc"]
+    assert (canonical(cc.parent_arr) == labels).all()
+
+
 def test_queries_during_stream(gz, oracle_mod):
     """TestQueryDuringStream / MTStreamWithMultipleQueries: 10 queries at stream breakpoints."""
     c, st, _, _ = load_case("c0_v1024")
