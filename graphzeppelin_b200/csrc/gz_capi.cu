@@ -143,6 +143,9 @@ struct gz_alg {
   uint64_t entry_cap = 0;       // capacity in endpoint updates
   uint64_t gutter_bytes = 0, gutter_used = 0, entries_pending = 0;
   double direct_factor = 1.0;   // scales the in-place threshold of sparse tiles (0 = never)
+  // every update so far reached both endpoints' sketches (records, gz_update): the XOR of all
+  // vertex sketches is zero, which lets a query merge its largest component from the rest
+  bool symmetric = true;
   bool hashed = false;          // records become hashed entries (each edge hashed once)
   bool hashed_default = false;
   uint32_t *d_hist2d = nullptr;
@@ -193,6 +196,7 @@ struct gz_alg {
     std::mutex m;
     std::condition_variable cv;
     bool stop = false, queued = false, running = false;
+    bool complement = false;  // the sketches' XOR was zero when the job was submitted
     uint64_t next_ticket = 1, job = 0;
     std::map<uint64_t, SnapResult> results;
   } snap;
@@ -242,8 +246,9 @@ struct gz_alg {
     g.B = B;
     g.sketch_words = nb * 3;
     g.flip_chk = gz::xxh3_flip(seed);
-    g.span = V >= (1u << 19) ? 128 : 64;  // fewer warps (and acc atomics) per round at large V
+    g.span = gz::kBoruvkaSpan;
     g.cps = cps;
+    g.complement = symmetric ? 1 : 0;
     return g;
   }
 
@@ -441,6 +446,9 @@ void destroy_alg(gz_alg *h) {
   dev_free(b.comp_key);
   dev_free(b.ncomp);
   dev_free(b.acc);
+  dev_free(b.part);
+  dev_free(b.part_comp);
+  dev_free(b.big);
   dev_free(b.flags);
   dev_free(b.forest);
   dev_free(b.forest_n);
@@ -700,7 +708,7 @@ int eager_from_device(gz_alg *h, bool have_forest) {
 
 // ---- Boruvka ---------------------------------------------------------------------------------------
 
-// Boruvka buffers for V vertices; acc_words per component spanning warps
+// Boruvka buffers for V vertices; acc_words per component spanning warps (and per merge warp)
 int alloc_bv(gz::BoruvkaBufs &b, size_t V, size_t acc_words, uint32_t *status) {
   GZ_TRY(dev_alloc(&b.parent, V));
   GZ_TRY(dev_alloc(&b.label, V));
@@ -716,6 +724,10 @@ int alloc_bv(gz::BoruvkaBufs &b, size_t V, size_t acc_words, uint32_t *status) {
   GZ_TRY(dev_alloc(&b.comp_key, V));
   GZ_TRY(dev_alloc(&b.ncomp, 1));
   GZ_TRY(dev_alloc(&b.acc, V * acc_words));
+  const size_t warps = (V + gz::kBoruvkaSpan - 1) / gz::kBoruvkaSpan;
+  GZ_TRY(dev_alloc(&b.part, warps * acc_words));
+  GZ_TRY(dev_alloc(&b.part_comp, warps));
+  GZ_TRY(dev_alloc(&b.big, 1));
   GZ_TRY(dev_alloc(&b.flags, 4));
   GZ_TRY(dev_alloc(&b.forest, V));
   GZ_TRY(dev_alloc(&b.forest_n, 1));
@@ -739,6 +751,9 @@ void free_bv(gz::BoruvkaBufs &b) {
   dev_free(b.comp_key);
   dev_free(b.ncomp);
   dev_free(b.acc);
+  dev_free(b.part);
+  dev_free(b.part_comp);
+  dev_free(b.big);
   dev_free(b.flags);
   dev_free(b.forest);
   dev_free(b.forest_n);
@@ -788,6 +803,7 @@ void snap_worker(gz_alg *h) {
   auto &S = h->snap;
   for (;;) {
     uint64_t t;
+    gz::BoruvkaGeom bg = h->bgeom();
     {
       std::unique_lock<std::mutex> lk(S.m);
       S.cv.wait(lk, [&] { return S.stop || S.queued; });
@@ -795,9 +811,10 @@ void snap_worker(gz_alg *h) {
       S.queued = false;
       S.running = true;
       t = S.job;
+      bg.complement = S.complement ? 1 : 0;
     }
     gz_alg::SnapResult r;
-    r.rc = boruvka_core(h->bgeom(), h->samples, S.d_sk, S.bv, S.d_final, S.d_ncc, S.h_pin, false, S.stream,
+    r.rc = boruvka_core(bg, h->samples, S.d_sk, S.bv, S.d_final, S.d_ncc, S.h_pin, false, S.stream,
                         r.rounds, r.ncc);
     if (r.rc == GZ_ERR_OUT_OF_SAMPLES) {
       r.err = "This sketch (seed=" + std::to_string(h->seed) + ", max samples=" + std::to_string(h->samples) +
@@ -1065,6 +1082,24 @@ int gz_create_from_serialized_ex(const char *path, double batch_factor, int sket
     return fail(GZ_ERR_CUDA, cudaGetErrorString(e));
   }
   h->dsu_valid = false;  // src/cc_sketch_alg.cpp:62-63
+  // loaded sketches keep the complement merge only if their XOR over all vertices is zero
+  {
+    uint32_t *d_tot = nullptr;
+    const uint32_t words = h->nb * 3;
+    std::vector<uint32_t> tot(words, 1);
+    e = cudaMalloc(&d_tot, words * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_tot, 0, words * sizeof(uint32_t), h->stream);
+    if (e == cudaSuccess) e = gz::sketch_total_xor(h->d_sk, V, words, d_tot, h->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(tot.data(), d_tot, words * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (d_tot) cudaFree(d_tot);
+    if (e != cudaSuccess) {
+      gz_destroy(h);
+      return fail(GZ_ERR_CUDA, cudaGetErrorString(e));
+    }
+    h->symmetric = std::all_of(tot.begin(), tot.end(), [](uint32_t x) { return x == 0; });
+  }
   *out = h;
   return GZ_OK;
 }
@@ -1152,6 +1187,7 @@ int gz_apply_update_batch(gz_alg_t *h, int, uint32_t src, const uint32_t *dsts, 
   for (size_t i = 0; i < n; ++i) {
     if (dsts[i] >= h->V) return fail(GZ_ERR_BAD_VERTEX, "dst vertex id >= V");
   }
+  h->symmetric = false;  // one endpoint's sketch only
   for (size_t i = 0; i < n; ++i) GZ_TRY(stage_entry(h, src, dsts[i]));
   return GZ_OK;
 }
@@ -1161,6 +1197,7 @@ int gz_apply_raw_buckets_update(gz_alg_t *h, uint32_t src, const void *raw) {
   Guard g(h);
   if (src >= h->V) return fail(GZ_ERR_BAD_VERTEX, "src vertex id >= V");
   invalidate_answer(h);
+  h->symmetric = false;
   GZ_TRY(dev_alloc(&h->d_raw, (size_t)h->nb * 3));
   GZ_CUDA(cudaMemcpyAsync(h->d_raw, raw, h->sketch_bytes, cudaMemcpyHostToDevice, h->stream));
   GZ_CUDA(gz::sketch_xor_raw(h->d_sk, h->nb * 3, src, h->d_raw, h->stream));
@@ -1273,6 +1310,7 @@ int gz_query_submit(gz_alg_t *h, uint64_t *ticket) {
     std::lock_guard<std::mutex> lk(S.m);
     S.job = S.next_ticket++;
     S.queued = true;
+    S.complement = h->symmetric;
     *ticket = S.job;
   }
   S.cv.notify_all();
@@ -1447,6 +1485,7 @@ int gz_clear(gz_alg_t *h) {
   const uint64_t v_pad = ((uint64_t)h->V + 63) & ~63ull;
   GZ_CUDA(cudaMemsetAsync(h->d_sk, 0, v_pad * h->sketch_bytes, h->stream));
   invalidate_answer(h);
+  h->symmetric = true;
   if (h->eager) {  // empty sketches: the eager DSU restarts from singletons, as at construction
     h->hdsu.resize(h->V);
     for (uint32_t v = 0; v < h->V; ++v) h->hdsu[v] = v;

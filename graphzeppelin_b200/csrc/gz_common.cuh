@@ -377,6 +377,69 @@ __device__ __forceinline__ int warp_sample_region(const uint32_t (&x)[NW], uint3
   return res;
 }
 
+// Sketch::sample of a region already in shared memory: s[0, W) the columns, s[W, W+3) the
+// deterministic bucket (same scan order as warp_sample_region).
+template <int CPS>
+__device__ __forceinline__ int warp_sample_smem(const uint32_t *s, uint32_t W, uint32_t B,
+                                                uint64_t flip_chk, uint64_t *idx) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t d0 = s[W], d1 = s[W + 1], d2 = s[W + 2];
+  if ((d0 | d1 | d2) == 0) {
+    *idx = 0;
+    return 1;  // ZERO
+  }
+  if (bucket_good(d0, d1, d2, flip_chk)) {
+    *idx = ((uint64_t)d1 << 32) | d0;
+    return 0;  // GOOD
+  }
+  int res = 2;
+  *idx = 0;
+#pragma unroll
+  for (int c = 0; c < CPS && res == 2; ++c) {
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      if ((uint32_t)q * 32 >= B || res != 2) break;
+      const uint32_t j = q * 32 + lane;
+      uint32_t a0 = 0, a1 = 0, a2 = 0;
+      if (j < B) {
+        const uint32_t *bk = s + 3 * (c * B + j);
+        a0 = bk[0];
+        a1 = bk[1];
+        a2 = bk[2];
+      }
+      const bool good = j < B && bucket_good(a0, a1, a2, flip_chk);
+      const uint32_t m = __ballot_sync(kFull, good);
+      if (m) {
+        const int src = __ffs(m) - 1;
+        const uint32_t x0 = __shfl_sync(kFull, a0, src);
+        const uint32_t x1 = __shfl_sync(kFull, a1, src);
+        *idx = ((uint64_t)x1 << 32) | x0;
+        res = 0;
+      }
+    }
+  }
+  return res;
+}
+
+// ---- asynchronous region copies (cp.async) ------------------------------------------------------
+// The query kernels keep many members' regions in flight per warp by copying them global ->
+// shared with cp.async (no registers held while a copy is outstanding), in commit groups of one
+// batch each; a warp waits for its oldest group, then reads the batch from shared memory.
+__device__ __forceinline__ void cp_async4(uint32_t *dst, const uint32_t *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+// Copies region words [0, W) at src and the deterministic bucket at det to slot[0, W + 3).
+__device__ __forceinline__ void region_copy_async(uint32_t *slot, const uint32_t *src,
+                                                  const uint32_t *det, uint32_t W, uint32_t lane) {
+  for (uint32_t w = lane; w < W; w += 32) cp_async4(slot + w, src + w);
+  if (lane < 3) cp_async4(slot + W + lane, det + lane);
+}
+
 // Warp-aggregated counter add: lanes in `active` holding the same key add one each to ctr[key]
 // with one atomic per distinct key; returns this lane's slot (old value + rank among its key's
 // lanes). stage is a 32-word per-warp shared array used to hand the base to the key's lanes.

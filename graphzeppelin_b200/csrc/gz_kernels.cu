@@ -687,46 +687,72 @@ __global__ void k_bv_reset(uint32_t V, uint32_t *parent) {
   if (v < V) parent[v] = v;
 }
 
+// Shared memory of the round-0 and merge kernels, per warp: two batches of KB member slots of
+// W + 3 words (the ring the cp.async copies land in) and one stage of W + 3 words.
+__host__ __device__ constexpr uint32_t bv_warp_words(uint32_t W, int KB) { return (2 * KB + 1) * (W + 3); }
+
 // Round 0 (run_round_zero, src/cc_sketch_alg.cpp:223-244): every vertex sketch samples its
 // sample 0 -- columns 0..CPS-1 and the deterministic bucket. A warp takes 32 consecutive
-// vertices, loads them KB at a time (all loads of a batch in flight together) and samples each
-// through its shared-memory stage; lane i keeps vertex i's result, and the 32 results are then
-// applied by the 32 lanes at once, so the union-find chains of one warp overlap.
+// vertices at a time, in batches of KB whose regions are copied to shared memory with cp.async
+// one batch ahead (also across its 32-vertex groups), and samples each vertex from there; lane
+// i keeps vertex i's result, and the 32 results are applied by the 32 lanes at once, so the
+// union-find chains of one warp overlap.
 template <int CPS, int KB>
-__global__ void __launch_bounds__(256, CPS == 1 ? 3 : 1) k_bv_round0(BoruvkaGeom g, const uint32_t *__restrict__ sk_words,
+__global__ void __launch_bounds__(256) k_bv_round0(BoruvkaGeom g, const uint32_t *__restrict__ sk_words,
                                                    BoruvkaBufs b) {
-  constexpr int NW = Region<CPS>::kNW;
-  extern __shared__ uint32_t bv_stage[];
+  extern __shared__ uint32_t bv_smem[];
+  constexpr uint32_t BPG = 32 / KB;  // batches per 32-vertex group
   const uint32_t lane = threadIdx.x & 31;
-  uint32_t *st = bv_stage + (threadIdx.x >> 5) * Region<CPS>::kStage;
+  const uint32_t W = 3 * CPS * g.B, SW = W + 3, detw = 3 * g.C * g.B;
+  uint32_t *ring = bv_smem + (threadIdx.x >> 5) * bv_warp_words(W, KB);
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  const uint32_t W = 3 * CPS * g.B, detw = 3 * g.C * g.B;
-  for (uint32_t base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; base < g.V;
-       base += nwarps * 32) {
-    const uint32_t n = g.V - base < 32 ? g.V - base : 32;
-    int my_res = 1;
-    uint64_t my_idx = 0;
-    for (uint32_t i = 0; i < n; i += KB) {
-      uint32_t x[KB][NW], dw[KB];
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t ngroups = (g.V + 31) / 32;
+  auto issue = [&](uint32_t t) {  // batch t of this warp -> ring half t & 1
+    const uint32_t grp = gw + (t / BPG) * nwarps;
+    if (grp < ngroups) {
+      const uint32_t v0 = grp * 32 + (t % BPG) * KB;
+      uint32_t *half = ring + (t & 1) * KB * SW;
 #pragma unroll
       for (int k = 0; k < KB; ++k)
-        if (i + k < n) {
-          const uint32_t *sk = sk_words + (uint64_t)(base + i + k) * g.sketch_words;
-          region_load(sk, sk + detw, W, lane, x[k], dw[k]);
-        }
-#pragma unroll
-      for (int k = 0; k < KB; ++k)
-        if (i + k < n) {
-          uint64_t idx;
-          const int res = warp_sample_region<CPS>(x[k], dw[k], W, g.B, g.flip_chk, st, &idx);
-          if (lane == i + k) {
-            my_res = res;
-            my_idx = idx;
-          }
+        if (v0 + k < g.V) {
+          const uint32_t *sk = sk_words + (uint64_t)(v0 + k) * g.sketch_words;
+          region_copy_async(half + k * SW, sk, sk + detw, W, lane);
         }
     }
-    if (lane < n) handle_result(my_res, my_idx, 0, base + lane, g, b);
+    cp_async_commit();
+  };
+  if (gw >= ngroups) return;
+  int my_res = 1;
+  uint64_t my_idx = 0;
+  issue(0);
+  for (uint32_t t = 0;; ++t) {
+    const uint32_t grp = gw + (t / BPG) * nwarps;
+    if (grp >= ngroups) break;
+    issue(t + 1);
+    cp_async_wait<1>();
+    __syncwarp();
+    const uint32_t v0 = grp * 32 + (t % BPG) * KB;
+    const uint32_t *half = ring + (t & 1) * KB * SW;
+#pragma unroll 1
+    for (int k = 0; k < KB; ++k)
+      if (v0 + k < g.V) {
+        uint64_t idx;
+        const int res = warp_sample_smem<CPS>(half + k * SW, W, g.B, g.flip_chk, &idx);
+        if (lane == (t % BPG) * KB + k) {
+          my_res = res;
+          my_idx = idx;
+        }
+      }
+    __syncwarp();
+    if (t % BPG == BPG - 1) {
+      if (grp * 32 + lane < g.V) handle_result(my_res, my_idx, 0, grp * 32 + lane, g, b);
+      __syncwarp();
+      my_res = 1;
+      my_idx = 0;
+    }
   }
+  cp_async_wait<0>();
 }
 
 // Root of every vertex and members per root; lanes of a warp that share a root add to its
@@ -763,7 +789,7 @@ __global__ void __launch_bounds__(256) k_bv_group(uint32_t V, uint32_t acc_words
                                                   uint32_t *fill, const uint32_t *minv,
                                                   uint32_t *order, uint32_t *order_comp,
                                                   uint32_t *comp_start, uint32_t *comp_key,
-                                                  uint32_t *ncomp, uint32_t *acc) {
+                                                  uint32_t *ncomp, uint32_t *acc, uint32_t *big) {
   __shared__ uint32_t stage[8][32];
   const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t active = __ballot_sync(kFull, v < V);
@@ -781,6 +807,7 @@ __global__ void __launch_bounds__(256) k_bv_group(uint32_t V, uint32_t acc_words
     if (start / span != (end - 1) / span) {
       uint32_t *ac = acc + (uint64_t)c * acc_words;
       for (uint32_t i = 0; i < acc_words; ++i) ac[i] = 0;
+      if (2ull * cnt[r] > V) *big = c;  // at most one component holds over half the vertices
     }
   }
   if (v == 0) {
@@ -792,26 +819,54 @@ __global__ void __launch_bounds__(256) k_bv_group(uint32_t V, uint32_t acc_words
 
 // perform_boruvka_round (src/cc_sketch_alg.cpp:246-380) for round >= 1: each warp XOR-merges
 // sample `round` (columns round*CPS .. +CPS, one contiguous word run) + the deterministic bucket
-// over `span` consecutive grouped members, KB members' loads in flight at a time; components
-// wholly inside the span are sampled right here, the rest are combined in acc (per component:
-// CPS*B column buckets, then the deterministic one) with one coalesced atomicXor per word.
-template <int CPS, int KB>
-__global__ void __launch_bounds__(256, CPS == 1 ? 3 : 1) k_bv_merge(BoruvkaGeom g, uint32_t round,
+// over its `span` (<= 32) consecutive grouped members, copied to shared memory with cp.async in
+// batches of KB, one batch ahead. A component wholly inside the span is sampled right here
+// (results applied 32 at a time by the lanes); a component covering the whole span leaves this
+// warp's XOR in its partial slot (k_bv_reduce_parts folds those); the parts of components
+// crossing a span edge go to acc (per component: CPS*B column buckets, then the deterministic
+// one) with one coalesced atomicXor per word.
+template <int CPS, int NW, int KB>
+__global__ void __launch_bounds__(256) k_bv_merge(BoruvkaGeom g, uint32_t round,
                                                   const uint32_t *__restrict__ sk_words, BoruvkaBufs b) {
-  constexpr int NW = Region<CPS>::kNW;
-  extern __shared__ uint32_t bv_stage[];
+  extern __shared__ uint32_t bv_smem[];
   const uint32_t lane = threadIdx.x & 31;
-  uint32_t *st = bv_stage + (threadIdx.x >> 5) * Region<CPS>::kStage;
+  const uint32_t W = 3 * CPS * g.B, SW = W + 3;
+  uint32_t *ring = bv_smem + (threadIdx.x >> 5) * bv_warp_words(W, KB);
+  uint32_t *st = ring + 2 * KB * SW;
   const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint64_t p0 = (uint64_t)w * g.span;
   if (p0 >= g.V) return;
-  const uint32_t p1 = (uint32_t)(p0 + g.span < (uint64_t)g.V ? p0 + g.span : (uint64_t)g.V);
+  const uint32_t n = (uint32_t)(g.V - p0 < g.span ? g.V - p0 : g.span);  // span <= 32
+  const uint32_t p1 = (uint32_t)p0 + n;
   const uint32_t col = 3 * round * CPS * g.B, detw = 3 * g.C * g.B;
-  const uint32_t W = 3 * CPS * g.B;
-  uint32_t acc[NW], dacc = 0;
+  // the component merged from its complement: its members are skipped, and every other
+  // member's words are also XORed into its acc
+  const uint32_t big = g.complement ? *b.big : 0xffffffffu;
+  if (big != 0xffffffffu && b.comp_start[big] <= p0 && b.comp_start[big + 1] >= p1) {
+    if (lane == 0) b.part_comp[w] = 0xffffffffu;
+    return;
+  }
+  const uint32_t my_v = lane < n ? b.order[p0 + lane] : 0u;
+  const uint32_t my_c = lane < n ? b.order_comp[p0 + lane] : 0u;
+  auto issue = [&](uint32_t t) {
+    uint32_t *half = ring + (t & 1) * KB * SW;
 #pragma unroll
-  for (int k = 0; k < NW; ++k) acc[k] = 0;
-  uint32_t cur = b.order_comp[p0];
+    for (int k = 0; k < KB; ++k) {
+      const uint32_t m = t * KB + k;
+      if (m < n && __shfl_sync(kFull, my_c, m) != big) {
+        const uint32_t v = __shfl_sync(kFull, my_v, m);
+        const uint32_t *sk = sk_words + (uint64_t)v * g.sketch_words;
+        region_copy_async(half + k * SW, sk + col, sk + detw, W, lane);
+      }
+    }
+    cp_async_commit();
+  };
+  issue(0);
+  uint32_t acc[NW], dacc = 0, cpl[NW], dcpl = 0;
+#pragma unroll
+  for (int k = 0; k < NW; ++k) acc[k] = cpl[k] = 0;
+  uint32_t cur = 0xffffffffu;
+  bool whole = false;  // one component covers [p0, p1)
   // results of components sampled here: lane j holds the j-th, applied 32 at a time
   int my_res = 1;
   uint64_t my_idx = 0;
@@ -824,16 +879,34 @@ __global__ void __launch_bounds__(256, CPS == 1 ? 3 : 1) k_bv_merge(BoruvkaGeom 
   auto flush = [&](uint32_t comp) {
     const uint32_t s = b.comp_start[comp], e = b.comp_start[comp + 1];
     if (s >= p0 && e <= p1) {
+#pragma unroll
+      for (int k = 0; k < NW; ++k) {
+        const uint32_t wi = k * 32 + lane;
+        if (wi < W) st[wi] = acc[k];
+      }
+      if (lane < 3) st[W + lane] = dacc;
+      __syncwarp();
       uint64_t idx;
-      const int res = warp_sample_region<CPS>(acc, dacc, W, g.B, g.flip_chk, st, &idx);
+      const int res = warp_sample_smem<CPS>(st, W, g.B, g.flip_chk, &idx);
+      __syncwarp();
       if (lane == nres) {
         my_res = res;
         my_idx = idx;
         my_key = b.comp_key[comp];
       }
       if (++nres == 32) apply();
+    } else if (s <= p0 && e >= p1) {
+      uint32_t *pt = b.part + (uint64_t)w * SW;
+#pragma unroll
+      for (int k = 0; k < NW; ++k) {
+        const uint32_t wi = k * 32 + lane;
+        if (wi < W) pt[wi] = acc[k];
+      }
+      if (lane < 3) pt[W + lane] = dacc;
+      if (lane == 0) b.part_comp[w] = comp;
+      whole = true;
     } else {
-      uint32_t *ac = b.acc + (uint64_t)comp * (W + 3);
+      uint32_t *ac = b.acc + (uint64_t)comp * SW;
 #pragma unroll
       for (int k = 0; k < NW; ++k) {
         const uint32_t wi = k * 32 + lane;
@@ -842,38 +915,112 @@ __global__ void __launch_bounds__(256, CPS == 1 ? 3 : 1) k_bv_merge(BoruvkaGeom 
       if (lane < 3 && dacc) atomicXor(ac + W + lane, dacc);
     }
   };
-  for (uint32_t cb = (uint32_t)p0; cb < p1; cb += 32) {
-    const uint32_t n = p1 - cb < 32 ? p1 - cb : 32;
-    const uint32_t my_v = lane < n ? b.order[cb + lane] : 0u;
-    const uint32_t my_c = lane < n ? b.order_comp[cb + lane] : 0u;
-    for (uint32_t i = 0; i < n; i += KB) {
-      uint32_t x[KB][NW], dw[KB];
+  const uint32_t nb = (n + KB - 1) / KB;
+  for (uint32_t t = 0; t < nb; ++t) {
+    if (t + 1 < nb) issue(t + 1);
+    else cp_async_commit();
+    cp_async_wait<1>();
+    __syncwarp();
+    const uint32_t *half = ring + (t & 1) * KB * SW;
 #pragma unroll
-      for (int k = 0; k < KB; ++k)
-        if (i + k < n) {
-          const uint32_t v = __shfl_sync(kFull, my_v, i + k);
-          const uint32_t *sk = sk_words + (uint64_t)v * g.sketch_words;
-          region_load(sk + col, sk + detw, W, lane, x[k], dw[k]);
+    for (int k = 0; k < KB; ++k) {
+      const uint32_t m = t * KB + k;
+      const uint32_t c = __shfl_sync(kFull, my_c, m < n ? m : 0);
+      if (m < n && c != big) {
+        if (c != cur) {
+          if (cur != 0xffffffffu) flush(cur);
+          cur = c;
+#pragma unroll
+          for (int q = 0; q < NW; ++q) acc[q] = 0;
+          dacc = 0;
         }
+        const uint32_t *sl = half + k * SW;
 #pragma unroll
-      for (int k = 0; k < KB; ++k)
-        if (i + k < n) {
-          const uint32_t c = __shfl_sync(kFull, my_c, i + k);
-          if (c != cur) {
-            flush(cur);
-            cur = c;
+        for (int q = 0; q < NW; ++q) {
+          const uint32_t wi = q * 32 + lane;
+          if (wi < W) acc[q] ^= sl[wi];
+        }
+        if (lane < 3) dacc ^= sl[W + lane];
+        if (big != 0xffffffffu) {
 #pragma unroll
-            for (int q = 0; q < NW; ++q) acc[q] = 0;
-            dacc = 0;
+          for (int q = 0; q < NW; ++q) {
+            const uint32_t wi = q * 32 + lane;
+            if (wi < W) cpl[q] ^= sl[wi];
           }
-#pragma unroll
-          for (int q = 0; q < NW; ++q) acc[q] ^= x[k][q];
-          dacc ^= dw[k];
+          if (lane < 3) dcpl ^= sl[W + lane];
         }
+      }
+    }
+    __syncwarp();
+  }
+  cp_async_wait<0>();
+  if (cur != 0xffffffffu) flush(cur);
+  apply();
+  if (big != 0xffffffffu) {
+    uint32_t *ac = b.acc + (uint64_t)big * SW;
+#pragma unroll
+    for (int k = 0; k < NW; ++k) {
+      const uint32_t wi = k * 32 + lane;
+      if (wi < W && cpl[k]) atomicXor(ac + wi, cpl[k]);
+    }
+    if (lane < 3 && dcpl) atomicXor(ac + W + lane, dcpl);
+  }
+  if (!whole && lane == 0) b.part_comp[w] = 0xffffffffu;
+}
+
+// Folds the partial slots of merge warps covered by one component into that component's acc:
+// one warp per 32 consecutive slots (KB slots' loads in flight), one atomicXor per word per
+// component per warp.
+template <int CPS, int NW, int KB>
+__global__ void __launch_bounds__(256) k_bv_reduce_parts(BoruvkaGeom g, uint32_t nslots, BoruvkaBufs b) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t s0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32;
+  if (s0 >= nslots) return;
+  const uint32_t n = nslots - s0 < 32 ? nslots - s0 : 32;
+  const uint32_t W = 3 * CPS * g.B;
+  const uint32_t my_c = lane < n ? b.part_comp[s0 + lane] : 0xffffffffu;
+  uint32_t live = __ballot_sync(kFull, my_c != 0xffffffffu);
+  if (!live) return;
+  uint32_t acc[NW], dacc = 0, cur = 0xffffffffu;
+#pragma unroll
+  for (int k = 0; k < NW; ++k) acc[k] = 0;
+  auto flush = [&]() {
+    uint32_t *ac = b.acc + (uint64_t)cur * (W + 3);
+#pragma unroll
+    for (int k = 0; k < NW; ++k) {
+      const uint32_t wi = k * 32 + lane;
+      if (wi < W && acc[k]) atomicXor(ac + wi, acc[k]);
+    }
+    if (lane < 3 && dacc) atomicXor(ac + W + lane, dacc);
+  };
+  while (live) {
+    uint32_t x[KB][NW], dw[KB], sl[KB];
+#pragma unroll
+    for (int k = 0; k < KB; ++k) {
+      sl[k] = live ? __ffs(live) - 1 : 32u;
+      if (live) live &= live - 1;
+      if (sl[k] < 32) {
+        const uint32_t *pt = b.part + (uint64_t)(s0 + sl[k]) * (W + 3);
+        region_load(pt, pt + W, W, lane, x[k], dw[k]);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < KB; ++k) {
+      if (sl[k] >= 32) break;
+      const uint32_t c = __shfl_sync(kFull, my_c, sl[k]);
+      if (c != cur) {
+        if (cur != 0xffffffffu) flush();
+        cur = c;
+#pragma unroll
+        for (int q = 0; q < NW; ++q) acc[q] = 0;
+        dacc = 0;
+      }
+#pragma unroll
+      for (int q = 0; q < NW; ++q) acc[q] ^= x[k][q];
+      dacc ^= dw[k];
     }
   }
-  flush(cur);
-  apply();
+  flush();
 }
 
 template <int CPS>
@@ -1205,9 +1352,32 @@ cudaError_t sketch_xor_raw(uint8_t *sketches, uint32_t words, uint32_t v, const 
   return cudaGetLastError();
 }
 
-// per-block stage of the round-0 and merge kernels: 8 warps x Region<CPS>::kStage words
-size_t bv_stage_bytes(int cps) {
-  return 8 * sizeof(uint32_t) * (cps == 1 ? dev::Region<1>::kStage : dev::Region<7>::kStage);
+__global__ void k_total_xor(const uint32_t *__restrict__ sk, uint32_t V, uint32_t words,
+                            uint32_t *total) {
+  const uint32_t wd = blockIdx.x * blockDim.x + threadIdx.x;
+  if (wd >= words) return;
+  uint32_t x = 0;
+  for (uint32_t v = blockIdx.y; v < V; v += gridDim.y) x ^= sk[(uint64_t)v * words + wd];
+  if (x) atomicXor(total + wd, x);
+}
+
+// Launch shape of the round-0 and merge kernels: members per cp.async batch, and the dynamic
+// shared memory of a 256-thread block (8 warps).
+int bv_batch(int cps) { return cps == 1 ? 8 : 1; }
+size_t bv_smem_bytes(const BoruvkaGeom &g) {
+  return 8 * sizeof(uint32_t) * bv_warp_words(3 * g.cps * g.B, bv_batch(g.cps));
+}
+template <class K>
+cudaError_t bv_smem_attr(K kern, size_t smem) {
+  return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+cudaError_t sketch_total_xor(const uint8_t *sketches, uint32_t V, uint32_t sketch_words,
+                             uint32_t *total, cudaStream_t s) {
+  const dim3 grid(blocks_for(sketch_words, 256), std::max<uint32_t>(1, std::min<uint32_t>(V, 512)));
+  k_total_xor<<<grid, 256, 0, s>>>(reinterpret_cast<const uint32_t *>(sketches), V, sketch_words, total);
+  g_launches++;
+  return cudaGetLastError();
 }
 
 cudaError_t boruvka_reset(const BoruvkaGeom &g, const BoruvkaBufs &b, cudaStream_t s) {
@@ -1220,12 +1390,22 @@ cudaError_t boruvka_reset(const BoruvkaGeom &g, const BoruvkaBufs &b, cudaStream
 
 cudaError_t boruvka_round0(const BoruvkaGeom &g, const uint8_t *sketches, const BoruvkaBufs &b,
                            cudaStream_t s) {
-  // one warp per 32 vertices, 8 warps per block, grid-stride beyond 8 blocks per SM
-  const unsigned blocks = std::min<unsigned>(blocks_for((uint64_t)g.V, 256), num_sms() * 8);
+  // one warp per 32 vertices, 8 warps per block; a grid of the resident blocks strides on
   const uint32_t *sk = reinterpret_cast<const uint32_t *>(sketches);
-  if (g.cps == 1) k_bv_round0<1, 4><<<blocks, 256, bv_stage_bytes(1), s>>>(g, sk, b);
-  else if (g.cps == 7) k_bv_round0<7, 1><<<blocks, 256, bv_stage_bytes(7), s>>>(g, sk, b);
-  else return cudaErrorInvalidValue;
+  const size_t smem = bv_smem_bytes(g);
+  auto launch = [&](auto kern) -> cudaError_t {
+    cudaError_t e = bv_smem_attr(kern, smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem) != cudaSuccess || per_sm < 1)
+      per_sm = 1;
+    const unsigned blocks = std::min<unsigned>(blocks_for((uint64_t)g.V, 256), num_sms() * per_sm);
+    kern<<<blocks, 256, smem, s>>>(g, sk, b);
+    return cudaSuccess;
+  };
+  cudaError_t e = g.cps == 1 ? launch(k_bv_round0<1, 8>)
+                  : g.cps == 7 ? launch(k_bv_round0<7, 1>) : cudaErrorInvalidValue;
+  if (e != cudaSuccess) return e;
   g_launches++;
   return cudaGetLastError();
 }
@@ -1235,6 +1415,7 @@ cudaError_t boruvka_round(const BoruvkaGeom &g, uint32_t round, const uint8_t *s
   const uint32_t V = g.V;
   cudaMemsetAsync(b.cnt, 0, sizeof(uint32_t) * V, s);
   cudaMemsetAsync(b.fill, 0, sizeof(uint32_t) * V, s);
+  cudaMemsetAsync(b.big, 0xff, sizeof(uint32_t), s);
   if (trace) cudaMemsetAsync(b.minv, 0xff, sizeof(uint32_t) * V, s);
   k_bv_label<<<blocks_for(V, 256), 256, 0, s>>>(V, b.parent, b.label, b.cnt,
                                                  trace ? b.minv : nullptr);
@@ -1247,14 +1428,27 @@ cudaError_t boruvka_round(const BoruvkaGeom &g, uint32_t round, const uint8_t *s
   k_bv_group<<<blocks_for(V, 256), 256, 0, s>>>(V, (g.cps * g.B + 1) * 3, g.span, b.label, b.packed, b.scan_total,
                                                  b.cnt, b.fill, trace ? b.minv : nullptr, b.order,
                                                  b.order_comp, b.comp_start, b.comp_key, b.ncomp,
-                                                 b.acc);
+                                                 b.acc, b.big);
   g_launches++;
   const uint64_t warps = (V + g.span - 1) / g.span;
   const uint32_t *sk = reinterpret_cast<const uint32_t *>(sketches);
   const unsigned sblocks = std::min<unsigned>(blocks_for((uint64_t)V * 32, 256), num_sms() * 16);
-  if (g.cps == 1) k_bv_merge<1, 4><<<blocks_for(warps * 32, 256), 256, bv_stage_bytes(1), s>>>(g, round, sk, b);
-  else k_bv_merge<7, 1><<<blocks_for(warps * 32, 256), 256, bv_stage_bytes(7), s>>>(g, round, sk, b);
-  g_launches++;
+  const unsigned mblocks = blocks_for(warps * 32, 256), rblocks = blocks_for(warps, 256);
+  const size_t smem = bv_smem_bytes(g);
+  if (g.cps == 1 && g.B <= 42) {
+    if ((e = bv_smem_attr(k_bv_merge<1, 4, 8>, smem)) != cudaSuccess) return e;
+    k_bv_merge<1, 4, 8><<<mblocks, 256, smem, s>>>(g, round, sk, b);
+    k_bv_reduce_parts<1, 4, 8><<<rblocks, 256, 0, s>>>(g, (uint32_t)warps, b);
+  } else if (g.cps == 1) {
+    if ((e = bv_smem_attr(k_bv_merge<1, 6, 8>, smem)) != cudaSuccess) return e;
+    k_bv_merge<1, 6, 8><<<mblocks, 256, smem, s>>>(g, round, sk, b);
+    k_bv_reduce_parts<1, 6, 4><<<rblocks, 256, 0, s>>>(g, (uint32_t)warps, b);
+  } else {
+    if ((e = bv_smem_attr(k_bv_merge<7, dev::Region<7>::kNW, 1>, smem)) != cudaSuccess) return e;
+    k_bv_merge<7, dev::Region<7>::kNW, 1><<<mblocks, 256, smem, s>>>(g, round, sk, b);
+    k_bv_reduce_parts<7, dev::Region<7>::kNW, 1><<<rblocks, 256, 0, s>>>(g, (uint32_t)warps, b);
+  }
+  g_launches += 2;
   if (g.cps == 1) k_bv_sample_spanning<1><<<sblocks, 256, 0, s>>>(g, round, b);
   else k_bv_sample_spanning<7><<<sblocks, 256, 0, s>>>(g, round, b);
   g_launches++;

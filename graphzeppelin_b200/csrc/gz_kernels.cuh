@@ -147,6 +147,9 @@ struct BoruvkaBufs {
   uint32_t *comp_key;    // V
   uint32_t *ncomp;       // 1
   uint32_t *acc;         // V * (B+1) * 3 words: merged buckets of components spanning warps
+  uint32_t *part;        // per merge warp: its members' XOR when one component covers its span
+  uint32_t *part_comp;   // per merge warp: that component, or ~0
+  uint32_t *big;         // 1   the component holding more than half the vertices, or ~0
   uint32_t *flags;       // [0] modified
   uint64_t *forest;      // V   spanning-forest edge indices
   uint32_t *forest_n;    // 1
@@ -156,12 +159,24 @@ struct BoruvkaBufs {
   uint32_t *status;
 };
 
+// Grouped members XOR-merged by one warp per Boruvka round (the per-warp partial slots are
+// sized by it).
+constexpr uint32_t kBoruvkaSpan = 32;
+
 struct BoruvkaGeom {
   uint32_t V, C, B, sketch_words;
   uint64_t flip_chk;
   uint32_t span;     // members merged per warp
   uint32_t cps = 1;  // columns per sample: round r merges and scans columns r*cps .. r*cps+cps-1
+  // Every update reached both endpoint sketches (records, gz_update), so the XOR of all vertex
+  // sketches is zero and a component's merged sketch equals the XOR over all other vertices:
+  // the largest component (over half the vertices) is merged from its complement.
+  uint32_t complement = 0;
 };
+
+// XOR of every vertex sketch, word by word, into total[sketch_words] (zeroed by the caller).
+cudaError_t sketch_total_xor(const uint8_t *sketches, uint32_t V, uint32_t sketch_words,
+                             uint32_t *total, cudaStream_t s);
 
 cudaError_t boruvka_reset(const BoruvkaGeom &g, const BoruvkaBufs &b, cudaStream_t s);
 cudaError_t boruvka_round0(const BoruvkaGeom &g, const uint8_t *sketches, const BoruvkaBufs &b,

@@ -186,6 +186,46 @@ def test_queries_during_stream(gz, oracle_mod):
     assert driver.get_total_updates() == 2 * n
 
 
+@pytest.mark.parametrize("path", ["records", "update_batch", "loaded"])
+def test_giant_component_merge_paths(gz, oracle_mod, path, tmp_path):
+    """A component holding over half the vertices is merged from the XOR of all other vertex
+    sketches when every update reached both endpoints (records; a loaded file whose sketches XOR
+    to zero), and by the plain merge once apply_update_batch has made the sketches one-sided.
+    Labels, rounds and every round's samples equal the oracle's on all three."""
+    from graphzeppelin_b200 import streams as S
+    V, seed = 3000, 91
+    st = S.erdos_renyi_stream(V, 0.0025, seed=7, churn_fraction=0.3)
+    alg = _alg(gz, V, seed)
+    if path == "update_batch":
+        r = st.records
+        for a, b_ in zip(r["src"].tolist(), r["dst"].tolist()):
+            alg.apply_update_batch(0, a, [b_])
+            alg.apply_update_batch(0, b_, [a])
+    else:
+        alg.ingest_records(st)
+    if path == "loaded":
+        f = str(tmp_path / "sk.bin")
+        alg.write_binary(f)
+        alg.close()
+        alg = gz.CCSketchAlg.construct_from_serialized_data(f)
+    alg.set_trace(True)
+    cc = alg.connected_components()
+    osk = oracle_mod.OracleSketches(V, seed)
+    osk.apply_records(st.raw())
+    assert (alg.dump_sketches() == osk.data).all()
+    rc, lab, rounds, tr = osk.boruvka()
+    assert rc == 0
+    assert np.bincount(lab).max() * 2 > V  # the case has a giant component
+    assert (canonical(cc.parent_arr) == lab).all()
+    assert alg.last_query_rounds == rounds
+    got = alg.get_trace()
+    assert got.size == tr.size
+    for fld in ("round", "key", "result", "idx"):
+        assert (got[fld] == tr[fld]).all(), fld
+    n, exact = oracle_mod.exact_cc(V, st.raw())
+    assert cc.size() == n
+
+
 @pytest.mark.parametrize("V", [2, 3, 5, 17, 100, 301])
 def test_odd_vertex_counts(gz, oracle_mod, V):
     from graphzeppelin_b200 import streams as S
