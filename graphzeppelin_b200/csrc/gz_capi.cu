@@ -178,28 +178,26 @@ struct gz_alg {
   bool eager = false, host_answer = false, boruvka_ran = false;
   std::vector<uint32_t> hdsu;
   std::unordered_set<uint64_t> hforest;
-  // snapshot queries (gz_query_submit / gz_query_wait): a copy of the sketches taken at
-  // submission, queried by a worker thread on its own stream and buffers while ingest goes on
-  struct SnapResult {
-    int rc = GZ_OK;
-    std::string err;
-    uint32_t ncc = 0, rounds = 0;
-    std::vector<uint32_t> labels;
+  // the query graph of blocking queries (device-driven Boruvka rounds)
+  gz::BoruvkaGraph qgraph;
+  uint32_t *h_qpin = nullptr;  // pinned: rounds, out-of-samples flag, components
+  // queries by ticket (gz_query_submit / gz_query_wait): the query graph enqueued on the
+  // handle's stream behind every update submitted before it, with its own buffers, so the
+  // answer is the state at submission while later updates queue up behind it
+  struct Ticket {
+    cudaEvent_t done = nullptr;
+    uint32_t *labels = nullptr;  // pinned, V entries
+    uint32_t *pin = nullptr;     // pinned: rounds, out-of-samples flag, components, status
   };
-  struct Snap {
-    uint8_t *d_sk = nullptr;
+  struct Tickets {
     gz::BoruvkaBufs bv{};
-    uint32_t *d_final = nullptr, *d_ncc = nullptr, *d_status = nullptr, *h_pin = nullptr;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t before = nullptr, copied = nullptr;
-    std::thread worker;
-    std::mutex m;
-    std::condition_variable cv;
-    bool stop = false, queued = false, running = false;
-    bool complement = false;  // the sketches' XOR was zero when the job was submitted
-    uint64_t next_ticket = 1, job = 0;
-    std::map<uint64_t, SnapResult> results;
-  } snap;
+    gz::BoruvkaGraph graph;
+    uint32_t *d_final = nullptr, *d_ncc = nullptr;
+    std::map<uint64_t, Ticket> live;
+    std::vector<Ticket> pool;
+    uint64_t next = 1;
+  } tq;
+  uint32_t deferred_status = 0;  // device status bits seen by a ticket, reported at the next flush
   std::atomic<bool> query_running{false};
   size_t last_rounds = 0;
   uint32_t last_ncc = 0;
@@ -402,10 +400,13 @@ int init_alg(gz_alg *h, uint32_t V, uint64_t seed, double sf, double bf, bool cu
   return GZ_OK;
 }
 
-void snap_shutdown(gz_alg *h);
+void tickets_shutdown(gz_alg *h);
+void free_bv(gz::BoruvkaBufs &b);
 
 void destroy_alg(gz_alg *h) {
-  snap_shutdown(h);
+  tickets_shutdown(h);
+  gz::boruvka_graph_free(h->qgraph);
+  host_free(h->h_qpin);
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
   dev_free(h->d_sk);
@@ -449,6 +450,8 @@ void destroy_alg(gz_alg *h) {
   dev_free(b.part);
   dev_free(b.part_comp);
   dev_free(b.big);
+  dev_free(b.round);
+  b.ctl = nullptr;
   dev_free(b.flags);
   dev_free(b.forest);
   dev_free(b.forest_n);
@@ -621,7 +624,8 @@ int stage_entry(gz_alg *h, uint32_t v, uint32_t w) {
 int check_status(gz_alg *h) {
   GZ_CUDA(cudaMemcpyAsync(h->h_status, h->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
   GZ_CUDA(cudaStreamSynchronize(h->stream));
-  const uint32_t st = h->h_status[0];
+  const uint32_t st = h->h_status[0] | h->deferred_status;
+  h->deferred_status = 0;
   if (st) {
     GZ_CUDA(cudaMemsetAsync(h->d_status, 0, sizeof(uint32_t), h->stream));
     GZ_CUDA(cudaStreamSynchronize(h->stream));
@@ -728,6 +732,8 @@ int alloc_bv(gz::BoruvkaBufs &b, size_t V, size_t acc_words, uint32_t *status) {
   GZ_TRY(dev_alloc(&b.part, warps * acc_words));
   GZ_TRY(dev_alloc(&b.part_comp, warps));
   GZ_TRY(dev_alloc(&b.big, 1));
+  GZ_TRY(dev_alloc(&b.round, 4));
+  b.ctl = b.round + 1;
   GZ_TRY(dev_alloc(&b.flags, 4));
   GZ_TRY(dev_alloc(&b.forest, V));
   GZ_TRY(dev_alloc(&b.forest_n, 1));
@@ -754,138 +760,65 @@ void free_bv(gz::BoruvkaBufs &b) {
   dev_free(b.part);
   dev_free(b.part_comp);
   dev_free(b.big);
+  dev_free(b.round);
+  b.ctl = nullptr;
   dev_free(b.flags);
   dev_free(b.forest);
   dev_free(b.forest_n);
   dev_free(b.trace_n);
 }
 
-// boruvka_emulation (src/cc_sketch_alg.cpp:464-513) on the sketches at sk with buffers b on
-// stream s, driven from the host one device round at a time until a round neither FAILs nor
-// merges; pin is a pinned 4-word host mirror. GZ_ERR_OUT_OF_SAMPLES when round `samples` is
-// reached (rounds_out = that round).
-int boruvka_core(const gz::BoruvkaGeom &g, uint32_t samples, const uint8_t *sk, gz::BoruvkaBufs &b,
-                 uint32_t *d_final, uint32_t *d_ncc, uint32_t *pin, bool trace, cudaStream_t s,
-                 uint32_t &rounds_out, uint32_t &ncc_out) {
-  auto modified = [&](bool &m) -> int {
-    GZ_CUDA(cudaMemcpyAsync(pin + 1, b.flags, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-    GZ_CUDA(cudaStreamSynchronize(s));
-    m = pin[1] != 0;
-    return GZ_OK;
-  };
-  GZ_CUDA(gz::boruvka_reset(g, b, s));
-  GZ_CUDA(cudaMemsetAsync(b.flags, 0, sizeof(uint32_t), s));
-  GZ_CUDA(gz::boruvka_round0(g, sk, b, s));
-  bool mod = false;
-  GZ_TRY(modified(mod));
-  uint32_t round = 0;
-  while (mod) {
-    ++round;
-    if (round >= samples) {
-      rounds_out = round;
-      return GZ_ERR_OUT_OF_SAMPLES;
-    }
-    GZ_CUDA(cudaMemsetAsync(b.flags, 0, sizeof(uint32_t), s));
-    GZ_CUDA(gz::boruvka_round(g, round, sk, b, trace, s));
-    GZ_TRY(modified(mod));
-  }
-  GZ_CUDA(gz::boruvka_final(g, b, d_final, d_ncc, s));
+// boruvka_emulation (src/cc_sketch_alg.cpp:464-513) on the sketches at sk with buffers b: the
+// query graph (every round on the device, no host round trip) enqueued on stream s, then the
+// rounds, the out-of-samples flag and the component count copied to pin[0..2] (pinned).
+int boruvka_enqueue(gz_alg *h, gz::BoruvkaGraph &q, const gz::BoruvkaGeom &g, const uint8_t *sk,
+                    gz::BoruvkaBufs &b, uint32_t *d_final, uint32_t *d_ncc, uint32_t *pin,
+                    cudaStream_t s) {
+  GZ_CUDA(gz::boruvka_graph_launch(q, g, h->samples, sk, b, d_final, d_ncc, s));
+  GZ_CUDA(cudaMemcpyAsync(pin, b.ctl, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   GZ_CUDA(cudaMemcpyAsync(pin + 2, d_ncc, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  GZ_CUDA(cudaStreamSynchronize(s));
-  ncc_out = pin[2];
-  rounds_out = round;
   return GZ_OK;
 }
 
-// ---- snapshot queries ---------------------------------------------------------------------------
-void snap_worker(gz_alg *h) {
-  cudaSetDevice(h->device);
-  auto &S = h->snap;
-  for (;;) {
-    uint64_t t;
-    gz::BoruvkaGeom bg = h->bgeom();
-    {
-      std::unique_lock<std::mutex> lk(S.m);
-      S.cv.wait(lk, [&] { return S.stop || S.queued; });
-      if (!S.queued) return;
-      S.queued = false;
-      S.running = true;
-      t = S.job;
-      bg.complement = S.complement ? 1 : 0;
-    }
-    gz_alg::SnapResult r;
-    r.rc = boruvka_core(bg, h->samples, S.d_sk, S.bv, S.d_final, S.d_ncc, S.h_pin, false, S.stream,
-                        r.rounds, r.ncc);
-    if (r.rc == GZ_ERR_OUT_OF_SAMPLES) {
-      r.err = "This sketch (seed=" + std::to_string(h->seed) + ", max samples=" + std::to_string(h->samples) +
-              ") cannot be sampled more times (cur idx=" + std::to_string(r.rounds) + ")!";
-    } else if (r.rc == GZ_OK) {
-      r.labels.resize(h->V);
-      cudaError_t e = cudaMemcpyAsync(r.labels.data(), S.d_final, sizeof(uint32_t) * h->V,
-                                      cudaMemcpyDeviceToHost, S.stream);
-      if (e == cudaSuccess) e = cudaMemcpyAsync(S.h_pin, S.d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, S.stream);
-      if (e == cudaSuccess) e = cudaStreamSynchronize(S.stream);
-      if (e != cudaSuccess) {
-        r.rc = GZ_ERR_CUDA;
-        r.err = cudaGetErrorString(e);
-      } else if (S.h_pin[0]) {
-        r.rc = (S.h_pin[0] & gz::kStatusTimeout) ? GZ_ERR_TIMEOUT : GZ_ERR_BAD_SAMPLE;
-        r.err = "the snapshot query's device status reported an error";
-        cudaMemsetAsync(S.d_status, 0, sizeof(uint32_t), S.stream);
-        cudaStreamSynchronize(S.stream);
-      }
-    } else {
-      r.err = gz_last_error();
-    }
-    {
-      std::lock_guard<std::mutex> lk(S.m);
-      S.results[t] = std::move(r);
-      S.running = false;
-    }
-    S.cv.notify_all();
-  }
+// Kernel launches of a finished query graph (its loop body ran once per round >= 1).
+void boruvka_account(const gz::BoruvkaGraph &q, const uint32_t *pin) {
+  const uint32_t body_runs = pin[1] ? pin[0] - 1 : pin[0];
+  gz::add_launches(q.fixed_kernels + (uint64_t)body_runs * q.round_kernels);
 }
 
-int snap_ensure(gz_alg *h) {
-  auto &S = h->snap;
-  if (S.worker.joinable()) return GZ_OK;
-  GZ_TRY(dev_alloc(&S.d_sk, (size_t)h->V * h->sketch_bytes));
-  GZ_TRY(dev_alloc(&S.d_status, 4));
-  GZ_TRY(alloc_bv(S.bv, h->V, (size_t)(h->cps * h->B + 1) * 3, S.d_status));
-  GZ_TRY(dev_alloc(&S.d_final, h->V));
-  GZ_TRY(dev_alloc(&S.d_ncc, 1));
-  GZ_TRY(host_alloc(&S.h_pin, 4));
-  GZ_CUDA(cudaStreamCreateWithFlags(&S.stream, cudaStreamNonBlocking));
-  GZ_CUDA(cudaEventCreateWithFlags(&S.before, cudaEventDisableTiming));
-  GZ_CUDA(cudaEventCreateWithFlags(&S.copied, cudaEventDisableTiming));
-  GZ_CUDA(cudaMemsetAsync(S.d_status, 0, 16, S.stream));
-  GZ_CUDA(cudaStreamSynchronize(S.stream));
-  S.worker = std::thread(snap_worker, h);
+std::string out_of_samples_msg(const gz_alg *h, uint32_t round) {
+  return "This sketch (seed=" + std::to_string(h->seed) + ", max samples=" + std::to_string(h->samples) +
+         ") cannot be sampled more times (cur idx=" + std::to_string(round) + ")!";
+}
+
+// ---- queries by ticket ----------------------------------------------------------------------------
+int tickets_ensure(gz_alg *h) {
+  auto &T = h->tq;
+  if (T.d_final) return GZ_OK;
+  GZ_TRY(alloc_bv(T.bv, h->V, (size_t)(h->cps * h->B + 1) * 3, h->d_status));
+  GZ_TRY(dev_alloc(&T.d_ncc, 1));
+  GZ_TRY(dev_alloc(&T.d_final, h->V));
   return GZ_OK;
 }
 
-void snap_shutdown(gz_alg *h) {
-  auto &S = h->snap;
-  if (S.worker.joinable()) {
-    {
-      std::lock_guard<std::mutex> lk(S.m);
-      S.stop = true;
-    }
-    S.cv.notify_all();
-    S.worker.join();
-  }
-  if (S.stream) cudaStreamSynchronize(S.stream);
-  dev_free(S.d_sk);
-  free_bv(S.bv);
-  dev_free(S.d_final);
-  dev_free(S.d_ncc);
-  dev_free(S.d_status);
-  host_free(S.h_pin);
-  if (S.before) cudaEventDestroy(S.before);
-  if (S.copied) cudaEventDestroy(S.copied);
-  if (S.stream) cudaStreamDestroy(S.stream);
-  S.before = S.copied = nullptr;
-  S.stream = nullptr;
+void ticket_free(gz_alg::Ticket &t) {
+  if (t.done) cudaEventDestroy(t.done);
+  host_free(t.labels);
+  host_free(t.pin);
+  t = gz_alg::Ticket{};
+}
+
+void tickets_shutdown(gz_alg *h) {
+  auto &T = h->tq;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (auto &kv : T.live) ticket_free(kv.second);
+  for (auto &t : T.pool) ticket_free(t);
+  T.live.clear();
+  T.pool.clear();
+  gz::boruvka_graph_free(T.graph);
+  free_bv(T.bv);
+  dev_free(T.d_final);
+  dev_free(T.d_ncc);
 }
 
 int ensure_query(gz_alg *h) {
@@ -913,24 +846,22 @@ int ensure_query(gz_alg *h) {
 // iteration until a round neither FAILs nor merges.
 int run_boruvka(gz_alg *h) {
   GZ_TRY(ensure_query(h));
+  if (!h->h_qpin) GZ_TRY(host_alloc(&h->h_qpin, 4));
   h->update_locked = true;  // stays set if the query fails, as in the reference
-  const gz::BoruvkaGeom g = h->bgeom();
   const int pi = h->prof_begin();
-  uint32_t round = 0, ncc = 0;
-  const int rc = boruvka_core(g, h->samples, h->d_sk, h->bv, h->d_final, h->d_ncc, h->h_status, h->trace,
-                              h->stream, round, ncc);
+  GZ_TRY(boruvka_enqueue(h, h->qgraph, h->bgeom(), h->d_sk, h->bv, h->d_final, h->d_ncc, h->h_qpin,
+                         h->stream));
   h->prof_end(pi, 2);
-  if (rc == GZ_ERR_OUT_OF_SAMPLES) {
+  GZ_CUDA(cudaStreamSynchronize(h->stream));
+  boruvka_account(h->qgraph, h->h_qpin);
+  const uint32_t round = h->h_qpin[0];
+  if (h->h_qpin[1]) {
     h->last_rounds = round;
-    return fail(GZ_ERR_OUT_OF_SAMPLES,
-                "This sketch (seed=" + std::to_string(h->seed) + ", max samples=" +
-                    std::to_string(h->samples) + ") cannot be sampled more times (cur idx=" +
-                    std::to_string(round) + ")!");
+    return fail(GZ_ERR_OUT_OF_SAMPLES, out_of_samples_msg(h, round));
   }
-  GZ_TRY(rc);
   h->prof_acc.query_rounds += round + 1;
   GZ_TRY(check_status(h));
-  h->last_ncc = ncc;
+  h->last_ncc = h->h_qpin[2];
   h->last_rounds = round;
   h->dsu_valid = true;
   h->labels_on_host = false;
@@ -1292,48 +1223,78 @@ int gz_flush(gz_alg_t *h) {
 int gz_query_submit(gz_alg_t *h, uint64_t *ticket) {
   if (!h || !ticket) return fail(GZ_ERR_INVALID, "null argument");
   Guard g(h);
-  GZ_TRY(flush_all(h));  // every update so far is in the sketches
-  auto &S = h->snap;
-  {
-    // one snapshot at a time: the previous query must be done with the copy
-    std::unique_lock<std::mutex> lk(S.m);
-    S.cv.wait(lk, [&] { return !S.queued && !S.running; });
+  // every update so far goes to the stream ahead of the query; nothing waits here
+  GZ_TRY(push_staged_entries(h));
+  GZ_TRY(apply_pending(h));
+  GZ_TRY(tickets_ensure(h));
+  auto &T = h->tq;
+  gz_alg::Ticket t;
+  if (!T.pool.empty()) {
+    t = T.pool.back();
+    T.pool.pop_back();
+  } else {
+    GZ_CUDA(cudaEventCreateWithFlags(&t.done, cudaEventDisableTiming));
+    const int rc1 = host_alloc(&t.labels, h->V);
+    const int rc2 = rc1 == GZ_OK ? host_alloc(&t.pin, 4) : rc1;
+    if (rc2 != GZ_OK) {
+      ticket_free(t);
+      return rc2;
+    }
   }
-  GZ_TRY(snap_ensure(h));
-  // the copy follows all sketch work so far; later sketch work waits for the copy
-  GZ_CUDA(cudaEventRecord(S.before, h->stream));
-  GZ_CUDA(cudaStreamWaitEvent(S.stream, S.before, 0));
-  GZ_CUDA(cudaMemcpyAsync(S.d_sk, h->d_sk, (size_t)h->V * h->sketch_bytes, cudaMemcpyDeviceToDevice, S.stream));
-  GZ_CUDA(cudaEventRecord(S.copied, S.stream));
-  GZ_CUDA(cudaStreamWaitEvent(h->stream, S.copied, 0));
-  {
-    std::lock_guard<std::mutex> lk(S.m);
-    S.job = S.next_ticket++;
-    S.queued = true;
-    S.complement = h->symmetric;
-    *ticket = S.job;
+  const int pi = h->prof_begin();
+  int rc = boruvka_enqueue(h, T.graph, h->bgeom(), h->d_sk, T.bv, T.d_final, T.d_ncc, t.pin, h->stream);
+  h->prof_end(pi, 2);
+  cudaError_t e = cudaSuccess;
+  if (rc == GZ_OK) e = cudaMemcpyAsync(t.labels, T.d_final, sizeof(uint32_t) * h->V, cudaMemcpyDeviceToHost, h->stream);
+  // the device status as the query left it (bits of earlier updates too), then cleared
+  if (rc == GZ_OK && e == cudaSuccess)
+    e = cudaMemcpyAsync(t.pin + 3, h->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream);
+  if (rc == GZ_OK && e == cudaSuccess) e = cudaMemsetAsync(h->d_status, 0, sizeof(uint32_t), h->stream);
+  if (rc == GZ_OK && e == cudaSuccess) e = cudaEventRecord(t.done, h->stream);
+  if (rc == GZ_OK && e != cudaSuccess) rc = fail(GZ_ERR_CUDA, cudaGetErrorString(e));
+  if (rc != GZ_OK) {
+    T.pool.push_back(t);
+    return rc;
   }
-  S.cv.notify_all();
+  *ticket = T.next++;
+  T.live[*ticket] = t;
   return GZ_OK;
 }
 
 int gz_query_wait(gz_alg_t *h, uint64_t ticket, uint32_t *parent_out, uint32_t *num_cc, size_t *rounds) {
   if (!h) return fail(GZ_ERR_INVALID, "null handle");
-  auto &S = h->snap;
-  gz_alg::SnapResult r;
+  gz_alg::Ticket t;
   {
-    std::unique_lock<std::mutex> lk(S.m);
-    const bool pending = S.job == ticket && (S.queued || S.running);
-    if (!pending && !S.results.count(ticket)) return fail(GZ_ERR_INVALID, "unknown or already collected ticket");
-    S.cv.wait(lk, [&] { return S.results.count(ticket) > 0; });
-    r = std::move(S.results[ticket]);
-    S.results.erase(ticket);
+    std::lock_guard<std::mutex> lk(h->mtx);
+    auto it = h->tq.live.find(ticket);
+    if (it == h->tq.live.end()) return fail(GZ_ERR_INVALID, "unknown or already collected ticket");
+    t = it->second;
+    h->tq.live.erase(it);
   }
-  if (rounds) *rounds = r.rounds;
-  if (r.rc != GZ_OK) return fail(r.rc, r.err);
-  if (num_cc) *num_cc = r.ncc;
-  if (parent_out) std::copy(r.labels.begin(), r.labels.end(), parent_out);
-  return GZ_OK;
+  cudaSetDevice(h->device);
+  const cudaError_t e = cudaEventSynchronize(t.done);  // no handle lock held: ingest goes on
+  std::lock_guard<std::mutex> lk(h->mtx);
+  if (e != cudaSuccess) {
+    h->tq.pool.push_back(t);
+    return fail(GZ_ERR_CUDA, cudaGetErrorString(e));
+  }
+  boruvka_account(h->tq.graph, t.pin);
+  const uint32_t round = t.pin[0], oos = t.pin[1], ncc = t.pin[2], st = t.pin[3];
+  // bits of updates submitted before the query are reported by the next flush, as usual
+  h->deferred_status |= st & (gz::kStatusBadVertex | gz::kStatusTimeout);
+  if (rounds) *rounds = round;
+  int rc = GZ_OK;
+  if (oos) {
+    rc = fail(GZ_ERR_OUT_OF_SAMPLES, out_of_samples_msg(h, round));
+  } else if (st & gz::kStatusBadSample) {
+    rc = fail(GZ_ERR_BAD_SAMPLE, "a sampled edge decoded to a vertex id >= V");
+  } else {
+    h->prof_acc.query_rounds += round + 1;
+    if (num_cc) *num_cc = ncc;
+    if (parent_out) std::copy(t.labels, t.labels + h->V, parent_out);
+  }
+  h->tq.pool.push_back(t);
+  return rc;
 }
 
 int gz_has_cached_query(const gz_alg_t *h, int code, int *out) {

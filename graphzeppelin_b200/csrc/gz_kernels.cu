@@ -17,6 +17,9 @@
 #include <algorithm>
 #include <atomic>
 #include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <vector>
 
 #include "gz_common.cuh"
 #include "gz_device.cuh"
@@ -774,6 +777,17 @@ __global__ void __launch_bounds__(256) k_bv_label(uint32_t V, uint32_t *parent, 
   }
 }
 
+// Per-round counters: members and scatter cursors per root, smallest member (traces), and no
+// component marked as merged from its complement yet.
+__global__ void k_bv_prep(uint32_t V, BoruvkaBufs b) {
+  const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= V) return;
+  b.cnt[v] = 0;
+  b.fill[v] = 0;
+  if (b.trace) b.minv[v] = 0xffffffffu;
+  if (v == 0) *b.big = 0xffffffffu;
+}
+
 __global__ void k_bv_pack(uint32_t V, const uint32_t *cnt, uint64_t *packed) {
   const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= V) return;
@@ -826,8 +840,9 @@ __global__ void __launch_bounds__(256) k_bv_group(uint32_t V, uint32_t acc_words
 // crossing a span edge go to acc (per component: CPS*B column buckets, then the deterministic
 // one) with one coalesced atomicXor per word.
 template <int CPS, int NW, int KB>
-__global__ void __launch_bounds__(256) k_bv_merge(BoruvkaGeom g, uint32_t round,
-                                                  const uint32_t *__restrict__ sk_words, BoruvkaBufs b) {
+__global__ void __launch_bounds__(256) k_bv_merge(BoruvkaGeom g, const uint32_t *__restrict__ sk_words,
+                                                  BoruvkaBufs b) {
+  const uint32_t round = *b.round;
   extern __shared__ uint32_t bv_smem[];
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t W = 3 * CPS * g.B, SW = W + 3;
@@ -848,6 +863,12 @@ __global__ void __launch_bounds__(256) k_bv_merge(BoruvkaGeom g, uint32_t round,
   }
   const uint32_t my_v = lane < n ? b.order[p0 + lane] : 0u;
   const uint32_t my_c = lane < n ? b.order_comp[p0 + lane] : 0u;
+  // the components of the positions just before and after the span: a component that also
+  // holds one of them crosses a span edge (members of a component are contiguous)
+  uint32_t edge_c = 0xffffffffu;
+  if (lane == 0 && p0 > 0) edge_c = b.order_comp[p0 - 1];
+  if (lane == 1 && p1 < g.V) edge_c = b.order_comp[p1];
+  const uint32_t prev_c = __shfl_sync(kFull, edge_c, 0), next_c = __shfl_sync(kFull, edge_c, 1);
   auto issue = [&](uint32_t t) {
     uint32_t *half = ring + (t & 1) * KB * SW;
 #pragma unroll
@@ -877,8 +898,8 @@ __global__ void __launch_bounds__(256) k_bv_merge(BoruvkaGeom g, uint32_t round,
     nres = 0;
   };
   auto flush = [&](uint32_t comp) {
-    const uint32_t s = b.comp_start[comp], e = b.comp_start[comp + 1];
-    if (s >= p0 && e <= p1) {
+    const bool before = comp == prev_c, after = comp == next_c;
+    if (!before && !after) {
 #pragma unroll
       for (int k = 0; k < NW; ++k) {
         const uint32_t wi = k * 32 + lane;
@@ -895,7 +916,7 @@ __global__ void __launch_bounds__(256) k_bv_merge(BoruvkaGeom g, uint32_t round,
         my_key = b.comp_key[comp];
       }
       if (++nres == 32) apply();
-    } else if (s <= p0 && e >= p1) {
+    } else if (before && after) {
       uint32_t *pt = b.part + (uint64_t)w * SW;
 #pragma unroll
       for (int k = 0; k < NW; ++k) {
@@ -922,7 +943,9 @@ __global__ void __launch_bounds__(256) k_bv_merge(BoruvkaGeom g, uint32_t round,
     cp_async_wait<1>();
     __syncwarp();
     const uint32_t *half = ring + (t & 1) * KB * SW;
-#pragma unroll
+    // not unrolled: one copy of the flush (and the sampling it inlines) keeps the kernel small
+    // enough for the instruction cache
+#pragma unroll 1
     for (int k = 0; k < KB; ++k) {
       const uint32_t m = t * KB + k;
       const uint32_t c = __shfl_sync(kFull, my_c, m < n ? m : 0);
@@ -1024,7 +1047,8 @@ __global__ void __launch_bounds__(256) k_bv_reduce_parts(BoruvkaGeom g, uint32_t
 }
 
 template <int CPS>
-__global__ void k_bv_sample_spanning(BoruvkaGeom g, uint32_t round, BoruvkaBufs b) {
+__global__ void k_bv_sample_spanning(BoruvkaGeom g, BoruvkaBufs b) {
+  const uint32_t round = *b.round;
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   const uint32_t nc = *b.ncomp;
@@ -1053,6 +1077,26 @@ __global__ void k_bv_sample_spanning(BoruvkaGeom g, uint32_t round, BoruvkaBufs 
     uint64_t idx;
     const int res = warp_sample_cols<CPS>(d, a, g.B, g.flip_chk, &idx);
     if (lane == 0) handle_result(res, idx, round, b.comp_key[comp], g, b);
+  }
+}
+
+// End of a round (the loop test of boruvka_emulation, src/cc_sketch_alg.cpp:490-509): stop when
+// nothing FAILed or merged, or when the next round would ask Sketch::sample for sample
+// `samples` (OutOfSamplesException); otherwise start the next round.
+__global__ void k_bv_check(BoruvkaBufs b, uint32_t samples, cudaGraphConditionalHandle cond) {
+  const uint32_t r = *b.round;
+  if (*b.flags == 0) {
+    b.ctl[0] = r;
+    b.ctl[1] = 0;
+    cudaGraphSetConditional(cond, 0);
+  } else if (r + 1 >= samples) {
+    b.ctl[0] = r + 1;
+    b.ctl[1] = 1;
+    cudaGraphSetConditional(cond, 0);
+  } else {
+    *b.round = r + 1;
+    *b.flags = 0;
+    cudaGraphSetConditional(cond, 1);
   }
 }
 
@@ -1118,6 +1162,7 @@ __global__ void k_hash_peak(uint64_t seed, uint32_t iters, uint64_t *out) {
 // host wrappers
 // ================================================================================================
 uint64_t launch_count() { return g_launches.load(); }
+void add_launches(uint64_t n) { g_launches += n; }
 
 cudaError_t update_peak(uint32_t nb, uint32_t iters, int blocks, uint32_t *out, cudaStream_t s) {
   const size_t smem = (size_t)nb * 12;
@@ -1410,13 +1455,12 @@ cudaError_t boruvka_round0(const BoruvkaGeom &g, const uint8_t *sketches, const 
   return cudaGetLastError();
 }
 
-cudaError_t boruvka_round(const BoruvkaGeom &g, uint32_t round, const uint8_t *sketches,
-                          const BoruvkaBufs &b, bool trace, cudaStream_t s) {
+cudaError_t boruvka_round(const BoruvkaGeom &g, const uint8_t *sketches, const BoruvkaBufs &b,
+                          cudaStream_t s) {
+  const bool trace = b.trace != nullptr;
   const uint32_t V = g.V;
-  cudaMemsetAsync(b.cnt, 0, sizeof(uint32_t) * V, s);
-  cudaMemsetAsync(b.fill, 0, sizeof(uint32_t) * V, s);
-  cudaMemsetAsync(b.big, 0xff, sizeof(uint32_t), s);
-  if (trace) cudaMemsetAsync(b.minv, 0xff, sizeof(uint32_t) * V, s);
+  k_bv_prep<<<blocks_for(V, 256), 256, 0, s>>>(V, b);
+  g_launches++;
   k_bv_label<<<blocks_for(V, 256), 256, 0, s>>>(V, b.parent, b.label, b.cnt,
                                                  trace ? b.minv : nullptr);
   g_launches++;
@@ -1437,20 +1481,20 @@ cudaError_t boruvka_round(const BoruvkaGeom &g, uint32_t round, const uint8_t *s
   const size_t smem = bv_smem_bytes(g);
   if (g.cps == 1 && g.B <= 42) {
     if ((e = bv_smem_attr(k_bv_merge<1, 4, 8>, smem)) != cudaSuccess) return e;
-    k_bv_merge<1, 4, 8><<<mblocks, 256, smem, s>>>(g, round, sk, b);
+    k_bv_merge<1, 4, 8><<<mblocks, 256, smem, s>>>(g, sk, b);
     k_bv_reduce_parts<1, 4, 8><<<rblocks, 256, 0, s>>>(g, (uint32_t)warps, b);
   } else if (g.cps == 1) {
     if ((e = bv_smem_attr(k_bv_merge<1, 6, 8>, smem)) != cudaSuccess) return e;
-    k_bv_merge<1, 6, 8><<<mblocks, 256, smem, s>>>(g, round, sk, b);
+    k_bv_merge<1, 6, 8><<<mblocks, 256, smem, s>>>(g, sk, b);
     k_bv_reduce_parts<1, 6, 4><<<rblocks, 256, 0, s>>>(g, (uint32_t)warps, b);
   } else {
     if ((e = bv_smem_attr(k_bv_merge<7, dev::Region<7>::kNW, 1>, smem)) != cudaSuccess) return e;
-    k_bv_merge<7, dev::Region<7>::kNW, 1><<<mblocks, 256, smem, s>>>(g, round, sk, b);
+    k_bv_merge<7, dev::Region<7>::kNW, 1><<<mblocks, 256, smem, s>>>(g, sk, b);
     k_bv_reduce_parts<7, dev::Region<7>::kNW, 1><<<rblocks, 256, 0, s>>>(g, (uint32_t)warps, b);
   }
   g_launches += 2;
-  if (g.cps == 1) k_bv_sample_spanning<1><<<sblocks, 256, 0, s>>>(g, round, b);
-  else k_bv_sample_spanning<7><<<sblocks, 256, 0, s>>>(g, round, b);
+  if (g.cps == 1) k_bv_sample_spanning<1><<<sblocks, 256, 0, s>>>(g, b);
+  else k_bv_sample_spanning<7><<<sblocks, 256, 0, s>>>(g, b);
   g_launches++;
   return cudaGetLastError();
 }
@@ -1461,6 +1505,120 @@ cudaError_t boruvka_final(const BoruvkaGeom &g, const BoruvkaBufs &b, uint32_t *
   k_bv_final<<<blocks_for(g.V, 256), 256, 0, s>>>(g.V, b.parent, labels_out, ncc);
   g_launches++;
   return cudaGetLastError();
+}
+
+namespace {
+cudaError_t build_graph(BoruvkaGraph &q, const BoruvkaGeom &g, uint32_t samples,
+                        const uint8_t *sketches, const BoruvkaBufs &b, uint32_t *labels_out,
+                        uint32_t *ncc) {
+  cudaStream_t cs = nullptr, bs = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaGraphCreate(&graph, 0);
+  cudaGraphConditionalHandle cond{};
+  if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&cond, graph, 0, cudaGraphCondAssignDefault);
+  bool capturing = false;
+  if (e == cudaSuccess) {
+    e = cudaStreamBeginCaptureToGraph(cs, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    capturing = e == cudaSuccess;
+  }
+  // kernels are counted as they are captured (the launch counter is this file's)
+  const uint64_t l0 = g_launches.load();
+  uint64_t l_body0 = 0, l_body1 = 0;
+  if (capturing) {
+    // round 0
+    e = boruvka_reset(g, b, cs);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b.flags, 0, sizeof(uint32_t), cs);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b.round, 0, sizeof(uint32_t), cs);
+    if (e == cudaSuccess) e = boruvka_round0(g, sketches, b, cs);
+    if (e == cudaSuccess) {
+      k_bv_check<<<1, 1, 0, cs>>>(b, samples, cond);
+      e = cudaGetLastError();
+    }
+    // while (cond) { one round; check }
+    cudaStreamCaptureStatus st;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    if (e == cudaSuccess) e = cudaStreamGetCaptureInfo(cs, &st, nullptr, nullptr, &deps, &ndeps);
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t wnode = nullptr;
+    if (e == cudaSuccess) e = cudaGraphAddNode(&wnode, graph, deps, ndeps, &cp);
+    if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(cs, &wnode, 1, cudaStreamSetCaptureDependencies);
+    if (e == cudaSuccess) {
+      cudaGraph_t body = cp.conditional.phGraph_out[0];
+      e = cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+      if (e == cudaSuccess) {
+        l_body0 = g_launches.load();
+        cudaError_t eb = boruvka_round(g, sketches, b, bs);
+        if (eb == cudaSuccess) {
+          k_bv_check<<<1, 1, 0, bs>>>(b, samples, cond);
+          eb = cudaGetLastError();
+        }
+        l_body1 = g_launches.load() + 1;  // + the check kernel
+        e = cudaStreamEndCapture(bs, &body);
+        if (e == cudaSuccess) e = eb;
+      }
+    }
+    if (e == cudaSuccess) e = boruvka_final(g, b, labels_out, ncc, cs);
+    cudaGraph_t out = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(cs, &out);
+    if (e == cudaSuccess) e = ec;
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&q.exec, graph, 0);
+  const cudaError_t d1 = bs ? cudaStreamDestroy(bs) : cudaSuccess;
+  const cudaError_t d2 = cs ? cudaStreamDestroy(cs) : cudaSuccess;
+  if (e == cudaSuccess) e = d1 != cudaSuccess ? d1 : d2;
+  if (e == cudaSuccess) {
+    // a call whose status was not returned to us must not surface in a later launch's check
+    const cudaError_t stale = cudaGetLastError();
+    if (stale != cudaSuccess)
+      std::fprintf(stderr, "gz: Boruvka query graph built; a runtime call reported %s\n",
+                   cudaGetErrorString(stale));
+  }
+  if (e != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    q.exec = nullptr;
+    return e;
+  }
+  q.graph = graph;
+  const uint64_t captured = g_launches.load() - l0 + 2;  // + the two check kernels
+  q.round_kernels = (uint32_t)(l_body1 - l_body0);
+  q.fixed_kernels = (uint32_t)(captured - q.round_kernels);
+  g_launches -= captured - 2;  // captured, not launched
+  q.g = g;
+  q.b = b;
+  q.sketches = sketches;
+  q.labels = labels_out;
+  q.ncc = ncc;
+  q.samples = samples;
+  return cudaSuccess;
+}
+}  // namespace
+
+void boruvka_graph_free(BoruvkaGraph &q) {
+  if (q.exec) cudaGraphExecDestroy(q.exec);
+  if (q.graph) cudaGraphDestroy(q.graph);
+  q.exec = nullptr;
+  q.graph = nullptr;
+}
+
+cudaError_t boruvka_graph_launch(BoruvkaGraph &q, const BoruvkaGeom &g, uint32_t samples,
+                                 const uint8_t *sketches, const BoruvkaBufs &b, uint32_t *labels_out,
+                                 uint32_t *ncc, cudaStream_t s) {
+  const bool same = q.exec && std::memcmp(&q.g, &g, sizeof(g)) == 0 &&
+                    std::memcmp(&q.b, &b, sizeof(b)) == 0 && q.sketches == sketches &&
+                    q.labels == labels_out && q.ncc == ncc && q.samples == samples;
+  if (!same) {
+    boruvka_graph_free(q);
+    cudaError_t e = build_graph(q, g, samples, sketches, b, labels_out, ncc);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaGraphLaunch(q.exec, s);
 }
 
 }  // namespace gz

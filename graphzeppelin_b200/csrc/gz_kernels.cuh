@@ -150,6 +150,8 @@ struct BoruvkaBufs {
   uint32_t *part;        // per merge warp: its members' XOR when one component covers its span
   uint32_t *part_comp;   // per merge warp: that component, or ~0
   uint32_t *big;         // 1   the component holding more than half the vertices, or ~0
+  uint32_t *round;       // 1   the current round (device-driven loop)
+  uint32_t *ctl;         // 2   after the loop: rounds run, out of samples (0/1)
   uint32_t *flags;       // [0] modified
   uint64_t *forest;      // V   spanning-forest edge indices
   uint32_t *forest_n;    // 1
@@ -181,11 +183,32 @@ cudaError_t sketch_total_xor(const uint8_t *sketches, uint32_t V, uint32_t sketc
 cudaError_t boruvka_reset(const BoruvkaGeom &g, const BoruvkaBufs &b, cudaStream_t s);
 cudaError_t boruvka_round0(const BoruvkaGeom &g, const uint8_t *sketches, const BoruvkaBufs &b,
                            cudaStream_t s);
-cudaError_t boruvka_round(const BoruvkaGeom &g, uint32_t round, const uint8_t *sketches,
-                          const BoruvkaBufs &b, bool trace, cudaStream_t s);
+// one round >= 1; the round number is read from b.round
+cudaError_t boruvka_round(const BoruvkaGeom &g, const uint8_t *sketches, const BoruvkaBufs &b,
+                          cudaStream_t s);
 // parent_out[v] = root of v; *ncc = number of roots (device pointers)
 cudaError_t boruvka_final(const BoruvkaGeom &g, const BoruvkaBufs &b, uint32_t *labels_out,
                           uint32_t *ncc, cudaStream_t s);
+
+// boruvka_emulation (src/cc_sketch_alg.cpp:464-513) as one CUDA graph: round 0, then a
+// conditional while node whose body is one round plus a check kernel that ends the loop when a
+// round neither FAILs nor merges, or when the next round would exceed `samples` (b.ctl then
+// holds the rounds and the out-of-samples flag), then the labels (labels_out, *ncc). No host
+// round trip between rounds.
+struct BoruvkaGraph {
+  cudaGraphExec_t exec = nullptr;
+  cudaGraph_t graph = nullptr;
+  uint32_t fixed_kernels = 0, round_kernels = 0;  // kernel nodes outside / inside the loop body
+  // what the graph was built for
+  BoruvkaGeom g{};
+  BoruvkaBufs b{};
+  const uint8_t *sketches = nullptr;
+  uint32_t *labels = nullptr, *ncc = nullptr, samples = 0;
+};
+cudaError_t boruvka_graph_launch(BoruvkaGraph &q, const BoruvkaGeom &g, uint32_t samples,
+                                 const uint8_t *sketches, const BoruvkaBufs &b, uint32_t *labels_out,
+                                 uint32_t *ncc, cudaStream_t s);
+void boruvka_graph_free(BoruvkaGraph &q);
 
 int num_sms();
 // columns C and buckets per column B of one vertex sketch for V vertices and sketches factor f
@@ -203,5 +226,7 @@ cudaError_t update_peak(uint32_t nb, uint32_t iters, int blocks, uint32_t *out, 
 
 // Kernel launches issued by the host wrappers of this file (monotonic, process-wide).
 uint64_t launch_count();
+// kernels launched by a CUDA graph (counted by its owner once the graph has run)
+void add_launches(uint64_t n);
 
 }  // namespace gz

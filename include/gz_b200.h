@@ -193,14 +193,15 @@ GZ_API int gz_flush(gz_alg_t *alg);
 /* CCSketchAlg::has_cached_query -- include/cc_sketch_alg.h:184-190. */
 GZ_API int gz_has_cached_query(const gz_alg_t *alg, int query_code, int *out);
 
-/* Connectivity query on a snapshot: gz_query_submit applies every update so far, copies the
- * sketches on a second stream (V x sketch_bytes more device memory, allocated on the first call)
- * and queues boruvka_emulation (src/cc_sketch_alg.cpp:464-513) of the copy on a worker thread;
- * it returns at once, and updates made after it proceed while the query runs (queries
- * interleaved with ingest). gz_query_wait returns the answer for the state at submission:
- * parent_out (NULL or V entries), the component count and the rounds, or GZ_ERR_OUT_OF_SAMPLES.
- * One snapshot is queried at a time: a submit waits for the previous query to finish. Snapshot
- * queries leave the handle's cached answer and update lock alone. */
+/* Connectivity query on the state at submission: gz_query_submit queues every update so far
+ * and then boruvka_emulation (src/cc_sketch_alg.cpp:464-513, every round on the device, with
+ * its own query buffers) on the handle's stream, and returns at once; updates made after it are
+ * queued behind the query, so the caller never waits for it and the answer is the state at
+ * submission without a copy of the sketches (queries interleaved with ingest). Several tickets
+ * may be in flight. gz_query_wait blocks until its query is done and returns parent_out (NULL or
+ * V entries), the component count and the rounds, or GZ_ERR_OUT_OF_SAMPLES / GZ_ERR_BAD_SAMPLE.
+ * Device errors of earlier updates are reported by the next flush. Ticket queries leave the
+ * handle's cached answer and update lock alone. */
 GZ_API int gz_query_submit(gz_alg_t *alg, uint64_t *ticket);
 GZ_API int gz_query_wait(gz_alg_t *alg, uint64_t ticket, uint32_t *parent_out, uint32_t *num_cc,
                          size_t *rounds);

@@ -49,3 +49,26 @@ def test_snapshot_query_out_of_samples(gz, oracle_mod, tmp_path):
         alg.query_wait(t)
     alg.update(gz.GraphUpdate((0, 1)))  # a failed snapshot query does not lock updates
     alg.close()
+
+
+def test_several_queries_in_flight(gz):
+    """Tickets need not be collected in order: three queries are queued between ingest calls,
+    then collected last to first; each answer is its own prefix's."""
+    from graphzeppelin_b200 import streams as S
+    V = 2000
+    st = S.chung_lu_stream_fast(V, 2.3, 10, 200, seed=9)
+    recs = st.records
+    cuts = np.linspace(0, len(recs), 4).astype(int)
+    alg = gz.CCSketchAlg(V, 5)
+    tickets = []
+    for k in range(3):
+        alg.ingest_records(recs[cuts[k]:cuts[k + 1]])
+        tickets.append(alg.query_submit())
+    for k in reversed(range(3)):
+        cc, rounds = alg.query_wait(tickets[k])
+        ref = gz.CCSketchAlg(V, 5)
+        ref.ingest_records(recs[:cuts[k + 1]])
+        rcc = ref.connected_components()
+        assert (cc.parent_arr == rcc.parent_arr).all() and rounds == ref.last_query_rounds
+        ref.close()
+    alg.close()
