@@ -241,6 +241,8 @@ def run_b200(args, cfg):
 
     V = cfg["num_vertices"]
     alg = gz.CCSketchAlg(V, cfg["sketch_seed"])
+    if args.host_rounds:
+        alg.set_query_graph(False)
     alg.set_gutter_capacity(2 * n + 1024)
     lib_stream = torch.cuda.ExternalStream(alg.stream_handle())
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
@@ -641,6 +643,11 @@ POWERLAW = dict(workload="powerlaw_v1048576_chunglu2.1_deg200_max16384_q10", num
                 sketch_seed=0x9E37)
 
 
+# profiling case of the same kind: V = 2^18 (2.8 GB of sketches, 3.2e7 records)
+POWERLAW_SMALL = dict(POWERLAW, workload="powerlaw_v262144_chunglu2.1_deg200_max16384_q10",
+                      num_vertices=1 << 18)
+
+
 def run_powerlaw(args):
     """Power-law graph with interleaved queries: a Chung-Lu stream (V = 2^20, exponent 2.1, mean
     degree 200 after a 2^14 degree cap; shuffled inserts, deletes of 15% of them, re-inserts of
@@ -655,7 +662,7 @@ def run_powerlaw(args):
     from graphzeppelin_b200 import streams as S
 
     torch.cuda.set_device(0)
-    cfg = POWERLAW
+    cfg = POWERLAW_SMALL if args.small else POWERLAW
     V, Q = cfg["num_vertices"], cfg["queries"]
     t = time.time()
     probe = S.chung_lu_stream_fast(V, cfg["exponent"], cfg["mean_degree"], cfg["max_degree"],
@@ -670,6 +677,8 @@ def run_powerlaw(args):
     log(f"[powerlaw] {n} records ({n * 9 / 1e9:.2f} GB) in {time.time() - t:.1f} s")
     cuts = np.linspace(0, n, Q + 1).astype(np.int64)
     alg = gz.CCSketchAlg(V, cfg["sketch_seed"])
+    if args.host_rounds:
+        alg.set_query_graph(False)
     alg.set_gutter_capacity(2 * int(cuts[1] - cuts[0]) + 1024)
     base = d_rec.data_ptr()
 
@@ -736,7 +745,7 @@ def run_powerlaw(args):
         "config": {"workload": cfg["workload"], "num_vertices": V, "num_updates": n, "queries": Q,
                    "num_columns": p.num_columns, "bkt_per_col": p.bkt_per_col,
                    "sketch_bytes_total": V * p.sketch_bytes,
-                   "l2": "inputs larger than L2 (1.2 GB of records, 14 GB of sketches)"},
+                   "l2": "inputs larger than L2 (GB of records and sketches)"},
         "timing": "wall clock between device synchronisations, whole stream with its queries",
         "snapshot_queries": {"ms_per_step": ms, "updates_per_s": n / (ms / 1e3),
                              "ingest_ms_per_step": (prof["gutter_ms"] + prof["sketch_update_ms"]) / args.steps},
@@ -761,8 +770,12 @@ def main():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--small", action="store_true", help="V=2^14 case (profiling)")
+    ap.add_argument("--small", action="store_true",
+                    help="profiling sizes: dense V=2^14, powerlaw V=2^18")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--host-rounds", action="store_true",
+                    help="queries with the Boruvka round loop on the host (profilers cannot see "
+                         "kernels inside the conditional query graph)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", default="dense",
                     choices=["dense", "many_graphs", "serving", "powerlaw"],

@@ -487,6 +487,11 @@ class CCSketchAlg:
         0 always stages."""
         _check(self.lib.gz_set_direct_factor(self._h, float(factor)))
 
+    def set_query_graph(self, enable: bool = True) -> None:
+        """Queries as one CUDA graph (default) or with the round loop on the host
+        (gz_set_query_graph; for profilers)."""
+        _check(self.lib.gz_set_query_graph(self._h, int(enable)))
+
     def set_gutter_capacity(self, endpoint_updates: int) -> None:
         _check(self.lib.gz_set_gutter_capacity(self._h, endpoint_updates))
 

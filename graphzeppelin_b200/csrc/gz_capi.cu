@@ -178,8 +178,10 @@ struct gz_alg {
   bool eager = false, host_answer = false, boruvka_ran = false;
   std::vector<uint32_t> hdsu;
   std::unordered_set<uint64_t> hforest;
-  // the query graph of blocking queries (device-driven Boruvka rounds)
+  // the query graph of blocking queries (device-driven Boruvka rounds); query_graph = 0 runs
+  // the same kernels with the round loop on the host
   gz::BoruvkaGraph qgraph;
+  bool query_graph = true;
   uint32_t *h_qpin = nullptr;  // pinned: rounds, out-of-samples flag, components
   // queries by ticket (gz_query_submit / gz_query_wait): the query graph enqueued on the
   // handle's stream behind every update submitted before it, with its own buffers, so the
@@ -188,6 +190,7 @@ struct gz_alg {
     cudaEvent_t done = nullptr;
     uint32_t *labels = nullptr;  // pinned, V entries
     uint32_t *pin = nullptr;     // pinned: rounds, out-of-samples flag, components, status
+    bool graph = true;           // ran as the query graph (its kernels are counted at the end)
   };
   struct Tickets {
     gz::BoruvkaBufs bv{};
@@ -774,14 +777,16 @@ void free_bv(gz::BoruvkaBufs &b) {
 int boruvka_enqueue(gz_alg *h, gz::BoruvkaGraph &q, const gz::BoruvkaGeom &g, const uint8_t *sk,
                     gz::BoruvkaBufs &b, uint32_t *d_final, uint32_t *d_ncc, uint32_t *pin,
                     cudaStream_t s) {
-  GZ_CUDA(gz::boruvka_graph_launch(q, g, h->samples, sk, b, d_final, d_ncc, s));
+  if (h->query_graph) GZ_CUDA(gz::boruvka_graph_launch(q, g, h->samples, sk, b, d_final, d_ncc, s));
+  else GZ_CUDA(gz::boruvka_host_loop(g, h->samples, sk, b, d_final, d_ncc, pin, s));
   GZ_CUDA(cudaMemcpyAsync(pin, b.ctl, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   GZ_CUDA(cudaMemcpyAsync(pin + 2, d_ncc, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   return GZ_OK;
 }
 
 // Kernel launches of a finished query graph (its loop body ran once per round >= 1).
-void boruvka_account(const gz::BoruvkaGraph &q, const uint32_t *pin) {
+void boruvka_account(const gz::BoruvkaGraph &q, const uint32_t *pin, bool graph) {
+  if (!graph) return;  // the host loop counted its launches as it went
   const uint32_t body_runs = pin[1] ? pin[0] - 1 : pin[0];
   gz::add_launches(q.fixed_kernels + (uint64_t)body_runs * q.round_kernels);
 }
@@ -853,7 +858,7 @@ int run_boruvka(gz_alg *h) {
                          h->stream));
   h->prof_end(pi, 2);
   GZ_CUDA(cudaStreamSynchronize(h->stream));
-  boruvka_account(h->qgraph, h->h_qpin);
+  boruvka_account(h->qgraph, h->h_qpin, h->query_graph);
   const uint32_t round = h->h_qpin[0];
   if (h->h_qpin[1]) {
     h->last_rounds = round;
@@ -1242,6 +1247,7 @@ int gz_query_submit(gz_alg_t *h, uint64_t *ticket) {
     }
   }
   const int pi = h->prof_begin();
+  t.graph = h->query_graph;
   int rc = boruvka_enqueue(h, T.graph, h->bgeom(), h->d_sk, T.bv, T.d_final, T.d_ncc, t.pin, h->stream);
   h->prof_end(pi, 2);
   cudaError_t e = cudaSuccess;
@@ -1278,7 +1284,7 @@ int gz_query_wait(gz_alg_t *h, uint64_t ticket, uint32_t *parent_out, uint32_t *
     h->tq.pool.push_back(t);
     return fail(GZ_ERR_CUDA, cudaGetErrorString(e));
   }
-  boruvka_account(h->tq.graph, t.pin);
+  boruvka_account(h->tq.graph, t.pin, t.graph);
   const uint32_t round = t.pin[0], oos = t.pin[1], ncc = t.pin[2], st = t.pin[3];
   // bits of updates submitted before the query are reported by the next flush, as usual
   h->deferred_status |= st & (gz::kStatusBadVertex | gz::kStatusTimeout);
@@ -1403,6 +1409,13 @@ int gz_get_trace(gz_alg_t *h, gz_trace_rec_t *out, size_t cap, size_t *len) {
   const size_t n = std::min<size_t>(h->h_status[3], h->bv.trace_cap);
   *len = n;
   if (out && cap) GZ_CUDA(cudaMemcpy(out, h->bv.trace, std::min(cap, n) * sizeof(gz_trace_rec_t), cudaMemcpyDeviceToHost));
+  return GZ_OK;
+}
+
+int gz_set_query_graph(gz_alg_t *h, int enable) {
+  if (!h) return fail(GZ_ERR_INVALID, "null handle");
+  Guard g(h);
+  h->query_graph = enable != 0;
   return GZ_OK;
 }
 

@@ -1083,21 +1083,25 @@ __global__ void k_bv_sample_spanning(BoruvkaGeom g, BoruvkaBufs b) {
 // End of a round (the loop test of boruvka_emulation, src/cc_sketch_alg.cpp:490-509): stop when
 // nothing FAILed or merged, or when the next round would ask Sketch::sample for sample
 // `samples` (OutOfSamplesException); otherwise start the next round.
-__global__ void k_bv_check(BoruvkaBufs b, uint32_t samples, cudaGraphConditionalHandle cond) {
+// In a query graph (in_graph) the verdict drives its while node; b.ctl[2] carries it for a loop
+// run from the host.
+__global__ void k_bv_check(BoruvkaBufs b, uint32_t samples, cudaGraphConditionalHandle cond,
+                           int in_graph) {
   const uint32_t r = *b.round;
+  uint32_t go = 0;
   if (*b.flags == 0) {
     b.ctl[0] = r;
     b.ctl[1] = 0;
-    cudaGraphSetConditional(cond, 0);
   } else if (r + 1 >= samples) {
     b.ctl[0] = r + 1;
     b.ctl[1] = 1;
-    cudaGraphSetConditional(cond, 0);
   } else {
     *b.round = r + 1;
     *b.flags = 0;
-    cudaGraphSetConditional(cond, 1);
+    go = 1;
   }
+  b.ctl[2] = go;
+  if (in_graph) cudaGraphSetConditional(cond, go);
 }
 
 __global__ void k_bv_final(uint32_t V, uint32_t *parent, uint32_t *out, uint32_t *ncc) {
@@ -1533,7 +1537,7 @@ cudaError_t build_graph(BoruvkaGraph &q, const BoruvkaGeom &g, uint32_t samples,
     if (e == cudaSuccess) e = cudaMemsetAsync(b.round, 0, sizeof(uint32_t), cs);
     if (e == cudaSuccess) e = boruvka_round0(g, sketches, b, cs);
     if (e == cudaSuccess) {
-      k_bv_check<<<1, 1, 0, cs>>>(b, samples, cond);
+      k_bv_check<<<1, 1, 0, cs>>>(b, samples, cond, 1);
       e = cudaGetLastError();
     }
     // while (cond) { one round; check }
@@ -1556,7 +1560,7 @@ cudaError_t build_graph(BoruvkaGraph &q, const BoruvkaGeom &g, uint32_t samples,
         l_body0 = g_launches.load();
         cudaError_t eb = boruvka_round(g, sketches, b, bs);
         if (eb == cudaSuccess) {
-          k_bv_check<<<1, 1, 0, bs>>>(b, samples, cond);
+          k_bv_check<<<1, 1, 0, bs>>>(b, samples, cond, 1);
           eb = cudaGetLastError();
         }
         l_body1 = g_launches.load() + 1;  // + the check kernel
@@ -1599,6 +1603,26 @@ cudaError_t build_graph(BoruvkaGraph &q, const BoruvkaGeom &g, uint32_t samples,
   return cudaSuccess;
 }
 }  // namespace
+
+cudaError_t boruvka_host_loop(const BoruvkaGeom &g, uint32_t samples, const uint8_t *sketches,
+                              const BoruvkaBufs &b, uint32_t *labels_out, uint32_t *ncc,
+                              uint32_t *pin, cudaStream_t s) {
+  cudaError_t e = boruvka_reset(g, b, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(b.flags, 0, sizeof(uint32_t), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(b.round, 0, sizeof(uint32_t), s);
+  if (e == cudaSuccess) e = boruvka_round0(g, sketches, b, s);
+  for (bool first = true; e == cudaSuccess; first = false) {
+    if (!first) e = boruvka_round(g, sketches, b, s);
+    if (e != cudaSuccess) break;
+    k_bv_check<<<1, 1, 0, s>>>(b, samples, cudaGraphConditionalHandle{}, 0);
+    g_launches++;
+    e = cudaMemcpyAsync(pin, b.ctl, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess || !pin[2]) break;
+  }
+  if (e == cudaSuccess) e = boruvka_final(g, b, labels_out, ncc, s);
+  return e;
+}
 
 void boruvka_graph_free(BoruvkaGraph &q) {
   if (q.exec) cudaGraphExecDestroy(q.exec);

@@ -151,7 +151,7 @@ struct BoruvkaBufs {
   uint32_t *part_comp;   // per merge warp: that component, or ~0
   uint32_t *big;         // 1   the component holding more than half the vertices, or ~0
   uint32_t *round;       // 1   the current round (device-driven loop)
-  uint32_t *ctl;         // 2   after the loop: rounds run, out of samples (0/1)
+  uint32_t *ctl;         // 3   after the loop: rounds run, out of samples (0/1); go on (0/1)
   uint32_t *flags;       // [0] modified
   uint64_t *forest;      // V   spanning-forest edge indices
   uint32_t *forest_n;    // 1
@@ -209,6 +209,12 @@ cudaError_t boruvka_graph_launch(BoruvkaGraph &q, const BoruvkaGeom &g, uint32_t
                                  const uint8_t *sketches, const BoruvkaBufs &b, uint32_t *labels_out,
                                  uint32_t *ncc, cudaStream_t s);
 void boruvka_graph_free(BoruvkaGraph &q);
+// The same kernels with the loop run from the host (a device-to-host copy and a synchronize per
+// round; for profilers that do not see kernels inside conditional graphs). Leaves b.ctl[0..1]
+// as the graph does; pin is pinned host memory of at least 3 words.
+cudaError_t boruvka_host_loop(const BoruvkaGeom &g, uint32_t samples, const uint8_t *sketches,
+                              const BoruvkaBufs &b, uint32_t *labels_out, uint32_t *ncc,
+                              uint32_t *pin, cudaStream_t s);
 
 int num_sms();
 // columns C and buckets per column B of one vertex sketch for V vertices and sketches factor f

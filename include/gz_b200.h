@@ -294,6 +294,11 @@ GZ_API int gz_set_tuning(gz_alg_t *alg, uint32_t vertices_per_tile, uint32_t thr
  * staging it in shared memory against updating its buckets in HBM -- is updated in place with
  * global atomics. 0 = always staged, 1 = the default. Same role as gz_batch_set_route. */
 GZ_API int gz_set_direct_factor(gz_alg_t *alg, double factor);
+/* Queries run as one CUDA graph whose conditional while node loops over the Boruvka rounds
+ * (enable = 1, the default). enable = 0 runs the same kernels with the round loop on the host
+ * (a synchronize per round; ticket submits then wait for their query): for profilers that do
+ * not see kernels inside conditional graphs. Answers are the same either way. */
+GZ_API int gz_set_query_graph(gz_alg_t *alg, int enable);
 
 /* ---- many graphs on one GPU ------------------------------------------------------------------
  * A gz_batch_t holds num_graphs independent CCSketchAlg instances (each its own V, seed and

@@ -226,6 +226,28 @@ def test_giant_component_merge_paths(gz, oracle_mod, path, tmp_path):
     assert cc.size() == n
 
 
+@pytest.mark.parametrize("name", ["c0_v1024", "mult_v1024", "cl_v2048"])
+def test_host_round_loop_equals_query_graph(gz, name):
+    """gz_set_query_graph(0) runs the Boruvka kernels with the round loop on the host: labels,
+    rounds and every round's samples equal the golden answer of the reference."""
+    c, st, labels, trace = load_case(name)
+    alg = _alg(gz, c["num_vertices"], c["seed"], c["sketches_factor"])
+    alg.set_query_graph(False)
+    alg.set_trace(True)
+    alg.ingest_records(st)
+    cc = alg.connected_components()
+    assert cc.size() == c["num_cc"]
+    assert (canonical(cc.parent_arr) == labels).all()
+    assert alg.last_query_rounds == c["rounds"]
+    tr = alg.get_trace()
+    assert tr.size == trace.size
+    for fld in ("round", "key", "result", "idx"):
+        assert (tr[fld] == trace[fld]).all(), fld
+    t = alg.query_submit()
+    cc2, rounds = alg.query_wait(t)
+    assert (cc2.parent_arr == cc.parent_arr).all() and rounds == c["rounds"]
+
+
 @pytest.mark.parametrize("V", [2, 3, 5, 17, 100, 301])
 def test_odd_vertex_counts(gz, oracle_mod, V):
     from graphzeppelin_b200 import streams as S
