@@ -632,6 +632,7 @@ def run_serving(args):
                               "paced": arms["plain"]["paced"].summary()} if "plain" in arms else None),
         "answers_equal": equal,
         "query_p50_ms": paced["query_p50_ms"], "query_p99_ms": paced["query_p99_ms"],
+        "service_p50_ms": paced["service_p50_ms"], "service_p99_ms": paced["service_p99_ms"],
         "admitted_tenants": paced["admitted_tenants"],
         "clocks": clocks,
     }

@@ -1010,13 +1010,21 @@ uint64_t graph_sketch_bytes(const GraphDesc &gd) {
   return (v_pad * gd.sketch_words * 4 + 255) & ~255ull;
 }
 
+// Scratch grows by at least half its size each time it is outgrown: a server whose calls vary in
+// size reallocates (a device-wide synchronisation, and a latency spike for every request in
+// flight) a few times while warming up instead of on every larger call.
+inline uint64_t headroom(uint64_t cap, uint64_t need) {
+  return need <= cap ? cap : std::max<uint64_t>(need, cap + cap / 2);
+}
+
 template <class T>
 int grow(T **p, uint64_t &cap, uint64_t need) {
   if (*p && cap >= need) return GZ_OK;
+  const uint64_t n = headroom(cap, need);
   mb_free(*p);
   cap = 0;
-  MB_TRY(mb_alloc(p, std::max<uint64_t>(need, 1)));
-  cap = need;
+  MB_TRY(mb_alloc(p, std::max<uint64_t>(n, 1)));
+  cap = n;
   return GZ_OK;
 }
 
@@ -1048,16 +1056,17 @@ int finalize_graphs(gz_batch *h) {
   MB_TRY(grow(&h->d_tile_graph, h->cap_tiles, h->total_tiles));
   MB_TRY(grow(&h->d_gov, h->cap_V, h->total_V));
   if (!h->d_bins || h->cap_bins < h->total_bins) {
+    const uint64_t nb = headroom(h->cap_bins, h->total_bins);
     mb_free(h->d_bins);
     mb_free(h->d_bin_fill);
     mb_free(h->d_scan_tmp);
     mb_free(h->d_bin_off);
     h->cap_bins = 0;
-    MB_TRY(mb_alloc(&h->d_bins, h->total_bins));
-    MB_TRY(mb_alloc(&h->d_bin_fill, h->total_bins));
-    MB_TRY(mb_alloc(&h->d_scan_tmp, scan_tmp_words(h->total_bins)));
-    MB_TRY(mb_alloc(&h->d_bin_off, h->total_bins + 1));
-    h->cap_bins = h->total_bins;
+    MB_TRY(mb_alloc(&h->d_bins, nb));
+    MB_TRY(mb_alloc(&h->d_bin_fill, nb));
+    MB_TRY(mb_alloc(&h->d_scan_tmp, scan_tmp_words(nb)));
+    MB_TRY(mb_alloc(&h->d_bin_off, nb + 1));
+    h->cap_bins = nb;
   }
   MB_CUDA(cudaMemcpyAsync(h->d_graphs, h->graphs.data(), sizeof(GraphDesc) * h->G, cudaMemcpyHostToDevice, h->stream));
   k_mb_fill_tables<<<std::min<uint32_t>(h->G, 4096), 256, 0, h->stream>>>(h->d_graphs, h->G, h->d_tile_graph, h->d_gov);
@@ -1222,6 +1231,7 @@ int batch_ingest(gz_batch *h, const void *d_rec, const uint64_t *off) {
 int ensure_boruvka(gz_batch *h) {
   const uint64_t V = h->total_V, G = h->G;
   if (!h->d_parent || h->cap_bv_V < V) {
+    const uint64_t Vn = headroom(h->cap_bv_V, V);
     mb_free(h->d_parent);
     mb_free(h->d_label);
     mb_free(h->d_cnt);
@@ -1232,27 +1242,28 @@ int ensure_boruvka(gz_batch *h) {
     mb_free(h->d_order_comp);
     mb_free(h->d_comp_start);
     h->cap_bv_V = 0;
-    MB_TRY(mb_alloc(&h->d_parent, V));
-    MB_TRY(mb_alloc(&h->d_label, V));
-    MB_TRY(mb_alloc(&h->d_cnt, V));
-    MB_TRY(mb_alloc(&h->d_fill, V));
-    MB_TRY(mb_alloc(&h->d_packed, V));
-    MB_TRY(mb_alloc(&h->d_vscan_tmp, scan_tmp_words(V)));
-    MB_TRY(mb_alloc(&h->d_order, V));
-    MB_TRY(mb_alloc(&h->d_order_comp, V));
-    MB_TRY(mb_alloc(&h->d_comp_start, V + 1));
-    h->cap_bv_V = V;
+    MB_TRY(mb_alloc(&h->d_parent, Vn));
+    MB_TRY(mb_alloc(&h->d_label, Vn));
+    MB_TRY(mb_alloc(&h->d_cnt, Vn));
+    MB_TRY(mb_alloc(&h->d_fill, Vn));
+    MB_TRY(mb_alloc(&h->d_packed, Vn));
+    MB_TRY(mb_alloc(&h->d_vscan_tmp, scan_tmp_words(Vn)));
+    MB_TRY(mb_alloc(&h->d_order, Vn));
+    MB_TRY(mb_alloc(&h->d_order_comp, Vn));
+    MB_TRY(mb_alloc(&h->d_comp_start, Vn + 1));
+    h->cap_bv_V = Vn;
   }
   MB_TRY(grow(&h->d_acc, h->cap_acc, V * (uint64_t)(h->max_B + 1) * 3));
   if (!h->d_active || h->cap_bv_G < G) {
+    const uint64_t Gn = headroom(h->cap_bv_G, G);
     mb_free(h->d_active);
     mb_free(h->d_modified);
     mb_free(h->d_ncc);
     h->cap_bv_G = 0;
-    MB_TRY(mb_alloc(&h->d_active, G));
-    MB_TRY(mb_alloc(&h->d_modified, G));
-    MB_TRY(mb_alloc(&h->d_ncc, G));
-    h->cap_bv_G = G;
+    MB_TRY(mb_alloc(&h->d_active, Gn));
+    MB_TRY(mb_alloc(&h->d_modified, Gn));
+    MB_TRY(mb_alloc(&h->d_ncc, Gn));
+    h->cap_bv_G = Gn;
   }
   MB_TRY(mb_alloc(&h->d_vscan_total, 1));
   MB_TRY(mb_alloc(&h->d_ncomp, 1));
@@ -1538,10 +1549,11 @@ int gz_batch_ingest(gz_batch_t *h, const void *records, const uint64_t *offsets)
   const uint64_t n = offsets[h->G];
   if (n == 0) return GZ_OK;
   if (h->rec_cap < n * 9) {
+    const uint64_t nr = headroom(h->rec_cap, n * 9);
     mb_free(h->d_rec);
     h->rec_cap = 0;
-    MB_TRY(mb_alloc(&h->d_rec, n * 9));
-    h->rec_cap = n * 9;
+    MB_TRY(mb_alloc(&h->d_rec, nr));
+    h->rec_cap = nr;
   }
   MB_CUDA(cudaMemcpyAsync(h->d_rec, records, n * 9, cudaMemcpyHostToDevice, h->stream));
   return batch_ingest(h, h->d_rec, offsets);

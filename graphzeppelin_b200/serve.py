@@ -293,6 +293,10 @@ class ServingResult:
     seconds: float = 0.0
     updates: int = 0
     latencies_ms: List[float] = field(default_factory=list)  # one per query, request order
+    # the same measured from when the query could first be served: its release, or its tenant's
+    # admission when the tenant was still waiting for budget
+    service_ms: List[float] = field(default_factory=list)
+    query_req: List[int] = field(default_factory=list)  # request index of each latency
     answers: Dict[int, tuple] = field(default_factory=dict)  # request index -> answer
     admitted: int = 0
     max_resident: int = 0
@@ -307,11 +311,14 @@ class ServingResult:
 
     def summary(self) -> dict:
         lat = np.asarray(self.latencies_ms) if self.latencies_ms else np.zeros(1)
+        svc = np.asarray(self.service_ms) if self.service_ms else np.zeros(1)
         return {"mode": self.mode, "seconds": self.seconds, "updates": self.updates,
                 "updates_per_s": self.updates / max(self.seconds, 1e-9),
                 "queries": len(self.latencies_ms),
                 "query_p50_ms": float(np.percentile(lat, 50)),
                 "query_p99_ms": float(np.percentile(lat, 99)),
+                "service_p50_ms": float(np.percentile(svc, 50)),
+                "service_p99_ms": float(np.percentile(svc, 99)),
                 "admitted_tenants": self.admitted, "max_resident_tenants": self.max_resident,
                 "max_used_bytes": self.max_used_bytes, "ticks": self.ticks,
                 "gpu_query_batches": self.gpu_queries, "rejected_tenants": self.rejected,
@@ -363,10 +370,16 @@ def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes:
     def now_trace():
         return (time.perf_counter() - t0) * time_scale
 
+    admitted_at = {}    # tenant -> wall seconds since start of its admission
+
     def finish(i, t, answer):
         res.answers[i] = answer
         if trace.kind[i] != UPDATE:
-            res.latencies_ms.append((time.perf_counter() - t0 - trace.time[i] / time_scale) * 1e3)
+            now = time.perf_counter() - t0
+            release = trace.time[i] / time_scale
+            res.latencies_ms.append((now - release) * 1e3)
+            res.service_ms.append((now - max(release, admitted_at.get(t, 0.0))) * 1e3)
+            res.query_req.append(i)
         served[t] += 1
         if served[t] == total[t]:
             depart(t)
@@ -407,6 +420,7 @@ def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes:
                 a.set_gutter_capacity(1 << 18)
                 state[t] = a
             res._add("admit", ts)
+            admitted_at[t] = time.perf_counter() - t0
             waiting.popleft()
             used[0] += c
             resident.add(t)
