@@ -50,6 +50,7 @@ struct GraphDesc {
 // tile {graph, first record (lo, hi), count} belongs to one graph, so its endpoint entries land in
 // that graph's gutter bins only (at most kMbBinsMax of them).
 constexpr uint32_t kMbRecTile = 4096;
+constexpr uint32_t kMbSpan = 32;  // grouped members merged per Boruvka merge warp
 constexpr uint32_t kMbBinsMax = 4096;
 constexpr uint32_t kMbTilesPerBinMax = 64;
 constexpr uint32_t kMbBinTarget = 4096;  // bins per graph aimed for with at most 16 tiles per bin
@@ -445,6 +446,11 @@ struct MBBufs {
   uint32_t *parent, *label, *cnt, *fill;
   uint64_t *packed, *scan_total;
   uint32_t *order, *order_comp, *comp_start, *ncomp, *acc;
+  uint32_t *part, *part_comp;  // per merge warp: its XOR when one component covers its span
+  // sample results of the round, per vertex (round 0) or per component (rounds >= 1): the
+  // sampled edge, or kResZero / kResFail; res_g = the component's graph
+  uint64_t *res;
+  uint32_t *res_g;
   uint32_t *active, *modified;  // per graph
   const uint32_t *round;        // current round (device)
   uint32_t *status;
@@ -466,6 +472,11 @@ __device__ bool mb_unite(uint32_t *parent, uint32_t a, uint32_t b, uint32_t vbas
     }
     if (atomicCAS(parent + b, b, a) == b) return true;
   }
+}
+
+constexpr uint64_t kResZero = ~0ull, kResFail = ~0ull - 1;  // never an edge index (min < max)
+__device__ __forceinline__ uint64_t res_code(int res, uint64_t idx) {
+  return res == 0 ? idx : res == 2 ? kResFail : kResZero;
 }
 
 __device__ void mb_handle(int res, uint64_t idx, uint32_t g, const GraphDesc &gd, const MBBufs &b) {
@@ -515,17 +526,21 @@ __device__ __forceinline__ MbVert mb_vert_shfl(const MbVert &m, uint32_t src) {
   return o;
 }
 
-constexpr int kMbKB = 4;  // vertices whose loads a warp keeps in flight together
-constexpr size_t kMbStageBytes = 8 * sizeof(uint32_t) * Region<1>::kStage;
+constexpr int kMbKB = 8;  // members per cp.async batch
+// dynamic shared memory of a 256-thread query block: per warp two batches of kMbKB member slots
+// and one stage, each slot acc_words (the largest graph's sample region + its deterministic
+// bucket)
+inline size_t mb_query_smem(uint32_t acc_words) { return 8 * sizeof(uint32_t) * (2 * kMbKB + 1) * acc_words; }
 
-// Round 0 for every active graph: a warp takes 32 consecutive global vertices (run_round_zero,
-// src/cc_sketch_alg.cpp:223-244), batches their loads, samples each in word space, and the 32
-// lanes then apply their vertex's result together.
-__global__ void __launch_bounds__(256, 3) k_mb_round0(MBBufs b) {
-  constexpr int NW = Region<1>::kNW;
-  extern __shared__ uint32_t mb_stage[];
+// Round 0 for every active graph (run_round_zero, src/cc_sketch_alg.cpp:223-244): a warp takes
+// 32 consecutive global vertices, copies their sample-0 regions to shared memory with cp.async
+// in batches of kMbKB (one batch ahead), samples each there, and the 32 lanes then apply their
+// vertex's result together.
+__global__ void __launch_bounds__(256) k_mb_round0(MBBufs b) {
+  extern __shared__ uint32_t mb_smem[];
   const uint32_t lane = threadIdx.x & 31;
-  uint32_t *st = mb_stage + (threadIdx.x >> 5) * Region<1>::kStage;
+  const uint32_t SW = b.acc_words;
+  uint32_t *ring = mb_smem + (threadIdx.x >> 5) * (2 * kMbKB + 1) * SW;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; base < b.total_V;
        base += nwarps * 32) {
@@ -537,30 +552,46 @@ __global__ void __launch_bounds__(256, 3) k_mb_round0(MBBufs b) {
       my_act = b.active[me.g] != 0;
     }
     const uint32_t act = __ballot_sync(kFull, my_act);
+    auto issue = [&](uint32_t t) {
+      uint32_t *half = ring + (t & 1) * kMbKB * SW;
+#pragma unroll
+      for (int k = 0; k < kMbKB; ++k) {
+        const uint32_t m = t * kMbKB + k;
+        if (m < n && (act >> m & 1)) {
+          const MbVert mk = mb_vert_shfl(me, m);
+          region_copy_async(half + k * SW, mk.sk, mk.sk + mk.det, 3 * mk.B, lane);
+        }
+      }
+      cp_async_commit();
+    };
     int my_res = 1;
     uint64_t my_idx = 0;
-    for (uint32_t i = 0; i < n; i += kMbKB) {
-      uint32_t x[kMbKB][NW], dw[kMbKB];
-      MbVert m[kMbKB];
-#pragma unroll
+    const uint32_t nb = (n + kMbKB - 1) / kMbKB;
+    issue(0);
+    for (uint32_t t = 0; t < nb; ++t) {
+      if (t + 1 < nb) issue(t + 1);
+      else cp_async_commit();
+      cp_async_wait<1>();
+      __syncwarp();
+      const uint32_t *half = ring + (t & 1) * kMbKB * SW;
+#pragma unroll 1
       for (int k = 0; k < kMbKB; ++k) {
-        if (i + k >= n) break;
-        m[k] = mb_vert_shfl(me, i + k);
-        if (act >> (i + k) & 1) region_load(m[k].sk, m[k].sk + m[k].det, 3 * m[k].B, lane, x[k], dw[k]);
-      }
-#pragma unroll
-      for (int k = 0; k < kMbKB; ++k) {
-        if (i + k >= n) break;
-        if (!(act >> (i + k) & 1)) continue;
+        const uint32_t m = t * kMbKB + k;
+        if (m >= n) break;
+        if (!(act >> m & 1)) continue;
+        const MbVert mk = mb_vert_shfl(me, m);
         uint64_t idx;
-        const int res = warp_sample_region<1>(x[k], dw[k], 3 * m[k].B, m[k].B, m[k].chk, st, &idx);
-        if (lane == i + k) {
+        const int res = warp_sample_smem<1>(half + k * SW, 3 * mk.B, mk.B, mk.chk, &idx);
+        if (lane == m) {
           my_res = res;
           my_idx = idx;
         }
       }
+      __syncwarp();
     }
-    if (my_act) mb_handle(my_res, my_idx, me.g, b.graphs[me.g], b);
+    cp_async_wait<0>();
+    if (lane < n) b.res[base + lane] = my_act ? res_code(my_res, my_idx) : kResZero;
+    __syncwarp();
   }
 }
 
@@ -604,55 +635,99 @@ __global__ void __launch_bounds__(256) k_mb_group(MBBufs b) {
     b.comp_start[c] = start;
     const uint32_t end = start + b.cnt[r];
     if (start / b.span != (end - 1) / b.span) {
-      uint32_t *ac = b.acc + (uint64_t)c * b.acc_words;
+      uint32_t *ac = b.acc + (uint64_t)(start / b.span) * b.acc_words;
       for (uint32_t i = 0; i < b.acc_words; ++i) ac[i] = 0;
     }
   }
 }
 
 // Round >= 1 merge (perform_boruvka_round, src/cc_sketch_alg.cpp:246-380) over the grouped
-// members of every active graph: `span` members per warp, kMbKB members' loads in flight,
-// column `round` of each graph XORed in word space; in-span components are sampled here (the
-// results applied 32 at a time by the lanes), the others combined in acc.
-__global__ void __launch_bounds__(256, 2) k_mb_merge(MBBufs b) {
+// members of every active graph: a warp takes kMbSpan consecutive members, copies column
+// `round` of each (its graph's B buckets) and the deterministic bucket to shared memory with
+// cp.async, one batch ahead, and XORs them in registers. A component wholly inside the span is
+// sampled here (the results applied 32 at a time by the lanes); a component covering the whole
+// span leaves the warp's XOR in its partial slot (folded by k_mb_reduce_parts); the parts of
+// components crossing a span edge go to acc with one atomicXor per word.
+__global__ void __launch_bounds__(256) k_mb_merge(MBBufs b) {
   constexpr int NW = Region<1>::kNW;
-  extern __shared__ uint32_t mb_stage[];
+  extern __shared__ uint32_t mb_smem[];
   const uint32_t lane = threadIdx.x & 31;
-  uint32_t *st = mb_stage + (threadIdx.x >> 5) * Region<1>::kStage;
+  const uint32_t SW = b.acc_words;
+  uint32_t *ring = mb_smem + (threadIdx.x >> 5) * (2 * kMbKB + 1) * SW;
+  uint32_t *st = ring + 2 * kMbKB * SW;
   const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nc = *b.ncomp;
   const uint32_t members = b.comp_start[nc];
-  const uint64_t p0 = (uint64_t)w * b.span;
-  if (p0 >= members) return;
-  const uint32_t p1 = (p0 + b.span < members) ? (uint32_t)(p0 + b.span) : members;
+  const uint64_t p0 = (uint64_t)w * kMbSpan;
+  if (p0 >= members) {  // past the active graphs' members: this slot holds nothing this round
+    if (lane == 0) b.part_comp[w] = 0xffffffffu;
+    return;
+  }
+  const uint32_t n = members - p0 < kMbSpan ? members - (uint32_t)p0 : kMbSpan;
+  const uint32_t p1 = (uint32_t)p0 + n;
   const uint32_t round = *b.round;
+  MbVert me{};
+  uint32_t my_c = 0;
+  if (lane < n) {
+    me = mb_vert(b, b.order[p0 + lane]);
+    my_c = b.order_comp[p0 + lane];
+  }
+  // components of the positions just outside the span (members of a component are contiguous)
+  uint32_t edge_c = 0xffffffffu;
+  if (lane == 0 && p0 > 0) edge_c = b.order_comp[p0 - 1];
+  if (lane == 1 && p1 < members) edge_c = b.order_comp[p1];
+  const uint32_t prev_c = __shfl_sync(kFull, edge_c, 0), next_c = __shfl_sync(kFull, edge_c, 1);
+  auto issue = [&](uint32_t t) {
+    uint32_t *half = ring + (t & 1) * kMbKB * SW;
+#pragma unroll
+    for (int k = 0; k < kMbKB; ++k) {
+      const uint32_t m = t * kMbKB + k;
+      if (m < n) {
+        const MbVert mk = mb_vert_shfl(me, m);
+        region_copy_async(half + k * SW, mk.sk + 3 * round * mk.B, mk.sk + mk.det, 3 * mk.B, lane);
+      }
+    }
+    cp_async_commit();
+  };
+  issue(0);
   uint32_t acc[NW], dacc = 0;
 #pragma unroll
   for (int k = 0; k < NW; ++k) acc[k] = 0;
   uint32_t cur = 0xffffffffu;
   MbVert cm{};  // a member of the current component (its graph's geometry)
-  int my_res = 1;
-  uint64_t my_idx = 0;
-  uint32_t my_g = 0, nres = 0;
-  auto apply = [&]() {
-    if (lane < nres) mb_handle(my_res, my_idx, my_g, b.graphs[my_g], b);
-    __syncwarp();
-    nres = 0;
-  };
+  bool whole = false;
   auto flush = [&]() {
-    const uint32_t s = b.comp_start[cur], e = b.comp_start[cur + 1];
+    const bool before = cur == prev_c, after = cur == next_c;
     const uint32_t W = 3 * cm.B;
-    if (s >= p0 && e <= p1) {
-      uint64_t idx;
-      const int res = warp_sample_region<1>(acc, dacc, W, cm.B, cm.chk, st, &idx);
-      if (lane == nres) {
-        my_res = res;
-        my_idx = idx;
-        my_g = cm.g;
+    if (!before && !after) {
+#pragma unroll
+      for (int k = 0; k < NW; ++k) {
+        const uint32_t wi = k * 32 + lane;
+        if (wi < W) st[wi] = acc[k];
       }
-      if (++nres == 32) apply();
+      if (lane < 3) st[W + lane] = dacc;
+      __syncwarp();
+      uint64_t idx;
+      const int res = warp_sample_smem<1>(st, W, cm.B, cm.chk, &idx);
+      __syncwarp();
+      if (lane == 0) {
+        b.res[cur] = res_code(res, idx);
+        b.res_g[cur] = cm.g;
+      }
+    } else if (before && after) {
+      uint32_t *pt = b.part + (uint64_t)w * SW;
+#pragma unroll
+      for (int k = 0; k < NW; ++k) {
+        const uint32_t wi = k * 32 + lane;
+        if (wi < W) pt[wi] = acc[k];
+      }
+      if (lane < 3) pt[W + lane] = dacc;
+      if (lane == 0) b.part_comp[w] = cur;
+      whole = true;
     } else {
-      uint32_t *ac = b.acc + (uint64_t)cur * b.acc_words;
+      // a component crossing a span edge owns acc slot (its first position / span)
+      const uint32_t slot = before ? b.comp_start[cur] / kMbSpan : w;
+      uint32_t *ac = b.acc + (uint64_t)slot * SW;
 #pragma unroll
       for (int k = 0; k < NW; ++k) {
         const uint32_t wi = k * 32 + lane;
@@ -661,43 +736,97 @@ __global__ void __launch_bounds__(256, 2) k_mb_merge(MBBufs b) {
       if (lane < 3 && dacc) atomicXor(ac + W + lane, dacc);
     }
   };
-  for (uint32_t cb = (uint32_t)p0; cb < p1; cb += 32) {
-    const uint32_t n = p1 - cb < 32 ? p1 - cb : 32;
-    MbVert me{};
-    uint32_t my_c = 0;
-    if (lane < n) {
-      me = mb_vert(b, b.order[cb + lane]);
-      my_c = b.order_comp[cb + lane];
+  const uint32_t nb = (n + kMbKB - 1) / kMbKB;
+  for (uint32_t t = 0; t < nb; ++t) {
+    if (t + 1 < nb) issue(t + 1);
+    else cp_async_commit();
+    cp_async_wait<1>();
+    __syncwarp();
+    const uint32_t *half = ring + (t & 1) * kMbKB * SW;
+    // not unrolled: one copy of the flush keeps the kernel small for the instruction cache
+#pragma unroll 1
+    for (int k = 0; k < kMbKB; ++k) {
+      const uint32_t m = t * kMbKB + k;
+      if (m >= n) break;
+      const uint32_t c = __shfl_sync(kFull, my_c, m);
+      if (c != cur) {
+        if (cur != 0xffffffffu) flush();
+        cur = c;
+        cm = mb_vert_shfl(me, m);
+#pragma unroll
+        for (int q = 0; q < NW; ++q) acc[q] = 0;
+        dacc = 0;
+      }
+      const uint32_t W = 3 * cm.B;
+      const uint32_t *sl = half + k * SW;
+#pragma unroll
+      for (int q = 0; q < NW; ++q) {
+        const uint32_t wi = q * 32 + lane;
+        if (wi < W) acc[q] ^= sl[wi];
+      }
+      if (lane < 3) dacc ^= sl[W + lane];
     }
-    for (uint32_t i = 0; i < n; i += kMbKB) {
-      uint32_t x[kMbKB][NW], dw[kMbKB];
-      MbVert m[kMbKB];
+    __syncwarp();
+  }
+  cp_async_wait<0>();
+  flush();
+  if (!whole && lane == 0) b.part_comp[w] = 0xffffffffu;
+}
+
+// Folds the partial slots of merge warps covered by one component into its acc: one warp per
+// 32 consecutive slots, one atomicXor per word per component per warp. Slots are folded whole
+// (acc_words): a smaller graph's slot tail lands in its acc's unused tail.
+__global__ void __launch_bounds__(256) k_mb_reduce_parts(MBBufs b, uint32_t nslots) {
+  constexpr int NW = Region<1>::kNW;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t s0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32;
+  if (s0 >= nslots) return;
+  const uint32_t n = nslots - s0 < 32 ? nslots - s0 : 32;
+  const uint32_t SW = b.acc_words, W = SW - 3;
+  const uint32_t my_c = lane < n ? b.part_comp[s0 + lane] : 0xffffffffu;
+  uint32_t live = __ballot_sync(kFull, my_c != 0xffffffffu);
+  if (!live) return;
+  uint32_t acc[NW], dacc = 0, cur = 0xffffffffu;
 #pragma unroll
-      for (int k = 0; k < kMbKB; ++k) {
-        if (i + k >= n) break;
-        m[k] = mb_vert_shfl(me, i + k);
-        region_load(m[k].sk + 3 * round * m[k].B, m[k].sk + m[k].det, 3 * m[k].B, lane, x[k], dw[k]);
+  for (int k = 0; k < NW; ++k) acc[k] = 0;
+  auto flush = [&]() {
+    uint32_t *ac = b.acc + (uint64_t)(b.comp_start[cur] / kMbSpan) * SW;
+#pragma unroll
+    for (int k = 0; k < NW; ++k) {
+      const uint32_t wi = k * 32 + lane;
+      if (wi < W && acc[k]) atomicXor(ac + wi, acc[k]);
+    }
+    if (lane < 3 && dacc) atomicXor(ac + W + lane, dacc);
+  };
+  while (live) {
+    constexpr int KB = 4;
+    uint32_t x[KB][NW], dw[KB], sl[KB];
+#pragma unroll
+    for (int k = 0; k < KB; ++k) {
+      sl[k] = live ? __ffs(live) - 1 : 32u;
+      if (live) live &= live - 1;
+      if (sl[k] < 32) {
+        const uint32_t *pt = b.part + (uint64_t)(s0 + sl[k]) * SW;
+        region_load(pt, pt + W, W, lane, x[k], dw[k]);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < KB; ++k) {
+      if (sl[k] >= 32) break;
+      const uint32_t c = __shfl_sync(kFull, my_c, sl[k]);
+      if (c != cur) {
+        if (cur != 0xffffffffu) flush();
+        cur = c;
+#pragma unroll
+        for (int q = 0; q < NW; ++q) acc[q] = 0;
+        dacc = 0;
       }
 #pragma unroll
-      for (int k = 0; k < kMbKB; ++k) {
-        if (i + k >= n) break;
-        const uint32_t c = __shfl_sync(kFull, my_c, i + k);
-        if (c != cur) {
-          if (cur != 0xffffffffu) flush();
-          cur = c;
-          cm = m[k];
-#pragma unroll
-          for (int q = 0; q < NW; ++q) acc[q] = 0;
-          dacc = 0;
-        }
-#pragma unroll
-        for (int q = 0; q < NW; ++q) acc[q] ^= x[k][q];
-        dacc ^= dw[k];
-      }
+      for (int q = 0; q < NW; ++q) acc[q] ^= x[k][q];
+      dacc ^= dw[k];
     }
   }
   flush();
-  apply();
 }
 
 __global__ void k_mb_sample_spanning(MBBufs b) {
@@ -709,7 +838,7 @@ __global__ void k_mb_sample_spanning(MBBufs b) {
     if (s / b.span == (e - 1) / b.span) continue;
     const uint32_t g = b.gov[b.order[s]];
     const GraphDesc gd = b.graphs[g];
-    const uint32_t *ac = b.acc + (uint64_t)c * b.acc_words;
+    const uint32_t *ac = b.acc + (uint64_t)(s / b.span) * b.acc_words;
     uint32_t a[2][3] = {{0, 0, 0}, {0, 0, 0}}, d[3];
     d[0] = __ldcg(ac + 3 * gd.B);
     d[1] = __ldcg(ac + 3 * gd.B + 1);
@@ -725,8 +854,29 @@ __global__ void k_mb_sample_spanning(MBBufs b) {
     }
     uint64_t idx;
     const int res = warp_sample(d, a, gd.B, b.flip[gd.flip_off + gd.C], &idx);
-    if (lane == 0) mb_handle(res, idx, g, gd, b);
+    if (lane == 0) {
+      b.res[c] = res_code(res, idx);
+      b.res_g[c] = g;
+    }
   }
+}
+
+// sample_supernode (src/cc_sketch_alg.cpp:137-166) for every result of the round: n results
+// (all vertices in round 0, else the components), visited transposed -- lane l of a warp takes
+// result l * ceil(n / 32) + warp -- so that the lanes of one warp work on distant components
+// (other graphs, mostly) rather than on neighbours that would race for one root's CAS.
+__global__ void k_mb_unite(MBBufs b, int round0) {
+  const uint32_t n = round0 ? b.total_V : *b.ncomp;
+  const uint32_t q = (n + 31) / 32;
+  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 32ull * q) return;
+  const uint64_t i64 = (t & 31) * (uint64_t)q + (t >> 5);
+  if (i64 >= n) return;
+  const uint32_t i = (uint32_t)i64;
+  const uint64_t r = b.res[i];
+  if (r == kResZero) return;
+  const uint32_t g = round0 ? b.gov[i] : b.res_g[i];
+  mb_handle(r == kResFail ? 2 : 0, r, g, b.graphs[g], b);
 }
 
 __global__ void k_mb_reset(uint32_t n, uint32_t *parent) {
@@ -866,6 +1016,11 @@ struct gz_batch {
   // Boruvka
   uint32_t *d_parent = nullptr, *d_label = nullptr, *d_cnt = nullptr, *d_fill = nullptr;
   uint64_t *d_packed = nullptr, *d_vscan_total = nullptr, *d_vscan_tmp = nullptr;
+  uint32_t *d_part = nullptr, *d_part_comp = nullptr;
+  uint64_t cap_part = 0, cap_part_comp = 0;
+  uint64_t *d_res = nullptr;
+  uint32_t *d_res_g = nullptr;
+  uint64_t cap_res = 0, cap_res_g = 0;
   uint32_t *d_order = nullptr, *d_order_comp = nullptr, *d_comp_start = nullptr, *d_ncomp = nullptr, *d_acc = nullptr;
   uint32_t *d_active = nullptr, *d_modified = nullptr, *d_round = nullptr, *d_ncc = nullptr;
   cudaGraphExec_t round_exec = nullptr;
@@ -892,6 +1047,10 @@ struct gz_batch {
     b.scan_total = d_vscan_total;
     b.order = d_order;
     b.order_comp = d_order_comp;
+    b.part = d_part;
+    b.part_comp = d_part_comp;
+    b.res = d_res;
+    b.res_g = d_res_g;
     b.comp_start = d_comp_start;
     b.ncomp = d_ncomp;
     b.acc = d_acc;
@@ -901,7 +1060,7 @@ struct gz_batch {
     b.status = d_status;
     b.total_V = (uint32_t)total_V;
     b.acc_words = (max_B + 1) * 3;
-    b.span = total_V >= (1u << 19) ? 128 : 64;
+    b.span = gz::kMbSpan;
     return b;
   }
 };
@@ -942,6 +1101,10 @@ void batch_destroy(gz_batch *h) {
   mb_free(h->d_vscan_tmp);
   mb_free(h->d_order);
   mb_free(h->d_order_comp);
+  mb_free(h->d_part);
+  mb_free(h->d_part_comp);
+  mb_free(h->d_res);
+  mb_free(h->d_res_g);
   mb_free(h->d_comp_start);
   mb_free(h->d_ncomp);
   mb_free(h->d_acc);
@@ -1253,7 +1416,12 @@ int ensure_boruvka(gz_batch *h) {
     MB_TRY(mb_alloc(&h->d_comp_start, Vn + 1));
     h->cap_bv_V = Vn;
   }
-  MB_TRY(grow(&h->d_acc, h->cap_acc, V * (uint64_t)(h->max_B + 1) * 3));
+  const uint64_t slots = (V + kMbSpan - 1) / kMbSpan;
+  MB_TRY(grow(&h->d_acc, h->cap_acc, (slots + 1) * (uint64_t)(h->max_B + 1) * 3));
+  MB_TRY(grow(&h->d_part, h->cap_part, slots * (uint64_t)(h->max_B + 1) * 3));
+  MB_TRY(grow(&h->d_part_comp, h->cap_part_comp, slots));
+  MB_TRY(grow(&h->d_res, h->cap_res, V));
+  MB_TRY(grow(&h->d_res_g, h->cap_res_g, V));
   if (!h->d_active || h->cap_bv_G < G) {
     const uint64_t Gn = headroom(h->cap_bv_G, G);
     mb_free(h->d_active);
@@ -1282,9 +1450,13 @@ int enqueue_round(gz_batch *h, cudaStream_t s) {
   k_mb_pack<<<cdiv(V, 256), 256, 0, s>>>(b);
   MB_CUDA(scan_exclusive_u64(h->d_packed, V, h->d_vscan_total, h->d_vscan_tmp, s));
   k_mb_group<<<cdiv(V, 256), 256, 0, s>>>(b);
-  const uint64_t warps = (V + b.span - 1) / b.span;
-  k_mb_merge<<<cdiv(warps * 32, 256), 256, kMbStageBytes, s>>>(b);
+  const uint64_t warps = (V + kMbSpan - 1) / kMbSpan;
+  const size_t smem = mb_query_smem(b.acc_words);
+  MB_CUDA(cudaFuncSetAttribute(k_mb_merge, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_mb_merge<<<cdiv(warps * 32, 256), 256, smem, s>>>(b);
+  k_mb_reduce_parts<<<cdiv(warps, 256), 256, 0, s>>>(b, (uint32_t)warps);
   k_mb_sample_spanning<<<std::min<unsigned>(cdiv(V * 32, 256), num_sms() * 16), 256, 0, s>>>(b);
+  k_mb_unite<<<cdiv(32 * ((V + 31) / 32), 256), 256, 0, s>>>(b, 0);
   MB_CUDA(cudaGetLastError());
   return GZ_OK;
 }
@@ -1308,7 +1480,16 @@ int batch_query(gz_batch *h, uint32_t *labels_out) {
   k_mb_reset<<<cdiv(V, 256), 256, 0, h->stream>>>((uint32_t)V, h->d_parent);
   MB_CUDA(cudaMemcpyAsync(h->d_active, active.data(), sizeof(uint32_t) * G, cudaMemcpyHostToDevice, h->stream));
   MB_CUDA(cudaMemsetAsync(h->d_modified, 0, sizeof(uint32_t) * G, h->stream));
-  k_mb_round0<<<std::min<unsigned>(cdiv(V, 256), num_sms() * 8), 256, kMbStageBytes, h->stream>>>(b);
+  {
+    const size_t smem = mb_query_smem(b.acc_words);
+    MB_CUDA(cudaFuncSetAttribute(k_mb_round0, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mb_round0, 256, smem) != cudaSuccess || per_sm < 1)
+      per_sm = 1;
+    k_mb_round0<<<std::min<unsigned>(cdiv(V, 256), num_sms() * per_sm), 256, smem, h->stream>>>(b);
+    k_mb_unite<<<cdiv(32 * ((V + 31) / 32), 256), 256, 0, h->stream>>>(b, 1);
+    h->launches++;
+  }
   h->launches += 2;
   MB_CUDA(cudaGetLastError());
   // The round runs as a captured CUDA graph once the same graphs and buffers come back (a batch
@@ -1377,7 +1558,7 @@ int batch_query(gz_batch *h, uint32_t *labels_out) {
     } else {
       const uint64_t l0 = launch_count();
       MB_TRY(enqueue_round(h, h->stream));
-      h->launches += 5 + (launch_count() - l0);
+      h->launches += 7 + (launch_count() - l0);  // label, pack, group, merge, reduce, sample, unite
     }
     h->prof_rounds++;
   }

@@ -730,8 +730,8 @@ int alloc_bv(gz::BoruvkaBufs &b, size_t V, size_t acc_words, uint32_t *status) {
   GZ_TRY(dev_alloc(&b.comp_start, V + 1));
   GZ_TRY(dev_alloc(&b.comp_key, V));
   GZ_TRY(dev_alloc(&b.ncomp, 1));
-  GZ_TRY(dev_alloc(&b.acc, V * acc_words));
   const size_t warps = (V + gz::kBoruvkaSpan - 1) / gz::kBoruvkaSpan;
+  GZ_TRY(dev_alloc(&b.acc, (warps + 1) * acc_words));
   GZ_TRY(dev_alloc(&b.part, warps * acc_words));
   GZ_TRY(dev_alloc(&b.part_comp, warps));
   GZ_TRY(dev_alloc(&b.big, 1));

@@ -819,7 +819,7 @@ __global__ void __launch_bounds__(256) k_bv_group(uint32_t V, uint32_t acc_words
     comp_key[c] = minv ? minv[r] : r;
     const uint32_t end = start + cnt[r];
     if (start / span != (end - 1) / span) {
-      uint32_t *ac = acc + (uint64_t)c * acc_words;
+      uint32_t *ac = acc + (uint64_t)(start / span) * acc_words;
       for (uint32_t i = 0; i < acc_words; ++i) ac[i] = 0;
       if (2ull * cnt[r] > V) *big = c;  // at most one component holds over half the vertices
     }
@@ -927,7 +927,9 @@ __global__ void __launch_bounds__(256) k_bv_merge(BoruvkaGeom g, const uint32_t 
       if (lane == 0) b.part_comp[w] = comp;
       whole = true;
     } else {
-      uint32_t *ac = b.acc + (uint64_t)comp * SW;
+      // a component crossing a span edge owns acc slot (its first position / span)
+      const uint32_t slot = before ? b.comp_start[comp] / g.span : w;
+      uint32_t *ac = b.acc + (uint64_t)slot * SW;
 #pragma unroll
       for (int k = 0; k < NW; ++k) {
         const uint32_t wi = k * 32 + lane;
@@ -980,7 +982,7 @@ __global__ void __launch_bounds__(256) k_bv_merge(BoruvkaGeom g, const uint32_t 
   if (cur != 0xffffffffu) flush(cur);
   apply();
   if (big != 0xffffffffu) {
-    uint32_t *ac = b.acc + (uint64_t)big * SW;
+    uint32_t *ac = b.acc + (uint64_t)(b.comp_start[big] / g.span) * SW;
 #pragma unroll
     for (int k = 0; k < NW; ++k) {
       const uint32_t wi = k * 32 + lane;
@@ -1008,7 +1010,7 @@ __global__ void __launch_bounds__(256) k_bv_reduce_parts(BoruvkaGeom g, uint32_t
 #pragma unroll
   for (int k = 0; k < NW; ++k) acc[k] = 0;
   auto flush = [&]() {
-    uint32_t *ac = b.acc + (uint64_t)cur * (W + 3);
+    uint32_t *ac = b.acc + (uint64_t)(b.comp_start[cur] / g.span) * (W + 3);
 #pragma unroll
     for (int k = 0; k < NW; ++k) {
       const uint32_t wi = k * 32 + lane;
@@ -1056,7 +1058,7 @@ __global__ void k_bv_sample_spanning(BoruvkaGeom g, BoruvkaBufs b) {
   for (uint32_t comp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; comp < nc; comp += nwarps) {
     const uint32_t s = b.comp_start[comp], e = b.comp_start[comp + 1];
     if (s / g.span == (e - 1) / g.span) continue;
-    const uint32_t *ac = b.acc + (uint64_t)comp * acc_words;
+    const uint32_t *ac = b.acc + (uint64_t)(s / g.span) * acc_words;
     uint32_t a[CPS][2][3], d[3];
     d[0] = __ldcg(ac + 3 * CPS * g.B);
     d[1] = __ldcg(ac + 3 * CPS * g.B + 1);

@@ -146,7 +146,8 @@ struct BoruvkaBufs {
   uint32_t *comp_start;  // V+1
   uint32_t *comp_key;    // V
   uint32_t *ncomp;       // 1
-  uint32_t *acc;         // V * (B+1) * 3 words: merged buckets of components spanning warps
+  uint32_t *acc;         // (V / span + 2) * (B+1) * 3 words: merged buckets of each component
+                         // crossing a span edge, at slot (its first grouped position / span)
   uint32_t *part;        // per merge warp: its members' XOR when one component covers its span
   uint32_t *part_comp;   // per merge warp: that component, or ~0
   uint32_t *big;         // 1   the component holding more than half the vertices, or ~0
