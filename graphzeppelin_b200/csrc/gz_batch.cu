@@ -930,6 +930,30 @@ void mb_free(T *&p) {
   p = nullptr;
 }
 
+// Stream-ordered reallocation of scratch that grows while the engine runs: cudaFree would wait
+// for the whole device (every request in flight, on every stream); cudaFreeAsync/cudaMallocAsync
+// only order against the engine's own stream. The device's default pool keeps freed memory
+// (release threshold raised once per process), so regrowth does not go back to the driver.
+template <class T>
+int mb_realloc_async(T **p, size_t count, cudaStream_t s) {
+  static std::once_flag keep;
+  std::call_once(keep, [] {
+    int dev = 0;
+    cudaMemPool_t pool;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+      uint64_t keep_all = ~0ull;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep_all);
+    }
+  });
+  if (*p) cudaFreeAsync(*p, s);
+  *p = nullptr;
+  void *q = nullptr;
+  cudaError_t e = cudaMallocAsync(&q, std::max<size_t>(count, 1) * sizeof(T), s);
+  if (e != cudaSuccess) return mb_fail(GZ_ERR_NOMEM, std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
+  *p = static_cast<T *>(q);
+  return GZ_OK;
+}
+
 // graph g owns global tiles [tile_base, +ntiles) and global vertices [vbase, +V)
 __global__ void k_mb_fill_tables(const GraphDesc *graphs, uint32_t G, uint32_t *tile_graph, uint32_t *gov) {
   for (uint32_t g = blockIdx.x; g < G; g += gridDim.x) {
@@ -1181,12 +1205,11 @@ inline uint64_t headroom(uint64_t cap, uint64_t need) {
 }
 
 template <class T>
-int grow(T **p, uint64_t &cap, uint64_t need) {
+int grow(T **p, uint64_t &cap, uint64_t need, cudaStream_t s) {
   if (*p && cap >= need) return GZ_OK;
   const uint64_t n = headroom(cap, need);
-  mb_free(*p);
   cap = 0;
-  MB_TRY(mb_alloc(p, std::max<uint64_t>(n, 1)));
+  MB_TRY(mb_realloc_async(p, std::max<uint64_t>(n, 1), s));
   cap = n;
   return GZ_OK;
 }
@@ -1215,20 +1238,16 @@ int finalize_graphs(gz_batch *h) {
   h->total_bins = bin_base;
   h->total_tiles = tile_base;
   if (h->G == 0) return GZ_OK;
-  MB_TRY(grow(&h->d_graphs, h->cap_graphs, h->G));
-  MB_TRY(grow(&h->d_tile_graph, h->cap_tiles, h->total_tiles));
-  MB_TRY(grow(&h->d_gov, h->cap_V, h->total_V));
+  MB_TRY(grow(&h->d_graphs, h->cap_graphs, h->G, h->stream));
+  MB_TRY(grow(&h->d_tile_graph, h->cap_tiles, h->total_tiles, h->stream));
+  MB_TRY(grow(&h->d_gov, h->cap_V, h->total_V, h->stream));
   if (!h->d_bins || h->cap_bins < h->total_bins) {
     const uint64_t nb = headroom(h->cap_bins, h->total_bins);
-    mb_free(h->d_bins);
-    mb_free(h->d_bin_fill);
-    mb_free(h->d_scan_tmp);
-    mb_free(h->d_bin_off);
     h->cap_bins = 0;
-    MB_TRY(mb_alloc(&h->d_bins, nb));
-    MB_TRY(mb_alloc(&h->d_bin_fill, nb));
-    MB_TRY(mb_alloc(&h->d_scan_tmp, scan_tmp_words(nb)));
-    MB_TRY(mb_alloc(&h->d_bin_off, nb + 1));
+    MB_TRY(mb_realloc_async(&h->d_bins, nb, h->stream));
+    MB_TRY(mb_realloc_async(&h->d_bin_fill, nb, h->stream));
+    MB_TRY(mb_realloc_async(&h->d_scan_tmp, scan_tmp_words(nb), h->stream));
+    MB_TRY(mb_realloc_async(&h->d_bin_off, nb + 1, h->stream));
     h->cap_bins = nb;
   }
   MB_CUDA(cudaMemcpyAsync(h->d_graphs, h->graphs.data(), sizeof(GraphDesc) * h->G, cudaMemcpyHostToDevice, h->stream));
@@ -1301,7 +1320,7 @@ int batch_ingest(gz_batch *h, const void *d_rec, const uint64_t *off) {
   if (rt_dense.empty() && rt_sparse.empty()) return GZ_OK;
   if (2 * n_dense >= 0xFFFFFFF0ull) return mb_fail(GZ_ERR_INVALID, "more than 2^31 records in one batch ingest");
   const size_t n_rt = rt_dense.size() + rt_sparse.size();
-  MB_TRY(grow(&h->d_rtiles, h->rtiles_cap, n_rt));
+  MB_TRY(grow(&h->d_rtiles, h->rtiles_cap, n_rt, h->stream));
   cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
   if (h->prof) {
     cudaEventCreate(&e0);
@@ -1314,8 +1333,8 @@ int batch_ingest(gz_batch *h, const void *d_rec, const uint64_t *off) {
   const uint32_t n_rt_dense = (uint32_t)(n_rt - rt_sparse.size());
   const uint8_t *rec = static_cast<const uint8_t *>(d_rec);
   if (n_rt_dense) {
-    MB_TRY(grow(&h->d_entries, h->entry_cap, 2 * n_dense));
-    MB_TRY(grow(&h->d_worklist, h->cap_worklist, h->total_tiles));
+    MB_TRY(grow(&h->d_entries, h->entry_cap, 2 * n_dense, h->stream));
+    MB_TRY(grow(&h->d_worklist, h->cap_worklist, h->total_tiles, h->stream));
     MB_TRY(mb_alloc(&h->d_wl_len, 1));
     MB_CUDA(cudaMemsetAsync(h->d_bins, 0, sizeof(uint64_t) * h->total_bins, h->stream));
     MB_CUDA(cudaMemsetAsync(h->d_bin_fill, 0, sizeof(uint32_t) * h->total_bins, h->stream));
@@ -1395,42 +1414,30 @@ int ensure_boruvka(gz_batch *h) {
   const uint64_t V = h->total_V, G = h->G;
   if (!h->d_parent || h->cap_bv_V < V) {
     const uint64_t Vn = headroom(h->cap_bv_V, V);
-    mb_free(h->d_parent);
-    mb_free(h->d_label);
-    mb_free(h->d_cnt);
-    mb_free(h->d_fill);
-    mb_free(h->d_packed);
-    mb_free(h->d_vscan_tmp);
-    mb_free(h->d_order);
-    mb_free(h->d_order_comp);
-    mb_free(h->d_comp_start);
     h->cap_bv_V = 0;
-    MB_TRY(mb_alloc(&h->d_parent, Vn));
-    MB_TRY(mb_alloc(&h->d_label, Vn));
-    MB_TRY(mb_alloc(&h->d_cnt, Vn));
-    MB_TRY(mb_alloc(&h->d_fill, Vn));
-    MB_TRY(mb_alloc(&h->d_packed, Vn));
-    MB_TRY(mb_alloc(&h->d_vscan_tmp, scan_tmp_words(Vn)));
-    MB_TRY(mb_alloc(&h->d_order, Vn));
-    MB_TRY(mb_alloc(&h->d_order_comp, Vn));
-    MB_TRY(mb_alloc(&h->d_comp_start, Vn + 1));
+    MB_TRY(mb_realloc_async(&h->d_parent, Vn, h->stream));
+    MB_TRY(mb_realloc_async(&h->d_label, Vn, h->stream));
+    MB_TRY(mb_realloc_async(&h->d_cnt, Vn, h->stream));
+    MB_TRY(mb_realloc_async(&h->d_fill, Vn, h->stream));
+    MB_TRY(mb_realloc_async(&h->d_packed, Vn, h->stream));
+    MB_TRY(mb_realloc_async(&h->d_vscan_tmp, scan_tmp_words(Vn), h->stream));
+    MB_TRY(mb_realloc_async(&h->d_order, Vn, h->stream));
+    MB_TRY(mb_realloc_async(&h->d_order_comp, Vn, h->stream));
+    MB_TRY(mb_realloc_async(&h->d_comp_start, Vn + 1, h->stream));
     h->cap_bv_V = Vn;
   }
   const uint64_t slots = (V + kMbSpan - 1) / kMbSpan;
-  MB_TRY(grow(&h->d_acc, h->cap_acc, (slots + 1) * (uint64_t)(h->max_B + 1) * 3));
-  MB_TRY(grow(&h->d_part, h->cap_part, slots * (uint64_t)(h->max_B + 1) * 3));
-  MB_TRY(grow(&h->d_part_comp, h->cap_part_comp, slots));
-  MB_TRY(grow(&h->d_res, h->cap_res, V));
-  MB_TRY(grow(&h->d_res_g, h->cap_res_g, V));
+  MB_TRY(grow(&h->d_acc, h->cap_acc, (slots + 1) * (uint64_t)(h->max_B + 1) * 3, h->stream));
+  MB_TRY(grow(&h->d_part, h->cap_part, slots * (uint64_t)(h->max_B + 1) * 3, h->stream));
+  MB_TRY(grow(&h->d_part_comp, h->cap_part_comp, slots, h->stream));
+  MB_TRY(grow(&h->d_res, h->cap_res, V, h->stream));
+  MB_TRY(grow(&h->d_res_g, h->cap_res_g, V, h->stream));
   if (!h->d_active || h->cap_bv_G < G) {
     const uint64_t Gn = headroom(h->cap_bv_G, G);
-    mb_free(h->d_active);
-    mb_free(h->d_modified);
-    mb_free(h->d_ncc);
     h->cap_bv_G = 0;
-    MB_TRY(mb_alloc(&h->d_active, Gn));
-    MB_TRY(mb_alloc(&h->d_modified, Gn));
-    MB_TRY(mb_alloc(&h->d_ncc, Gn));
+    MB_TRY(mb_realloc_async(&h->d_active, Gn, h->stream));
+    MB_TRY(mb_realloc_async(&h->d_modified, Gn, h->stream));
+    MB_TRY(mb_realloc_async(&h->d_ncc, Gn, h->stream));
     h->cap_bv_G = Gn;
   }
   MB_TRY(mb_alloc(&h->d_vscan_total, 1));
@@ -1731,9 +1738,8 @@ int gz_batch_ingest(gz_batch_t *h, const void *records, const uint64_t *offsets)
   if (n == 0) return GZ_OK;
   if (h->rec_cap < n * 9) {
     const uint64_t nr = headroom(h->rec_cap, n * 9);
-    mb_free(h->d_rec);
     h->rec_cap = 0;
-    MB_TRY(mb_alloc(&h->d_rec, nr));
+    MB_TRY(mb_realloc_async(&h->d_rec, nr, h->stream));
     h->rec_cap = nr;
   }
   MB_CUDA(cudaMemcpyAsync(h->d_rec, records, n * 9, cudaMemcpyHostToDevice, h->stream));
@@ -2025,7 +2031,7 @@ namespace {
 
 int serve_run_job(gz_server *s, QueryJob *j) {
   gz_batch *q = &s->query;
-  MB_TRY(grow(&s->d_qflip, s->qflip_cap, j->flips.size()));
+  MB_TRY(grow(&s->d_qflip, s->qflip_cap, j->flips.size(), s->query.stream));
   q->d_flip = s->d_qflip;
   MB_CUDA(cudaMemcpyAsync(s->d_qflip, j->flips.data(), 8 * j->flips.size(), cudaMemcpyHostToDevice, q->stream));
   q->graphs = j->descs;
@@ -2294,7 +2300,7 @@ int gz_server_ingest(gz_server_t *s, uint32_t n, const uint32_t *ids, const void
   for (uint32_t i = 0; i < n; ++i) e->graphs[i] = s->tenants[ids[i]].desc;
   e->d_flip = s->d_flip;
   MB_TRY(finalize_graphs(e));
-  MB_TRY(grow(&s->d_rec, s->rec_cap, nrec * 9));
+  MB_TRY(grow(&s->d_rec, s->rec_cap, nrec * 9, s->ingest.stream));
   MB_CUDA(cudaMemcpyAsync(s->d_rec, static_cast<const uint8_t *>(records) + offsets[0] * 9, nrec * 9,
                           cudaMemcpyHostToDevice, e->stream));
   std::vector<uint64_t> rel(n + 1);
@@ -2328,7 +2334,7 @@ int gz_server_ingest_segments(gz_server_t *s, uint32_t nseg, const uint32_t *ten
   for (size_t i = 0; i < ids.size(); ++i) e->graphs[i] = s->tenants[ids[i]].desc;
   e->d_flip = s->d_flip;
   MB_TRY(finalize_graphs(e));
-  MB_TRY(grow(&s->d_rec, s->rec_cap, nrec * 9));
+  MB_TRY(grow(&s->d_rec, s->rec_cap, nrec * 9, s->ingest.stream));
   uint64_t pos = 0;
   for (uint32_t k = 0; k < nseg; ++k) {
     if (!counts[k]) continue;
