@@ -243,6 +243,8 @@ def run_b200(args, cfg):
     alg = gz.CCSketchAlg(V, cfg["sketch_seed"])
     if args.host_rounds:
         alg.set_query_graph(False)
+    if args.pipeline is not None:
+        alg.set_pipeline(args.pipeline)
     alg.set_gutter_capacity(2 * n + 1024)
     lib_stream = torch.cuda.ExternalStream(alg.stream_handle())
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
@@ -687,6 +689,8 @@ def run_powerlaw(args):
     alg = gz.CCSketchAlg(V, cfg["sketch_seed"])
     if args.host_rounds:
         alg.set_query_graph(False)
+    if args.pipeline is not None:
+        alg.set_pipeline(args.pipeline)
     alg.set_gutter_capacity(2 * int(cuts[1] - cuts[0]) + 1024)
     base = d_rec.data_ptr()
 
@@ -781,6 +785,9 @@ def main():
     ap.add_argument("--small", action="store_true",
                     help="profiling sizes: dense V=2^14, powerlaw V=2^18")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--pipeline", type=int, default=None, choices=[-1, 0, 1],
+                    help="sketch-update kernel: 1 two-buffer pipeline, 0 one tile at a time, "
+                         "-1 the handle's choice (default)")
     ap.add_argument("--host-rounds", action="store_true",
                     help="queries with the Boruvka round loop on the host (profilers cannot see "
                          "kernels inside the conditional query graph)")

@@ -95,6 +95,7 @@ SIGNATURES = [
     ("gz_set_tuning", _i, [_H, _u32, _u32, _u32, _u32]),
     ("gz_set_direct_factor", _i, [_H, ctypes.c_double]),
     ("gz_set_query_graph", _i, [_H, _i]),
+    ("gz_set_pipeline", _i, [_H, _i]),
     ("gz_set_eager_dsu", _i, [_H, _i]),
     ("gz_ingest_records_noalloc", _i, [_P, _u32, _u64, _d, _P, _sz, _P]),
     ("gz_batch_create", _i, [_u32, _P, _P, _d, _P, ctypes.POINTER(_H)]),

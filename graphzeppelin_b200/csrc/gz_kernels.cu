@@ -596,6 +596,140 @@ k_sketch_update(SketchGeom g, uint8_t *__restrict__ sketches, const uint8_t *__r
   if (threadIdx.x == 0) bulk_wait_all();
 }
 
+// Two-buffer variant of k_sketch_update for tiles of one bin each and plain CameoSketch entries
+// (large graphs, where a tile's sketches dwarf its entries and staging dominates): the last
+// warp's lane 0 claims tile k + 1 and bulk-loads it into one buffer, and writes tile k - 1 back,
+// while the other 31 warps XOR tile k's entries into the other buffer. Buffers change hands
+// through full/empty mbarriers (bounded waits), so loads and write-backs overlap the hashing.
+// A tile with fewer entries than g.direct_max is updated in place in HBM without staging.
+struct PipeSlot {
+  uint32_t t, total, direct;
+};
+
+__global__ void __launch_bounds__(1024, 1)
+k_sketch_update_pipe(SketchGeom g, uint8_t *__restrict__ sketches, const uint8_t *__restrict__ gutter,
+                     ChunkTable chunks, const uint32_t *__restrict__ bin_off, int nchunks,
+                     const uint64_t *__restrict__ flip, uint32_t *work_counter, uint32_t *status) {
+  extern __shared__ __align__(128) uint8_t dsm[];
+  __shared__ __align__(8) uint64_t s_full[2], s_empty[2];
+  __shared__ PipeSlot s_slot[2];
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t ncw = (blockDim.x >> 5) - 1, nct = ncw * 32;
+  const uint32_t vpt = 1u << g.tile_shift;
+  const uint32_t tile_bytes = vpt * g.sketch_words * 4;
+  uint64_t *s_flip = reinterpret_cast<uint64_t *>(dsm + 2 * (size_t)tile_bytes);
+  for (uint32_t i = threadIdx.x; i <= g.C; i += blockDim.x) s_flip[i] = flip[i];
+  if (threadIdx.x == 0) {
+    mbar_init(smem_u32(&s_full[0]), 1);
+    mbar_init(smem_u32(&s_full[1]), 1);
+    mbar_init(smem_u32(&s_empty[0]), nct);
+    mbar_init(smem_u32(&s_empty[1]), nct);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  const uint32_t stride = g.nbins + 1;
+
+  if (warp == ncw) {  // ---------------- producer ----------------
+    if (lane != 0) return;
+    auto claim = [&]() {
+      PipeSlot c;
+      c.t = atomicAdd(work_counter, 1u);
+      c.total = 0;
+      c.direct = 0;
+      if (c.t < g.ntiles) {
+        for (int k = 0; k < nchunks; ++k)
+          c.total += bin_off[(uint64_t)k * stride + c.t + 1] - bin_off[(uint64_t)k * stride + c.t];
+        c.direct = c.total < g.direct_max;
+      }
+      return c;
+    };
+    uint8_t *pdst[2] = {nullptr, nullptr};  // where a staged buffer goes back
+    uint32_t issued = 0, lastk[2] = {0, 0};
+    uint32_t k = 0;
+    bool ok = true;
+    PipeSlot c = claim();
+    for (;; ++k) {
+      const uint32_t s = k & 1;
+      if (k >= 2) {  // consumers must be done with tile k - 2 (same buffer) before reuse
+        if (!mbar_wait_bounded(smem_u32(&s_empty[s]), ((k - 2) >> 1) & 1, kWaitLimitNs)) {
+          ok = false;
+          break;
+        }
+        if (pdst[s]) {
+          for (uint32_t off = 0; off < tile_bytes; off += kBulkPiece)
+            bulk_s2g(pdst[s] + off, smem_u32(dsm + (size_t)s * tile_bytes) + off, min(kBulkPiece, tile_bytes - off));
+          bulk_commit();
+          bulk_wait_read_all();
+        }
+      }
+      s_slot[s] = c;
+      const uint32_t full = smem_u32(&s_full[s]);
+      const bool stage = c.t < g.ntiles && c.total && !c.direct;
+      pdst[s] = stage ? sketches + (uint64_t)c.t * tile_bytes : nullptr;
+      if (stage) {
+        mbar_expect_tx(full, tile_bytes);
+        for (uint32_t off = 0; off < tile_bytes; off += kBulkPiece)
+          bulk_g2s(smem_u32(dsm + (size_t)s * tile_bytes) + off, pdst[s] + off, min(kBulkPiece, tile_bytes - off), full);
+        issued |= 1u << s;
+        lastk[s] = k;
+      } else {
+        mbar_arrive(full);  // in place, empty, or the end of the work: hand over at once
+      }
+      if (c.t >= g.ntiles) break;
+      c = claim();  // the next tile's counts are read while this tile loads
+    }
+    if (ok && k >= 1) {  // write back the last tile
+      const uint32_t s = (k - 1) & 1;
+      ok = mbar_wait_bounded(smem_u32(&s_empty[s]), ((k - 1) >> 1) & 1, kWaitLimitNs);
+      if (ok && pdst[s]) {
+        for (uint32_t off = 0; off < tile_bytes; off += kBulkPiece)
+          bulk_s2g(pdst[s] + off, smem_u32(dsm + (size_t)s * tile_bytes) + off, min(kBulkPiece, tile_bytes - off));
+        bulk_commit();
+      }
+    }
+    if (!ok) {
+      atomicOr(status, kStatusTimeout);
+      // every load issued must land before the CTA's shared memory goes away
+      for (uint32_t s = 0; s < 2; ++s)
+        if (issued & (1u << s)) mbar_wait_bounded(smem_u32(&s_full[s]), (lastk[s] >> 1) & 1, kWaitLimitNs);
+    }
+    bulk_wait_all();
+    return;
+  }
+
+  // ---------------- consumers ----------------
+  const uint64_t flip_chk = s_flip[g.C];
+  const uint32_t ct = threadIdx.x;
+  for (uint32_t k = 0;; ++k) {
+    const uint32_t s = k & 1;
+    if (!mbar_wait_bounded(smem_u32(&s_full[s]), (k >> 1) & 1, kWaitLimitNs)) {
+      if (lane == 0) atomicOr(status, kStatusTimeout);
+      return;
+    }
+    const PipeSlot m = s_slot[s];
+    if (m.t >= g.ntiles) return;
+    if (m.total) {
+      uint32_t *s_sk = reinterpret_cast<uint32_t *>(dsm + (size_t)s * tile_bytes);
+      uint32_t *gsk = reinterpret_cast<uint32_t *>(sketches);
+      for (int c = 0; c < nchunks; ++c) {
+        const uint2 *E = reinterpret_cast<const uint2 *>(gutter + chunks.base[c]);
+        const uint32_t b = bin_off[(uint64_t)c * stride + m.t], e = bin_off[(uint64_t)c * stride + m.t + 1];
+        // the next entry's load is in flight while the current one is hashed
+        uint32_t i = b + ct;
+        uint2 cur = i < e ? E[i] : make_uint2(0, 0);
+        for (; i < e; i += nct) {
+          const uint2 x = cur;
+          if (i + nct < e) cur = E[i + nct];
+          if (m.direct) apply_entry_global(x, gsk, g.sketch_words, s_flip, flip_chk, g.C, g.B);
+          else apply_entry(x, s_sk, vpt - 1, g.sketch_words, s_flip, flip_chk, g.C, g.B);
+        }
+      }
+      fence_proxy_async_smem();  // this thread's bucket writes, before the bulk write-back
+    }
+    mbar_arrive(smem_u32(&s_empty[s]));
+  }
+}
+
 template <int INPUT, bool CUBE>
 __global__ void __launch_bounds__(512)
 k_in_place(const void *__restrict__ in, uint64_t n, SketchGeom g, uint32_t *__restrict__ sk_words,
@@ -1369,6 +1503,23 @@ cudaError_t sketch_update(SketchGeom g, uint8_t *sketches, const uint8_t *gutter
   if (e != cudaSuccess) return e;
   kern<<<grid, threads, smem, s>>>(g, sketches, gutter, chunks, bin_off, nchunks, flip,
                                    work_counter, status);
+  g_launches++;
+  return cudaGetLastError();
+}
+
+size_t sketch_update_pipe_smem_bytes(SketchGeom g) {
+  return 2 * ((size_t)g.sketch_words * 4 << g.tile_shift) + (((size_t)g.C + 2) & ~(size_t)1) * 8;
+}
+
+cudaError_t sketch_update_pipe(SketchGeom g, uint8_t *sketches, const uint8_t *gutter,
+                               const ChunkTable &chunks, const uint32_t *bin_off, int nchunks,
+                               const uint64_t *flip, uint32_t *work_counter, uint32_t *status,
+                               int grid, cudaStream_t s) {
+  const size_t smem = sketch_update_pipe_smem_bytes(g);
+  cudaError_t e = cudaFuncSetAttribute(k_sketch_update_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  k_sketch_update_pipe<<<grid, 1024, smem, s>>>(g, sketches, gutter, chunks, bin_off, nchunks, flip,
+                                                work_counter, status);
   g_launches++;
   return cudaGetLastError();
 }

@@ -118,6 +118,13 @@ int sketch_update_ctas_per_sm(SketchGeom g, int threads);
 // Applies every buffered entry of `nchunks` chunks: for each tile whose bin has entries, stage
 // its sketches in shared memory with bulk async copies, XOR in the bin entries that belong to
 // the tile, write the tile back.
+// Two-buffer tile pipeline (one tile per bin, plain CameoSketch entries only): 1024 threads
+// (31 consumer warps + a producer warp), one CTA per SM.
+size_t sketch_update_pipe_smem_bytes(SketchGeom g);
+cudaError_t sketch_update_pipe(SketchGeom g, uint8_t *sketches, const uint8_t *gutter,
+                               const ChunkTable &chunks, const uint32_t *bin_off, int nchunks,
+                               const uint64_t *flip, uint32_t *work_counter, uint32_t *status,
+                               int grid, cudaStream_t s);
 cudaError_t sketch_update(SketchGeom g, uint8_t *sketches, const uint8_t *gutter,
                           const ChunkTable &chunks, const uint32_t *bin_off, int nchunks,
                           const uint64_t *flip, uint32_t *work_counter, uint32_t *status,

@@ -299,6 +299,11 @@ GZ_API int gz_set_direct_factor(gz_alg_t *alg, double factor);
  * (a synchronize per round; ticket submits then wait for their query): for profilers that do
  * not see kernels inside conditional graphs. Answers are the same either way. */
 GZ_API int gz_set_query_graph(gz_alg_t *alg, int enable);
+/* Sketch-update kernel of a handle: mode 1 = the two-buffer pipeline (a producer warp loads the
+ * next tile's sketches and writes the previous one back while the other warps hash; one tile per
+ * gutter bin; CameoSketch with plain entries only, ignored otherwise), 0 = one staged tile per
+ * CTA at a time, -1 = chosen by the handle (the default). Re-picks the default tiling. */
+GZ_API int gz_set_pipeline(gz_alg_t *alg, int mode);
 
 /* ---- many graphs on one GPU ------------------------------------------------------------------
  * A gz_batch_t holds num_graphs independent CCSketchAlg instances (each its own V, seed and

@@ -158,6 +158,31 @@ def test_direct_route_bit_exact(gz, oracle_mod, vpt, factor):
     assert (canonical(cc.parent_arr) == labels).all()
 
 
+@pytest.mark.parametrize("name", ["c0_v1024", "cl_v2048", "mult_v1024"])
+def test_pipelined_sketch_update_bit_exact(gz, oracle_mod, name):
+    """The two-buffer sketch-update kernel (gz_set_pipeline(1)): staged tiles, in-place tiles
+    of a sparse launch, several gutter chunks per launch; bytes and answer as the reference's."""
+    c, st, labels, _ = load_case(name)
+    V, seed = c["num_vertices"], c["seed"]
+    alg = _alg(gz, V, seed, c["sketches_factor"])
+    alg.set_pipeline(1)
+    assert alg.params.vertices_per_bin == alg.params.vertices_per_tile
+    alg.set_gutter_capacity(4096)  # many chunks per launch
+    rec = st.records
+    half = len(rec) // 2
+    alg.ingest_records(rec[:half])
+    alg.flush()
+    alg.ingest_records(rec[half:half + 300])  # a sparse launch: tiles go in place
+    alg.flush()
+    alg.ingest_records(rec[half + 300:])
+    osk = oracle_mod.OracleSketches(V, seed, c["sketches_factor"])
+    osk.apply_records(st.raw())
+    assert (alg.dump_sketches() == osk.data).all()
+    cc = alg.connected_components()
+    assert cc.size() == c["num_cc"]
+    assert (canonical(cc.parent_arr) == labels).all()
+
+
 def test_queries_during_stream(gz, oracle_mod):
     """TestQueryDuringStream / MTStreamWithMultipleQueries: 10 queries at stream breakpoints."""
     c, st, _, _ = load_case("c0_v1024")
