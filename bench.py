@@ -785,9 +785,9 @@ def main():
     ap.add_argument("--small", action="store_true",
                     help="profiling sizes: dense V=2^14, powerlaw V=2^18")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--pipeline", type=int, default=None, choices=[-1, 0, 1],
-                    help="sketch-update kernel: 1 two-buffer pipeline, 0 one tile at a time, "
-                         "-1 the handle's choice (default)")
+    ap.add_argument("--pipeline", type=int, default=None, choices=[-1, 0, 1, 2, 3, 4],
+                    help="sketch-update kernel: 1 tile pipeline (2..4: with that many buffers), "
+                         "0 one tile at a time, -1 the handle's choice (default)")
     ap.add_argument("--host-rounds", action="store_true",
                     help="queries with the Boruvka round loop on the host (profilers cannot see "
                          "kernels inside the conditional query graph)")

@@ -488,8 +488,9 @@ class CCSketchAlg:
         _check(self.lib.gz_set_direct_factor(self._h, float(factor)))
 
     def set_pipeline(self, mode: int = -1) -> None:
-        """Sketch-update kernel: 1 two-buffer pipeline, 0 one staged tile at a time, -1 the
-        handle's choice (gz_set_pipeline). Re-picks the default tiling."""
+        """Sketch-update kernel: 1 tile pipeline (2..4: with that many tile buffers), 0 one
+        staged tile at a time, -1 the handle's choice (gz_set_pipeline). Re-picks the default
+        tiling."""
         _check(self.lib.gz_set_pipeline(self._h, int(mode)))
         p = _lib.gz_params_t()
         _check(self.lib.gz_get_params(self._h, ctypes.byref(p)))

@@ -143,8 +143,10 @@ struct gz_alg {
   uint64_t entry_cap = 0;       // capacity in endpoint updates
   uint64_t gutter_bytes = 0, gutter_used = 0, entries_pending = 0;
   double direct_factor = 1.0;   // scales the in-place threshold of sparse tiles (0 = never)
-  int pipe_mode = -1;           // two-buffer sketch update: 1 on, 0 off, -1 automatic
-  bool pipe = false;            // the two-buffer kernel is the one in use
+  int pipe_mode = -1;           // pipelined sketch update: 1 on, 2..4 on with that many buffers,
+                                // 0 off, -1 automatic
+  bool pipe = false;            // the pipelined kernel is the one in use
+  uint32_t nbuf = 2;            // its tile buffers
   // every update so far reached both endpoints' sketches (records, gz_update): the XOR of all
   // vertex sketches is zero, which lets a query merge its largest component from the rest
   bool symmetric = true;
@@ -232,6 +234,7 @@ struct gz_alg {
     g.bin_shift = bin_shift;
     g.nbins = nbins;
     g.cube = cube ? 1 : 0;
+    g.nbuf = nbuf;
     // Staging a tile moves its sketches twice (bulk load + write-back); updating it in place
     // costs about C + 1 bucket sectors read and written per entry. Below the break-even entry
     // count a tile goes in place (one tile per bin and plain CameoSketch entries only).
@@ -312,8 +315,10 @@ constexpr uint32_t kMaxTilesPerBin = 16;
 // per bin anyway, so overlapping a tile's load and write-back with the hashing pays (measured at
 // 2^20 vertices: 6.1 -> 5.5 ms per 1.3e7 records). Below, the one-tile kernel keeps its larger
 // tiles and coarser bins (2^17 vertices: 17.6 ms ingest against 25.8 ms pipelined).
+constexpr uint32_t kPipeBuffers = 2;  // default tile buffers of the pipelined kernel
+
 bool want_pipe(const gz_alg *h) {
-  if (h->pipe_mode >= 0) return h->pipe_mode == 1;
+  if (h->pipe_mode >= 0) return h->pipe_mode >= 1;
   return h->V > (1u << 18);
 }
 
@@ -349,11 +354,15 @@ int choose_tiling(gz_alg *h, uint32_t vpt_req, uint32_t threads_req, uint32_t tp
   h->pipe = false;
   if (!h->in_place && !h->hashed && !h->cube && !tpb_req && want_pipe(h)) {
     const size_t room = (size_t)smem_optin - 1024 - (((size_t)h->C + 2) & ~(size_t)1) * 8;
-    uint32_t ps = vpt_req ? shift : 6;
-    while (ps > 2 && 2 * (h->sketch_bytes << ps) > room) --ps;
-    if (2 * (h->sketch_bytes << ps) <= room) {
-      h->pipe = true;
-      shift = ps;
+    // the most buffers asked for (or kPipeBuffers) that hold tiles of at least 4 vertices
+    for (uint32_t nb = h->pipe_mode >= 2 ? (uint32_t)h->pipe_mode : kPipeBuffers; nb >= 2 && !h->pipe; --nb) {
+      uint32_t ps = vpt_req ? shift : 6;
+      while (ps > 2 && nb * (h->sketch_bytes << ps) > room) --ps;
+      if (nb * (h->sketch_bytes << ps) <= room) {
+        h->pipe = true;
+        h->nbuf = nb;
+        shift = ps;
+      }
     }
   }
   h->tile_shift = shift;
@@ -1444,7 +1453,7 @@ int gz_get_trace(gz_alg_t *h, gz_trace_rec_t *out, size_t cap, size_t *len) {
 }
 
 int gz_set_pipeline(gz_alg_t *h, int mode) {
-  if (!h || mode < -1 || mode > 1) return fail(GZ_ERR_INVALID, "mode must be -1, 0 or 1");
+  if (!h || mode < -1 || mode > 4) return fail(GZ_ERR_INVALID, "mode must be -1 .. 4");
   {
     Guard g(h);
     h->pipe_mode = mode;

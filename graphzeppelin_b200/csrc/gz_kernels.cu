@@ -596,34 +596,37 @@ k_sketch_update(SketchGeom g, uint8_t *__restrict__ sketches, const uint8_t *__r
   if (threadIdx.x == 0) bulk_wait_all();
 }
 
-// Two-buffer variant of k_sketch_update for tiles of one bin each and plain CameoSketch entries
-// (large graphs, where a tile's sketches dwarf its entries and staging dominates): the last
-// warp's lane 0 claims tile k + 1 and bulk-loads it into one buffer, and writes tile k - 1 back,
-// while the other 31 warps XOR tile k's entries into the other buffer. Buffers change hands
-// through full/empty mbarriers (bounded waits), so loads and write-backs overlap the hashing.
-// A tile with fewer entries than g.direct_max is updated in place in HBM without staging.
+// Pipelined variant of k_sketch_update for tiles of one bin each and plain CameoSketch entries
+// (large graphs, where a tile's sketches dwarf its entries and staging dominates): a ring of
+// g.nbuf tile buffers. The last warp's lane 0 claims tiles, bulk-loads them up to nbuf - 1 ahead
+// and writes finished ones back, while the other 31 warps XOR each tile's entries into its
+// buffer. Buffers change hands through full/empty mbarriers (bounded waits), so loads and
+// write-backs of several tiles overlap the hashing. A tile with fewer entries than g.direct_max
+// is updated in place in HBM without staging.
 struct PipeSlot {
   uint32_t t, total, direct;
 };
+constexpr uint32_t kPipeMaxBuf = 4;
 
 __global__ void __launch_bounds__(1024, 1)
 k_sketch_update_pipe(SketchGeom g, uint8_t *__restrict__ sketches, const uint8_t *__restrict__ gutter,
                      ChunkTable chunks, const uint32_t *__restrict__ bin_off, int nchunks,
                      const uint64_t *__restrict__ flip, uint32_t *work_counter, uint32_t *status) {
   extern __shared__ __align__(128) uint8_t dsm[];
-  __shared__ __align__(8) uint64_t s_full[2], s_empty[2];
-  __shared__ PipeSlot s_slot[2];
+  __shared__ __align__(8) uint64_t s_full[kPipeMaxBuf], s_empty[kPipeMaxBuf];
+  __shared__ PipeSlot s_slot[kPipeMaxBuf];
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t ncw = (blockDim.x >> 5) - 1, nct = ncw * 32;
+  const uint32_t nbuf = g.nbuf;
   const uint32_t vpt = 1u << g.tile_shift;
   const uint32_t tile_bytes = vpt * g.sketch_words * 4;
-  uint64_t *s_flip = reinterpret_cast<uint64_t *>(dsm + 2 * (size_t)tile_bytes);
+  uint64_t *s_flip = reinterpret_cast<uint64_t *>(dsm + (size_t)nbuf * tile_bytes);
   for (uint32_t i = threadIdx.x; i <= g.C; i += blockDim.x) s_flip[i] = flip[i];
   if (threadIdx.x == 0) {
-    mbar_init(smem_u32(&s_full[0]), 1);
-    mbar_init(smem_u32(&s_full[1]), 1);
-    mbar_init(smem_u32(&s_empty[0]), nct);
-    mbar_init(smem_u32(&s_empty[1]), nct);
+    for (uint32_t i = 0; i < nbuf; ++i) {
+      mbar_init(smem_u32(&s_full[i]), 1);
+      mbar_init(smem_u32(&s_empty[i]), nct);
+    }
     mbar_fence_init();
   }
   __syncthreads();
@@ -643,15 +646,15 @@ k_sketch_update_pipe(SketchGeom g, uint8_t *__restrict__ sketches, const uint8_t
       }
       return c;
     };
-    uint8_t *pdst[2] = {nullptr, nullptr};  // where a staged buffer goes back
-    uint32_t issued = 0, lastk[2] = {0, 0};
+    uint8_t *pdst[kPipeMaxBuf] = {nullptr, nullptr, nullptr, nullptr};  // where a staged buffer goes back
+    uint32_t issued = 0, lastk[kPipeMaxBuf] = {0, 0, 0, 0};
     uint32_t k = 0;
     bool ok = true;
     PipeSlot c = claim();
     for (;; ++k) {
-      const uint32_t s = k & 1;
-      if (k >= 2) {  // consumers must be done with tile k - 2 (same buffer) before reuse
-        if (!mbar_wait_bounded(smem_u32(&s_empty[s]), ((k - 2) >> 1) & 1, kWaitLimitNs)) {
+      const uint32_t s = k % nbuf;
+      if (k >= nbuf) {  // consumers must be done with tile k - nbuf (same buffer) before reuse
+        if (!mbar_wait_bounded(smem_u32(&s_empty[s]), ((k - nbuf) / nbuf) & 1, kWaitLimitNs)) {
           ok = false;
           break;
         }
@@ -678,20 +681,23 @@ k_sketch_update_pipe(SketchGeom g, uint8_t *__restrict__ sketches, const uint8_t
       if (c.t >= g.ntiles) break;
       c = claim();  // the next tile's counts are read while this tile loads
     }
-    if (ok && k >= 1) {  // write back the last tile
-      const uint32_t s = (k - 1) & 1;
-      ok = mbar_wait_bounded(smem_u32(&s_empty[s]), ((k - 1) >> 1) & 1, kWaitLimitNs);
-      if (ok && pdst[s]) {
-        for (uint32_t off = 0; off < tile_bytes; off += kBulkPiece)
-          bulk_s2g(pdst[s] + off, smem_u32(dsm + (size_t)s * tile_bytes) + off, min(kBulkPiece, tile_bytes - off));
-        bulk_commit();
+    if (ok) {  // write back the tiles still in the ring, oldest first
+      const uint32_t first = k + 1 > nbuf ? k + 1 - nbuf : 0;
+      for (uint32_t j = first; j < k && ok; ++j) {
+        const uint32_t s = j % nbuf;
+        ok = mbar_wait_bounded(smem_u32(&s_empty[s]), (j / nbuf) & 1, kWaitLimitNs);
+        if (ok && pdst[s]) {
+          for (uint32_t off = 0; off < tile_bytes; off += kBulkPiece)
+            bulk_s2g(pdst[s] + off, smem_u32(dsm + (size_t)s * tile_bytes) + off, min(kBulkPiece, tile_bytes - off));
+          bulk_commit();
+        }
       }
     }
     if (!ok) {
       atomicOr(status, kStatusTimeout);
       // every load issued must land before the CTA's shared memory goes away
-      for (uint32_t s = 0; s < 2; ++s)
-        if (issued & (1u << s)) mbar_wait_bounded(smem_u32(&s_full[s]), (lastk[s] >> 1) & 1, kWaitLimitNs);
+      for (uint32_t s = 0; s < nbuf; ++s)
+        if (issued & (1u << s)) mbar_wait_bounded(smem_u32(&s_full[s]), (lastk[s] / nbuf) & 1, kWaitLimitNs);
     }
     bulk_wait_all();
     return;
@@ -701,8 +707,8 @@ k_sketch_update_pipe(SketchGeom g, uint8_t *__restrict__ sketches, const uint8_t
   const uint64_t flip_chk = s_flip[g.C];
   const uint32_t ct = threadIdx.x;
   for (uint32_t k = 0;; ++k) {
-    const uint32_t s = k & 1;
-    if (!mbar_wait_bounded(smem_u32(&s_full[s]), (k >> 1) & 1, kWaitLimitNs)) {
+    const uint32_t s = k % nbuf;
+    if (!mbar_wait_bounded(smem_u32(&s_full[s]), (k / nbuf) & 1, kWaitLimitNs)) {
       if (lane == 0) atomicOr(status, kStatusTimeout);
       return;
     }
@@ -1508,7 +1514,7 @@ cudaError_t sketch_update(SketchGeom g, uint8_t *sketches, const uint8_t *gutter
 }
 
 size_t sketch_update_pipe_smem_bytes(SketchGeom g) {
-  return 2 * ((size_t)g.sketch_words * 4 << g.tile_shift) + (((size_t)g.C + 2) & ~(size_t)1) * 8;
+  return (size_t)g.nbuf * ((size_t)g.sketch_words * 4 << g.tile_shift) + (((size_t)g.C + 2) & ~(size_t)1) * 8;
 }
 
 cudaError_t sketch_update_pipe(SketchGeom g, uint8_t *sketches, const uint8_t *gutter,

@@ -53,6 +53,7 @@ struct SketchGeom {
   uint32_t cube = 0;           // CubeSketch update rule (every depth 0..d) instead of CameoSketch
   uint32_t direct_max = 0;     // one tile per bin only: a tile with fewer plain entries than this
                                // is updated in place in HBM (global atomics) instead of staged
+  uint32_t nbuf = 2;           // tile buffers of the pipelined kernel (2..4)
 };
 
 // Records per staging tile of the gutter kernels, and the largest bin count for which the
@@ -118,7 +119,7 @@ int sketch_update_ctas_per_sm(SketchGeom g, int threads);
 // Applies every buffered entry of `nchunks` chunks: for each tile whose bin has entries, stage
 // its sketches in shared memory with bulk async copies, XOR in the bin entries that belong to
 // the tile, write the tile back.
-// Two-buffer tile pipeline (one tile per bin, plain CameoSketch entries only): 1024 threads
+// Tile pipeline with g.nbuf buffers (one tile per bin, plain CameoSketch entries only): 1024 threads
 // (31 consumer warps + a producer warp), one CTA per SM.
 size_t sketch_update_pipe_smem_bytes(SketchGeom g);
 cudaError_t sketch_update_pipe(SketchGeom g, uint8_t *sketches, const uint8_t *gutter,

@@ -299,10 +299,11 @@ GZ_API int gz_set_direct_factor(gz_alg_t *alg, double factor);
  * (a synchronize per round; ticket submits then wait for their query): for profilers that do
  * not see kernels inside conditional graphs. Answers are the same either way. */
 GZ_API int gz_set_query_graph(gz_alg_t *alg, int enable);
-/* Sketch-update kernel of a handle: mode 1 = the two-buffer pipeline (a producer warp loads the
- * next tile's sketches and writes the previous one back while the other warps hash; one tile per
- * gutter bin; CameoSketch with plain entries only, ignored otherwise), 0 = one staged tile per
- * CTA at a time, -1 = chosen by the handle (the default). Re-picks the default tiling. */
+/* Sketch-update kernel of a handle: mode 1 = the tile pipeline (a producer warp loads the next
+ * tiles' sketches and writes finished ones back while the other warps hash; one tile per gutter
+ * bin; CameoSketch with plain entries only, ignored otherwise), 2..4 = the pipeline with that
+ * many tile buffers, 0 = one staged tile per CTA at a time, -1 = chosen by the handle (the
+ * default). Re-picks the default tiling. */
 GZ_API int gz_set_pipeline(gz_alg_t *alg, int mode);
 
 /* ---- many graphs on one GPU ------------------------------------------------------------------

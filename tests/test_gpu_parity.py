@@ -158,14 +158,16 @@ def test_direct_route_bit_exact(gz, oracle_mod, vpt, factor):
     assert (canonical(cc.parent_arr) == labels).all()
 
 
+@pytest.mark.parametrize("mode", [1, 3, 4])
 @pytest.mark.parametrize("name", ["c0_v1024", "cl_v2048", "mult_v1024"])
-def test_pipelined_sketch_update_bit_exact(gz, oracle_mod, name):
-    """The two-buffer sketch-update kernel (gz_set_pipeline(1)): staged tiles, in-place tiles
-    of a sparse launch, several gutter chunks per launch; bytes and answer as the reference's."""
+def test_pipelined_sketch_update_bit_exact(gz, oracle_mod, name, mode):
+    """The pipelined sketch-update kernel (gz_set_pipeline: default, 3 and 4 tile buffers):
+    staged tiles, in-place tiles of a sparse launch, several gutter chunks per launch; bytes and
+    answer as the reference's."""
     c, st, labels, _ = load_case(name)
     V, seed = c["num_vertices"], c["seed"]
     alg = _alg(gz, V, seed, c["sketches_factor"])
-    alg.set_pipeline(1)
+    alg.set_pipeline(mode)
     assert alg.params.vertices_per_bin == alg.params.vertices_per_tile
     alg.set_gutter_capacity(4096)  # many chunks per launch
     rec = st.records
