@@ -595,9 +595,9 @@ def run_serving(args):
     budget = SERVING["budget_bytes"]
     kw = dict(snapshot_bytes=SERVING["snapshot_bytes"])
     arms = {}
-    # warm-up (untimed): a short trace of its own through both paths, so that module loading,
+    # warm-up (untimed): a 200-tenant trace of its own through both paths, so that module loading,
     # first allocations and pinned staging of this process are not charged to the measured replays
-    warm = SV.serving_trace(40, SERVING["trace_seed"] + 1000)
+    warm = SV.serving_trace(200, SERVING["trace_seed"] + 1000)
     for mode in ("batched", "plain"):
         if mode == "plain" and args.no_plain:
             continue
@@ -635,7 +635,7 @@ def run_serving(args):
                    "budget_bytes": budget, "snapshot_bytes": SERVING["snapshot_bytes"],
                    "trace_seconds": float(tr.time[-1]), "time_scale": args.time_scale},
         "timing": "wall clock of the replay loop (host + GPU), from the first release to the "
-                  "last answer, after an untimed 40-tenant warm-up replay",
+                  "last answer, after an untimed 200-tenant warm-up replay",
         "batched": {"saturated": sat, "paced": paced},
         "plain_per_tenant": ({"saturated": arms["plain"]["saturated"].summary(),
                               "paced": arms["plain"]["paced"].summary()} if "plain" in arms else None),

@@ -123,6 +123,7 @@ SIGNATURES = [
     ("gz_server_ingest_segments", _i, [_H, _u32, _P, _P, _P]),
     ("gz_server_query_submit", _i, [_H, _u32, _P, ctypes.POINTER(_u64)]),
     ("gz_server_query_wait", _i, [_H, _u64, _P, _P, _P, _P]),
+    ("gz_server_query_ready", _i, [_H, _u64, ctypes.POINTER(_i)]),
     ("gz_server_dump_sketches", _i, [_H, _u32, _P, _sz]),
     ("gz_server_write_binary", _i, [_H, _u32, ctypes.c_char_p]),
     ("gz_server_admit_serialized", _i, [_H, ctypes.c_char_p, ctypes.POINTER(_u32)]),

@@ -2417,6 +2417,15 @@ int gz_server_query_submit(gz_server_t *s, uint32_t n, const uint32_t *ids, uint
 // Waits for a submitted query. labels_out (NULL or the sum of the tenants' V, in submission
 // order) gets each vertex's tenant-local root; num_cc, rounds and status (NULL or one per tenant)
 // as gz_batch_connected_components.
+int gz_server_query_ready(gz_server_t *s, uint64_t ticket, int *ready) {
+  if (!s || !ready) return mb_fail(GZ_ERR_INVALID, "null argument");
+  std::lock_guard<std::mutex> ql(s->qmtx);
+  auto it = s->jobs.find(ticket);
+  if (it == s->jobs.end()) return mb_fail(GZ_ERR_INVALID, "unknown ticket");
+  *ready = it->second->done ? 1 : 0;
+  return GZ_OK;
+}
+
 int gz_server_query_wait(gz_server_t *s, uint64_t ticket, uint32_t *labels_out, uint32_t *num_cc,
                          uint32_t *rounds, int *status) {
   if (!s) return mb_fail(GZ_ERR_INVALID, "null handle");

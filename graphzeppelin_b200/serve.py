@@ -130,6 +130,12 @@ class SketchServer:
         _check(self.lib.gz_server_query_submit(self._h, ids.size, _ptr(ids), ctypes.byref(t)))
         return int(t.value)
 
+    def query_ready(self, ticket: int) -> bool:
+        """Whether query_wait(ticket, ...) would return at once (gz_server_query_ready)."""
+        out = ctypes.c_int()
+        _check(self.lib.gz_server_query_ready(self._h, int(ticket), ctypes.byref(out)))
+        return bool(out.value)
+
     def query_wait(self, ticket: int, tenants: Sequence[int]):
         """Per tenant (labels, num_cc, rounds, status) of a submitted query."""
         sizes = [self.num_vertices[t] for t in tenants]
@@ -469,7 +475,7 @@ def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes:
                     if nxt >= N and not resident and not waiting:
                         break
                     if nxt < N:
-                        time.sleep(max(0.0, min(0.002, (trace.time[nxt] - tnow) / time_scale)))
+                        time.sleep(max(0.0, min(0.0005, (trace.time[nxt] - tnow) / time_scale)))
                     continue
                 i, t = best
                 pending[t].popleft()
@@ -488,7 +494,12 @@ def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes:
                     u, v = trace.point[i]
                     finish(i, t, (bool(a.point_query(int(u), int(v))),))
                 continue
-            # batched: one tick
+            # batched: one tick. Answers of earlier ticks that are ready already go out first.
+            if inflight:
+                ready = [job for job in inflight if server.query_ready(job[0])]
+                if ready:
+                    collect(ready)
+                    inflight = [job for job in inflight if job not in ready]
             ing_t, ing_seg, ing_req = [], [], []
             qreq = []
             budget_left = max_tick_updates
@@ -517,7 +528,7 @@ def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes:
                 if nxt >= N and not resident and not waiting:
                     break
                 if nxt < N:
-                    time.sleep(max(0.0, min(0.002, (trace.time[nxt] - tnow) / time_scale)))
+                    time.sleep(max(0.0, min(0.0005, (trace.time[nxt] - tnow) / time_scale)))
                 continue
             res.ticks += 1
             if ing_t:

@@ -403,6 +403,8 @@ GZ_API int gz_server_ingest_segments(gz_server_t *server, uint32_t num_segments,
                                      const uint64_t *counts);
 GZ_API int gz_server_query_submit(gz_server_t *server, uint32_t n, const uint32_t *tenants,
                                   uint64_t *ticket);
+/* Whether a submitted query's answer is ready (gz_server_query_wait would not block). */
+GZ_API int gz_server_query_ready(gz_server_t *server, uint64_t ticket, int *ready);
 /* Waits for a submitted query: labels_out (NULL or the sum of the tenants' V, in submission
  * order) gets each vertex's tenant-local root; num_cc, rounds, status (NULL or n entries) as
  * gz_batch_connected_components. */
