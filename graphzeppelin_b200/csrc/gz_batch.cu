@@ -1627,7 +1627,7 @@ int gz_batch_create(uint32_t num_graphs, const uint32_t *num_vertices, const uin
   if (rc != GZ_OK) return bail(rc);
   cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) return bail(mb_fail(GZ_ERR_CUDA, cudaGetErrorString(e)));
-  if ((rc = mb_alloc(&h->d_sk, h->sk_bytes)) || (rc = mb_alloc(&h->d_status, 4)) ||
+  if ((rc = mb_alloc(&h->d_sk, h->sk_bytes + kSketchTail)) || (rc = mb_alloc(&h->d_status, 4)) ||
       (rc = mb_alloc(&h->d_total, 1)))
     return bail(rc);
   uint64_t nflip = 0;
@@ -2141,7 +2141,8 @@ int gz_server_create(uint64_t budget_bytes, uint64_t snapshot_bytes, double sket
   s->factor = sketches_factor > 0 ? sketches_factor : 1;
   s->budget = (budget_bytes + 255) & ~255ull;
   int rc;
-  if ((rc = mb_alloc(&s->arena, s->budget)) || (rc = mb_alloc(&s->snap, (snapshot_bytes + 255) & ~255ull)))
+  if ((rc = mb_alloc(&s->arena, s->budget + kSketchTail)) ||
+      (rc = mb_alloc(&s->snap, ((snapshot_bytes + 255) & ~255ull) + kSketchTail)))
     return bail(rc);
   s->arena_alloc.init(s->budget);
   s->snap_alloc.init((snapshot_bytes + 255) & ~255ull);

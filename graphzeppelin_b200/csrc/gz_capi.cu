@@ -421,8 +421,9 @@ int init_alg(gz_alg *h, uint32_t V, uint64_t seed, double sf, double bf, bool cu
   GZ_CUDA(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
   // V rounded up to 64 so any tile size stays inside the allocation
   const uint64_t v_pad = ((uint64_t)V + 63) & ~63ull;
-  GZ_TRY(dev_alloc(&h->d_sk, v_pad * h->sketch_bytes));
-  GZ_CUDA(cudaMemsetAsync(h->d_sk, 0, v_pad * h->sketch_bytes, h->stream));
+  // + kSketchTail: the query's bulk copies read 16-byte-aligned supersets of a vertex's buckets
+  GZ_TRY(dev_alloc(&h->d_sk, v_pad * h->sketch_bytes + gz::kSketchTail));
+  GZ_CUDA(cudaMemsetAsync(h->d_sk, 0, v_pad * h->sketch_bytes + gz::kSketchTail, h->stream));
   std::vector<uint64_t> flip(h->C + 1);
   for (uint32_t c = 0; c < h->C; ++c) flip[c] = gz::xxh3_flip(seed + 5ull * c);  // column_seed
   flip[h->C] = gz::xxh3_flip(seed);                                                  // checksum_seed

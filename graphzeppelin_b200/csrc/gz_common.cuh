@@ -377,13 +377,13 @@ __device__ __forceinline__ int warp_sample_region(const uint32_t (&x)[NW], uint3
   return res;
 }
 
-// Sketch::sample of a region already in shared memory: s[0, W) the columns, s[W, W+3) the
-// deterministic bucket (same scan order as warp_sample_region).
+// Sketch::sample of a region already in shared memory: s[0, 3 * CPS * B) the columns, det[0, 3)
+// the deterministic bucket (same scan order as warp_sample_region).
 template <int CPS>
-__device__ __forceinline__ int warp_sample_smem(const uint32_t *s, uint32_t W, uint32_t B,
-                                                uint64_t flip_chk, uint64_t *idx) {
+__device__ __forceinline__ int warp_sample_smem_split(const uint32_t *s, const uint32_t *det,
+                                                      uint32_t B, uint64_t flip_chk, uint64_t *idx) {
   const uint32_t lane = threadIdx.x & 31;
-  const uint32_t d0 = s[W], d1 = s[W + 1], d2 = s[W + 2];
+  const uint32_t d0 = det[0], d1 = det[1], d2 = det[2];
   if ((d0 | d1 | d2) == 0) {
     *idx = 0;
     return 1;  // ZERO
@@ -421,6 +421,13 @@ __device__ __forceinline__ int warp_sample_smem(const uint32_t *s, uint32_t W, u
   return res;
 }
 
+// The same with the deterministic bucket right after the columns: s[W, W + 3).
+template <int CPS>
+__device__ __forceinline__ int warp_sample_smem(const uint32_t *s, uint32_t W, uint32_t B,
+                                                uint64_t flip_chk, uint64_t *idx) {
+  return warp_sample_smem_split<CPS>(s, s + W, B, flip_chk, idx);
+}
+
 // ---- asynchronous region copies (cp.async) ------------------------------------------------------
 // The query kernels keep many members' regions in flight per warp by copying them global ->
 // shared with cp.async (no registers held while a copy is outstanding), in commit groups of one
@@ -438,6 +445,26 @@ __device__ __forceinline__ void region_copy_async(uint32_t *slot, const uint32_t
                                                   const uint32_t *det, uint32_t W, uint32_t lane) {
   for (uint32_t w = lane; w < W; w += 32) cp_async4(slot + w, src + w);
   if (lane < 3) cp_async4(slot + W + lane, det + lane);
+}
+
+// ---- bulk-copied bucket runs (cp.async.bulk) -----------------------------------------------------
+// One lane moves a member's whole bucket run with one bulk copy instead of every lane issuing
+// 4-byte copies. A bulk copy needs 16-byte-aligned addresses and sizes, so the 16-byte-aligned
+// superset of the run is copied (up to 15 bytes either side, inside the sketch buffer's tail
+// padding at the end) and the run starts (p & 15) bytes into its slot.
+__host__ __device__ constexpr uint32_t bulk_run_cap(uint32_t words) {  // slot bytes for a run
+  return (words * 4 + 12 + 15) & ~15u;
+}
+__device__ __forceinline__ uint32_t bulk_run_bytes(const uint32_t *p, uint32_t words) {
+  const uintptr_t a = (uintptr_t)p & ~(uintptr_t)15, e = ((uintptr_t)(p + words) + 15) & ~(uintptr_t)15;
+  return (uint32_t)(e - a);
+}
+__device__ __forceinline__ void bulk_run_copy(uint8_t *slot, const uint32_t *p, uint32_t words, uint32_t bar) {
+  const uintptr_t a = (uintptr_t)p & ~(uintptr_t)15;
+  bulk_g2s(smem_u32(slot), reinterpret_cast<const void *>(a), bulk_run_bytes(p, words), bar);
+}
+__device__ __forceinline__ const uint32_t *bulk_run_at(const uint8_t *slot, const uint32_t *p) {
+  return reinterpret_cast<const uint32_t *>(slot + ((uintptr_t)p & 15));
 }
 
 // Warp-aggregated counter add: lanes in `active` holding the same key add one each to ctr[key]

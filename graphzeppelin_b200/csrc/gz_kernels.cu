@@ -830,72 +830,124 @@ __global__ void k_bv_reset(uint32_t V, uint32_t *parent) {
   if (v < V) parent[v] = v;
 }
 
-// Shared memory of the round-0 and merge kernels, per warp: two batches of KB member slots of
-// W + 3 words (the ring the cp.async copies land in) and one stage of W + 3 words.
-__host__ __device__ constexpr uint32_t bv_warp_words(uint32_t W, int KB) { return (2 * KB + 1) * (W + 3); }
+// Shared memory of the round-0 and merge kernels, per warp: two batches of KB member slots (the
+// ring the bulk copies land in; a slot holds the 16-byte-aligned supersets of a member's column
+// run and of its deterministic bucket), one stage of W + 3 words, and one mbarrier per batch.
+__host__ __device__ constexpr uint32_t bv_slot_bytes(uint32_t W) { return bulk_run_cap(W) + bulk_run_cap(3); }
+__host__ __device__ constexpr uint32_t bv_warp_bytes(uint32_t W, int KB) {
+  return 2 * KB * bv_slot_bytes(W) + (((W + 3) * 4 + 15) & ~15u) + 16;
+}
+
+// A warp's two batch buffers: init of their mbarriers (one arrival: the issuing lane's
+// expect_tx), issue of a batch's bulk copies, and the bounded wait for a batch.
+struct BvRing {
+  uint8_t *slots;   // 2 * KB slots
+  uint32_t *stage;  // W + 3 words
+  uint64_t *bars;   // 2
+  uint32_t slot_bytes;
+  __device__ void init(uint8_t *warp_smem, uint32_t W, int KB) {
+    slot_bytes = bv_slot_bytes(W);
+    slots = warp_smem;
+    stage = reinterpret_cast<uint32_t *>(warp_smem + 2 * KB * slot_bytes);
+    bars = reinterpret_cast<uint64_t *>(warp_smem + 2 * KB * slot_bytes + (((W + 3) * 4 + 15) & ~15u));
+    if ((threadIdx.x & 31) == 0) {
+      mbar_init(smem_u32(&bars[0]), 1);
+      mbar_init(smem_u32(&bars[1]), 1);
+      mbar_fence_init();
+    }
+    __syncwarp();
+  }
+  __device__ uint8_t *slot(uint32_t t, uint32_t k, int KB) const { return slots + ((t & 1) * KB + k) * slot_bytes; }
+  // Lane k < KB with `mine` copies its run [run, run + W) and deterministic bucket det into slot
+  // k of batch t; lane 0 arms the batch's barrier with the bytes of the whole batch first.
+  __device__ void issue(uint32_t t, bool mine, const uint32_t *run, const uint32_t *det, uint32_t W, int KB) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t bar = smem_u32(&bars[t & 1]);
+    const uint32_t bytes = mine ? bulk_run_bytes(run, W) + bulk_run_bytes(det, 3) : 0;
+    const uint32_t total = __reduce_add_sync(kFull, bytes);
+    // this lane's reads of the slots it is about to overwrite, before the async proxy writes
+    fence_proxy_async_smem();
+    __syncwarp();
+    if (lane == 0) {
+      if (total) mbar_expect_tx(bar, total);
+      else mbar_arrive(bar);
+    }
+    __syncwarp();
+    if (mine) {
+      uint8_t *sl = slot(t, lane, KB);
+      bulk_run_copy(sl, run, W, bar);
+      bulk_run_copy(sl + bulk_run_cap(W), det, 3, bar);
+    }
+  }
+  __device__ bool wait(uint32_t t) const {
+    const bool ok = mbar_wait_bounded(smem_u32(&bars[t & 1]), (t >> 1) & 1, kWaitLimitNs);
+    return __all_sync(kFull, ok);
+  }
+};
 
 // Round 0 (run_round_zero, src/cc_sketch_alg.cpp:223-244): every vertex sketch samples its
 // sample 0 -- columns 0..CPS-1 and the deterministic bucket. A warp takes 32 consecutive
-// vertices at a time, in batches of KB whose regions are copied to shared memory with cp.async
-// one batch ahead (also across its 32-vertex groups), and samples each vertex from there; lane
-// i keeps vertex i's result, and the 32 results are applied by the 32 lanes at once, so the
-// union-find chains of one warp overlap.
+// vertices at a time, in batches of KB whose runs are bulk-copied to shared memory one batch
+// ahead (also across its 32-vertex groups), and samples each vertex from there; lane i keeps
+// vertex i's result, and the 32 results are applied by the 32 lanes at once.
 template <int CPS, int KB>
 __global__ void __launch_bounds__(256) k_bv_round0(BoruvkaGeom g, const uint32_t *__restrict__ sk_words,
                                                    BoruvkaBufs b) {
-  extern __shared__ uint32_t bv_smem[];
+  extern __shared__ __align__(16) uint8_t bv_smem[];
   constexpr uint32_t BPG = 32 / KB;  // batches per 32-vertex group
   const uint32_t lane = threadIdx.x & 31;
-  const uint32_t W = 3 * CPS * g.B, SW = W + 3, detw = 3 * g.C * g.B;
-  uint32_t *ring = bv_smem + (threadIdx.x >> 5) * bv_warp_words(W, KB);
+  const uint32_t W = 3 * CPS * g.B, detw = 3 * g.C * g.B;
+  BvRing ring;
+  ring.init(bv_smem + (threadIdx.x >> 5) * bv_warp_bytes(W, KB), W, KB);
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t ngroups = (g.V + 31) / 32;
-  auto issue = [&](uint32_t t) {  // batch t of this warp -> ring half t & 1
+  auto first_vertex = [&](uint32_t t) {  // first vertex of batch t, or ~0 past the work
     const uint32_t grp = gw + (t / BPG) * nwarps;
-    if (grp < ngroups) {
-      const uint32_t v0 = grp * 32 + (t % BPG) * KB;
-      uint32_t *half = ring + (t & 1) * KB * SW;
-#pragma unroll
-      for (int k = 0; k < KB; ++k)
-        if (v0 + k < g.V) {
-          const uint32_t *sk = sk_words + (uint64_t)(v0 + k) * g.sketch_words;
-          region_copy_async(half + k * SW, sk, sk + detw, W, lane);
-        }
-    }
-    cp_async_commit();
+    return grp < ngroups ? grp * 32 + (t % BPG) * KB : 0xffffffffu;
+  };
+  auto issue = [&](uint32_t t) {
+    const uint32_t v0 = first_vertex(t);
+    const bool mine = v0 != 0xffffffffu && lane < (uint32_t)KB && v0 + lane < g.V;
+    const uint32_t *sk = sk_words + (uint64_t)(mine ? v0 + lane : 0) * g.sketch_words;
+    ring.issue(t, mine, sk, sk + detw, W, KB);
   };
   if (gw >= ngroups) return;
   int my_res = 1;
   uint64_t my_idx = 0;
   issue(0);
   for (uint32_t t = 0;; ++t) {
-    const uint32_t grp = gw + (t / BPG) * nwarps;
-    if (grp >= ngroups) break;
+    const uint32_t v0 = first_vertex(t);
+    if (v0 == 0xffffffffu) break;
     issue(t + 1);
-    cp_async_wait<1>();
-    __syncwarp();
-    const uint32_t v0 = grp * 32 + (t % BPG) * KB;
-    const uint32_t *half = ring + (t & 1) * KB * SW;
+    if (!ring.wait(t)) {
+      if (lane == 0) atomicOr(b.status, kStatusTimeout);
+      ring.wait(t + 1);  // its copies must land before the block's shared memory goes away
+      return;
+    }
 #pragma unroll 1
     for (int k = 0; k < KB; ++k)
       if (v0 + k < g.V) {
+        const uint32_t *sk = sk_words + (uint64_t)(v0 + k) * g.sketch_words;
+        const uint8_t *sl = ring.slot(t, k, KB);
+        const uint32_t *run = bulk_run_at(sl, sk), *det = bulk_run_at(sl + bulk_run_cap(W), sk + detw);
         uint64_t idx;
-        const int res = warp_sample_smem<CPS>(half + k * SW, W, g.B, g.flip_chk, &idx);
+        const int res = warp_sample_smem_split<CPS>(run, det, g.B, g.flip_chk, &idx);
         if (lane == (t % BPG) * KB + k) {
           my_res = res;
           my_idx = idx;
         }
       }
     __syncwarp();
-    if (t % BPG == BPG - 1) {
-      if (grp * 32 + lane < g.V) handle_result(my_res, my_idx, 0, grp * 32 + lane, g, b);
+    if (t % BPG == BPG - 1) {  // end of a 32-vertex group: its results, one lane each
+      const uint32_t base = v0 - (t % BPG) * KB;
+      if (base + lane < g.V) handle_result(my_res, my_idx, 0, base + lane, g, b);
       __syncwarp();
       my_res = 1;
       my_idx = 0;
     }
   }
-  cp_async_wait<0>();
+  // the batch issued last covered no vertex (nothing in flight)
 }
 
 // Root of every vertex and members per root; lanes of a warp that share a root add to its
@@ -983,11 +1035,12 @@ template <int CPS, int NW, int KB>
 __global__ void __launch_bounds__(256) k_bv_merge(BoruvkaGeom g, const uint32_t *__restrict__ sk_words,
                                                   BoruvkaBufs b) {
   const uint32_t round = *b.round;
-  extern __shared__ uint32_t bv_smem[];
+  extern __shared__ __align__(16) uint8_t bv_smem[];
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t W = 3 * CPS * g.B, SW = W + 3;
-  uint32_t *ring = bv_smem + (threadIdx.x >> 5) * bv_warp_words(W, KB);
-  uint32_t *st = ring + 2 * KB * SW;
+  BvRing ring;
+  ring.init(bv_smem + (threadIdx.x >> 5) * bv_warp_bytes(W, KB), W, KB);
+  uint32_t *st = ring.stage;
   const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint64_t p0 = (uint64_t)w * g.span;
   if (p0 >= g.V) return;
@@ -1009,18 +1062,17 @@ __global__ void __launch_bounds__(256) k_bv_merge(BoruvkaGeom g, const uint32_t 
   if (lane == 0 && p0 > 0) edge_c = b.order_comp[p0 - 1];
   if (lane == 1 && p1 < g.V) edge_c = b.order_comp[p1];
   const uint32_t prev_c = __shfl_sync(kFull, edge_c, 0), next_c = __shfl_sync(kFull, edge_c, 1);
+  // lane k < KB copies member t * KB + k of batch t (its vertex and component come by shuffle)
+  auto member_sketch = [&](uint32_t m) {
+    const uint32_t v = __shfl_sync(kFull, my_v, m & 31);
+    return sk_words + (uint64_t)v * g.sketch_words;
+  };
   auto issue = [&](uint32_t t) {
-    uint32_t *half = ring + (t & 1) * KB * SW;
-#pragma unroll
-    for (int k = 0; k < KB; ++k) {
-      const uint32_t m = t * KB + k;
-      if (m < n && __shfl_sync(kFull, my_c, m) != big) {
-        const uint32_t v = __shfl_sync(kFull, my_v, m);
-        const uint32_t *sk = sk_words + (uint64_t)v * g.sketch_words;
-        region_copy_async(half + k * SW, sk + col, sk + detw, W, lane);
-      }
-    }
-    cp_async_commit();
+    const uint32_t m = t * KB + lane;
+    const uint32_t *sk = member_sketch(m);
+    const uint32_t c = __shfl_sync(kFull, my_c, m & 31);
+    const bool mine = lane < (uint32_t)KB && m < n && c != big;
+    ring.issue(t, mine, sk + col, sk + detw, W, KB);
   };
   issue(0);
   uint32_t acc[NW], dacc = 0, cpl[NW], dcpl = 0;
@@ -1081,16 +1133,18 @@ __global__ void __launch_bounds__(256) k_bv_merge(BoruvkaGeom g, const uint32_t 
   const uint32_t nb = (n + KB - 1) / KB;
   for (uint32_t t = 0; t < nb; ++t) {
     if (t + 1 < nb) issue(t + 1);
-    else cp_async_commit();
-    cp_async_wait<1>();
-    __syncwarp();
-    const uint32_t *half = ring + (t & 1) * KB * SW;
+    if (!ring.wait(t)) {
+      if (lane == 0) atomicOr(b.status, kStatusTimeout);
+      if (t + 1 < nb) ring.wait(t + 1);  // its copies must land before the block's shared memory goes away
+      return;
+    }
     // not unrolled: one copy of the flush (and the sampling it inlines) keeps the kernel small
     // enough for the instruction cache
 #pragma unroll 1
     for (int k = 0; k < KB; ++k) {
       const uint32_t m = t * KB + k;
       const uint32_t c = __shfl_sync(kFull, my_c, m < n ? m : 0);
+      const uint32_t *sk = member_sketch(m < n ? m : 0);
       if (m < n && c != big) {
         if (c != cur) {
           if (cur != 0xffffffffu) flush(cur);
@@ -1099,26 +1153,27 @@ __global__ void __launch_bounds__(256) k_bv_merge(BoruvkaGeom g, const uint32_t 
           for (int q = 0; q < NW; ++q) acc[q] = 0;
           dacc = 0;
         }
-        const uint32_t *sl = half + k * SW;
+        const uint8_t *slt = ring.slot(t, k, KB);
+        const uint32_t *sl = bulk_run_at(slt, sk + col);
+        const uint32_t *sd = bulk_run_at(slt + bulk_run_cap(W), sk + detw);
 #pragma unroll
         for (int q = 0; q < NW; ++q) {
           const uint32_t wi = q * 32 + lane;
           if (wi < W) acc[q] ^= sl[wi];
         }
-        if (lane < 3) dacc ^= sl[W + lane];
+        if (lane < 3) dacc ^= sd[lane];
         if (big != 0xffffffffu) {
 #pragma unroll
           for (int q = 0; q < NW; ++q) {
             const uint32_t wi = q * 32 + lane;
             if (wi < W) cpl[q] ^= sl[wi];
           }
-          if (lane < 3) dcpl ^= sl[W + lane];
+          if (lane < 3) dcpl ^= sd[lane];
         }
       }
     }
     __syncwarp();
   }
-  cp_async_wait<0>();
   if (cur != 0xffffffffu) flush(cur);
   apply();
   if (big != 0xffffffffu) {
@@ -1573,7 +1628,7 @@ __global__ void k_total_xor(const uint32_t *__restrict__ sk, uint32_t V, uint32_
 // shared memory of a 256-thread block (8 warps).
 int bv_batch(int cps) { return cps == 1 ? 8 : 1; }
 size_t bv_smem_bytes(const BoruvkaGeom &g) {
-  return 8 * sizeof(uint32_t) * bv_warp_words(3 * g.cps * g.B, bv_batch(g.cps));
+  return 8 * (size_t)bv_warp_bytes(3 * g.cps * g.B, bv_batch(g.cps));
 }
 template <class K>
 cudaError_t bv_smem_attr(K kern, size_t smem) {

@@ -170,6 +170,10 @@ struct BoruvkaBufs {
   uint32_t *status;
 };
 
+// Bytes allocated past the last vertex sketch of any sketch buffer a query reads: its bulk copies
+// read 16-byte-aligned supersets of bucket runs, up to 15 bytes beyond the last sketch.
+constexpr size_t kSketchTail = 256;
+
 // Grouped members XOR-merged by one warp per Boruvka round (the per-warp partial slots are
 // sized by it).
 constexpr uint32_t kBoruvkaSpan = 32;
