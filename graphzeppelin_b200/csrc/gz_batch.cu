@@ -530,18 +530,19 @@ constexpr int kMbKB = 8;  // members per cp.async batch
 // dynamic shared memory of a 256-thread query block: per warp two batches of kMbKB member slots
 // and one stage, each slot acc_words (the largest graph's sample region + its deterministic
 // bucket)
-inline size_t mb_query_smem(uint32_t acc_words) { return 8 * sizeof(uint32_t) * (2 * kMbKB + 1) * acc_words; }
+inline size_t mb_query_smem(uint32_t acc_words) { return 8 * (size_t)bv_warp_bytes(acc_words - 3, kMbKB); }
 
 // Round 0 for every active graph (run_round_zero, src/cc_sketch_alg.cpp:223-244): a warp takes
 // 32 consecutive global vertices, copies their sample-0 regions to shared memory with cp.async
 // in batches of kMbKB (one batch ahead), samples each there, and the 32 lanes then apply their
 // vertex's result together.
 __global__ void __launch_bounds__(256) k_mb_round0(MBBufs b) {
-  extern __shared__ uint32_t mb_smem[];
+  extern __shared__ __align__(16) uint8_t mb_smem[];
   const uint32_t lane = threadIdx.x & 31;
-  const uint32_t SW = b.acc_words;
-  uint32_t *ring = mb_smem + (threadIdx.x >> 5) * (2 * kMbKB + 1) * SW;
+  BvRing ring;
+  ring.init(mb_smem + (threadIdx.x >> 5) * bv_warp_bytes(b.acc_words - 3, kMbKB), b.acc_words - 3, kMbKB);
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  uint32_t tb = 0;  // batches this warp ran before the current group (the ring's phases go on)
   for (uint32_t base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; base < b.total_V;
        base += nwarps * 32) {
     const uint32_t n = b.total_V - base < 32 ? b.total_V - base : 32;
@@ -552,36 +553,36 @@ __global__ void __launch_bounds__(256) k_mb_round0(MBBufs b) {
       my_act = b.active[me.g] != 0;
     }
     const uint32_t act = __ballot_sync(kFull, my_act);
+    // batch t of this group: lane k < kMbKB copies vertex t * kMbKB + k
     auto issue = [&](uint32_t t) {
-      uint32_t *half = ring + (t & 1) * kMbKB * SW;
-#pragma unroll
-      for (int k = 0; k < kMbKB; ++k) {
-        const uint32_t m = t * kMbKB + k;
-        if (m < n && (act >> m & 1)) {
-          const MbVert mk = mb_vert_shfl(me, m);
-          region_copy_async(half + k * SW, mk.sk, mk.sk + mk.det, 3 * mk.B, lane);
-        }
-      }
-      cp_async_commit();
+      const uint32_t m = t * kMbKB + lane;
+      const MbVert mk = mb_vert_shfl(me, m & 31);
+      const bool mine = lane < (uint32_t)kMbKB && m < n && (act >> m & 1);
+      ring.issue(tb + t, mine, mk.sk, 3 * mk.B, mk.sk + mk.det, kMbKB);
     };
     int my_res = 1;
     uint64_t my_idx = 0;
     const uint32_t nb = (n + kMbKB - 1) / kMbKB;
     issue(0);
-    for (uint32_t t = 0; t < nb; ++t) {
+    bool ok = true;
+    for (uint32_t t = 0; t < nb && ok; ++t) {
       if (t + 1 < nb) issue(t + 1);
-      else cp_async_commit();
-      cp_async_wait<1>();
-      __syncwarp();
-      const uint32_t *half = ring + (t & 1) * kMbKB * SW;
+      if (!ring.wait(tb + t)) {
+        if (lane == 0) atomicOr(b.status, kStatusTimeout);
+        if (t + 1 < nb) ring.wait(tb + t + 1);  // its copies must land before shared memory goes away
+        ok = false;
+        break;
+      }
 #pragma unroll 1
       for (int k = 0; k < kMbKB; ++k) {
         const uint32_t m = t * kMbKB + k;
         if (m >= n) break;
         if (!(act >> m & 1)) continue;
         const MbVert mk = mb_vert_shfl(me, m);
+        const uint8_t *sl = ring.slot(tb + t, k, kMbKB);
         uint64_t idx;
-        const int res = warp_sample_smem<1>(half + k * SW, 3 * mk.B, mk.B, mk.chk, &idx);
+        const int res = warp_sample_smem_split<1>(bulk_run_at(sl, mk.sk), bulk_run_at(sl + ring.run_cap, mk.sk + mk.det),
+                                                  mk.B, mk.chk, &idx);
         if (lane == m) {
           my_res = res;
           my_idx = idx;
@@ -589,7 +590,8 @@ __global__ void __launch_bounds__(256) k_mb_round0(MBBufs b) {
       }
       __syncwarp();
     }
-    cp_async_wait<0>();
+    if (!ok) return;
+    tb += nb;
     if (lane < n) b.res[base + lane] = my_act ? res_code(my_res, my_idx) : kResZero;
     __syncwarp();
   }
@@ -650,11 +652,12 @@ __global__ void __launch_bounds__(256) k_mb_group(MBBufs b) {
 // components crossing a span edge go to acc with one atomicXor per word.
 __global__ void __launch_bounds__(256) k_mb_merge(MBBufs b) {
   constexpr int NW = Region<1>::kNW;
-  extern __shared__ uint32_t mb_smem[];
+  extern __shared__ __align__(16) uint8_t mb_smem[];
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t SW = b.acc_words;
-  uint32_t *ring = mb_smem + (threadIdx.x >> 5) * (2 * kMbKB + 1) * SW;
-  uint32_t *st = ring + 2 * kMbKB * SW;
+  BvRing ring;
+  ring.init(mb_smem + (threadIdx.x >> 5) * bv_warp_bytes(SW - 3, kMbKB), SW - 3, kMbKB);
+  uint32_t *st = ring.stage;
   const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nc = *b.ncomp;
   const uint32_t members = b.comp_start[nc];
@@ -677,17 +680,12 @@ __global__ void __launch_bounds__(256) k_mb_merge(MBBufs b) {
   if (lane == 0 && p0 > 0) edge_c = b.order_comp[p0 - 1];
   if (lane == 1 && p1 < members) edge_c = b.order_comp[p1];
   const uint32_t prev_c = __shfl_sync(kFull, edge_c, 0), next_c = __shfl_sync(kFull, edge_c, 1);
+  // batch t: lane k < kMbKB copies member t * kMbKB + k
   auto issue = [&](uint32_t t) {
-    uint32_t *half = ring + (t & 1) * kMbKB * SW;
-#pragma unroll
-    for (int k = 0; k < kMbKB; ++k) {
-      const uint32_t m = t * kMbKB + k;
-      if (m < n) {
-        const MbVert mk = mb_vert_shfl(me, m);
-        region_copy_async(half + k * SW, mk.sk + 3 * round * mk.B, mk.sk + mk.det, 3 * mk.B, lane);
-      }
-    }
-    cp_async_commit();
+    const uint32_t m = t * kMbKB + lane;
+    const MbVert mk = mb_vert_shfl(me, m & 31);
+    const bool mine = lane < (uint32_t)kMbKB && m < n;
+    ring.issue(t, mine, mk.sk + 3 * round * mk.B, 3 * mk.B, mk.sk + mk.det, kMbKB);
   };
   issue(0);
   uint32_t acc[NW], dacc = 0;
@@ -739,36 +737,39 @@ __global__ void __launch_bounds__(256) k_mb_merge(MBBufs b) {
   const uint32_t nb = (n + kMbKB - 1) / kMbKB;
   for (uint32_t t = 0; t < nb; ++t) {
     if (t + 1 < nb) issue(t + 1);
-    else cp_async_commit();
-    cp_async_wait<1>();
-    __syncwarp();
-    const uint32_t *half = ring + (t & 1) * kMbKB * SW;
+    if (!ring.wait(t)) {
+      if (lane == 0) atomicOr(b.status, kStatusTimeout);
+      if (t + 1 < nb) ring.wait(t + 1);  // its copies must land before shared memory goes away
+      return;
+    }
     // not unrolled: one copy of the flush keeps the kernel small for the instruction cache
 #pragma unroll 1
     for (int k = 0; k < kMbKB; ++k) {
       const uint32_t m = t * kMbKB + k;
       if (m >= n) break;
       const uint32_t c = __shfl_sync(kFull, my_c, m);
+      const MbVert mk = mb_vert_shfl(me, m);
       if (c != cur) {
         if (cur != 0xffffffffu) flush();
         cur = c;
-        cm = mb_vert_shfl(me, m);
+        cm = mk;
 #pragma unroll
         for (int q = 0; q < NW; ++q) acc[q] = 0;
         dacc = 0;
       }
       const uint32_t W = 3 * cm.B;
-      const uint32_t *sl = half + k * SW;
+      const uint8_t *slt = ring.slot(t, k, kMbKB);
+      const uint32_t *sl = bulk_run_at(slt, mk.sk + 3 * round * mk.B);
+      const uint32_t *sd = bulk_run_at(slt + ring.run_cap, mk.sk + mk.det);
 #pragma unroll
       for (int q = 0; q < NW; ++q) {
         const uint32_t wi = q * 32 + lane;
         if (wi < W) acc[q] ^= sl[wi];
       }
-      if (lane < 3) dacc ^= sl[W + lane];
+      if (lane < 3) dacc ^= sd[lane];
     }
     __syncwarp();
   }
-  cp_async_wait<0>();
   flush();
   if (!whole && lane == 0) b.part_comp[w] = 0xffffffffu;
 }

@@ -467,6 +467,63 @@ __device__ __forceinline__ const uint32_t *bulk_run_at(const uint8_t *slot, cons
   return reinterpret_cast<const uint32_t *>(slot + ((uintptr_t)p & 15));
 }
 
+// Shared memory of the query kernels' bulk-copy rings, per warp: two batches of KB member slots
+// (a slot holds the 16-byte-aligned supersets of a member's column run, up to Wmax words, and of
+// its deterministic bucket), one stage of Wmax + 3 words, and one mbarrier per batch.
+__host__ __device__ constexpr uint32_t bv_slot_bytes(uint32_t Wmax) { return bulk_run_cap(Wmax) + bulk_run_cap(3); }
+__host__ __device__ constexpr uint32_t bv_warp_bytes(uint32_t Wmax, int KB) {
+  return 2 * KB * bv_slot_bytes(Wmax) + (((Wmax + 3) * 4 + 15) & ~15u) + 16;
+}
+
+// A warp's two batch buffers: init of their mbarriers (one arrival: lane 0's expect_tx), issue of
+// a batch's bulk copies, and the bounded wait for a batch.
+struct BvRing {
+  uint8_t *slots;   // 2 * KB slots
+  uint32_t *stage;  // Wmax + 3 words
+  uint64_t *bars;   // 2
+  uint32_t slot_bytes, run_cap;
+  __device__ void init(uint8_t *warp_smem, uint32_t Wmax, int KB) {
+    run_cap = bulk_run_cap(Wmax);
+    slot_bytes = bv_slot_bytes(Wmax);
+    slots = warp_smem;
+    stage = reinterpret_cast<uint32_t *>(warp_smem + 2 * KB * slot_bytes);
+    bars = reinterpret_cast<uint64_t *>(warp_smem + 2 * KB * slot_bytes + (((Wmax + 3) * 4 + 15) & ~15u));
+    if ((threadIdx.x & 31) == 0) {
+      mbar_init(smem_u32(&bars[0]), 1);
+      mbar_init(smem_u32(&bars[1]), 1);
+      mbar_fence_init();
+    }
+    __syncwarp();
+  }
+  __device__ uint8_t *slot(uint32_t t, uint32_t k, int KB) const { return slots + ((t & 1) * KB + k) * slot_bytes; }
+  // Lane k < KB with `mine` copies its run [run, run + words) (words <= Wmax) and its
+  // deterministic bucket det into slot k of batch t; lane 0 arms the batch's barrier with the
+  // bytes of the whole batch first. Every lane of the warp calls it.
+  __device__ void issue(uint32_t t, bool mine, const uint32_t *run, uint32_t words, const uint32_t *det, int KB) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t bar = smem_u32(&bars[t & 1]);
+    const uint32_t bytes = mine ? bulk_run_bytes(run, words) + bulk_run_bytes(det, 3) : 0;
+    const uint32_t total = __reduce_add_sync(kFull, bytes);
+    // this lane's reads of the slots about to be overwritten, before the async proxy writes
+    fence_proxy_async_smem();
+    __syncwarp();
+    if (lane == 0) {
+      if (total) mbar_expect_tx(bar, total);
+      else mbar_arrive(bar);
+    }
+    __syncwarp();
+    if (mine) {
+      uint8_t *sl = slot(t, lane, KB);
+      bulk_run_copy(sl, run, words, bar);
+      bulk_run_copy(sl + run_cap, det, 3, bar);
+    }
+  }
+  __device__ bool wait(uint32_t t) const {
+    const bool ok = mbar_wait_bounded(smem_u32(&bars[t & 1]), (t >> 1) & 1, kWaitLimitNs);
+    return __all_sync(kFull, ok);
+  }
+};
+
 // Warp-aggregated counter add: lanes in `active` holding the same key add one each to ctr[key]
 // with one atomic per distinct key; returns this lane's slot (old value + rank among its key's
 // lanes). stage is a 32-word per-warp shared array used to hand the base to the key's lanes.

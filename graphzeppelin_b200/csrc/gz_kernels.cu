@@ -830,61 +830,6 @@ __global__ void k_bv_reset(uint32_t V, uint32_t *parent) {
   if (v < V) parent[v] = v;
 }
 
-// Shared memory of the round-0 and merge kernels, per warp: two batches of KB member slots (the
-// ring the bulk copies land in; a slot holds the 16-byte-aligned supersets of a member's column
-// run and of its deterministic bucket), one stage of W + 3 words, and one mbarrier per batch.
-__host__ __device__ constexpr uint32_t bv_slot_bytes(uint32_t W) { return bulk_run_cap(W) + bulk_run_cap(3); }
-__host__ __device__ constexpr uint32_t bv_warp_bytes(uint32_t W, int KB) {
-  return 2 * KB * bv_slot_bytes(W) + (((W + 3) * 4 + 15) & ~15u) + 16;
-}
-
-// A warp's two batch buffers: init of their mbarriers (one arrival: the issuing lane's
-// expect_tx), issue of a batch's bulk copies, and the bounded wait for a batch.
-struct BvRing {
-  uint8_t *slots;   // 2 * KB slots
-  uint32_t *stage;  // W + 3 words
-  uint64_t *bars;   // 2
-  uint32_t slot_bytes;
-  __device__ void init(uint8_t *warp_smem, uint32_t W, int KB) {
-    slot_bytes = bv_slot_bytes(W);
-    slots = warp_smem;
-    stage = reinterpret_cast<uint32_t *>(warp_smem + 2 * KB * slot_bytes);
-    bars = reinterpret_cast<uint64_t *>(warp_smem + 2 * KB * slot_bytes + (((W + 3) * 4 + 15) & ~15u));
-    if ((threadIdx.x & 31) == 0) {
-      mbar_init(smem_u32(&bars[0]), 1);
-      mbar_init(smem_u32(&bars[1]), 1);
-      mbar_fence_init();
-    }
-    __syncwarp();
-  }
-  __device__ uint8_t *slot(uint32_t t, uint32_t k, int KB) const { return slots + ((t & 1) * KB + k) * slot_bytes; }
-  // Lane k < KB with `mine` copies its run [run, run + W) and deterministic bucket det into slot
-  // k of batch t; lane 0 arms the batch's barrier with the bytes of the whole batch first.
-  __device__ void issue(uint32_t t, bool mine, const uint32_t *run, const uint32_t *det, uint32_t W, int KB) {
-    const uint32_t lane = threadIdx.x & 31;
-    const uint32_t bar = smem_u32(&bars[t & 1]);
-    const uint32_t bytes = mine ? bulk_run_bytes(run, W) + bulk_run_bytes(det, 3) : 0;
-    const uint32_t total = __reduce_add_sync(kFull, bytes);
-    // this lane's reads of the slots it is about to overwrite, before the async proxy writes
-    fence_proxy_async_smem();
-    __syncwarp();
-    if (lane == 0) {
-      if (total) mbar_expect_tx(bar, total);
-      else mbar_arrive(bar);
-    }
-    __syncwarp();
-    if (mine) {
-      uint8_t *sl = slot(t, lane, KB);
-      bulk_run_copy(sl, run, W, bar);
-      bulk_run_copy(sl + bulk_run_cap(W), det, 3, bar);
-    }
-  }
-  __device__ bool wait(uint32_t t) const {
-    const bool ok = mbar_wait_bounded(smem_u32(&bars[t & 1]), (t >> 1) & 1, kWaitLimitNs);
-    return __all_sync(kFull, ok);
-  }
-};
-
 // Round 0 (run_round_zero, src/cc_sketch_alg.cpp:223-244): every vertex sketch samples its
 // sample 0 -- columns 0..CPS-1 and the deterministic bucket. A warp takes 32 consecutive
 // vertices at a time, in batches of KB whose runs are bulk-copied to shared memory one batch
@@ -910,7 +855,7 @@ __global__ void __launch_bounds__(256) k_bv_round0(BoruvkaGeom g, const uint32_t
     const uint32_t v0 = first_vertex(t);
     const bool mine = v0 != 0xffffffffu && lane < (uint32_t)KB && v0 + lane < g.V;
     const uint32_t *sk = sk_words + (uint64_t)(mine ? v0 + lane : 0) * g.sketch_words;
-    ring.issue(t, mine, sk, sk + detw, W, KB);
+    ring.issue(t, mine, sk, W, sk + detw, KB);
   };
   if (gw >= ngroups) return;
   int my_res = 1;
@@ -930,7 +875,7 @@ __global__ void __launch_bounds__(256) k_bv_round0(BoruvkaGeom g, const uint32_t
       if (v0 + k < g.V) {
         const uint32_t *sk = sk_words + (uint64_t)(v0 + k) * g.sketch_words;
         const uint8_t *sl = ring.slot(t, k, KB);
-        const uint32_t *run = bulk_run_at(sl, sk), *det = bulk_run_at(sl + bulk_run_cap(W), sk + detw);
+        const uint32_t *run = bulk_run_at(sl, sk), *det = bulk_run_at(sl + ring.run_cap, sk + detw);
         uint64_t idx;
         const int res = warp_sample_smem_split<CPS>(run, det, g.B, g.flip_chk, &idx);
         if (lane == (t % BPG) * KB + k) {
@@ -1072,7 +1017,7 @@ __global__ void __launch_bounds__(256) k_bv_merge(BoruvkaGeom g, const uint32_t 
     const uint32_t *sk = member_sketch(m);
     const uint32_t c = __shfl_sync(kFull, my_c, m & 31);
     const bool mine = lane < (uint32_t)KB && m < n && c != big;
-    ring.issue(t, mine, sk + col, sk + detw, W, KB);
+    ring.issue(t, mine, sk + col, W, sk + detw, KB);
   };
   issue(0);
   uint32_t acc[NW], dacc = 0, cpl[NW], dcpl = 0;
@@ -1155,7 +1100,7 @@ __global__ void __launch_bounds__(256) k_bv_merge(BoruvkaGeom g, const uint32_t 
         }
         const uint8_t *slt = ring.slot(t, k, KB);
         const uint32_t *sl = bulk_run_at(slt, sk + col);
-        const uint32_t *sd = bulk_run_at(slt + bulk_run_cap(W), sk + detw);
+        const uint32_t *sd = bulk_run_at(slt + ring.run_cap, sk + detw);
 #pragma unroll
         for (int q = 0; q < NW; ++q) {
           const uint32_t wi = q * 32 + lane;
