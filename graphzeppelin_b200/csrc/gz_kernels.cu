@@ -147,20 +147,31 @@ k_gutter_sort_scatter(const void *__restrict__ in, uint64_t n, GutterGeom g, uin
     uint32_t shift = 0;
     if (INPUT == kInputRecords) shift = stage_records(rec, t0, cnt, s_rec);
     __syncthreads();
-    // 1. count entries per bin
-    for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
-      uint32_t u, v;
-      if (INPUT == kInputRecords) {
-        parse_record(s_rec, shift, i, u, v);
-      } else {
-        const uint2 x = ein[t0 + i];
-        u = x.x;
-        v = x.y;
+    // 1. this thread's inputs (at most RPT; blockDim = 1024 and rec_tile <= RPT * 1024) into
+    //    registers, then their per-bin counts
+    constexpr int RPT = INPUT == kInputRecords ? 8 : 16;
+    uint32_t ru[RPT], rv[RPT];
+#pragma unroll
+    for (int k = 0; k < RPT; ++k) {
+      const uint32_t i = threadIdx.x + k * blockDim.x;
+      ru[k] = rv[k] = 0xffffffffu;
+      if (i < cnt) {
+        if (INPUT == kInputRecords) {
+          parse_record(s_rec, shift, i, ru[k], rv[k]);
+        } else {
+          const uint2 x = ein[t0 + i];
+          ru[k] = x.x;
+          rv[k] = x.y;
+        }
+        if (ru[k] >= g.V || rv[k] >= g.V) ru[k] = 0xffffffffu;  // dropped (status set by the count pass)
       }
-      if (u >= g.V || v >= g.V) continue;
-      atomicAdd(&s_cur[u >> g.bin_shift], 1u);
-      if (INPUT == kInputRecords) atomicAdd(&s_cur[v >> g.bin_shift], 1u);
     }
+#pragma unroll
+    for (int k = 0; k < RPT; ++k)
+      if (ru[k] != 0xffffffffu) {
+        atomicAdd(&s_cur[ru[k] >> g.bin_shift], 1u);
+        if (INPUT == kInputRecords) atomicAdd(&s_cur[rv[k] >> g.bin_shift], 1u);
+      }
     __syncthreads();
     // 2. run offsets inside the tile (bins [tid*per_thread, +per_thread) per thread)
     uint32_t local[4] = {0, 0, 0, 0}, sum = 0;
@@ -180,20 +191,21 @@ k_gutter_sort_scatter(const void *__restrict__ in, uint64_t n, GutterGeom g, uin
       run += local[k];
     }
     __syncthreads();
-    // 3. place entries in bin order
-    for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
-      uint32_t u, v;
-      if (INPUT == kInputRecords) {
-        parse_record(s_rec, shift, i, u, v);
-      } else {
-        const uint2 x = ein[t0 + i];
-        u = x.x;
-        v = x.y;
+    // 3. place entries in bin order: every slot claimed first (independent atomics in flight
+    //    together), then the stores
+    uint32_t pu[RPT], pv[RPT];
+#pragma unroll
+    for (int k = 0; k < RPT; ++k)
+      if (ru[k] != 0xffffffffu) {
+        pu[k] = atomicAdd(&s_cur[ru[k] >> g.bin_shift], 1u);
+        if (INPUT == kInputRecords) pv[k] = atomicAdd(&s_cur[rv[k] >> g.bin_shift], 1u);
       }
-      if (u >= g.V || v >= g.V) continue;
-      s_sorted[atomicAdd(&s_cur[u >> g.bin_shift], 1u)] = make_uint2(u, v);
-      if (INPUT == kInputRecords) s_sorted[atomicAdd(&s_cur[v >> g.bin_shift], 1u)] = make_uint2(v, u);
-    }
+#pragma unroll
+    for (int k = 0; k < RPT; ++k)
+      if (ru[k] != 0xffffffffu) {
+        s_sorted[pu[k]] = make_uint2(ru[k], rv[k]);
+        if (INPUT == kInputRecords) s_sorted[pv[k]] = make_uint2(rv[k], ru[k]);
+      }
     __syncthreads();
     // 4. coalesced write-out of the runs
     const uint32_t total = s_cur[nb - 1];
