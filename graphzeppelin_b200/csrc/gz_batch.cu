@@ -599,12 +599,29 @@ __global__ void __launch_bounds__(256) k_mb_round0(MBBufs b) {
 
 // Roots and members per root of the active graphs' vertices (one atomic per root per warp).
 __global__ void __launch_bounds__(256) k_mb_label(MBBufs b) {
+  __shared__ uint32_t s_r0;
   const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool ok = v < b.total_V && b.active[b.gov[v]];
+  const bool in = v < b.total_V;
+  const bool ok = in && b.active[b.gov[v]];
+  uint32_t r = 0xffffffffu;
+  if (ok) {
+    r = dsu_find(b.parent, v);
+    b.label[v] = r;
+    // full path compression (no union runs during the labelling)
+    if (__ldcg(b.parent + v) != r) __stcg(b.parent + v, r);
+  }
+  if (threadIdx.x == 0) s_r0 = r;
+  __syncthreads();
+  // every in-range vertex of the block active and under one root: one counter add for all
+  if (__syncthreads_and(!in || (ok && r == s_r0))) {
+    if (threadIdx.x == 0 && ok) {
+      const uint32_t nin = b.total_V - blockIdx.x * blockDim.x < blockDim.x ? b.total_V - blockIdx.x * blockDim.x : blockDim.x;
+      atomicAdd(&b.cnt[r], nin);
+    }
+    return;
+  }
   const uint32_t act = __ballot_sync(kFull, ok);
   if (!ok) return;
-  const uint32_t r = dsu_find(b.parent, v);
-  b.label[v] = r;
   const uint32_t peers = __match_any_sync(act, r);
   if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&b.cnt[r], (uint32_t)__popc(peers));
 }
@@ -618,19 +635,36 @@ __global__ void k_mb_pack(MBBufs b) {
 
 __global__ void __launch_bounds__(256) k_mb_group(MBBufs b) {
   __shared__ uint32_t stage[8][32];
+  __shared__ uint32_t s_r0, s_base;
   const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
   if (v == 0) {
     const uint32_t nc = (uint32_t)(*b.scan_total >> 32), members = (uint32_t)*b.scan_total;
     b.comp_start[nc] = members;
     *b.ncomp = nc;
   }
-  const bool ok = v < b.total_V && b.active[b.gov[v]];
-  const uint32_t act = __ballot_sync(kFull, ok);
-  if (!ok) return;
-  const uint32_t r = b.label[v];
+  const bool in = v < b.total_V;
+  const bool ok = in && b.active[b.gov[v]];
+  const uint32_t r = ok ? b.label[v] : 0xffffffffu;
+  if (threadIdx.x == 0) s_r0 = r;
+  __syncthreads();
+  uint32_t slot;
+  if (__syncthreads_and(!in || (ok && r == s_r0))) {
+    // every in-range vertex of the block active and under one root: one cursor claim
+    if (threadIdx.x == 0 && ok) {
+      const uint32_t nin = b.total_V - blockIdx.x * blockDim.x < blockDim.x ? b.total_V - blockIdx.x * blockDim.x : blockDim.x;
+      s_base = atomicAdd(&b.fill[r], nin);
+    }
+    __syncthreads();
+    if (!ok) return;
+    slot = s_base + threadIdx.x;
+  } else {
+    const uint32_t act = __ballot_sync(kFull, ok);
+    if (!ok) return;
+    slot = warp_agg_inc(b.fill, r, act, stage[threadIdx.x >> 5]);
+  }
   const uint64_t s = b.packed[r];
   const uint32_t start = (uint32_t)s, c = (uint32_t)(s >> 32);
-  const uint32_t pos = start + warp_agg_inc(b.fill, r, act, stage[threadIdx.x >> 5]);
+  const uint32_t pos = start + slot;
   b.order[pos] = v;
   b.order_comp[pos] = c;
   if (v == r) {

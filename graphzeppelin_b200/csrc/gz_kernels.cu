@@ -913,11 +913,30 @@ __global__ void __launch_bounds__(256) k_bv_round0(BoruvkaGeom g, const uint32_t
 // lane of each root group.
 __global__ void __launch_bounds__(256) k_bv_label(uint32_t V, uint32_t *parent, uint32_t *label,
                                                   uint32_t *cnt, uint32_t *minv) {
+  __shared__ uint32_t s_r0;
   const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t active = __ballot_sync(kFull, v < V);
-  if (v >= V) return;
-  const uint32_t r = dsu_find(parent, v);
-  label[v] = r;
+  const bool in = v < V;
+  uint32_t r = 0;
+  if (in) {
+    r = dsu_find(parent, v);
+    label[v] = r;
+    // full path compression: no union runs during the labelling, and a root is as valid an
+    // ancestor as any, so later rounds find this vertex's root in a hop or two
+    if (__ldcg(parent + v) != r) __stcg(parent + v, r);
+  }
+  if (threadIdx.x == 0) s_r0 = r;
+  __syncthreads();
+  // a block whose vertices all have one root (a giant component) adds to its counter once
+  if (__syncthreads_and(!in || r == s_r0)) {
+    if (threadIdx.x == 0) {
+      const uint32_t nin = V - blockIdx.x * blockDim.x < blockDim.x ? V - blockIdx.x * blockDim.x : blockDim.x;
+      atomicAdd(&cnt[r], nin);
+      if (minv) atomicMin(&minv[r], v);
+    }
+    return;
+  }
+  const uint32_t active = __ballot_sync(kFull, in);
+  if (!in) return;
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t peers = __match_any_sync(active, r);
   if (lane == __ffs(peers) - 1) {
@@ -954,13 +973,30 @@ __global__ void __launch_bounds__(256) k_bv_group(uint32_t V, uint32_t acc_words
                                                   uint32_t *comp_start, uint32_t *comp_key,
                                                   uint32_t *ncomp, uint32_t *acc, uint32_t *big) {
   __shared__ uint32_t stage[8][32];
+  __shared__ uint32_t s_r0, s_base;
   const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t active = __ballot_sync(kFull, v < V);
-  if (v >= V) return;
-  const uint32_t r = label[v];
+  const bool in = v < V;
+  const uint32_t r = in ? label[v] : 0u;
+  if (threadIdx.x == 0) s_r0 = r;
+  __syncthreads();
+  uint32_t slot;
+  if (__syncthreads_and(!in || r == s_r0)) {
+    // one root for the whole block (a giant component): one cursor claim for all its vertices
+    if (threadIdx.x == 0) {
+      const uint32_t nin = V - blockIdx.x * blockDim.x < blockDim.x ? V - blockIdx.x * blockDim.x : blockDim.x;
+      s_base = atomicAdd(&fill[r], nin);
+    }
+    __syncthreads();
+    if (!in) return;
+    slot = s_base + threadIdx.x;
+  } else {
+    const uint32_t active = __ballot_sync(kFull, in);
+    if (!in) return;
+    slot = warp_agg_inc(fill, r, active, stage[threadIdx.x >> 5]);
+  }
   const uint64_t s = packed[r];
   const uint32_t start = (uint32_t)s, c = (uint32_t)(s >> 32);
-  const uint32_t pos = start + warp_agg_inc(fill, r, active, stage[threadIdx.x >> 5]);
+  const uint32_t pos = start + slot;
   order[pos] = v;
   order_comp[pos] = c;
   if (v == r) {
