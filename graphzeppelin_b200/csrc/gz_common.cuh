@@ -307,7 +307,6 @@ __device__ __forceinline__ int warp_sample_cols(const uint32_t (&d)[3], const ui
 template <int CPS>
 struct Region {
   static constexpr int kNW = (3 * CPS * 64 + 31) / 32;  // word slots per lane (B <= 64)
-  static constexpr int kStage = 3 * CPS * 64 + 4;        // per-warp stage words
 };
 
 // Load region words [0, W) at src and the deterministic bucket at det into x / dw.
@@ -323,62 +322,10 @@ __device__ __forceinline__ void region_load(const uint32_t *__restrict__ src,
   dw = lane < 3 ? det[lane] : 0u;
 }
 
-// Sketch::sample (src/sketch.cpp:94-116) of a region held in word space: the deterministic
-// bucket first, then columns 0..CPS-1, depths 0..B-1 in each, the first good bucket wins.
-// s is this warp's stage (Region<CPS>::kStage words). Returns 0 GOOD / 1 ZERO / 2 FAIL.
-template <int CPS, int NW>
-__device__ __forceinline__ int warp_sample_region(const uint32_t (&x)[NW], uint32_t dw,
-                                                  uint32_t W, uint32_t B, uint64_t flip_chk,
-                                                  uint32_t *s, uint64_t *idx) {
-  const uint32_t lane = threadIdx.x & 31;
-  const uint32_t d0 = __shfl_sync(kFull, dw, 0), d1 = __shfl_sync(kFull, dw, 1),
-                 d2 = __shfl_sync(kFull, dw, 2);
-  if ((d0 | d1 | d2) == 0) {
-    *idx = 0;
-    return 1;  // ZERO
-  }
-  if (bucket_good(d0, d1, d2, flip_chk)) {
-    *idx = ((uint64_t)d1 << 32) | d0;
-    return 0;  // GOOD
-  }
-  __syncwarp();
-#pragma unroll
-  for (int k = 0; k < NW; ++k) {
-    const uint32_t w = k * 32 + lane;
-    if (w < W) s[w] = x[k];
-  }
-  __syncwarp();
-  int res = 2;
-  *idx = 0;
-#pragma unroll
-  for (int c = 0; c < CPS && res == 2; ++c) {
-#pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      if ((uint32_t)q * 32 >= B || res != 2) break;
-      const uint32_t j = q * 32 + lane;
-      uint32_t a0 = 0, a1 = 0, a2 = 0;
-      if (j < B) {
-        const uint32_t *bk = s + 3 * (c * B + j);
-        a0 = bk[0];
-        a1 = bk[1];
-        a2 = bk[2];
-      }
-      const bool good = j < B && bucket_good(a0, a1, a2, flip_chk);
-      const uint32_t m = __ballot_sync(kFull, good);
-      if (m) {
-        const int src = __ffs(m) - 1;
-        const uint32_t x0 = __shfl_sync(kFull, a0, src);
-        const uint32_t x1 = __shfl_sync(kFull, a1, src);
-        *idx = ((uint64_t)x1 << 32) | x0;
-        res = 0;
-      }
-    }
-  }
-  return res;
-}
-
-// Sketch::sample of a region already in shared memory: s[0, 3 * CPS * B) the columns, det[0, 3)
-// the deterministic bucket (same scan order as warp_sample_region).
+// Sketch::sample (src/sketch.cpp:94-116) of a region in shared memory: s[0, 3 * CPS * B) the
+// columns, det[0, 3) the deterministic bucket; the deterministic bucket first, then columns
+// 0..CPS-1, depths 0..B-1 in each, the first good bucket wins (ballot + lowest lane). Returns 0
+// GOOD / 1 ZERO / 2 FAIL.
 template <int CPS>
 __device__ __forceinline__ int warp_sample_smem_split(const uint32_t *s, const uint32_t *det,
                                                       uint32_t B, uint64_t flip_chk, uint64_t *idx) {
@@ -426,25 +373,6 @@ template <int CPS>
 __device__ __forceinline__ int warp_sample_smem(const uint32_t *s, uint32_t W, uint32_t B,
                                                 uint64_t flip_chk, uint64_t *idx) {
   return warp_sample_smem_split<CPS>(s, s + W, B, flip_chk, idx);
-}
-
-// ---- asynchronous region copies (cp.async) ------------------------------------------------------
-// The query kernels keep many members' regions in flight per warp by copying them global ->
-// shared with cp.async (no registers held while a copy is outstanding), in commit groups of one
-// batch each; a warp waits for its oldest group, then reads the batch from shared memory.
-__device__ __forceinline__ void cp_async4(uint32_t *dst, const uint32_t *src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-// Copies region words [0, W) at src and the deterministic bucket at det to slot[0, W + 3).
-__device__ __forceinline__ void region_copy_async(uint32_t *slot, const uint32_t *src,
-                                                  const uint32_t *det, uint32_t W, uint32_t lane) {
-  for (uint32_t w = lane; w < W; w += 32) cp_async4(slot + w, src + w);
-  if (lane < 3) cp_async4(slot + W + lane, det + lane);
 }
 
 // ---- bulk-copied bucket runs (cp.async.bulk) -----------------------------------------------------
@@ -608,12 +536,6 @@ __device__ __forceinline__ int warp_sample(const uint32_t (&d)[3], const uint32_
   }
   *idx = 0;
   return 2;  // FAIL
-}
-
-__device__ __forceinline__ void load_bucket(const uint32_t *p, uint32_t (&x)[3]) {
-  x[0] = p[0];
-  x[1] = p[1];
-  x[2] = p[2];
 }
 
 
