@@ -557,7 +557,7 @@ def run_many_graphs(args):
         "e2e": ({"value": n / (max(e2e_ms) / 1e3), "unit": UNIT, "h2d_bytes_per_step": n * 9,
                  "d2h_bytes_per_step": int(Vs.sum()) * 4 + 12 * G,
                  "note": "pinned host records -> gz_batch_ingest -> "
-                         "gz_batch_connected_components with labels; wall clock, max of 3"}
+                         "gz_batch_connected_components with labels; wall clock, max of 3 after one untimed pass"}
                 if e2e_ms else None),
         "autotune": tune,
         "components_total": int(res.num_cc.sum()),
