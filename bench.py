@@ -302,10 +302,22 @@ def run_b200(args, cfg):
         e2e_s = [float("nan")]
     else:
         assert cc.size() == cfg["components"]
+    # the ceiling e2e works against: one plain pinned host -> HBM copy of the step's records
+    copy_ms = []
+    for _ in range(0 if args.no_e2e else 3):
+        c0, c1 = ev(), ev()
+        c0.record()
+        d_rec.copy_(pinned, non_blocking=True)
+        c1.record()
+        c1.synchronize()
+        copy_ms.append(c0.elapsed_time(c1))
     e2e = {"value": world * n / max(e2e_s), "unit": UNIT, "h2d_bytes_per_step": n * 9,
            "d2h_bytes_per_step": V * 4 + 4,
+           "h2d_copy_gbs": round(n * 9 / (min(copy_ms) * 1e6), 1) if copy_ms else None,
+           "copy_bound_value": world * n / (min(copy_ms) / 1e3) if copy_ms else None,
            "note": "pinned host records -> gz_ingest_records (pipelined H2D) -> "
-                   "gz_connected_components -> parent array on host; wall clock, max of steps"}
+                   "gz_connected_components -> parent array on host; wall clock, max of steps; "
+                   "copy_bound_value = updates/s of the records' plain host->device copy alone"}
 
     line = None
     if rank == 0:

@@ -396,8 +396,9 @@ def test_mixed_hashed_and_plain_chunks(gz, oracle_mod):
 
 
 def test_host_ingest_waves_match_device_ingest(gz, oracle_mod):
-    """4e7 host records cross a wave boundary (the gutter is folded into the sketches while later
-    records are still being copied); bytes must equal one device-resident ingest."""
+    """4e7 host records cross many wave boundaries (the gutter is folded into the sketches while
+    later records are still being copied; the call is cut into a doubling first chunk, full chunks
+    and a short last chunk); bytes must equal one device-resident ingest."""
     torch = pytest.importorskip("torch")
     from graphzeppelin_b200 import streams as S
     V = 1 << 14
