@@ -137,7 +137,9 @@ k_gutter_sort_scatter(const void *__restrict__ in, uint64_t n, GutterGeom g, uin
   uint32_t *s_dst = s_off + nb4;                         // run start inside the gutter
   const uint32_t ept = INPUT == kInputRecords ? 2 * rec_tile : rec_tile;
   uint2 *s_sorted = reinterpret_cast<uint2 *>(s_dst + nb4);
-  uint8_t *s_rec = reinterpret_cast<uint8_t *>(s_sorted + ept);
+  // the staged records share the sorted-entry area: they are parsed into registers before the
+  // first entry is placed, and the next tile is staged only after the write-out
+  uint8_t *s_rec = reinterpret_cast<uint8_t *>(s_sorted);
   const uint8_t *rec = reinterpret_cast<const uint8_t *>(in);
   const uint2 *ein = reinterpret_cast<const uint2 *>(in);
   const uint32_t per_thread = (nb + blockDim.x - 1) / blockDim.x;  // bins per thread (<= 4)
@@ -1480,8 +1482,8 @@ cudaError_t gutter_hash_scatter(const void *rec, uint64_t n, GutterGeom g, HashG
 uint32_t sort_scatter_tile(int input, GutterGeom g, size_t smem_budget) {
   const size_t fixed = (size_t)3 * ((g.nbins + 3) & ~3u) * 4 + 64;
   if (g.nbins > kSortBinsMax || fixed >= smem_budget) return 0;
-  const size_t per = input == kInputRecords ? 9 + 16 : 8;
-  size_t t = (smem_budget - fixed - (input == kInputRecords ? 48 : 0)) / per;
+  const size_t per = input == kInputRecords ? 16 : 8;  // records are staged in the entry area
+  size_t t = (smem_budget - fixed) / per;
   t = std::min<size_t>(t, input == kInputRecords ? 8192 : 16384);
   t &= ~(size_t)127;
   return (uint32_t)t;
@@ -1491,8 +1493,10 @@ cudaError_t gutter_sort_scatter(int input, const void *in, uint64_t n, GutterGeo
                                 uint32_t rec_tile, const uint64_t *base, uint32_t *fill,
                                 uint2 *entries, cudaStream_t s) {
   const size_t nb4 = (g.nbins + 3) & ~3u;
-  const size_t smem = 3 * nb4 * 4 + (size_t)rec_tile * (input == kInputRecords ? 16 : 8) +
-                      (input == kInputRecords ? (size_t)rec_tile * 9 + 48 : 0);
+  // records: 16 B of sorted entries per record, which also hold the 9 B staged record (plus the
+  // 16-byte alignment slack of the staging) as long as the tile has at least 7 records
+  const size_t smem = 3 * nb4 * 4 + (size_t)rec_tile * (input == kInputRecords ? 16 : 8);
+  if (input == kInputRecords && rec_tile < 7) return cudaErrorInvalidValue;
   const int G = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)num_sms(),
                                                                (n + rec_tile - 1) / rec_tile));
   if (input == kInputRecords) {
