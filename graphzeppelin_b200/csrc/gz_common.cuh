@@ -154,13 +154,18 @@ __device__ __forceinline__ void apply_entry(uint2 e, uint32_t *s_sk, uint32_t vm
   const uint32_t chk = hash_lo32(in64 ^ flip_chk);
   xor_bucket(sk + 3 * C * B, lo, hi, chk);
   uint32_t c = 0;
-  for (; c + 1 < C; c += 2) {
+  // four independent hash chains per step keep the integer pipes fed between dependent ops
+  for (; c + 3 < C; c += 4) {
     const uint32_t d0 = hash_depth(in64 ^ s_flip[c], B);
     const uint32_t d1 = hash_depth(in64 ^ s_flip[c + 1], B);
+    const uint32_t d2 = hash_depth(in64 ^ s_flip[c + 2], B);
+    const uint32_t d3 = hash_depth(in64 ^ s_flip[c + 3], B);
     if (d0 < B) xor_bucket(sk + 3 * (c * B + d0), lo, hi, chk);
     if (d1 < B) xor_bucket(sk + 3 * ((c + 1) * B + d1), lo, hi, chk);
+    if (d2 < B) xor_bucket(sk + 3 * ((c + 2) * B + d2), lo, hi, chk);
+    if (d3 < B) xor_bucket(sk + 3 * ((c + 3) * B + d3), lo, hi, chk);
   }
-  if (c < C) {
+  for (; c < C; ++c) {
     const uint32_t d = hash_depth(in64 ^ s_flip[c], B);
     if (d < B) xor_bucket(sk + 3 * (c * B + d), lo, hi, chk);
   }
