@@ -18,6 +18,7 @@
 #include "../../include/gz_b200.h"
 #include "gz_device.cuh"
 #include "gz_kernels.cuh"
+#include "gz_ingest_plan.h"
 
 namespace {
 
@@ -73,23 +74,8 @@ void host_free(T *&p) {
   p = nullptr;
 }
 
-constexpr uint64_t kStageRecords = 1ull << 24;  // records per host->device pipeline chunk
-constexpr int kStageBuffers = 4;                 // device staging buffers of the copy pipeline
-// Host-record ingest applies the gutter to the sketches whenever this many endpoint updates are
-// pending, so the sketch update of one wave runs while later records are still being copied.
-constexpr uint64_t kWaveEntries = 1ull << 26;
-// A long host-record call is cut so that the sketch update overlaps the copies from start to end:
-// the first chunk is kFirstChunk records and the chunks double up to kStageRecords, every chunk is
-// folded into the sketches as soon as it lands (a wave of its own), and the last chunk is
-// kLastChunk records, so little is left to sort and apply once the last copy has landed. A wave
-// re-reads and re-writes every vertex sketch it touches, so this shape is used only while all
-// sketches together are at most kShapeSketchBytes (a pass over them then costs a fraction of a
-// millisecond, and a chunk's sketch update keeps pace with the copy of the next); larger sketch
-// sets fold one wave per kWaveEntries endpoint updates.
-constexpr uint64_t kFirstChunk = 1ull << 23;
-constexpr uint64_t kLastChunk = 1ull << 23;
-constexpr uint64_t kShapeSketchBytes = 3ull << 29;
-static_assert(kFirstChunk <= kStageRecords && kLastChunk <= kStageRecords, "shaped chunks fit a stage");
+using gz::kStageBuffers;
+using gz::kStageRecords;
 constexpr uint64_t kEntStage = 1ull << 20;      // staged apply_update_batch entries per flush
 constexpr uint64_t kMaxChunkEntries = 1ull << 31;
 constexpr int kNumPhases = 3;  // gutter, sketch update, query
@@ -1232,7 +1218,8 @@ int gz_ingest_records(gz_alg_t *h, const void *rec, size_t n) {
     invalidate_answer(h);
   }
   if (n == 0) return GZ_OK;
-  const uint64_t chunk = std::min<uint64_t>(kStageRecords, n);
+  gz::IngestPlan plan(n, h->in_place, (uint64_t)h->V * h->sketch_bytes);
+  const uint64_t chunk = plan.chunk;
   const int nbuf = (int)std::min<uint64_t>(kStageBuffers, (n + chunk - 1) / chunk);
   if (chunk > h->stage_cap) {
     // staging buffers are sized for the largest chunk seen (small update batches stay small)
@@ -1255,15 +1242,9 @@ int gz_ingest_records(gz_alg_t *h, const void *rec, size_t n) {
     }
   }
   const uint8_t *src = static_cast<const uint8_t *>(rec);
-  const bool shaped = n > 2 * kStageRecords && !h->in_place &&
-                      (uint64_t)h->V * h->sketch_bytes <= kShapeSketchBytes;
-  uint64_t ramp = shaped ? std::min(kFirstChunk, chunk) : chunk;
   int buf = 0;
   for (uint64_t off = 0, m = 0; off < n; off += m, buf = (buf + 1) % nbuf) {
-    const uint64_t left = n - off;
-    m = std::min(ramp, left);
-    if (shaped && left > kLastChunk && left - m < kLastChunk) m = left - kLastChunk;
-    ramp = std::min(2 * ramp, chunk);
+    m = plan.next(off);
     GZ_CUDA(cudaStreamWaitEvent(h->copy_stream, h->ev_free[buf], 0));
     GZ_CUDA(cudaMemcpyAsync(h->d_stage[buf], src + off * 9, m * 9, cudaMemcpyHostToDevice, h->copy_stream));
     GZ_CUDA(cudaEventRecord(h->ev_copied[buf], h->copy_stream));
@@ -1271,7 +1252,7 @@ int gz_ingest_records(gz_alg_t *h, const void *rec, size_t n) {
     GZ_TRY(gutter_chunk(h, gz::kInputRecords, h->d_stage[buf], m));
     GZ_CUDA(cudaEventRecord(h->ev_free[buf], h->stream));
     // fold a wave into the sketches while the copy engine keeps streaming records
-    if (off + m < n && (shaped || h->entries_pending >= kWaveEntries)) GZ_TRY(apply_pending(h));
+    if (plan.wave_after(off + m, h->entries_pending)) GZ_TRY(apply_pending(h));
   }
   // the caller's buffer may be reused once every copy has landed
   GZ_CUDA(cudaStreamSynchronize(h->copy_stream));
