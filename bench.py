@@ -113,24 +113,28 @@ class ClockSampler:
 # ------------------------------------------------------------------------------------------------
 # CPU baseline: the reference's CCSketchAlg on the host cores
 # ------------------------------------------------------------------------------------------------
-def cpu_reference_run(stream, cfg, n_records: int, threads: int, timeout=600):
-    """Ingest the first n_records through oracle/_ref/gz_ref_eager (reference sources, default
-    eager-DSU build, stand-in gutter) and return its JSON (ingest_s, query_s, ...)."""
+def cpu_reference_run(stream, cfg, n_records: int, threads: int, timeout=600, path=None,
+                      eager=True, dump_path=None, labels_path=None):
+    """Ingest the first n_records through the reference's CCSketchAlg compiled from its sources
+    (oracle/_ref: gz_ref_eager = the default eager-DSU build, timed as the baseline;
+    gz_ref_noeager = the -DNO_EAGER_DSU build whose query always runs Boruvka) with the stand-in
+    gutter, and return its JSON (ingest_s, query_s, num_cc, rounds, ...). `path`: the stream
+    already written to a file."""
     from oracle import oracle as O
-    if not O.have_reference():
-        try:
-            O.build()
-        except Exception:
-            pass
     from graphzeppelin_b200 import streams as S
-    with tempfile.TemporaryDirectory() as td:
-        p = os.path.join(td, "sample.gzs")
-        S.Stream(stream.num_vertices, stream.records[:n_records]).write(p)
-        if O.have_reference():
-            r = O.ref_ingest(p, cfg["sketch_seed"], 1.0, threads=threads, eager=True,
+    if O.have_reference():
+        with tempfile.TemporaryDirectory() as td:
+            if path is None:
+                path = os.path.join(td, "sample.gzs")
+                S.Stream(stream.num_vertices, stream.records[:n_records]).write(path)
+                n_arg = 0
+            else:
+                n_arg = n_records if n_records < stream.num_updates else 0
+            r = O.ref_ingest(path, cfg["sketch_seed"], 1.0, threads=threads, eager=eager,
+                             max_records=n_arg, dump_path=dump_path, labels_path=labels_path,
                              timeout=timeout)
-            r["kind"] = "reference"
-            return r
+        r["kind"] = "reference"
+        return r
     # the compiled reference is unavailable: time the C restatement (single thread)
     osk = O.OracleSketches(stream.num_vertices, cfg["sketch_seed"])
     t0 = time.perf_counter()
@@ -142,46 +146,113 @@ def cpu_reference_run(stream, cfg, n_records: int, threads: int, timeout=600):
             "updates": n_records, "rounds": rounds}
 
 
-def cpu_baseline(stream, cfg, target_s=12.0):
-    threads = os.cpu_count() or 1
-    n_total = stream.num_updates
-    cal = min(n_total, 1 << 21)
-    r = cpu_reference_run(stream, cfg, cal, threads)
-    rate = cal / max(r["ingest_s"] + r["query_s"], 1e-9)
-    n = int(min(n_total, max(cal, rate * target_s)))
-    if n > cal:
-        r = cpu_reference_run(stream, cfg, n, threads)
-    value = n / (r["ingest_s"] + r["query_s"])
-    return {"value": value, "unit": UNIT, "cores": int(r.get("threads", threads)),
-            "kind": r["kind"],
-            "sample": f"first {n} of {n_total} records of the same stream "
-                      f"(ingest {r['ingest_s']:.3f} s + query {r['query_s']:.3f} s, "
-                      f"{r.get('num_cc', '?')} components on the prefix)",
-            "ingest_updates_per_s": n / r["ingest_s"], "query_ms": r["query_s"] * 1e3}
+def sha256_file(path):
+    import hashlib
+    h = hashlib.sha256()
+    with open(path, "rb") as f:
+        for blk in iter(lambda: f.read(1 << 24), b""):
+            h.update(blk)
+    return h.hexdigest()
+
+
+def cpu_baseline_and_parity(alg, stream, cfg, cc, threads=None):
+    """The reference on the host cores over the whole stream, twice: the default eager-DSU
+    build timed (the CPU baseline), and the -DNO_EAGER_DSU build (whose query runs Boruvka) for
+    parity. Parity: the GPU's write_binary file against the reference's (SHA-256; the format of
+    src/cc_sketch_alg.cpp:614-623), the partition and the Boruvka rounds against the reference's
+    connected_components (src/cc_sketch_alg.cpp:515-557), and the partition against an exact
+    union-find over the stream's final edge set."""
+    import numpy as np
+    from oracle import oracle as O
+    threads = threads or os.cpu_count() or 1
+    n = stream.num_updates
+    V = stream.num_vertices
+    with tempfile.TemporaryDirectory() as td:
+        spath = os.path.join(td, "stream.gzs")
+        stream.write(spath)
+        r = cpu_reference_run(stream, cfg, n, threads, path=spath, eager=True)
+        value = n / (r["ingest_s"] + r["query_s"])
+        cpu = {"value": value, "unit": UNIT, "cores": int(r.get("threads", threads)),
+               "kind": r["kind"],
+               "sample": f"all {n} records of the same stream (ingest {r['ingest_s']:.3f} s + "
+                         f"query {r['query_s']:.3f} s, {r.get('num_cc', '?')} components)",
+               "ingest_updates_per_s": n / r["ingest_s"], "query_ms": r["query_s"] * 1e3}
+        parity = {"reference": "unavailable"}
+        if r["kind"] == "reference":
+            gpath, rdump, rlab = (os.path.join(td, x) for x in ("gpu.bin", "ref.bin", "ref.labels"))
+            alg.write_binary(gpath)
+            ref = cpu_reference_run(stream, cfg, n, threads, path=spath, eager=False,
+                                    dump_path=rdump, labels_path=rlab)
+            gsha, rsha = sha256_file(gpath), sha256_file(rdump)
+            labels = cc.canonical_labels()
+            rlabels = np.fromfile(rlab, np.uint32)
+            n_exact, exact = O.exact_cc_mt(V, stream.raw(), threads)
+            parity = {
+                "sketch_sha256_equal": gsha == rsha, "partition_equal": bool((labels == rlabels).all()),
+                "rounds_equal": int(alg.last_query_rounds) == int(ref["rounds"]),
+                "exact_partition_equal": bool((labels == exact).all()),
+                "components": {"gpu": cc.size(), "reference": int(ref["num_cc"]), "exact": n_exact},
+                "rounds": {"gpu": int(alg.last_query_rounds), "reference": int(ref["rounds"])},
+                "sketch_sha256": gsha,
+                "reference": "reference CCSketchAlg compiled from its sources (-DNO_EAGER_DSU) on "
+                             "the whole stream; exact union-find over the final edge set"}
+    return cpu, parity
 
 
 # ------------------------------------------------------------------------------------------------
-def roofline_terms(alg, n_records, t_launch_s, hash_peak, hbm_peak_gbs, update_peak):
+def roofline(alg, n, prof, steps, ingest_ms, hash_peak, hbm_peak_gbs, update_peak):
+    """Roofline of the ingest (one pass of the hot path over the step's records) per the
+    algorithmic work of one record: 1 + C XXH3 hashes (one per column and the checksum, hashed
+    once per edge), 9 B of stream read, and the touched sketches read and written once. The path
+    is bound by the slower of the hash term (over the measured hash rate) and the HBM term.
+    Per kernel: the gutter phase (count + hash sort-scatter) against its own hashes (C per
+    record) and bytes, the sketch update against the shared-memory slot rate (2 (C + 1) bucket
+    updates per record, made as 2 x 32 slot steps) and its bytes."""
     p = alg.params
-    V, C, sb = p.num_vertices, p.num_columns, p.sketch_bytes
-    entries = 2 * n_records
-    # sketch-update kernel (plain entries): reads every gutter entry (8 B) once, reads + writes
-    # every touched sketch once; evaluates 1 + C hashes and XORs 1 + C buckets (3 shared-memory
-    # atomics each) per endpoint update
-    bytes_alg = entries * 8 + 2 * V * sb
-    hashes = entries * (C + 1)
-    updates = entries * (C + 1)
-    t = {"hbm": bytes_alg / (hbm_peak_gbs * 1e9), "int": hashes / hash_peak,
-         "smem_atomic": updates / update_peak}
-    hbm = {"achieved": bytes_alg / t_launch_s / 1e9, "peak": hbm_peak_gbs, "unit": "GB/s",
-           "frac": (bytes_alg / t_launch_s / 1e9) / hbm_peak_gbs, "bytes_per_launch": bytes_alg}
-    integer = {"achieved": hashes / t_launch_s / 1e9, "peak": hash_peak / 1e9, "unit": "Ghash/s",
-               "frac": (hashes / t_launch_s) / hash_peak, "hashes_per_launch": hashes}
-    smem = {"achieved": updates / t_launch_s / 1e9, "peak": update_peak / 1e9,
-            "unit": "Gupdate/s", "frac": (updates / t_launch_s) / update_peak,
-            "bucket_updates_per_launch": updates}
-    bound = max(t, key=t.get)
-    return {"hbm": hbm, "int": integer, "smem_atomic": smem}, bound
+    V, C, B, sb = p.num_vertices, p.num_columns, p.bkt_per_col, p.sketch_bytes
+    t_ing = statistics.mean(ingest_ms) / 1e3
+    hashes = n * (C + 1)
+    path_bytes = 9 * n + 2 * V * sb
+    t_hash, t_hbm = hashes / hash_peak, path_bytes / (hbm_peak_gbs * 1e9)
+    bound = "int" if t_hash >= t_hbm else "hbm"
+    kernels = {}
+    t_g = prof["gutter_ms"] / max(1, prof["gutter_launches"]) / 1e3
+    t_u = prof["sketch_update_ms"] / max(1, prof["sketch_update_launches"]) / 1e3
+    if p.entry_form == 2:
+        g_bytes = 9 * n + 9 * n + 2 * n * 24
+        kernels["gutter"] = {
+            "kernels": "k_gutter (count) + k_hash_sort_scatter", "launch_ms": t_g * 1e3,
+            "bound": "int", "hashes_per_launch": n * C,
+            "int": {"achieved": n * C / t_g / 1e9, "peak": hash_peak / 1e9, "unit": "Ghash/s",
+                    "frac": n * C / t_g / hash_peak},
+            "hbm": {"achieved": g_bytes / t_g / 1e9, "peak": hbm_peak_gbs, "unit": "GB/s",
+                    "frac": g_bytes / t_g / 1e9 / hbm_peak_gbs, "bytes_per_launch": g_bytes}}
+        rows = min(B, 11)
+        u_bytes = 2 * n * 24 + 2 * V * 12 * (C * rows + 1)
+        slots = 2 * n * 32
+        kernels["sketch_update"] = {
+            "kernels": "k_plane_update", "launch_ms": t_u * 1e3, "bound": "smem",
+            "bucket_updates_per_launch": 2 * n * (C + 1), "slot_steps_per_launch": slots,
+            "smem": {"achieved": slots / t_u / 1e9, "peak": update_peak / 1e9,
+                     "unit": "Gslot/s", "frac": slots / t_u / update_peak,
+                     "useful_frac": 2 * n * (C + 1) / t_u / update_peak},
+            "hbm": {"achieved": u_bytes / t_u / 1e9, "peak": hbm_peak_gbs, "unit": "GB/s",
+                    "frac": u_bytes / t_u / 1e9 / hbm_peak_gbs, "bytes_per_launch": u_bytes}}
+    else:
+        kernels["gutter"] = {"kernels": "k_gutter (count) + k_gutter_sort_scatter", "launch_ms": t_g * 1e3}
+        kernels["sketch_update"] = {"kernels": "k_sketch_update (staged tiles, hashed per endpoint)",
+                                    "launch_ms": t_u * 1e3, "hashes_per_launch": 2 * n * (C + 1),
+                                    "int": {"achieved": 2 * n * (C + 1) / t_u / 1e9,
+                                            "frac": 2 * n * (C + 1) / t_u / hash_peak}}
+    achieved = hashes / t_ing if bound == "int" else path_bytes / t_ing
+    peak = hash_peak if bound == "int" else hbm_peak_gbs * 1e9
+    return {"bound": bound, "achieved": achieved / 1e9, "peak": peak / 1e9,
+            "unit": "Ghash/s" if bound == "int" else "GB/s", "frac": achieved / peak,
+            "kernel": "ingest = " + " + ".join(k["kernels"] for k in kernels.values()),
+            "launch_ms": t_ing * 1e3,
+            "units_per_launch": {"records": n, "hashes": hashes, "bytes": path_bytes},
+            "terms_ms": {"int": t_hash * 1e3, "hbm": t_hbm * 1e3},
+            "kernels": kernels}
 
 
 def load_traffic(workload):
@@ -330,37 +401,18 @@ def run_b200(args, cfg):
             peak_src = "fallback 6546.2 GB/s"
         hash_peak = gzcc.measure_hash_rate(5)
         update_peak = gzcc.measure_update_rate(5)
-        launches = max(1, prof["sketch_update_launches"])
-        t_launch = prof["sketch_update_ms"] / launches / 1e3
-        terms, bound = roofline_terms(alg, n, t_launch, hash_peak, hbm_peak, update_peak)
-        main = terms[bound]
-        traffic = load_traffic(cfg["workload"])
-        roof = {"bound": bound, "achieved": main["achieved"], "peak": main["peak"],
-                "unit": main["unit"], "frac": main["frac"], "traffic": traffic,
-                "kernel": "k_sketch_update",
-                "launch_ms": t_launch * 1e3,
-                "terms": terms,
-                "peaks": {"hbm": peak_src,
-                          "int": "measured here: gz_measure_hash_rate (register-only XXH3-8B + "
-                                 "depth ctz kernel, best of 5)",
-                          "smem_atomic": "measured here: gz_measure_update_rate (3 x 32-bit "
-                                         "shared atomicXor per random 12-byte bucket, 1024 "
-                                         "threads/SM, best of 5)"}}
-        # the whole ingest (gutter + sketch update) against the path roofline: 9 B read per
-        # record + sketch RMW, 1 + C hashes per record (one hash per edge)
+        roof = roofline(alg, n, prof, args.steps, ingest_ms, hash_peak, hbm_peak, update_peak)
+        roof["traffic"] = load_traffic(cfg["workload"])
+        roof["peaks"] = {"hbm": peak_src,
+                         "int": "measured here: gz_measure_hash_rate (register-only per-column "
+                                "XXH3-8B of premixed input and seed + depth ctz, best of 5)",
+                         "smem": "measured here: gz_measure_update_rate (bucket-plane slot "
+                                 "steps, two conflict-free red.shared.xor each, best of 5)"}
         p = alg.params
-        ing_s = statistics.mean(ingest_ms) / 1e3
-        path_bytes = 9 * n + 2 * V * p.sketch_bytes
-        path_hashes = n * (p.num_columns + 1)
-        path_updates = 2 * n * (p.num_columns + 1)
-        path_terms = {"hbm_ms": path_bytes / (hbm_peak * 1e9) * 1e3,
-                      "int_ms": path_hashes / hash_peak * 1e3,
-                      "smem_atomic_ms": path_updates / update_peak * 1e3}
-        path_t = max(path_bytes / (hbm_peak * 1e9), path_hashes / hash_peak)
-        cpu = None
+        cpu, parity = None, None
         if world == 1 and not args.no_cpu_baseline:
-            log("[rank 0] timing the CPU reference baseline ...")
-            cpu = cpu_baseline(stream, cfg)
+            log("[rank 0] timing the CPU reference baseline and checking full-size parity ...")
+            cpu, parity = cpu_baseline_and_parity(alg, stream, cfg, cc)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
@@ -369,18 +421,15 @@ def run_b200(args, cfg):
             "config": {"workload": cfg["workload"], "num_vertices": V, "num_updates": n,
                        "components": cfg["components"], "num_columns": p.num_columns,
                        "bkt_per_col": p.bkt_per_col, "sketch_bytes_total": V * p.sketch_bytes,
+                       "entry_form": "coded (each record hashed once), bucket planes"
+                       if p.entry_form == 2 else "plain (hashed per endpoint), staged tiles",
                        "stream_seed": cfg["stream_seed"], "sketch_seed": cfg["sketch_seed"],
                        "l2": "inputs larger than L2: 1.26 GB records + 1.29 GB sketches per step",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
             "query_ms": statistics.mean(query_ms),
             "ingest_ms": statistics.mean(ingest_ms),
-            "ingest_updates_per_s": n / ing_s,
-            "path_roofline": {"time_ms": path_t * 1e3, "frac": path_t / ing_s,
-                              "bytes": path_bytes, "hashes": path_hashes,
-                              "definition": "max(9 B/record + sketch RMW over HBM, one hash "
-                                            "per record per column over the hash peak)",
-                              "terms_ms": path_terms,
-                              "frac_with_smem_term": max(path_terms.values()) / 1e3 / ing_s},
+            "ingest_updates_per_s": n / (statistics.mean(ingest_ms) / 1e3),
+            "parity": parity,
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": e2e,
@@ -405,14 +454,14 @@ def run_reference(args, cfg):
     stream, _ = gen_stream(cfg)
     n_total = stream.num_updates
     threads = os.cpu_count() or 1
-    # size one step to a few seconds of reference work
-    cal = min(n_total, 1 << 21)
-    r = cpu_reference_run(stream, cfg, cal, threads)
-    rate = cal / max(r["ingest_s"] + r["query_s"], 1e-9)
-    n = int(min(n_total, max(cal, rate * 4.0)))
-    for _ in range(args.warmup):
-        cpu_reference_run(stream, cfg, n, threads)
-    runs = [cpu_reference_run(stream, cfg, n, threads) for _ in range(args.steps)]
+    # every step ingests the whole stream and answers the query, as the GPU arm's step does
+    n = n_total
+    with tempfile.TemporaryDirectory() as td:
+        spath = os.path.join(td, "stream.gzs")
+        stream.write(spath)
+        for _ in range(args.warmup):
+            cpu_reference_run(stream, cfg, n, threads, path=spath)
+        runs = [cpu_reference_run(stream, cfg, n, threads, path=spath) for _ in range(args.steps)]
     total = sum(x["ingest_s"] + x["query_s"] for x in runs)
     value = n * args.steps / total
     kind = runs[0]["kind"]
@@ -422,14 +471,14 @@ def run_reference(args, cfg):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
         "data": "synthetic (seeded planted-partition stream, C generator)",
         "config": {"workload": cfg["workload"], "num_vertices": cfg["num_vertices"],
-                   "num_updates": n_total, "sample_records": n,
+                   "num_updates": n_total,
                    "parallelism": f"{runs[0].get('threads', threads)} host threads"},
         "impl": "reference",
         "query_ms": statistics.mean(x["query_s"] for x in runs) * 1e3,
         "ingest_updates_per_s": n / statistics.mean(x["ingest_s"] for x in runs),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": int(runs[0].get("threads", threads)),
                          "kind": kind,
-                         "sample": f"first {n} of {n_total} records per step "
+                         "sample": f"all {n} records of the stream per step, then the query "
                                    f"(reference CCSketchAlg, eager DSU, stand-in gutter)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }

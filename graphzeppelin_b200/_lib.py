@@ -37,7 +37,7 @@ class gz_params_t(ctypes.Structure):
                 ("vertices_per_tile", ctypes.c_uint32), ("num_tiles", ctypes.c_uint32),
                 ("vertices_per_bin", ctypes.c_uint32), ("num_bins", ctypes.c_uint32),
                 ("cols_per_sample", ctypes.c_uint32), ("sketch_algorithm", ctypes.c_uint32),
-                ("in_place", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+                ("in_place", ctypes.c_uint32), ("entry_form", ctypes.c_uint32)]
 
 
 class gz_trace_rec_t(ctypes.Structure):

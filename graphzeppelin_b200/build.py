@@ -16,7 +16,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libgz_b200.so")
 GEN_LIB = os.path.join(PKG, "libgz_gen.so")
-SOURCES = ["gz_kernels.cu", "gz_capi.cu", "gz_noalloc.cu", "gz_batch.cu"]
+SOURCES = ["gz_kernels.cu", "gz_planes.cu", "gz_capi.cu", "gz_noalloc.cu", "gz_batch.cu"]
 HEADERS = ["gz_device.cuh", "gz_kernels.cuh", "gz_common.cuh", "gz_ingest_plan.h", os.path.join("..", "..", "include", "gz_b200.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -1375,7 +1375,7 @@ int batch_ingest(gz_batch *h, const void *d_rec, const uint64_t *off) {
     MB_CUDA(cudaMemsetAsync(h->d_bin_fill, 0, sizeof(uint32_t) * h->total_bins, h->stream));
     MB_CUDA(cudaMemsetAsync(h->d_wl_len, 0, sizeof(uint32_t), h->stream));
     {
-      MB_CUDA(cudaFuncSetAttribute(k_mb_count, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMbCountSmem));
+      MB_CUDA(smem_optin(k_mb_count));
       int per_sm = 1;
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mb_count, 1024, kMbCountSmem);
       const unsigned grid = (unsigned)std::min<uint64_t>(n_rt_dense, (uint64_t)num_sms() * std::max(per_sm, 1));
@@ -1391,7 +1391,7 @@ int batch_ingest(gz_batch *h, const void *d_rec, const uint64_t *off) {
                                                                        h->d_bin_off);
     h->launches++;
     {
-      MB_CUDA(cudaFuncSetAttribute(k_mb_sort_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMbSortSmem));
+      MB_CUDA(smem_optin(k_mb_sort_scatter));
       const unsigned grid = (unsigned)std::min<uint64_t>(n_rt_dense, (uint64_t)num_sms());
       k_mb_sort_scatter<<<grid, 1024, kMbSortSmem, h->stream>>>(rec, h->d_rtiles, n_rt_dense, h->d_graphs,
                                                                 h->d_bins, h->d_bin_fill, h->d_entries);
@@ -1410,7 +1410,7 @@ int batch_ingest(gz_batch *h, const void *d_rec, const uint64_t *off) {
     const uint32_t tile_stride = (h->max_tile_bytes + 127) & ~127u;
     const uint32_t flip_stride = ((h->max_C + 2) & ~1u) * 8;
     const size_t ksmem = 2 * (size_t)tile_stride + 2 * (size_t)flip_stride + (size_t)(h->threads / 32) * 256;
-    MB_CUDA(cudaFuncSetAttribute(k_mb_sketch_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ksmem));
+    MB_CUDA(smem_optin(k_mb_sketch_update));
     int per_sm = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mb_sketch_update, (int)h->threads, ksmem);
     const int grid = (int)std::min<uint64_t>(h->total_tiles, (uint64_t)num_sms() * std::max(per_sm, 1));
@@ -1421,7 +1421,7 @@ int batch_ingest(gz_batch *h, const void *d_rec, const uint64_t *off) {
     MB_CUDA(cudaGetLastError());
   }
   if (!rt_sparse.empty()) {
-    MB_CUDA(cudaFuncSetAttribute(k_mb_direct, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMbDirectSmem));
+    MB_CUDA(smem_optin(k_mb_direct));
     int per_sm = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mb_direct, 512, kMbDirectSmem);
     const unsigned grid = (unsigned)std::min<uint64_t>(rt_sparse.size(), (uint64_t)num_sms() * std::max(per_sm, 1));
@@ -1494,7 +1494,7 @@ int enqueue_round(gz_batch *h, cudaStream_t s) {
   k_mb_group<<<cdiv(V, 256), 256, 0, s>>>(b);
   const uint64_t warps = (V + kMbSpan - 1) / kMbSpan;
   const size_t smem = mb_query_smem(b.acc_words);
-  MB_CUDA(cudaFuncSetAttribute(k_mb_merge, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  MB_CUDA(smem_optin(k_mb_merge));
   k_mb_merge<<<cdiv(warps * 32, 256), 256, smem, s>>>(b);
   k_mb_reduce_parts<<<cdiv(warps, 256), 256, 0, s>>>(b, (uint32_t)warps);
   k_mb_sample_spanning<<<std::min<unsigned>(cdiv(V * 32, 256), num_sms() * 16), 256, 0, s>>>(b);
@@ -1524,7 +1524,7 @@ int batch_query(gz_batch *h, uint32_t *labels_out) {
   MB_CUDA(cudaMemsetAsync(h->d_modified, 0, sizeof(uint32_t) * G, h->stream));
   {
     const size_t smem = mb_query_smem(b.acc_words);
-    MB_CUDA(cudaFuncSetAttribute(k_mb_round0, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    MB_CUDA(smem_optin(k_mb_round0));
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mb_round0, 256, smem) != cudaSuccess || per_sm < 1)
       per_sm = 1;

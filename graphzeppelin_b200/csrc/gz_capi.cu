@@ -137,7 +137,7 @@ struct gz_alg {
   uint32_t *d_status = nullptr;  // [0] status bits, [1] work counter
   uint32_t *h_status = nullptr;  // pinned mirror
   // device gutter
-  uint8_t *d_gutter = nullptr;  // chunks of plain (8 B) or hashed (32 B) endpoint entries
+  uint8_t *d_gutter = nullptr;  // chunks of plain (8 B) or coded (8 B key + 16 B codes) entries
   uint64_t entry_cap = 0;       // capacity in endpoint updates
   uint64_t gutter_bytes = 0, gutter_used = 0, entries_pending = 0;
   double direct_factor = 1.0;   // scales the in-place threshold of sparse tiles (0 = never)
@@ -148,10 +148,10 @@ struct gz_alg {
   // every update so far reached both endpoints' sketches (records, gz_update): the XOR of all
   // vertex sketches is zero, which lets a query merge its largest component from the rest
   bool symmetric = true;
-  bool hashed = false;          // records become hashed entries (each edge hashed once)
-  bool hashed_default = false;
-  uint32_t *d_hist2d = nullptr;
-  size_t hist2d_words = 0;
+  // records become coded entries (each record hashed once) applied through bucket planes
+  bool planes = false;
+  int planes_mode = -1;         // entry form asked for: -1 automatic, 0 plain, 1 coded
+  gz::PlaneHash ph{};
   gz::ChunkTable chunks{};
   int nchunks = 0;
   uint32_t *d_bin_off = nullptr;
@@ -236,13 +236,30 @@ struct gz_alg {
     // Staging a tile moves its sketches twice (bulk load + write-back); updating it in place
     // costs about C + 1 bucket sectors read and written per entry. Below the break-even entry
     // count a tile goes in place (one tile per bin and plain CameoSketch entries only).
-    if (bin_shift == tile_shift && !cube && !hashed) {
+    if (bin_shift == tile_shift && !cube && !planes) {
       const double even = (double)((uint64_t)nb * 12 << tile_shift) / (32.0 * (C + 1));
       g.direct_max = (uint32_t)std::min(even * direct_factor, 4.0e9);
     }
     return g;
   }
   gz::GutterGeom ggeom() const { return gz::GutterGeom{V, bin_shift, nbins}; }
+  gz::PlaneGeom pgeom() const {
+    gz::PlaneGeom g;
+    g.V = V;
+    g.C = C;
+    g.B = B;
+    g.sketch_words = nb * 3;
+    g.tile_shift = tile_shift;
+    g.ntiles = ntiles;
+    // A tile through the planes costs its write-back, about 2 x 12 x (C min(B, rows) + 1) bytes
+    // per vertex read and written; in place an entry costs its C + 1 buckets' sectors, each read
+    // and written by an L2 atomic. Below the break-even entry count a tile goes in place.
+    const double wb = 24.0 * ((double)C * std::min<uint32_t>(B, gz::kPlaneRows - 1) + 1) *
+                      (double)(1u << tile_shift);
+    const double even = wb / (64.0 * (C + 1));
+    g.direct_max = (uint32_t)std::min(even * direct_factor, 4.0e9);
+    return g;
+  }
   gz::BoruvkaGeom bgeom() const {
     gz::BoruvkaGeom g;
     g.V = V;
@@ -320,12 +337,59 @@ bool want_pipe(const gz_alg *h) {
   return h->V > (1u << 18);
 }
 
+// Coded entries and bucket planes by default: CameoSketch of at most 31 columns whose gutter bins
+// of 32 vertices fit the shared-memory sort (up to 2^18 vertices). Larger graphs keep the
+// pipelined staged update.
+bool planes_possible(const gz_alg *h, uint32_t shift) {
+  return !h->cube && h->C <= gz::kPlaneMaxColumns &&
+         ((h->V + (1u << shift) - 1) >> shift) <= gz::kSortBinsMax;
+}
+
+int choose_planes(gz_alg *h, uint32_t vpt_req, uint32_t threads_req, uint32_t tpb_req, bool &done) {
+  done = false;
+  const bool asked = h->planes_mode == 1;
+  if (h->planes_mode == 0) return GZ_OK;
+  if (h->cube || h->C > gz::kPlaneMaxColumns) {
+    if (asked) return fail(GZ_ERR_INVALID, "coded entries need CameoSketch with at most 31 columns");
+    return GZ_OK;
+  }
+  if (tpb_req > 1 || (vpt_req && (vpt_req < 4 || (vpt_req & (vpt_req - 1)) || vpt_req > gz::kPlaneMaxTile))) {
+    if (asked) return fail(GZ_ERR_INVALID, "coded entries take one tile per bin of 4 to 32 vertices");
+    return GZ_OK;
+  }
+  const uint32_t shift = vpt_req ? (uint32_t)__builtin_ctz(vpt_req) : 5;
+  if (!planes_possible(h, shift)) {
+    if (asked) return fail(GZ_ERR_INVALID, "too many gutter bins for coded entries at this tile size");
+    return GZ_OK;
+  }
+  uint32_t threads = threads_req ? threads_req : 1024;
+  if (threads_req && (threads_req < 64 || threads_req > 1024 || threads_req % 32))
+    return fail(GZ_ERR_INVALID, "threads_per_block must be a multiple of 32 in [64, 1024]");
+  if (gz::plane_update_smem(shift, (int)threads) > h->smem_optin)
+    return fail(GZ_ERR_INVALID, "this tile does not fit in shared memory");
+  h->planes = true;
+  h->in_place = false;
+  h->pipe = false;
+  h->threads = threads;
+  h->tile_shift = h->bin_shift = shift;
+  h->ntiles = h->nbins = (uint32_t)((h->V + (1u << shift) - 1) >> shift);
+  done = true;
+  return GZ_OK;
+}
+
 int choose_tiling(gz_alg *h, uint32_t vpt_req, uint32_t threads_req, uint32_t tpb_req) {
   int dev = h->device;
   int smem_optin = 0;
   cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   if (smem_optin <= 0) smem_optin = 227 * 1024;
   h->smem_optin = (size_t)smem_optin;
+  h->planes = false;
+  h->threads = 1024;
+  {
+    bool done = false;
+    GZ_TRY(choose_planes(h, vpt_req, threads_req, tpb_req, done));
+    if (done) return GZ_OK;
+  }
   const size_t budget = (size_t)smem_optin - 64 - gz::kQueueBytes;
   const size_t flip_bytes = (size_t)(h->C + 1) * 8;
   uint32_t shift;
@@ -350,7 +414,7 @@ int choose_tiling(gz_alg *h, uint32_t vpt_req, uint32_t threads_req, uint32_t tp
   }
   // two-buffer pipeline: two tiles (one bin each) and the hash constants in shared memory
   h->pipe = false;
-  if (!h->in_place && !h->hashed && !h->cube && !tpb_req && want_pipe(h)) {
+  if (!h->in_place && !h->cube && !tpb_req && want_pipe(h)) {
     const size_t room = (size_t)smem_optin - 1024 - (((size_t)h->C + 2) & ~(size_t)1) * 8;
     // the most buffers asked for (or kPipeBuffers) that hold tiles of at least 4 vertices
     for (uint32_t nb = h->pipe_mode >= 2 ? (uint32_t)h->pipe_mode : kPipeBuffers; nb >= 2 && !h->pipe; --nb) {
@@ -372,7 +436,7 @@ int choose_tiling(gz_alg *h, uint32_t vpt_req, uint32_t threads_req, uint32_t tp
     if (tpb_req & (tpb_req - 1) || tpb_req > 64)
       return fail(GZ_ERR_INVALID, "tiles_per_bin must be a power of two <= 64");
     bshift = shift + (uint32_t)__builtin_ctz(tpb_req);
-  } else if (!h->hashed) {
+  } else {
     while (((h->V + (1u << bshift) - 1) >> bshift) > kBinTarget &&
            (1u << (bshift - shift)) < kMaxTilesPerBin)
       ++bshift;
@@ -380,7 +444,7 @@ int choose_tiling(gz_alg *h, uint32_t vpt_req, uint32_t threads_req, uint32_t tp
     // (measured at 2^20 vertices: 16 tiles per bin cost 9.1 ms per 1.3e7 records against 6.3 ms
     // for one tile per bin, whose scatter uses global cursors and costs 0.25 ms more).
     if (bshift - shift > 2) bshift = shift;
-  }  // hashed entries are full 32-byte sectors: one bin per tile, no compaction pass needed
+  }
   h->bin_shift = bshift;
   h->nbins = (uint32_t)((h->V + (1u << bshift) - 1) >> bshift);
   if (threads_req) {
@@ -405,9 +469,8 @@ int init_alg(gz_alg *h, uint32_t V, uint64_t seed, double sf, double bf, bool cu
   gz::sketch_sizing_alg(V, h->sketches_factor, cube, h->samples, h->cps, h->B);
   h->C = h->samples * h->cps;
   if (h->B > 63) return fail(GZ_ERR_INVALID, "bkt_per_col above 63 is not supported");
-  h->hashed_default = false;  // plain entries measured faster on B200 (see the design notes)
-  h->hashed = h->hashed_default;
   h->nb = h->C * h->B + 1;
+  h->ph = gz::plane_hash(seed, h->C, h->B);
   h->sketch_bytes = (uint64_t)h->nb * gz::kBucketBytes;
   {
     size_t num = h->sketch_bytes / sizeof(uint32_t);
@@ -450,7 +513,6 @@ void destroy_alg(gz_alg *h) {
   dev_free(h->d_status);
   host_free(h->h_status);
   dev_free(h->d_gutter);
-  dev_free(h->d_hist2d);
   dev_free(h->d_bin_off);
   dev_free(h->d_hist);
   dev_free(h->d_scan_tmp);
@@ -506,13 +568,16 @@ void destroy_alg(gz_alg *h) {
 
 // ---- device gutter -------------------------------------------------------------------------------
 
+// Gutter bytes per endpoint entry: 8 B keys, plus 16 B of depth codes for records on the
+// bucket-plane path.
 uint64_t entry_bytes(const gz_alg *h, int input) {
-  return input == gz::kInputRecords && h->hashed ? 32 : 8;
+  return input == gz::kInputRecords && h->planes ? 24 : 8;
 }
+constexpr uint64_t kGutterSlack = 64;  // alignment of a chunk's code array
 
 int ensure_gutter(gz_alg *h) {
   if (!h->d_gutter) {
-    h->gutter_bytes = h->entry_cap * (h->hashed ? 32 : 8);
+    h->gutter_bytes = h->entry_cap * (h->planes ? 24 : 8) + kGutterSlack;
     GZ_TRY(dev_alloc(&h->d_gutter, h->gutter_bytes));
   }
   GZ_TRY(dev_alloc(&h->d_bin_off, (size_t)gz::kMaxChunks * (h->nbins + 1)));
@@ -538,7 +603,12 @@ int apply_pending(gz_alg *h) {
   const gz::SketchGeom g = h->sgeom();
   GZ_CUDA(cudaMemsetAsync(h->d_status + 1, 0, sizeof(uint32_t), h->stream));
   const int pi = h->prof_begin();
-  if (h->pipe) {
+  if (h->planes) {
+    const int per_sm = gz::plane_update_ctas_per_sm(h->tile_shift, (int)h->threads);
+    const int grid = (int)std::min<uint64_t>(h->ntiles, (uint64_t)gz::num_sms() * per_sm);
+    GZ_CUDA(gz::plane_update(h->pgeom(), h->ph, h->d_sk, h->d_gutter, h->chunks, h->d_bin_off,
+                             h->nchunks, h->d_status + 1, h->d_status, grid, (int)h->threads, h->stream));
+  } else if (h->pipe) {
     const int grid = (int)std::min<uint64_t>(h->ntiles, (uint64_t)gz::num_sms());
     GZ_CUDA(gz::sketch_update_pipe(g, h->d_sk, h->d_gutter, h->chunks, h->d_bin_off, h->nchunks, h->d_flip,
                                    h->d_status + 1, h->d_status, grid, h->stream));
@@ -567,8 +637,9 @@ int gutter_chunk(gz_alg *h, int input, const void *d_in, uint64_t n) {
   }
   const uint64_t per = input == gz::kInputRecords ? 2 : 1;
   const uint64_t esz = entry_bytes(h, input);
+  const bool coded = esz == 24;
   GZ_TRY(ensure_gutter(h));
-  const uint64_t max_n = std::min(h->gutter_bytes / esz, kMaxChunkEntries) / per;
+  const uint64_t max_n = std::min((h->gutter_bytes - kGutterSlack) / esz, kMaxChunkEntries) / per;
   if (max_n == 0) return fail(GZ_ERR_INVALID, "gutter capacity is below one update");
   if (n > max_n) {
     const size_t isz = input == gz::kInputRecords ? 9 : sizeof(uint2);
@@ -576,7 +647,11 @@ int gutter_chunk(gz_alg *h, int input, const void *d_in, uint64_t n) {
       GZ_TRY(gutter_chunk(h, input, (const uint8_t *)d_in + off * isz, std::min(max_n, n - off)));
     return GZ_OK;
   }
-  if (h->gutter_used + n * per * esz > h->gutter_bytes || h->nchunks == gz::kMaxChunks)
+  // a chunk: its keys (8 B per entry), then for coded entries their codes, 16-byte aligned
+  const uint64_t n_ent = n * per;
+  const uint64_t key_bytes = (n_ent * 8 + 15) & ~15ull;
+  const uint64_t need = coded ? key_bytes + n_ent * 16 : key_bytes;
+  if (h->gutter_used + need > h->gutter_bytes || h->nchunks == gz::kMaxChunks)
     GZ_TRY(apply_pending(h));
   const gz::GutterGeom gg = h->ggeom();
   const uint64_t unit = input == gz::kInputRecords ? gz::kRecTile : 4096;
@@ -584,39 +659,19 @@ int gutter_chunk(gz_alg *h, int input, const void *d_in, uint64_t n) {
   uint8_t *out = h->d_gutter + h->gutter_used;
   uint32_t *bin_off = h->d_bin_off + (size_t)h->nchunks * (h->nbins + 1);
   const int pi = h->prof_begin();
-  if (esz == 32) {
-    // records -> hashed 32-byte entries, each record hashed once
-    const gz::HashGeom hg{h->C, h->B, h->d_flip};
-    const uint64_t n_ct = (n + gz::kCountTile - 1) / gz::kCountTile;
-    if (h->nbins <= gz::kSmemBinsMax) {
-      const size_t words = n_ct * h->nbins;
-      if (h->hist2d_words < words) {
-        dev_free(h->d_hist2d);
-        h->hist2d_words = 0;
-        GZ_TRY(dev_alloc(&h->d_hist2d, words));
-        h->hist2d_words = words;
-      }
-      GZ_CUDA(gz::gutter_count_tiles(d_in, n, gg, h->d_hist2d, h->d_status, h->stream));
-      GZ_CUDA(gz::gutter_colscan(h->d_hist2d, (uint32_t)n_ct, h->nbins, h->d_hist, h->stream));
-      GZ_CUDA(gz::scan_exclusive_u64(h->d_hist, h->nbins, h->d_total, h->d_scan_tmp, h->stream));
-      GZ_CUDA(gz::gutter_bin_offsets(h->d_hist, 1, h->nbins, h->d_total, bin_off, h->stream));
-      GZ_CUDA(gz::gutter_hash_scatter(d_in, n, gg, hg, h->d_hist2d, h->d_hist, nullptr,
-                                      reinterpret_cast<uint4 *>(out), h->stream));
-    } else {
-      GZ_CUDA(cudaMemsetAsync(h->d_hist, 0, sizeof(uint64_t) * h->nbins, h->stream));
-      GZ_CUDA(gz::gutter_count(input, d_in, n, gg, G, h->d_hist, h->d_status, h->stream));
-      GZ_CUDA(gz::scan_exclusive_u64(h->d_hist, h->nbins, h->d_total, h->d_scan_tmp, h->stream));
-      GZ_CUDA(gz::gutter_bin_offsets(h->d_hist, 1, h->nbins, h->d_total, bin_off, h->stream));
-      GZ_CUDA(gz::copy_u64(h->d_hist, h->d_cursor, h->nbins, h->stream));
-      GZ_CUDA(gz::gutter_hash_scatter(d_in, n, gg, hg, nullptr, h->d_hist, h->d_cursor,
-                                      reinterpret_cast<uint4 *>(out), h->stream));
-    }
+  uint2 *out2 = reinterpret_cast<uint2 *>(out);
+  GZ_CUDA(cudaMemsetAsync(h->d_hist, 0, sizeof(uint64_t) * h->nbins, h->stream));
+  GZ_CUDA(gz::gutter_count(input, d_in, n, gg, G, h->d_hist, h->d_status, h->stream));
+  GZ_CUDA(gz::scan_exclusive_u64(h->d_hist, h->nbins, h->d_total, h->d_scan_tmp, h->stream));
+  GZ_CUDA(gz::gutter_bin_offsets(h->d_hist, 1, h->nbins, h->d_total, bin_off, h->stream));
+  if (coded) {
+    // records -> coded entries, each record hashed once
+    const uint32_t tile = gz::hash_sort_tile(h->nbins, h->smem_optin - 1024);
+    if (tile == 0) return fail(GZ_ERR_INVALID, "gutter bins do not fit the hash sort");
+    GZ_CUDA(cudaMemsetAsync(h->d_fill, 0, sizeof(uint32_t) * h->nbins, h->stream));
+    GZ_CUDA(gz::gutter_hash_sort(d_in, n, gg, h->ph, tile, h->d_hist, h->d_fill, out2,
+                                 reinterpret_cast<uint4 *>(out + key_bytes), h->stream));
   } else {
-    uint2 *out2 = reinterpret_cast<uint2 *>(out);
-    GZ_CUDA(cudaMemsetAsync(h->d_hist, 0, sizeof(uint64_t) * h->nbins, h->stream));
-    GZ_CUDA(gz::gutter_count(input, d_in, n, gg, G, h->d_hist, h->d_status, h->stream));
-    GZ_CUDA(gz::scan_exclusive_u64(h->d_hist, h->nbins, h->d_total, h->d_scan_tmp, h->stream));
-    GZ_CUDA(gz::gutter_bin_offsets(h->d_hist, 1, h->nbins, h->d_total, bin_off, h->stream));
     const uint32_t tile = gz::sort_scatter_tile(input, gg, h->smem_optin - 1024);
     if (tile >= 1024) {
       GZ_CUDA(cudaMemsetAsync(h->d_fill, 0, sizeof(uint32_t) * h->nbins, h->stream));
@@ -628,10 +683,11 @@ int gutter_chunk(gz_alg *h, int input, const void *d_in, uint64_t n) {
   }
   h->prof_end(pi, 0);
   h->chunks.base[h->nchunks] = h->gutter_used;
-  h->chunks.kind[h->nchunks] = esz == 32 ? gz::kEntryHashed : gz::kEntryPlain;
+  h->chunks.aux[h->nchunks] = coded ? h->gutter_used + key_bytes : 0;
+  h->chunks.kind[h->nchunks] = coded ? gz::kEntryCoded : gz::kEntryPlain;
   h->nchunks++;
-  h->gutter_used += n * per * esz;
-  h->entries_pending += n * per;
+  h->gutter_used += need;
+  h->entries_pending += n_ent;
   return GZ_OK;
 }
 
@@ -960,6 +1016,35 @@ int labels_to_host(gz_alg *h) {
   return GZ_OK;
 }
 
+// Best of `repeats` timed launches of a probe kernel (after one warm-up) on a private stream:
+// units / second, units = the work count of one launch.
+template <class F>
+int time_probe(int repeats, double units, F launch, double *rate) {
+  cudaStream_t s = nullptr;
+  GZ_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  double best = 0;
+  cudaError_t e = launch(s, 0);
+  for (int r = 0; r < repeats && e == cudaSuccess; ++r) {
+    cudaEventRecord(a, s);
+    e = launch(s, 1);
+    cudaEventRecord(b, s);
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    if (ms > 0) best = std::max(best, units / (ms * 1e-3));
+  }
+  if (e == cudaSuccess) e = cudaGetLastError();
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaStreamDestroy(s);
+  if (e != cudaSuccess) return fail(GZ_ERR_CUDA, cudaGetErrorString(e));
+  *rate = best;
+  return GZ_OK;
+}
+
 struct Guard {
   gz_alg *h;
   std::lock_guard<std::mutex> lk;
@@ -1106,6 +1191,7 @@ int gz_get_params(const gz_alg_t *h, gz_params_t *o) {
   o->cols_per_sample = h->cps;
   o->sketch_algorithm = h->cube ? GZ_CUBE_SKETCH : GZ_CAMEO_SKETCH;
   o->in_place = h->in_place ? 1 : 0;
+  o->entry_form = h->planes ? 2 : 1;
   return GZ_OK;
 }
 
@@ -1116,7 +1202,6 @@ int gz_set_gutter_capacity(gz_alg_t *h, uint64_t n) {
   GZ_TRY(apply_pending(h));
   GZ_CUDA(cudaStreamSynchronize(h->stream));
   dev_free(h->d_gutter);
-  dev_free(h->d_hist2d);
   h->entry_cap = n;
   return GZ_OK;
 }
@@ -1458,7 +1543,8 @@ int gz_set_pipeline(gz_alg_t *h, int mode) {
     Guard g(h);
     h->pipe_mode = mode;
   }
-  return gz_set_tuning(h, 0, 0, 0, 0);  // re-pick the default tiling for the chosen kernel
+  // re-pick the default tiling for the chosen kernel; the staged-tile kernels take plain entries
+  return gz_set_tuning(h, 0, 0, 0, mode >= 0 ? 1 : 0);
 }
 
 int gz_set_query_graph(gz_alg_t *h, int enable) {
@@ -1524,33 +1610,16 @@ int gz_measure_update_rate(int repeats, double *updates_per_s) {
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(GZ_ERR_NO_DEVICE, "no CUDA device");
   const int blocks = gz::num_sms();
-  const uint32_t nb = 16 * 817, iters = 4096;  // 16 sketches of 817 buckets (2^17 vertices)
+  const uint32_t iters = 512;  // entries per thread; 32 bucket slots each
   uint32_t *out = nullptr;
   GZ_CUDA(cudaMalloc(&out, sizeof(uint32_t) * 1024 * blocks));
-  cudaStream_t s = nullptr;
-  GZ_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-  cudaEvent_t a, b;
-  cudaEventCreate(&a);
-  cudaEventCreate(&b);
-  double best = 0;
-  gz::update_peak(nb, 16, blocks, out, s);  // warm-up
-  for (int r = 0; r < repeats; ++r) {
-    cudaEventRecord(a, s);
-    gz::update_peak(nb, iters, blocks, out, s);
-    cudaEventRecord(b, s);
-    cudaEventSynchronize(b);
-    float ms = 0;
-    cudaEventElapsedTime(&ms, a, b);
-    best = std::max(best, (double)blocks * 1024 * iters / (ms * 1e-3));
-  }
-  cudaError_t e = cudaGetLastError();
-  cudaEventDestroy(a);
-  cudaEventDestroy(b);
-  cudaStreamDestroy(s);
+  const int rc = time_probe(repeats, (double)blocks * 1024 * iters * gz::kPlaneSlots,
+                            [&](cudaStream_t s, int timed) {
+                              return gz::plane_update_peak(timed ? iters : 8, blocks, out, s);
+                            },
+                            updates_per_s);
   cudaFree(out);
-  if (e != cudaSuccess) return fail(GZ_ERR_CUDA, cudaGetErrorString(e));
-  *updates_per_s = best;
-  return GZ_OK;
+  return rc;
 }
 
 int gz_measure_hash_rate(int repeats, double *hashes_per_s) {
@@ -1561,31 +1630,13 @@ int gz_measure_hash_rate(int repeats, double *hashes_per_s) {
   const uint32_t iters = 4096;
   uint64_t *out = nullptr;
   GZ_CUDA(cudaMalloc(&out, sizeof(uint64_t) * threads * blocks));
-  cudaStream_t s = nullptr;
-  GZ_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-  cudaEvent_t a, b;
-  cudaEventCreate(&a);
-  cudaEventCreate(&b);
-  double best = 0;
-  gz::hash_peak(1, 16, blocks, threads, out, s);  // warm-up
-  for (int r = 0; r < repeats; ++r) {
-    cudaEventRecord(a, s);
-    gz::hash_peak(12345 + r, iters, blocks, threads, out, s);
-    cudaEventRecord(b, s);
-    cudaEventSynchronize(b);
-    float ms = 0;
-    cudaEventElapsedTime(&ms, a, b);
-    const double rate = (double)threads * blocks * iters * 8 / (ms * 1e-3);
-    best = std::max(best, rate);
-  }
-  cudaError_t e = cudaGetLastError();
-  cudaEventDestroy(a);
-  cudaEventDestroy(b);
-  cudaStreamDestroy(s);
+  const int rc = time_probe(repeats, (double)threads * blocks * iters * 8,
+                            [&](cudaStream_t s, int timed) {
+                              return gz::plane_hash_peak(timed ? iters : 16, blocks, threads, out, s);
+                            },
+                            hashes_per_s);
   cudaFree(out);
-  if (e != cudaSuccess) return fail(GZ_ERR_CUDA, cudaGetErrorString(e));
-  *hashes_per_s = best;
-  return GZ_OK;
+  return rc;
 }
 
 int gz_get_stream(gz_alg_t *h, void **s) {
@@ -1598,29 +1649,32 @@ int gz_set_tuning(gz_alg_t *h, uint32_t vpt, uint32_t threads, uint32_t tiles_pe
                   uint32_t entry_form) {
   if (!h) return fail(GZ_ERR_INVALID, "null handle");
   if (entry_form > 2) return fail(GZ_ERR_INVALID, "entry_form must be 0, 1 or 2");
-  if (entry_form == 2 && (h->C > gz::kHashedMaxColumns || h->cube))
-    return fail(GZ_ERR_INVALID, "hashed entries need CameoSketch with at most 32 columns");
+  if (entry_form == 2 && (h->C > gz::kPlaneMaxColumns || h->cube))
+    return fail(GZ_ERR_INVALID, "coded entries need CameoSketch with at most 31 columns");
   if (h->in_place && (vpt || threads || tiles_per_bin || entry_form == 2))
     return fail(GZ_ERR_INVALID, "this handle updates its sketches in place: there are no tiles to tune");
   Guard g(h);
   GZ_TRY(push_staged_entries(h));
   GZ_TRY(apply_pending(h));
   GZ_CUDA(cudaStreamSynchronize(h->stream));
-  const bool want_hashed = entry_form == 0 ? h->hashed_default : entry_form == 2;
-  if (want_hashed != h->hashed) {
-    dev_free(h->d_gutter);  // entry size changes: reallocated on the next ingest
-    h->hashed = want_hashed;
-  }
+  const int keep_mode = h->planes_mode;
+  const bool keep_planes = h->planes, keep_pipe = h->pipe;
+  const uint32_t keep[5] = {h->tile_shift, h->ntiles, h->bin_shift, h->nbins, h->threads};
+  h->planes_mode = entry_form == 0 ? -1 : (entry_form == 2 ? 1 : 0);
   const uint32_t old_nb = h->nbins;
-  const uint32_t keep[4] = {h->tile_shift, h->ntiles, h->bin_shift, h->nbins};
   const int rc = choose_tiling(h, vpt, threads, tiles_per_bin);
   if (rc != GZ_OK) {
+    h->planes_mode = keep_mode;
+    h->planes = keep_planes;
+    h->pipe = keep_pipe;
     h->tile_shift = keep[0];
     h->ntiles = keep[1];
     h->bin_shift = keep[2];
     h->nbins = keep[3];
+    h->threads = keep[4];
     return rc;
   }
+  if (h->planes != keep_planes) dev_free(h->d_gutter);  // entry size changes: reallocated on the next ingest
   if (h->nbins != old_nb) {
     dev_free(h->d_bin_off);
     dev_free(h->d_hist);

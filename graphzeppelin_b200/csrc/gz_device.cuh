@@ -90,4 +90,43 @@ __device__ __forceinline__ uint32_t smem_u32(const void *p) {
 }
 #endif
 
+// The first step of rrmxmx, h ^ rotl(h, 49) ^ rotl(h, 24), is linear over GF(2). Hence
+// rrmxmx8(in ^ flip) = rrmxmx8_tail(premix(in) ^ premix(flip)): premix of the record's input is
+// computed once per record and premix(flip) once per column seed, which leaves two multiplies, a
+// shift-add-xor and the final xorshift per column.
+__host__ __device__ inline uint64_t xxh3_premix(uint64_t h) {
+  return h ^ ((h << 49) | (h >> 15)) ^ ((h << 24) | (h >> 40));
+}
+
+#ifdef __CUDACC__
+// rrmxmx8 after its premix step, without the final xorshift, as 32-bit halves.
+__device__ __forceinline__ void rrmxmx8_tail_pre(uint64_t h, uint32_t &lo, uint32_t &hi) {
+  h *= kPrimeMx2;
+  h ^= (h >> 35) + 8;
+  h *= kPrimeMx2;
+  lo = (uint32_t)h;
+  hi = (uint32_t)(h >> 32);
+}
+// low word of rrmxmx8 given the premixed input (the bucket checksum, and the low bits the depth
+// is counted in)
+__device__ __forceinline__ uint32_t tail_lo32(uint64_t pm) {
+  uint32_t lo, hi;
+  rrmxmx8_tail_pre(pm, lo, hi);
+  return lo ^ __funnelshift_r(lo, hi, 28);
+}
+// Depth code of one column: min(depth, 15) where depth = ctz(hash | 1 << B); cap = 1 << min(B, 15).
+// For B <= 15 this is the depth itself (depth <= B); for B > 15 the code 15 stands for "15 or
+// more" and the exact depth is recomputed by depth_exact where it is needed.
+__device__ __forceinline__ uint32_t depth_code(uint64_t pm, uint32_t cap) {
+  return __clz(__brev(tail_lo32(pm) | cap));
+}
+// depth = ctz(hash | 1 << B), B <= 63, given the premixed input
+__device__ __forceinline__ uint32_t depth_exact(uint64_t pm, uint32_t B) {
+  uint32_t lo, hi;
+  rrmxmx8_tail_pre(pm, lo, hi);
+  const uint64_t r = (((uint64_t)(hi ^ (hi >> 28))) << 32) | (lo ^ __funnelshift_r(lo, hi, 28));
+  return (uint32_t)(__ffsll((long long)(r | (1ull << B))) - 1);
+}
+#endif
+
 }  // namespace gz

@@ -19,6 +19,9 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
+#include <set>
+#include <utility>
 #include <vector>
 
 #include "gz_common.cuh"
@@ -112,7 +115,7 @@ cudaError_t launch_gutter(const void *in, uint64_t n, GutterGeom g, int G, uint6
   const size_t smem = gutter_smem(INPUT, g, SMEM);
   auto kern = k_gutter<INPUT, COUNT, SMEM>;
   if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = smem_optin(kern);
     if (e != cudaSuccess) return e;
   }
   kern<<<G, 512, smem, s>>>(in, n, g, hist, entries, status);
@@ -135,14 +138,13 @@ k_gutter_sort_scatter(const void *__restrict__ in, uint64_t n, GutterGeom g, uin
   uint32_t *s_cur = reinterpret_cast<uint32_t *>(gsm);  // counts, then placement cursors
   uint32_t *s_off = s_cur + nb4;                         // run start inside the tile
   uint32_t *s_dst = s_off + nb4;                         // run start inside the gutter
-  const uint32_t ept = INPUT == kInputRecords ? 2 * rec_tile : rec_tile;
   uint2 *s_sorted = reinterpret_cast<uint2 *>(s_dst + nb4);
   // the staged records share the sorted-entry area: they are parsed into registers before the
   // first entry is placed, and the next tile is staged only after the write-out
   uint8_t *s_rec = reinterpret_cast<uint8_t *>(s_sorted);
   const uint8_t *rec = reinterpret_cast<const uint8_t *>(in);
   const uint2 *ein = reinterpret_cast<const uint2 *>(in);
-  const uint32_t per_thread = (nb + blockDim.x - 1) / blockDim.x;  // bins per thread (<= 4)
+  const uint32_t per_thread = (nb + blockDim.x - 1) / blockDim.x;  // bins per thread (<= 8)
   for (uint64_t t0 = blockIdx.x * (uint64_t)rec_tile; t0 < n; t0 += (uint64_t)gridDim.x * rec_tile) {
     const uint32_t cnt = (uint32_t)(n - t0 < rec_tile ? n - t0 : rec_tile);
     for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) s_cur[b] = 0u;
@@ -176,7 +178,7 @@ k_gutter_sort_scatter(const void *__restrict__ in, uint64_t n, GutterGeom g, uin
       }
     __syncthreads();
     // 2. run offsets inside the tile (bins [tid*per_thread, +per_thread) per thread)
-    uint32_t local[4] = {0, 0, 0, 0}, sum = 0;
+    uint32_t local[8] = {0, 0, 0, 0, 0, 0, 0, 0}, sum = 0;
     for (uint32_t k = 0; k < per_thread; ++k) {
       const uint32_t b = threadIdx.x * per_thread + k;
       local[k] = b < nb ? s_cur[b] : 0u;
@@ -217,140 +219,6 @@ k_gutter_sort_scatter(const void *__restrict__ in, uint64_t n, GutterGeom g, uin
       entries[s_dst[b] + (j - s_off[b])] = x;
     }
     __syncthreads();
-  }
-}
-
-// ---- hashed gutter ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(512)
-k_count_tiles(const uint8_t *__restrict__ rec, uint64_t n, GutterGeom g, uint32_t *__restrict__ hist2d,
-              uint32_t *__restrict__ status) {
-  extern __shared__ __align__(16) uint8_t gsm[];
-  uint32_t *s_bin = reinterpret_cast<uint32_t *>(gsm);
-  uint8_t *s_rec = gsm + ((g.nbins + 3) & ~3u) * 4;
-  const uint64_t r0 = (uint64_t)blockIdx.x * kCountTile;
-  const uint64_t r1 = r0 + kCountTile < n ? r0 + kCountTile : n;
-  for (uint32_t b = threadIdx.x; b < g.nbins; b += blockDim.x) s_bin[b] = 0u;
-  bool bad = false;
-  for (uint64_t t = r0; t < r1; t += kRecTile) {
-    const uint32_t cnt = (uint32_t)(r1 - t < (uint64_t)kRecTile ? r1 - t : (uint64_t)kRecTile);
-    __syncthreads();
-    const uint32_t shift = stage_records(rec, t, cnt, s_rec);
-    __syncthreads();
-    for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
-      uint32_t u, v;
-      parse_record(s_rec, shift, i, u, v);
-      if (u >= g.V || v >= g.V) {
-        bad = true;
-        continue;
-      }
-      atomicAdd(&s_bin[u >> g.bin_shift], 1u);
-      atomicAdd(&s_bin[v >> g.bin_shift], 1u);
-    }
-  }
-  __syncthreads();
-  uint32_t *row = hist2d + (uint64_t)blockIdx.x * g.nbins;
-  for (uint32_t b = threadIdx.x; b < g.nbins; b += blockDim.x) row[b] = s_bin[b];
-  if (bad) atomicOr(status, kStatusBadVertex);
-}
-
-// Column-wise exclusive scan of hist2d (count tiles x bins): a CTA owns 32 bins (one per lane,
-// so every row access is one coalesced 128-byte line) and its 16 warps split the count tiles.
-__global__ void __launch_bounds__(512)
-k_colscan(uint32_t *hist2d, uint32_t n_ct, uint32_t nbins, uint64_t *totals) {
-  __shared__ uint32_t part[16][32];
-  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const uint32_t b = blockIdx.x * 32 + lane;
-  const uint32_t t0 = (uint32_t)((uint64_t)n_ct * warp / 16);
-  const uint32_t t1 = (uint32_t)((uint64_t)n_ct * (warp + 1) / 16);
-  uint32_t sum = 0;
-  if (b < nbins)
-    for (uint32_t t = t0; t < t1; ++t) sum += hist2d[(uint64_t)t * nbins + b];
-  part[warp][lane] = sum;
-  __syncthreads();
-  uint32_t run = 0;
-  for (uint32_t w = 0; w < warp; ++w) run += part[w][lane];
-  if (b < nbins) {
-    for (uint32_t t = t0; t < t1; ++t) {
-      uint32_t *p = hist2d + (uint64_t)t * nbins + b;
-      const uint32_t c = *p;
-      *p = run;
-      run += c;
-    }
-    if (warp == 15) totals[b] = run;
-  }
-}
-
-// Checksum and the 4-bit depth codes of every column for one edge index (hash once per record).
-__device__ __forceinline__ void hash_record(uint32_t lo, uint32_t hi, const uint64_t *s_flip,
-                                            uint32_t C, uint32_t B, uint32_t &chk,
-                                            uint32_t (&codes)[4]) {
-  const uint64_t in64 = ((uint64_t)lo << 32) | hi;
-  chk = hash_lo32(in64 ^ s_flip[C]);
-#pragma unroll
-  for (int w = 0; w < 4; ++w) {
-    uint32_t word = 0;
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const uint32_t c = w * 8 + j;
-      if (c < C) {
-        const uint32_t d = hash_depth(in64 ^ s_flip[c], B);
-        word |= min(d, kDepthEscape) << (4 * j);
-      }
-    }
-    codes[w] = word;
-  }
-}
-
-template <bool SMEM_CURSOR>
-__global__ void __launch_bounds__(512)
-k_hash_scatter(const uint8_t *__restrict__ rec, uint64_t n, GutterGeom g, HashGeom hg,
-               const uint32_t *__restrict__ hist2d, const uint64_t *__restrict__ base,
-               uint64_t *__restrict__ cursor, uint4 *__restrict__ out) {
-  extern __shared__ __align__(16) uint8_t gsm[];
-  uint64_t *s_flip = reinterpret_cast<uint64_t *>(gsm);
-  const uint32_t flip_bytes = ((hg.C + 1) * 8 + 15) & ~15u;
-  uint32_t *s_cur = reinterpret_cast<uint32_t *>(gsm + flip_bytes);
-  uint8_t *s_rec = gsm + flip_bytes + (SMEM_CURSOR ? ((g.nbins + 3) & ~3u) * 4 : 0);
-  for (uint32_t i = threadIdx.x; i <= hg.C; i += blockDim.x) s_flip[i] = hg.flip[i];
-  uint64_t r0, r1, step;
-  if (SMEM_CURSOR) {
-    r0 = (uint64_t)blockIdx.x * kCountTile;
-    r1 = r0 + kCountTile < n ? r0 + kCountTile : n;
-    step = kRecTile;
-    const uint32_t *row = hist2d + (uint64_t)blockIdx.x * g.nbins;
-    for (uint32_t b = threadIdx.x; b < g.nbins; b += blockDim.x)
-      s_cur[b] = (uint32_t)base[b] + row[b];
-  } else {
-    r0 = (uint64_t)blockIdx.x * kRecTile;
-    r1 = n;
-    step = (uint64_t)gridDim.x * kRecTile;
-  }
-  for (uint64_t t = r0; t < r1; t += step) {
-    const uint32_t cnt = (uint32_t)(r1 - t < (uint64_t)kRecTile ? r1 - t : (uint64_t)kRecTile);
-    __syncthreads();
-    const uint32_t shift = stage_records(rec, t, cnt, s_rec);
-    __syncthreads();
-    for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
-      uint32_t u, v;
-      parse_record(s_rec, shift, i, u, v);
-      if (u >= g.V || v >= g.V) continue;
-      const uint32_t lo = max(u, v), hi = min(u, v);
-      uint32_t chk, codes[4];
-      hash_record(lo, hi, s_flip, hg.C, hg.B, chk, codes);
-      const uint4 tail = make_uint4(codes[0], codes[1], codes[2], codes[3]);
-      uint64_t pu, pv;
-      if (SMEM_CURSOR) {
-        pu = atomicAdd(&s_cur[u >> g.bin_shift], 1u);
-        pv = atomicAdd(&s_cur[v >> g.bin_shift], 1u);
-      } else {
-        pu = atomicAdd(reinterpret_cast<unsigned long long *>(&cursor[u >> g.bin_shift]), 1ull);
-        pv = atomicAdd(reinterpret_cast<unsigned long long *>(&cursor[v >> g.bin_shift]), 1ull);
-      }
-      out[2 * pu] = make_uint4(u, lo, hi, chk);
-      out[2 * pu + 1] = tail;
-      out[2 * pv] = make_uint4(v, lo, hi, chk);
-      out[2 * pv + 1] = tail;
-    }
   }
 }
 
@@ -437,62 +305,16 @@ k_scan_down(uint64_t *__restrict__ d, uint64_t n, const uint64_t *__restrict__ p
 // ------------------------------------------------------------------------------------------------
 // sketch update
 // ------------------------------------------------------------------------------------------------
-// Same for a hashed entry: the checksum and depths come with it (a depth code of 15 means
-// "15 or more" and is recomputed).
-__device__ __forceinline__ void apply_hashed(uint4 e0, uint4 e1, uint32_t *s_sk, uint32_t vmask,
-                                             uint32_t sketch_words, const uint64_t *s_flip,
-                                             uint32_t C, uint32_t B) {
-  const uint32_t v = e0.x, lo = e0.y, hi = e0.z, chk = e0.w;
-  uint32_t *sk = s_sk + (v & vmask) * sketch_words;
-  uint32_t *det = sk + 3 * C * B;
-  atomicXor(det, lo);
-  atomicXor(det + 1, hi);
-  atomicXor(det + 2, chk);
-  const uint32_t codes[4] = {e1.x, e1.y, e1.z, e1.w};
-#pragma unroll
-  for (int w = 0; w < 4; ++w) {
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const uint32_t c = w * 8 + j;
-      if (c < C) {
-        uint32_t d = (codes[w] >> (4 * j)) & 0xfu;
-        if (d == kDepthEscape) d = hash_depth((((uint64_t)lo << 32) | hi) ^ s_flip[c], B);
-        if (d < B) {
-          uint32_t *bk = sk + 3 * (c * B + d);
-          atomicXor(bk, lo);
-          atomicXor(bk + 1, hi);
-          atomicXor(bk + 2, chk);
-        }
-      }
-    }
-  }
-}
-
-template <bool HASHED>
-__device__ __forceinline__ uint32_t entry_vertex(const uint8_t *cb, int kind, uint64_t i) {
-  return HASHED && kind == kEntryHashed ? reinterpret_cast<const uint4 *>(cb)[2 * i].x
-                                        : reinterpret_cast<const uint2 *>(cb)[i].x;
-}
-
-template <bool HASHED>
-__device__ __forceinline__ void apply_any(const uint8_t *cb, int kind, uint64_t i, uint32_t *s_sk,
+__device__ __forceinline__ void apply_any(const uint8_t *cb, uint64_t i, uint32_t *s_sk,
                                           uint32_t vmask, const SketchGeom &g,
                                           const uint64_t *s_flip, uint64_t flip_chk) {
-  if (HASHED && kind == kEntryHashed) {
-    const uint4 *E = reinterpret_cast<const uint4 *>(cb);
-    apply_hashed(E[2 * i], E[2 * i + 1], s_sk, vmask, g.sketch_words, s_flip, g.C, g.B);
-  } else if (g.cube) {
-    apply_entry_cube(reinterpret_cast<const uint2 *>(cb)[i], s_sk, vmask, g.sketch_words, s_flip,
-                     flip_chk, g.C, g.B);
-  } else {
-    apply_entry(reinterpret_cast<const uint2 *>(cb)[i], s_sk, vmask, g.sketch_words, s_flip,
-                flip_chk, g.C, g.B);
-  }
+  const uint2 e = reinterpret_cast<const uint2 *>(cb)[i];
+  if (g.cube)
+    apply_entry_cube(e, s_sk, vmask, g.sketch_words, s_flip, flip_chk, g.C, g.B);
+  else
+    apply_entry(e, s_sk, vmask, g.sketch_words, s_flip, flip_chk, g.C, g.B);
 }
 
-// HASHED = some buffered chunk holds hashed entries (otherwise the plain-only variant, which
-// needs fewer registers, is launched).
-template <bool HASHED>
 __global__ void __launch_bounds__(1024, 1)
 k_sketch_update(SketchGeom g, uint8_t *__restrict__ sketches, const uint8_t *__restrict__ gutter,
                 ChunkTable chunks, const uint32_t *__restrict__ bin_off, int nchunks,
@@ -528,7 +350,7 @@ k_sketch_update(SketchGeom g, uint8_t *__restrict__ sketches, const uint8_t *__r
           total += bin_off[(uint64_t)k * stride + bin + 1] - bin_off[(uint64_t)k * stride + bin];
       }
       // a tile with too few entries to pay for staging its sketches is updated in place in HBM
-      const bool direct = !HASHED && per_bin == 0 && total < g.direct_max;
+      const bool direct = per_bin == 0 && total < g.direct_max;
       s_tile = t;
       s_total = total;
       s_direct = direct;
@@ -565,33 +387,32 @@ k_sketch_update(SketchGeom g, uint8_t *__restrict__ sketches, const uint8_t *__r
       const uint32_t bin = t >> per_bin;
       for (int k = 0; k < nchunks; ++k) {
         const uint8_t *cb = gutter + chunks.base[k];
-        const int kind = chunks.kind[k];
         const uint64_t b = bin_off[(uint64_t)k * stride + bin];
         const uint64_t e = bin_off[(uint64_t)k * stride + bin + 1];
         if (per_bin == 0) {
           // the bin is this tile: every entry applies
           for (uint64_t i = b + threadIdx.x; i < e; i += blockDim.x)
-            apply_any<HASHED>(cb, kind, i, s_sk, vpt - 1, g, s_flip, flip_chk);
+            apply_any(cb, i, s_sk, vpt - 1, g, s_flip, flip_chk);
         } else {
           // the bin holds several tiles: each warp ballots 32 entries, queues the indices of
           // this tile's, and applies only full warps of queued entries
           uint32_t qn = 0;
           for (uint64_t i0 = b + (uint64_t)warp * 32; i0 < e; i0 += (uint64_t)nwarps * 32) {
             const uint64_t i = i0 + lane;
-            const bool mine = i < e && (entry_vertex<HASHED>(cb, kind, i) >> g.tile_shift) == t;
+            const bool mine = i < e && (reinterpret_cast<const uint2 *>(cb)[i].x >> g.tile_shift) == t;
             const uint32_t m = __ballot_sync(kFull, mine);
             if (mine) q[qn + __popc(m & ((1u << lane) - 1u))] = (uint32_t)i;
             qn += __popc(m);
             __syncwarp();
             if (qn >= 32) {
-              apply_any<HASHED>(cb, kind, q[lane], s_sk, vpt - 1, g, s_flip, flip_chk);
+              apply_any(cb, q[lane], s_sk, vpt - 1, g, s_flip, flip_chk);
               __syncwarp();
               qn -= 32;
               if (lane < qn) q[lane] = q[32 + lane];
               __syncwarp();
             }
           }
-          if (lane < qn) apply_any<HASHED>(cb, kind, q[lane], s_sk, vpt - 1, g, s_flip, flip_chk);
+          if (lane < qn) apply_any(cb, q[lane], s_sk, vpt - 1, g, s_flip, flip_chk);
           __syncwarp();
         }
       }
@@ -1307,50 +1128,7 @@ __global__ void k_bv_final(uint32_t V, uint32_t *parent, uint32_t *out, uint32_t
 // Shared-memory bucket-update probe: every thread XORs 96-bit updates into random 12-byte
 // buckets of a 16-vertex staged tile with three 32-bit atomicXor each -- the sketch-update
 // kernel's per-bucket operation, without hashing or global traffic.
-__global__ void __launch_bounds__(1024, 1) k_update_peak(uint32_t nb, uint32_t iters, uint32_t *out) {
-  extern __shared__ __align__(16) uint32_t usm[];
-  for (uint32_t i = threadIdx.x; i < nb * 3; i += blockDim.x) usm[i] = 0;
-  __syncthreads();
-  uint32_t seed = fmix32_(blockIdx.x * 1024u + threadIdx.x);
-  for (uint32_t it = 0; it < iters; ++it) {
-    seed = fmix32_(seed + it);
-    uint32_t *p = usm + 3 * (seed % nb);
-    atomicXor(p, seed);
-    atomicXor(p + 1, seed * 3u);
-    atomicXor(p + 2, seed ^ 0x5555u);
-  }
-  __syncthreads();
-  uint32_t x = 0;
-  for (uint32_t i = threadIdx.x; i < nb * 3; i += blockDim.x) x ^= usm[i];
-  out[blockIdx.x * 1024u + threadIdx.x] = x;
-}
-
 inline unsigned blocks_for(uint64_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
-
-// Eight independent hash chains per thread: each step is one 8-byte XXH3 (rrmxmx with a column
-// constant) to a bucket depth -- the per-column work of the ingest kernel -- plus one IMAD to make
-// the next input, with no memory traffic.
-__global__ void k_hash_peak(uint64_t seed, uint32_t iters, uint64_t *out) {
-  const uint64_t flip = xxh3_flip(seed);
-  uint64_t x[8];
-  const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-#pragma unroll
-  for (int k = 0; k < 8; ++k) x[k] = tid * 8 + k;
-  uint32_t acc = 0;
-  for (uint32_t i = 0; i < iters; ++i) {
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      // the sketch-update kernel's per-column work: one hash to a bucket depth (B = 34)
-      const uint32_t d = hash_depth(x[k] ^ flip, 34);
-      acc += d;
-      x[k] = x[k] * 0x9E3779B97F4A7C15ULL + d;
-    }
-  }
-  uint64_t r = acc;
-#pragma unroll
-  for (int k = 0; k < 8; ++k) r ^= x[k];
-  out[tid] = r;
-}
 
 }  // namespace
 
@@ -1360,21 +1138,25 @@ __global__ void k_hash_peak(uint64_t seed, uint32_t iters, uint64_t *out) {
 uint64_t launch_count() { return g_launches.load(); }
 void add_launches(uint64_t n) { g_launches += n; }
 
-cudaError_t update_peak(uint32_t nb, uint32_t iters, int blocks, uint32_t *out, cudaStream_t s) {
-  const size_t smem = (size_t)nb * 12;
-  cudaError_t e = cudaFuncSetAttribute(k_update_peak, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem);
+cudaError_t smem_optin_fn(const void *fn) {
+  static std::mutex mtx;
+  static std::set<std::pair<const void *, int>> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  k_update_peak<<<blocks, 1024, smem, s>>>(nb, iters, out);
-  g_launches++;
-  return cudaGetLastError();
-}
-
-cudaError_t hash_peak(uint64_t seed, uint32_t iters, int blocks, int threads, uint64_t *out,
-                      cudaStream_t s) {
-  k_hash_peak<<<blocks, threads, 0, s>>>(seed, iters, out);
-  g_launches++;
-  return cudaGetLastError();
+  std::lock_guard<std::mutex> lk(mtx);
+  if (done.count({fn, dev})) return cudaSuccess;
+  int optin = 0;
+  e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e != cudaSuccess) return e;
+  cudaFuncAttributes fa{};
+  e = cudaFuncGetAttributes(&fa, fn);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           optin - (int)fa.sharedSizeBytes);
+  if (e != cudaSuccess) return e;
+  done.insert({fn, dev});
+  return cudaSuccess;
 }
 
 int num_sms() {
@@ -1433,51 +1215,6 @@ cudaError_t gutter_scatter_global(int input, const void *in, uint64_t n, GutterG
              : launch_gutter<kInputEntries, false, false>(in, n, g, G, cursor, entries, nullptr, s);
 }
 
-cudaError_t gutter_count_tiles(const void *rec, uint64_t n, GutterGeom g, uint32_t *hist2d,
-                               uint32_t *status, cudaStream_t s) {
-  const size_t smem = ((g.nbins + 3) & ~3u) * 4 + kRecStageBytes;
-  cudaError_t e = cudaFuncSetAttribute(k_count_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem);
-  if (e != cudaSuccess) return e;
-  const unsigned grid = (unsigned)((n + kCountTile - 1) / kCountTile);
-  k_count_tiles<<<grid, 512, smem, s>>>(reinterpret_cast<const uint8_t *>(rec), n, g, hist2d, status);
-  g_launches++;
-  return cudaGetLastError();
-}
-
-cudaError_t gutter_colscan(uint32_t *hist2d, uint32_t n_ct, uint32_t nbins, uint64_t *totals,
-                           cudaStream_t s) {
-  k_colscan<<<blocks_for(nbins, 32), 512, 0, s>>>(hist2d, n_ct, nbins, totals);
-  g_launches++;
-  return cudaGetLastError();
-}
-
-cudaError_t gutter_hash_scatter(const void *rec, uint64_t n, GutterGeom g, HashGeom hg,
-                                const uint32_t *hist2d, const uint64_t *base, uint64_t *cursor,
-                                uint4 *out, cudaStream_t s) {
-  const size_t flip_bytes = ((hg.C + 1) * 8 + 15) & ~15u;
-  const bool smem_cursor = hist2d != nullptr;
-  const size_t smem = flip_bytes + (smem_cursor ? ((g.nbins + 3) & ~3u) * 4 : 0) + kRecStageBytes;
-  const uint8_t *r = reinterpret_cast<const uint8_t *>(rec);
-  if (smem_cursor) {
-    cudaError_t e = cudaFuncSetAttribute(k_hash_scatter<true>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    const unsigned grid = (unsigned)((n + kCountTile - 1) / kCountTile);
-    k_hash_scatter<true><<<grid, 512, smem, s>>>(r, n, g, hg, hist2d, base, cursor, out);
-  } else {
-    cudaError_t e = cudaFuncSetAttribute(k_hash_scatter<false>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hash_scatter<false>, 512, smem);
-    const uint64_t tiles = (n + kRecTile - 1) / kRecTile;
-    const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(tiles, (uint64_t)num_sms() * std::max(per_sm, 1)));
-    k_hash_scatter<false><<<grid, 512, smem, s>>>(r, n, g, hg, hist2d, base, cursor, out);
-  }
-  g_launches++;
-  return cudaGetLastError();
-}
 
 uint32_t sort_scatter_tile(int input, GutterGeom g, size_t smem_budget) {
   const size_t fixed = (size_t)3 * ((g.nbins + 3) & ~3u) * 4 + 64;
@@ -1500,13 +1237,11 @@ cudaError_t gutter_sort_scatter(int input, const void *in, uint64_t n, GutterGeo
   const int G = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)num_sms(),
                                                                (n + rec_tile - 1) / rec_tile));
   if (input == kInputRecords) {
-    cudaError_t e = cudaFuncSetAttribute(k_gutter_sort_scatter<kInputRecords>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = smem_optin(k_gutter_sort_scatter<kInputRecords>);
     if (e != cudaSuccess) return e;
     k_gutter_sort_scatter<kInputRecords><<<G, 1024, smem, s>>>(in, n, g, rec_tile, base, fill, entries);
   } else {
-    cudaError_t e = cudaFuncSetAttribute(k_gutter_sort_scatter<kInputEntries>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = smem_optin(k_gutter_sort_scatter<kInputEntries>);
     if (e != cudaSuccess) return e;
     k_gutter_sort_scatter<kInputEntries><<<G, 1024, smem, s>>>(in, n, g, rec_tile, base, fill, entries);
   }
@@ -1532,17 +1267,13 @@ size_t sketch_update_smem_bytes(SketchGeom g) {
 }
 
 cudaError_t sketch_update_prepare(SketchGeom g, int /*threads*/) {
-  const size_t smem = sketch_update_smem_bytes(g);
-  cudaError_t e = cudaFuncSetAttribute(k_sketch_update<false>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_sketch_update<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)smem);
+  (void)g;
+  return smem_optin(k_sketch_update);
 }
 
 int sketch_update_ctas_per_sm(SketchGeom g, int threads) {
   int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sketch_update<false>, threads,
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sketch_update, threads,
                                                     sketch_update_smem_bytes(g)) != cudaSuccess)
     return 1;
   return n > 0 ? n : 1;
@@ -1553,14 +1284,10 @@ cudaError_t sketch_update(SketchGeom g, uint8_t *sketches, const uint8_t *gutter
                           const uint64_t *flip, uint32_t *work_counter, uint32_t *status, int grid,
                           int threads, cudaStream_t s) {
   const size_t smem = sketch_update_smem_bytes(g);
-  bool hashed = false;
-  for (int k = 0; k < nchunks; ++k) hashed |= chunks.kind[k] == kEntryHashed;
-  auto kern = hashed ? k_sketch_update<true> : k_sketch_update<false>;
-  // the limit is per function, and other handles may have set it for a smaller geometry
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = smem_optin(k_sketch_update);
   if (e != cudaSuccess) return e;
-  kern<<<grid, threads, smem, s>>>(g, sketches, gutter, chunks, bin_off, nchunks, flip,
-                                   work_counter, status);
+  k_sketch_update<<<grid, threads, smem, s>>>(g, sketches, gutter, chunks, bin_off, nchunks, flip,
+                                              work_counter, status);
   g_launches++;
   return cudaGetLastError();
 }
@@ -1574,7 +1301,7 @@ cudaError_t sketch_update_pipe(SketchGeom g, uint8_t *sketches, const uint8_t *g
                                const uint64_t *flip, uint32_t *work_counter, uint32_t *status,
                                int grid, cudaStream_t s) {
   const size_t smem = sketch_update_pipe_smem_bytes(g);
-  cudaError_t e = cudaFuncSetAttribute(k_sketch_update_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = smem_optin(k_sketch_update_pipe);
   if (e != cudaSuccess) return e;
   k_sketch_update_pipe<<<grid, 1024, smem, s>>>(g, sketches, gutter, chunks, bin_off, nchunks, flip,
                                                 work_counter, status);
@@ -1592,7 +1319,7 @@ cudaError_t apply_in_place(int input, const void *in, uint64_t n, SketchGeom g, 
   uint32_t *sk = reinterpret_cast<uint32_t *>(sketches);
   auto launch = [&](auto kern) -> cudaError_t {
     if (smem > 48 * 1024) {
-      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaError_t e = smem_optin(kern);
       if (e != cudaSuccess) return e;
     }
     kern<<<grid, 512, smem, s>>>(in, n, g, sk, flip, status);
@@ -1629,7 +1356,7 @@ size_t bv_smem_bytes(const BoruvkaGeom &g) {
 }
 template <class K>
 cudaError_t bv_smem_attr(K kern, size_t smem) {
-  return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  return smem_optin(kern);
 }
 
 cudaError_t sketch_total_xor(const uint8_t *sketches, uint32_t V, uint32_t sketch_words,

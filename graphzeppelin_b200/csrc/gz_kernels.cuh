@@ -31,13 +31,14 @@ struct GutterGeom {
 constexpr int kMaxChunks = 128;
 // Entry kinds of a gutter chunk.
 enum EntryKind : uint8_t {
-  kEntryPlain = 0,   // uint2 {vertex, neighbour}: hashed by the sketch-update kernel
-  kEntryHashed = 1,  // 32 bytes {vertex, idx lo, idx hi, checksum, 4 x 8 depth codes}
+  kEntryPlain = 0,   // uint2 {vertex, neighbour}: hashed where it is applied
+  kEntryCoded = 1,   // uint2 {vertex, neighbour} at base, and at aux a parallel uint4 of 4-bit
+                     // depth codes (column c in bits 4c..4c+3): every record hashed once
 };
-constexpr uint32_t kHashedMaxColumns = 32;  // 4-bit depth codes in 128 bits
-constexpr uint32_t kDepthEscape = 15;       // code for depth >= 15: recomputed where applied
+constexpr uint32_t kDepthEscape = 15;  // depth code for "15 or more"
 struct ChunkTable {
-  uint64_t base[kMaxChunks];  // byte offset of the chunk in the gutter buffer
+  uint64_t base[kMaxChunks];  // byte offset of the chunk's keys in the gutter buffer
+  uint64_t aux[kMaxChunks];   // kEntryCoded: byte offset of its depth codes
   uint8_t kind[kMaxChunks];
 };
 
@@ -55,6 +56,15 @@ struct SketchGeom {
                                // is updated in place in HBM (global atomics) instead of staged
   uint32_t nbuf = 2;           // tile buffers of the pipelined kernel (2..4)
 };
+
+// Raises a kernel's dynamic shared-memory limit to the device's opt-in maximum, once per kernel
+// and device. One fixed maximum, instead of each launch's own size set just before it, leaves no
+// window in which another host thread lowers the limit between that set and the launch.
+cudaError_t smem_optin_fn(const void *kernel);
+template <class K>
+cudaError_t smem_optin(K kernel) {
+  return smem_optin_fn(reinterpret_cast<const void *>(kernel));
+}
 
 // Records per staging tile of the gutter kernels, and the largest bin count for which the
 // per-CTA histogram lives in shared memory.
@@ -84,24 +94,49 @@ cudaError_t gutter_sort_scatter(int input, const void *d_in, uint64_t n, GutterG
 cudaError_t gutter_scatter_global(int input, const void *d_in, uint64_t n, GutterGeom g, int G,
                                   uint64_t *cursor, uint2 *entries, cudaStream_t s);
 
-// ---- hashed gutter (records in, 32-byte entries out; every record hashed once) ---------------
-constexpr uint32_t kCountTile = 65536;  // records per count tile
-struct HashGeom {
+// ---- hash-once ingest into bucket planes (gz_planes.cu) ------------------------------------
+// A vertex sketch is accumulated in shared memory as three planes of kPlaneRows rows x
+// kPlaneSlots 32-bit slots: slot c < C is column c, slot C the deterministic bucket (row 0).
+// Row d of a column holds depth d; the last row is scratch (depth codes at or above it are
+// handled in HBM). Plane A XORs (neighbour | 1 << 31) of the entries whose neighbour is above
+// the vertex, plane B of the others, plane G their checksums.
+constexpr uint32_t kPlaneSlots = 32;
+constexpr uint32_t kPlaneRows = 12;
+constexpr uint32_t kPlaneMaxColumns = kPlaneSlots - 1;
+constexpr uint32_t kPlaneMaxTile = 32;     // vertices per tile (one tile per gutter bin)
+struct PlaneHash {
   uint32_t C, B;
-  const uint64_t *flip;  // C column constants, then the checksum constant
+  uint64_t kcol[kPlaneMaxColumns];  // xxh3_premix(flip of column seed c)
+  uint64_t kchk;                    // xxh3_premix(flip of the checksum seed)
 };
-// hist2d[ct * nbins + b] = entries of bin b among the records of count tile ct
-cudaError_t gutter_count_tiles(const void *d_rec, uint64_t n, GutterGeom g, uint32_t *hist2d,
-                               uint32_t *status, cudaStream_t s);
-// per bin: hist2d column -> exclusive prefix over count tiles; totals[b] = column sum
-cudaError_t gutter_colscan(uint32_t *hist2d, uint32_t n_ct, uint32_t nbins, uint64_t *totals,
-                           cudaStream_t s);
-// Hash every record once and write its two 32-byte entries. With hist2d: positions are
-// base[b] + hist2d[ct][b] + rank inside the count tile; without: global cursors (cursor[b]
-// starts at base[b]).
-cudaError_t gutter_hash_scatter(const void *d_rec, uint64_t n, GutterGeom g, HashGeom hg,
-                                const uint32_t *hist2d, const uint64_t *base, uint64_t *cursor,
-                                uint4 *out, cudaStream_t s);
+struct PlaneGeom {
+  uint32_t V, C, B, sketch_words;
+  uint32_t tile_shift;  // W = 1 << tile_shift vertices per tile = per gutter bin
+  uint32_t ntiles;
+  uint32_t direct_max;  // a tile with fewer entries is updated in place in HBM
+};
+PlaneHash plane_hash(uint64_t seed, uint32_t C, uint32_t B);
+// Records per tile of the hash sort-scatter for this bin count (0: the bins do not fit).
+uint32_t hash_sort_tile(uint32_t nbins, size_t smem_budget);
+// Hash every record once and write its two endpoint entries, counting-sorted by bin: keys to
+// keys[base[b] + ...], depth codes to codes[base[b] + ...]; fill (nbins u32) starts at zero.
+cudaError_t gutter_hash_sort(const void *d_rec, uint64_t n, GutterGeom g, const PlaneHash &ph,
+                             uint32_t rec_tile, const uint64_t *base, uint32_t *fill, uint2 *keys,
+                             uint4 *codes, cudaStream_t s);
+// Applies every buffered chunk (coded or plain entries) tile by tile through bucket planes.
+size_t plane_update_smem(uint32_t tile_shift, int threads);
+int plane_update_ctas_per_sm(uint32_t tile_shift, int threads);
+cudaError_t plane_update(const PlaneGeom &g, const PlaneHash &ph, uint8_t *sketches,
+                         const uint8_t *gutter, const ChunkTable &chunks, const uint32_t *bin_off,
+                         int nchunks, uint32_t *work_counter, uint32_t *status, int grid,
+                         int threads, cudaStream_t s);
+// Register-only rate of the per-column hash of this ingest: premixed input XOR a premixed
+// column constant, rrmxmx tail, depth code (blocks x threads x iters x 8 hashes).
+cudaError_t plane_hash_peak(uint32_t iters, int blocks, int threads, uint64_t *out, cudaStream_t s);
+// Rate of the bucket-plane update's shared-memory step without hashing or global traffic:
+// blocks x 1024 threads x iters entries, each 32 slot steps of two red.shared.xor.
+cudaError_t plane_update_peak(uint32_t iters, int blocks, uint32_t *out, cudaStream_t s);
+
 // bin_off[b] = scanned[b * stride], bin_off[nbins] = *total  (u32, relative to chunk base)
 cudaError_t gutter_bin_offsets(const uint64_t *scanned, uint32_t stride, uint32_t nbins,
                                const uint64_t *total, uint32_t *bin_off, cudaStream_t s);
@@ -234,14 +269,6 @@ int num_sms();
 void sketch_sizing(uint32_t V, double f, uint32_t &C, uint32_t &B);
 // samples, columns per sample and B of CameoSketch (cube = false: C = samples) or CubeSketch
 void sketch_sizing_alg(uint32_t V, double f, bool cube, uint32_t &samples, uint32_t &cps, uint32_t &B);
-
-// Register-only hash throughput probe: n_threads * iters * 8 hashes.
-cudaError_t hash_peak(uint64_t seed, uint32_t iters, int blocks, int threads, uint64_t *out,
-                      cudaStream_t s);
-
-// Shared-memory bucket-update probe: blocks x 1024 threads x iters updates of 3 atomicXor
-// each into nb staged buckets (out: blocks * 1024 words).
-cudaError_t update_peak(uint32_t nb, uint32_t iters, int blocks, uint32_t *out, cudaStream_t s);
 
 // Kernel launches issued by the host wrappers of this file (monotonic, process-wide).
 uint64_t launch_count();

@@ -122,6 +122,17 @@ __global__ void k_noalloc_tail(uint32_t *sketches, const uint2 *entries, const u
       return noalloc_fail(GZ_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
   } while (0)
 
+// Once a call has queued work on its stream, every return waits for that work: the scratch array
+// must be idle before the lock is released, or the next call (on any stream) would overwrite the
+// regions the queued kernels still use. Declared after the lock guard, so it runs first.
+struct StreamDrain {
+  cudaStream_t s;
+  bool armed = false;
+  ~StreamDrain() {
+    if (armed) cudaStreamSynchronize(s);
+  }
+};
+
 }  // namespace
 
 extern "C" {
@@ -146,6 +157,7 @@ int gz_ingest_records_noalloc(void *d_sketches, uint32_t num_vertices, uint64_t 
   cudaStream_t s = static_cast<cudaStream_t>(stream_ptr);
 
   std::lock_guard<std::mutex> lk(g_noalloc_mtx);
+  StreamDrain drain{s};
   uint8_t *scratch = nullptr;
   int rc = scratch_for_current_device(&scratch);
   if (rc != GZ_OK) return rc;
@@ -188,6 +200,7 @@ int gz_ingest_records_noalloc(void *d_sketches, uint32_t num_vertices, uint64_t 
   uint64_t hflip[kNoAllocMaxColumns + 1];
   for (uint32_t c = 0; c < C; ++c) hflip[c] = gz::xxh3_flip(seed + 5ull * c);
   hflip[C] = gz::xxh3_flip(seed);
+  drain.armed = true;
   NA_CUDA(cudaMemcpyAsync(flip, hflip, flip_bytes, cudaMemcpyHostToDevice, s));
   NA_CUDA(cudaMemsetAsync(counts, 0, sizeof(uint64_t) * nbins, s));
   NA_CUDA(cudaMemsetAsync(fill, 0, sizeof(uint32_t) * nbins, s));
@@ -234,9 +247,9 @@ int gz_ingest_records_noalloc(void *d_sketches, uint32_t num_vertices, uint64_t 
         nb * 3, C, B, flip);
     NA_CUDA(cudaGetLastError());
   }
-  NA_CUDA(cudaStreamSynchronize(s));
   uint32_t st = 0;
-  NA_CUDA(cudaMemcpy(&st, status, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  NA_CUDA(cudaMemcpyAsync(&st, status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  NA_CUDA(cudaStreamSynchronize(s));
   if (st & gz::kStatusTimeout) return noalloc_fail(GZ_ERR_TIMEOUT, "a bounded device wait timed out");
   if (st & gz::kStatusBadVertex)
     return noalloc_fail(GZ_ERR_BAD_VERTEX, "a record named a vertex id >= V; it was dropped");

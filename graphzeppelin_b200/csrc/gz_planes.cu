@@ -1,0 +1,602 @@
+// gz_planes.cu -- hash-once record ingest for CameoSketch sketches of at most 31 columns.
+//
+// Sketch::update (src/sketch.cpp:69-83) XORs an edge index and its checksum into the
+// deterministic bucket and into bucket (c, depth_c(idx)) of every column c, and
+// CCSketchAlg::update / apply_update_batch (src/cc_sketch_alg.cpp:106-133) apply it to both
+// endpoint sketches. Every vertex sketch uses the same seed (src/cc_sketch_alg.cpp:21), so the two
+// endpoints get the same depths and the same checksum: here the C depth hashes of a record are
+// computed once, where the reference computes them per endpoint.
+//
+//   k_hash_sort_scatter  per tile of records: the two endpoint entries counting-sorted by gutter
+//                        bin in shared memory, each record hashed once into C 4-bit depth codes,
+//                        the runs written out coalesced as keys {vertex, neighbour} plus a
+//                        parallel array of codes (one uint4 per entry).
+//   k_plane_update       per tile of W vertices (one gutter bin): the entries XORed into bucket
+//                        planes in shared memory that start at zero, then each vertex's rows XORed
+//                        into its sketch in HBM.
+//
+// Bucket planes. A warp takes 32 entries, one per lane. At step t = 0..31 lane l handles slot
+// l ^ t of its entry: slot c < C is column c, slot C the deterministic bucket, higher slots are
+// unused. A plane row is 32 words, so slot s is shared-memory bank s and the 32 lanes of a step hit
+// 32 different banks whatever their vertices and depths: the red.shared.xor never conflict (the
+// per-entry ordering, every lane on column c at once, concentrates lanes on a few banks because
+// depth 0 takes half the updates). Each bucket is kept as three words,
+//   A = XOR of (neighbour | 1 << 31) over the entries whose neighbour is above the vertex,
+//   B = the same over the other entries,
+//   G = XOR of their checksums,
+// so one update XORs two words (A or B, and G) instead of three. With idx = (min << 32) | max
+// (concat_pairing_fn, src/util.cpp:45-51) the bucket's alpha is recovered as
+//   alpha low  = low31(A) ^ (top bit of B ? vertex : 0),
+//   alpha high = low31(B) ^ (top bit of A ? vertex : 0),
+// the top bits holding the parity of each kind's entry count (vertex ids are below 2^31).
+// Rows hold depths 0 .. kPlaneRows - 2; the last row is scratch. Depths at or above it (2^-11 of
+// the column updates) are XORed into the sketch in HBM with global atomics; those rows are never
+// touched by the write-back, which rewrites only the rows the planes hold.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "gz_common.cuh"
+#include "gz_device.cuh"
+#include "gz_kernels.cuh"
+
+namespace gz {
+
+namespace {
+
+using namespace gz::dev;
+
+constexpr uint32_t kPlaneThr = kPlaneRows - 1;               // first depth not held in the planes
+constexpr uint32_t kPlaneBytes = kPlaneRows * kPlaneSlots * 4;  // one plane of one vertex
+constexpr uint32_t kVertBytes = 3 * kPlaneBytes;              // planes A, B, G of one vertex
+constexpr uint32_t kWbRows = 4;                               // rows per write-back pass
+constexpr uint32_t kWbStride = 3 * kWbRows + 1;               // words per slot (odd: no conflicts)
+constexpr uint32_t kWbWords = kPlaneSlots * kWbStride;        // write-back buffer of one warp
+
+// C depth codes of one record (edge index (hi << 32) | lo), column c in bits 4c..4c+3 of the
+// 128-bit result; unused nibbles are zero.
+__device__ __forceinline__ uint4 record_codes(uint32_t lo, uint32_t hi, const PlaneHash &ph) {
+  const uint64_t pm = xxh3_premix(((uint64_t)lo << 32) | hi);
+  const uint32_t cap = 1u << min(ph.B, kDepthEscape);
+  uint32_t w[4] = {0, 0, 0, 0};
+#pragma unroll
+  for (int c = 0; c < 18; ++c) w[c >> 3] |= depth_code(pm ^ ph.kcol[c], cap) << (4 * (c & 7));
+#pragma unroll
+  for (int c = 18; c < (int)kPlaneMaxColumns; ++c)
+    if (c < (int)ph.C) w[c >> 3] |= depth_code(pm ^ ph.kcol[c], cap) << (4 * (c & 7));
+  return make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+// ------------------------------------------------------------------------------------------------
+// hash sort-scatter (records in, coded entries out)
+// ------------------------------------------------------------------------------------------------
+// Exclusive scan over the threads of a block of any multiple of 32 threads (<= 1024).
+__device__ __forceinline__ uint32_t block_scan(uint32_t x, uint32_t *ws /*32*/) {
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  uint32_t inc = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(kFull, inc, o);
+    if (lane >= (uint32_t)o) inc += y;
+  }
+  if (lane == 31) ws[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = lane < nwarps ? ws[lane] : 0u;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(kFull, w, o);
+      if (lane >= (uint32_t)o) w += y;
+    }
+    ws[lane] = w;
+  }
+  __syncthreads();
+  const uint32_t r = (warp ? ws[warp - 1] : 0u) + inc - x;
+  __syncthreads();
+  return r;
+}
+
+// Two CTAs of 512 threads per SM, so that one CTA's staging, scan and write-out overlap the
+// other's hashing. Per tile of rec_tile records: stage them (coalesced 128-bit loads), count
+// their endpoint entries per bin, reserve one run per non-empty bin in the gutter (one global
+// atomic each), hash every record once, place both entries in bin order in shared memory, and
+// write the runs out.
+constexpr int kHashSortThreads = 512;
+template <int RPT>
+__global__ void __launch_bounds__(kHashSortThreads, 2)
+k_hash_sort_scatter(const uint8_t *__restrict__ rec, uint64_t n, GutterGeom g, PlaneHash ph,
+                    uint32_t rec_tile, const uint64_t *__restrict__ base,
+                    uint32_t *__restrict__ fill, uint2 *__restrict__ keys,
+                    uint4 *__restrict__ codes) {
+  extern __shared__ __align__(16) uint8_t gsm[];
+  __shared__ uint32_t ws[32];
+  const uint32_t nb = g.nbins, nb4 = (nb + 3) & ~3u;
+  uint32_t *s_cur = reinterpret_cast<uint32_t *>(gsm);  // counts, then placement cursors
+  uint32_t *s_rel = s_cur + nb4;  // a bin's run: gutter position minus position in the tile
+  uint2 *s_key = reinterpret_cast<uint2 *>(s_rel + nb4);
+  uint4 *s_code = reinterpret_cast<uint4 *>(s_key + 2 * (size_t)rec_tile);
+  // the staged records share the key area: they are parsed into registers before the first key
+  // is placed, and the next tile is staged only after the write-out
+  uint8_t *s_rec = reinterpret_cast<uint8_t *>(s_key);
+  const uint32_t per_thread = (nb + blockDim.x - 1) / blockDim.x;  // bins per thread (<= 16)
+  for (uint64_t t0 = blockIdx.x * (uint64_t)rec_tile; t0 < n; t0 += (uint64_t)gridDim.x * rec_tile) {
+    const uint32_t cnt = (uint32_t)(n - t0 < rec_tile ? n - t0 : rec_tile);
+    for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) s_cur[b] = 0u;
+    const uint32_t shift = stage_records(rec, t0, cnt, s_rec);
+    __syncthreads();
+    // 1. this thread's records into registers, then their per-bin counts
+    uint32_t ru[RPT], rv[RPT];
+#pragma unroll
+    for (int k = 0; k < RPT; ++k) {
+      const uint32_t i = threadIdx.x + k * blockDim.x;
+      ru[k] = rv[k] = 0xffffffffu;
+      if (i < cnt) {
+        parse_record(s_rec, shift, i, ru[k], rv[k]);
+        if (ru[k] >= g.V || rv[k] >= g.V) ru[k] = 0xffffffffu;  // dropped (the count pass flags it)
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < RPT; ++k)
+      if (ru[k] != 0xffffffffu) {
+        atomicAdd(&s_cur[ru[k] >> g.bin_shift], 1u);
+        atomicAdd(&s_cur[rv[k] >> g.bin_shift], 1u);
+      }
+    __syncthreads();
+    // 2. run offsets inside the tile (bins [tid*per_thread, +per_thread) per thread) and one run
+    //    reserved per non-empty bin in the gutter
+    uint32_t sum = 0;
+    for (uint32_t k = 0; k < per_thread; ++k) {
+      const uint32_t b = threadIdx.x * per_thread + k;
+      sum += b < nb ? s_cur[b] : 0u;
+    }
+    uint32_t run = block_scan(sum, ws);
+    for (uint32_t k = 0; k < per_thread; ++k) {
+      const uint32_t b = threadIdx.x * per_thread + k;
+      if (b < nb) {
+        const uint32_t c = s_cur[b];
+        s_rel[b] = c ? (uint32_t)base[b] + atomicAdd(&fill[b], c) - run : 0u;
+        s_cur[b] = run;
+        run += c;
+      }
+    }
+    __syncthreads();
+    // 3. slots claimed, each record hashed once, both endpoint entries placed in bin order
+    uint32_t pu[RPT], pv[RPT];
+#pragma unroll
+    for (int k = 0; k < RPT; ++k)
+      if (ru[k] != 0xffffffffu) {
+        pu[k] = atomicAdd(&s_cur[ru[k] >> g.bin_shift], 1u);
+        pv[k] = atomicAdd(&s_cur[rv[k] >> g.bin_shift], 1u);
+      }
+#pragma unroll
+    for (int k = 0; k < RPT; ++k)
+      if (ru[k] != 0xffffffffu) {
+        const uint4 cw = record_codes(max(ru[k], rv[k]), min(ru[k], rv[k]), ph);
+        s_key[pu[k]] = make_uint2(ru[k], rv[k]);
+        s_key[pv[k]] = make_uint2(rv[k], ru[k]);
+        s_code[pu[k]] = cw;
+        s_code[pv[k]] = cw;
+      }
+    __syncthreads();
+    // 4. coalesced write-out of the runs
+    const uint32_t total = s_cur[nb - 1];
+    for (uint32_t j = threadIdx.x; j < total; j += blockDim.x) {
+      const uint2 x = s_key[j];
+      const uint32_t dst = s_rel[x.x >> g.bin_shift] + j;
+      keys[dst] = x;
+      codes[dst] = s_code[j];
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// bucket-plane sketch update
+// ------------------------------------------------------------------------------------------------
+__device__ __forceinline__ void red_xor_shared(uint32_t addr, uint32_t v) {
+  asm volatile("red.shared.xor.b32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ uint32_t nibble_of(const uint32_t (&c4)[4], uint32_t c) {
+  const uint32_t w = c < 16 ? (c < 8 ? c4[0] : c4[1]) : (c < 24 ? c4[2] : c4[3]);
+  return (w >> (4 * (c & 7))) & 15u;
+}
+
+// Flags of the codes at or above the scratch row: per word, bit 4 of byte lane j flags nibble 2j
+// and bit 5 flags nibble 2j + 1 (for a nibble n < 16, n + 5 carries into bit 4 of its byte lane
+// exactly when n >= 11).
+__device__ __forceinline__ uint32_t high_code_flags(uint32_t w) {
+  static_assert(kPlaneThr == 11, "the byte-lane test below is written for threshold 11");
+  const uint32_t lo = ((w & 0x0f0f0f0fu) + 0x05050505u) & 0x10101010u;
+  const uint32_t hi = ((((w >> 4) & 0x0f0f0f0fu) + 0x05050505u) & 0x10101010u) << 1;
+  return lo | hi;
+}
+
+// Bucket (c, d) of vertex v's sketch in HBM, three 32-bit atomics (alpha low, alpha high, gamma).
+__device__ __forceinline__ void xor_bucket_global(uint32_t *sk, uint32_t bucket, uint32_t lo,
+                                                  uint32_t hi, uint32_t chk) {
+  uint32_t *p = sk + 3 * bucket;
+  atomicXor(p, lo);
+  atomicXor(p + 1, hi);
+  atomicXor(p + 2, chk);
+}
+
+// Moves the codes at or above the scratch row into HBM (exact depth; code 15 means 15 or more
+// and is recomputed) and points them at the scratch row. Rare per column (2^-11), so only the
+// flagged nibbles are visited.
+__device__ __noinline__ uint4 spill_high_codes(uint4 cw, uint4 fl, uint64_t pm, uint32_t lo,
+                                               uint32_t hi, uint32_t chk, uint32_t *sk,
+                                               const uint64_t *s_kcol, uint32_t B) {
+  uint32_t c4[4] = {cw.x, cw.y, cw.z, cw.w};
+  const uint32_t f4[4] = {fl.x, fl.y, fl.z, fl.w};
+#pragma unroll
+  for (int w = 0; w < 4; ++w) {
+    uint32_t f = f4[w];
+    while (f) {
+      const uint32_t bit = __ffs(f) - 1;  // 4 + 8j (nibble 2j) or 5 + 8j (nibble 2j + 1)
+      f &= f - 1;
+      const uint32_t nib = 2 * (bit >> 3) + (bit & 1u);  // nibble inside the word
+      const uint32_t c = 8 * w + nib, sh = 4 * nib;
+      const uint32_t code = (c4[w] >> sh) & 15u;
+      const uint32_t d = code < kDepthEscape ? code : depth_exact(pm ^ s_kcol[c], B);
+      if (d < B) xor_bucket_global(sk, c * B + d, lo, hi, chk);
+      c4[w] = (c4[w] & ~(15u << sh)) | (kPlaneThr << sh);
+    }
+  }
+  return make_uint4(c4[0], c4[1], c4[2], c4[3]);
+}
+
+// nibble t of the result = nibble t ^ lane of the input (5 index bits: half-byte, byte pair in
+// the word, word)
+__device__ __forceinline__ void permute_codes(uint32_t (&c4)[4], uint32_t lane) {
+  if (lane & 1) {
+#pragma unroll
+    for (int w = 0; w < 4; ++w) c4[w] = ((c4[w] >> 4) & 0x0f0f0f0fu) | ((c4[w] & 0x0f0f0f0fu) << 4);
+  }
+  const uint32_t q = (lane >> 1) & 3u;
+  const uint32_t sel = q | ((1u ^ q) << 4) | ((2u ^ q) << 8) | ((3u ^ q) << 12);
+#pragma unroll
+  for (int w = 0; w < 4; ++w) c4[w] = __byte_perm(c4[w], 0, sel);
+  if (lane & 8) {
+    uint32_t x = c4[0]; c4[0] = c4[1]; c4[1] = x;
+    x = c4[2]; c4[2] = c4[3]; c4[3] = x;
+  }
+  if (lane & 16) {
+    uint32_t x = c4[0]; c4[0] = c4[2]; c4[2] = x;
+    x = c4[1]; c4[1] = c4[3]; c4[3] = x;
+  }
+}
+
+__device__ __forceinline__ void plane_entry(uint2 key, uint4 cw, bool valid, uint32_t lane,
+                                            uint32_t sp, uint32_t tile_mask, uint32_t *gsk,
+                                            uint32_t sketch_words, const uint64_t *s_kcol,
+                                            uint64_t kchk, uint32_t C, uint32_t B) {
+  const uint32_t v = key.x, u = key.y;
+  const uint32_t lo = max(u, v), hi = min(u, v);  // idx = (min << 32) | max
+  const uint64_t pm = xxh3_premix(((uint64_t)lo << 32) | hi);
+  const uint32_t chk = valid ? tail_lo32(pm ^ kchk) : 0u;
+  const uint32_t val = valid ? (u | 0x80000000u) : 0u;  // invalid lanes XOR zeros
+  const uint32_t p = u > v ? 0u : 1u;                    // plane A or B
+  uint32_t c4[4] = {cw.x, cw.y, cw.z, cw.w};
+  const uint4 fl = make_uint4(high_code_flags(cw.x), high_code_flags(cw.y), high_code_flags(cw.z),
+                              high_code_flags(cw.w));
+  if (valid && (fl.x | fl.y | fl.z | fl.w)) {
+    const uint4 x = spill_high_codes(cw, fl, pm, lo, hi, chk, gsk + (uint64_t)v * sketch_words, s_kcol, B);
+    c4[0] = x.x;
+    c4[1] = x.y;
+    c4[2] = x.z;
+    c4[3] = x.w;
+  }
+  permute_codes(c4, lane);
+  // bits 2..6 of base are the lane (sp is 128-byte aligned, the rest multiples of 128), so
+  // base ^ (t << 2) addresses slot lane ^ t of the same row
+  const uint32_t base = sp + (v & tile_mask) * kVertBytes + p * kPlaneBytes + (lane << 2);
+  const uint32_t dg = (2u - p) * kPlaneBytes;
+#pragma unroll
+  for (int t = 0; t < 32; ++t) {
+    const uint32_t d = (c4[t >> 3] >> (4 * (t & 7))) & 15u;
+    const uint32_t a = (base ^ (uint32_t)(t << 2)) + (d << 7);
+    red_xor_shared(a, val);
+    red_xor_shared(a + dg, chk);
+  }
+}
+
+// One entry applied straight to HBM (sparse tiles): deterministic bucket, then each column.
+__device__ __forceinline__ void entry_in_place(uint2 key, uint4 cw, uint32_t *gsk,
+                                               uint32_t sketch_words, const uint64_t *s_kcol,
+                                               uint64_t kchk, uint32_t C, uint32_t B) {
+  const uint32_t v = key.x, u = key.y;
+  const uint32_t lo = max(u, v), hi = min(u, v);
+  const uint64_t pm = xxh3_premix(((uint64_t)lo << 32) | hi);
+  const uint32_t chk = tail_lo32(pm ^ kchk);
+  uint32_t *sk = gsk + (uint64_t)v * sketch_words;
+  xor_bucket_global(sk, C * B, lo, hi, chk);
+  const uint32_t c4[4] = {cw.x, cw.y, cw.z, cw.w};
+  for (uint32_t c = 0; c < C; ++c) {
+    const uint32_t code = nibble_of(c4, c);
+    const uint32_t d = code < kDepthEscape ? code : depth_exact(pm ^ s_kcol[c], B);
+    if (d < B) xor_bucket_global(sk, c * B + d, lo, hi, chk);
+  }
+}
+
+__global__ void __launch_bounds__(1024, 1)
+k_plane_update(PlaneGeom g, PlaneHash ph, uint8_t *__restrict__ sketches,
+               const uint8_t *__restrict__ gutter, ChunkTable chunks,
+               const uint32_t *__restrict__ bin_off, int nchunks, uint32_t *work_counter) {
+  extern __shared__ __align__(16) uint8_t dsm[];
+  __shared__ uint64_t s_kcol[kPlaneMaxColumns];
+  __shared__ uint32_t s_claim[2];
+  const uint32_t W = 1u << g.tile_shift, tile_mask = W - 1;
+  const uint32_t nwarps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t s0 = smem_u32(dsm);
+  const uint32_t pad = (128u - (s0 & 127u)) & 127u;
+  uint8_t *planes = dsm + pad;  // W vertices x planes A, B, G x kPlaneRows x 32 words
+  const uint32_t sp = s0 + pad;
+  uint32_t *wbuf = reinterpret_cast<uint32_t *>(planes + (size_t)W * kVertBytes) + warp * kWbWords;
+  for (uint32_t i = threadIdx.x; i < g.C; i += blockDim.x) s_kcol[i] = ph.kcol[i];
+  uint32_t *gsk = reinterpret_cast<uint32_t *>(sketches);
+  const uint32_t stride = g.ntiles + 1;  // one bin per tile
+  const uint32_t C = g.C, B = g.B;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const uint32_t t = atomicAdd(work_counter, 1u);
+      uint32_t total = 0;
+      if (t < g.ntiles)
+        for (int k = 0; k < nchunks; ++k)
+          total += bin_off[(uint64_t)k * stride + t + 1] - bin_off[(uint64_t)k * stride + t];
+      s_claim[0] = t;
+      s_claim[1] = total;
+    }
+    __syncthreads();
+    const uint32_t t = s_claim[0], total = s_claim[1];
+    if (t >= g.ntiles) break;
+    if (total == 0) {
+      __syncthreads();
+      continue;
+    }
+    if (total < g.direct_max) {
+      // few entries: updated in place in HBM (no planes to clear and write back)
+      for (int k = 0; k < nchunks; ++k) {
+        const uint64_t b = bin_off[(uint64_t)k * stride + t], e = bin_off[(uint64_t)k * stride + t + 1];
+        const uint2 *keys = reinterpret_cast<const uint2 *>(gutter + chunks.base[k]);
+        const uint4 *codes = chunks.kind[k] == kEntryCoded ? reinterpret_cast<const uint4 *>(gutter + chunks.aux[k]) : nullptr;
+        for (uint64_t i = b + threadIdx.x; i < e; i += blockDim.x) {
+          const uint2 key = keys[i];
+          const uint4 cw = codes ? codes[i] : record_codes(max(key.x, key.y), min(key.x, key.y), ph);
+          entry_in_place(key, cw, gsk, g.sketch_words, s_kcol, ph.kchk, C, B);
+        }
+      }
+      __syncthreads();
+      continue;
+    }
+    {
+      uint4 *pz = reinterpret_cast<uint4 *>(planes);
+      const uint32_t n16 = W * (kVertBytes / 16);
+      for (uint32_t i = threadIdx.x; i < n16; i += blockDim.x) pz[i] = make_uint4(0, 0, 0, 0);
+    }
+    __syncthreads();
+    for (int k = 0; k < nchunks; ++k) {
+      const uint32_t b = bin_off[(uint64_t)k * stride + t], e = bin_off[(uint64_t)k * stride + t + 1];
+      const uint2 *keys = reinterpret_cast<const uint2 *>(gutter + chunks.base[k]);
+      const uint4 *codes = chunks.kind[k] == kEntryCoded ? reinterpret_cast<const uint4 *>(gutter + chunks.aux[k]) : nullptr;
+      // each warp takes batches of 32 entries; the next batch's entry is loaded while this one
+      // is applied (an invalid lane XORs zeros into vertex 0 of the tile)
+      const uint2 pad_key = make_uint2((uint32_t)t << g.tile_shift, (uint32_t)t << g.tile_shift);
+      uint32_t i0 = b + warp * 32;
+      bool nvalid = i0 + lane < e;
+      uint2 nkey = nvalid ? keys[i0 + lane] : pad_key;
+      uint4 ncw = nvalid && codes ? codes[i0 + lane] : make_uint4(0, 0, 0, 0);
+      for (; i0 < e; i0 += nwarps * 32) {
+        const uint2 key = nkey;
+        uint4 cw = ncw;
+        const bool valid = nvalid;
+        const uint32_t in = i0 + nwarps * 32 + lane;
+        nvalid = in < e;
+        if (nvalid) {
+          nkey = keys[in];
+          if (codes) ncw = codes[in];
+        }
+        if (valid && !codes) cw = record_codes(max(key.x, key.y), min(key.x, key.y), ph);
+        plane_entry(key, cw, valid, lane, sp, tile_mask, gsk, g.sketch_words, s_kcol, ph.kchk, C, B);
+      }
+    }
+    __syncthreads();
+    // write-back: one warp per vertex; rows [r0, r0 + 4) of every slot are converted to the
+    // reference bucket words (lanes = slots, conflict-free), staged with an odd stride, and XORed
+    // into the sketch in HBM column run by column run
+    const uint32_t R = min(B, kPlaneThr);
+    for (uint32_t vl = warp; vl < W; vl += nwarps) {
+      const uint32_t vg = (t << g.tile_shift) + vl;
+      if (vg >= g.V) continue;
+      const uint32_t *pa = reinterpret_cast<const uint32_t *>(planes + (size_t)vl * kVertBytes);
+      const uint32_t *pb = pa + kPlaneRows * kPlaneSlots;
+      const uint32_t *pg = pb + kPlaneRows * kPlaneSlots;
+      uint32_t *sk = gsk + (uint64_t)vg * g.sketch_words;
+      for (uint32_t r0 = 0; r0 < R; r0 += kWbRows) {
+        const uint32_t nr = min(kWbRows, R - r0);
+        for (uint32_t rr = 0; rr < nr; ++rr) {
+          const uint32_t r = r0 + rr;
+          const uint32_t a = pa[r * kPlaneSlots + lane], bq = pb[r * kPlaneSlots + lane];
+          const uint32_t gm = pg[r * kPlaneSlots + lane];
+          wbuf[lane * kWbStride + rr * 3 + 0] = (a & 0x7fffffffu) ^ ((bq >> 31) ? vg : 0u);
+          wbuf[lane * kWbStride + rr * 3 + 1] = (bq & 0x7fffffffu) ^ ((a >> 31) ? vg : 0u);
+          wbuf[lane * kWbStride + rr * 3 + 2] = gm;
+        }
+        __syncwarp();
+        const uint32_t nw = 3 * nr, j = lane & 15u;
+        if (j < nw) {
+#pragma unroll 4
+          for (uint32_t c = lane >> 4; c < C; c += 2) {
+            const uint32_t x = wbuf[c * kWbStride + j];
+            if (x) {
+              uint32_t *q = sk + 3 * (c * B + r0) + j;
+              *q ^= x;
+            }
+          }
+        }
+        if (r0 == 0 && lane < 3) {  // deterministic bucket: slot C, row 0
+          const uint32_t x = wbuf[C * kWbStride + lane];
+          if (x) sk[3 * C * B + lane] ^= x;
+        }
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Register-only rate of the per-column hash above: eight independent chains per thread, each
+// step a premixed input XOR a column constant, the rrmxmx tail and the depth code, the next input
+// being this one XOR its code.
+__global__ void k_plane_hash_peak(uint32_t iters, uint64_t *out) {
+  const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  uint64_t x[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) x[k] = xxh3_premix(tid * 8 + k);
+  uint32_t acc = 0;
+  for (uint32_t i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const uint32_t d = depth_code(x[k] ^ (0x9E3779B97F4A7C15ULL * (uint64_t)(k + 1)), 1u << kDepthEscape);
+      acc += d;
+      x[k] ^= d;
+    }
+  }
+  uint64_t r = acc;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) r ^= x[k];
+  out[tid] = r;
+}
+
+// Rate of the plane update's shared-memory step alone: 32 vertices of planes, each thread one
+// synthetic entry per iteration (codes 0..3, random vertex and plane), 32 slot steps of two
+// red.shared.xor each, addressed exactly as plane_entry does.
+__global__ void __launch_bounds__(1024, 1) k_plane_update_peak(uint32_t iters, uint32_t *out) {
+  extern __shared__ __align__(16) uint8_t dsm[];
+  const uint32_t s0 = smem_u32(dsm);
+  const uint32_t pad = (128u - (s0 & 127u)) & 127u;
+  uint8_t *planes = dsm + pad;
+  const uint32_t sp = s0 + pad, lane = threadIdx.x & 31;
+  uint32_t *pw = reinterpret_cast<uint32_t *>(planes);
+  for (uint32_t i = threadIdx.x; i < kPlaneMaxTile * kVertBytes / 4; i += blockDim.x) pw[i] = 0;
+  __syncthreads();
+  uint32_t x = fmix32_(blockIdx.x * 1024u + threadIdx.x);
+  for (uint32_t it = 0; it < iters; ++it) {
+    x = x * 1664525u + 1013904223u;
+    uint32_t c4[4];
+#pragma unroll
+    for (int w = 0; w < 4; ++w) c4[w] = fmix32_(x + (uint32_t)w) & 0x33333333u;
+    const uint32_t v = x >> 27, p = (x >> 26) & 1u;
+    const uint32_t val = x | 0x80000000u, chk = x * 747796405u;
+    const uint32_t base = sp + v * kVertBytes + p * kPlaneBytes + (lane << 2);
+    const uint32_t dg = (2u - p) * kPlaneBytes;
+#pragma unroll
+    for (int t = 0; t < 32; ++t) {
+      const uint32_t d = (c4[t >> 3] >> (4 * (t & 7))) & 15u;
+      const uint32_t a = (base ^ (uint32_t)(t << 2)) + (d << 7);
+      red_xor_shared(a, val);
+      red_xor_shared(a + dg, chk);
+    }
+  }
+  __syncthreads();
+  uint32_t acc = 0;
+  for (uint32_t i = threadIdx.x; i < kPlaneMaxTile * kVertBytes / 4; i += blockDim.x) acc ^= pw[i];
+  out[blockIdx.x * 1024u + threadIdx.x] = acc;
+}
+
+}  // namespace
+
+// ================================================================================================
+// host wrappers
+// ================================================================================================
+PlaneHash plane_hash(uint64_t seed, uint32_t C, uint32_t B) {
+  PlaneHash ph{};
+  ph.C = C;
+  ph.B = B;
+  for (uint32_t c = 0; c < C && c < kPlaneMaxColumns; ++c)
+    ph.kcol[c] = xxh3_premix(xxh3_flip(seed + 5ull * c));  // column_seed (include/sketch.h:175-176)
+  ph.kchk = xxh3_premix(xxh3_flip(seed));                  // checksum_seed
+  return ph;
+}
+
+uint32_t hash_sort_tile(uint32_t nbins, size_t smem_budget) {
+  // two CTAs per SM: each gets half the SM's shared memory (less the per-CTA reservation)
+  const size_t per_cta = std::min<size_t>(smem_budget, (228 * 1024 - 2 * 1024) / 2);
+  const size_t fixed = (size_t)2 * ((nbins + 3) & ~3u) * 4 + 256;
+  if (nbins > kSortBinsMax || fixed >= per_cta) return 0;
+  // 2 entries per record: 8 B of key + 16 B of codes each
+  const size_t t = std::min<size_t>((per_cta - fixed) / 48, 4 * kHashSortThreads);
+  return (uint32_t)(t / kHashSortThreads * kHashSortThreads);
+}
+
+cudaError_t gutter_hash_sort(const void *d_rec, uint64_t n, GutterGeom g, const PlaneHash &ph,
+                             uint32_t rec_tile, const uint64_t *base, uint32_t *fill, uint2 *keys,
+                             uint4 *codes, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  if (rec_tile < kHashSortThreads || rec_tile > 4 * kHashSortThreads || rec_tile % kHashSortThreads)
+    return cudaErrorInvalidValue;
+  const size_t smem = (size_t)2 * ((g.nbins + 3) & ~3u) * 4 + (size_t)rec_tile * 48;
+  const uint64_t tiles = (n + rec_tile - 1) / rec_tile;
+  const uint8_t *rec = reinterpret_cast<const uint8_t *>(d_rec);
+  auto launch = [&](auto kern) -> cudaError_t {
+    cudaError_t e = smem_optin(kern);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kHashSortThreads, smem) != cudaSuccess || per_sm < 1)
+      per_sm = 1;
+    const int G = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)num_sms() * per_sm, tiles));
+    kern<<<G, kHashSortThreads, smem, s>>>(rec, n, g, ph, rec_tile, base, fill, keys, codes);
+    add_launches(1);
+    return cudaGetLastError();
+  };
+  switch (rec_tile / kHashSortThreads) {
+    case 1: return launch(k_hash_sort_scatter<1>);
+    case 2: return launch(k_hash_sort_scatter<2>);
+    case 3: return launch(k_hash_sort_scatter<3>);
+    default: return launch(k_hash_sort_scatter<4>);
+  }
+}
+
+size_t plane_update_smem(uint32_t tile_shift, int threads) {
+  return 128 + ((size_t)kVertBytes << tile_shift) + (size_t)(threads / 32) * kWbWords * 4;
+}
+
+int plane_update_ctas_per_sm(uint32_t tile_shift, int threads) {
+  int n = 0;
+  if (smem_optin(k_plane_update) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_plane_update, threads,
+                                                    plane_update_smem(tile_shift, threads)) != cudaSuccess)
+    return 1;
+  return n > 0 ? n : 1;
+}
+
+cudaError_t plane_update(const PlaneGeom &g, const PlaneHash &ph, uint8_t *sketches,
+                         const uint8_t *gutter, const ChunkTable &chunks, const uint32_t *bin_off,
+                         int nchunks, uint32_t *work_counter, uint32_t * /*status*/, int grid,
+                         int threads, cudaStream_t s) {
+  if (g.C > kPlaneMaxColumns || g.tile_shift > 5 || threads % 32 || threads < 32 || threads > 1024)
+    return cudaErrorInvalidValue;
+  cudaError_t e = smem_optin(k_plane_update);
+  if (e != cudaSuccess) return e;
+  k_plane_update<<<grid, threads, plane_update_smem(g.tile_shift, threads), s>>>(
+      g, ph, sketches, gutter, chunks, bin_off, nchunks, work_counter);
+  add_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t plane_hash_peak(uint32_t iters, int blocks, int threads, uint64_t *out, cudaStream_t s) {
+  k_plane_hash_peak<<<blocks, threads, 0, s>>>(iters, out);
+  add_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t plane_update_peak(uint32_t iters, int blocks, uint32_t *out, cudaStream_t s) {
+  cudaError_t e = smem_optin(k_plane_update_peak);
+  if (e != cudaSuccess) return e;
+  k_plane_update_peak<<<blocks, 1024, 128 + kPlaneMaxTile * kVertBytes, s>>>(iters, out);
+  add_launches(1);
+  return cudaGetLastError();
+}
+
+}  // namespace gz

@@ -80,7 +80,8 @@ typedef struct gz_params {
   uint32_t cols_per_sample;     /* Sketch::cols_per_sample: 1 (CameoSketch) or 7 (CubeSketch) */
   uint32_t sketch_algorithm;    /* enum gz_sketch_algorithm */
   uint32_t in_place;            /* 1: sketches too large to stage in shared memory are updated in HBM */
-  uint32_t reserved;
+  uint32_t entry_form;          /* gutter entries of records: 1 = plain (hashed per endpoint where
+                                   applied), 2 = coded (each record hashed once, bucket planes) */
 } gz_params_t;
 
 /* One sampled component of one Boruvka round (parity tracing). key = smallest member id. */
@@ -251,10 +252,14 @@ GZ_API int gz_dump_sketches(gz_alg_t *alg, void *host_buf, size_t bytes);
  * file-scope device array of about 34 MiB that every GPU loading the library holds until the
  * process exits. Limits: at most 2,097,152 records per call and at most 4,194,304 vertices;
  * larger calls return GZ_ERR_INVALID without touching memory. The first call on each device looks
- * up the array's address (cudaGetSymbolAddress), so it should come before any stream capture.
- * Every call shares the array, which keeps the previous call's contents (each call clears what
- * must start at zero), so two calls whose GPU work overlapped would race on it: the entry point
- * therefore serializes its callers with a lock and returns only after its GPU work is done. */
+ * up the array's address (cudaGetSymbolAddress). Every call synchronizes `stream` before it
+ * returns (and reads a status word back from the GPU), so it must not be called while `stream` is
+ * being captured into a CUDA graph. Every call shares the array, which keeps the previous call's
+ * contents (each call clears what must start at zero), so two calls whose GPU work overlapped
+ * would race on it: the entry point therefore serializes its callers with a process-wide lock
+ * that it holds until its GPU work is done, on success and on failure alike. On a failure after
+ * the work was queued (a CUDA error, a timed-out device wait), the caller's sketches may be
+ * partly updated. */
 GZ_API int gz_ingest_records_noalloc(void *d_sketches, uint32_t num_vertices, uint64_t seed,
                                      double sketches_factor, const void *d_records,
                                      size_t n_records, void *stream);
@@ -272,21 +277,27 @@ GZ_API int gz_get_profile(gz_alg_t *alg, gz_profile_t *out);
 /* The cudaStream_t (as void*) every kernel of this handle is launched on. */
 GZ_API int gz_get_stream(gz_alg_t *alg, void **stream_out);
 
-/* Peak rate of this GPU at the ingest's hash arithmetic: a register-only kernel evaluating the
- * 8-byte XXH3 plus the bucket-depth count-trailing-zeros, timed with CUDA events on the current
- * device. *hashes_per_s gets the best of `repeats` launches. */
+/* Peak rate of this GPU at the ingest's per-column hash: a register-only kernel evaluating the
+ * 8-byte XXH3 of a column (the record's premixed input XOR the column's premixed seed constant,
+ * the two rrmxmx multiplies and shifts) and the bucket-depth count-trailing-zeros, eight
+ * independent chains per thread, each next input being the last one XOR its depth code. Timed
+ * with CUDA events on the current device; *hashes_per_s gets the best of `repeats` launches. */
 GZ_API int gz_measure_hash_rate(int repeats, double *hashes_per_s);
 
-/* Peak rate of this GPU at the sketch update's shared-memory operation: 96-bit XOR updates of
- * random 12-byte buckets in a 157 KB staged tile with three 32-bit atomicXor each (1024 threads
- * per SM, no hashing, no global traffic). *updates_per_s gets the best of `repeats` launches. */
+/* Peak rate of this GPU at the sketch update's shared-memory operation: bucket-slot updates of
+ * the bucket planes, each two conflict-free 32-bit red.shared.xor (one entry = 32 slot steps,
+ * 1024 threads per SM, no hashing, no global traffic). *updates_per_s gets the best of
+ * `repeats` launches, in slot updates per second. */
 GZ_API int gz_measure_update_rate(int repeats, double *updates_per_s);
 
-/* Tuning knobs of the ingest kernels (0 picks the default): vertices staged per shared-memory
- * tile (power of two in [4, 64]), threads per block of the sketch-update kernel, tiles per
- * gutter bin (power of two <= 64), and the gutter entry form for records: 1 = plain entries
- * (hashed per endpoint by the sketch-update kernel), 2 = hashed entries (each record hashed
- * once in the gutter; needs at most 32 columns). Buffered updates are applied first. */
+/* Tuning knobs of the ingest kernels (0 picks the default): vertices per shared-memory tile
+ * (power of two in [4, 64]; at most 32 with coded entries), threads per block of the
+ * sketch-update kernel, tiles per gutter bin (power of two <= 64; 1 with coded entries), and the
+ * gutter entry form for records: 1 = plain entries {vertex, neighbour} (hashed per endpoint by a
+ * staged-tile sketch-update kernel), 2 = coded entries (each record hashed once in the gutter into
+ * per-column depth codes, applied through bucket planes; CameoSketch with at most 31 columns and
+ * at most 8192 gutter bins). 0 picks coded entries where they apply. Buffered updates are applied
+ * first. */
 GZ_API int gz_set_tuning(gz_alg_t *alg, uint32_t vertices_per_tile, uint32_t threads_per_block,
                          uint32_t tiles_per_bin, uint32_t entry_form);
 /* Route of sparse tiles (one tile per gutter bin, plain CameoSketch entries): a tile holding
@@ -301,9 +312,10 @@ GZ_API int gz_set_direct_factor(gz_alg_t *alg, double factor);
 GZ_API int gz_set_query_graph(gz_alg_t *alg, int enable);
 /* Sketch-update kernel of a handle: mode 1 = the tile pipeline (a producer warp loads the next
  * tiles' sketches and writes finished ones back while the other warps hash; one tile per gutter
- * bin; CameoSketch with plain entries only, ignored otherwise), 2..4 = the pipeline with that
- * many tile buffers, 0 = one staged tile per CTA at a time, -1 = chosen by the handle (the
- * default). Re-picks the default tiling. */
+ * bin; CameoSketch only, ignored otherwise), 2..4 = the pipeline with that many tile buffers,
+ * 0 = one staged tile per CTA at a time, -1 = chosen by the handle (the default: coded entries
+ * and bucket planes where they apply). Modes 0..4 select plain entries. Re-picks the default
+ * tiling. */
 GZ_API int gz_set_pipeline(gz_alg_t *alg, int mode);
 
 /* ---- many graphs on one GPU ------------------------------------------------------------------

@@ -9,6 +9,7 @@
 
 #include <math.h>
 #include <stdlib.h>
+#include <omp.h>
 #include <string.h>
 
 /* ---- xxHash XXH3, 8-byte input path (published algorithm, xxHash 0.8.x) ---------------- */
@@ -295,6 +296,104 @@ uint32_t gzo_exact_cc(uint32_t V, const uint8_t *rec, size_t n, uint32_t *labels
     if (r == v) ++ncc;
   }
   free(e); free(parent);
+  return ncc;
+}
+
+/* The same answer for full-size streams, on `threads` host threads: the edge indices are
+ * bucketed by their smaller endpoint, each bucket sorted on its own, the indices of odd
+ * multiplicity (present after the stream's toggles) unioned; labels = smallest member id. */
+static void sort_u64(uint64_t *a, size_t n) {
+  /* LSD radix sort, 8 bits per pass through a scratch array; a byte that is the same in every
+   * key is skipped (inside a bucket of smaller endpoints the top bytes are) */
+  if (n < 2) return;
+  uint64_t *tmp = (uint64_t *)malloc(sizeof(uint64_t) * n);
+  uint64_t *src = a, *dst = tmp;
+  for (int pass = 0; pass < 8; ++pass) {
+    const int sh = 8 * pass;
+    size_t cnt[256] = {0};
+    uint64_t all_or = 0, all_and = ~(uint64_t)0;
+    for (size_t i = 0; i < n; ++i) { all_or |= src[i]; all_and &= src[i]; }
+    if ((((all_or ^ all_and) >> sh) & 0xff) == 0) continue; /* this byte is constant */
+    for (size_t i = 0; i < n; ++i) cnt[(src[i] >> sh) & 0xff]++;
+    size_t run = 0;
+    for (int b = 0; b < 256; ++b) { size_t c = cnt[b]; cnt[b] = run; run += c; }
+    for (size_t i = 0; i < n; ++i) dst[cnt[(src[i] >> sh) & 0xff]++] = src[i];
+    uint64_t *t = src; src = dst; dst = t;
+  }
+  if (src != a) memcpy(a, src, sizeof(uint64_t) * n);
+  free(tmp);
+}
+
+uint32_t gzo_exact_cc_mt(uint32_t V, const uint8_t *rec, size_t n, uint32_t *labels, int threads) {
+  if (threads < 1) threads = 1;
+  const uint32_t nb = 4096;
+  uint64_t *keys = (uint64_t *)malloc(sizeof(uint64_t) * (n ? n : 1));
+  uint64_t *out = (uint64_t *)malloc(sizeof(uint64_t) * (n ? n : 1));
+  size_t *cnt = (size_t *)calloc((size_t)threads * nb, sizeof(size_t));
+  size_t *bstart = (size_t *)calloc(nb + 1, sizeof(size_t));
+  size_t *bkeep = (size_t *)calloc(nb, sizeof(size_t));
+  uint32_t *parent = (uint32_t *)malloc(sizeof(uint32_t) * (V ? V : 1));
+  int bad = 0;
+#pragma omp parallel num_threads(threads)
+  {
+    const int t = omp_get_thread_num(), T = omp_get_num_threads();
+    const size_t i0 = n * (size_t)t / T, i1 = n * (size_t)(t + 1) / T;
+    size_t *c = cnt + (size_t)t * nb;
+    for (size_t i = i0; i < i1; ++i) {
+      uint32_t u = read_le32(rec + 9 * i + 1), v = read_le32(rec + 9 * i + 5);
+      if (u >= V || v >= V) { bad = 1; u = v = 0; }
+      keys[i] = gzo_concat_pairing(u, v);
+      c[(uint32_t)(((uint64_t)(u < v ? u : v) * nb) / V)]++;
+    }
+#pragma omp barrier
+#pragma omp single
+    {
+      size_t run = 0;
+      for (uint32_t b = 0; b < nb; ++b) {
+        bstart[b] = run;
+        for (int k = 0; k < T; ++k) {
+          const size_t x = cnt[(size_t)k * nb + b];
+          cnt[(size_t)k * nb + b] = run;
+          run += x;
+        }
+      }
+      bstart[nb] = run;
+    }
+    for (size_t i = i0; i < i1; ++i) {
+      const uint32_t lo = (uint32_t)(keys[i] >> 32);
+      out[c[(uint32_t)(((uint64_t)lo * nb) / V)]++] = keys[i];
+    }
+#pragma omp barrier
+#pragma omp for schedule(dynamic, 16)
+    for (uint32_t b = 0; b < nb; ++b) {
+      uint64_t *e = out + bstart[b];
+      const size_t m = bstart[b + 1] - bstart[b];
+      sort_u64(e, m);
+      size_t w = 0;
+      for (size_t i = 0; i < m;) {
+        size_t j = i;
+        while (j < m && e[j] == e[i]) ++j;
+        if ((j - i) & 1) e[w++] = e[i]; /* odd multiplicity => present */
+        i = j;
+      }
+      bkeep[b] = w;
+    }
+  }
+  uint32_t ncc = 0;
+  if (!bad) {
+    for (uint32_t v = 0; v < V; ++v) parent[v] = v;
+    for (uint32_t b = 0; b < nb; ++b)
+      for (size_t i = 0; i < bkeep[b]; ++i) {
+        const uint64_t k = out[bstart[b] + i];
+        uf_union(parent, (uint32_t)(k >> 32), (uint32_t)k);
+      }
+    for (uint32_t v = 0; v < V; ++v) {
+      const uint32_t r = uf_find(parent, v);
+      labels[v] = r;
+      if (r == v) ++ncc;
+    }
+  }
+  free(keys); free(out); free(cnt); free(bstart); free(bkeep); free(parent);
   return ncc;
 }
 

@@ -109,6 +109,9 @@ int gzo_boruvka_alg(const uint8_t *sketches, uint32_t V, uint32_t C, uint32_t B,
  * (test/util/graph_verifier.cpp). labels_out[v] = smallest vertex id of v's component.
  * Returns the number of components, or 0 on a bad vertex id. */
 uint32_t gzo_exact_cc(uint32_t V, const uint8_t *records, size_t n_records, uint32_t *labels_out);
+/* gzo_exact_cc on `threads` host threads (for full-size streams). */
+uint32_t gzo_exact_cc_mt(uint32_t V, const uint8_t *records, size_t n_records, uint32_t *labels_out,
+                         int threads);
 
 /* Eager DSU of the default build: CCSketchAlg::pre_insert (src/cc_sketch_alg.cpp:87-102) over
  * the records in stream order, from a valid DSU of singletons. An update joining two sets merges

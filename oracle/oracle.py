@@ -30,15 +30,16 @@ TRACE_DTYPE = np.dtype([("round", "<u4"), ("key", "<u4"), ("result", "<u4"), ("p
 _lib = None
 
 
-def build(force: bool = False) -> None:
-    """Compile liboracle.so (and oracle/_ref when the reference tree exists)."""
+def build(force: bool = False, reference: str | None = None) -> None:
+    """Compile liboracle.so, and oracle/_ref from the reference source tree at `reference`
+    (default: the GZ_REFERENCE environment variable) when that tree exists."""
     targets = ["oracle"]
-    if os.path.isdir(os.environ.get("GZ_REFERENCE", "/root/reference")):
-        targets.append("ref")
-    args = ["make", "-C", HERE] + (["-B"] if force else []) + targets
+    ref = reference or os.environ.get("GZ_REFERENCE", "")
     env = dict(os.environ)
-    if "GZ_REFERENCE" in os.environ:
-        env["REF"] = os.environ["GZ_REFERENCE"]
+    if ref and os.path.isdir(ref):
+        targets.append("ref")
+        env["REF"] = ref
+    args = ["make", "-C", HERE] + (["-B"] if force else []) + targets
     subprocess.run(args, check=True, env=env, stdout=subprocess.DEVNULL)
 
 
@@ -68,6 +69,8 @@ def lib():
                                   ctypes.POINTER(ctypes.c_size_t)]
         L.gzo_exact_cc.restype = ctypes.c_uint32
         L.gzo_exact_cc.argtypes = [ctypes.c_uint32, u8p, ctypes.c_size_t, u32p]
+        L.gzo_exact_cc_mt.restype = ctypes.c_uint32
+        L.gzo_exact_cc_mt.argtypes = [ctypes.c_uint32, u8p, ctypes.c_size_t, u32p, ctypes.c_int]
         L.gzo_params_alg.restype = ctypes.c_int
         L.gzo_params_alg.argtypes = [ctypes.c_uint32, ctypes.c_double, ctypes.c_int, u32p, u32p, u32p]
         L.gzo_apply_records_alg.restype = ctypes.c_int
@@ -164,6 +167,15 @@ def exact_cc(num_vertices: int, raw: np.ndarray):
     labels = np.zeros(num_vertices, np.uint32)
     n = lib().gzo_exact_cc(num_vertices, _p(raw, ctypes.c_uint8), raw.size // 9,
                            _p(labels, ctypes.c_uint32))
+    return int(n), labels
+
+
+def exact_cc_mt(num_vertices: int, raw: np.ndarray, threads: int | None = None):
+    """exact_cc on several host threads (full-size streams)."""
+    raw = np.ascontiguousarray(raw, np.uint8)
+    labels = np.zeros(num_vertices, np.uint32)
+    n = lib().gzo_exact_cc_mt(num_vertices, _p(raw, ctypes.c_uint8), raw.size // 9,
+                              _p(labels, ctypes.c_uint32), int(threads or os.cpu_count() or 1))
     return int(n), labels
 
 

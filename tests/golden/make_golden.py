@@ -1,12 +1,15 @@
 """Regenerate the golden fixtures in tests/golden/ from the compiled reference (oracle/_ref).
 
-    python tests/golden/make_golden.py
+    GZ_REFERENCE=<reference source tree> python tests/golden/make_golden.py
 
-Needs the reference tree (to build oracle/_ref with oracle/Makefile) and the `xxhash` Python
-package; the tests only read the files this writes. Outputs:
+Needs the reference tree (to build oracle/_ref with oracle/Makefile, and for the stream fixture
+the reference's own tests read) and the `xxhash` Python package; the tests only read the files
+this writes. Outputs:
   xxh3_vectors.json   XXH3_64bits_withSeed over 8-byte inputs, from libxxhash (python xxhash)
   params.json         sizing from the reference's own Sketch::calc_* functions
   <case>.gzs          seeded streams in the 9-byte binary format
+  ref_mult_v1024.data the reference's own test stream test/res/multiples_graph_1024_stream.data,
+                      copied byte for byte (read by test/cc_alg_test.cpp:300-350; 78 components)
   <case>.labels.npy   partition from CCSketchAlg::connected_components (smallest member id)
   <case>.trace.npy    every sampled component of every Boruvka round (reference Sketch code)
   manifest.json       per case: vertices, seeds, dump SHA-256, components, rounds
@@ -17,6 +20,7 @@ import hashlib
 import json
 import os
 import random
+import shutil
 import struct
 import subprocess
 import sys
@@ -45,6 +49,13 @@ CASES = [
 ]
 
 
+# Stream fixtures of the reference's own test suite, copied unchanged from its tree:
+# name, path inside the reference tree, sketch seed, sketches_factor, components its tests expect
+REF_FIXTURES = [
+    ("ref_mult_v1024", "test/res/multiples_graph_1024_stream.data", 4242, 1.0, 78),
+]
+
+
 def xxh3_vectors(n=256):
     import xxhash
     rng = random.Random(20261203)
@@ -61,7 +72,9 @@ def xxh3_vectors(n=256):
 
 
 def main():
-    O.build()
+    ref_tree = os.environ.get("GZ_REFERENCE", "")
+    assert ref_tree and os.path.isdir(ref_tree), "set GZ_REFERENCE to the reference source tree"
+    O.build(reference=ref_tree)
     assert O.have_reference(), "oracle/_ref was not built (reference tree missing?)"
     with open(os.path.join(HERE, "xxh3_vectors.json"), "w") as f:
         json.dump({"source": "python xxhash %s (libxxhash %s)" % (
@@ -81,11 +94,17 @@ def main():
         json.dump(params, f, indent=0)
 
     manifest = []
+    jobs = [(name, builder, seed, factor, name + ".gzs", None) for name, builder, seed, factor in CASES]
+    jobs += [(name, rel, seed, factor, name + ".data", want) for name, rel, seed, factor, want in REF_FIXTURES]
     with tempfile.TemporaryDirectory() as td:
-        for name, builder, seed, factor in CASES:
-            st = builder()
-            spath = os.path.join(HERE, name + ".gzs")
-            st.write(spath)
+        for name, builder, seed, factor, fname, want_cc in jobs:
+            spath = os.path.join(HERE, fname)
+            if want_cc is None:
+                st = builder()
+                st.write(spath)
+            else:
+                shutil.copyfile(os.path.join(ref_tree, builder), spath)
+                st = S.read_stream(spath)
             dump = os.path.join(td, name + ".dump")
             lab = os.path.join(td, name + ".labels")
             info = O.ref_ingest(spath, seed, factor, threads=2, dump_path=dump, labels_path=lab)
@@ -99,7 +118,9 @@ def main():
             np.save(os.path.join(HERE, name + ".trace.npy"), trace)
             sha = hashlib.sha256(open(dump, "rb").read()).hexdigest()
             ncc, _ = O.exact_cc(st.num_vertices, st.raw())
-            manifest.append({"name": name, "stream": name + ".gzs", "num_vertices": st.num_vertices,
+            if want_cc is not None:
+                assert info["num_cc"] == ncc == want_cc, (name, info["num_cc"], ncc)
+            manifest.append({"name": name, "stream": fname, "num_vertices": st.num_vertices,
                              "num_updates": st.num_updates, "seed": seed, "sketches_factor": factor,
                              "dump_sha256": sha, "dump_bytes": os.path.getsize(dump),
                              "num_cc": info["num_cc"], "exact_num_cc": ncc,

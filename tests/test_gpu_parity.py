@@ -119,29 +119,58 @@ def test_tile_that_does_not_fit_is_rejected(gz):
         alg.set_tuning(64, 1024)  # 64 * 4332 bytes > shared memory per block
 
 
-@pytest.mark.parametrize("form", [1, 2])
 @pytest.mark.parametrize("vpt,threads,tpb", [(4, 128, 1), (8, 256, 2), (16, 1024, 8), (32, 512, 4),
                                              (32, 1024, 1), (4, 1024, 64), (16, 640, 16)])
-def test_tile_shapes_bit_exact(gz, oracle_mod, vpt, threads, tpb, form):
+def test_tile_shapes_bit_exact(gz, oracle_mod, vpt, threads, tpb):
+    """Plain entries through the staged-tile kernel: tiles, bins and block sizes."""
     c, st, labels, _ = load_case("c0_v1024")
     alg = _alg(gz, 1024, c["seed"])
-    alg.set_tuning(vpt, threads, tpb, form)
+    alg.set_tuning(vpt, threads, tpb, 1)
     assert alg.params.vertices_per_tile == vpt
     assert alg.params.vertices_per_bin == vpt * tpb
+    assert alg.params.entry_form == 1
     alg.ingest_records(st)
     osk = oracle_mod.OracleSketches(1024, c["seed"])
     osk.apply_records(st.raw())
     assert (alg.dump_sketches() == osk.data).all()
 
 
-@pytest.mark.parametrize("factor", [0.0, 1.0, 1e9])
-@pytest.mark.parametrize("vpt", [4, 16])
-def test_direct_route_bit_exact(gz, oracle_mod, vpt, factor):
-    """Sparse tiles updated in place in HBM (global atomics) instead of staged: 0 stages every
-    tile, 1e9 sends every tile in place, 1 mixes the two by entry count. Bytes must not move."""
+@pytest.mark.parametrize("vpt,threads", [(4, 64), (8, 256), (16, 640), (32, 1024), (32, 96),
+                                         (16, 1024)])
+def test_plane_tile_shapes_bit_exact(gz, oracle_mod, vpt, threads):
+    """Coded entries through the bucket planes: every tile size and block size (several warps per
+    vertex, or several vertices per warp in the write-back)."""
     c, st, labels, _ = load_case("c0_v1024")
     alg = _alg(gz, 1024, c["seed"])
-    alg.set_tuning(vpt, 1024, 1)
+    alg.set_tuning(vpt, threads, 1, 2)
+    assert alg.params.vertices_per_tile == alg.params.vertices_per_bin == vpt
+    assert alg.params.entry_form == 2
+    alg.ingest_records(st)
+    osk = oracle_mod.OracleSketches(1024, c["seed"])
+    osk.apply_records(st.raw())
+    assert (alg.dump_sketches() == osk.data).all()
+    assert (canonical(alg.connected_components().parent_arr) == labels).all()
+
+
+def test_coded_entries_need_one_tile_per_bin(gz):
+    alg = _alg(gz, 1024, 5)
+    with pytest.raises(gz.GZError):
+        alg.set_tuning(8, 1024, 2, 2)
+    with pytest.raises(gz.GZError):
+        alg.set_tuning(64, 1024, 1, 2)
+    assert alg.params.entry_form == 2  # the handle keeps its tiling after a rejected request
+
+
+@pytest.mark.parametrize("form", [1, 2])
+@pytest.mark.parametrize("factor", [0.0, 1.0, 1e9])
+@pytest.mark.parametrize("vpt", [4, 16])
+def test_direct_route_bit_exact(gz, oracle_mod, vpt, factor, form):
+    """Sparse tiles updated in place in HBM (global atomics) instead of staged (plain entries) or
+    run through the bucket planes (coded entries): 0 never goes in place, 1e9 sends every tile in
+    place, 1 mixes the two by entry count. Bytes must not move."""
+    c, st, labels, _ = load_case("c0_v1024")
+    alg = _alg(gz, 1024, c["seed"])
+    alg.set_tuning(vpt, 1024, 1, form)
     alg.set_direct_factor(factor)
     half = st.num_updates // 2
     rec = st.records
@@ -323,7 +352,7 @@ def test_many_bins_gutter_paths(gz, oracle_mod, vpt, tpb):
     V = 20000
     st = S.erdos_renyi_stream(V, 0.0004, seed=21, churn_fraction=0.2)
     alg = _alg(gz, V, 77)
-    alg.set_tuning(vpt, 1024, tpb)
+    alg.set_tuning(vpt, 1024, tpb, 1)
     alg.ingest_records(st)
     rng = np.random.default_rng(5)
     pick = rng.choice(V, 64, replace=False)
@@ -341,11 +370,12 @@ def test_many_bins_gutter_paths(gz, oracle_mod, vpt, tpb):
     assert (canonical(cc.parent_arr) == exact).all()
 
 
-def test_records_with_more_than_32_columns_use_plain_entries(gz, oracle_mod):
+def test_records_with_more_than_31_columns_use_plain_entries(gz, oracle_mod):
     """sketches_factor 3 gives 41 columns: records are hashed per endpoint (plain entries)."""
     c, st, _, _ = load_case("c0_v1024")
     alg = _alg(gz, 1024, 99, 3.0)
     assert alg.params.num_columns == 41
+    assert alg.params.entry_form == 1
     alg.ingest_records(st)
     osk = oracle_mod.OracleSketches(1024, 99, 3.0)
     osk.apply_records(st.raw())
@@ -355,14 +385,17 @@ def test_records_with_more_than_32_columns_use_plain_entries(gz, oracle_mod):
     assert alg.last_query_rounds == rounds
 
 
-def test_hashed_entries_with_global_cursors(gz, oracle_mod):
-    """65536 vertices at 4 per tile: 16384 bins, above the shared-memory cursor limit."""
+def test_coded_entries_at_the_bin_limit(gz, oracle_mod):
+    """65536 vertices at 8 per tile: 8192 bins, the most the hash sort-scatter takes (8 bins per
+    thread in its scan); 4 per tile (16384 bins) is refused for coded entries."""
     from graphzeppelin_b200 import streams as S
     V = 1 << 16
     st = S.erdos_renyi_stream(V, 0.0002, seed=23, churn_fraction=0.1)
     alg = _alg(gz, V, 31)
-    alg.set_tuning(4, 1024, 1, 2)
-    assert alg.params.num_bins == 16384
+    with pytest.raises(gz.GZError):
+        alg.set_tuning(4, 1024, 1, 2)
+    alg.set_tuning(8, 1024, 1, 2)
+    assert alg.params.num_bins == 8192
     alg.ingest_records(st)
     rng = np.random.default_rng(8)
     pick = rng.choice(V, 64, replace=False)
@@ -378,8 +411,9 @@ def test_hashed_entries_with_global_cursors(gz, oracle_mod):
     assert (canonical(alg.connected_components().parent_arr) == exact).all()
 
 
-def test_mixed_hashed_and_plain_chunks(gz, oracle_mod):
-    """Records (hashed entries) and apply_update_batch (plain entries) buffered together."""
+def test_mixed_coded_and_plain_chunks(gz, oracle_mod):
+    """Records (coded entries) and apply_update_batch (plain entries, hashed where the planes
+    apply them) buffered together."""
     c, st, labels, _ = load_case("cl_v2048")
     alg = _alg(gz, 2048, c["seed"])
     alg.set_tuning(0, 0, 1, 2)

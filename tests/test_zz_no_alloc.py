@@ -3,7 +3,8 @@ inside a framework that owns every device byte through its own pool, or a latenc
 where cudaMalloc / cudaFree would synchronize the device). Its scratch is a fixed device array
 inside the library, so the test checks that two calls in a row leave the caller's sketches
 byte-identical (the tolerance of every parity test here) to what a handle produces with
-gz_ingest_records_device + gz_flush, and that oversize calls are refused.
+gz_ingest_records_device + gz_flush and to the oracle, that a call at the record limit is
+exact, and that oversize calls are refused.
 
 This file is collected last on purpose, and passes alone in a fresh process as well as after the
 other tests."""
@@ -21,7 +22,7 @@ def _noalloc(lib, d_sk, V, seed, factor, d_rec, n):
 
 
 @pytest.mark.parametrize("name,V", [("cl_v2048", 2048), ("sparse_v300", 300), ("er_v64", 64)])
-def test_noalloc_matches_handle_on_two_calls(name, V):
+def test_noalloc_matches_handle_on_two_calls(name, V, oracle_mod):
     torch = pytest.importorskip("torch")
     import graphzeppelin_b200 as gz
     from graphzeppelin_b200 import _lib
@@ -44,6 +45,41 @@ def test_noalloc_matches_handle_on_two_calls(name, V):
         ref.flush()
         assert (d_sk.cpu().numpy() == ref.dump_sketches()).all()
     ref.close()
+    # and directly against the oracle (the CPU restatement of Sketch::update)
+    osk = oracle_mod.OracleSketches(V, seed)
+    osk.apply_records(st.raw())
+    assert (d_sk.cpu().numpy() == osk.data).all()
+
+
+def test_noalloc_call_at_the_record_limit(oracle_mod):
+    """One call of exactly 2,097,152 records (the entries region of the scratch array filled to
+    the last byte), after a small call that left other contents in the array."""
+    torch = pytest.importorskip("torch")
+    from graphzeppelin_b200 import _lib
+    from graphzeppelin_b200 import streams as S
+    V, seed = 1 << 15, 777
+    st, _ = S.planted_partition_stream_fast(V, 8, seed=4, mean_degree=160, min_size=256,
+                                            churn_fraction=0.1)
+    assert st.num_updates >= 1 << 21
+    recs = st.records[:1 << 21]
+    lib = _lib.load()
+    _, _, _, sb = oracle_mod.params(V, 1.0)
+    d_sk = torch.zeros(V * sb, dtype=torch.uint8, device="cuda")
+    small = np.ascontiguousarray(st.records[-1000:]).view(np.uint8).reshape(-1)
+    d_small = torch.from_numpy(small.copy()).cuda()
+    d_rec = torch.from_numpy(np.ascontiguousarray(recs).view(np.uint8).reshape(-1).copy()).cuda()
+    torch.cuda.synchronize()
+    assert _noalloc(lib, d_sk.data_ptr(), V, seed, 1.0, d_small.data_ptr(), 1000) == 0, _lib.last_error()
+    assert _noalloc(lib, d_sk.data_ptr(), V, seed, 1.0, d_rec.data_ptr(), 1 << 21) == 0, _lib.last_error()
+    pick = np.random.default_rng(6).choice(V, 48, replace=False)
+    filt = np.zeros(V, np.uint8)
+    filt[pick] = 1
+    osk = oracle_mod.OracleSketches(V, seed)
+    osk.apply_records(small, vertex_filter=filt)
+    osk.apply_records(np.ascontiguousarray(recs).view(np.uint8).reshape(-1), vertex_filter=filt)
+    got = d_sk.cpu().numpy()
+    for v in pick:
+        assert (got[v * sb:(v + 1) * sb] == osk.sketch(v)).all(), v
 
 
 @pytest.mark.parametrize("V", [1001, 3])
