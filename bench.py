@@ -205,9 +205,10 @@ def roofline(alg, n, prof, steps, ingest_ms, hash_peak, hbm_peak_gbs, update_pea
     algorithmic work of one record: 1 + C XXH3 hashes (one per column and the checksum, hashed
     once per edge), 9 B of stream read, and the touched sketches read and written once. The path
     is bound by the slower of the hash term (over the measured hash rate) and the HBM term.
-    Per kernel: the gutter phase (count + hash sort-scatter) against its own hashes (C per
-    record) and bytes, the sketch update against the shared-memory slot rate (2 (C + 1) bucket
-    updates per record, made as 2 x 32 slot steps) and its bytes."""
+    Per kernel: the gutter phase (count + hash sort-scatter) against its own hashes (the first 16
+    columns per record) and bytes, the sketch update against the shared-memory slot rate
+    (2 (C + 1) bucket updates per record, made as 2 x 32 slot steps), its hashes (the other
+    C - 16 columns and the checksum, per endpoint) and its bytes."""
     p = alg.params
     V, C, B, sb = p.num_vertices, p.num_columns, p.bkt_per_col, p.sketch_bytes
     t_ing = statistics.mean(ingest_ms) / 1e3
@@ -219,23 +220,28 @@ def roofline(alg, n, prof, steps, ingest_ms, hash_peak, hbm_peak_gbs, update_pea
     t_g = prof["gutter_ms"] / max(1, prof["gutter_launches"]) / 1e3
     t_u = prof["sketch_update_ms"] / max(1, prof["sketch_update_launches"]) / 1e3
     if p.entry_form == 2:
-        g_bytes = 9 * n + 9 * n + 2 * n * 24
+        coded = min(C, 16)  # columns hashed once per record in the gutter pass (kCodedColumns)
+        g_bytes = 9 * n + 9 * n + 2 * n * 16
         kernels["gutter"] = {
             "kernels": "k_gutter (count) + k_hash_sort_scatter", "launch_ms": t_g * 1e3,
-            "bound": "int", "hashes_per_launch": n * C,
-            "int": {"achieved": n * C / t_g / 1e9, "peak": hash_peak / 1e9, "unit": "Ghash/s",
-                    "frac": n * C / t_g / hash_peak},
+            "bound": "int", "hashes_per_launch": n * coded,
+            "int": {"achieved": n * coded / t_g / 1e9, "peak": hash_peak / 1e9, "unit": "Ghash/s",
+                    "frac": n * coded / t_g / hash_peak},
             "hbm": {"achieved": g_bytes / t_g / 1e9, "peak": hbm_peak_gbs, "unit": "GB/s",
                     "frac": g_bytes / t_g / 1e9 / hbm_peak_gbs, "bytes_per_launch": g_bytes}}
         rows = min(B, 11)
-        u_bytes = 2 * n * 24 + 2 * V * 12 * (C * rows + 1)
+        u_bytes = 2 * n * 16 + 2 * V * 12 * (C * rows + 1)
         slots = 2 * n * 32
+        u_hashes = 2 * n * (C - coded + 1)
         kernels["sketch_update"] = {
             "kernels": "k_plane_update", "launch_ms": t_u * 1e3, "bound": "smem",
             "bucket_updates_per_launch": 2 * n * (C + 1), "slot_steps_per_launch": slots,
+            "hashes_per_launch": u_hashes,
             "smem": {"achieved": slots / t_u / 1e9, "peak": update_peak / 1e9,
                      "unit": "Gslot/s", "frac": slots / t_u / update_peak,
                      "useful_frac": 2 * n * (C + 1) / t_u / update_peak},
+            "int": {"achieved": u_hashes / t_u / 1e9, "peak": hash_peak / 1e9, "unit": "Ghash/s",
+                    "frac": u_hashes / t_u / hash_peak},
             "hbm": {"achieved": u_bytes / t_u / 1e9, "peak": hbm_peak_gbs, "unit": "GB/s",
                     "frac": u_bytes / t_u / 1e9 / hbm_peak_gbs, "bytes_per_launch": u_bytes}}
     else:
@@ -413,6 +419,15 @@ def run_b200(args, cfg):
         if world == 1 and not args.no_cpu_baseline:
             log("[rank 0] timing the CPU reference baseline and checking full-size parity ...")
             cpu, parity = cpu_baseline_and_parity(alg, stream, cfg, cc)
+        serving = None
+        if world == 1 and not args.no_serving:
+            log("[rank 0] short serving replay with the admission queue in use ...")
+            try:
+                serving = serving_short()
+            except SystemExit:
+                raise
+            except Exception as e:  # reported in the line, the headline stands
+                serving = {"error": repr(e)}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
@@ -430,6 +445,7 @@ def run_b200(args, cfg):
             "ingest_ms": statistics.mean(ingest_ms),
             "ingest_updates_per_s": n / (statistics.mean(ingest_ms) / 1e3),
             "parity": parity,
+            "serving": serving,
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": e2e,
@@ -630,6 +646,47 @@ def run_many_graphs(args):
 
 SERVING = dict(workload="serving_t2000_v2e10-2e18_chunglu2.3_budget120GB", num_tenants=2000,
                trace_seed=7, budget_bytes=120 * 10**9, snapshot_bytes=40 * 10**9)
+
+
+# The serving check of the default run: a short trace whose sketch demand exceeds the budget, so
+# that tenants queue for admission while query latency is measured.
+SERVING_SHORT = dict(num_tenants=400, trace_seed=11, budget_bytes=16 * 10**9,
+                     snapshot_bytes=8 * 10**9, time_scale=4.0)
+
+
+def serving_short():
+    """Paced replay of a 400-tenant serving trace through the batched server (continuous
+    batching, snapshot queries) under a 16 GB sketch budget, and the same trace saturated through
+    the batched server and through the plain per-tenant path; answers must agree."""
+    from graphzeppelin_b200 import serve as SV
+    cfg = SERVING_SHORT
+    tr = SV.serving_trace(cfg["num_tenants"], cfg["trace_seed"])
+    demand = sum(SV.tenant_bytes(int(v)) for v in tr.num_vertices)
+    kw = dict(snapshot_bytes=cfg["snapshot_bytes"])
+    warm = SV.serving_trace(60, cfg["trace_seed"] + 1000)
+    SV.replay(warm, "batched", cfg["budget_bytes"], time_scale=1e12, **kw)
+    SV.replay(warm, "plain", cfg["budget_bytes"], time_scale=1e12, **kw)
+    paced = SV.replay(tr, "batched", cfg["budget_bytes"], time_scale=cfg["time_scale"], **kw)
+    sat = SV.replay(tr, "batched", cfg["budget_bytes"], time_scale=1e12, **kw)
+    plain = SV.replay(tr, "plain", cfg["budget_bytes"], time_scale=1e12, **kw)
+    if not (paced.answers == sat.answers == plain.answers):
+        raise SystemExit("serving answers differ between the batched server and the plain path")
+    p, s_, pl = paced.summary(), sat.summary(), plain.summary()
+    return {"workload": f"serving_t{cfg['num_tenants']}_v2e10-2e18_chunglu2.3_budget16GB",
+            "tenants": cfg["num_tenants"], "requests": int(tr.time.size), "updates": tr.num_updates,
+            "budget_bytes": cfg["budget_bytes"], "sketch_demand_bytes": int(demand),
+            "time_scale": cfg["time_scale"],
+            "query_p50_ms": p["query_p50_ms"], "query_p99_ms": p["query_p99_ms"],
+            "service_p50_ms": p["service_p50_ms"], "service_p99_ms": p["service_p99_ms"],
+            "tenants_waited_for_budget": p["tenants_waited_for_budget"],
+            "max_waiting_tenants": p["max_waiting_tenants"],
+            "paced_updates_per_s": p["updates_per_s"],
+            "saturated_updates_per_s": s_["updates_per_s"],
+            "plain_path_updates_per_s": pl["updates_per_s"],
+            "saturated_over_plain": s_["updates_per_s"] / max(pl["updates_per_s"], 1e-9),
+            "answers_equal": True,
+            "note": "query_* from release, service_* from release or admission; wall clock; "
+                    "plain path = one CCSketchAlg per tenant, requests one at a time"}
 
 
 def run_serving(args):
@@ -855,6 +912,8 @@ def main():
                     help="queries with the Boruvka round loop on the host (profilers cannot see "
                          "kernels inside the conditional query graph)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-serving", action="store_true",
+                    help="skip the short serving replay of the default run")
     ap.add_argument("--workload", default="dense",
                     choices=["dense", "many_graphs", "serving", "powerlaw"],
                     help="dense: one V=2^17 graph (the headline); many_graphs: 512 uneven graphs; "

@@ -137,7 +137,7 @@ struct gz_alg {
   uint32_t *d_status = nullptr;  // [0] status bits, [1] work counter
   uint32_t *h_status = nullptr;  // pinned mirror
   // device gutter
-  uint8_t *d_gutter = nullptr;  // chunks of plain (8 B) or coded (8 B key + 16 B codes) entries
+  uint8_t *d_gutter = nullptr;  // chunks of plain (8 B) or coded (16 B) endpoint entries
   uint64_t entry_cap = 0;       // capacity in endpoint updates
   uint64_t gutter_bytes = 0, gutter_used = 0, entries_pending = 0;
   double direct_factor = 1.0;   // scales the in-place threshold of sparse tiles (0 = never)
@@ -251,6 +251,8 @@ struct gz_alg {
     g.sketch_words = nb * 3;
     g.tile_shift = tile_shift;
     g.ntiles = ntiles;
+    g.bin_shift = bin_shift;
+    g.nbins = nbins;
     // A tile through the planes costs its write-back, about 2 x 12 x (C min(B, rows) + 1) bytes
     // per vertex read and written; in place an entry costs its C + 1 buckets' sectors, each read
     // and written by an L2 atomic. Below the break-even entry count a tile goes in place.
@@ -337,13 +339,15 @@ bool want_pipe(const gz_alg *h) {
   return h->V > (1u << 18);
 }
 
-// Coded entries and bucket planes by default: CameoSketch of at most 31 columns whose gutter bins
-// of 32 vertices fit the shared-memory sort (up to 2^18 vertices). Larger graphs keep the
-// pipelined staged update.
-bool planes_possible(const gz_alg *h, uint32_t shift) {
-  return !h->cube && h->C <= gz::kPlaneMaxColumns &&
-         ((h->V + (1u << shift) - 1) >> shift) <= gz::kSortBinsMax;
-}
+// Coded entries and bucket planes by default: CameoSketch of at most 31 columns up to 2^18
+// vertices (asked for explicitly: while the gutter bins fit the shared-memory hash sort). By
+// default a gutter bin is one tile of 32 vertices. Coarser bins (set_tuning tiles_per_bin 2..8)
+// lengthen the sort's runs but make every tile filter its bin's entries; measured on B200 over
+// 1.4e8 records at 2^17 vertices, gutter + sketch update took 5.2 + 6.4 ms at 1 tile per bin,
+// 5.0 + 7.1 ms at 2 and 4.8 + 8.0 ms at 4.
+constexpr uint32_t kPlaneBinTarget = 1024;
+constexpr uint32_t kPlaneTilesPerBin = 1;
+constexpr uint32_t kPlaneDefaultMaxV = 1u << 18;
 
 int choose_planes(gz_alg *h, uint32_t vpt_req, uint32_t threads_req, uint32_t tpb_req, bool &done) {
   done = false;
@@ -353,13 +357,30 @@ int choose_planes(gz_alg *h, uint32_t vpt_req, uint32_t threads_req, uint32_t tp
     if (asked) return fail(GZ_ERR_INVALID, "coded entries need CameoSketch with at most 31 columns");
     return GZ_OK;
   }
-  if (tpb_req > 1 || (vpt_req && (vpt_req < 4 || (vpt_req & (vpt_req - 1)) || vpt_req > gz::kPlaneMaxTile))) {
-    if (asked) return fail(GZ_ERR_INVALID, "coded entries take one tile per bin of 4 to 32 vertices");
+  if ((tpb_req && ((tpb_req & (tpb_req - 1)) || tpb_req > 8)) ||
+      (vpt_req && (vpt_req < 4 || (vpt_req & (vpt_req - 1)) || vpt_req > gz::kPlaneMaxTile))) {
+    if (asked) return fail(GZ_ERR_INVALID, "coded entries take tiles of 4 to 32 vertices, 1 to 8 per bin");
     return GZ_OK;
   }
+  // By default past 2^18 vertices the pipelined staged kernel stays in use (large sparse graphs,
+  // where a wave brings few entries per tile)
+  if (!asked && h->V > kPlaneDefaultMaxV) return GZ_OK;
   const uint32_t shift = vpt_req ? (uint32_t)__builtin_ctz(vpt_req) : 5;
-  if (!planes_possible(h, shift)) {
+  uint32_t bshift = shift;
+  if (tpb_req) {
+    bshift = shift + (uint32_t)__builtin_ctz(tpb_req);
+  } else {
+    while (((h->V + (1u << bshift) - 1) >> bshift) > kPlaneBinTarget &&
+           (1u << (bshift - shift)) < kPlaneTilesPerBin)
+      ++bshift;
+  }
+  const uint32_t nbins = (uint32_t)((h->V + (1u << bshift) - 1) >> bshift);
+  if (nbins > gz::kSortBinsMax) {
     if (asked) return fail(GZ_ERR_INVALID, "too many gutter bins for coded entries at this tile size");
+    return GZ_OK;
+  }
+  if (!gz::coded_entry_fits(h->V, h->C, bshift)) {
+    if (asked) return fail(GZ_ERR_INVALID, "the codes of this sketch do not fit a 16-byte coded entry");
     return GZ_OK;
   }
   uint32_t threads = threads_req ? threads_req : 1024;
@@ -371,8 +392,10 @@ int choose_planes(gz_alg *h, uint32_t vpt_req, uint32_t threads_req, uint32_t tp
   h->in_place = false;
   h->pipe = false;
   h->threads = threads;
-  h->tile_shift = h->bin_shift = shift;
-  h->ntiles = h->nbins = (uint32_t)((h->V + (1u << shift) - 1) >> shift);
+  h->tile_shift = shift;
+  h->ntiles = (uint32_t)((h->V + (1u << shift) - 1) >> shift);
+  h->bin_shift = bshift;
+  h->nbins = nbins;
   done = true;
   return GZ_OK;
 }
@@ -568,16 +591,16 @@ void destroy_alg(gz_alg *h) {
 
 // ---- device gutter -------------------------------------------------------------------------------
 
-// Gutter bytes per endpoint entry: 8 B keys, plus 16 B of depth codes for records on the
-// bucket-plane path.
+// Gutter bytes per endpoint entry: 8 B {vertex, neighbour}, or 16 B with the depth codes of the
+// first columns (records on the bucket-plane path).
 uint64_t entry_bytes(const gz_alg *h, int input) {
-  return input == gz::kInputRecords && h->planes ? 24 : 8;
+  return input == gz::kInputRecords && h->planes ? 16 : 8;
 }
-constexpr uint64_t kGutterSlack = 64;  // alignment of a chunk's code array
+constexpr uint64_t kGutterSlack = 64;  // 16-byte alignment of each chunk
 
 int ensure_gutter(gz_alg *h) {
   if (!h->d_gutter) {
-    h->gutter_bytes = h->entry_cap * (h->planes ? 24 : 8) + kGutterSlack;
+    h->gutter_bytes = h->entry_cap * (h->planes ? 16 : 8) + kGutterSlack;
     GZ_TRY(dev_alloc(&h->d_gutter, h->gutter_bytes));
   }
   GZ_TRY(dev_alloc(&h->d_bin_off, (size_t)gz::kMaxChunks * (h->nbins + 1)));
@@ -637,7 +660,7 @@ int gutter_chunk(gz_alg *h, int input, const void *d_in, uint64_t n) {
   }
   const uint64_t per = input == gz::kInputRecords ? 2 : 1;
   const uint64_t esz = entry_bytes(h, input);
-  const bool coded = esz == 24;
+  const bool coded = esz == 16;
   GZ_TRY(ensure_gutter(h));
   const uint64_t max_n = std::min((h->gutter_bytes - kGutterSlack) / esz, kMaxChunkEntries) / per;
   if (max_n == 0) return fail(GZ_ERR_INVALID, "gutter capacity is below one update");
@@ -647,10 +670,9 @@ int gutter_chunk(gz_alg *h, int input, const void *d_in, uint64_t n) {
       GZ_TRY(gutter_chunk(h, input, (const uint8_t *)d_in + off * isz, std::min(max_n, n - off)));
     return GZ_OK;
   }
-  // a chunk: its keys (8 B per entry), then for coded entries their codes, 16-byte aligned
+  // a chunk's entries, 16-byte aligned
   const uint64_t n_ent = n * per;
-  const uint64_t key_bytes = (n_ent * 8 + 15) & ~15ull;
-  const uint64_t need = coded ? key_bytes + n_ent * 16 : key_bytes;
+  const uint64_t need = (n_ent * esz + 15) & ~15ull;
   if (h->gutter_used + need > h->gutter_bytes || h->nchunks == gz::kMaxChunks)
     GZ_TRY(apply_pending(h));
   const gz::GutterGeom gg = h->ggeom();
@@ -669,8 +691,8 @@ int gutter_chunk(gz_alg *h, int input, const void *d_in, uint64_t n) {
     const uint32_t tile = gz::hash_sort_tile(h->nbins, h->smem_optin - 1024);
     if (tile == 0) return fail(GZ_ERR_INVALID, "gutter bins do not fit the hash sort");
     GZ_CUDA(cudaMemsetAsync(h->d_fill, 0, sizeof(uint32_t) * h->nbins, h->stream));
-    GZ_CUDA(gz::gutter_hash_sort(d_in, n, gg, h->ph, tile, h->d_hist, h->d_fill, out2,
-                                 reinterpret_cast<uint4 *>(out + key_bytes), h->stream));
+    GZ_CUDA(gz::gutter_hash_sort(d_in, n, gg, h->ph, tile, h->d_hist, h->d_fill,
+                                 reinterpret_cast<uint4 *>(out), h->stream));
   } else {
     const uint32_t tile = gz::sort_scatter_tile(input, gg, h->smem_optin - 1024);
     if (tile >= 1024) {
@@ -683,7 +705,6 @@ int gutter_chunk(gz_alg *h, int input, const void *d_in, uint64_t n) {
   }
   h->prof_end(pi, 0);
   h->chunks.base[h->nchunks] = h->gutter_used;
-  h->chunks.aux[h->nchunks] = coded ? h->gutter_used + key_bytes : 0;
   h->chunks.kind[h->nchunks] = coded ? gz::kEntryCoded : gz::kEntryPlain;
   h->nchunks++;
   h->gutter_used += need;

@@ -32,13 +32,19 @@ constexpr int kMaxChunks = 128;
 // Entry kinds of a gutter chunk.
 enum EntryKind : uint8_t {
   kEntryPlain = 0,   // uint2 {vertex, neighbour}: hashed where it is applied
-  kEntryCoded = 1,   // uint2 {vertex, neighbour} at base, and at aux a parallel uint4 of 4-bit
-                     // depth codes (column c in bits 4c..4c+3): every record hashed once
+  kEntryCoded = 1,   // 128 bits: the 4-bit depth codes of all C columns, computed once per
+                     // record (column c in bits 4c .. 4c + 3), then from bit 4C the neighbour
+                     // shifted left by bin_shift OR the vertex's offset inside its gutter bin
 };
 constexpr uint32_t kDepthEscape = 15;  // depth code for "15 or more"
+// Whether coded entries hold the codes of C columns for V vertices in bins of 2^bin_shift.
+inline bool coded_entry_fits(uint32_t V, uint32_t C, uint32_t bin_shift) {
+  uint32_t ubits = 1;
+  while (ubits < 32 && (1ull << ubits) < V) ++ubits;  // bits of a neighbour id (< V)
+  return C >= 18 && 4 * C + bin_shift + ubits <= 128;
+}
 struct ChunkTable {
-  uint64_t base[kMaxChunks];  // byte offset of the chunk's keys in the gutter buffer
-  uint64_t aux[kMaxChunks];   // kEntryCoded: byte offset of its depth codes
+  uint64_t base[kMaxChunks];  // byte offset of the chunk's entries in the gutter buffer
   uint8_t kind[kMaxChunks];
 };
 
@@ -94,7 +100,7 @@ cudaError_t gutter_sort_scatter(int input, const void *d_in, uint64_t n, GutterG
 cudaError_t gutter_scatter_global(int input, const void *d_in, uint64_t n, GutterGeom g, int G,
                                   uint64_t *cursor, uint2 *entries, cudaStream_t s);
 
-// ---- hash-once ingest into bucket planes (gz_planes.cu) ------------------------------------
+// ---- coded entries and bucket planes (gz_planes.cu) ---------------------------------------
 // A vertex sketch is accumulated in shared memory as three planes of kPlaneRows rows x
 // kPlaneSlots 32-bit slots: slot c < C is column c, slot C the deterministic bucket (row 0).
 // Row d of a column holds depth d; the last row is scratch (depth codes at or above it are
@@ -103,7 +109,7 @@ cudaError_t gutter_scatter_global(int input, const void *d_in, uint64_t n, Gutte
 constexpr uint32_t kPlaneSlots = 32;
 constexpr uint32_t kPlaneRows = 12;
 constexpr uint32_t kPlaneMaxColumns = kPlaneSlots - 1;
-constexpr uint32_t kPlaneMaxTile = 32;     // vertices per tile (one tile per gutter bin)
+constexpr uint32_t kPlaneMaxTile = 32;     // vertices per shared-memory tile
 struct PlaneHash {
   uint32_t C, B;
   uint64_t kcol[kPlaneMaxColumns];  // xxh3_premix(flip of column seed c)
@@ -111,18 +117,20 @@ struct PlaneHash {
 };
 struct PlaneGeom {
   uint32_t V, C, B, sketch_words;
-  uint32_t tile_shift;  // W = 1 << tile_shift vertices per tile = per gutter bin
+  uint32_t tile_shift;  // W = 1 << tile_shift vertices per tile
   uint32_t ntiles;
+  uint32_t bin_shift;   // gutter bin (>= tile_shift): a bin holds 1 << (bin - tile) tiles
+  uint32_t nbins;
   uint32_t direct_max;  // a tile with fewer entries is updated in place in HBM
 };
 PlaneHash plane_hash(uint64_t seed, uint32_t C, uint32_t B);
 // Records per tile of the hash sort-scatter for this bin count (0: the bins do not fit).
 uint32_t hash_sort_tile(uint32_t nbins, size_t smem_budget);
-// Hash every record once and write its two endpoint entries, counting-sorted by bin: keys to
-// keys[base[b] + ...], depth codes to codes[base[b] + ...]; fill (nbins u32) starts at zero.
+// Hash every record once (all C columns) and write its two coded endpoint entries,
+// counting-sorted by bin, to entries[base[b] + ...]; fill (nbins u32) starts at zero.
 cudaError_t gutter_hash_sort(const void *d_rec, uint64_t n, GutterGeom g, const PlaneHash &ph,
-                             uint32_t rec_tile, const uint64_t *base, uint32_t *fill, uint2 *keys,
-                             uint4 *codes, cudaStream_t s);
+                             uint32_t rec_tile, const uint64_t *base, uint32_t *fill,
+                             uint4 *entries, cudaStream_t s);
 // Applies every buffered chunk (coded or plain entries) tile by tile through bucket planes.
 size_t plane_update_smem(uint32_t tile_shift, int threads);
 int plane_update_ctas_per_sm(uint32_t tile_shift, int threads);

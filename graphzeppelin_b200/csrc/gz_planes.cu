@@ -1,19 +1,22 @@
-// gz_planes.cu -- hash-once record ingest for CameoSketch sketches of at most 31 columns.
+// gz_planes.cu -- coded-entry record ingest for CameoSketch sketches of at most 31 columns.
 //
 // Sketch::update (src/sketch.cpp:69-83) XORs an edge index and its checksum into the
 // deterministic bucket and into bucket (c, depth_c(idx)) of every column c, and
 // CCSketchAlg::update / apply_update_batch (src/cc_sketch_alg.cpp:106-133) apply it to both
 // endpoint sketches. Every vertex sketch uses the same seed (src/cc_sketch_alg.cpp:21), so the two
-// endpoints get the same depths and the same checksum: here the C depth hashes of a record are
-// computed once, where the reference computes them per endpoint.
+// endpoints get the same depths and the same checksum.
 //
 //   k_hash_sort_scatter  per tile of records: the two endpoint entries counting-sorted by gutter
-//                        bin in shared memory, each record hashed once into C 4-bit depth codes,
-//                        the runs written out coalesced as keys {vertex, neighbour} plus a
-//                        parallel array of codes (one uint4 per entry).
-//   k_plane_update       per tile of W vertices (one gutter bin): the entries XORed into bucket
-//                        planes in shared memory that start at zero, then each vertex's rows XORed
-//                        into its sketch in HBM.
+//                        bin in shared memory, each record's C column depths hashed once into
+//                        4-bit codes carried by both entries, the runs written out coalesced.
+//   k_plane_update       per tile of W vertices: the tile's entries (filtered out of their gutter
+//                        bin when a bin holds several tiles) XORed into bucket planes in shared
+//                        memory that start at zero, then each vertex's rows XORed into its sketch
+//                        in HBM. The checksum is hashed here, per entry.
+// A coded entry is 128 bits: the C codes in bits 0 .. 4C - 1 (column c in bits 4c .. 4c + 3),
+// then the neighbour shifted left by bin_shift bits OR the vertex's offset inside its gutter bin
+// (the bin is known from where the entry lies). It is used when 4C + bin_shift + the neighbour's
+// bits fit in 128 (every CameoSketch up to 2^18 vertices).
 //
 // Bucket planes. A warp takes 32 entries, one per lane. At step t = 0..31 lane l handles slot
 // l ^ t of its entry: slot c < C is column c, slot C the deterministic bucket, higher slots are
@@ -52,74 +55,74 @@ constexpr uint32_t kPlaneBytes = kPlaneRows * kPlaneSlots * 4;  // one plane of 
 constexpr uint32_t kVertBytes = 3 * kPlaneBytes;              // planes A, B, G of one vertex
 constexpr uint32_t kWbRows = 4;                               // rows per write-back pass
 constexpr uint32_t kWbStride = 3 * kWbRows + 1;               // words per slot (odd: no conflicts)
-constexpr uint32_t kWbWords = kPlaneSlots * kWbStride;        // write-back buffer of one warp
+constexpr uint32_t kWbWords = kPlaneSlots * kWbStride;        // per-warp buffer (write-back, queue)
+constexpr uint32_t kQueueSlots = 64;                          // per-warp queue of filtered entries
+static_assert(kQueueSlots * 16 <= kWbWords * 4, "the entry queue shares the write-back buffer");
 
-// C depth codes of one record (edge index (hi << 32) | lo), column c in bits 4c..4c+3 of the
-// 128-bit result; unused nibbles are zero.
-__device__ __forceinline__ uint4 record_codes(uint32_t lo, uint32_t hi, const PlaneHash &ph) {
-  const uint64_t pm = xxh3_premix(((uint64_t)lo << 32) | hi);
-  const uint32_t cap = 1u << min(ph.B, kDepthEscape);
-  uint32_t w[4] = {0, 0, 0, 0};
+// Depth codes of all C columns into the nibble words w (column c in bits 4(c % 8) of word c / 8;
+// nibbles past C are zero); pm = premixed edge index. Every sketch has at least 18 columns: the
+// first 18 are unrolled, the rest a loop of exactly C - 18 steps.
+__device__ __forceinline__ void all_codes(uint64_t pm, const uint64_t *kcol, uint32_t C,
+                                          uint32_t cap, uint32_t (&w)[4]) {
+  w[0] = w[1] = 0;
 #pragma unroll
-  for (int c = 0; c < 18; ++c) w[c >> 3] |= depth_code(pm ^ ph.kcol[c], cap) << (4 * (c & 7));
-#pragma unroll
-  for (int c = 18; c < (int)kPlaneMaxColumns; ++c)
-    if (c < (int)ph.C) w[c >> 3] |= depth_code(pm ^ ph.kcol[c], cap) << (4 * (c & 7));
-  return make_uint4(w[0], w[1], w[2], w[3]);
+  for (int c = 0; c < 16; ++c) w[c >> 3] |= depth_code(pm ^ kcol[c], cap) << (4 * (c & 7));
+  uint64_t hiw = (uint64_t)depth_code(pm ^ kcol[16], cap) |
+                 ((uint64_t)depth_code(pm ^ kcol[17], cap) << 4);
+#pragma unroll 2
+  for (uint32_t c = 18; c < C; ++c) hiw |= (uint64_t)depth_code(pm ^ kcol[c], cap) << (4 * (c - 16));
+  w[2] = (uint32_t)hiw;
+  w[3] = (uint32_t)(hiw >> 32);
+}
+
+// Coded entry of vertex a (neighbour b): the codes, then from bit 4C the payload
+// (b << bin_shift) | (a & bin mask).
+__device__ __forceinline__ uint4 pack_entry(const uint32_t (&w)[4], uint32_t a, uint32_t b,
+                                            uint32_t C, uint32_t bin_shift) {
+  const uint64_t pay = ((uint64_t)b << bin_shift) | (a & ((1u << bin_shift) - 1u));
+  const uint64_t hi = (((uint64_t)w[3] << 32) | w[2]) | (pay << (4 * C - 64));
+  return make_uint4(w[0], w[1], (uint32_t)hi, (uint32_t)(hi >> 32));
+}
+
+// Vertex, neighbour and codes of a coded entry lying in gutter bin `bin`.
+__device__ __forceinline__ void unpack_entry(uint4 e, uint32_t bin, uint32_t C, uint32_t bin_shift,
+                                             uint32_t &v, uint32_t &u, uint32_t (&w)[4]) {
+  const uint64_t hi = ((uint64_t)e.w << 32) | e.z;
+  const uint32_t sh = 4 * C - 64;
+  const uint64_t pay = hi >> sh;
+  const uint64_t codes_hi = hi & ((1ull << sh) - 1ull);
+  v = (bin << bin_shift) | ((uint32_t)pay & ((1u << bin_shift) - 1u));
+  u = (uint32_t)(pay >> bin_shift);
+  w[0] = e.x;
+  w[1] = e.y;
+  w[2] = (uint32_t)codes_hi;
+  w[3] = (uint32_t)(codes_hi >> 32);
 }
 
 // ------------------------------------------------------------------------------------------------
 // hash sort-scatter (records in, coded entries out)
 // ------------------------------------------------------------------------------------------------
-// Exclusive scan over the threads of a block of any multiple of 32 threads (<= 1024).
-__device__ __forceinline__ uint32_t block_scan(uint32_t x, uint32_t *ws /*32*/) {
-  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  uint32_t inc = x;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t y = __shfl_up_sync(kFull, inc, o);
-    if (lane >= (uint32_t)o) inc += y;
-  }
-  if (lane == 31) ws[warp] = inc;
-  __syncthreads();
-  if (warp == 0) {
-    uint32_t w = lane < nwarps ? ws[lane] : 0u;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(kFull, w, o);
-      if (lane >= (uint32_t)o) w += y;
-    }
-    ws[lane] = w;
-  }
-  __syncthreads();
-  const uint32_t r = (warp ? ws[warp - 1] : 0u) + inc - x;
-  __syncthreads();
-  return r;
-}
-
-// Two CTAs of 512 threads per SM, so that one CTA's staging, scan and write-out overlap the
-// other's hashing. Per tile of rec_tile records: stage them (coalesced 128-bit loads), count
-// their endpoint entries per bin, reserve one run per non-empty bin in the gutter (one global
-// atomic each), hash every record once, place both entries in bin order in shared memory, and
-// write the runs out.
-constexpr int kHashSortThreads = 512;
+// Per tile of rec_tile records: stage them (coalesced 128-bit loads), count their endpoint entries
+// per bin, reserve one run per non-empty bin in the gutter (one global atomic each), hash every
+// record's C columns once, place both entries (and their bins) in bin order in shared memory,
+// and write the runs out.
 template <int RPT>
-__global__ void __launch_bounds__(kHashSortThreads, 2)
+__global__ void __launch_bounds__(1024, 1)
 k_hash_sort_scatter(const uint8_t *__restrict__ rec, uint64_t n, GutterGeom g, PlaneHash ph,
                     uint32_t rec_tile, const uint64_t *__restrict__ base,
-                    uint32_t *__restrict__ fill, uint2 *__restrict__ keys,
-                    uint4 *__restrict__ codes) {
+                    uint32_t *__restrict__ fill, uint4 *__restrict__ entries) {
   extern __shared__ __align__(16) uint8_t gsm[];
   __shared__ uint32_t ws[32];
   const uint32_t nb = g.nbins, nb4 = (nb + 3) & ~3u;
   uint32_t *s_cur = reinterpret_cast<uint32_t *>(gsm);  // counts, then placement cursors
   uint32_t *s_rel = s_cur + nb4;  // a bin's run: gutter position minus position in the tile
-  uint2 *s_key = reinterpret_cast<uint2 *>(s_rel + nb4);
-  uint4 *s_code = reinterpret_cast<uint4 *>(s_key + 2 * (size_t)rec_tile);
-  // the staged records share the key area: they are parsed into registers before the first key
-  // is placed, and the next tile is staged only after the write-out
-  uint8_t *s_rec = reinterpret_cast<uint8_t *>(s_key);
-  const uint32_t per_thread = (nb + blockDim.x - 1) / blockDim.x;  // bins per thread (<= 16)
+  uint4 *s_ent = reinterpret_cast<uint4 *>(s_rel + nb4);
+  uint16_t *s_bin = reinterpret_cast<uint16_t *>(s_ent + 2 * (size_t)rec_tile);  // bin of each entry
+  // the staged records share the entry area: they are parsed into registers before the first
+  // entry is placed, and the next tile is staged only after the write-out
+  uint8_t *s_rec = reinterpret_cast<uint8_t *>(s_ent);
+  const uint32_t per_thread = (nb + blockDim.x - 1) / blockDim.x;  // bins per thread (<= 8)
+  const uint32_t cap = 1u << min(ph.B, kDepthEscape);
   for (uint64_t t0 = blockIdx.x * (uint64_t)rec_tile; t0 < n; t0 += (uint64_t)gridDim.x * rec_tile) {
     const uint32_t cnt = (uint32_t)(n - t0 < rec_tile ? n - t0 : rec_tile);
     for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) s_cur[b] = 0u;
@@ -150,7 +153,7 @@ k_hash_sort_scatter(const uint8_t *__restrict__ rec, uint64_t n, GutterGeom g, P
       const uint32_t b = threadIdx.x * per_thread + k;
       sum += b < nb ? s_cur[b] : 0u;
     }
-    uint32_t run = block_scan(sum, ws);
+    uint32_t run = block_scan_1024(sum, ws);
     for (uint32_t k = 0; k < per_thread; ++k) {
       const uint32_t b = threadIdx.x * per_thread + k;
       if (b < nb) {
@@ -172,21 +175,19 @@ k_hash_sort_scatter(const uint8_t *__restrict__ rec, uint64_t n, GutterGeom g, P
 #pragma unroll
     for (int k = 0; k < RPT; ++k)
       if (ru[k] != 0xffffffffu) {
-        const uint4 cw = record_codes(max(ru[k], rv[k]), min(ru[k], rv[k]), ph);
-        s_key[pu[k]] = make_uint2(ru[k], rv[k]);
-        s_key[pv[k]] = make_uint2(rv[k], ru[k]);
-        s_code[pu[k]] = cw;
-        s_code[pv[k]] = cw;
+        const uint32_t lo = max(ru[k], rv[k]), hi = min(ru[k], rv[k]);
+        const uint64_t pm = xxh3_premix(((uint64_t)lo << 32) | hi);
+        uint32_t w[4];
+        all_codes(pm, ph.kcol, ph.C, cap, w);
+        s_ent[pu[k]] = pack_entry(w, ru[k], rv[k], ph.C, g.bin_shift);
+        s_ent[pv[k]] = pack_entry(w, rv[k], ru[k], ph.C, g.bin_shift);
+        s_bin[pu[k]] = (uint16_t)(ru[k] >> g.bin_shift);
+        s_bin[pv[k]] = (uint16_t)(rv[k] >> g.bin_shift);
       }
     __syncthreads();
     // 4. coalesced write-out of the runs
     const uint32_t total = s_cur[nb - 1];
-    for (uint32_t j = threadIdx.x; j < total; j += blockDim.x) {
-      const uint2 x = s_key[j];
-      const uint32_t dst = s_rel[x.x >> g.bin_shift] + j;
-      keys[dst] = x;
-      codes[dst] = s_code[j];
-    }
+    for (uint32_t j = threadIdx.x; j < total; j += blockDim.x) entries[s_rel[s_bin[j]] + j] = s_ent[j];
     __syncthreads();
   }
 }
@@ -268,56 +269,115 @@ __device__ __forceinline__ void permute_codes(uint32_t (&c4)[4], uint32_t lane) 
   }
 }
 
-__device__ __forceinline__ void plane_entry(uint2 key, uint4 cw, bool valid, uint32_t lane,
-                                            uint32_t sp, uint32_t tile_mask, uint32_t *gsk,
-                                            uint32_t sketch_words, const uint64_t *s_kcol,
-                                            uint64_t kchk, uint32_t C, uint32_t B) {
-  const uint32_t v = key.x, u = key.y;
-  const uint32_t lo = max(u, v), hi = min(u, v);  // idx = (min << 32) | max
-  const uint64_t pm = xxh3_premix(((uint64_t)lo << 32) | hi);
-  const uint32_t chk = valid ? tail_lo32(pm ^ kchk) : 0u;
-  const uint32_t val = valid ? (u | 0x80000000u) : 0u;  // invalid lanes XOR zeros
-  const uint32_t p = u > v ? 0u : 1u;                    // plane A or B
-  uint32_t c4[4] = {cw.x, cw.y, cw.z, cw.w};
-  const uint4 fl = make_uint4(high_code_flags(cw.x), high_code_flags(cw.y), high_code_flags(cw.z),
-                              high_code_flags(cw.w));
-  if (valid && (fl.x | fl.y | fl.z | fl.w)) {
-    const uint4 x = spill_high_codes(cw, fl, pm, lo, hi, chk, gsk + (uint64_t)v * sketch_words, s_kcol, B);
-    c4[0] = x.x;
-    c4[1] = x.y;
-    c4[2] = x.z;
-    c4[3] = x.w;
+struct PlaneCtx {
+  uint32_t sp, tile_mask, sketch_words, C, B, cap, bin_shift;
+  uint32_t *gsk;
+  const uint64_t *s_kcol;
+  uint64_t kchk;
+};
+
+// All codes of a plain {vertex, neighbour} entry (apply_update_batch), hashed where it is applied;
+// out of line, so the coded path keeps its registers.
+__device__ __noinline__ uint4 plain_codes(uint64_t pm, const uint64_t *kcol, uint32_t C, uint32_t cap) {
+  uint32_t w[4];
+  all_codes(pm, kcol, C, cap, w);
+  return make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+// Vertex, neighbour and codes of a gutter entry of bin `bin`: unpacked from a coded entry, or
+// hashed here for a plain {vertex, neighbour} entry (apply_update_batch).
+__device__ __forceinline__ void decode_entry(uint4 e, bool coded, uint32_t bin, const PlaneCtx &x,
+                                             uint32_t &v, uint32_t &u, uint64_t &pm, uint32_t (&c4)[4]) {
+  if (coded) {
+    unpack_entry(e, bin, x.C, x.bin_shift, v, u, c4);
+  } else {
+    v = e.x;
+    u = e.y;
+  }
+  pm = xxh3_premix(((uint64_t)max(u, v) << 32) | min(u, v));  // idx = (min << 32) | max
+  if (!coded) {
+    const uint4 w = plain_codes(pm, x.s_kcol, x.C, x.cap);
+    c4[0] = w.x;
+    c4[1] = w.y;
+    c4[2] = w.z;
+    c4[3] = w.w;
+  }
+}
+
+// Vertex of a gutter entry of bin `bin` (for filtering a bin's entries by tile).
+__device__ __forceinline__ uint32_t entry_vertex(uint4 e, bool coded, uint32_t bin, const PlaneCtx &x) {
+  if (!coded) return e.x;
+  const uint64_t hi = ((uint64_t)e.w << 32) | e.z;
+  return (bin << x.bin_shift) | ((uint32_t)(hi >> (4 * x.C - 64)) & ((1u << x.bin_shift) - 1u));
+}
+
+// One entry per lane into the tile's planes (invalid lanes XOR zeros into vertex 0 of the tile).
+__device__ __forceinline__ void plane_entry(uint4 e, bool coded, bool valid, uint32_t bin,
+                                            uint32_t lane, const PlaneCtx &x) {
+  uint32_t v, u, c4[4];
+  uint64_t pm;
+  decode_entry(e, coded, bin, x, v, u, pm, c4);
+  const uint32_t lo = max(u, v), hi = min(u, v);
+  const uint32_t chk = valid ? tail_lo32(pm ^ x.kchk) : 0u;
+  const uint32_t val = valid ? (u | 0x80000000u) : 0u;
+  const uint32_t p = u > v ? 0u : 1u;  // plane A or B
+  if (!valid) c4[0] = c4[1] = c4[2] = c4[3] = 0;
+  const uint4 fl = make_uint4(high_code_flags(c4[0]), high_code_flags(c4[1]), high_code_flags(c4[2]),
+                              high_code_flags(c4[3]));
+  if (fl.x | fl.y | fl.z | fl.w) {
+    const uint4 y = spill_high_codes(make_uint4(c4[0], c4[1], c4[2], c4[3]), fl, pm, lo, hi, chk,
+                                     x.gsk + (uint64_t)v * x.sketch_words, x.s_kcol, x.B);
+    c4[0] = y.x;
+    c4[1] = y.y;
+    c4[2] = y.z;
+    c4[3] = y.w;
   }
   permute_codes(c4, lane);
-  // bits 2..6 of base are the lane (sp is 128-byte aligned, the rest multiples of 128), so
-  // base ^ (t << 2) addresses slot lane ^ t of the same row
-  const uint32_t base = sp + (v & tile_mask) * kVertBytes + p * kPlaneBytes + (lane << 2);
+  // one byte per step: byte k of ev[w] (od[w]) = 8 x code of nibble 2k (2k + 1) of word w, so a
+  // step takes its row offset with one byte extract
+  uint32_t ev[4], od[4];
+#pragma unroll
+  for (int w = 0; w < 4; ++w) {
+    ev[w] = (c4[w] & 0x0f0f0f0fu) << 3;
+    od[w] = ((c4[w] >> 4) & 0x0f0f0f0fu) << 3;
+  }
+  // bits 2..6 of base are the lane (sp is 128-byte aligned, the rest multiples of 128), and the
+  // row offset (a multiple of 128) leaves them alone, so (base + row) ^ (t << 2) addresses slot
+  // lane ^ t of the row
+  const uint32_t base = x.sp + (v & x.tile_mask) * kVertBytes + p * kPlaneBytes + (lane << 2);
   const uint32_t dg = (2u - p) * kPlaneBytes;
 #pragma unroll
   for (int t = 0; t < 32; ++t) {
-    const uint32_t d = (c4[t >> 3] >> (4 * (t & 7))) & 15u;
-    const uint32_t a = (base ^ (uint32_t)(t << 2)) + (d << 7);
+    const uint32_t w = (uint32_t)t >> 3, k = ((uint32_t)t & 7u) >> 1;
+    const uint32_t d8 = __byte_perm((t & 1) ? od[w] : ev[w], 0, 0x4440u + k);
+    const uint32_t a = (base + d8 * 16u) ^ (uint32_t)(t << 2);
     red_xor_shared(a, val);
     red_xor_shared(a + dg, chk);
   }
 }
 
 // One entry applied straight to HBM (sparse tiles): deterministic bucket, then each column.
-__device__ __forceinline__ void entry_in_place(uint2 key, uint4 cw, uint32_t *gsk,
-                                               uint32_t sketch_words, const uint64_t *s_kcol,
-                                               uint64_t kchk, uint32_t C, uint32_t B) {
-  const uint32_t v = key.x, u = key.y;
+__device__ __forceinline__ void entry_in_place(uint4 e, bool coded, uint32_t bin, uint32_t tile,
+                                               uint32_t tile_shift, const PlaneCtx &x) {
+  uint32_t v, u, c4[4];
+  uint64_t pm;
+  decode_entry(e, coded, bin, x, v, u, pm, c4);
+  if ((v >> tile_shift) != tile) return;
   const uint32_t lo = max(u, v), hi = min(u, v);
-  const uint64_t pm = xxh3_premix(((uint64_t)lo << 32) | hi);
-  const uint32_t chk = tail_lo32(pm ^ kchk);
-  uint32_t *sk = gsk + (uint64_t)v * sketch_words;
-  xor_bucket_global(sk, C * B, lo, hi, chk);
-  const uint32_t c4[4] = {cw.x, cw.y, cw.z, cw.w};
-  for (uint32_t c = 0; c < C; ++c) {
+  const uint32_t chk = tail_lo32(pm ^ x.kchk);
+  uint32_t *sk = x.gsk + (uint64_t)v * x.sketch_words;
+  xor_bucket_global(sk, x.C * x.B, lo, hi, chk);
+  for (uint32_t c = 0; c < x.C; ++c) {
     const uint32_t code = nibble_of(c4, c);
-    const uint32_t d = code < kDepthEscape ? code : depth_exact(pm ^ s_kcol[c], B);
-    if (d < B) xor_bucket_global(sk, c * B + d, lo, hi, chk);
+    const uint32_t d = code < kDepthEscape ? code : depth_exact(pm ^ x.s_kcol[c], x.B);
+    if (d < x.B) xor_bucket_global(sk, c * x.B + d, lo, hi, chk);
   }
+}
+
+__device__ __forceinline__ uint4 load_entry(const uint8_t *cb, bool coded, uint32_t i) {
+  if (coded) return reinterpret_cast<const uint4 *>(cb)[i];
+  const uint2 k = reinterpret_cast<const uint2 *>(cb)[i];
+  return make_uint4(k.x, k.y, 0, 0);
 }
 
 __global__ void __launch_bounds__(1024, 1)
@@ -327,45 +387,56 @@ k_plane_update(PlaneGeom g, PlaneHash ph, uint8_t *__restrict__ sketches,
   extern __shared__ __align__(16) uint8_t dsm[];
   __shared__ uint64_t s_kcol[kPlaneMaxColumns];
   __shared__ uint32_t s_claim[2];
-  const uint32_t W = 1u << g.tile_shift, tile_mask = W - 1;
+  const uint32_t W = 1u << g.tile_shift;
   const uint32_t nwarps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t per_bin = g.bin_shift - g.tile_shift;  // log2(tiles per bin)
   const uint32_t s0 = smem_u32(dsm);
   const uint32_t pad = (128u - (s0 & 127u)) & 127u;
   uint8_t *planes = dsm + pad;  // W vertices x planes A, B, G x kPlaneRows x 32 words
-  const uint32_t sp = s0 + pad;
   uint32_t *wbuf = reinterpret_cast<uint32_t *>(planes + (size_t)W * kVertBytes) + warp * kWbWords;
+  uint4 *queue = reinterpret_cast<uint4 *>(wbuf);  // the apply phase's per-warp entry queue
   for (uint32_t i = threadIdx.x; i < g.C; i += blockDim.x) s_kcol[i] = ph.kcol[i];
-  uint32_t *gsk = reinterpret_cast<uint32_t *>(sketches);
-  const uint32_t stride = g.ntiles + 1;  // one bin per tile
+  PlaneCtx x;
+  x.sp = s0 + pad;
+  x.tile_mask = W - 1;
+  x.sketch_words = g.sketch_words;
+  x.C = g.C;
+  x.B = g.B;
+  x.cap = 1u << min(g.B, kDepthEscape);
+  x.bin_shift = g.bin_shift;
+  x.gsk = reinterpret_cast<uint32_t *>(sketches);
+  x.s_kcol = s_kcol;
+  x.kchk = ph.kchk;
+  const uint32_t stride = g.nbins + 1;
   const uint32_t C = g.C, B = g.B;
   for (;;) {
     if (threadIdx.x == 0) {
       const uint32_t t = atomicAdd(work_counter, 1u);
       uint32_t total = 0;
-      if (t < g.ntiles)
+      if (t < g.ntiles) {
+        const uint32_t bin = t >> per_bin;
         for (int k = 0; k < nchunks; ++k)
-          total += bin_off[(uint64_t)k * stride + t + 1] - bin_off[(uint64_t)k * stride + t];
+          total += bin_off[(uint64_t)k * stride + bin + 1] - bin_off[(uint64_t)k * stride + bin];
+      }
       s_claim[0] = t;
       s_claim[1] = total;
     }
     __syncthreads();
-    const uint32_t t = s_claim[0], total = s_claim[1];
+    const uint32_t t = s_claim[0], total = s_claim[1];  // total: entries of the tile's bin
     if (t >= g.ntiles) break;
+    const uint32_t bin = t >> per_bin;
     if (total == 0) {
       __syncthreads();
       continue;
     }
-    if (total < g.direct_max) {
+    if (total < (g.direct_max << per_bin)) {
       // few entries: updated in place in HBM (no planes to clear and write back)
       for (int k = 0; k < nchunks; ++k) {
-        const uint64_t b = bin_off[(uint64_t)k * stride + t], e = bin_off[(uint64_t)k * stride + t + 1];
-        const uint2 *keys = reinterpret_cast<const uint2 *>(gutter + chunks.base[k]);
-        const uint4 *codes = chunks.kind[k] == kEntryCoded ? reinterpret_cast<const uint4 *>(gutter + chunks.aux[k]) : nullptr;
-        for (uint64_t i = b + threadIdx.x; i < e; i += blockDim.x) {
-          const uint2 key = keys[i];
-          const uint4 cw = codes ? codes[i] : record_codes(max(key.x, key.y), min(key.x, key.y), ph);
-          entry_in_place(key, cw, gsk, g.sketch_words, s_kcol, ph.kchk, C, B);
-        }
+        const uint32_t b = bin_off[(uint64_t)k * stride + bin], e = bin_off[(uint64_t)k * stride + bin + 1];
+        const uint8_t *cb = gutter + chunks.base[k];
+        const bool coded = chunks.kind[k] == kEntryCoded;
+        for (uint32_t i = b + threadIdx.x; i < e; i += blockDim.x)
+          entry_in_place(load_entry(cb, coded, i), coded, bin, t, g.tile_shift, x);
       }
       __syncthreads();
       continue;
@@ -376,29 +447,59 @@ k_plane_update(PlaneGeom g, PlaneHash ph, uint8_t *__restrict__ sketches,
       for (uint32_t i = threadIdx.x; i < n16; i += blockDim.x) pz[i] = make_uint4(0, 0, 0, 0);
     }
     __syncthreads();
+    // an invalid lane carries an entry of vertex 0 of the tile with neighbour 0 and no codes
+    const uint4 pad_entry = make_uint4(t << g.tile_shift, 0, 0, 0);
     for (int k = 0; k < nchunks; ++k) {
-      const uint32_t b = bin_off[(uint64_t)k * stride + t], e = bin_off[(uint64_t)k * stride + t + 1];
-      const uint2 *keys = reinterpret_cast<const uint2 *>(gutter + chunks.base[k]);
-      const uint4 *codes = chunks.kind[k] == kEntryCoded ? reinterpret_cast<const uint4 *>(gutter + chunks.aux[k]) : nullptr;
-      // each warp takes batches of 32 entries; the next batch's entry is loaded while this one
-      // is applied (an invalid lane XORs zeros into vertex 0 of the tile)
-      const uint2 pad_key = make_uint2((uint32_t)t << g.tile_shift, (uint32_t)t << g.tile_shift);
+      const uint32_t b = bin_off[(uint64_t)k * stride + bin], e = bin_off[(uint64_t)k * stride + bin + 1];
+      const uint8_t *cb = gutter + chunks.base[k];
+      const bool coded = chunks.kind[k] == kEntryCoded;
+      // each warp takes groups of 32 entries; the next group is loaded while this one is used
       uint32_t i0 = b + warp * 32;
       bool nvalid = i0 + lane < e;
-      uint2 nkey = nvalid ? keys[i0 + lane] : pad_key;
-      uint4 ncw = nvalid && codes ? codes[i0 + lane] : make_uint4(0, 0, 0, 0);
-      for (; i0 < e; i0 += nwarps * 32) {
-        const uint2 key = nkey;
-        uint4 cw = ncw;
-        const bool valid = nvalid;
-        const uint32_t in = i0 + nwarps * 32 + lane;
-        nvalid = in < e;
-        if (nvalid) {
-          nkey = keys[in];
-          if (codes) ncw = codes[in];
+      uint4 nx = nvalid ? load_entry(cb, coded, i0 + lane) : pad_entry;
+      if (per_bin == 0) {
+        // the bin is this tile: every entry applies
+        for (; i0 < e; i0 += nwarps * 32) {
+          const uint4 en = nx;
+          const bool valid = nvalid;
+          const uint32_t in = i0 + nwarps * 32 + lane;
+          nvalid = in < e;
+          if (nvalid) nx = load_entry(cb, coded, in);
+          plane_entry(en, coded, valid, bin, lane, x);
         }
-        if (valid && !codes) cw = record_codes(max(key.x, key.y), min(key.x, key.y), ph);
-        plane_entry(key, cw, valid, lane, sp, tile_mask, gsk, g.sketch_words, s_kcol, ph.kchk, C, B);
+      } else {
+        // the bin holds several tiles: each warp ballots its group, queues this tile's entries,
+        // and applies full warps of queued entries; two groups are in flight ahead of the one
+        // ballotted
+        uint32_t qn = 0;
+        const uint32_t step = nwarps * 32;
+        bool nvalid2 = i0 + step + lane < e;
+        uint4 nx2 = nvalid2 ? load_entry(cb, coded, i0 + step + lane) : pad_entry;
+        for (; i0 < e; i0 += step) {
+          const uint4 en = nx;
+          const bool mine = nvalid && (entry_vertex(en, coded, bin, x) >> g.tile_shift) == t;
+          nx = nx2;
+          nvalid = nvalid2;
+          const uint32_t in = i0 + 2 * step + lane;
+          nvalid2 = in < e;
+          if (nvalid2) nx2 = load_entry(cb, coded, in);
+          const uint32_t m = __ballot_sync(kFull, mine);
+          if (mine) queue[qn + __popc(m & ((1u << lane) - 1u))] = en;
+          qn += __popc(m);
+          __syncwarp();
+          if (qn >= 32) {
+            const uint4 q = queue[lane];
+            __syncwarp();
+            qn -= 32;
+            if (lane < qn) queue[lane] = queue[32 + lane];
+            __syncwarp();
+            plane_entry(q, coded, true, bin, lane, x);
+          }
+        }
+        const bool valid = lane < qn;
+        const uint4 q = valid ? queue[lane] : pad_entry;
+        __syncwarp();
+        if (qn) plane_entry(q, coded, valid, bin, lane, x);
       }
     }
     __syncthreads();
@@ -412,7 +513,7 @@ k_plane_update(PlaneGeom g, PlaneHash ph, uint8_t *__restrict__ sketches,
       const uint32_t *pa = reinterpret_cast<const uint32_t *>(planes + (size_t)vl * kVertBytes);
       const uint32_t *pb = pa + kPlaneRows * kPlaneSlots;
       const uint32_t *pg = pb + kPlaneRows * kPlaneSlots;
-      uint32_t *sk = gsk + (uint64_t)vg * g.sketch_words;
+      uint32_t *sk = x.gsk + (uint64_t)vg * g.sketch_words;
       for (uint32_t r0 = 0; r0 < R; r0 += kWbRows) {
         const uint32_t nr = min(kWbRows, R - r0);
         for (uint32_t rr = 0; rr < nr; ++rr) {
@@ -428,16 +529,16 @@ k_plane_update(PlaneGeom g, PlaneHash ph, uint8_t *__restrict__ sketches,
         if (j < nw) {
 #pragma unroll 4
           for (uint32_t c = lane >> 4; c < C; c += 2) {
-            const uint32_t x = wbuf[c * kWbStride + j];
-            if (x) {
+            const uint32_t y = wbuf[c * kWbStride + j];
+            if (y) {
               uint32_t *q = sk + 3 * (c * B + r0) + j;
-              *q ^= x;
+              *q ^= y;
             }
           }
         }
         if (r0 == 0 && lane < 3) {  // deterministic bucket: slot C, row 0
-          const uint32_t x = wbuf[C * kWbStride + lane];
-          if (x) sk[3 * C * B + lane] ^= x;
+          const uint32_t y = wbuf[C * kWbStride + lane];
+          if (y) sk[3 * C * B + lane] ^= y;
         }
         __syncwarp();
       }
@@ -451,21 +552,21 @@ k_plane_update(PlaneGeom g, PlaneHash ph, uint8_t *__restrict__ sketches,
 // being this one XOR its code.
 __global__ void k_plane_hash_peak(uint32_t iters, uint64_t *out) {
   const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  uint64_t x[8];
+  uint64_t y[8];
 #pragma unroll
-  for (int k = 0; k < 8; ++k) x[k] = xxh3_premix(tid * 8 + k);
+  for (int k = 0; k < 8; ++k) y[k] = xxh3_premix(tid * 8 + k);
   uint32_t acc = 0;
   for (uint32_t i = 0; i < iters; ++i) {
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-      const uint32_t d = depth_code(x[k] ^ (0x9E3779B97F4A7C15ULL * (uint64_t)(k + 1)), 1u << kDepthEscape);
+      const uint32_t d = depth_code(y[k] ^ (0x9E3779B97F4A7C15ULL * (uint64_t)(k + 1)), 1u << kDepthEscape);
       acc += d;
-      x[k] ^= d;
+      y[k] ^= d;
     }
   }
   uint64_t r = acc;
 #pragma unroll
-  for (int k = 0; k < 8; ++k) r ^= x[k];
+  for (int k = 0; k < 8; ++k) r ^= y[k];
   out[tid] = r;
 }
 
@@ -481,20 +582,27 @@ __global__ void __launch_bounds__(1024, 1) k_plane_update_peak(uint32_t iters, u
   uint32_t *pw = reinterpret_cast<uint32_t *>(planes);
   for (uint32_t i = threadIdx.x; i < kPlaneMaxTile * kVertBytes / 4; i += blockDim.x) pw[i] = 0;
   __syncthreads();
-  uint32_t x = fmix32_(blockIdx.x * 1024u + threadIdx.x);
+  uint32_t z = fmix32_(blockIdx.x * 1024u + threadIdx.x);
   for (uint32_t it = 0; it < iters; ++it) {
-    x = x * 1664525u + 1013904223u;
+    z = z * 1664525u + 1013904223u;
     uint32_t c4[4];
 #pragma unroll
-    for (int w = 0; w < 4; ++w) c4[w] = fmix32_(x + (uint32_t)w) & 0x33333333u;
-    const uint32_t v = x >> 27, p = (x >> 26) & 1u;
-    const uint32_t val = x | 0x80000000u, chk = x * 747796405u;
+    for (int w = 0; w < 4; ++w) c4[w] = fmix32_(z + (uint32_t)w) & 0x33333333u;
+    const uint32_t v = z >> 27, p = (z >> 26) & 1u;
+    const uint32_t val = z | 0x80000000u, chk = z * 747796405u;
+    uint32_t ev[4], od[4];
+#pragma unroll
+    for (int w = 0; w < 4; ++w) {
+      ev[w] = (c4[w] & 0x0f0f0f0fu) << 3;
+      od[w] = ((c4[w] >> 4) & 0x0f0f0f0fu) << 3;
+    }
     const uint32_t base = sp + v * kVertBytes + p * kPlaneBytes + (lane << 2);
     const uint32_t dg = (2u - p) * kPlaneBytes;
 #pragma unroll
     for (int t = 0; t < 32; ++t) {
-      const uint32_t d = (c4[t >> 3] >> (4 * (t & 7))) & 15u;
-      const uint32_t a = (base ^ (uint32_t)(t << 2)) + (d << 7);
+      const uint32_t w = (uint32_t)t >> 3, k = ((uint32_t)t & 7u) >> 1;
+      const uint32_t d8 = __byte_perm((t & 1) ? od[w] : ev[w], 0, 0x4440u + k);
+      const uint32_t a = (base + d8 * 16u) ^ (uint32_t)(t << 2);
       red_xor_shared(a, val);
       red_xor_shared(a + dg, chk);
     }
@@ -520,41 +628,38 @@ PlaneHash plane_hash(uint64_t seed, uint32_t C, uint32_t B) {
   return ph;
 }
 
+constexpr int kHashSortMaxRpt = 6;
+
 uint32_t hash_sort_tile(uint32_t nbins, size_t smem_budget) {
-  // two CTAs per SM: each gets half the SM's shared memory (less the per-CTA reservation)
-  const size_t per_cta = std::min<size_t>(smem_budget, (228 * 1024 - 2 * 1024) / 2);
   const size_t fixed = (size_t)2 * ((nbins + 3) & ~3u) * 4 + 256;
-  if (nbins > kSortBinsMax || fixed >= per_cta) return 0;
-  // 2 entries per record: 8 B of key + 16 B of codes each
-  const size_t t = std::min<size_t>((per_cta - fixed) / 48, 4 * kHashSortThreads);
-  return (uint32_t)(t / kHashSortThreads * kHashSortThreads);
+  if (nbins > kSortBinsMax || fixed >= smem_budget) return 0;
+  // 2 coded entries of 16 B per record, and their 2-byte bins
+  const size_t t = std::min<size_t>((smem_budget - fixed) / 36, kHashSortMaxRpt * 1024);
+  return (uint32_t)(t / 1024 * 1024);
 }
 
 cudaError_t gutter_hash_sort(const void *d_rec, uint64_t n, GutterGeom g, const PlaneHash &ph,
-                             uint32_t rec_tile, const uint64_t *base, uint32_t *fill, uint2 *keys,
-                             uint4 *codes, cudaStream_t s) {
+                             uint32_t rec_tile, const uint64_t *base, uint32_t *fill,
+                             uint4 *entries, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
-  if (rec_tile < kHashSortThreads || rec_tile > 4 * kHashSortThreads || rec_tile % kHashSortThreads)
-    return cudaErrorInvalidValue;
-  const size_t smem = (size_t)2 * ((g.nbins + 3) & ~3u) * 4 + (size_t)rec_tile * 48;
-  const uint64_t tiles = (n + rec_tile - 1) / rec_tile;
+  if (rec_tile < 1024 || rec_tile > kHashSortMaxRpt * 1024 || rec_tile % 1024) return cudaErrorInvalidValue;
+  const size_t smem = (size_t)2 * ((g.nbins + 3) & ~3u) * 4 + (size_t)rec_tile * 36;
+  const int G = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)num_sms(), (n + rec_tile - 1) / rec_tile));
   const uint8_t *rec = reinterpret_cast<const uint8_t *>(d_rec);
   auto launch = [&](auto kern) -> cudaError_t {
     cudaError_t e = smem_optin(kern);
     if (e != cudaSuccess) return e;
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kHashSortThreads, smem) != cudaSuccess || per_sm < 1)
-      per_sm = 1;
-    const int G = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)num_sms() * per_sm, tiles));
-    kern<<<G, kHashSortThreads, smem, s>>>(rec, n, g, ph, rec_tile, base, fill, keys, codes);
+    kern<<<G, 1024, smem, s>>>(rec, n, g, ph, rec_tile, base, fill, entries);
     add_launches(1);
     return cudaGetLastError();
   };
-  switch (rec_tile / kHashSortThreads) {
+  switch (rec_tile / 1024) {
     case 1: return launch(k_hash_sort_scatter<1>);
     case 2: return launch(k_hash_sort_scatter<2>);
     case 3: return launch(k_hash_sort_scatter<3>);
-    default: return launch(k_hash_sort_scatter<4>);
+    case 4: return launch(k_hash_sort_scatter<4>);
+    case 5: return launch(k_hash_sort_scatter<5>);
+    default: return launch(k_hash_sort_scatter<6>);
   }
 }
 
@@ -575,7 +680,8 @@ cudaError_t plane_update(const PlaneGeom &g, const PlaneHash &ph, uint8_t *sketc
                          const uint8_t *gutter, const ChunkTable &chunks, const uint32_t *bin_off,
                          int nchunks, uint32_t *work_counter, uint32_t * /*status*/, int grid,
                          int threads, cudaStream_t s) {
-  if (g.C > kPlaneMaxColumns || g.tile_shift > 5 || threads % 32 || threads < 32 || threads > 1024)
+  if (g.C > kPlaneMaxColumns || g.C < 18 || g.tile_shift > 5 ||
+      g.bin_shift < g.tile_shift || threads % 32 || threads < 32 || threads > 1024)
     return cudaErrorInvalidValue;
   cudaError_t e = smem_optin(k_plane_update);
   if (e != cudaSuccess) return e;

@@ -310,6 +310,8 @@ class ServingResult:
     ticks: int = 0
     gpu_queries: int = 0
     rejected: int = 0
+    waited: set = field(default_factory=set)  # tenants that waited for budget before admission
+    max_waiting: int = 0                      # longest queue of tenants waiting for budget
     phase_s: Dict[str, float] = field(default_factory=dict)  # wall seconds per loop phase
 
     def _add(self, phase: str, t0: float) -> None:
@@ -328,6 +330,7 @@ class ServingResult:
                 "admitted_tenants": self.admitted, "max_resident_tenants": self.max_resident,
                 "max_used_bytes": self.max_used_bytes, "ticks": self.ticks,
                 "gpu_query_batches": self.gpu_queries, "rejected_tenants": self.rejected,
+                "tenants_waited_for_budget": len(self.waited), "max_waiting_tenants": self.max_waiting,
                 "phase_s": {k: round(v, 4) for k, v in self.phase_s.items()}}
 
 
@@ -414,12 +417,16 @@ def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes:
                     res.answers[i] = ("rejected",)
                 continue
             if used[0] + c > budget_bytes:
+                res.waited.update(waiting)
+                res.max_waiting = max(res.max_waiting, len(waiting))
                 return
             ts = time.perf_counter()
             if mode == "batched":
                 try:
                     state[t] = server.admit(int(trace.num_vertices[t]), int(trace.seeds[t]))
                 except BudgetExhausted:
+                    res.waited.update(waiting)
+                    res.max_waiting = max(res.max_waiting, len(waiting))
                     return
             else:
                 a = CCSketchAlg(int(trace.num_vertices[t]), int(trace.seeds[t]))

@@ -32,7 +32,8 @@ def test_roofline_arithmetic():
     assert abs(r["frac"] - (hashes / 1358e9) / 6e-3) < 1e-12
     assert abs(r["terms_ms"]["int"] - hashes / 1358e9 * 1e3) < 1e-9
     g, u = r["kernels"]["gutter"], r["kernels"]["sketch_update"]
-    assert g["hashes_per_launch"] == n * 24 and abs(g["launch_ms"] - 3.0) < 1e-12
+    assert g["hashes_per_launch"] == n * 16 and abs(g["launch_ms"] - 3.0) < 1e-12
+    assert u["hashes_per_launch"] == 2 * n * 9
     assert u["slot_steps_per_launch"] == 2 * n * 32
     assert u["bucket_updates_per_launch"] == 2 * n * 25
     assert abs(u["smem"]["frac"] - (2 * n * 32 / 2.5e-3) / 3667e9) < 1e-12
@@ -44,6 +45,6 @@ def test_committed_traffic_is_per_step_of_each_workload():
         return
     n, V, sb = 139_997_155, 1 << 17, 9804
     algorithmic = 9 * n + 2 * V * sb
-    # DRAM bytes of the ingest kernels of one step: the coded entries (24 B per endpoint) are
+    # DRAM bytes of the ingest kernels of one step: the coded entries (16 B per endpoint) are
     # written and read once on top of the path's algorithmic bytes
-    assert algorithmic < traffic < algorithmic + 2 * 2 * n * 24 * 1.1
+    assert algorithmic < traffic < algorithmic + 2 * 2 * n * 16 * 1.1

@@ -152,10 +152,31 @@ def test_plane_tile_shapes_bit_exact(gz, oracle_mod, vpt, threads):
     assert (canonical(alg.connected_components().parent_arr) == labels).all()
 
 
-def test_coded_entries_need_one_tile_per_bin(gz):
+@pytest.mark.parametrize("vpt,tpb", [(32, 2), (32, 4), (16, 8), (8, 4)])
+def test_plane_tiles_per_bin_bit_exact(gz, oracle_mod, vpt, tpb):
+    """Coded entries in gutter bins of several tiles: each tile filters its entries out of the
+    bin (per-warp queues), coded and plain chunks alike."""
+    c, st, labels, _ = load_case("cl_v2048")
+    alg = _alg(gz, 2048, c["seed"])
+    alg.set_tuning(vpt, 1024, tpb, 2)
+    assert alg.params.vertices_per_tile == vpt
+    assert alg.params.vertices_per_bin == vpt * tpb
+    half = st.num_updates // 2
+    alg.ingest_records(st.records[:half])
+    for r in st.records[half:half + 200]:  # plain entries in the same bins
+        alg.apply_update_batch(0, int(r["src"]), [int(r["dst"])])
+        alg.apply_update_batch(1, int(r["dst"]), [int(r["src"])])
+    alg.ingest_records(st.records[half + 200:])
+    osk = oracle_mod.OracleSketches(2048, c["seed"])
+    osk.apply_records(st.raw())
+    assert (alg.dump_sketches() == osk.data).all()
+    assert (canonical(alg.connected_components().parent_arr) == labels).all()
+
+
+def test_coded_entries_reject_bad_shapes(gz):
     alg = _alg(gz, 1024, 5)
     with pytest.raises(gz.GZError):
-        alg.set_tuning(8, 1024, 2, 2)
+        alg.set_tuning(8, 1024, 16, 2)
     with pytest.raises(gz.GZError):
         alg.set_tuning(64, 1024, 1, 2)
     assert alg.params.entry_form == 2  # the handle keeps its tiling after a rejected request

@@ -37,8 +37,11 @@ def _check(gz, oracle_mod, V, seed, recs, form=2):
 
 
 def test_default_entry_form(gz):
-    """Coded entries by default while the 32-vertex gutter bins fit the hash sort (8192 bins)."""
-    assert gz.CCSketchAlg(1 << 18, 1).params.entry_form == 2
+    """Coded entries by default up to 2^18 vertices (gutter bins of one tile of 32 vertices)."""
+    a = gz.CCSketchAlg(1 << 18, 1)
+    assert a.params.entry_form == 2
+    assert a.params.vertices_per_tile == 32 and a.params.vertices_per_bin == 32
+    a.close()
     assert gz.CCSketchAlg((1 << 18) + 1, 1).params.entry_form == 1
     a = gz.CCSketchAlg(1024, 1)
     a.set_pipeline(1)
