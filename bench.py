@@ -205,10 +205,10 @@ def roofline(alg, n, prof, steps, ingest_ms, hash_peak, hbm_peak_gbs, update_pea
     algorithmic work of one record: 1 + C XXH3 hashes (one per column and the checksum, hashed
     once per edge), 9 B of stream read, and the touched sketches read and written once. The path
     is bound by the slower of the hash term (over the measured hash rate) and the HBM term.
-    Per kernel: the gutter phase (count + hash sort-scatter) against its own hashes (the first 16
-    columns per record) and bytes, the sketch update against the shared-memory slot rate
-    (2 (C + 1) bucket updates per record, made as 2 x 32 slot steps), its hashes (the other
-    C - 16 columns and the checksum, per endpoint) and its bytes."""
+    Per kernel: the gutter phase (count + hash sort-scatter) against its own hashes (C columns per
+    record, once) and bytes, the sketch update against the shared-memory slot rate (2 (C + 1)
+    bucket updates per record, made as 2 x 32 slot steps), its hashes (the checksum, per
+    endpoint) and its bytes."""
     p = alg.params
     V, C, B, sb = p.num_vertices, p.num_columns, p.bkt_per_col, p.sketch_bytes
     t_ing = statistics.mean(ingest_ms) / 1e3
@@ -220,7 +220,7 @@ def roofline(alg, n, prof, steps, ingest_ms, hash_peak, hbm_peak_gbs, update_pea
     t_g = prof["gutter_ms"] / max(1, prof["gutter_launches"]) / 1e3
     t_u = prof["sketch_update_ms"] / max(1, prof["sketch_update_launches"]) / 1e3
     if p.entry_form == 2:
-        coded = min(C, 16)  # columns hashed once per record in the gutter pass (kCodedColumns)
+        coded = C  # every column hashed once per record in the gutter pass
         g_bytes = 9 * n + 9 * n + 2 * n * 16
         kernels["gutter"] = {
             "kernels": "k_gutter (count) + k_hash_sort_scatter", "launch_ms": t_g * 1e3,
@@ -232,7 +232,7 @@ def roofline(alg, n, prof, steps, ingest_ms, hash_peak, hbm_peak_gbs, update_pea
         rows = min(B, 11)
         u_bytes = 2 * n * 16 + 2 * V * 12 * (C * rows + 1)
         slots = 2 * n * 32
-        u_hashes = 2 * n * (C - coded + 1)
+        u_hashes = 2 * n  # the checksum, per endpoint
         kernels["sketch_update"] = {
             "kernels": "k_plane_update", "launch_ms": t_u * 1e3, "bound": "smem",
             "bucket_updates_per_launch": 2 * n * (C + 1), "slot_steps_per_launch": slots,

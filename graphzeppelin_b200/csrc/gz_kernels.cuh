@@ -131,6 +131,8 @@ uint32_t hash_sort_tile(uint32_t nbins, size_t smem_budget);
 cudaError_t gutter_hash_sort(const void *d_rec, uint64_t n, GutterGeom g, const PlaneHash &ph,
                              uint32_t rec_tile, const uint64_t *base, uint32_t *fill,
                              uint4 *entries, cudaStream_t s);
+// Threads per CTA of the hash sort-scatter (1024: one CTA per SM; 512: two), process-wide.
+void set_hash_sort_threads(int threads);
 // Applies every buffered chunk (coded or plain entries) tile by tile through bucket planes.
 size_t plane_update_smem(uint32_t tile_shift, int threads);
 int plane_update_ctas_per_sm(uint32_t tile_shift, int threads);

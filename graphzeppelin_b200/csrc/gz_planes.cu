@@ -106,8 +106,36 @@ __device__ __forceinline__ void unpack_entry(uint4 e, uint32_t bin, uint32_t C, 
 // per bin, reserve one run per non-empty bin in the gutter (one global atomic each), hash every
 // record's C columns once, place both entries (and their bins) in bin order in shared memory,
 // and write the runs out.
-template <int RPT>
-__global__ void __launch_bounds__(1024, 1)
+// Exclusive scan over the threads of a block of NT threads (a multiple of 32, <= 1024).
+template <int NT>
+__device__ __forceinline__ uint32_t block_scan(uint32_t x, uint32_t *ws /*32*/) {
+  if (NT == 1024) return block_scan_1024(x, ws);
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t inc = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(kFull, inc, o);
+    if (lane >= (uint32_t)o) inc += y;
+  }
+  if (lane == 31) ws[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = lane < NT / 32 ? ws[lane] : 0u;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(kFull, w, o);
+      if (lane >= (uint32_t)o) w += y;
+    }
+    ws[lane] = w;
+  }
+  __syncthreads();
+  const uint32_t r = (warp ? ws[warp - 1] : 0u) + inc - x;
+  __syncthreads();
+  return r;
+}
+
+template <int RPT, int NT>
+__global__ void __launch_bounds__(NT, 1024 / NT)
 k_hash_sort_scatter(const uint8_t *__restrict__ rec, uint64_t n, GutterGeom g, PlaneHash ph,
                     uint32_t rec_tile, const uint64_t *__restrict__ base,
                     uint32_t *__restrict__ fill, uint4 *__restrict__ entries) {
@@ -121,7 +149,7 @@ k_hash_sort_scatter(const uint8_t *__restrict__ rec, uint64_t n, GutterGeom g, P
   // the staged records share the entry area: they are parsed into registers before the first
   // entry is placed, and the next tile is staged only after the write-out
   uint8_t *s_rec = reinterpret_cast<uint8_t *>(s_ent);
-  const uint32_t per_thread = (nb + blockDim.x - 1) / blockDim.x;  // bins per thread (<= 8)
+  const uint32_t per_thread = (nb + NT - 1) / NT;  // bins per thread
   const uint32_t cap = 1u << min(ph.B, kDepthEscape);
   for (uint64_t t0 = blockIdx.x * (uint64_t)rec_tile; t0 < n; t0 += (uint64_t)gridDim.x * rec_tile) {
     const uint32_t cnt = (uint32_t)(n - t0 < rec_tile ? n - t0 : rec_tile);
@@ -153,7 +181,7 @@ k_hash_sort_scatter(const uint8_t *__restrict__ rec, uint64_t n, GutterGeom g, P
       const uint32_t b = threadIdx.x * per_thread + k;
       sum += b < nb ? s_cur[b] : 0u;
     }
-    uint32_t run = block_scan_1024(sum, ws);
+    uint32_t run = block_scan<NT>(sum, ws);
     for (uint32_t k = 0; k < per_thread; ++k) {
       const uint32_t b = threadIdx.x * per_thread + k;
       if (b < nb) {
@@ -629,39 +657,62 @@ PlaneHash plane_hash(uint64_t seed, uint32_t C, uint32_t B) {
 }
 
 constexpr int kHashSortMaxRpt = 6;
+// Threads per CTA of the hash sort-scatter: one CTA of 1024 per SM, or two of 512 (each with half
+// the shared memory), whose phases then overlap.
+int g_hash_sort_threads = 1024;
 
 uint32_t hash_sort_tile(uint32_t nbins, size_t smem_budget) {
+  const int nt = g_hash_sort_threads;
+  const size_t budget = nt == 1024 ? smem_budget : std::min<size_t>(smem_budget, (228 * 1024 - 2 * 1024) / 2);
   const size_t fixed = (size_t)2 * ((nbins + 3) & ~3u) * 4 + 256;
-  if (nbins > kSortBinsMax || fixed >= smem_budget) return 0;
+  if (nbins > kSortBinsMax || fixed >= budget) return 0;
   // 2 coded entries of 16 B per record, and their 2-byte bins
-  const size_t t = std::min<size_t>((smem_budget - fixed) / 36, kHashSortMaxRpt * 1024);
-  return (uint32_t)(t / 1024 * 1024);
+  const size_t t = std::min<size_t>((budget - fixed) / 36, (size_t)kHashSortMaxRpt * nt);
+  return (uint32_t)(t / nt * nt);
 }
 
 cudaError_t gutter_hash_sort(const void *d_rec, uint64_t n, GutterGeom g, const PlaneHash &ph,
                              uint32_t rec_tile, const uint64_t *base, uint32_t *fill,
                              uint4 *entries, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
-  if (rec_tile < 1024 || rec_tile > kHashSortMaxRpt * 1024 || rec_tile % 1024) return cudaErrorInvalidValue;
+  const int nt = g_hash_sort_threads;
+  if (rec_tile < (uint32_t)nt || rec_tile > (uint32_t)(kHashSortMaxRpt * nt) || rec_tile % nt)
+    return cudaErrorInvalidValue;
   const size_t smem = (size_t)2 * ((g.nbins + 3) & ~3u) * 4 + (size_t)rec_tile * 36;
-  const int G = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)num_sms(), (n + rec_tile - 1) / rec_tile));
+  const uint64_t tiles = (n + rec_tile - 1) / rec_tile;
   const uint8_t *rec = reinterpret_cast<const uint8_t *>(d_rec);
-  auto launch = [&](auto kern) -> cudaError_t {
+  auto launch = [&](auto kern, int threads) -> cudaError_t {
     cudaError_t e = smem_optin(kern);
     if (e != cudaSuccess) return e;
-    kern<<<G, 1024, smem, s>>>(rec, n, g, ph, rec_tile, base, fill, entries);
+    int per_sm = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess || per_sm < 1)
+      per_sm = 1;
+    const int G = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)num_sms() * per_sm, tiles));
+    kern<<<G, threads, smem, s>>>(rec, n, g, ph, rec_tile, base, fill, entries);
     add_launches(1);
     return cudaGetLastError();
   };
+  if (nt == 512) {
+    switch (rec_tile / 512) {
+      case 1: return launch(k_hash_sort_scatter<1, 512>, 512);
+      case 2: return launch(k_hash_sort_scatter<2, 512>, 512);
+      case 3: return launch(k_hash_sort_scatter<3, 512>, 512);
+      case 4: return launch(k_hash_sort_scatter<4, 512>, 512);
+      case 5: return launch(k_hash_sort_scatter<5, 512>, 512);
+      default: return launch(k_hash_sort_scatter<6, 512>, 512);
+    }
+  }
   switch (rec_tile / 1024) {
-    case 1: return launch(k_hash_sort_scatter<1>);
-    case 2: return launch(k_hash_sort_scatter<2>);
-    case 3: return launch(k_hash_sort_scatter<3>);
-    case 4: return launch(k_hash_sort_scatter<4>);
-    case 5: return launch(k_hash_sort_scatter<5>);
-    default: return launch(k_hash_sort_scatter<6>);
+    case 1: return launch(k_hash_sort_scatter<1, 1024>, 1024);
+    case 2: return launch(k_hash_sort_scatter<2, 1024>, 1024);
+    case 3: return launch(k_hash_sort_scatter<3, 1024>, 1024);
+    case 4: return launch(k_hash_sort_scatter<4, 1024>, 1024);
+    case 5: return launch(k_hash_sort_scatter<5, 1024>, 1024);
+    default: return launch(k_hash_sort_scatter<6, 1024>, 1024);
   }
 }
+
+void set_hash_sort_threads(int threads) { g_hash_sort_threads = threads == 512 ? 512 : 1024; }
 
 size_t plane_update_smem(uint32_t tile_shift, int threads) {
   return 128 + ((size_t)kVertBytes << tile_shift) + (size_t)(threads / 32) * kWbWords * 4;

@@ -32,8 +32,8 @@ def test_roofline_arithmetic():
     assert abs(r["frac"] - (hashes / 1358e9) / 6e-3) < 1e-12
     assert abs(r["terms_ms"]["int"] - hashes / 1358e9 * 1e3) < 1e-9
     g, u = r["kernels"]["gutter"], r["kernels"]["sketch_update"]
-    assert g["hashes_per_launch"] == n * 16 and abs(g["launch_ms"] - 3.0) < 1e-12
-    assert u["hashes_per_launch"] == 2 * n * 9
+    assert g["hashes_per_launch"] == n * 24 and abs(g["launch_ms"] - 3.0) < 1e-12
+    assert u["hashes_per_launch"] == 2 * n
     assert u["slot_steps_per_launch"] == 2 * n * 32
     assert u["bucket_updates_per_launch"] == 2 * n * 25
     assert abs(u["smem"]["frac"] - (2 * n * 32 / 2.5e-3) / 3667e9) < 1e-12
