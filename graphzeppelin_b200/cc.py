@@ -497,10 +497,11 @@ class CCSketchAlg:
         _check(self.lib.gz_get_params(self._h, ctypes.byref(p)))
         self.params = p
 
-    def set_query_graph(self, enable: bool = True) -> None:
-        """Queries as one CUDA graph (default) or with the round loop on the host
-        (gz_set_query_graph; for profilers)."""
-        _check(self.lib.gz_set_query_graph(self._h, int(enable)))
+    def set_query_graph(self, mode=2) -> None:
+        """How queries run (gz_set_query_graph): 2 one cooperative kernel (the default), 1 (or
+        True) a CUDA graph of per-phase kernels, 0 (or False) those kernels with the round loop
+        on the host (for profilers)."""
+        _check(self.lib.gz_set_query_graph(self._h, int(mode)))
 
     def set_gutter_capacity(self, endpoint_updates: int) -> None:
         _check(self.lib.gz_set_gutter_capacity(self._h, endpoint_updates))

@@ -180,10 +180,11 @@ struct gz_alg {
   bool eager = false, host_answer = false, boruvka_ran = false;
   std::vector<uint32_t> hdsu;
   std::unordered_set<uint64_t> hforest;
-  // the query graph of blocking queries (device-driven Boruvka rounds); query_graph = 0 runs
-  // the same kernels with the round loop on the host
+  // how a query runs: 2 = one cooperative kernel (every round on the device), 1 = a CUDA graph of
+  // the per-phase kernels with a conditional while node over the rounds (qgraph), 0 = the same
+  // kernels with the round loop on the host
   gz::BoruvkaGraph qgraph;
-  bool query_graph = true;
+  int query_mode = 2;
   uint32_t *h_qpin = nullptr;  // pinned: rounds, out-of-samples flag, components
   // queries by ticket (gz_query_submit / gz_query_wait): the query graph enqueued on the
   // handle's stream behind every update submitted before it, with its own buffers, so the
@@ -574,6 +575,10 @@ void destroy_alg(gz_alg *h) {
   dev_free(b.round);
   b.ctl = nullptr;
   dev_free(b.flags);
+  dev_free(b.cross);
+  dev_free(b.ncross);
+  dev_free(b.qbar);
+  dev_free(b.btot);
   dev_free(b.forest);
   dev_free(b.forest_n);
   if (b.trace) cudaFree(b.trace);
@@ -854,6 +859,10 @@ int alloc_bv(gz::BoruvkaBufs &b, size_t V, size_t acc_words, uint32_t *status) {
   GZ_TRY(dev_alloc(&b.round, 4));
   b.ctl = b.round + 1;
   GZ_TRY(dev_alloc(&b.flags, 4));
+  GZ_TRY(dev_alloc(&b.cross, warps + 1));
+  GZ_TRY(dev_alloc(&b.ncross, 1));
+  GZ_TRY(dev_alloc(&b.qbar, 1));
+  GZ_TRY(dev_alloc(&b.btot, gz::kBvQueryMaxBlocks));
   GZ_TRY(dev_alloc(&b.forest, V));
   GZ_TRY(dev_alloc(&b.forest_n, 1));
   GZ_TRY(dev_alloc(&b.trace_n, 1));
@@ -882,6 +891,10 @@ void free_bv(gz::BoruvkaBufs &b) {
   dev_free(b.round);
   b.ctl = nullptr;
   dev_free(b.flags);
+  dev_free(b.cross);
+  dev_free(b.ncross);
+  dev_free(b.qbar);
+  dev_free(b.btot);
   dev_free(b.forest);
   dev_free(b.forest_n);
   dev_free(b.trace_n);
@@ -893,7 +906,8 @@ void free_bv(gz::BoruvkaBufs &b) {
 int boruvka_enqueue(gz_alg *h, gz::BoruvkaGraph &q, const gz::BoruvkaGeom &g, const uint8_t *sk,
                     gz::BoruvkaBufs &b, uint32_t *d_final, uint32_t *d_ncc, uint32_t *pin,
                     cudaStream_t s) {
-  if (h->query_graph) GZ_CUDA(gz::boruvka_graph_launch(q, g, h->samples, sk, b, d_final, d_ncc, s));
+  if (h->query_mode == 2) GZ_CUDA(gz::boruvka_query_launch(g, h->samples, sk, b, d_final, d_ncc, s));
+  else if (h->query_mode == 1) GZ_CUDA(gz::boruvka_graph_launch(q, g, h->samples, sk, b, d_final, d_ncc, s));
   else GZ_CUDA(gz::boruvka_host_loop(g, h->samples, sk, b, d_final, d_ncc, pin, s));
   GZ_CUDA(cudaMemcpyAsync(pin, b.ctl, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   GZ_CUDA(cudaMemcpyAsync(pin + 2, d_ncc, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
@@ -974,7 +988,7 @@ int run_boruvka(gz_alg *h) {
                          h->stream));
   h->prof_end(pi, 2);
   GZ_CUDA(cudaStreamSynchronize(h->stream));
-  boruvka_account(h->qgraph, h->h_qpin, h->query_graph);
+  boruvka_account(h->qgraph, h->h_qpin, h->query_mode == 1);
   const uint32_t round = h->h_qpin[0];
   if (h->h_qpin[1]) {
     h->last_rounds = round;
@@ -1393,7 +1407,7 @@ int gz_query_submit(gz_alg_t *h, uint64_t *ticket) {
     }
   }
   const int pi = h->prof_begin();
-  t.graph = h->query_graph;
+  t.graph = h->query_mode == 1;
   int rc = boruvka_enqueue(h, T.graph, h->bgeom(), h->d_sk, T.bv, T.d_final, T.d_ncc, t.pin, h->stream);
   h->prof_end(pi, 2);
   cudaError_t e = cudaSuccess;
@@ -1571,7 +1585,8 @@ int gz_set_pipeline(gz_alg_t *h, int mode) {
 int gz_set_query_graph(gz_alg_t *h, int enable) {
   if (!h) return fail(GZ_ERR_INVALID, "null handle");
   Guard g(h);
-  h->query_graph = enable != 0;
+  if (enable < 0 || enable > 2) return fail(GZ_ERR_INVALID, "query mode is 0, 1 or 2");
+  h->query_mode = enable;
   return GZ_OK;
 }
 

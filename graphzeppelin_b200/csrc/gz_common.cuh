@@ -50,6 +50,18 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
+// try_wait that may suspend the thread for up to hint_ns until the phase completes.
+__device__ __forceinline__ bool mbar_try_wait_hint(uint32_t bar, uint32_t parity, uint32_t hint_ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity), "r"(hint_ns)
+      : "memory");
+  return ok != 0;
+}
 __device__ __forceinline__ uint64_t global_ns() {
   uint64_t t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -314,17 +326,18 @@ struct Region {
   static constexpr int kNW = (3 * CPS * 64 + 31) / 32;  // word slots per lane (B <= 64)
 };
 
-// Load region words [0, W) at src and the deterministic bucket at det into x / dw.
-template <int NW>
+// Load region words [0, W) at src and the deterministic bucket at det into x / dw (CG: through
+// L2 only, for words written earlier in the same kernel by another SM).
+template <int NW, bool CG = false>
 __device__ __forceinline__ void region_load(const uint32_t *__restrict__ src,
                                             const uint32_t *__restrict__ det, uint32_t W,
                                             uint32_t lane, uint32_t (&x)[NW], uint32_t &dw) {
 #pragma unroll
   for (int k = 0; k < NW; ++k) {
     const uint32_t w = k * 32 + lane;
-    x[k] = w < W ? src[w] : 0u;
+    x[k] = w < W ? (CG ? __ldcg(src + w) : src[w]) : 0u;
   }
-  dw = lane < 3 ? det[lane] : 0u;
+  dw = lane < 3 ? (CG ? __ldcg(det + lane) : det[lane]) : 0u;
 }
 
 // Sketch::sample (src/sketch.cpp:94-116) of a region in shared memory: s[0, 3 * CPS * B) the
@@ -400,41 +413,43 @@ __device__ __forceinline__ const uint32_t *bulk_run_at(const uint8_t *slot, cons
   return reinterpret_cast<const uint32_t *>(slot + ((uintptr_t)p & 15));
 }
 
-// Shared memory of the query kernels' bulk-copy rings, per warp: two batches of KB member slots
+// Shared memory of the query kernels' bulk-copy rings, per warp: NS batches of KB member slots
 // (a slot holds the 16-byte-aligned supersets of a member's column run, up to Wmax words, and of
 // its deterministic bucket), one stage of Wmax + 3 words, and one mbarrier per batch.
 __host__ __device__ constexpr uint32_t bv_slot_bytes(uint32_t Wmax) { return bulk_run_cap(Wmax) + bulk_run_cap(3); }
-__host__ __device__ constexpr uint32_t bv_warp_bytes(uint32_t Wmax, int KB) {
-  return 2 * KB * bv_slot_bytes(Wmax) + (((Wmax + 3) * 4 + 15) & ~15u) + 16;
+__host__ __device__ constexpr uint32_t bv_warp_bytes(uint32_t Wmax, int KB, int NS = 2) {
+  return NS * KB * bv_slot_bytes(Wmax) + (((Wmax + 3) * 4 + 15) & ~15u) + ((8 * NS + 15) & ~15u);
 }
 
-// A warp's two batch buffers: init of their mbarriers (one arrival: lane 0's expect_tx), issue of
-// a batch's bulk copies, and the bounded wait for a batch.
-struct BvRing {
-  uint8_t *slots;   // 2 * KB slots
+// A warp's NS batch buffers: init of their mbarriers (one arrival: lane 0's expect_tx), issue of
+// a batch's bulk copies, and the bounded wait for a batch. Batch t uses buffer t % NS; its
+// barrier completes its (t / NS)-th phase.
+template <int NS>
+struct BvRingN {
+  uint8_t *slots;   // NS * KB slots
   uint32_t *stage;  // Wmax + 3 words
-  uint64_t *bars;   // 2
+  uint64_t *bars;   // NS
   uint32_t slot_bytes, run_cap;
   __device__ void init(uint8_t *warp_smem, uint32_t Wmax, int KB) {
     run_cap = bulk_run_cap(Wmax);
     slot_bytes = bv_slot_bytes(Wmax);
     slots = warp_smem;
-    stage = reinterpret_cast<uint32_t *>(warp_smem + 2 * KB * slot_bytes);
-    bars = reinterpret_cast<uint64_t *>(warp_smem + 2 * KB * slot_bytes + (((Wmax + 3) * 4 + 15) & ~15u));
+    stage = reinterpret_cast<uint32_t *>(warp_smem + NS * KB * slot_bytes);
+    bars = reinterpret_cast<uint64_t *>(warp_smem + NS * KB * slot_bytes + (((Wmax + 3) * 4 + 15) & ~15u));
     if ((threadIdx.x & 31) == 0) {
-      mbar_init(smem_u32(&bars[0]), 1);
-      mbar_init(smem_u32(&bars[1]), 1);
+#pragma unroll
+      for (int i = 0; i < NS; ++i) mbar_init(smem_u32(&bars[i]), 1);
       mbar_fence_init();
     }
     __syncwarp();
   }
-  __device__ uint8_t *slot(uint32_t t, uint32_t k, int KB) const { return slots + ((t & 1) * KB + k) * slot_bytes; }
+  __device__ uint8_t *slot(uint32_t t, uint32_t k, int KB) const { return slots + ((t % NS) * KB + k) * slot_bytes; }
   // Lane k < KB with `mine` copies its run [run, run + words) (words <= Wmax) and its
   // deterministic bucket det into slot k of batch t; lane 0 arms the batch's barrier with the
   // bytes of the whole batch first. Every lane of the warp calls it.
   __device__ void issue(uint32_t t, bool mine, const uint32_t *run, uint32_t words, const uint32_t *det, int KB) {
     const uint32_t lane = threadIdx.x & 31;
-    const uint32_t bar = smem_u32(&bars[t & 1]);
+    const uint32_t bar = smem_u32(&bars[t % NS]);
     const uint32_t bytes = mine ? bulk_run_bytes(run, words) + bulk_run_bytes(det, 3) : 0;
     const uint32_t total = __reduce_add_sync(kFull, bytes);
     // this lane's reads of the slots about to be overwritten, before the async proxy writes
@@ -451,11 +466,19 @@ struct BvRing {
       bulk_run_copy(sl + run_cap, det, 3, bar);
     }
   }
+  // The thread sleeps in the barrier (20 us per try) instead of spinning; limit_ns bounds the wait.
   __device__ bool wait(uint32_t t) const {
-    const bool ok = mbar_wait_bounded(smem_u32(&bars[t & 1]), (t >> 1) & 1, kWaitLimitNs);
+    const uint32_t bar = smem_u32(&bars[t % NS]), parity = (t / NS) & 1;
+    bool ok = mbar_try_wait_hint(bar, parity, 20000);
+    if (!ok) {
+      const uint64_t t0 = global_ns();
+      while (!(ok = mbar_try_wait_hint(bar, parity, 20000)) && global_ns() - t0 < kWaitLimitNs) {
+      }
+    }
     return __all_sync(kFull, ok);
   }
 };
+using BvRing = BvRingN<2>;
 
 // Warp-aggregated counter add: lanes in `active` holding the same key add one each to ctr[key]
 // with one atomic per distinct key; returns this lane's slot (old value + rank among its key's

@@ -629,9 +629,9 @@ __global__ void k_sketch_xor_raw(uint32_t *sketches, uint32_t words, uint32_t v,
 // Boruvka
 // ------------------------------------------------------------------------------------------------
 // sample_supernode (src/cc_sketch_alg.cpp:137-166): FAIL marks the round modified, GOOD unions
-// the sampled edge and marks modified if the partition changed.
+// the sampled edge and marks modified if the partition changed. flags = the round's modified word.
 __device__ void handle_result(int res, uint64_t idx, uint32_t round, uint32_t key,
-                              const BoruvkaGeom &g, const BoruvkaBufs &b) {
+                              const BoruvkaGeom &g, const BoruvkaBufs &b, uint32_t *flags) {
   if (b.trace) {
     const uint32_t ti = atomicAdd(b.trace_n, 1u);
     if (ti < b.trace_cap) {
@@ -645,7 +645,7 @@ __device__ void handle_result(int res, uint64_t idx, uint32_t round, uint32_t ke
     }
   }
   if (res == 2) {
-    atomicOr(b.flags, 1u);
+    atomicOr(flags, 1u);
   } else if (res == 0) {
     const uint32_t x = (uint32_t)(idx >> 32), y = (uint32_t)idx;
     if (x >= g.V || y >= g.V) {
@@ -653,7 +653,7 @@ __device__ void handle_result(int res, uint64_t idx, uint32_t round, uint32_t ke
       return;
     }
     if (dsu_unite(b.parent, x, y)) {
-      atomicOr(b.flags, 1u);
+      atomicOr(flags, 1u);
       const uint32_t fi = atomicAdd(b.forest_n, 1u);
       if (fi < g.V) b.forest[fi] = idx;
     }
@@ -665,23 +665,27 @@ __global__ void k_bv_reset(uint32_t V, uint32_t *parent) {
   if (v < V) parent[v] = v;
 }
 
-// Round 0 (run_round_zero, src/cc_sketch_alg.cpp:223-244): every vertex sketch samples its
-// sample 0 -- columns 0..CPS-1 and the deterministic bucket. A warp takes 32 consecutive
-// vertices at a time, in batches of KB whose runs are bulk-copied to shared memory one batch
-// ahead (also across its 32-vertex groups), and samples each vertex from there; lane i keeps
-// vertex i's result, and the 32 results are applied by the 32 lanes at once.
-template <int CPS, int KB>
-__global__ void __launch_bounds__(256) k_bv_round0(BoruvkaGeom g, const uint32_t *__restrict__ sk_words,
-                                                   BoruvkaBufs b) {
-  extern __shared__ __align__(16) uint8_t bv_smem[];
+// The Boruvka phases below are device functions shared by the per-phase kernels (one launch
+// each, the CUDA-graph and host-loop queries) and by k_bv_query (every phase of every round in
+// one cooperative launch). Data written earlier in the same query is read through L2 (__ldcg):
+// in k_bv_query another SM wrote it in an earlier phase of the same kernel. A warp's copy ring
+// counts its batches in T across calls, so its two mbarriers' phases stay in step.
+
+// Round 0 (run_round_zero, src/cc_sketch_alg.cpp:223-244) for warp gw of nwarps: every vertex
+// sketch samples its sample 0 -- columns 0..CPS-1 and the deterministic bucket. The warp takes
+// 32 consecutive vertices at a time, in batches of KB whose runs are bulk-copied to shared memory
+// one batch ahead (also across its 32-vertex groups), and samples each vertex from there; lane i
+// keeps vertex i's result, and the 32 results are applied by the 32 lanes at once. False when a
+// copy did not land in time (status set).
+template <int CPS, int KB, int NS>
+__device__ bool bv_round0_warp(const BoruvkaGeom &g, const uint32_t *__restrict__ sk_words,
+                               const BoruvkaBufs &b, uint32_t *flags, BvRingN<NS> &ring, uint32_t &T,
+                               uint32_t gw, uint32_t nwarps) {
   constexpr uint32_t BPG = 32 / KB;  // batches per 32-vertex group
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t W = 3 * CPS * g.B, detw = 3 * g.C * g.B;
-  BvRing ring;
-  ring.init(bv_smem + (threadIdx.x >> 5) * bv_warp_bytes(W, KB), W, KB);
-  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t ngroups = (g.V + 31) / 32;
+  if (gw >= ngroups) return true;
   auto first_vertex = [&](uint32_t t) {  // first vertex of batch t, or ~0 past the work
     const uint32_t grp = gw + (t / BPG) * nwarps;
     return grp < ngroups ? grp * 32 + (t % BPG) * KB : 0xffffffffu;
@@ -690,26 +694,27 @@ __global__ void __launch_bounds__(256) k_bv_round0(BoruvkaGeom g, const uint32_t
     const uint32_t v0 = first_vertex(t);
     const bool mine = v0 != 0xffffffffu && lane < (uint32_t)KB && v0 + lane < g.V;
     const uint32_t *sk = sk_words + (uint64_t)(mine ? v0 + lane : 0) * g.sketch_words;
-    ring.issue(t, mine, sk, W, sk + detw, KB);
+    ring.issue(T + t, mine, sk, W, sk + detw, KB);
   };
-  if (gw >= ngroups) return;
   int my_res = 1;
   uint64_t my_idx = 0;
-  issue(0);
-  for (uint32_t t = 0;; ++t) {
+  for (uint32_t a = 0; a + 1 < (uint32_t)NS; ++a) issue(a);
+  uint32_t t = 0;
+  for (;; ++t) {
     const uint32_t v0 = first_vertex(t);
     if (v0 == 0xffffffffu) break;
-    issue(t + 1);
-    if (!ring.wait(t)) {
+    issue(t + NS - 1);
+    if (!ring.wait(T + t)) {
       if (lane == 0) atomicOr(b.status, kStatusTimeout);
-      ring.wait(t + 1);  // its copies must land before the block's shared memory goes away
-      return;
+      // their copies must land before the shared memory is reused or freed
+      for (uint32_t a = 1; a < (uint32_t)NS; ++a) ring.wait(T + t + a);
+      return false;
     }
 #pragma unroll 1
     for (int k = 0; k < KB; ++k)
       if (v0 + k < g.V) {
         const uint32_t *sk = sk_words + (uint64_t)(v0 + k) * g.sketch_words;
-        const uint8_t *sl = ring.slot(t, k, KB);
+        const uint8_t *sl = ring.slot(T + t, k, KB);
         const uint32_t *run = bulk_run_at(sl, sk), *det = bulk_run_at(sl + ring.run_cap, sk + detw);
         uint64_t idx;
         const int res = warp_sample_smem_split<CPS>(run, det, g.B, g.flip_chk, &idx);
@@ -721,51 +726,116 @@ __global__ void __launch_bounds__(256) k_bv_round0(BoruvkaGeom g, const uint32_t
     __syncwarp();
     if (t % BPG == BPG - 1) {  // end of a 32-vertex group: its results, one lane each
       const uint32_t base = v0 - (t % BPG) * KB;
-      if (base + lane < g.V) handle_result(my_res, my_idx, 0, base + lane, g, b);
+      if (base + lane < g.V) handle_result(my_res, my_idx, 0, base + lane, g, b, flags);
       __syncwarp();
       my_res = 1;
       my_idx = 0;
     }
   }
-  // the batch issued last covered no vertex (nothing in flight)
+  // batches 0 .. t + NS - 2 were issued; those from t on covered no vertex (nothing in flight)
+  T += t + NS - 1;
+  return true;
 }
 
-// Root of every vertex and members per root; lanes of a warp that share a root add to its
-// counter with one atomic (a giant component would otherwise serialise V atomics on one word).
-// minv (trace keys) gets the smallest member: lanes hold consecutive vertices, so the lowest
-// lane of each root group.
+template <int CPS, int KB>
+__global__ void __launch_bounds__(256) k_bv_round0(BoruvkaGeom g, const uint32_t *__restrict__ sk_words,
+                                                   BoruvkaBufs b) {
+  extern __shared__ __align__(16) uint8_t bv_smem[];
+  const uint32_t W = 3 * CPS * g.B;
+  BvRing ring;
+  ring.init(bv_smem + (threadIdx.x >> 5) * bv_warp_bytes(W, KB), W, KB);
+  uint32_t T = 0;
+  bv_round0_warp<CPS, KB, 2>(g, sk_words, b, b.flags, ring, T,
+                          (blockIdx.x * blockDim.x + threadIdx.x) >> 5,
+                          (gridDim.x * blockDim.x) >> 5);
+}
+
+// Per-block table of the distinct roots among a block's vertices (at most 512 of them in 1024
+// slots, open addressing): the block's members per root are counted in shared memory, so a root
+// shared by many vertices (late rounds: a few large components) gets one global atomic per block
+// instead of one per warp.
+constexpr uint32_t kRootSlots = 1024;
+struct RootTable {
+  uint32_t key[kRootSlots], cnt[kRootSlots], aux[kRootSlots];
+};
+__device__ __forceinline__ void root_table_clear(RootTable &t, uint32_t aux0) {
+  for (uint32_t e = threadIdx.x; e < kRootSlots; e += blockDim.x) {
+    t.key[e] = 0xffffffffu;
+    t.cnt[e] = 0;
+    t.aux[e] = aux0;
+  }
+}
+// Slot of root r (inserted if new); the table has room for every distinct root of a block.
+__device__ __forceinline__ uint32_t root_slot(RootTable &t, uint32_t r) {
+  uint32_t h = (r * 0x9E3779B1u) >> 22;
+  for (uint32_t i = 0; i < kRootSlots; ++i, h = (h + 1) & (kRootSlots - 1)) {
+    const uint32_t k = atomicCAS(&t.key[h], 0xffffffffu, r);
+    if (k == 0xffffffffu || k == r) break;
+  }
+  return h;
+}
+
+// Root of every vertex of [v0, v0 + VPT * blockDim.x) (thread t: vertices v0 + k * blockDim.x + t)
+// and members per root (cnt) and smallest member per root (minv, for trace keys). The VPT parent
+// chains of a thread are followed together, one hop per pass with all VPT loads in flight (no
+// union runs during the labelling), then each vertex's parent is set to its root: later rounds
+// find it in a hop or two. VPT * blockDim.x <= 512. Every thread of the block calls it.
+template <int VPT>
+__device__ __forceinline__ void bv_label_block(uint32_t V, uint32_t v0, uint32_t *parent,
+                                               uint32_t *label, uint32_t *cnt, uint32_t *minv,
+                                               RootTable &tab) {
+  uint32_t r[VPT], p1[VPT];
+  bool in[VPT];
+  root_table_clear(tab, 0xffffffffu);
+#pragma unroll
+  for (int k = 0; k < VPT; ++k) {
+    const uint32_t v = v0 + k * blockDim.x + threadIdx.x;
+    in[k] = v < V;
+    r[k] = in[k] ? v : 0u;
+    p1[k] = in[k] ? __ldcg(parent + v) : 0u;
+  }
+  // x[k] = parent of r[k]; r[k] is the root once they are equal
+  uint32_t x[VPT];
+#pragma unroll
+  for (int k = 0; k < VPT; ++k) x[k] = in[k] ? p1[k] : r[k];
+  for (;;) {
+    bool more = false;
+#pragma unroll
+    for (int k = 0; k < VPT; ++k) more = more || x[k] != r[k];
+    if (!more) break;
+#pragma unroll
+    for (int k = 0; k < VPT; ++k)
+      if (x[k] != r[k]) {
+        r[k] = x[k];
+        x[k] = __ldcg(parent + x[k]);
+      }
+  }
+  __syncthreads();  // the table is clear
+#pragma unroll
+  for (int k = 0; k < VPT; ++k)
+    if (in[k]) {
+      const uint32_t v = v0 + k * blockDim.x + threadIdx.x;
+      label[v] = r[k];
+      if (p1[k] != r[k]) __stcg(parent + v, r[k]);
+      const uint32_t h = root_slot(tab, r[k]);
+      atomicAdd(&tab.cnt[h], 1u);
+      if (minv) atomicMin(&tab.aux[h], v);
+    }
+  __syncthreads();
+  for (uint32_t e = threadIdx.x; e < kRootSlots; e += blockDim.x) {
+    const uint32_t key = tab.key[e];
+    if (key != 0xffffffffu) {
+      atomicAdd(&cnt[key], tab.cnt[e]);
+      if (minv) atomicMin(&minv[key], tab.aux[e]);
+    }
+  }
+  __syncthreads();  // the table's next user clears it
+}
+
 __global__ void __launch_bounds__(256) k_bv_label(uint32_t V, uint32_t *parent, uint32_t *label,
                                                   uint32_t *cnt, uint32_t *minv) {
-  __shared__ uint32_t s_r0;
-  const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool in = v < V;
-  uint32_t r = 0;
-  if (in) {
-    r = dsu_find(parent, v);
-    label[v] = r;
-    // full path compression: no union runs during the labelling, and a root is as valid an
-    // ancestor as any, so later rounds find this vertex's root in a hop or two
-    if (__ldcg(parent + v) != r) __stcg(parent + v, r);
-  }
-  if (threadIdx.x == 0) s_r0 = r;
-  __syncthreads();
-  // a block whose vertices all have one root (a giant component) adds to its counter once
-  if (__syncthreads_and(!in || r == s_r0)) {
-    if (threadIdx.x == 0) {
-      const uint32_t nin = V - blockIdx.x * blockDim.x < blockDim.x ? V - blockIdx.x * blockDim.x : blockDim.x;
-      atomicAdd(&cnt[r], nin);
-      if (minv) atomicMin(&minv[r], v);
-    }
-    return;
-  }
-  const uint32_t active = __ballot_sync(kFull, in);
-  if (!in) return;
-  const uint32_t lane = threadIdx.x & 31;
-  const uint32_t peers = __match_any_sync(active, r);
-  if (lane == __ffs(peers) - 1) {
-    atomicAdd(&cnt[r], (uint32_t)__popc(peers));
-    if (minv) atomicMin(&minv[r], v);
-  }
+  __shared__ RootTable tab;
+  bv_label_block<1>(V, blockIdx.x * blockDim.x, parent, label, cnt, minv, tab);
 }
 
 // Per-round counters: members and scatter cursors per root, smallest member (traces), and no
@@ -776,7 +846,10 @@ __global__ void k_bv_prep(uint32_t V, BoruvkaBufs b) {
   b.cnt[v] = 0;
   b.fill[v] = 0;
   if (b.trace) b.minv[v] = 0xffffffffu;
-  if (v == 0) *b.big = 0xffffffffu;
+  if (v == 0) {
+    *b.big = 0xffffffffu;
+    *b.ncross = 0;
+  }
 }
 
 __global__ void k_bv_pack(uint32_t V, const uint32_t *cnt, uint64_t *packed) {
@@ -786,97 +859,128 @@ __global__ void k_bv_pack(uint32_t V, const uint32_t *cnt, uint64_t *packed) {
   packed[v] = (uint64_t)c | (c ? (1ull << 32) : 0ull);
 }
 
-// create_merge_instructions (src/cc_sketch_alg.cpp:382-462): group vertices by root so each
-// component's members are contiguous in `order` (slots taken with warp-aggregated atomics).
+// create_merge_instructions (src/cc_sketch_alg.cpp:382-462) for the vertices [v0, v0 + VPT *
+// blockDim.x) (thread t: vertices v0 + k * blockDim.x + t): group vertices by root so each
+// component's members are contiguous in `order` (slots taken with warp-aggregated atomics, or one
+// claim when the block's vertices share one root). packed_at(r) = the exclusive scan over the
+// roots below r of (members | 1 << 32): root r's first grouped position and its component index;
+// nc = the number of components. Components crossing a span edge get their acc slot cleared and
+// are listed in cross. Every thread of the block (8 warps) calls it.
+template <int VPT, class PackedAt>
+__device__ __forceinline__ void bv_group_block(uint32_t V, uint32_t v0, uint32_t acc_words,
+                                               uint32_t span, const uint32_t *label,
+                                               PackedAt packed_at, uint32_t nc, const uint32_t *cnt,
+                                               uint32_t *fill, const uint32_t *minv, uint32_t *order,
+                                               uint32_t *order_comp, uint32_t *comp_start,
+                                               uint32_t *comp_key, uint32_t *ncomp, uint32_t *acc,
+                                               uint32_t *big, uint32_t *cross, uint32_t *ncross,
+                                               RootTable &tab) {
+  uint32_t r[VPT], slot[VPT], h[VPT];
+  bool in[VPT];
+  root_table_clear(tab, 0u);
+#pragma unroll
+  for (int k = 0; k < VPT; ++k) {
+    const uint32_t v = v0 + k * blockDim.x + threadIdx.x;
+    in[k] = v < V;
+    r[k] = in[k] ? __ldcg(label + v) : 0u;
+  }
+  __syncthreads();  // the table is clear
+  // rank of each vertex among the block's members of its root, then one cursor claim per root
+#pragma unroll
+  for (int k = 0; k < VPT; ++k)
+    if (in[k]) {
+      h[k] = root_slot(tab, r[k]);
+      slot[k] = atomicAdd(&tab.cnt[h[k]], 1u);
+    }
+  __syncthreads();
+  for (uint32_t e = threadIdx.x; e < kRootSlots; e += blockDim.x) {
+    const uint32_t key = tab.key[e];
+    if (key != 0xffffffffu) tab.aux[e] = atomicAdd(&fill[key], tab.cnt[e]);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < VPT; ++k)
+    if (in[k]) slot[k] += tab.aux[h[k]];
+  __syncthreads();  // the table's next user clears it
+#pragma unroll
+  for (int k = 0; k < VPT; ++k) {
+    if (!in[k]) continue;
+    const uint32_t v = v0 + k * blockDim.x + threadIdx.x;
+    const uint64_t s = packed_at(r[k]);
+    const uint32_t start = (uint32_t)s, c = (uint32_t)(s >> 32);
+    const uint32_t pos = start + slot[k];
+    order[pos] = v;
+    order_comp[pos] = c;
+    if (v == r[k]) {
+      const uint32_t members = __ldcg(cnt + v);
+      comp_start[c] = start;
+      comp_key[c] = minv ? __ldcg(minv + v) : v;
+      const uint32_t end = start + members;
+      if (start / span != (end - 1) / span) {
+        uint32_t *ac = acc + (uint64_t)(start / span) * acc_words;
+        for (uint32_t i = 0; i < acc_words; ++i) ac[i] = 0;
+        if (2ull * members > V) *big = c;  // at most one component holds over half the vertices
+        // listed for the sampling from acc (one component at most per span edge)
+        cross[atomicAdd(ncross, 1u)] = c;
+      }
+    }
+    if (v == 0) {
+      comp_start[nc] = V;
+      *ncomp = nc;
+    }
+  }
+}
+
 __global__ void __launch_bounds__(256) k_bv_group(uint32_t V, uint32_t acc_words, uint32_t span,
                                                   const uint32_t *label, const uint64_t *packed,
                                                   const uint64_t *total, const uint32_t *cnt,
                                                   uint32_t *fill, const uint32_t *minv,
                                                   uint32_t *order, uint32_t *order_comp,
                                                   uint32_t *comp_start, uint32_t *comp_key,
-                                                  uint32_t *ncomp, uint32_t *acc, uint32_t *big) {
-  __shared__ uint32_t stage[8][32];
-  __shared__ uint32_t s_r0, s_base;
-  const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool in = v < V;
-  const uint32_t r = in ? label[v] : 0u;
-  if (threadIdx.x == 0) s_r0 = r;
-  __syncthreads();
-  uint32_t slot;
-  if (__syncthreads_and(!in || r == s_r0)) {
-    // one root for the whole block (a giant component): one cursor claim for all its vertices
-    if (threadIdx.x == 0) {
-      const uint32_t nin = V - blockIdx.x * blockDim.x < blockDim.x ? V - blockIdx.x * blockDim.x : blockDim.x;
-      s_base = atomicAdd(&fill[r], nin);
-    }
-    __syncthreads();
-    if (!in) return;
-    slot = s_base + threadIdx.x;
-  } else {
-    const uint32_t active = __ballot_sync(kFull, in);
-    if (!in) return;
-    slot = warp_agg_inc(fill, r, active, stage[threadIdx.x >> 5]);
-  }
-  const uint64_t s = packed[r];
-  const uint32_t start = (uint32_t)s, c = (uint32_t)(s >> 32);
-  const uint32_t pos = start + slot;
-  order[pos] = v;
-  order_comp[pos] = c;
-  if (v == r) {
-    comp_start[c] = start;
-    comp_key[c] = minv ? minv[r] : r;
-    const uint32_t end = start + cnt[r];
-    if (start / span != (end - 1) / span) {
-      uint32_t *ac = acc + (uint64_t)(start / span) * acc_words;
-      for (uint32_t i = 0; i < acc_words; ++i) ac[i] = 0;
-      if (2ull * cnt[r] > V) *big = c;  // at most one component holds over half the vertices
-    }
-  }
-  if (v == 0) {
-    const uint32_t nc = (uint32_t)(*total >> 32);
-    comp_start[nc] = V;
-    *ncomp = nc;
-  }
+                                                  uint32_t *ncomp, uint32_t *acc, uint32_t *big,
+                                                  uint32_t *cross, uint32_t *ncross) {
+  const uint32_t nc = (uint32_t)(*total >> 32);
+  __shared__ RootTable tab;
+  bv_group_block<1>(V, blockIdx.x * blockDim.x, acc_words, span, label,
+                    [&](uint32_t r) { return packed[r]; }, nc, cnt, fill, minv, order, order_comp,
+                    comp_start, comp_key, ncomp, acc, big, cross, ncross, tab);
 }
 
-// perform_boruvka_round (src/cc_sketch_alg.cpp:246-380) for round >= 1: each warp XOR-merges
-// sample `round` (columns round*CPS .. +CPS, one contiguous word run) + the deterministic bucket
-// over its `span` (<= 32) consecutive grouped members, copied to shared memory with cp.async in
-// batches of KB, one batch ahead. A component wholly inside the span is sampled right here
-// (results applied 32 at a time by the lanes); a component covering the whole span leaves this
-// warp's XOR in its partial slot (k_bv_reduce_parts folds those); the parts of components
-// crossing a span edge go to acc (per component: CPS*B column buckets, then the deterministic
-// one) with one coalesced atomicXor per word.
-template <int CPS, int NW, int KB>
-__global__ void __launch_bounds__(256) k_bv_merge(BoruvkaGeom g, const uint32_t *__restrict__ sk_words,
-                                                  BoruvkaBufs b) {
-  const uint32_t round = *b.round;
-  extern __shared__ __align__(16) uint8_t bv_smem[];
+// perform_boruvka_round (src/cc_sketch_alg.cpp:246-380) for round >= 1, grouped positions
+// [w * span, w * span + span) (span <= 32): the warp XOR-merges sample `round` (columns
+// round*CPS .. +CPS, one contiguous word run) + the deterministic bucket of those members, copied
+// to shared memory with bulk copies in batches of KB, one batch ahead. A component wholly inside
+// the span is sampled right here (results applied 32 at a time by the lanes); a component
+// covering the whole span leaves this warp's XOR in its partial slot w (bv_reduce_parts_warp folds
+// those); the parts of components crossing a span edge go to acc (per component: CPS*B column
+// buckets, then the deterministic one) with one coalesced atomicXor per word. False when a copy did
+// not land in time (status set).
+template <int CPS, int NW, int KB, int NS>
+__device__ bool bv_merge_span(const BoruvkaGeom &g, const uint32_t *__restrict__ sk_words,
+                              const BoruvkaBufs &b, uint32_t round, uint32_t *flags,
+                              BvRingN<NS> &ring, uint32_t &T, uint32_t w) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t W = 3 * CPS * g.B, SW = W + 3;
-  BvRing ring;
-  ring.init(bv_smem + (threadIdx.x >> 5) * bv_warp_bytes(W, KB), W, KB);
   uint32_t *st = ring.stage;
-  const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint64_t p0 = (uint64_t)w * g.span;
-  if (p0 >= g.V) return;
+  if (p0 >= g.V) return true;
   const uint32_t n = (uint32_t)(g.V - p0 < g.span ? g.V - p0 : g.span);  // span <= 32
   const uint32_t p1 = (uint32_t)p0 + n;
   const uint32_t col = 3 * round * CPS * g.B, detw = 3 * g.C * g.B;
   // the component merged from its complement: its members are skipped, and every other
   // member's words are also XORed into its acc
-  const uint32_t big = g.complement ? *b.big : 0xffffffffu;
-  if (big != 0xffffffffu && b.comp_start[big] <= p0 && b.comp_start[big + 1] >= p1) {
+  const uint32_t big = g.complement ? __ldcg(b.big) : 0xffffffffu;
+  if (big != 0xffffffffu && __ldcg(b.comp_start + big) <= p0 && __ldcg(b.comp_start + big + 1) >= p1) {
     if (lane == 0) b.part_comp[w] = 0xffffffffu;
-    return;
+    return true;
   }
-  const uint32_t my_v = lane < n ? b.order[p0 + lane] : 0u;
-  const uint32_t my_c = lane < n ? b.order_comp[p0 + lane] : 0u;
+  const uint32_t my_v = lane < n ? __ldcg(b.order + p0 + lane) : 0u;
+  const uint32_t my_c = lane < n ? __ldcg(b.order_comp + p0 + lane) : 0u;
   // the components of the positions just before and after the span: a component that also
   // holds one of them crosses a span edge (members of a component are contiguous)
   uint32_t edge_c = 0xffffffffu;
-  if (lane == 0 && p0 > 0) edge_c = b.order_comp[p0 - 1];
-  if (lane == 1 && p1 < g.V) edge_c = b.order_comp[p1];
+  if (lane == 0 && p0 > 0) edge_c = __ldcg(b.order_comp + p0 - 1);
+  if (lane == 1 && p1 < g.V) edge_c = __ldcg(b.order_comp + p1);
   const uint32_t prev_c = __shfl_sync(kFull, edge_c, 0), next_c = __shfl_sync(kFull, edge_c, 1);
   // lane k < KB copies member t * KB + k of batch t (its vertex and component come by shuffle)
   auto member_sketch = [&](uint32_t m) {
@@ -888,9 +992,10 @@ __global__ void __launch_bounds__(256) k_bv_merge(BoruvkaGeom g, const uint32_t 
     const uint32_t *sk = member_sketch(m);
     const uint32_t c = __shfl_sync(kFull, my_c, m & 31);
     const bool mine = lane < (uint32_t)KB && m < n && c != big;
-    ring.issue(t, mine, sk + col, W, sk + detw, KB);
+    ring.issue(T + t, mine, sk + col, W, sk + detw, KB);
   };
-  issue(0);
+  const uint32_t nb = (n + KB - 1) / KB;
+  for (uint32_t a = 0; a + 1 < (uint32_t)NS && a < nb; ++a) issue(a);
   uint32_t acc[NW], dacc = 0, cpl[NW], dcpl = 0;
 #pragma unroll
   for (int k = 0; k < NW; ++k) acc[k] = cpl[k] = 0;
@@ -901,7 +1006,7 @@ __global__ void __launch_bounds__(256) k_bv_merge(BoruvkaGeom g, const uint32_t 
   uint64_t my_idx = 0;
   uint32_t my_key = 0, nres = 0;
   auto apply = [&]() {
-    if (lane < nres) handle_result(my_res, my_idx, round, my_key, g, b);
+    if (lane < nres) handle_result(my_res, my_idx, round, my_key, g, b, flags);
     __syncwarp();
     nres = 0;
   };
@@ -921,7 +1026,7 @@ __global__ void __launch_bounds__(256) k_bv_merge(BoruvkaGeom g, const uint32_t 
       if (lane == nres) {
         my_res = res;
         my_idx = idx;
-        my_key = b.comp_key[comp];
+        my_key = __ldcg(b.comp_key + comp);
       }
       if (++nres == 32) apply();
     } else if (before && after) {
@@ -936,7 +1041,7 @@ __global__ void __launch_bounds__(256) k_bv_merge(BoruvkaGeom g, const uint32_t 
       whole = true;
     } else {
       // a component crossing a span edge owns acc slot (its first position / span)
-      const uint32_t slot = before ? b.comp_start[comp] / g.span : w;
+      const uint32_t slot = before ? __ldcg(b.comp_start + comp) / g.span : w;
       uint32_t *ac = b.acc + (uint64_t)slot * SW;
 #pragma unroll
       for (int k = 0; k < NW; ++k) {
@@ -946,13 +1051,13 @@ __global__ void __launch_bounds__(256) k_bv_merge(BoruvkaGeom g, const uint32_t 
       if (lane < 3 && dacc) atomicXor(ac + W + lane, dacc);
     }
   };
-  const uint32_t nb = (n + KB - 1) / KB;
   for (uint32_t t = 0; t < nb; ++t) {
-    if (t + 1 < nb) issue(t + 1);
-    if (!ring.wait(t)) {
+    if (t + NS - 1 < nb) issue(t + NS - 1);
+    if (!ring.wait(T + t)) {
       if (lane == 0) atomicOr(b.status, kStatusTimeout);
-      if (t + 1 < nb) ring.wait(t + 1);  // its copies must land before the block's shared memory goes away
-      return;
+      // their copies must land before the shared memory is reused or freed
+      for (uint32_t a = 1; a < (uint32_t)NS && t + a < nb; ++a) ring.wait(T + t + a);
+      return false;
     }
     // not unrolled: one copy of the flush (and the sampling it inlines) keeps the kernel small
     // enough for the instruction cache
@@ -969,7 +1074,7 @@ __global__ void __launch_bounds__(256) k_bv_merge(BoruvkaGeom g, const uint32_t 
           for (int q = 0; q < NW; ++q) acc[q] = 0;
           dacc = 0;
         }
-        const uint8_t *slt = ring.slot(t, k, KB);
+        const uint8_t *slt = ring.slot(T + t, k, KB);
         const uint32_t *sl = bulk_run_at(slt, sk + col);
         const uint32_t *sd = bulk_run_at(slt + ring.run_cap, sk + detw);
 #pragma unroll
@@ -990,10 +1095,11 @@ __global__ void __launch_bounds__(256) k_bv_merge(BoruvkaGeom g, const uint32_t 
     }
     __syncwarp();
   }
+  T += nb;
   if (cur != 0xffffffffu) flush(cur);
   apply();
   if (big != 0xffffffffu) {
-    uint32_t *ac = b.acc + (uint64_t)(b.comp_start[big] / g.span) * SW;
+    uint32_t *ac = b.acc + (uint64_t)(__ldcg(b.comp_start + big) / g.span) * SW;
 #pragma unroll
     for (int k = 0; k < NW; ++k) {
       const uint32_t wi = k * 32 + lane;
@@ -1002,26 +1108,38 @@ __global__ void __launch_bounds__(256) k_bv_merge(BoruvkaGeom g, const uint32_t 
     if (lane < 3 && dcpl) atomicXor(ac + W + lane, dcpl);
   }
   if (!whole && lane == 0) b.part_comp[w] = 0xffffffffu;
+  return true;
 }
 
-// Folds the partial slots of merge warps covered by one component into that component's acc:
-// one warp per 32 consecutive slots (KB slots' loads in flight), one atomicXor per word per
-// component per warp.
 template <int CPS, int NW, int KB>
-__global__ void __launch_bounds__(256) k_bv_reduce_parts(BoruvkaGeom g, uint32_t nslots, BoruvkaBufs b) {
-  const uint32_t lane = threadIdx.x & 31;
-  const uint32_t s0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32;
-  if (s0 >= nslots) return;
-  const uint32_t n = nslots - s0 < 32 ? nslots - s0 : 32;
+__global__ void __launch_bounds__(256) k_bv_merge(BoruvkaGeom g, const uint32_t *__restrict__ sk_words,
+                                                  BoruvkaBufs b) {
+  extern __shared__ __align__(16) uint8_t bv_smem[];
   const uint32_t W = 3 * CPS * g.B;
-  const uint32_t my_c = lane < n ? b.part_comp[s0 + lane] : 0xffffffffu;
+  BvRing ring;
+  ring.init(bv_smem + (threadIdx.x >> 5) * bv_warp_bytes(W, KB), W, KB);
+  uint32_t T = 0;
+  bv_merge_span<CPS, NW, KB, 2>(g, sk_words, b, *b.round, b.flags, ring, T,
+                             (blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+}
+
+// Folds the partial slots [s0, s0 + per) (per <= 32) of merge warps covered by one component into
+// that component's acc (KB slots' loads in flight), one atomicXor per word per component.
+template <int CPS, int NW, int KB>
+__device__ void bv_reduce_parts_warp(const BoruvkaGeom &g, uint32_t nslots, const BoruvkaBufs &b,
+                                     uint32_t s0, uint32_t per) {
+  const uint32_t lane = threadIdx.x & 31;
+  if (s0 >= nslots) return;
+  const uint32_t n = nslots - s0 < per ? nslots - s0 : per;
+  const uint32_t W = 3 * CPS * g.B;
+  const uint32_t my_c = lane < n ? __ldcg(b.part_comp + s0 + lane) : 0xffffffffu;
   uint32_t live = __ballot_sync(kFull, my_c != 0xffffffffu);
   if (!live) return;
   uint32_t acc[NW], dacc = 0, cur = 0xffffffffu;
 #pragma unroll
   for (int k = 0; k < NW; ++k) acc[k] = 0;
   auto flush = [&]() {
-    uint32_t *ac = b.acc + (uint64_t)(b.comp_start[cur] / g.span) * (W + 3);
+    uint32_t *ac = b.acc + (uint64_t)(__ldcg(b.comp_start + cur) / g.span) * (W + 3);
 #pragma unroll
     for (int k = 0; k < NW; ++k) {
       const uint32_t wi = k * 32 + lane;
@@ -1037,7 +1155,7 @@ __global__ void __launch_bounds__(256) k_bv_reduce_parts(BoruvkaGeom g, uint32_t
       if (live) live &= live - 1;
       if (sl[k] < 32) {
         const uint32_t *pt = b.part + (uint64_t)(s0 + sl[k]) * (W + 3);
-        region_load(pt, pt + W, W, lane, x[k], dw[k]);
+        region_load<NW, true>(pt, pt + W, W, lane, x[k], dw[k]);
       }
     }
 #pragma unroll
@@ -1059,38 +1177,54 @@ __global__ void __launch_bounds__(256) k_bv_reduce_parts(BoruvkaGeom g, uint32_t
   flush();
 }
 
+// Partial slots folded per warp.
+constexpr uint32_t kPartsPerWarp = 8;
+
+template <int CPS, int NW, int KB>
+__global__ void __launch_bounds__(256) k_bv_reduce_parts(BoruvkaGeom g, uint32_t nslots, BoruvkaBufs b) {
+  bv_reduce_parts_warp<CPS, NW, KB>(g, nslots, b,
+                                    ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * kPartsPerWarp,
+                                    kPartsPerWarp);
+}
+
+// Sampling of component comp when it crosses a span edge (its merged sample is in acc).
+template <int CPS>
+__device__ void bv_sample_spanning_comp(const BoruvkaGeom &g, const BoruvkaBufs &b, uint32_t round,
+                                        uint32_t *flags, uint32_t comp) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t acc_words = (CPS * g.B + 1) * 3;
+  const uint32_t s = __ldcg(b.comp_start + comp), e = __ldcg(b.comp_start + comp + 1);
+  if (s / g.span == (e - 1) / g.span) return;
+  const uint32_t *ac = b.acc + (uint64_t)(s / g.span) * acc_words;
+  uint32_t a[CPS][2][3], d[3];
+  d[0] = __ldcg(ac + 3 * CPS * g.B);
+  d[1] = __ldcg(ac + 3 * CPS * g.B + 1);
+  d[2] = __ldcg(ac + 3 * CPS * g.B + 2);
+#pragma unroll
+  for (int c = 0; c < CPS; ++c)
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const uint32_t j = q * 32 + lane;
+      a[c][q][0] = a[c][q][1] = a[c][q][2] = 0;
+      if (j < g.B) {
+        const uint32_t *bk = ac + 3 * (c * g.B + j);
+        a[c][q][0] = __ldcg(bk);
+        a[c][q][1] = __ldcg(bk + 1);
+        a[c][q][2] = __ldcg(bk + 2);
+      }
+    }
+  uint64_t idx;
+  const int res = warp_sample_cols<CPS>(d, a, g.B, g.flip_chk, &idx);
+  if (lane == 0) handle_result(res, idx, round, __ldcg(b.comp_key + comp), g, b, flags);
+}
+
 template <int CPS>
 __global__ void k_bv_sample_spanning(BoruvkaGeom g, BoruvkaBufs b) {
   const uint32_t round = *b.round;
-  const uint32_t lane = threadIdx.x & 31;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  const uint32_t nc = *b.ncomp;
-  const uint32_t acc_words = (CPS * g.B + 1) * 3;
-  for (uint32_t comp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; comp < nc; comp += nwarps) {
-    const uint32_t s = b.comp_start[comp], e = b.comp_start[comp + 1];
-    if (s / g.span == (e - 1) / g.span) continue;
-    const uint32_t *ac = b.acc + (uint64_t)(s / g.span) * acc_words;
-    uint32_t a[CPS][2][3], d[3];
-    d[0] = __ldcg(ac + 3 * CPS * g.B);
-    d[1] = __ldcg(ac + 3 * CPS * g.B + 1);
-    d[2] = __ldcg(ac + 3 * CPS * g.B + 2);
-#pragma unroll
-    for (int c = 0; c < CPS; ++c)
-#pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        const uint32_t j = q * 32 + lane;
-        a[c][q][0] = a[c][q][1] = a[c][q][2] = 0;
-        if (j < g.B) {
-          const uint32_t *bk = ac + 3 * (c * g.B + j);
-          a[c][q][0] = __ldcg(bk);
-          a[c][q][1] = __ldcg(bk + 1);
-          a[c][q][2] = __ldcg(bk + 2);
-        }
-      }
-    uint64_t idx;
-    const int res = warp_sample_cols<CPS>(d, a, g.B, g.flip_chk, &idx);
-    if (lane == 0) handle_result(res, idx, round, b.comp_key[comp], g, b);
-  }
+  const uint32_t nx = *b.ncross;
+  for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < nx; i += nwarps)
+    bv_sample_spanning_comp<CPS>(g, b, round, b.flags, b.cross[i]);
 }
 
 // End of a round (the loop test of boruvka_emulation, src/cc_sketch_alg.cpp:490-509): stop when
@@ -1117,12 +1251,214 @@ __global__ void k_bv_check(BoruvkaBufs b, uint32_t samples, cudaGraphConditional
   if (in_graph) cudaGraphSetConditional(cond, go);
 }
 
-__global__ void k_bv_final(uint32_t V, uint32_t *parent, uint32_t *out, uint32_t *ncc) {
-  const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-  if (v >= V) return;
+__device__ __forceinline__ void bv_final_vertex(uint32_t v, uint32_t *parent, uint32_t *out,
+                                                uint32_t *ncc) {
   const uint32_t r = dsu_find(parent, v);
   out[v] = r;
   if (r == v) atomicAdd(ncc, 1u);
+}
+
+__global__ void k_bv_final(uint32_t V, uint32_t *parent, uint32_t *out, uint32_t *ncc) {
+  const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v < V) bv_final_vertex(v, parent, out, ncc);
+}
+
+// ---- the whole query in one cooperative launch ------------------------------------------------
+__device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t *p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Grid-wide barrier of a cooperative launch: the blocks count their arrivals in *count (zeroed
+// before the launch); barrier number k completes at k * gridDim.x arrivals. Writes before it are
+// seen by every block after it (fence, arrival, acquire, fence). A block with a failed warp
+// (failed = true in any thread) leaves without arriving; a block that waits longer than
+// kWaitLimitNs sets the timeout status. Both return false, and the caller returns from the kernel
+// (the other blocks then time out at their next barrier).
+__device__ bool grid_barrier(uint32_t *count, uint32_t k, bool failed, uint32_t *status) {
+  __shared__ uint32_t s_ok;
+  if (__syncthreads_or(failed)) return false;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(count, 1u);
+    const uint32_t target = k * gridDim.x;
+    uint32_t ok = 1;
+    if (ld_acquire_gpu(count) < target) {
+      const uint64_t t0 = global_ns();
+      while (ld_acquire_gpu(count) < target) {
+        if (global_ns() - t0 > kWaitLimitNs) {
+          atomicOr(status, kStatusTimeout);
+          ok = 0;
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    __threadfence();
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// Batches of the one-launch query's copy rings: NS - 1 of them in flight while one is read (a
+// third batch measured no faster than two).
+constexpr int kBvQueryRing = 2;
+
+// Exclusive scan of one u64 per thread over a block of 256 threads.
+__device__ __forceinline__ uint64_t block_scan_u64_256(uint64_t x, uint64_t *ws /*8*/) {
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint64_t inc = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint64_t y = __shfl_up_sync(kFull, inc, o);
+    if (lane >= (uint32_t)o) inc += y;
+  }
+  if (lane == 31) ws[warp] = inc;
+  __syncthreads();
+  uint64_t pre = 0;
+  for (uint32_t k = 0; k < warp; ++k) pre += ws[k];
+  __syncthreads();
+  return pre + inc - x;
+}
+
+// boruvka_emulation (src/cc_sketch_alg.cpp:464-513) in one cooperative launch of 256-thread
+// blocks: a fresh DSU, round 0, then per round the phases of the per-phase kernels separated by
+// grid barriers -- (1) roots and members per root; (2) each block's exclusive scan of (members |
+// 1 << 32) over its range of CH vertices; (3) each block's scan of the blocks' totals, then the
+// grouping; (4) the merge over spans, sampling the components inside a span, with the next round's
+// counters cleared; (5) the partial slots folded; (6) the components crossing span edges sampled
+// -- then the loop test of k_bv_check, taken by every block alike, and the labels. A round's
+// "modified" word is b.flags[round % 3]: the word of round r + 1 is cleared during round r, long
+// after every block read it as the word of round r - 2.
+template <int CPS, int NW, int KB, int KBP>
+__global__ void __launch_bounds__(256) k_bv_query(BoruvkaGeom g, const uint32_t *__restrict__ sk_words,
+                                                  BoruvkaBufs b, uint32_t samples,
+                                                  uint32_t *labels_out, uint32_t *ncc) {
+  extern __shared__ __align__(16) uint8_t bv_smem[];
+  __shared__ uint64_t s_pref[kBvQueryMaxBlocks + 1];
+  __shared__ uint64_t s_ws[8];
+  __shared__ RootTable tab;
+  const uint32_t V = g.V, nblk = gridDim.x, tid = threadIdx.x;
+  const uint32_t W = 3 * CPS * g.B;
+  BvRingN<kBvQueryRing> ring;
+  ring.init(bv_smem + (tid >> 5) * bv_warp_bytes(W, KB, kBvQueryRing), W, KB);
+  uint32_t T = 0;     // batches through this warp's copy ring
+  uint32_t nbar = 0;  // grid barriers passed
+  bool failed = false;
+  auto sync = [&]() { return grid_barrier(b.qbar, ++nbar, failed, b.status); };
+  const uint32_t gw = (blockIdx.x * blockDim.x + tid) >> 5, nwarps = (nblk * blockDim.x) >> 5;
+  const uint32_t gt = blockIdx.x * blockDim.x + tid, nthreads = nblk * blockDim.x;
+  uint32_t *minv = b.trace ? b.minv : nullptr;
+  for (uint32_t v = gt; v < V; v += nthreads) {
+    b.parent[v] = v;
+    b.cnt[v] = 0;
+    b.fill[v] = 0;
+    if (minv) minv[v] = 0xffffffffu;
+  }
+  if (gt == 0) {
+    *b.forest_n = 0;
+    if (b.trace) *b.trace_n = 0;
+    b.flags[0] = b.flags[1] = b.flags[2] = 0;
+    *b.big = 0xffffffffu;
+    *b.ncross = 0;
+    *ncc = 0;
+  }
+  if (!sync()) return;
+  failed = !bv_round0_warp<CPS, KB, kBvQueryRing>(g, sk_words, b, b.flags, ring, T, gw, nwarps);
+  if (!sync()) return;
+  const uint32_t CH = (((V + nblk - 1) / nblk) + 255) & ~255u;  // scan range of a block
+  const uint32_t nspans = (V + g.span - 1) / g.span;
+  const uint32_t acc_words = (CPS * g.B + 1) * 3;
+  uint32_t round = 0;
+  for (;;) {
+    const uint32_t modified = __ldcg(b.flags + round % 3);
+    if (modified == 0 || round + 1 >= samples) {
+      if (gt == 0) {
+        b.ctl[0] = modified ? round + 1 : round;
+        b.ctl[1] = modified ? 1u : 0u;
+        b.ctl[2] = 0;
+        *b.round = round;
+      }
+      break;
+    }
+    ++round;
+    uint32_t *flags = b.flags + round % 3;
+    // (1)
+    if (gt == 0) {
+      b.flags[(round + 1) % 3] = 0;
+      if (round > 1) *b.ncross = 0;  // the previous round's list was read before the last barrier
+    }
+    for (uint32_t v0 = blockIdx.x * 512; v0 < V; v0 += nblk * 512)
+      bv_label_block<2>(V, v0, b.parent, b.label, b.cnt, minv, tab);
+    if (!sync()) return;
+    // (2)
+    {
+      const uint32_t ipt = CH / 256, a = blockIdx.x * CH + tid * ipt;
+      uint64_t sum = 0;
+      for (uint32_t i = 0; i < ipt; ++i)
+        if (a + i < V) {
+          const uint32_t c = __ldcg(b.cnt + a + i);
+          sum += (uint64_t)c | (c ? (1ull << 32) : 0ull);
+        }
+      uint64_t run = block_scan_u64_256(sum, s_ws);
+      for (uint32_t i = 0; i < ipt; ++i)
+        if (a + i < V) {
+          const uint32_t c = __ldcg(b.cnt + a + i);
+          b.packed[a + i] = run;
+          run += (uint64_t)c | (c ? (1ull << 32) : 0ull);
+        }
+      if (tid == 255) b.btot[blockIdx.x] = run;
+    }
+    if (!sync()) return;
+    // (3)
+    {
+      const uint32_t per = (nblk + 255) / 256;
+      uint64_t sum = 0;
+      for (uint32_t k = 0; k < per; ++k) {
+        const uint32_t i = tid * per + k;
+        if (i < nblk) sum += __ldcg(b.btot + i);
+      }
+      uint64_t run = block_scan_u64_256(sum, s_ws);
+      for (uint32_t k = 0; k < per; ++k) {
+        const uint32_t i = tid * per + k;
+        if (i < nblk) {
+          s_pref[i] = run;
+          run += __ldcg(b.btot + i);
+        }
+      }
+      if (tid == 255) s_pref[nblk] = run;
+      __syncthreads();
+      const uint32_t nc = (uint32_t)(s_pref[nblk] >> 32);
+      for (uint32_t v0 = blockIdx.x * 512; v0 < V; v0 += nblk * 512)
+        bv_group_block<2>(V, v0, acc_words, g.span, b.label,
+                       [&](uint32_t r) { return __ldcg(b.packed + r) + s_pref[r / CH]; }, nc, b.cnt,
+                       b.fill, minv, b.order, b.order_comp, b.comp_start, b.comp_key, b.ncomp,
+                       b.acc, b.big, b.cross, b.ncross, tab);
+    }
+    if (!sync()) return;
+    // (4)
+    for (uint32_t w = gw; w < nspans && !failed; w += nwarps)
+      failed = !bv_merge_span<CPS, NW, KB, kBvQueryRing>(g, sk_words, b, round, flags, ring, T, w);
+    for (uint32_t v = gt; v < V; v += nthreads) {
+      b.cnt[v] = 0;
+      b.fill[v] = 0;
+      if (minv) minv[v] = 0xffffffffu;
+    }
+    if (!sync()) return;
+    // (5)
+    for (uint32_t s0 = gw * kPartsPerWarp; s0 < nspans; s0 += nwarps * kPartsPerWarp)
+      bv_reduce_parts_warp<CPS, NW, KBP>(g, nspans, b, s0, kPartsPerWarp);
+    if (gt == 0) *b.big = 0xffffffffu;
+    if (!sync()) return;
+    // (6)
+    const uint32_t nx = __ldcg(b.ncross);
+    for (uint32_t i = gw; i < nx; i += nwarps)
+      bv_sample_spanning_comp<CPS>(g, b, round, flags, __ldcg(b.cross + i));
+    if (!sync()) return;
+  }
+  for (uint32_t v = gt; v < V; v += nthreads) bv_final_vertex(v, b.parent, labels_out, ncc);
 }
 
 // Shared-memory bucket-update probe: every thread XORs 96-bit updates into random 12-byte
@@ -1348,7 +1684,7 @@ __global__ void k_total_xor(const uint32_t *__restrict__ sk, uint32_t V, uint32_
   if (x) atomicXor(total + wd, x);
 }
 
-// Launch shape of the round-0 and merge kernels: members per cp.async batch, and the dynamic
+// Launch shape of the round-0 and merge kernels: members per bulk-copy batch, and the dynamic
 // shared memory of a 256-thread block (8 warps).
 int bv_batch(int cps) { return cps == 1 ? 8 : 1; }
 size_t bv_smem_bytes(const BoruvkaGeom &g) {
@@ -1414,12 +1750,13 @@ cudaError_t boruvka_round(const BoruvkaGeom &g, const uint8_t *sketches, const B
   k_bv_group<<<blocks_for(V, 256), 256, 0, s>>>(V, (g.cps * g.B + 1) * 3, g.span, b.label, b.packed, b.scan_total,
                                                  b.cnt, b.fill, trace ? b.minv : nullptr, b.order,
                                                  b.order_comp, b.comp_start, b.comp_key, b.ncomp,
-                                                 b.acc, b.big);
+                                                 b.acc, b.big, b.cross, b.ncross);
   g_launches++;
   const uint64_t warps = (V + g.span - 1) / g.span;
   const uint32_t *sk = reinterpret_cast<const uint32_t *>(sketches);
   const unsigned sblocks = std::min<unsigned>(blocks_for((uint64_t)V * 32, 256), num_sms() * 16);
-  const unsigned mblocks = blocks_for(warps * 32, 256), rblocks = blocks_for(warps, 256);
+  const unsigned mblocks = blocks_for(warps * 32, 256);
+  const unsigned rblocks = blocks_for((warps + kPartsPerWarp - 1) / kPartsPerWarp * 32, 256);
   const size_t smem = bv_smem_bytes(g);
   if (g.cps == 1 && g.B <= 42) {
     if ((e = bv_smem_attr(k_bv_merge<1, 4, 8>, smem)) != cudaSuccess) return e;
@@ -1439,6 +1776,41 @@ cudaError_t boruvka_round(const BoruvkaGeom &g, const uint8_t *sketches, const B
   else k_bv_sample_spanning<7><<<sblocks, 256, 0, s>>>(g, b);
   g_launches++;
   return cudaGetLastError();
+}
+
+constexpr int kBvQueryBlocksPerSm = 4;
+
+cudaError_t boruvka_query_launch(const BoruvkaGeom &g, uint32_t samples, const uint8_t *sketches,
+                                 const BoruvkaBufs &b, uint32_t *labels_out, uint32_t *ncc,
+                                 cudaStream_t s) {
+  const size_t smem = 8 * (size_t)bv_warp_bytes(3 * g.cps * g.B, bv_batch(g.cps), kBvQueryRing);
+  auto launch = [&](auto kern) -> cudaError_t {
+    cudaError_t e = smem_optin(kern);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    // every block resident at once (the launch fails otherwise): a grid barrier never waits for
+    // a block that has not started
+    const int blocks = std::min<int>(std::min(per_sm, kBvQueryBlocksPerSm) * num_sms(), (int)kBvQueryMaxBlocks);
+    e = cudaMemsetAsync(b.qbar, 0, sizeof(uint32_t), s);
+    if (e != cudaSuccess) return e;
+    BoruvkaGeom a_g = g;
+    const uint32_t *a_sk = reinterpret_cast<const uint32_t *>(sketches);
+    BoruvkaBufs a_b = b;
+    uint32_t a_samples = samples;
+    uint32_t *a_labels = labels_out, *a_ncc = ncc;
+    void *args[] = {&a_g, &a_sk, &a_b, &a_samples, &a_labels, &a_ncc};
+    e = cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(kern), dim3(blocks), dim3(256), args,
+                                    smem, s);
+    g_launches++;
+    return e;
+  };
+  if (g.cps == 1 && g.B <= 42) return launch(k_bv_query<1, 4, 8, 4>);
+  if (g.cps == 1) return launch(k_bv_query<1, 6, 8, 4>);
+  if (g.cps == 7) return launch(k_bv_query<7, dev::Region<7>::kNW, 1, 1>);
+  return cudaErrorInvalidValue;
 }
 
 cudaError_t boruvka_final(const BoruvkaGeom &g, const BoruvkaBufs &b, uint32_t *labels_out,

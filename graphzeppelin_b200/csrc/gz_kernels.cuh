@@ -206,7 +206,11 @@ struct BoruvkaBufs {
   uint32_t *big;         // 1   the component holding more than half the vertices, or ~0
   uint32_t *round;       // 1   the current round (device-driven loop)
   uint32_t *ctl;         // 3   after the loop: rounds run, out of samples (0/1); go on (0/1)
-  uint32_t *flags;       // [0] modified
+  uint32_t *flags;       // [0] modified (k_bv_query: [round % 3])
+  uint32_t *cross;       // V / span + 1  components crossing a span edge (sampled from acc)
+  uint32_t *ncross;      // 1
+  uint32_t *qbar;        // 1   arrivals at the grid barriers of k_bv_query
+  uint64_t *btot;        // kBvQueryMaxBlocks  per-block totals of k_bv_query's scan
   uint64_t *forest;      // V   spanning-forest edge indices
   uint32_t *forest_n;    // 1
   void *trace;           // gz_trace_rec_t[trace_cap] or null
@@ -218,6 +222,10 @@ struct BoruvkaBufs {
 // Bytes allocated past the last vertex sketch of any sketch buffer a query reads: its bulk copies
 // read 16-byte-aligned supersets of bucket runs, up to 15 bytes beyond the last sketch.
 constexpr size_t kSketchTail = 256;
+
+// Blocks of the one-launch query (k_bv_query), at most: per-block scan totals are kept for
+// each, and each block scans all of them in shared memory.
+constexpr uint32_t kBvQueryMaxBlocks = 1184;
 
 // Grouped members XOR-merged by one warp per Boruvka round (the per-warp partial slots are
 // sized by it).
@@ -270,6 +278,12 @@ void boruvka_graph_free(BoruvkaGraph &q);
 // The same kernels with the loop run from the host (a device-to-host copy and a synchronize per
 // round; for profilers that do not see kernels inside conditional graphs). Leaves b.ctl[0..1]
 // as the graph does; pin is pinned host memory of at least 3 words.
+// boruvka_emulation in one cooperative kernel launch (all rounds on the device, grid barriers
+// between the phases of a round): the same answer, rounds, samples and trace as the graph and the
+// host loop. b.ctl then holds the rounds and the out-of-samples flag.
+cudaError_t boruvka_query_launch(const BoruvkaGeom &g, uint32_t samples, const uint8_t *sketches,
+                                 const BoruvkaBufs &b, uint32_t *labels_out, uint32_t *ncc,
+                                 cudaStream_t s);
 cudaError_t boruvka_host_loop(const BoruvkaGeom &g, uint32_t samples, const uint8_t *sketches,
                               const BoruvkaBufs &b, uint32_t *labels_out, uint32_t *ncc,
                               uint32_t *pin, cudaStream_t s);

@@ -303,13 +303,16 @@ def test_giant_component_merge_paths(gz, oracle_mod, path, tmp_path):
     assert cc.size() == n
 
 
+@pytest.mark.parametrize("mode", [0, 1])
 @pytest.mark.parametrize("name", ["c0_v1024", "mult_v1024", "cl_v2048"])
-def test_host_round_loop_equals_query_graph(gz, name):
-    """gz_set_query_graph(0) runs the Boruvka kernels with the round loop on the host: labels,
-    rounds and every round's samples equal the golden answer of the reference."""
+def test_per_phase_query_modes(gz, name, mode):
+    """gz_set_query_graph(1) runs the Boruvka rounds as a CUDA graph of per-phase kernels, (0) the
+    same kernels with the round loop on the host; the default (2) is one cooperative kernel. In
+    every mode labels, rounds and every round's samples equal the golden answer of the
+    reference."""
     c, st, labels, trace = load_case(name)
     alg = _alg(gz, c["num_vertices"], c["seed"], c["sketches_factor"])
-    alg.set_query_graph(False)
+    alg.set_query_graph(mode)
     alg.set_trace(True)
     alg.ingest_records(st)
     cc = alg.connected_components()
