@@ -419,6 +419,15 @@ def run_b200(args, cfg):
         if world == 1 and not args.no_cpu_baseline:
             log("[rank 0] timing the CPU reference baseline and checking full-size parity ...")
             cpu, parity = cpu_baseline_and_parity(alg, stream, cfg, cc)
+        checks = None
+        if world == 1 and not args.no_checks:
+            log("[rank 0] full-size parity of the power-law and many-graph workloads ...")
+            checks = {}
+            for name, fn in (("powerlaw", powerlaw_check), ("many_graphs", many_graphs_check)):
+                try:
+                    checks[name] = fn()
+                except Exception as e:  # reported in the line, the headline stands
+                    checks[name] = {"error": repr(e)}
         serving = None
         if world == 1 and not args.no_serving:
             log("[rank 0] short serving replay with the admission queue in use ...")
@@ -445,6 +454,7 @@ def run_b200(args, cfg):
             "ingest_ms": statistics.mean(ingest_ms),
             "ingest_updates_per_s": n / (statistics.mean(ingest_ms) / 1e3),
             "parity": parity,
+            "checks": checks,
             "serving": serving,
             "roofline": roof,
             "cpu_baseline": cpu,
@@ -778,6 +788,106 @@ POWERLAW_SMALL = dict(POWERLAW, workload="powerlaw_v262144_chunglu2.1_deg200_max
                       num_vertices=1 << 18)
 
 
+def powerlaw_check(threads=None):
+    """The power-law workload at full size (V = 2^20, 10 segments, a snapshot query after each),
+    checked in the CPU-baseline leg: every snapshot answer equals the blocking query's at the same
+    point, and the final partition equals the exact union-find over the stream's final edge set
+    and the reference's connected_components (-DNO_EAGER_DSU build, src/cc_sketch_alg.cpp:515-557)
+    over the whole stream, with the same Boruvka rounds."""
+    import numpy as np
+    import torch
+
+    import graphzeppelin_b200 as gz
+    from graphzeppelin_b200 import streams as S
+    from oracle import oracle as O
+    threads = threads or os.cpu_count() or 1
+    cfg = POWERLAW
+    V, Q = cfg["num_vertices"], cfg["queries"]
+    t0 = time.perf_counter()
+    st = S.chung_lu_stream_fast(V, cfg["exponent"], cfg["mean_degree"], cfg["max_degree"],
+                                cfg["stream_seed"])
+    n = st.num_updates
+    d_rec = torch.from_numpy(st.raw()).cuda()
+    cuts = np.linspace(0, n, Q + 1).astype(np.int64)
+    alg = gz.CCSketchAlg(V, cfg["sketch_seed"])
+    alg.set_gutter_capacity(2 * int(cuts[1] - cuts[0]) + 1024)
+    base = d_rec.data_ptr()
+    snap, tickets, final = [], [], None
+    for k in range(Q):
+        alg.ingest_records_device(base + 9 * int(cuts[k]), int(cuts[k + 1] - cuts[k]))
+        tickets.append(alg.query_submit())
+    for t in tickets:
+        final, rounds = alg.query_wait(t)
+        snap.append(final.size())
+    alg.clear()
+    block = []
+    for k in range(Q):
+        alg.ingest_records_device(base + 9 * int(cuts[k]), int(cuts[k + 1] - cuts[k]))
+        block.append(alg.num_connected_components())
+    labels = final.canonical_labels()
+    alg.close()
+    del d_rec
+    torch.cuda.empty_cache()
+    out = {"workload": cfg["workload"], "num_updates": n, "components_at_each_query": snap,
+           "snapshot_equals_blocking": snap == block}
+    n_exact, exact = O.exact_cc_mt(V, st.raw(), threads)
+    out["exact_partition_equal"] = bool((labels == exact).all())
+    out["components"] = {"gpu": snap[-1], "exact": n_exact}
+    if O.have_reference():
+        with tempfile.TemporaryDirectory() as td:
+            spath, rlab = os.path.join(td, "stream.gzs"), os.path.join(td, "ref.labels")
+            st.write(spath)
+            ref = cpu_reference_run(st, cfg, n, threads, path=spath, eager=False, labels_path=rlab)
+            rlabels = np.fromfile(rlab, np.uint32)
+        out["reference_partition_equal"] = bool((labels == rlabels).all())
+        out["rounds_equal"] = int(rounds) == int(ref["rounds"])
+        out["rounds"] = {"gpu": int(rounds), "reference": int(ref["rounds"])}
+        out["components"]["reference"] = int(ref["num_cc"])
+    out["seconds"] = round(time.perf_counter() - t0, 1)
+    return out
+
+
+def many_graphs_check(num_graphs=64):
+    """The many-graph engine checked graph by graph against the single-graph path on the
+    many-graph workload's generator (the first num_graphs graphs' streams): each graph's sketch
+    bytes (SHA-256 of its dump), partition and Boruvka rounds are the same."""
+    import hashlib
+
+    import numpy as np
+    import torch
+
+    import graphzeppelin_b200 as gz
+    from graphzeppelin_b200 import streams as S
+    t0 = time.perf_counter()
+    Vs, seeds, raw, off = S.many_graph_streams(num_graphs, MANY["stream_seed"])
+    d_rec = torch.from_numpy(raw).cuda()
+    base = d_rec.data_ptr()
+    b = gz.CCSketchBatch(Vs, seeds)
+    b.ingest_device(base, off)
+    res = b.connected_components(labels=True)
+    same_sketch = same_labels = same_rounds = 0
+    for g in range(num_graphs):
+        a = gz.CCSketchAlg(int(Vs[g]), int(seeds[g]))
+        cnt = int(off[g + 1] - off[g])
+        if cnt:
+            a.ingest_records_device(base + 9 * int(off[g]), cnt)
+        cc = a.connected_components()
+        h1 = hashlib.sha256(a.dump_sketches().tobytes()).hexdigest()
+        h2 = hashlib.sha256(b.dump_sketches(g).tobytes()).hexdigest()
+        same_sketch += h1 == h2
+        same_labels += bool((cc.canonical_labels() == res.connected_components(g).canonical_labels()).all())
+        same_rounds += int(a.last_query_rounds) == int(res.rounds[g])
+        a.close()
+    b.close()
+    del d_rec
+    torch.cuda.empty_cache()
+    return {"graphs": num_graphs, "vertices": int(Vs.sum()), "num_updates": int(off[-1]),
+            "sketch_sha256_equal": same_sketch == num_graphs,
+            "partition_equal": same_labels == num_graphs, "rounds_equal": same_rounds == num_graphs,
+            "graphs_equal": {"sketch": same_sketch, "partition": same_labels, "rounds": same_rounds},
+            "seconds": round(time.perf_counter() - t0, 1)}
+
+
 def run_powerlaw(args):
     """Power-law graph with interleaved queries: a Chung-Lu stream (V = 2^20, exponent 2.1, mean
     degree 200 after a 2^14 degree cap; shuffled inserts, deletes of 15% of them, re-inserts of
@@ -912,6 +1022,9 @@ def main():
                     help="queries with the Boruvka round loop on the host (profilers cannot see "
                          "kernels inside the conditional query graph)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-checks", action="store_true",
+                    help="skip the full-size parity checks of the power-law and many-graph "
+                         "workloads in the default run")
     ap.add_argument("--no-serving", action="store_true",
                     help="skip the short serving replay of the default run")
     ap.add_argument("--workload", default="dense",

@@ -1,7 +1,8 @@
 // Properties of the host-record ingest chunk plan (graphzeppelin_b200/csrc/gz_ingest_plan.h) over
 // many call lengths: the chunks tile [0, n) exactly, fit the staging buffers, take the shaped form
-// (doubling first chunks, a short last chunk, a wave after every chunk but the last) exactly when
-// it applies, and otherwise keep full chunks with one wave per kWaveEntries endpoint updates.
+// (doubling first chunks, a wave after every chunk before a tail of 8, 4 and 2 Mi records that
+// has none) exactly when it applies, and otherwise keep full chunks with one wave per kWaveEntries
+// endpoint updates.
 #include <cstdio>
 #include <cstdlib>
 #include <vector>
@@ -46,16 +47,21 @@ static void check(uint64_t n, bool in_place, uint64_t sketch_total) {
   const size_t k = m.size();
   if (plan.shaped) {
     CHECK(m[0] == kFirstChunk, "n=%llu first=%llu", (unsigned long long)n, (unsigned long long)m[0]);
-    CHECK(m[k - 1] == kLastChunk, "n=%llu last=%llu", (unsigned long long)n, (unsigned long long)m[k - 1]);
-    for (size_t i = 0; i + 1 < k; ++i) CHECK(wave[i], "n=%llu chunk %zu has no wave", (unsigned long long)n, i);
-    // doubling up to full chunks, then full chunks, then at most one shortened chunk and the last
+    CHECK(k >= 4, "n=%llu k=%zu", (unsigned long long)n, k);
+    // the tail: 8, 4 and 2 Mi records, no wave after any of them; a wave after every other chunk
+    CHECK(m[k - 1] == kLastChunk && m[k - 2] == 2 * kLastChunk && m[k - 3] == 4 * kLastChunk,
+          "n=%llu tail %llu %llu %llu", (unsigned long long)n, (unsigned long long)m[k - 3],
+          (unsigned long long)m[k - 2], (unsigned long long)m[k - 1]);
+    for (size_t i = 0; i + 3 < k; ++i) CHECK(wave[i], "n=%llu chunk %zu has no wave", (unsigned long long)n, i);
+    for (size_t i = k - 3; i < k; ++i) CHECK(!wave[i], "n=%llu tail chunk %zu has a wave", (unsigned long long)n, i);
+    // doubling up to full chunks, then full chunks, then at most one shortened chunk and the tail
     size_t i = 1;
     while (i < k && m[i] == 2 * m[i - 1] && m[i] <= kStageRecords) ++i;
-    while (i + 2 < k) {
+    while (i + 4 < k) {
       CHECK(m[i] == kStageRecords, "n=%llu chunk %zu = %llu", (unsigned long long)n, i, (unsigned long long)m[i]);
       ++i;
     }
-    CHECK(k <= (n + kStageRecords - 1) / kStageRecords + 3, "n=%llu k=%zu", (unsigned long long)n, k);
+    CHECK(k <= (n + kStageRecords - 1) / kStageRecords + 5, "n=%llu k=%zu", (unsigned long long)n, k);
   } else {
     for (size_t i = 0; i + 1 < k; ++i)
       CHECK(m[i] == plan.chunk, "n=%llu chunk %zu = %llu", (unsigned long long)n, i, (unsigned long long)m[i]);
