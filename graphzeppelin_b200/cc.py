@@ -497,10 +497,10 @@ class CCSketchAlg:
         _check(self.lib.gz_get_params(self._h, ctypes.byref(p)))
         self.params = p
 
-    def set_query_graph(self, mode=2) -> None:
-        """How queries run (gz_set_query_graph): 2 one cooperative kernel (the default), 1 (or
-        True) a CUDA graph of per-phase kernels, 0 (or False) those kernels with the round loop
-        on the host (for profilers)."""
+    def set_query_graph(self, mode=-1) -> None:
+        """How queries run (gz_set_query_graph): 2 one cooperative kernel, 1 (or True) a CUDA
+        graph of per-phase kernels, 0 (or False) those kernels with the round loop on the host
+        (for profilers), -1 by size (the default: 2 up to 2^18 vertices, 1 above)."""
         _check(self.lib.gz_set_query_graph(self._h, int(mode)))
 
     def set_gutter_capacity(self, endpoint_updates: int) -> None:

@@ -182,9 +182,9 @@ struct gz_alg {
   std::unordered_set<uint64_t> hforest;
   // how a query runs: 2 = one cooperative kernel (every round on the device), 1 = a CUDA graph of
   // the per-phase kernels with a conditional while node over the rounds (qgraph), 0 = the same
-  // kernels with the round loop on the host
+  // kernels with the round loop on the host, -1 = by size (query_mode_of)
   gz::BoruvkaGraph qgraph;
-  int query_mode = 2;
+  int query_mode = -1;
   uint32_t *h_qpin = nullptr;  // pinned: rounds, out-of-samples flag, components
   // queries by ticket (gz_query_submit / gz_query_wait): the query graph enqueued on the
   // handle's stream behind every update submitted before it, with its own buffers, so the
@@ -903,11 +903,22 @@ void free_bv(gz::BoruvkaBufs &b) {
 // boruvka_emulation (src/cc_sketch_alg.cpp:464-513) on the sketches at sk with buffers b: the
 // query graph (every round on the device, no host round trip) enqueued on stream s, then the
 // rounds, the out-of-samples flag and the component count copied to pin[0..2] (pinned).
+// The query mode in effect. By size: the one-launch query up to 2^18 vertices (a round's phases
+// are short there, and launches and gaps between them dominated: 0.59 against 0.64 ms at 2^17);
+// the graph of per-phase kernels above (each phase then has work for more resident warps than the
+// cooperative kernel's registers allow: 1.8-2.0 against 2.1-2.2 ms per query at 2^20).
+constexpr uint32_t kOneLaunchQueryMaxV = 1u << 18;
+int query_mode_of(const gz_alg *h) {
+  if (h->query_mode >= 0) return h->query_mode;
+  return h->V <= kOneLaunchQueryMaxV ? 2 : 1;
+}
+
 int boruvka_enqueue(gz_alg *h, gz::BoruvkaGraph &q, const gz::BoruvkaGeom &g, const uint8_t *sk,
                     gz::BoruvkaBufs &b, uint32_t *d_final, uint32_t *d_ncc, uint32_t *pin,
                     cudaStream_t s) {
-  if (h->query_mode == 2) GZ_CUDA(gz::boruvka_query_launch(g, h->samples, sk, b, d_final, d_ncc, s));
-  else if (h->query_mode == 1) GZ_CUDA(gz::boruvka_graph_launch(q, g, h->samples, sk, b, d_final, d_ncc, s));
+  const int mode = query_mode_of(h);
+  if (mode == 2) GZ_CUDA(gz::boruvka_query_launch(g, h->samples, sk, b, d_final, d_ncc, s));
+  else if (mode == 1) GZ_CUDA(gz::boruvka_graph_launch(q, g, h->samples, sk, b, d_final, d_ncc, s));
   else GZ_CUDA(gz::boruvka_host_loop(g, h->samples, sk, b, d_final, d_ncc, pin, s));
   GZ_CUDA(cudaMemcpyAsync(pin, b.ctl, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   GZ_CUDA(cudaMemcpyAsync(pin + 2, d_ncc, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
@@ -988,7 +999,7 @@ int run_boruvka(gz_alg *h) {
                          h->stream));
   h->prof_end(pi, 2);
   GZ_CUDA(cudaStreamSynchronize(h->stream));
-  boruvka_account(h->qgraph, h->h_qpin, h->query_mode == 1);
+  boruvka_account(h->qgraph, h->h_qpin, query_mode_of(h) == 1);
   const uint32_t round = h->h_qpin[0];
   if (h->h_qpin[1]) {
     h->last_rounds = round;
@@ -1407,7 +1418,7 @@ int gz_query_submit(gz_alg_t *h, uint64_t *ticket) {
     }
   }
   const int pi = h->prof_begin();
-  t.graph = h->query_mode == 1;
+  t.graph = query_mode_of(h) == 1;
   int rc = boruvka_enqueue(h, T.graph, h->bgeom(), h->d_sk, T.bv, T.d_final, T.d_ncc, t.pin, h->stream);
   h->prof_end(pi, 2);
   cudaError_t e = cudaSuccess;
@@ -1585,7 +1596,7 @@ int gz_set_pipeline(gz_alg_t *h, int mode) {
 int gz_set_query_graph(gz_alg_t *h, int enable) {
   if (!h) return fail(GZ_ERR_INVALID, "null handle");
   Guard g(h);
-  if (enable < 0 || enable > 2) return fail(GZ_ERR_INVALID, "query mode is 0, 1 or 2");
+  if (enable < -1 || enable > 2) return fail(GZ_ERR_INVALID, "query mode is -1, 0, 1 or 2");
   h->query_mode = enable;
   return GZ_OK;
 }

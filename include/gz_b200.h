@@ -305,11 +305,12 @@ GZ_API int gz_set_tuning(gz_alg_t *alg, uint32_t vertices_per_tile, uint32_t thr
  * staging it in shared memory against updating its buckets in HBM -- is updated in place with
  * global atomics. 0 = always staged, 1 = the default. Same role as gz_batch_set_route. */
 GZ_API int gz_set_direct_factor(gz_alg_t *alg, double factor);
-/* How queries run. mode = 2 (the default): the whole Boruvka emulation in one cooperative kernel
- * launch, every round on the device with grid barriers between its phases. mode = 1: one CUDA
- * graph of per-phase kernels whose conditional while node loops over the rounds. mode = 0: the
- * same per-phase kernels with the round loop on the host (a synchronize per round; ticket submits
- * then wait for their query), for profilers that do not see kernels inside conditional graphs.
+/* How queries run. mode = 2: the whole Boruvka emulation in one cooperative kernel launch, every
+ * round on the device with grid barriers between its phases. mode = 1: one CUDA graph of
+ * per-phase kernels whose conditional while node loops over the rounds. mode = 0: the same
+ * per-phase kernels with the round loop on the host (a synchronize per round; ticket submits then
+ * wait for their query), for profilers that do not see kernels inside conditional graphs.
+ * mode = -1 (the default): 2 up to 2^18 vertices, 1 above (the faster of the two at each size).
  * Answers, rounds and sample traces are the same in every mode. GZ_ERR_INVALID for another mode. */
 GZ_API int gz_set_query_graph(gz_alg_t *alg, int mode);
 /* Sketch-update kernel of a handle: mode 1 = the tile pipeline (a producer warp loads the next

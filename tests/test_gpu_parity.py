@@ -303,7 +303,7 @@ def test_giant_component_merge_paths(gz, oracle_mod, path, tmp_path):
     assert cc.size() == n
 
 
-@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("mode", [0, 1, 2])
 @pytest.mark.parametrize("name", ["c0_v1024", "mult_v1024", "cl_v2048"])
 def test_per_phase_query_modes(gz, name, mode):
     """gz_set_query_graph(1) runs the Boruvka rounds as a CUDA graph of per-phase kernels, (0) the
@@ -326,6 +326,30 @@ def test_per_phase_query_modes(gz, name, mode):
     t = alg.query_submit()
     cc2, rounds = alg.query_wait(t)
     assert (cc2.parent_arr == cc.parent_arr).all() and rounds == c["rounds"]
+
+
+def test_query_modes_past_the_size_switch(gz, oracle_mod):
+    """2^18 + 5 vertices, past the size where the default query switches from the one-launch
+    kernel to the graph of per-phase kernels: both (and the host loop) give the exact partition
+    and the same rounds."""
+    from graphzeppelin_b200 import streams as S
+    V = (1 << 18) + 5
+    rng = np.random.default_rng(41)
+    src = rng.integers(0, V, 600000, dtype=np.uint32)
+    dst = (src + rng.integers(1, 64, src.size, dtype=np.uint32)) % V  # local edges: many components
+    st = S.Stream(V, S.make_records(src, dst))
+    n, exact = oracle_mod.exact_cc(V, st.raw())
+    rounds = set()
+    for mode in (-1, 2, 1, 0):
+        alg = gz.CCSketchAlg(V, 777)
+        alg.set_query_graph(mode)
+        alg.ingest_records(st)
+        cc = alg.connected_components()
+        assert cc.size() == n, mode
+        assert (canonical(cc.parent_arr) == exact).all(), mode
+        rounds.add(alg.last_query_rounds)
+        alg.close()
+    assert len(rounds) == 1
 
 
 @pytest.mark.parametrize("V", [2, 3, 5, 17, 100, 301])
