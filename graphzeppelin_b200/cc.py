@@ -476,7 +476,8 @@ class CCSketchAlg:
     def set_tuning(self, vertices_per_tile: int = 0, threads_per_block: int = 0,
                    tiles_per_bin: int = 0, entry_form: int = 0) -> None:
         """0 keeps defaults; entry_form 1 = plain entries (hashed per endpoint), 2 = coded entries
-        (each record hashed once, applied through bucket planes; gz_set_tuning)."""
+        (each record hashed once, applied through bucket planes), 3 = coded entries with 3-bit
+        depth codes (gz_set_tuning)."""
         _check(self.lib.gz_set_tuning(self._h, vertices_per_tile, threads_per_block,
                                       tiles_per_bin, entry_form))
         p = _lib.gz_params_t()

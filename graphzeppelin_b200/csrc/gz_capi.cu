@@ -150,7 +150,9 @@ struct gz_alg {
   bool symmetric = true;
   // records become coded entries (each record hashed once) applied through bucket planes
   bool planes = false;
-  int planes_mode = -1;         // entry form asked for: -1 automatic, 0 plain, 1 coded
+  bool codes3 = false;          // the coded entries carry 3-bit codes (kEntryCoded3)
+  int planes_mode = -1;         // entry form asked for: -1 automatic, 0 plain, 1 coded (4-bit
+                                // codes where they fit, else 3-bit), 2 coded with 3-bit codes
   gz::PlaneHash ph{};
   gz::ChunkTable chunks{};
   int nchunks = 0;
@@ -352,7 +354,7 @@ constexpr uint32_t kPlaneDefaultMaxV = 1u << 18;
 
 int choose_planes(gz_alg *h, uint32_t vpt_req, uint32_t threads_req, uint32_t tpb_req, bool &done) {
   done = false;
-  const bool asked = h->planes_mode == 1;
+  const bool asked = h->planes_mode >= 1;
   if (h->planes_mode == 0) return GZ_OK;
   if (h->cube || h->C > gz::kPlaneMaxColumns) {
     if (asked) return fail(GZ_ERR_INVALID, "coded entries need CameoSketch with at most 31 columns");
@@ -374,13 +376,17 @@ int choose_planes(gz_alg *h, uint32_t vpt_req, uint32_t threads_req, uint32_t tp
     while (((h->V + (1u << bshift) - 1) >> bshift) > kPlaneBinTarget &&
            (1u << (bshift - shift)) < kPlaneTilesPerBin)
       ++bshift;
+    // large graphs: bins of several tiles, as many as the hash sort's shared memory holds
+    while (((h->V + (1u << bshift) - 1) >> bshift) > gz::kSortBinsMax && bshift < shift + 3) ++bshift;
   }
   const uint32_t nbins = (uint32_t)((h->V + (1u << bshift) - 1) >> bshift);
   if (nbins > gz::kSortBinsMax) {
     if (asked) return fail(GZ_ERR_INVALID, "too many gutter bins for coded entries at this tile size");
     return GZ_OK;
   }
-  if (!gz::coded_entry_fits(h->V, h->C, bshift)) {
+  // 4-bit codes where they fit (unless 3-bit ones are asked for), else 3-bit codes
+  const bool fits4 = h->planes_mode != 2 && gz::coded_entry_fits(h->V, h->C, bshift, 4);
+  if (!fits4 && !gz::coded_entry_fits(h->V, h->C, bshift, 3)) {
     if (asked) return fail(GZ_ERR_INVALID, "the codes of this sketch do not fit a 16-byte coded entry");
     return GZ_OK;
   }
@@ -390,6 +396,7 @@ int choose_planes(gz_alg *h, uint32_t vpt_req, uint32_t threads_req, uint32_t tp
   if (gz::plane_update_smem(shift, (int)threads) > h->smem_optin)
     return fail(GZ_ERR_INVALID, "this tile does not fit in shared memory");
   h->planes = true;
+  h->codes3 = !fits4;
   h->in_place = false;
   h->pipe = false;
   h->threads = threads;
@@ -408,6 +415,7 @@ int choose_tiling(gz_alg *h, uint32_t vpt_req, uint32_t threads_req, uint32_t tp
   if (smem_optin <= 0) smem_optin = 227 * 1024;
   h->smem_optin = (size_t)smem_optin;
   h->planes = false;
+  h->codes3 = false;
   h->threads = 1024;
   {
     bool done = false;
@@ -697,7 +705,8 @@ int gutter_chunk(gz_alg *h, int input, const void *d_in, uint64_t n) {
     if (tile == 0) return fail(GZ_ERR_INVALID, "gutter bins do not fit the hash sort");
     GZ_CUDA(cudaMemsetAsync(h->d_fill, 0, sizeof(uint32_t) * h->nbins, h->stream));
     GZ_CUDA(gz::gutter_hash_sort(d_in, n, gg, h->ph, tile, h->d_hist, h->d_fill,
-                                 reinterpret_cast<uint4 *>(out), h->stream));
+                                 reinterpret_cast<uint4 *>(out),
+                                 h->codes3 ? gz::kEntryCoded3 : gz::kEntryCoded, h->stream));
   } else {
     const uint32_t tile = gz::sort_scatter_tile(input, gg, h->smem_optin - 1024);
     if (tile >= 1024) {
@@ -710,7 +719,7 @@ int gutter_chunk(gz_alg *h, int input, const void *d_in, uint64_t n) {
   }
   h->prof_end(pi, 0);
   h->chunks.base[h->nchunks] = h->gutter_used;
-  h->chunks.kind[h->nchunks] = coded ? gz::kEntryCoded : gz::kEntryPlain;
+  h->chunks.kind[h->nchunks] = !coded ? gz::kEntryPlain : h->codes3 ? gz::kEntryCoded3 : gz::kEntryCoded;
   h->nchunks++;
   h->gutter_used += need;
   h->entries_pending += n_ent;
@@ -1237,7 +1246,7 @@ int gz_get_params(const gz_alg_t *h, gz_params_t *o) {
   o->cols_per_sample = h->cps;
   o->sketch_algorithm = h->cube ? GZ_CUBE_SKETCH : GZ_CAMEO_SKETCH;
   o->in_place = h->in_place ? 1 : 0;
-  o->entry_form = h->planes ? 2 : 1;
+  o->entry_form = h->planes ? (h->codes3 ? 3 : 2) : 1;
   return GZ_OK;
 }
 
@@ -1695,24 +1704,25 @@ int gz_get_stream(gz_alg_t *h, void **s) {
 int gz_set_tuning(gz_alg_t *h, uint32_t vpt, uint32_t threads, uint32_t tiles_per_bin,
                   uint32_t entry_form) {
   if (!h) return fail(GZ_ERR_INVALID, "null handle");
-  if (entry_form > 2) return fail(GZ_ERR_INVALID, "entry_form must be 0, 1 or 2");
-  if (entry_form == 2 && (h->C > gz::kPlaneMaxColumns || h->cube))
+  if (entry_form > 3) return fail(GZ_ERR_INVALID, "entry_form must be 0, 1, 2 or 3");
+  if (entry_form >= 2 && (h->C > gz::kPlaneMaxColumns || h->cube))
     return fail(GZ_ERR_INVALID, "coded entries need CameoSketch with at most 31 columns");
-  if (h->in_place && (vpt || threads || tiles_per_bin || entry_form == 2))
+  if (h->in_place && (vpt || threads || tiles_per_bin || entry_form >= 2))
     return fail(GZ_ERR_INVALID, "this handle updates its sketches in place: there are no tiles to tune");
   Guard g(h);
   GZ_TRY(push_staged_entries(h));
   GZ_TRY(apply_pending(h));
   GZ_CUDA(cudaStreamSynchronize(h->stream));
   const int keep_mode = h->planes_mode;
-  const bool keep_planes = h->planes, keep_pipe = h->pipe;
+  const bool keep_planes = h->planes, keep_pipe = h->pipe, keep_codes3 = h->codes3;
   const uint32_t keep[5] = {h->tile_shift, h->ntiles, h->bin_shift, h->nbins, h->threads};
-  h->planes_mode = entry_form == 0 ? -1 : (entry_form == 2 ? 1 : 0);
+  h->planes_mode = entry_form == 0 ? -1 : (int)entry_form - 1;
   const uint32_t old_nb = h->nbins;
   const int rc = choose_tiling(h, vpt, threads, tiles_per_bin);
   if (rc != GZ_OK) {
     h->planes_mode = keep_mode;
     h->planes = keep_planes;
+    h->codes3 = keep_codes3;
     h->pipe = keep_pipe;
     h->tile_shift = keep[0];
     h->ntiles = keep[1];

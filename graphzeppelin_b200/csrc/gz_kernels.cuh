@@ -35,13 +35,20 @@ enum EntryKind : uint8_t {
   kEntryCoded = 1,   // 128 bits: the 4-bit depth codes of all C columns, computed once per
                      // record (column c in bits 4c .. 4c + 3), then from bit 4C the neighbour
                      // shifted left by bin_shift OR the vertex's offset inside its gutter bin
+  kEntryCoded3 = 2,  // the same with 3-bit codes (column c in bits 3c .. 3c + 2; the payload from
+                     // bit 3C): code 7 = "7 or more", recomputed where the entry is applied
 };
 constexpr uint32_t kDepthEscape = 15;  // depth code for "15 or more"
-// Whether coded entries hold the codes of C columns for V vertices in bins of 2^bin_shift.
-inline bool coded_entry_fits(uint32_t V, uint32_t C, uint32_t bin_shift) {
+constexpr uint32_t kDepthEscape3 = 7;  // 3-bit depth code for "7 or more"
+inline uint32_t neighbour_bits(uint32_t V) {
   uint32_t ubits = 1;
   while (ubits < 32 && (1ull << ubits) < V) ++ubits;  // bits of a neighbour id (< V)
-  return C >= 18 && 4 * C + bin_shift + ubits <= 128;
+  return ubits;
+}
+// Whether coded entries hold the codes of C columns for V vertices in bins of 2^bin_shift
+// (code_bits = 4 or 3).
+inline bool coded_entry_fits(uint32_t V, uint32_t C, uint32_t bin_shift, uint32_t code_bits = 4) {
+  return C >= 18 && code_bits * C + bin_shift + neighbour_bits(V) <= 128;
 }
 struct ChunkTable {
   uint64_t base[kMaxChunks];  // byte offset of the chunk's entries in the gutter buffer
@@ -128,11 +135,10 @@ PlaneHash plane_hash(uint64_t seed, uint32_t C, uint32_t B);
 uint32_t hash_sort_tile(uint32_t nbins, size_t smem_budget);
 // Hash every record once (all C columns) and write its two coded endpoint entries,
 // counting-sorted by bin, to entries[base[b] + ...]; fill (nbins u32) starts at zero.
+// kind = kEntryCoded or kEntryCoded3.
 cudaError_t gutter_hash_sort(const void *d_rec, uint64_t n, GutterGeom g, const PlaneHash &ph,
                              uint32_t rec_tile, const uint64_t *base, uint32_t *fill,
-                             uint4 *entries, cudaStream_t s);
-// Threads per CTA of the hash sort-scatter (1024: one CTA per SM; 512: two), process-wide.
-void set_hash_sort_threads(int threads);
+                             uint4 *entries, uint32_t kind, cudaStream_t s);
 // Applies every buffered chunk (coded or plain entries) tile by tile through bucket planes.
 size_t plane_update_smem(uint32_t tile_shift, int threads);
 int plane_update_ctas_per_sm(uint32_t tile_shift, int threads);

@@ -8,7 +8,8 @@
 //
 //   k_hash_sort_scatter  per tile of records: the two endpoint entries counting-sorted by gutter
 //                        bin in shared memory, each record's C column depths hashed once into
-//                        4-bit codes carried by both entries, the runs written out coalesced.
+//                        4-bit (or 3-bit) codes carried by both entries, the runs written out
+//                        coalesced.
 //   k_plane_update       per tile of W vertices: the tile's entries (filtered out of their gutter
 //                        bin when a bin holds several tiles) XORed into bucket planes in shared
 //                        memory that start at zero, then each vertex's rows XORed into its sketch
@@ -16,7 +17,10 @@
 // A coded entry is 128 bits: the C codes in bits 0 .. 4C - 1 (column c in bits 4c .. 4c + 3),
 // then the neighbour shifted left by bin_shift bits OR the vertex's offset inside its gutter bin
 // (the bin is known from where the entry lies). It is used when 4C + bin_shift + the neighbour's
-// bits fit in 128 (every CameoSketch up to 2^18 vertices).
+// bits fit in 128 (every CameoSketch up to 2^18 vertices). Past that, codes of 3 bits (code 7 =
+// depth 7 or more) fit larger graphs (3C + bin_shift + neighbour bits <= 128: 2^20 vertices and
+// far beyond); an escaped column (1 in 128 column updates) is hashed again where the entry is
+// applied, so the planes see the same 4-bit codes either way.
 //
 // Bucket planes. A warp takes 32 entries, one per lane. At step t = 0..31 lane l handles slot
 // l ^ t of its entry: slot c < C is column c, slot C the deterministic bucket, higher slots are
@@ -39,6 +43,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <type_traits>
 
 #include "gz_common.cuh"
 #include "gz_device.cuh"
@@ -99,6 +104,81 @@ __device__ __forceinline__ void unpack_entry(uint4 e, uint32_t bin, uint32_t C, 
   w[3] = (uint32_t)(codes_hi >> 32);
 }
 
+// 3-bit codes (kEntryCoded3). Eight nibbles holding values <= 7 <-> their low 3 bits packed into
+// 24 bits (nibble k at bits 3k .. 3k + 2), in three steps of pairs.
+__device__ __forceinline__ uint32_t squeeze3(uint32_t w) {
+  w = (w & 0x07070707u) | ((w >> 1) & 0x38383838u);
+  w = (w & 0x003f003fu) | ((w >> 2) & 0x0fc00fc0u);
+  return (w & 0x00000fffu) | ((w >> 4) & 0x00fff000u);
+}
+__device__ __forceinline__ uint32_t spread3(uint32_t x) {
+  x = (x & 0x00000fffu) | ((x << 4) & 0x0fff0000u);
+  x = (x & 0x003f003fu) | ((x << 2) & 0x3f003f00u);
+  return (x & 0x07070707u) | ((x << 1) & 0x70707070u);
+}
+
+// Coded entry with 3-bit codes of vertex a (neighbour b): codes (each <= 7, as nibbles in w) in
+// bits 0 .. 3C - 1, then from bit 3C the payload (b << bin_shift) | (a & bin mask). 3C >= 54.
+__device__ __forceinline__ uint4 pack_entry3(const uint32_t (&w)[4], uint32_t a, uint32_t b,
+                                             uint32_t C, uint32_t bin_shift) {
+  const uint64_t z2 = squeeze3(w[2]);
+  uint64_t lo = (uint64_t)squeeze3(w[0]) | ((uint64_t)squeeze3(w[1]) << 24) | (z2 << 48);
+  uint64_t hi = (z2 >> 16) | ((uint64_t)squeeze3(w[3]) << 8);
+  const uint64_t pay = ((uint64_t)b << bin_shift) | (a & ((1u << bin_shift) - 1u));
+  const uint32_t sh = 3 * C;
+  if (sh >= 64) {
+    hi |= pay << (sh - 64);
+  } else {
+    lo |= pay << sh;
+    hi |= pay >> (64 - sh);
+  }
+  return make_uint4((uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi, (uint32_t)(hi >> 32));
+}
+
+// Payload (bits from 3C on) of a 3-bit coded entry.
+__device__ __forceinline__ uint64_t payload3(uint4 e, uint32_t C) {
+  const uint64_t lo = ((uint64_t)e.y << 32) | e.x, hi = ((uint64_t)e.w << 32) | e.z;
+  const uint32_t sh = 3 * C;
+  return sh >= 64 ? hi >> (sh - 64) : (lo >> sh) | (hi << (64 - sh));
+}
+
+// Vertex, neighbour and codes (as nibbles, escapes = 7 left in place) of a 3-bit coded entry
+// lying in gutter bin `bin`.
+__device__ __forceinline__ void unpack_entry3(uint4 e, uint32_t bin, uint32_t C, uint32_t bin_shift,
+                                              uint32_t &v, uint32_t &u, uint32_t (&w)[4]) {
+  uint64_t lo = ((uint64_t)e.y << 32) | e.x, hi = ((uint64_t)e.w << 32) | e.z;
+  const uint32_t sh = 3 * C;
+  const uint64_t pay = sh >= 64 ? hi >> (sh - 64) : (lo >> sh) | (hi << (64 - sh));
+  v = (bin << bin_shift) | ((uint32_t)pay & ((1u << bin_shift) - 1u));
+  u = (uint32_t)(pay >> bin_shift);
+  if (sh >= 64) {
+    hi &= (1ull << (sh - 64)) - 1ull;
+  } else {
+    lo &= (1ull << sh) - 1ull;
+    hi = 0;
+  }
+  w[0] = spread3((uint32_t)lo & 0xffffffu);
+  w[1] = spread3((uint32_t)(lo >> 24) & 0xffffffu);
+  w[2] = spread3((uint32_t)((lo >> 48) | (hi << 16)) & 0xffffffu);
+  w[3] = spread3((uint32_t)(hi >> 8) & 0xffffffu);
+}
+
+// The 4-bit codes of a 3-bit coded entry: every escaped column (code 7: depth 7 or more) hashed
+// again for min(depth, 15). Out of line: about one entry in five at 28 columns has an escape.
+__device__ __noinline__ uint4 fix_escapes3(uint4 w4, uint64_t pm, const uint64_t *kcol, uint32_t cap) {
+  uint32_t w[4] = {w4.x, w4.y, w4.z, w4.w};
+#pragma unroll
+  for (int g = 0; g < 4; ++g) {
+    // nibbles <= 7: adding 1 carries into bit 3 of a nibble exactly when it is 7
+    for (uint32_t f = (w[g] + 0x11111111u) & 0x88888888u; f; f &= f - 1) {
+      const uint32_t k = (__ffs(f) - 1) >> 2;  // nibble index in the word
+      const uint32_t code = depth_code(pm ^ kcol[8 * g + k], cap);
+      w[g] = (w[g] & ~(15u << (4 * k))) | (code << (4 * k));
+    }
+  }
+  return make_uint4(w[0], w[1], w[2], w[3]);
+}
+
 // ------------------------------------------------------------------------------------------------
 // hash sort-scatter (records in, coded entries out)
 // ------------------------------------------------------------------------------------------------
@@ -134,7 +214,8 @@ __device__ __forceinline__ uint32_t block_scan(uint32_t x, uint32_t *ws /*32*/) 
   return r;
 }
 
-template <int RPT, int NT>
+// C3: 3-bit codes (kEntryCoded3), else 4-bit (kEntryCoded).
+template <int RPT, int NT, bool C3>
 __global__ void __launch_bounds__(NT, 1024 / NT)
 k_hash_sort_scatter(const uint8_t *__restrict__ rec, uint64_t n, GutterGeom g, PlaneHash ph,
                     uint32_t rec_tile, const uint64_t *__restrict__ base,
@@ -150,7 +231,7 @@ k_hash_sort_scatter(const uint8_t *__restrict__ rec, uint64_t n, GutterGeom g, P
   // entry is placed, and the next tile is staged only after the write-out
   uint8_t *s_rec = reinterpret_cast<uint8_t *>(s_ent);
   const uint32_t per_thread = (nb + NT - 1) / NT;  // bins per thread
-  const uint32_t cap = 1u << min(ph.B, kDepthEscape);
+  const uint32_t cap = 1u << min(ph.B, C3 ? kDepthEscape3 : kDepthEscape);
   for (uint64_t t0 = blockIdx.x * (uint64_t)rec_tile; t0 < n; t0 += (uint64_t)gridDim.x * rec_tile) {
     const uint32_t cnt = (uint32_t)(n - t0 < rec_tile ? n - t0 : rec_tile);
     for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) s_cur[b] = 0u;
@@ -207,8 +288,10 @@ k_hash_sort_scatter(const uint8_t *__restrict__ rec, uint64_t n, GutterGeom g, P
         const uint64_t pm = xxh3_premix(((uint64_t)lo << 32) | hi);
         uint32_t w[4];
         all_codes(pm, ph.kcol, ph.C, cap, w);
-        s_ent[pu[k]] = pack_entry(w, ru[k], rv[k], ph.C, g.bin_shift);
-        s_ent[pv[k]] = pack_entry(w, rv[k], ru[k], ph.C, g.bin_shift);
+        s_ent[pu[k]] = C3 ? pack_entry3(w, ru[k], rv[k], ph.C, g.bin_shift)
+                          : pack_entry(w, ru[k], rv[k], ph.C, g.bin_shift);
+        s_ent[pv[k]] = C3 ? pack_entry3(w, rv[k], ru[k], ph.C, g.bin_shift)
+                          : pack_entry(w, rv[k], ru[k], ph.C, g.bin_shift);
         s_bin[pu[k]] = (uint16_t)(ru[k] >> g.bin_shift);
         s_bin[pv[k]] = (uint16_t)(rv[k] >> g.bin_shift);
       }
@@ -312,18 +395,31 @@ __device__ __noinline__ uint4 plain_codes(uint64_t pm, const uint64_t *kcol, uin
   return make_uint4(w[0], w[1], w[2], w[3]);
 }
 
-// Vertex, neighbour and codes of a gutter entry of bin `bin`: unpacked from a coded entry, or
-// hashed here for a plain {vertex, neighbour} entry (apply_update_batch).
-__device__ __forceinline__ void decode_entry(uint4 e, bool coded, uint32_t bin, const PlaneCtx &x,
+// Vertex, neighbour and 4-bit codes of a gutter entry (kind) of bin `bin`: unpacked from a coded
+// entry (3-bit codes: escapes hashed again), or hashed here for a plain {vertex, neighbour} entry
+// (apply_update_batch).
+__device__ __forceinline__ void decode_entry(uint4 e, uint32_t kind, uint32_t bin, const PlaneCtx &x,
                                              uint32_t &v, uint32_t &u, uint64_t &pm, uint32_t (&c4)[4]) {
-  if (coded) {
+  if (kind == kEntryCoded) {
     unpack_entry(e, bin, x.C, x.bin_shift, v, u, c4);
+  } else if (kind == kEntryCoded3) {
+    unpack_entry3(e, bin, x.C, x.bin_shift, v, u, c4);
   } else {
     v = e.x;
     u = e.y;
   }
   pm = xxh3_premix(((uint64_t)max(u, v) << 32) | min(u, v));  // idx = (min << 32) | max
-  if (!coded) {
+  if (kind == kEntryCoded3) {
+    const uint32_t esc = ((c4[0] + 0x11111111u) | (c4[1] + 0x11111111u) | (c4[2] + 0x11111111u) |
+                          (c4[3] + 0x11111111u)) & 0x88888888u;
+    if (esc) {
+      const uint4 w = fix_escapes3(make_uint4(c4[0], c4[1], c4[2], c4[3]), pm, x.s_kcol, x.cap);
+      c4[0] = w.x;
+      c4[1] = w.y;
+      c4[2] = w.z;
+      c4[3] = w.w;
+    }
+  } else if (kind == kEntryPlain) {
     const uint4 w = plain_codes(pm, x.s_kcol, x.C, x.cap);
     c4[0] = w.x;
     c4[1] = w.y;
@@ -333,18 +429,19 @@ __device__ __forceinline__ void decode_entry(uint4 e, bool coded, uint32_t bin, 
 }
 
 // Vertex of a gutter entry of bin `bin` (for filtering a bin's entries by tile).
-__device__ __forceinline__ uint32_t entry_vertex(uint4 e, bool coded, uint32_t bin, const PlaneCtx &x) {
-  if (!coded) return e.x;
-  const uint64_t hi = ((uint64_t)e.w << 32) | e.z;
-  return (bin << x.bin_shift) | ((uint32_t)(hi >> (4 * x.C - 64)) & ((1u << x.bin_shift) - 1u));
+__device__ __forceinline__ uint32_t entry_vertex(uint4 e, uint32_t kind, uint32_t bin, const PlaneCtx &x) {
+  if (kind == kEntryPlain) return e.x;
+  const uint64_t pay = kind == kEntryCoded3 ? payload3(e, x.C)
+                                            : (((uint64_t)e.w << 32) | e.z) >> (4 * x.C - 64);
+  return (bin << x.bin_shift) | ((uint32_t)pay & ((1u << x.bin_shift) - 1u));
 }
 
 // One entry per lane into the tile's planes (invalid lanes XOR zeros into vertex 0 of the tile).
-__device__ __forceinline__ void plane_entry(uint4 e, bool coded, bool valid, uint32_t bin,
+__device__ __forceinline__ void plane_entry(uint4 e, uint32_t kind, bool valid, uint32_t bin,
                                             uint32_t lane, const PlaneCtx &x) {
   uint32_t v, u, c4[4];
   uint64_t pm;
-  decode_entry(e, coded, bin, x, v, u, pm, c4);
+  decode_entry(e, kind, bin, x, v, u, pm, c4);
   const uint32_t lo = max(u, v), hi = min(u, v);
   const uint32_t chk = valid ? tail_lo32(pm ^ x.kchk) : 0u;
   const uint32_t val = valid ? (u | 0x80000000u) : 0u;
@@ -385,11 +482,11 @@ __device__ __forceinline__ void plane_entry(uint4 e, bool coded, bool valid, uin
 }
 
 // One entry applied straight to HBM (sparse tiles): deterministic bucket, then each column.
-__device__ __forceinline__ void entry_in_place(uint4 e, bool coded, uint32_t bin, uint32_t tile,
+__device__ __forceinline__ void entry_in_place(uint4 e, uint32_t kind, uint32_t bin, uint32_t tile,
                                                uint32_t tile_shift, const PlaneCtx &x) {
   uint32_t v, u, c4[4];
   uint64_t pm;
-  decode_entry(e, coded, bin, x, v, u, pm, c4);
+  decode_entry(e, kind, bin, x, v, u, pm, c4);
   if ((v >> tile_shift) != tile) return;
   const uint32_t lo = max(u, v), hi = min(u, v);
   const uint32_t chk = tail_lo32(pm ^ x.kchk);
@@ -402,8 +499,8 @@ __device__ __forceinline__ void entry_in_place(uint4 e, bool coded, uint32_t bin
   }
 }
 
-__device__ __forceinline__ uint4 load_entry(const uint8_t *cb, bool coded, uint32_t i) {
-  if (coded) return reinterpret_cast<const uint4 *>(cb)[i];
+__device__ __forceinline__ uint4 load_entry(const uint8_t *cb, uint32_t kind, uint32_t i) {
+  if (kind != kEntryPlain) return reinterpret_cast<const uint4 *>(cb)[i];
   const uint2 k = reinterpret_cast<const uint2 *>(cb)[i];
   return make_uint4(k.x, k.y, 0, 0);
 }
@@ -462,9 +559,9 @@ k_plane_update(PlaneGeom g, PlaneHash ph, uint8_t *__restrict__ sketches,
       for (int k = 0; k < nchunks; ++k) {
         const uint32_t b = bin_off[(uint64_t)k * stride + bin], e = bin_off[(uint64_t)k * stride + bin + 1];
         const uint8_t *cb = gutter + chunks.base[k];
-        const bool coded = chunks.kind[k] == kEntryCoded;
+        const uint32_t kind = chunks.kind[k];
         for (uint32_t i = b + threadIdx.x; i < e; i += blockDim.x)
-          entry_in_place(load_entry(cb, coded, i), coded, bin, t, g.tile_shift, x);
+          entry_in_place(load_entry(cb, kind, i), kind, bin, t, g.tile_shift, x);
       }
       __syncthreads();
       continue;
@@ -480,11 +577,11 @@ k_plane_update(PlaneGeom g, PlaneHash ph, uint8_t *__restrict__ sketches,
     for (int k = 0; k < nchunks; ++k) {
       const uint32_t b = bin_off[(uint64_t)k * stride + bin], e = bin_off[(uint64_t)k * stride + bin + 1];
       const uint8_t *cb = gutter + chunks.base[k];
-      const bool coded = chunks.kind[k] == kEntryCoded;
+      const uint32_t kind = chunks.kind[k];
       // each warp takes groups of 32 entries; the next group is loaded while this one is used
       uint32_t i0 = b + warp * 32;
       bool nvalid = i0 + lane < e;
-      uint4 nx = nvalid ? load_entry(cb, coded, i0 + lane) : pad_entry;
+      uint4 nx = nvalid ? load_entry(cb, kind, i0 + lane) : pad_entry;
       if (per_bin == 0) {
         // the bin is this tile: every entry applies
         for (; i0 < e; i0 += nwarps * 32) {
@@ -492,8 +589,8 @@ k_plane_update(PlaneGeom g, PlaneHash ph, uint8_t *__restrict__ sketches,
           const bool valid = nvalid;
           const uint32_t in = i0 + nwarps * 32 + lane;
           nvalid = in < e;
-          if (nvalid) nx = load_entry(cb, coded, in);
-          plane_entry(en, coded, valid, bin, lane, x);
+          if (nvalid) nx = load_entry(cb, kind, in);
+          plane_entry(en, kind, valid, bin, lane, x);
         }
       } else {
         // the bin holds several tiles: each warp ballots its group, queues this tile's entries,
@@ -502,15 +599,15 @@ k_plane_update(PlaneGeom g, PlaneHash ph, uint8_t *__restrict__ sketches,
         uint32_t qn = 0;
         const uint32_t step = nwarps * 32;
         bool nvalid2 = i0 + step + lane < e;
-        uint4 nx2 = nvalid2 ? load_entry(cb, coded, i0 + step + lane) : pad_entry;
+        uint4 nx2 = nvalid2 ? load_entry(cb, kind, i0 + step + lane) : pad_entry;
         for (; i0 < e; i0 += step) {
           const uint4 en = nx;
-          const bool mine = nvalid && (entry_vertex(en, coded, bin, x) >> g.tile_shift) == t;
+          const bool mine = nvalid && (entry_vertex(en, kind, bin, x) >> g.tile_shift) == t;
           nx = nx2;
           nvalid = nvalid2;
           const uint32_t in = i0 + 2 * step + lane;
           nvalid2 = in < e;
-          if (nvalid2) nx2 = load_entry(cb, coded, in);
+          if (nvalid2) nx2 = load_entry(cb, kind, in);
           const uint32_t m = __ballot_sync(kFull, mine);
           if (mine) queue[qn + __popc(m & ((1u << lane) - 1u))] = en;
           qn += __popc(m);
@@ -521,20 +618,23 @@ k_plane_update(PlaneGeom g, PlaneHash ph, uint8_t *__restrict__ sketches,
             qn -= 32;
             if (lane < qn) queue[lane] = queue[32 + lane];
             __syncwarp();
-            plane_entry(q, coded, true, bin, lane, x);
+            plane_entry(q, kind, true, bin, lane, x);
           }
         }
         const bool valid = lane < qn;
         const uint4 q = valid ? queue[lane] : pad_entry;
         __syncwarp();
-        if (qn) plane_entry(q, coded, valid, bin, lane, x);
+        if (qn) plane_entry(q, kind, valid, bin, lane, x);
       }
     }
     __syncthreads();
-    // write-back: one warp per vertex; rows [r0, r0 + 4) of every slot are converted to the
-    // reference bucket words (lanes = slots, conflict-free), staged with an odd stride, and XORed
-    // into the sketch in HBM column run by column run
+    // write-back: one warp per vertex. The words of rows 0 .. R - 1 of every column (one run of
+    // 3R words per column in the sketch) are taken as one list: word i of the list is column
+    // i / 3R, row (i % 3R) / 3, word (i % 3R) % 3 of the bucket, converted from the planes, and
+    // XORed into the sketch in HBM where it is not zero. Lane l takes words l, l + 32, ... (runs of
+    // consecutive words: coalesced), eight read-modify-writes in flight at a time.
     const uint32_t R = min(B, kPlaneThr);
+    const uint32_t runw = 3 * R, nwl = C * runw;
     for (uint32_t vl = warp; vl < W; vl += nwarps) {
       const uint32_t vg = (t << g.tile_shift) + vl;
       if (vg >= g.V) continue;
@@ -542,33 +642,42 @@ k_plane_update(PlaneGeom g, PlaneHash ph, uint8_t *__restrict__ sketches,
       const uint32_t *pb = pa + kPlaneRows * kPlaneSlots;
       const uint32_t *pg = pb + kPlaneRows * kPlaneSlots;
       uint32_t *sk = x.gsk + (uint64_t)vg * g.sketch_words;
-      for (uint32_t r0 = 0; r0 < R; r0 += kWbRows) {
-        const uint32_t nr = min(kWbRows, R - r0);
-        for (uint32_t rr = 0; rr < nr; ++rr) {
-          const uint32_t r = r0 + rr;
-          const uint32_t a = pa[r * kPlaneSlots + lane], bq = pb[r * kPlaneSlots + lane];
-          const uint32_t gm = pg[r * kPlaneSlots + lane];
-          wbuf[lane * kWbStride + rr * 3 + 0] = (a & 0x7fffffffu) ^ ((bq >> 31) ? vg : 0u);
-          wbuf[lane * kWbStride + rr * 3 + 1] = (bq & 0x7fffffffu) ^ ((a >> 31) ? vg : 0u);
-          wbuf[lane * kWbStride + rr * 3 + 2] = gm;
-        }
-        __syncwarp();
-        const uint32_t nw = 3 * nr, j = lane & 15u;
-        if (j < nw) {
-#pragma unroll 4
-          for (uint32_t c = lane >> 4; c < C; c += 2) {
-            const uint32_t y = wbuf[c * kWbStride + j];
-            if (y) {
-              uint32_t *q = sk + 3 * (c * B + r0) + j;
-              *q ^= y;
-            }
+      // word (c, w) of lane l's current list position; w < runw
+      uint32_t c = 0, w = lane;
+      while (w >= runw) {
+        w -= runw;
+        ++c;
+      }
+      auto word = [&](uint32_t cc, uint32_t ww) -> uint32_t {
+        const uint32_t r = (ww * 0xAAABu) >> 17;  // ww / 3 for ww < 2^15
+        const uint32_t s = r * kPlaneSlots + cc, kk = ww - 3 * r;
+        const uint32_t a = pa[s], bq = pb[s];
+        return kk == 0 ? (a & 0x7fffffffu) ^ ((bq >> 31) ? vg : 0u)
+             : kk == 1 ? (bq & 0x7fffffffu) ^ ((a >> 31) ? vg : 0u) : pg[s];
+      };
+      for (uint32_t i0 = 0; i0 < nwl; i0 += 8 * 32) {
+        uint32_t y[8], old[8], off[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const bool in = i0 + k * 32 + lane < nwl;
+          y[k] = in ? word(c, w) : 0u;
+          off[k] = 3 * c * B + w;
+          old[k] = y[k] ? sk[off[k]] : 0u;
+          w += 32;
+          while (w >= runw) {
+            w -= runw;
+            ++c;
           }
         }
-        if (r0 == 0 && lane < 3) {  // deterministic bucket: slot C, row 0
-          const uint32_t y = wbuf[C * kWbStride + lane];
-          if (y) sk[3 * C * B + lane] ^= y;
-        }
-        __syncwarp();
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+          if (y[k]) sk[off[k]] = old[k] ^ y[k];
+      }
+      if (lane < 3) {  // deterministic bucket: slot C, row 0
+        const uint32_t a = pa[C], bq = pb[C];
+        const uint32_t y = lane == 0 ? (a & 0x7fffffffu) ^ ((bq >> 31) ? vg : 0u)
+                         : lane == 1 ? (bq & 0x7fffffffu) ^ ((a >> 31) ? vg : 0u) : pg[C];
+        if (y) sk[3 * C * B + lane] ^= y;
       }
     }
     __syncthreads();
@@ -657,62 +766,49 @@ PlaneHash plane_hash(uint64_t seed, uint32_t C, uint32_t B) {
 }
 
 constexpr int kHashSortMaxRpt = 6;
-// Threads per CTA of the hash sort-scatter: one CTA of 1024 per SM, or two of 512 (each with half
-// the shared memory), whose phases then overlap.
-int g_hash_sort_threads = 1024;
+constexpr int kHashSortThreads = 1024;  // one CTA per SM (every register of the SM)
 
 uint32_t hash_sort_tile(uint32_t nbins, size_t smem_budget) {
-  const int nt = g_hash_sort_threads;
-  const size_t budget = nt == 1024 ? smem_budget : std::min<size_t>(smem_budget, (228 * 1024 - 2 * 1024) / 2);
+  const int nt = kHashSortThreads;
   const size_t fixed = (size_t)2 * ((nbins + 3) & ~3u) * 4 + 256;
-  if (nbins > kSortBinsMax || fixed >= budget) return 0;
+  if (nbins > kSortBinsMax || fixed >= smem_budget) return 0;
   // 2 coded entries of 16 B per record, and their 2-byte bins
-  const size_t t = std::min<size_t>((budget - fixed) / 36, (size_t)kHashSortMaxRpt * nt);
+  const size_t t = std::min<size_t>((smem_budget - fixed) / 36, (size_t)kHashSortMaxRpt * nt);
   return (uint32_t)(t / nt * nt);
 }
 
 cudaError_t gutter_hash_sort(const void *d_rec, uint64_t n, GutterGeom g, const PlaneHash &ph,
                              uint32_t rec_tile, const uint64_t *base, uint32_t *fill,
-                             uint4 *entries, cudaStream_t s) {
+                             uint4 *entries, uint32_t kind, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
-  const int nt = g_hash_sort_threads;
-  if (rec_tile < (uint32_t)nt || rec_tile > (uint32_t)(kHashSortMaxRpt * nt) || rec_tile % nt)
+  constexpr int NT = kHashSortThreads;
+  if (rec_tile < (uint32_t)NT || rec_tile > (uint32_t)(kHashSortMaxRpt * NT) || rec_tile % NT ||
+      (kind != kEntryCoded && kind != kEntryCoded3))
     return cudaErrorInvalidValue;
   const size_t smem = (size_t)2 * ((g.nbins + 3) & ~3u) * 4 + (size_t)rec_tile * 36;
   const uint64_t tiles = (n + rec_tile - 1) / rec_tile;
   const uint8_t *rec = reinterpret_cast<const uint8_t *>(d_rec);
-  auto launch = [&](auto kern, int threads) -> cudaError_t {
+  auto launch = [&](auto kern) -> cudaError_t {
     cudaError_t e = smem_optin(kern);
     if (e != cudaSuccess) return e;
-    int per_sm = 1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess || per_sm < 1)
-      per_sm = 1;
-    const int G = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)num_sms() * per_sm, tiles));
-    kern<<<G, threads, smem, s>>>(rec, n, g, ph, rec_tile, base, fill, entries);
+    const int G = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)num_sms(), tiles));
+    kern<<<G, NT, smem, s>>>(rec, n, g, ph, rec_tile, base, fill, entries);
     add_launches(1);
     return cudaGetLastError();
   };
-  if (nt == 512) {
-    switch (rec_tile / 512) {
-      case 1: return launch(k_hash_sort_scatter<1, 512>, 512);
-      case 2: return launch(k_hash_sort_scatter<2, 512>, 512);
-      case 3: return launch(k_hash_sort_scatter<3, 512>, 512);
-      case 4: return launch(k_hash_sort_scatter<4, 512>, 512);
-      case 5: return launch(k_hash_sort_scatter<5, 512>, 512);
-      default: return launch(k_hash_sort_scatter<6, 512>, 512);
+  auto by_rpt = [&](auto c3) -> cudaError_t {
+    constexpr bool K = decltype(c3)::value;
+    switch (rec_tile / NT) {
+      case 1: return launch(k_hash_sort_scatter<1, NT, K>);
+      case 2: return launch(k_hash_sort_scatter<2, NT, K>);
+      case 3: return launch(k_hash_sort_scatter<3, NT, K>);
+      case 4: return launch(k_hash_sort_scatter<4, NT, K>);
+      case 5: return launch(k_hash_sort_scatter<5, NT, K>);
+      default: return launch(k_hash_sort_scatter<6, NT, K>);
     }
-  }
-  switch (rec_tile / 1024) {
-    case 1: return launch(k_hash_sort_scatter<1, 1024>, 1024);
-    case 2: return launch(k_hash_sort_scatter<2, 1024>, 1024);
-    case 3: return launch(k_hash_sort_scatter<3, 1024>, 1024);
-    case 4: return launch(k_hash_sort_scatter<4, 1024>, 1024);
-    case 5: return launch(k_hash_sort_scatter<5, 1024>, 1024);
-    default: return launch(k_hash_sort_scatter<6, 1024>, 1024);
-  }
+  };
+  return kind == kEntryCoded3 ? by_rpt(std::true_type{}) : by_rpt(std::false_type{});
 }
-
-void set_hash_sort_threads(int threads) { g_hash_sort_threads = threads == 512 ? 512 : 1024; }
 
 size_t plane_update_smem(uint32_t tile_shift, int threads) {
   return 128 + ((size_t)kVertBytes << tile_shift) + (size_t)(threads / 32) * kWbWords * 4;

@@ -81,7 +81,8 @@ typedef struct gz_params {
   uint32_t sketch_algorithm;    /* enum gz_sketch_algorithm */
   uint32_t in_place;            /* 1: sketches too large to stage in shared memory are updated in HBM */
   uint32_t entry_form;          /* gutter entries of records: 1 = plain (hashed per endpoint where
-                                   applied), 2 = coded (each record hashed once, bucket planes) */
+                                   applied), 2 = coded (each record hashed once, bucket planes),
+                                   3 = coded with 3-bit depth codes (larger graphs) */
 } gz_params_t;
 
 /* One sampled component of one Boruvka round (parity tracing). key = smallest member id. */
@@ -296,8 +297,9 @@ GZ_API int gz_measure_update_rate(int repeats, double *updates_per_s);
  * gutter entry form for records: 1 = plain entries {vertex, neighbour} (hashed per endpoint by a
  * staged-tile sketch-update kernel), 2 = coded entries (each record hashed once in the gutter into
  * per-column depth codes, applied through bucket planes; CameoSketch with at most 31 columns and
- * at most 8192 gutter bins). 0 picks coded entries where they apply. Buffered updates are applied
- * first. */
+ * at most 8192 gutter bins; 4-bit codes where they fit a 16-byte entry, else 3-bit codes),
+ * 3 = coded entries with 3-bit codes (code 7 = depth 7 or more, hashed again where applied).
+ * 0 picks coded entries where they apply. Buffered updates are applied first. */
 GZ_API int gz_set_tuning(gz_alg_t *alg, uint32_t vertices_per_tile, uint32_t threads_per_block,
                          uint32_t tiles_per_bin, uint32_t entry_form);
 /* Route of sparse tiles (one tile per gutter bin, plain CameoSketch entries): a tile holding

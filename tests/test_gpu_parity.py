@@ -21,7 +21,7 @@ def _header(seed, V, factor):
             + np.array([factor], "<f8").tobytes())
 
 
-@pytest.mark.parametrize("form", [1, 2])
+@pytest.mark.parametrize("form", [1, 2, 3])
 @pytest.mark.parametrize("name", case_names())
 def test_golden_case_bit_exact(gz, name, form, tmp_path):
     c, st, labels, trace = load_case(name)

@@ -50,7 +50,7 @@ def test_default_entry_form(gz):
     assert a.params.entry_form == 2
 
 
-@pytest.mark.parametrize("form", [1, 2])
+@pytest.mark.parametrize("form", [1, 2, 3])
 def test_reference_stream_fixture_with_queries(gz, oracle_mod, form):
     """The reference's test/res/multiples_graph_1024_stream.data, unchanged, as its
     MTStreamWithMultipleQueries test reads it (test/cc_alg_test.cpp:300-350): a query after each
@@ -88,7 +88,7 @@ def test_self_loops_cancel(gz, oracle_mod):
     _check(gz, oracle_mod, V, 91, S.make_records(src, dst))
 
 
-@pytest.mark.parametrize("form", [1, 2])
+@pytest.mark.parametrize("form", [1, 2, 3])
 def test_star_vertex(gz, oracle_mod, form):
     """One vertex adjacent to every other: its 4095 entries land in one tile, all of them in
     the same bucket rows of its sketch."""
@@ -112,16 +112,17 @@ def test_vertex_counts(gz, oracle_mod, V):
     _check(gz, oracle_mod, V, 1000 + V, S.make_records(src, dst))
 
 
-def test_deep_depths_of_a_dense_graph(gz, oracle_mod):
+@pytest.mark.parametrize("form", [2, 3])
+def test_deep_depths_of_a_dense_graph(gz, oracle_mod, form):
     """2^12 vertices and 3e6 records: about 2^-11 of the column updates go to depths past the
     planes' rows (XORed into HBM), and a few per million to depths of 15 or more (code 15,
-    recomputed)."""
+    recomputed); with 3-bit codes, 1 in 128 column updates is an escape (code 7) hashed again."""
     from graphzeppelin_b200 import streams as S
     V = 1 << 12
     st, _ = S.planted_partition_stream_fast(V, 4, seed=9, mean_degree=1400, min_size=256,
                                             churn_fraction=0.1)
     assert st.num_updates > 2_500_000
-    alg = _alg(gz, V, 0xDEC0DE)
+    alg = _alg(gz, V, 0xDEC0DE, form)
     alg.ingest_records(st)
     osk = oracle_mod.OracleSketches(V, 0xDEC0DE)
     osk.apply_records(st.raw())
@@ -136,7 +137,7 @@ def test_coded_and_plain_equal_across_flushes(gz, oracle_mod):
     rec = st.records
     cuts = [0, 3, 50, 1000, 1001, 4000, rec.size]
     dumps = []
-    for form in (1, 2):
+    for form in (1, 2, 3):
         alg = _alg(gz, 2048, c["seed"], form)
         for a, b in zip(cuts[:-1], cuts[1:]):
             alg.ingest_records(rec[a:b])
@@ -145,5 +146,53 @@ def test_coded_and_plain_equal_across_flushes(gz, oracle_mod):
         assert (canonical(alg.connected_components().parent_arr) == labels).all()
     osk = oracle_mod.OracleSketches(2048, c["seed"])
     osk.apply_records(st.raw())
-    assert (dumps[0] == osk.data).all()
-    assert (dumps[1] == osk.data).all()
+    for d in dumps:
+        assert (d == osk.data).all()
+
+
+@pytest.mark.parametrize("tiles_per_bin", [1, 4])
+def test_three_bit_codes_with_multi_tile_bins(gz, oracle_mod, tiles_per_bin):
+    """3-bit coded entries at 2^17 vertices (24 columns: the payload starts past bit 64), in bins
+    of one and of four tiles (each tile filters its bin's entries): the oracle's bytes and the
+    exact partition."""
+    from graphzeppelin_b200 import streams as S
+    V = 1 << 17
+    rng = np.random.default_rng(70 + tiles_per_bin)
+    src = rng.integers(0, V, 400_000, dtype=np.uint32)
+    dst = (src + rng.integers(1, 2000, src.size, dtype=np.uint32)) % V
+    st = S.Stream(V, S.make_records(src, dst))
+    alg = gz.CCSketchAlg(V, 4321)
+    alg.set_tuning(0, 0, tiles_per_bin, 3)
+    assert alg.params.entry_form == 3
+    assert alg.params.vertices_per_bin == 32 * tiles_per_bin
+    alg.ingest_records(st)
+    osk = oracle_mod.OracleSketches(V, 4321)
+    osk.apply_records(st.raw())
+    assert (alg.dump_sketches() == osk.data).all()
+    n, exact = oracle_mod.exact_cc(V, st.raw())
+    cc = alg.connected_components()
+    assert cc.size() == n and (canonical(cc.parent_arr) == exact).all()
+
+
+def test_three_bit_codes_chosen_past_2_19_vertices(gz, oracle_mod):
+    """2^19 + 1 vertices (26 columns, 20-bit neighbours): coded entries asked for take 3-bit codes
+    (4-bit ones do not fit 16 bytes) in bins of two tiles; the bytes equal the oracle's."""
+    from graphzeppelin_b200 import streams as S
+    V = (1 << 19) + 1
+    rng = np.random.default_rng(19)
+    src = rng.integers(0, V, 1_000_000, dtype=np.uint32)
+    dst = rng.integers(0, V, src.size, dtype=np.uint32)
+    st = S.Stream(V, S.make_records(src, dst))
+    alg = gz.CCSketchAlg(V, 1919)
+    alg.set_tuning(0, 0, 0, 2)
+    assert alg.params.entry_form == 3
+    assert alg.params.num_bins <= 8192
+    alg.ingest_records(st)
+    osk = oracle_mod.OracleSketches(V, 1919)
+    osk.apply_records(st.raw())
+    assert (alg.dump_sketches() == osk.data).all()
+    del osk
+    n, exact = oracle_mod.exact_cc(V, st.raw())
+    cc = alg.connected_components()
+    assert cc.size() == n and (canonical(cc.parent_arr) == exact).all()
+    alg.close()
