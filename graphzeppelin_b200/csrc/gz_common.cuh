@@ -136,6 +136,29 @@ __device__ __forceinline__ uint32_t stage_records(const uint8_t *base, uint64_t 
   return (uint32_t)(start - a0);
 }
 
+// src / dst of record i of the stream [rec, rec_end) straight from global memory: three 4-byte
+// loads (through L1, which a warp's 32 consecutive records share) from the aligned words that
+// hold bytes 9i + 1 .. 9i + 8, or byte loads where those words would reach outside the stream.
+__device__ __forceinline__ void load_record(const uint8_t *rec, const uint8_t *rec_end, uint64_t i,
+                                            uint32_t &u, uint32_t &v) {
+  const uint8_t *p = rec + 9 * i + 1;
+  const uintptr_t w0 = (uintptr_t)p & ~(uintptr_t)3;
+  if (w0 >= (uintptr_t)rec && w0 + 12 <= (uintptr_t)rec_end) {
+    const uint32_t *w = reinterpret_cast<const uint32_t *>(w0);
+    const uint32_t a0 = __ldg(w), a1 = __ldg(w + 1), a2 = __ldg(w + 2);
+    const uint32_t sh = ((uintptr_t)p & 3) * 8;
+    u = __funnelshift_r(a0, a1, sh);
+    v = __funnelshift_r(a1, a2, sh);
+  } else {
+    u = v = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      u |= (uint32_t)__ldg(p + k) << (8 * k);
+      v |= (uint32_t)__ldg(p + 4 + k) << (8 * k);
+    }
+  }
+}
+
 // src / dst of staged record i (the type byte is not needed).
 __device__ __forceinline__ void parse_record(const uint8_t *s, uint32_t shift, uint32_t i,
                                              uint32_t &u, uint32_t &v) {

@@ -103,6 +103,44 @@ k_gutter(const void *__restrict__ in, uint64_t n, GutterGeom g, uint64_t *__rest
   if (COUNT && bad) atomicOr(status, kStatusBadVertex);
 }
 
+// Counting pass over records, unstaged: each thread takes RPI records per iteration (all their
+// loads in flight together, straight from global memory), the block counts bins in shared
+// memory, and adds its counts to the global ones once per bin.
+template <int RPI>
+__global__ void __launch_bounds__(512)
+k_count_records(const uint8_t *__restrict__ rec, uint64_t n, GutterGeom g, uint64_t *__restrict__ hist,
+                uint32_t *__restrict__ status) {
+  extern __shared__ __align__(16) uint32_t s_cnt[];
+  for (uint32_t b = threadIdx.x; b < g.nbins; b += blockDim.x) s_cnt[b] = 0u;
+  __syncthreads();
+  const uint8_t *rec_end = rec + 9 * n;
+  const uint64_t step = (uint64_t)gridDim.x * blockDim.x * RPI;
+  bool bad = false;
+  for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x * RPI + threadIdx.x; i0 < n; i0 += step) {
+    uint32_t u[RPI], v[RPI];
+#pragma unroll
+    for (int k = 0; k < RPI; ++k) {
+      const uint64_t i = i0 + (uint64_t)k * blockDim.x;
+      u[k] = v[k] = 0xffffffffu;
+      if (i < n) load_record(rec, rec_end, i, u[k], v[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < RPI; ++k) {
+      if (i0 + (uint64_t)k * blockDim.x >= n) continue;
+      if (u[k] >= g.V || v[k] >= g.V) {
+        bad = true;
+        continue;
+      }
+      atomicAdd(&s_cnt[u[k] >> g.bin_shift], 1u);
+      atomicAdd(&s_cnt[v[k] >> g.bin_shift], 1u);
+    }
+  }
+  __syncthreads();
+  for (uint32_t b = threadIdx.x; b < g.nbins; b += blockDim.x)
+    if (s_cnt[b]) atomicAdd(reinterpret_cast<unsigned long long *>(&hist[b]), (unsigned long long)s_cnt[b]);
+  if (bad) atomicOr(status, kStatusBadVertex);
+}
+
 size_t gutter_smem(int input, GutterGeom g, bool smem) {
   size_t s = smem ? ((g.nbins + 3) & ~3u) * 4 : 0;
   if (input == kInputRecords) s += kRecStageBytes;
@@ -1534,9 +1572,27 @@ cudaError_t scan_exclusive_u64(uint64_t *d, uint64_t n, uint64_t *total, uint64_
   return cudaGetLastError();
 }
 
+constexpr int kCountRpi = 8;  // records per thread per iteration of the counting pass
+
 cudaError_t gutter_count(int input, const void *in, uint64_t n, GutterGeom g, int G,
                          uint64_t *counts, uint32_t *status, cudaStream_t s) {
   const bool smem = g.nbins <= kSmemBinsMax;
+  if (input == kInputRecords && smem) {
+    auto kern = k_count_records<kCountRpi>;
+    const size_t sm = (size_t)((g.nbins + 3) & ~3u) * 4;
+    if (sm > 48 * 1024) {
+      cudaError_t e = smem_optin(kern);
+      if (e != cudaSuccess) return e;
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 512, sm) != cudaSuccess || per_sm < 1)
+      per_sm = 1;
+    const uint64_t need = (n + 512ull * kCountRpi - 1) / (512ull * kCountRpi);
+    const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(need, (uint64_t)num_sms() * per_sm));
+    kern<<<blocks, 512, sm, s>>>(reinterpret_cast<const uint8_t *>(in), n, g, counts, status);
+    g_launches++;
+    return cudaGetLastError();
+  }
   if (input == kInputRecords)
     return smem ? launch_gutter<kInputRecords, true, true>(in, n, g, G, counts, nullptr, status, s)
                 : launch_gutter<kInputRecords, true, false>(in, n, g, G, counts, nullptr, status, s);
