@@ -73,14 +73,19 @@ class ClockSampler:
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
                  "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.first = threading.Event()
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # nvidia-smi takes a moment to print its first sample: the timed region starts after it
+            self.first.wait(timeout=3.0)
+            self.lines.clear()
         except Exception:
             self.proc = None
 
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
+            self.first.set()
 
     def stop(self):
         if not self.proc:
@@ -337,6 +342,10 @@ def run_b200(args, cfg):
         e2.record(lib_stream)
         return e0, e1, e2, ncc
 
+    # the clock sampler runs from before the warm-up (its first sample takes a moment); only the
+    # samples taken from the start of the timed steps are kept
+    sampler = ClockSampler(local)
+    sampler.start()
     for _ in range(args.warmup):
         *_, ncc = step()
     torch.cuda.synchronize()
@@ -346,8 +355,7 @@ def run_b200(args, cfg):
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    sampler = ClockSampler(local)
-    sampler.start()
+    sampler.lines.clear()
     alg.set_profiling(True)
     marks = []
     tw0 = time.perf_counter()
