@@ -121,6 +121,9 @@ SIGNATURES = [
     ("gz_server_get_params", _i, [_H, _u32, ctypes.POINTER(gz_params_t)]),
     ("gz_server_ingest", _i, [_H, _u32, _P, _P, _P]),
     ("gz_server_ingest_segments", _i, [_H, _u32, _P, _P, _P]),
+    ("gz_host_register", _i, [_P, _u64]),
+    ("gz_host_unregister", _i, [_P]),
+    ("gz_server_set_query_snapshot", _i, [_H, _i]),
     ("gz_server_query_submit", _i, [_H, _u32, _P, ctypes.POINTER(_u64)]),
     ("gz_server_query_wait", _i, [_H, _u64, _P, _P, _P, _P]),
     ("gz_server_query_ready", _i, [_H, _u64, ctypes.POINTER(_i)]),

@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(512)
 k_mb_direct(const uint8_t *__restrict__ rec, const uint4 *__restrict__ rtiles, uint32_t n_rt,
             const GraphDesc *__restrict__ graphs, uint8_t *__restrict__ sketches,
             const uint64_t *__restrict__ flip, uint32_t *__restrict__ status) {
-  extern __shared__ __align__(16) uint8_t dsm[];
+  extern __shared__ __align__(128) uint8_t dsm[];
   uint64_t *s_flip = reinterpret_cast<uint64_t *>(dsm);
   uint8_t *s_rec = dsm + kMbFlipMax * 8;
   bool bad = false;
@@ -1969,6 +1969,7 @@ namespace {
 
 constexpr uint32_t kServeFlipWords = 64;  // hash-constant slot per tenant (C <= 62)
 constexpr uint32_t kServeTileC = 62;      // column count the tiling budget is reserved for
+constexpr uint64_t kServeQueryMaxV = 1ull << 24;  // vertices of queued jobs merged into one run
 
 // First-fit allocator over [0, size) in 256-byte units.
 struct RangeAlloc {
@@ -2019,9 +2020,10 @@ struct ServeTenant {
 struct QueryJob {
   uint64_t ticket = 0;
   std::vector<uint32_t> tenants;
-  std::vector<GraphDesc> descs;  // sk_off into the snapshot pool, flip_off into `flips`
+  std::vector<GraphDesc> descs;  // sk_off into the snapshot pool (or the arena), flip_off into `flips`
   std::vector<uint64_t> flips;
   std::vector<std::pair<uint64_t, uint64_t>> snaps;  // snapshot regions to release
+  bool live = false;  // reads the tenants' sketches in the arena (sk_off into the arena), no snapshot
   bool done = false;
   int rc = GZ_OK;
   std::string err;
@@ -2060,42 +2062,95 @@ struct gz_server {
   bool stop = false;
   std::thread worker;
   cudaEvent_t snap_done = nullptr;
+  bool live = false;  // queries submitted now read the arena in place (gz_server_set_query_snapshot)
 };
 
 namespace {
 
-int serve_run_job(gz_server *s, QueryJob *j) {
+// Blocks until no unfinished in-place query reads any of the n tenants, whose sketches may then be
+// written or freed. The worker never takes s->mtx, so callers may hold it.
+void serve_wait_live(gz_server *s, const uint32_t *ids, uint32_t n) {
+  std::unique_lock<std::mutex> ql(s->qmtx);
+  s->done_cv.wait(ql, [&] {
+    for (const auto &kv : s->jobs) {
+      const QueryJob *j = kv.second;
+      if (!j->live || j->done) continue;
+      for (uint32_t t : j->tenants)
+        for (uint32_t k = 0; k < n; ++k)
+          if (ids[k] == t) return false;
+    }
+    return true;
+  });
+}
+
+// One batched Boruvka over every tenant of the given jobs (all live, or all on snapshots); each
+// job gets its own tenants' slice of the answer.
+int serve_run_jobs(gz_server *s, const std::vector<QueryJob *> &js) {
   gz_batch *q = &s->query;
-  MB_TRY(grow(&s->d_qflip, s->qflip_cap, j->flips.size(), s->query.stream));
+  std::vector<uint64_t> flips;
+  std::vector<GraphDesc> descs;
+  for (QueryJob *j : js) {
+    const uint32_t base = (uint32_t)flips.size();  // even: every job's constants stay 16-byte aligned
+    flips.insert(flips.end(), j->flips.begin(), j->flips.end());
+    for (GraphDesc gd : j->descs) {
+      gd.flip_off += base;
+      descs.push_back(gd);
+    }
+  }
+  MB_TRY(grow(&s->d_qflip, s->qflip_cap, flips.size(), s->query.stream));
   q->d_flip = s->d_qflip;
-  MB_CUDA(cudaMemcpyAsync(s->d_qflip, j->flips.data(), 8 * j->flips.size(), cudaMemcpyHostToDevice, q->stream));
-  q->graphs = j->descs;
+  q->d_sk = js[0]->live ? s->arena : s->snap;
+  MB_CUDA(cudaMemcpyAsync(s->d_qflip, flips.data(), 8 * flips.size(), cudaMemcpyHostToDevice, q->stream));
+  q->graphs = descs;
   MB_TRY(finalize_graphs(q));
-  j->labels.resize(q->total_V);
-  MB_TRY(batch_query(q, j->labels.data()));
-  j->ncc = q->ncc;
-  j->rounds = q->rounds;
-  j->status.assign(q->status.begin(), q->status.end());
+  std::vector<uint32_t> labels(q->total_V);
+  MB_TRY(batch_query(q, labels.data()));
+  size_t v0 = 0, g0 = 0;
+  for (QueryJob *j : js) {
+    size_t nv = 0;
+    for (const GraphDesc &gd : j->descs) nv += gd.V;
+    const size_t ng = j->descs.size();
+    j->labels.assign(labels.begin() + v0, labels.begin() + v0 + nv);
+    j->ncc.assign(q->ncc.begin() + g0, q->ncc.begin() + g0 + ng);
+    j->rounds.assign(q->rounds.begin() + g0, q->rounds.begin() + g0 + ng);
+    j->status.assign(q->status.begin() + g0, q->status.begin() + g0 + ng);
+    v0 += nv;
+    g0 += ng;
+  }
   return GZ_OK;
 }
 
 void serve_worker(gz_server *s) {
   cudaSetDevice(s->device);
   for (;;) {
-    QueryJob *j = nullptr;
+    std::vector<QueryJob *> js;
     {
       std::unique_lock<std::mutex> lk(s->qmtx);
       s->qcv.wait(lk, [&] { return s->stop || !s->queue.empty(); });
       if (s->queue.empty()) return;
-      j = s->queue.front();
-      s->queue.pop_front();
+      // every queued job of the same kind as the first runs in one batched query: jobs that
+      // arrive while one runs wait for it anyway, and one run over all their tenants costs
+      // about as many rounds as the longest of them
+      uint64_t nv = 0;
+      while (!s->queue.empty() && s->queue.front()->live == (js.empty() ? s->queue.front()->live : js[0]->live)) {
+        uint64_t v = 0;
+        for (const GraphDesc &gd : s->queue.front()->descs) v += gd.V;
+        if (!js.empty() && nv + v > kServeQueryMaxV) break;
+        nv += v;
+        js.push_back(s->queue.front());
+        s->queue.pop_front();
+      }
     }
-    j->rc = serve_run_job(s, j);
-    if (j->rc != GZ_OK) j->err = gz_last_error();
+    const int rc = serve_run_jobs(s, js);
+    const std::string err = rc != GZ_OK ? std::string(gz_last_error()) : std::string();
     {
       std::lock_guard<std::mutex> lk(s->qmtx);
-      for (auto &r : j->snaps) s->snap_alloc.release(r.first, r.second);
-      j->done = true;
+      for (QueryJob *j : js) {
+        j->rc = rc;
+        j->err = err;
+        for (auto &r : j->snaps) s->snap_alloc.release(r.first, r.second);
+        j->done = true;
+      }
     }
     s->done_cv.notify_all();
   }
@@ -2122,12 +2177,14 @@ void serve_destroy(gz_server *s) {
   mb_free(s->d_rec);
 }
 
-int serve_engine_init(gz_server *s, gz_batch *e, uint8_t *storage) {
+int serve_engine_init(gz_server *s, gz_batch *e, uint8_t *storage, bool urgent) {
   e->device = s->device;
   e->factor = s->factor;
   e->own_storage = false;
   e->d_sk = storage;
-  MB_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+  int least = 0, greatest = 0;
+  MB_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+  MB_CUDA(cudaStreamCreateWithPriority(&e->stream, cudaStreamNonBlocking, urgent ? greatest : least));
   MB_TRY(mb_alloc(&e->d_status, 4));
   MB_TRY(mb_alloc(&e->d_total, 1));
   MB_CUDA(cudaMemsetAsync(e->d_status, 0, 16, e->stream));
@@ -2181,7 +2238,8 @@ int gz_server_create(uint64_t budget_bytes, uint64_t snapshot_bytes, double sket
     return bail(rc);
   s->arena_alloc.init(s->budget);
   s->snap_alloc.init((snapshot_bytes + 255) & ~255ull);
-  if ((rc = serve_engine_init(s, &s->ingest, s->arena)) || (rc = serve_engine_init(s, &s->query, s->snap)))
+  // the query stream has the greatest priority: its kernels take SMs ahead of queued ingest blocks
+  if ((rc = serve_engine_init(s, &s->ingest, s->arena, false)) || (rc = serve_engine_init(s, &s->query, s->snap, true)))
     return bail(rc);
   if (cudaEventCreateWithFlags(&s->snap_done, cudaEventDisableTiming) != cudaSuccess)
     return bail(mb_fail(GZ_ERR_CUDA, "cudaEventCreate"));
@@ -2267,6 +2325,7 @@ int gz_server_evict(gz_server_t *s, uint32_t tenant) {
   std::lock_guard<std::mutex> lk(s->mtx);
   cudaSetDevice(s->device);
   MB_TRY(serve_check_tenants(s, 1, &tenant));
+  serve_wait_live(s, &tenant, 1);
   ServeTenant &t = s->tenants[tenant];
   // queries already submitted read their snapshots, whose copies the ingest stream waits for
   // before any later work on the range (a new tenant's zeroing included)
@@ -2284,6 +2343,13 @@ int gz_server_set_route(gz_server_t *s, double sparse_factor) {
   if (!s || !(sparse_factor >= 0)) return mb_fail(GZ_ERR_INVALID, "bad argument");
   std::lock_guard<std::mutex> lk(s->mtx);
   s->ingest.sparse_factor = sparse_factor;
+  return GZ_OK;
+}
+
+int gz_server_set_query_snapshot(gz_server_t *s, int snapshot) {
+  if (!s) return mb_fail(GZ_ERR_INVALID, "null handle");
+  std::lock_guard<std::mutex> lk(s->mtx);
+  s->live = snapshot == 0;
   return GZ_OK;
 }
 
@@ -2328,6 +2394,7 @@ int gz_server_ingest(gz_server_t *s, uint32_t n, const uint32_t *ids, const void
   std::lock_guard<std::mutex> lk(s->mtx);
   cudaSetDevice(s->device);
   MB_TRY(serve_check_tenants(s, n, ids));
+  serve_wait_live(s, ids, n);
   const uint64_t nrec = offsets[n] - offsets[0];
   if (nrec == 0) return GZ_OK;
   if (!records) return mb_fail(GZ_ERR_INVALID, "null records");
@@ -2363,6 +2430,7 @@ int gz_server_ingest_segments(gz_server_t *s, uint32_t nseg, const uint32_t *ten
     off.back() += counts[k];
   }
   MB_TRY(serve_check_tenants(s, (uint32_t)ids.size(), ids.data()));
+  serve_wait_live(s, ids.data(), (uint32_t)ids.size());
   const uint64_t nrec = off.back();
   if (nrec == 0) return GZ_OK;
   gz_batch *e = &s->ingest;
@@ -2390,6 +2458,34 @@ int gz_server_query_submit(gz_server_t *s, uint32_t n, const uint32_t *ids, uint
   MB_TRY(serve_check_tenants(s, n, ids));
   QueryJob *j = new QueryJob();
   j->tenants.assign(ids, ids + n);
+  if (s->live) {
+    // read in place: ordered after every earlier ingest call; the tenants' later ingest calls and
+    // evictions wait for the query (serve_wait_live)
+    j->live = true;
+    cudaEvent_t ev;
+    MB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    MB_CUDA(cudaEventRecord(ev, s->ingest.stream));
+    MB_CUDA(cudaStreamWaitEvent(s->query.stream, ev, 0));
+    cudaEventDestroy(ev);
+    uint64_t flip_off = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+      const ServeTenant &t = s->tenants[ids[i]];
+      GraphDesc gd = t.desc;
+      gd.flip_off = (uint32_t)flip_off;
+      j->flips.insert(j->flips.end(), t.flips.begin(), t.flips.end());
+      flip_off += t.flips.size();
+      j->descs.push_back(gd);
+    }
+    {
+      std::lock_guard<std::mutex> ql(s->qmtx);
+      j->ticket = s->next_ticket++;
+      s->jobs[j->ticket] = j;
+      s->queue.push_back(j);
+      *ticket = j->ticket;
+    }
+    s->qcv.notify_all();
+    return GZ_OK;
+  }
   uint64_t need = 0;
   for (uint32_t i = 0; i < n; ++i) need += (s->tenants[ids[i]].bytes + 255) & ~255ull;
   if (need > s->snap_alloc.size) {

@@ -78,7 +78,6 @@ using gz::kStageBuffers;
 using gz::kStageRecords;
 constexpr uint64_t kEntStage = 1ull << 20;      // staged apply_update_batch entries per flush
 constexpr uint64_t kMaxChunkEntries = 1ull << 31;
-constexpr int kNumPhases = 3;  // gutter, sketch update, query
 
 }  // namespace
 
@@ -1658,6 +1657,24 @@ int gz_clear(gz_alg_t *h) {
     h->dsu_valid = true;
     h->host_answer = true;
   }
+  return GZ_OK;
+}
+
+// Page-locks a caller's host buffer for this process (portable across contexts), so copies of
+// records from it run at full host-link speed instead of through the driver's pageable staging;
+// gz_host_unregister releases it. Used by callers that keep incoming update batches in one long
+// lived buffer (a serving loop's receive buffers).
+int gz_host_register(void *ptr, uint64_t bytes) {
+  if (!ptr || bytes == 0) return fail(GZ_ERR_INVALID, "null or empty host buffer");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(GZ_ERR_NO_DEVICE, "no CUDA device");
+  GZ_CUDA(cudaHostRegister(ptr, bytes, cudaHostRegisterPortable));
+  return GZ_OK;
+}
+
+int gz_host_unregister(void *ptr) {
+  if (!ptr) return fail(GZ_ERR_INVALID, "null host buffer");
+  GZ_CUDA(cudaHostUnregister(ptr));
   return GZ_OK;
 }
 

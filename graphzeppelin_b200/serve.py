@@ -3,7 +3,8 @@
 A tenant is one CCSketchAlg (include/cc_sketch_alg.h:69) with its own vertex count and seed.
 ``SketchServer`` wraps the gz_server_* entry points: tenants are admitted while their sketch bytes
 fit a device budget, update batches of many tenants are applied by one batched ingest, and
-connectivity queries run on a device snapshot while later ingests proceed.
+connectivity queries run on a device snapshot (or on the sketches in place, the tenant's ingest
+held until the answer) while later ingests proceed.
 
 ``serving_trace`` builds a seeded request trace (tenant arrivals and per-tenant requests on
 Poisson processes; update batches with deletions of live edges; connectivity and point queries),
@@ -15,6 +16,7 @@ from __future__ import annotations
 
 import ctypes
 import hashlib
+import threading
 import time
 from collections import deque
 from dataclasses import dataclass, field
@@ -55,6 +57,7 @@ class SketchServer:
                                          ctypes.byref(h)))
         self._h = h
         self.num_vertices: Dict[int, int] = {}
+        self._sizes: Dict[int, List[int]] = {}  # ticket -> V of each queried tenant
 
     def close(self):
         if getattr(self, "_h", None):
@@ -87,6 +90,12 @@ class SketchServer:
     def set_route(self, sparse_factor: float) -> None:
         """Per-call routing between in-place and staged ingest (gz_server_set_route)."""
         _check(self.lib.gz_server_set_route(self._h, float(sparse_factor)))
+
+    def set_query_snapshot(self, snapshot: bool) -> None:
+        """True (the default): queries copy their tenants' sketches to a snapshot, so ingest of
+        those tenants may go on at once. False: queries read the sketches in place; an ingest or
+        eviction naming a tenant with an unfinished query waits for it."""
+        _check(self.lib.gz_server_set_query_snapshot(self._h, int(bool(snapshot))))
 
     def usage(self):
         used, budget, n = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint32()
@@ -128,6 +137,8 @@ class SketchServer:
         ids = np.ascontiguousarray(tenants, dtype=np.uint32)
         t = ctypes.c_uint64()
         _check(self.lib.gz_server_query_submit(self._h, ids.size, _ptr(ids), ctypes.byref(t)))
+        # the answer's layout, kept with the ticket: a tenant may be evicted before it is read
+        self._sizes[int(t.value)] = [self.num_vertices[int(k)] for k in ids]
         return int(t.value)
 
     def query_ready(self, ticket: int) -> bool:
@@ -138,7 +149,9 @@ class SketchServer:
 
     def query_wait(self, ticket: int, tenants: Sequence[int]):
         """Per tenant (labels, num_cc, rounds, status) of a submitted query."""
-        sizes = [self.num_vertices[t] for t in tenants]
+        sizes = self._sizes.pop(int(ticket), None)
+        if sizes is None or len(sizes) != len(tenants):
+            raise GZError(_lib.GZ_ERR_INVALID, "unknown ticket, or not the tenants it was submitted for")
         labels = np.empty(sum(sizes), np.uint32)
         ncc = np.zeros(len(tenants), np.uint32)
         rounds = np.zeros(len(tenants), np.uint32)
@@ -357,15 +370,49 @@ def _digest_answers(answers: Dict[int, tuple]) -> None:
             answers[i] = done[key]
 
 
+class pinned_host:
+    """Page-locks a host buffer (gz_host_register) for the life of the ``with`` block, so record
+    copies from it run at full host-link speed. A serving process keeps its incoming update
+    batches in such buffers; a pageable buffer is copied through the driver's staging, several
+    times slower."""
+
+    def __init__(self, buf: np.ndarray):
+        self.buf = buf
+        self.ptr = None
+
+    def __enter__(self):
+        if self.buf.nbytes:
+            _check(_lib.load().gz_host_register(self.buf.ctypes.data, self.buf.nbytes))
+            self.ptr = self.buf.ctypes.data
+        return self.buf
+
+    def __exit__(self, *exc):
+        if self.ptr is not None:
+            _check(_lib.load().gz_host_unregister(self.ptr))
+            self.ptr = None
+
+
 def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes: int = 0,
            time_scale: float = 1.0, sketches_factor: float = 1.0,
-           max_tick_updates: int = 1 << 24, route: float | None = None) -> ServingResult:
+           max_tick_updates: int = 1 << 21, route: float | None = None,
+           pin: bool = True, query_snapshot: bool = False) -> ServingResult:
     """Serve every request of `trace`. mode "batched": the gz_server path (continuous batching:
-    each tick applies the arrived update batches of all admitted tenants in one ingest and
-    submits their queries to the snapshot worker; answers are collected one tick later).
-    mode "plain": one CCSketchAlg per tenant, every request handled on its own in arrival order.
-    Requests are released at trace time / time_scale after the start; tenants are admitted in
-    arrival order while their sketch bytes fit the budget and leave after their last request."""
+    each tick submits the queries that need no update of this tick, applies the arrived update
+    batches of all admitted tenants, up to max_tick_updates records, in one ingest, then submits
+    the queries behind those updates; a collector thread takes each answer as soon as its query
+    finishes). mode "plain": one CCSketchAlg per tenant, every request handled on its own in
+    arrival order. Requests are released at trace time / time_scale after the start; tenants are
+    admitted in arrival order while their sketch bytes fit the budget and leave after their last
+    request. pin: the trace's records are page-locked for the replay (both modes), as a server's
+    receive buffers would be; the page-locking is outside the timed replay. query_snapshot:
+    whether the batched server copies a query's tenants to a snapshot; by default it reads them in
+    place, which is safe here because a tenant's later requests wait until its answer is in."""
+    if pin and trace.raw.nbytes:
+        with pinned_host(trace.raw):
+            return replay(trace, mode, budget_bytes, snapshot_bytes=snapshot_bytes,
+                          time_scale=time_scale, sketches_factor=sketches_factor,
+                          max_tick_updates=max_tick_updates, route=route, pin=False,
+                          query_snapshot=query_snapshot)
     res = ServingResult(mode)
     N = trace.time.size
     T = trace.num_vertices.size
@@ -384,10 +431,17 @@ def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes:
         server = SketchServer(budget_bytes, snap, sketches_factor)
         if route is not None:
             server.set_route(route)
-        snap_job_bytes = snap // 2  # two query jobs fit the snapshot pool at once
+        server.set_query_snapshot(query_snapshot)
+        # with snapshots, jobs of at most half the pool, so one runs while the next is copied
+        snap_job_bytes = snap // 2 if query_snapshot else 1 << 62
     cache = {}          # batched: tenant -> (labels, ncc, version it answers for)
     version = np.zeros(T, np.int64)  # update batches applied per tenant
-    inflight = []       # batched: jobs of the previous tick, (ticket, tenants, [(req, t)], versions)
+    queued_q: Dict[int, int] = {}     # batched: released queries not yet taken, per tenant
+    inflight = []       # batched: submitted jobs not yet taken in, (ticket, tenants, ids, reqs, versions)
+    done_jobs: deque = deque()  # batched: (job, per-tenant results, answers, seconds) from the collector
+    jobs_in: deque = deque()    # batched: jobs for the collector, in submission order
+    wake = threading.Condition()
+    collector_error = []
     t0 = time.perf_counter()
     nxt = 0
 
@@ -396,10 +450,10 @@ def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes:
 
     admitted_at = {}    # tenant -> wall seconds since start of its admission
 
-    def finish(i, t, answer):
+    def finish(i, t, answer, at=None):
         res.answers[i] = answer
         if trace.kind[i] != UPDATE:
-            now = time.perf_counter() - t0
+            now = (time.perf_counter() if at is None else at) - t0
             release = trace.time[i] / time_scale
             res.latencies_ms.append((now - release) * 1e3)
             res.service_ms.append((now - max(release, admitted_at.get(t, 0.0))) * 1e3)
@@ -456,25 +510,81 @@ def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes:
             res.max_resident = max(res.max_resident, len(resident))
             res.max_used_bytes = max(res.max_used_bytes, used[0])
 
-    def collect(jobs):
-        for ticket, tens, reqs, vers in jobs:
-            ts = time.perf_counter()
-            out = server.query_wait(ticket, [state[t] for t in tens])
-            res._add("query_wait", ts)
-            got = {}
-            for t, (lab, ncc, rounds, status), v in zip(tens, out, vers):
-                got[t] = (lab.copy(), ncc, v)
-                cache[t] = got[t]
-            for i, t in reqs:
-                lab, ncc, _ = got[t]
-                finish(i, t, _answer(i, lab, ncc))
-
     def _answer(i, lab, ncc):
         if trace.kind[i] == CONNECTIVITY_QUERY:
             return ("cc", lab, ncc)  # digested after the replay
         u, v = trace.point[i]
         return (bool(lab[u] == lab[v]),)
 
+    def collector():
+        # waits for each submitted query in submission order and hands its answers back with the
+        # time they were ready; the wait releases the interpreter lock, so ingest calls of the
+        # main loop proceed meanwhile
+        try:
+            while True:
+                with wake:
+                    while not jobs_in:
+                        wake.wait()
+                    job = jobs_in.popleft()
+                if job is None:
+                    return
+                ticket, tens, ids, reqs, vers = job
+                out = server.query_wait(ticket, ids)
+                got = {t: (lab.copy(), ncc, v) for t, (lab, ncc, rounds, status), v in zip(tens, out, vers)}
+                answers = [(i, t, _answer(i, got[t][0], got[t][1])) for i, t in reqs]
+                done_jobs.append((job, got, answers, time.perf_counter()))
+        except BaseException as e:  # re-raised by the main loop
+            collector_error.append(e)
+
+    def take_answers():
+        while done_jobs:
+            job, got, answers, at = done_jobs.popleft()
+            inflight.remove(job)
+            cache.update(got)
+            for i, t, answer in answers:
+                finish(i, t, answer, at)
+        if collector_error:
+            raise collector_error[0]
+
+    def submit(fresh):
+        groups, cur, cur_bytes = [], [], 0
+        for t in sorted({t for _, t in fresh}):
+            if cur and cur_bytes + cost[t] > snap_job_bytes:
+                groups.append(cur)
+                cur, cur_bytes = [], 0
+            cur.append(t)
+            cur_bytes += cost[t]
+        groups.append(cur)
+        for tens in groups:
+            members = set(tens)
+            ids = [state[t] for t in tens]
+            ts = time.perf_counter()
+            ticket = server.query_submit(ids)
+            res._add("query_submit", ts)
+            res.gpu_queries += 1
+            job = (ticket, tens, ids, [(i, t) for i, t in fresh if t in members],
+                   [int(version[t]) for t in tens])
+            inflight.append(job)
+            with wake:
+                jobs_in.append(job)
+                wake.notify()
+
+    def queries(qreq):
+        # cached answers at once, the rest on the device
+        fresh = []
+        for i, t in qreq:
+            c = cache.get(t)
+            if c is not None and c[2] == version[t]:  # nothing applied since: cached answer
+                finish(i, t, _answer(i, c[0], c[1]))
+            else:
+                fresh.append((i, t))
+        if fresh:
+            submit(fresh)
+
+    thread = None
+    if mode == "batched":
+        thread = threading.Thread(target=collector, daemon=True)
+        thread.start()
     try:
         while True:
             tnow = now_trace()
@@ -484,6 +594,8 @@ def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes:
                     pending[t] = deque()
                     waiting.append(t)
                 pending[t].append(nxt)
+                if trace.kind[nxt] != UPDATE:
+                    queued_q[t] = queued_q.get(t, 0) + 1
                 nxt += 1
             admit()
             if mode == "plain":
@@ -516,24 +628,24 @@ def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes:
                     u, v = trace.point[i]
                     finish(i, t, (bool(a.point_query(int(u), int(v))),))
                 continue
-            # batched: one tick. Answers of earlier ticks that are ready already go out first.
-            if inflight:
-                ready = [job for job in inflight if server.query_ready(job[0])]
-                if ready:
-                    collect(ready)
-                    inflight = [job for job in inflight if job not in ready]
+            # batched: one tick. Answers that are ready go out first.
+            take_answers()
             ing_t, ing_seg, ing_req = [], [], []
-            qreq = []
+            early, late = [], []  # queries needing no update of this tick / behind this tick's updates
             budget_left = max_tick_updates
             busy = {t for job in inflight for t in job[1]}
-            for t in sorted(resident, key=lambda x: pending[x][0] if pending.get(x) else N):
+            # tenants with a query waiting first (their updates up to the query), then the others by
+            # their oldest request; update-only work fills what the tick's cap leaves
+            for t in sorted(resident, key=lambda x: (not queued_q.get(x), pending[x][0] if pending.get(x) else N)):
                 q = pending.get(t)
                 if not q or t in busy:
                     continue
                 nparts = 0
-                while q and budget_left > 0:
+                while q:
                     i = q[0]
                     if trace.kind[i] == UPDATE:
+                        if budget_left <= 0:
+                            break
                         ing_t.append(state[t])
                         ing_seg.append(trace.records(i))
                         nparts += 1
@@ -541,18 +653,21 @@ def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes:
                         ing_req.append((i, t))
                         q.popleft()
                     else:
-                        qreq.append((i, t))
+                        (late if nparts else early).append((i, t))
                         q.popleft()
+                        queued_q[t] -= 1
                         break
                 if nparts:
                     version[t] += 1
-            if not ing_t and not qreq and not inflight:
+            if not ing_t and not early and not late:
                 if nxt >= N and not resident and not waiting:
                     break
-                if nxt < N:
-                    time.sleep(max(0.0, min(0.0005, (trace.time[nxt] - tnow) / time_scale)))
+                wait = 0.0005 if nxt >= N else min(0.0005, (trace.time[nxt] - tnow) / time_scale)
+                time.sleep(max(0.0, wait) if not inflight else min(max(0.0, wait), 0.0002))
                 continue
             res.ticks += 1
+            if early:
+                queries(early)
             if ing_t:
                 ts = time.perf_counter()
                 server.ingest_segments(ing_t, ing_seg)
@@ -560,40 +675,14 @@ def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes:
                 for i, t in ing_req:
                     res.updates += int(trace.rec_off[i + 1] - trace.rec_off[i])
                     finish(i, t, ())
-            # queries: cached answers at once, the rest on a device snapshot
-            fresh = []
-            for i, t in qreq:
-                c = cache.get(t)
-                if c is not None and c[2] == version[t]:  # nothing applied since: cached answer
-                    finish(i, t, _answer(i, c[0], c[1]))
-                else:
-                    fresh.append((i, t))
-            prev, inflight = inflight, []
-            new = []
-            if fresh:
-                # jobs of at most half the snapshot pool, so one runs while the next is copied
-                groups, cur, cur_bytes = [], [], 0
-                for t in sorted({t for _, t in fresh}):
-                    if cur and cur_bytes + cost[t] > snap_job_bytes:
-                        groups.append(cur)
-                        cur, cur_bytes = [], 0
-                    cur.append(t)
-                    cur_bytes += cost[t]
-                groups.append(cur)
-                for tens in groups:
-                    members = set(tens)
-                    ts = time.perf_counter()
-                    ticket = server.query_submit([state[t] for t in tens])
-                    res._add("query_submit", ts)
-                    res.gpu_queries += 1
-                    new.append((ticket, tens, [(i, t) for i, t in fresh if t in members],
-                                [int(version[t]) for t in tens]))
-            collect(prev)
-            inflight = new
+            if late:
+                queries(late)
     finally:
-        if inflight:
-            jobs, inflight = inflight, []
-            collect(jobs)
+        if thread is not None:
+            with wake:
+                jobs_in.append(None)
+                wake.notify()
+            thread.join()
         res.seconds = time.perf_counter() - t0
         for t in list(state):
             if mode == "plain":

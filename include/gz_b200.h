@@ -407,6 +407,13 @@ GZ_API int gz_server_usage(gz_server_t *server, uint64_t *used_bytes, uint64_t *
                            uint32_t *tenants);
 /* gz_batch_set_route for the server's ingest calls. */
 GZ_API int gz_server_set_route(gz_server_t *server, double sparse_factor);
+/* How later gz_server_query_submit calls read the tenants' sketches. snapshot = 1 (the default):
+ * copied into the snapshot pool first, so ingest of those tenants may continue at once. snapshot
+ * = 0: read in place, no copy; an ingest call or eviction naming a tenant of an unfinished query
+ * waits until that query is done (the answer is still the state at submission). For callers that
+ * hold a tenant's updates while its query runs, as a per-tenant request queue does. Queries
+ * queued behind a running one are answered together by one batched Boruvka. */
+GZ_API int gz_server_set_query_snapshot(gz_server_t *server, int snapshot);
 GZ_API int gz_server_get_params(gz_server_t *server, uint32_t tenant, gz_params_t *out);
 /* Tenant tenants[i]'s packed 9-byte records are records[offsets[i] .. offsets[i+1]) in host
  * memory (offsets: n + 1 entries; each tenant at most once per call). Synchronous. */
@@ -418,6 +425,12 @@ GZ_API int gz_server_ingest(gz_server_t *server, uint32_t n, const uint32_t *ten
 GZ_API int gz_server_ingest_segments(gz_server_t *server, uint32_t num_segments,
                                      const uint32_t *tenants, const void *const *ptrs,
                                      const uint64_t *counts);
+/* Page-locks (gz_host_register) or releases (gz_host_unregister) a host buffer the caller keeps
+ * its incoming records in, so that gz_ingest_records and gz_server_ingest* copy from it at full
+ * host-link speed; pageable buffers go through the driver's staging at a fraction of that.
+ * No counterpart in the reference: its update buffers never leave host memory. */
+GZ_API int gz_host_register(void *ptr, uint64_t bytes);
+GZ_API int gz_host_unregister(void *ptr);
 GZ_API int gz_server_query_submit(gz_server_t *server, uint32_t n, const uint32_t *tenants,
                                   uint64_t *ticket);
 /* Whether a submitted query's answer is ready (gz_server_query_wait would not block). */

@@ -71,6 +71,41 @@ def test_server_query_is_a_snapshot(gz):
         b.close()
 
 
+def test_server_in_place_queries_and_merged_jobs(gz):
+    """Queries that read the sketches in place answer for the state at submission: an ingest or
+    an eviction naming a queried tenant waits for the query. Queries queued back to back are
+    answered by merged batched runs, each exactly as the tenant's own CCSketchAlg."""
+    from graphzeppelin_b200.serve import SketchServer
+    specs = _streams()
+    halves = [np.array_split(r, 2) for _, _, r in specs]
+    with SketchServer(1 << 30, 1 << 26) as srv:
+        srv.set_query_snapshot(False)
+        ids = [srv.admit(V, seed) for V, seed, _ in specs]
+        srv.ingest(ids, [h[0] for h in halves])
+        tickets = [srv.query_submit([i]) for i in ids]
+        t_all = srv.query_submit(ids[::-1])
+        srv.ingest(ids, [h[1] for h in halves])  # waits for the queries above
+        out_all = srv.query_wait(t_all, ids[::-1])[::-1]
+        for k, (V, seed, _) in enumerate(specs):
+            a, cc = _single(gz, V, seed, halves[k][0])
+            for lab, ncc, rounds, status in (srv.query_wait(tickets[k], [ids[k]])[0], out_all[k]):
+                assert status == 0 and ncc == cc.size() and rounds == a.last_query_rounds
+                assert (lab == cc.parent_arr).all()
+            a.close()
+        final = srv.connected_components(ids)
+        tk = srv.query_submit([ids[2]])
+        srv.evict(ids[2])  # waits for the query reading its sketches
+        lab_e, ncc_e, _, _ = srv.query_wait(tk, [ids[2]])[0]
+        for k, (V, seed, recs) in enumerate(specs):
+            a, cc = _single(gz, V, seed, recs)
+            lab, ncc, rounds, status = final[k]
+            assert status == 0 and ncc == cc.size() and rounds == a.last_query_rounds
+            assert (lab == cc.parent_arr).all()
+            if k == 2:
+                assert ncc_e == cc.size() and (lab_e == cc.parent_arr).all()
+            a.close()
+
+
 def test_server_budget_admission_and_eviction(gz):
     from graphzeppelin_b200.serve import BudgetExhausted, SketchServer, tenant_bytes
     c = tenant_bytes(5000)
@@ -115,6 +150,10 @@ def test_serving_replay_batched_equals_plain_and_alone(gz, oracle_mod):
     p = SV.replay(tr, "plain", budget, time_scale=4.0)
     assert len(b.answers) == tr.time.size == len(p.answers)
     assert b.answers == p.answers
+    # queries on snapshots, pageable records and one-batch ticks answer the same
+    bs = SV.replay(tr, "batched", budget, time_scale=4.0, query_snapshot=True, pin=False,
+                   max_tick_updates=1)
+    assert bs.answers == p.answers
     assert b.admitted == 24 and b.max_resident < 24 and b.gpu_queries >= 1
     # alone vs in the mix
     for t in (0, 7, 19):
