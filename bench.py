@@ -670,12 +670,16 @@ SERVING = dict(workload="serving_t2000_v2e10-2e18_chunglu2.3_budget120GB", num_t
 # that tenants queue for admission while query latency is measured.
 SERVING_SHORT = dict(num_tenants=400, trace_seed=11, budget_bytes=16 * 10**9,
                      snapshot_bytes=8 * 10**9, time_scale=4.0)
+# records per tick of the saturated (throughput) replays; the paced ones use the replay's default,
+# a smaller cap that bounds how long a released query waits behind one ingest call
+SERVING_SAT_TICK = 1 << 21
 
 
 def serving_short():
     """Paced replay of a 400-tenant serving trace through the batched server (continuous
-    batching, snapshot queries) under a 16 GB sketch budget, and the same trace saturated through
-    the batched server and through the plain per-tenant path; answers must agree."""
+    batching, in-place queries, ticks of at most 2^19 records with queries first) under a 16 GB
+    sketch budget, and the same trace saturated through the batched server (ticks of up to 2^21
+    records) and through the plain per-tenant path; answers must agree."""
     from graphzeppelin_b200 import serve as SV
     cfg = SERVING_SHORT
     tr = SV.serving_trace(cfg["num_tenants"], cfg["trace_seed"])
@@ -685,7 +689,8 @@ def serving_short():
     SV.replay(warm, "batched", cfg["budget_bytes"], time_scale=1e12, **kw)
     SV.replay(warm, "plain", cfg["budget_bytes"], time_scale=1e12, **kw)
     paced = SV.replay(tr, "batched", cfg["budget_bytes"], time_scale=cfg["time_scale"], **kw)
-    sat = SV.replay(tr, "batched", cfg["budget_bytes"], time_scale=1e12, **kw)
+    sat = SV.replay(tr, "batched", cfg["budget_bytes"], time_scale=1e12,
+                    max_tick_updates=SERVING_SAT_TICK, **kw)
     plain = SV.replay(tr, "plain", cfg["budget_bytes"], time_scale=1e12, **kw)
     if not (paced.answers == sat.answers == plain.answers):
         raise SystemExit("serving answers differ between the batched server and the plain path")
@@ -702,6 +707,8 @@ def serving_short():
             "saturated_updates_per_s": s_["updates_per_s"],
             "plain_path_updates_per_s": pl["updates_per_s"],
             "saturated_over_plain": s_["updates_per_s"] / max(pl["updates_per_s"], 1e-9),
+            "paced_over_plain": p["updates_per_s"] / max(pl["updates_per_s"], 1e-9),
+            "tick_records_paced": SV.REPLAY_TICK_RECORDS, "tick_records_saturated": SERVING_SAT_TICK,
             "answers_equal": True,
             "note": "query_* from release, service_* from release or admission; wall clock; "
                     "plain path = one CCSketchAlg per tenant, requests one at a time"}
@@ -711,7 +718,7 @@ def run_serving(args):
     """Serving loop: a seeded trace of tenants (V log-uniform 2^10..2^18, Chung-Lu endpoints,
     exponent 2.3) whose requests are update batches of 1k-64k records (20% deletions of live
     edges), connectivity queries and point queries, served by the batched server (continuous
-    batching, snapshot queries) and by the plain per-tenant CCSketchAlg path, both admitting
+    batching, in-place queries) and by the plain per-tenant CCSketchAlg path, both admitting
     tenants against a 120 GB sketch budget. Each arm runs the trace twice: paced (requests
     released at their arrival times, compressed by --time-scale) for query latency, and saturated
     (every request released at once) for throughput."""
@@ -726,10 +733,8 @@ def run_serving(args):
     tr = SV.serving_trace(T, SERVING["trace_seed"])
     log(f"[serving] {T} tenants, {tr.time.size} requests, {tr.num_updates} updates "
         f"({tr.raw.size / 1e9:.2f} GB) over {tr.time[-1]:.1f} s of trace in {time.time() - t:.1f} s")
-    # the request payloads live in pinned host memory, as a server's receive buffers would
-    pinned = torch.empty(tr.raw.size, dtype=torch.uint8, pin_memory=True)
-    pinned.numpy()[:] = tr.raw
-    tr.raw = pinned.numpy()
+    # the request payloads are page-locked by each replay (outside its timing), as a server's
+    # receive buffers would be
     budget = SERVING["budget_bytes"]
     kw = dict(snapshot_bytes=SERVING["snapshot_bytes"])
     arms = {}
@@ -746,7 +751,7 @@ def run_serving(args):
         if mode == "plain" and args.no_plain:
             continue
         paced = SV.replay(tr, mode, budget, time_scale=args.time_scale, **kw)
-        sat = SV.replay(tr, mode, budget, time_scale=1e12, **kw)
+        sat = SV.replay(tr, mode, budget, time_scale=1e12, max_tick_updates=SERVING_SAT_TICK, **kw)
         arms[mode] = {"paced": paced, "saturated": sat}
         log(f"[serving] {mode}: paced {paced.summary()}; saturated {sat.summary()}")
         torch.cuda.empty_cache()

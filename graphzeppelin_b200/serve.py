@@ -15,6 +15,7 @@ admissions and every answer, so the two can be compared answer for answer.
 from __future__ import annotations
 
 import ctypes
+import gc
 import hashlib
 import threading
 import time
@@ -381,8 +382,9 @@ class pinned_host:
         self.ptr = None
 
     def __enter__(self):
-        if self.buf.nbytes:
-            _check(_lib.load().gz_host_register(self.buf.ctypes.data, self.buf.nbytes))
+        # a buffer that is page-locked already (or cannot be) is used as it is: only the copy
+        # speed depends on it
+        if self.buf.nbytes and _lib.load().gz_host_register(self.buf.ctypes.data, self.buf.nbytes) == 0:
             self.ptr = self.buf.ctypes.data
         return self.buf
 
@@ -392,9 +394,14 @@ class pinned_host:
             self.ptr = None
 
 
+# records one tick of a batched replay ingests at most: with queries taken first, it bounds how
+# long a query released during a tick waits for that tick's ingest
+REPLAY_TICK_RECORDS = 1 << 19
+
+
 def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes: int = 0,
            time_scale: float = 1.0, sketches_factor: float = 1.0,
-           max_tick_updates: int = 1 << 21, route: float | None = None,
+           max_tick_updates: int = REPLAY_TICK_RECORDS, route: float | None = None,
            pin: bool = True, query_snapshot: bool = False) -> ServingResult:
     """Serve every request of `trace`. mode "batched": the gz_server path (continuous batching:
     each tick submits the queries that need no update of this tick, applies the arrived update
@@ -442,6 +449,10 @@ def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes:
     jobs_in: deque = deque()    # batched: jobs for the collector, in submission order
     wake = threading.Condition()
     collector_error = []
+    # a cyclic garbage collection pass can stall the loop for many milliseconds in a process that
+    # holds many objects: one pass now, none while requests are served
+    gc_on = gc.isenabled()
+    gc.collect()
     t0 = time.perf_counter()
     nxt = 0
 
@@ -585,6 +596,7 @@ def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes:
     if mode == "batched":
         thread = threading.Thread(target=collector, daemon=True)
         thread.start()
+    gc.disable()
     try:
         while True:
             tnow = now_trace()
@@ -684,6 +696,8 @@ def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes:
                 wake.notify()
             thread.join()
         res.seconds = time.perf_counter() - t0
+        if gc_on:
+            gc.enable()
         for t in list(state):
             if mode == "plain":
                 state.pop(t).close()
