@@ -271,3 +271,26 @@ def test_batch_routes_agree(gz, route):
         res = b.connected_components()
         for g, V in enumerate(Vs):
             _check_graph(gz, b, res, g, V, seeds[g], sts[g])
+
+
+def test_batch_hub_bins(gz):
+    """Star hubs put up to 40k entries of one call into a single tile's bin, next to tiles of a
+    few entries: every graph's bytes and answers equal the single-graph handle's, over several
+    calls."""
+    from graphzeppelin_b200 import streams as S
+    Vs = [10000, 3000, 40000, 700]
+    seeds = [31, 32, 33, 34]
+    hubs, rests = [], []
+    for V in Vs:
+        hubs.append(S.edges_to_stream(V, S.edge_index(np.zeros(V - 1, np.uint64),
+                                                      np.arange(1, V, dtype=np.uint64)), V).records)
+        rests.append(S.erdos_renyi_stream(V, min(1.0, 6.0 / V), seed=V + 1, churn_fraction=0.2).records)
+    full = [np.concatenate([h, r]) for h, r in zip(hubs, rests)]
+    with gz.CCSketchBatch(Vs, seeds) as b:
+        b.ingest(hubs)  # the hubs' bins: 9999 and 39999 entries in one call
+        parts = [np.array_split(r, 2) for r in rests]
+        for k in range(2):
+            b.ingest([p[k] for p in parts])
+        res = b.connected_components()
+        for g, V in enumerate(Vs):
+            _check_graph(gz, b, res, g, V, seeds[g], full[g])
