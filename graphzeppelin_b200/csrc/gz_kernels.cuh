@@ -108,11 +108,11 @@ cudaError_t gutter_scatter_global(int input, const void *d_in, uint64_t n, Gutte
                                   uint64_t *cursor, uint2 *entries, cudaStream_t s);
 
 // ---- coded entries and bucket planes (gz_planes.cu) ---------------------------------------
-// A vertex sketch is accumulated in shared memory as three planes of kPlaneRows rows x
+// A vertex sketch is accumulated in shared memory as four planes of kPlaneRows rows x
 // kPlaneSlots 32-bit slots: slot c < C is column c, slot C the deterministic bucket (row 0).
 // Row d of a column holds depth d; the last row is scratch (depth codes at or above it are
 // handled in HBM). Plane A XORs (neighbour | 1 << 31) of the entries whose neighbour is above
-// the vertex, plane B of the others, plane G their checksums.
+// the vertex, plane B of the others; planes GA and GB their checksums.
 constexpr uint32_t kPlaneSlots = 32;
 constexpr uint32_t kPlaneRows = 12;
 constexpr uint32_t kPlaneMaxColumns = kPlaneSlots - 1;

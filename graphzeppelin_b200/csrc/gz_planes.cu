@@ -57,12 +57,13 @@ using namespace gz::dev;
 
 constexpr uint32_t kPlaneThr = kPlaneRows - 1;               // first depth not held in the planes
 constexpr uint32_t kPlaneBytes = kPlaneRows * kPlaneSlots * 4;  // one plane of one vertex
-constexpr uint32_t kVertBytes = 3 * kPlaneBytes;              // planes A, B, G of one vertex
-constexpr uint32_t kWbRows = 4;                               // rows per write-back pass
-constexpr uint32_t kWbStride = 3 * kWbRows + 1;               // words per slot (odd: no conflicts)
-constexpr uint32_t kWbWords = kPlaneSlots * kWbStride;        // per-warp buffer (write-back, queue)
+// Planes of one vertex: A, its checksums GA, B, its checksums GB. Each checksum plane sits one
+// plane after the plane it pairs with, so a slot step's second address is the first plus a
+// constant (an immediate of the reduction) whichever of A and B the entry goes to; the sketch's
+// checksum word is GA ^ GB.
+constexpr uint32_t kVertBytes = 4 * kPlaneBytes;
 constexpr uint32_t kQueueSlots = 64;                          // per-warp queue of filtered entries
-static_assert(kQueueSlots * 16 <= kWbWords * 4, "the entry queue shares the write-back buffer");
+constexpr uint32_t kWbWords = kQueueSlots * 4;                // per-warp buffer: the entry queue
 
 // Depth codes of all C columns into the nibble words w (column c in bits 4(c % 8) of word c / 8;
 // nibbles past C are zero); pm = premixed edge index. Every sketch has at least 18 columns: the
@@ -309,6 +310,10 @@ k_hash_sort_scatter(const uint8_t *__restrict__ rec, uint64_t n, GutterGeom g, P
 __device__ __forceinline__ void red_xor_shared(uint32_t addr, uint32_t v) {
   asm volatile("red.shared.xor.b32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
 }
+// The same slot of the checksum plane that follows the plane of addr.
+__device__ __forceinline__ void red_xor_shared_g(uint32_t addr, uint32_t v) {
+  asm volatile("red.shared.xor.b32 [%0+%2], %1;" ::"r"(addr), "r"(v), "n"(kPlaneBytes) : "memory");
+}
 
 __device__ __forceinline__ uint32_t nibble_of(const uint32_t (&c4)[4], uint32_t c) {
   const uint32_t w = c < 16 ? (c < 8 ? c4[0] : c4[1]) : (c < 24 ? c4[2] : c4[3]);
@@ -469,15 +474,14 @@ __device__ __forceinline__ void plane_entry(uint4 e, uint32_t kind, bool valid, 
   // bits 2..6 of base are the lane (sp is 128-byte aligned, the rest multiples of 128), and the
   // row offset (a multiple of 128) leaves them alone, so (base + row) ^ (t << 2) addresses slot
   // lane ^ t of the row
-  const uint32_t base = x.sp + (v & x.tile_mask) * kVertBytes + p * kPlaneBytes + (lane << 2);
-  const uint32_t dg = (2u - p) * kPlaneBytes;
+  const uint32_t base = x.sp + (v & x.tile_mask) * kVertBytes + p * 2 * kPlaneBytes + (lane << 2);
 #pragma unroll
   for (int t = 0; t < 32; ++t) {
     const uint32_t w = (uint32_t)t >> 3, k = ((uint32_t)t & 7u) >> 1;
     const uint32_t d8 = __byte_perm((t & 1) ? od[w] : ev[w], 0, 0x4440u + k);
     const uint32_t a = (base + d8 * 16u) ^ (uint32_t)(t << 2);
     red_xor_shared(a, val);
-    red_xor_shared(a + dg, chk);
+    red_xor_shared_g(a, chk);
   }
 }
 
@@ -517,7 +521,7 @@ k_plane_update(PlaneGeom g, PlaneHash ph, uint8_t *__restrict__ sketches,
   const uint32_t per_bin = g.bin_shift - g.tile_shift;  // log2(tiles per bin)
   const uint32_t s0 = smem_u32(dsm);
   const uint32_t pad = (128u - (s0 & 127u)) & 127u;
-  uint8_t *planes = dsm + pad;  // W vertices x planes A, B, G x kPlaneRows x 32 words
+  uint8_t *planes = dsm + pad;  // W vertices x planes A, GA, B, GB x kPlaneRows x 32 words
   uint32_t *wbuf = reinterpret_cast<uint32_t *>(planes + (size_t)W * kVertBytes) + warp * kWbWords;
   uint4 *queue = reinterpret_cast<uint4 *>(wbuf);  // the apply phase's per-warp entry queue
   for (uint32_t i = threadIdx.x; i < g.C; i += blockDim.x) s_kcol[i] = ph.kcol[i];
@@ -639,8 +643,9 @@ k_plane_update(PlaneGeom g, PlaneHash ph, uint8_t *__restrict__ sketches,
       const uint32_t vg = (t << g.tile_shift) + vl;
       if (vg >= g.V) continue;
       const uint32_t *pa = reinterpret_cast<const uint32_t *>(planes + (size_t)vl * kVertBytes);
-      const uint32_t *pb = pa + kPlaneRows * kPlaneSlots;
-      const uint32_t *pg = pb + kPlaneRows * kPlaneSlots;
+      const uint32_t *pga = pa + kPlaneRows * kPlaneSlots;
+      const uint32_t *pb = pga + kPlaneRows * kPlaneSlots;
+      const uint32_t *pgb = pb + kPlaneRows * kPlaneSlots;
       uint32_t *sk = x.gsk + (uint64_t)vg * g.sketch_words;
       // word (c, w) of lane l's current list position; w < runw
       uint32_t c = 0, w = lane;
@@ -653,7 +658,7 @@ k_plane_update(PlaneGeom g, PlaneHash ph, uint8_t *__restrict__ sketches,
         const uint32_t s = r * kPlaneSlots + cc, kk = ww - 3 * r;
         const uint32_t a = pa[s], bq = pb[s];
         return kk == 0 ? (a & 0x7fffffffu) ^ ((bq >> 31) ? vg : 0u)
-             : kk == 1 ? (bq & 0x7fffffffu) ^ ((a >> 31) ? vg : 0u) : pg[s];
+             : kk == 1 ? (bq & 0x7fffffffu) ^ ((a >> 31) ? vg : 0u) : pga[s] ^ pgb[s];
       };
       for (uint32_t i0 = 0; i0 < nwl; i0 += 8 * 32) {
         uint32_t y[8], old[8], off[8];
@@ -676,7 +681,7 @@ k_plane_update(PlaneGeom g, PlaneHash ph, uint8_t *__restrict__ sketches,
       if (lane < 3) {  // deterministic bucket: slot C, row 0
         const uint32_t a = pa[C], bq = pb[C];
         const uint32_t y = lane == 0 ? (a & 0x7fffffffu) ^ ((bq >> 31) ? vg : 0u)
-                         : lane == 1 ? (bq & 0x7fffffffu) ^ ((a >> 31) ? vg : 0u) : pg[C];
+                         : lane == 1 ? (bq & 0x7fffffffu) ^ ((a >> 31) ? vg : 0u) : pga[C] ^ pgb[C];
         if (y) sk[3 * C * B + lane] ^= y;
       }
     }
@@ -733,15 +738,14 @@ __global__ void __launch_bounds__(1024, 1) k_plane_update_peak(uint32_t iters, u
       ev[w] = (c4[w] & 0x0f0f0f0fu) << 3;
       od[w] = ((c4[w] >> 4) & 0x0f0f0f0fu) << 3;
     }
-    const uint32_t base = sp + v * kVertBytes + p * kPlaneBytes + (lane << 2);
-    const uint32_t dg = (2u - p) * kPlaneBytes;
+    const uint32_t base = sp + v * kVertBytes + p * 2 * kPlaneBytes + (lane << 2);
 #pragma unroll
     for (int t = 0; t < 32; ++t) {
       const uint32_t w = (uint32_t)t >> 3, k = ((uint32_t)t & 7u) >> 1;
       const uint32_t d8 = __byte_perm((t & 1) ? od[w] : ev[w], 0, 0x4440u + k);
       const uint32_t a = (base + d8 * 16u) ^ (uint32_t)(t << 2);
       red_xor_shared(a, val);
-      red_xor_shared(a + dg, chk);
+      red_xor_shared_g(a, chk);
     }
   }
   __syncthreads();
