@@ -932,6 +932,8 @@ def run_powerlaw(args):
     alg = gz.CCSketchAlg(V, cfg["sketch_seed"])
     if args.host_rounds:
         alg.set_query_graph(False)
+    if args.entry_form:
+        alg.set_tuning(entry_form=args.entry_form)
     if args.pipeline is not None:
         alg.set_pipeline(args.pipeline)
     alg.set_gutter_capacity(2 * int(cuts[1] - cuts[0]) + 1024)
@@ -1028,6 +1030,9 @@ def main():
     ap.add_argument("--small", action="store_true",
                     help="profiling sizes: dense V=2^14, powerlaw V=2^18")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--entry-form", type=int, default=0, choices=[0, 1, 2, 3],
+                    help="power-law workload: gutter entry form (0 the handle's choice, 1 plain, "
+                         "2 coded, 3 coded with 3-bit depth codes)")
     ap.add_argument("--pipeline", type=int, default=None, choices=[-1, 0, 1, 2, 3, 4],
                     help="sketch-update kernel: 1 tile pipeline (2..4: with that many buffers), "
                          "0 one tile at a time, -1 the handle's choice (default)")
