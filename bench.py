@@ -669,7 +669,7 @@ SERVING = dict(workload="serving_t2000_v2e10-2e18_chunglu2.3_budget120GB", num_t
 # The serving check of the default run: a short trace whose sketch demand exceeds the budget, so
 # that tenants queue for admission while query latency is measured.
 SERVING_SHORT = dict(num_tenants=400, trace_seed=11, budget_bytes=16 * 10**9,
-                     snapshot_bytes=8 * 10**9, time_scale=4.0)
+                     snapshot_bytes=8 * 10**9, time_scale=5.0)
 # records per tick of the saturated (throughput) replays; the paced ones use the replay's default,
 # a smaller cap that bounds how long a released query waits behind one ingest call
 SERVING_SAT_TICK = 1 << 21

@@ -394,6 +394,42 @@ class pinned_host:
             self.ptr = None
 
 
+def plan_tick(resident, pending: Dict[int, deque], queued_q: Dict[int, int], busy, kind: np.ndarray,
+              rec_off: np.ndarray, max_records: int):
+    """The requests one tick of the batched replay takes, in order; taken requests leave
+    `pending`, and `queued_q` (released queries not yet taken, per tenant) counts down.
+
+    Tenants with a query waiting come first (their updates up to that query), then the others by
+    their oldest request; a tenant in `busy` (its query still running) is skipped. A tenant's
+    update batches are taken while the tick has records left (the last one may overshoot
+    max_records), and its first query ends its part of the tick: an `early` query needs no update
+    of this tick (it can go out before the tick's ingest), a `late` one comes after this tick's
+    updates of its tenant. Returns (updates, early, late), lists of (request, tenant)."""
+    updates, early, late = [], [], []
+    left = max_records
+    end = len(kind)
+    for t in sorted(resident, key=lambda x: (not queued_q.get(x), pending[x][0] if pending.get(x) else end)):
+        q = pending.get(t)
+        if not q or t in busy:
+            continue
+        took = False
+        while q:
+            i = q[0]
+            if kind[i] == UPDATE:
+                if left <= 0:
+                    break
+                left -= int(rec_off[i + 1] - rec_off[i])
+                updates.append((i, t))
+                took = True
+                q.popleft()
+            else:
+                (late if took else early).append((i, t))
+                q.popleft()
+                queued_q[t] -= 1
+                break
+    return updates, early, late
+
+
 # records one tick of a batched replay ingests at most: with queries taken first, it bounds how
 # long a query released during a tick waits for that tick's ingest
 REPLAY_TICK_RECORDS = 1 << 19
@@ -642,35 +678,13 @@ def replay(trace: ServingTrace, mode: str, budget_bytes: int, *, snapshot_bytes:
                 continue
             # batched: one tick. Answers that are ready go out first.
             take_answers()
-            ing_t, ing_seg, ing_req = [], [], []
-            early, late = [], []  # queries needing no update of this tick / behind this tick's updates
-            budget_left = max_tick_updates
             busy = {t for job in inflight for t in job[1]}
-            # tenants with a query waiting first (their updates up to the query), then the others by
-            # their oldest request; update-only work fills what the tick's cap leaves
-            for t in sorted(resident, key=lambda x: (not queued_q.get(x), pending[x][0] if pending.get(x) else N)):
-                q = pending.get(t)
-                if not q or t in busy:
-                    continue
-                nparts = 0
-                while q:
-                    i = q[0]
-                    if trace.kind[i] == UPDATE:
-                        if budget_left <= 0:
-                            break
-                        ing_t.append(state[t])
-                        ing_seg.append(trace.records(i))
-                        nparts += 1
-                        budget_left -= int(trace.rec_off[i + 1] - trace.rec_off[i])
-                        ing_req.append((i, t))
-                        q.popleft()
-                    else:
-                        (late if nparts else early).append((i, t))
-                        q.popleft()
-                        queued_q[t] -= 1
-                        break
-                if nparts:
-                    version[t] += 1
+            ing_req, early, late = plan_tick(resident, pending, queued_q, busy, trace.kind,
+                                             trace.rec_off, max_tick_updates)
+            ing_t = [state[t] for _, t in ing_req]
+            ing_seg = [trace.records(i) for i, _ in ing_req]
+            for t in {t for _, t in ing_req}:
+                version[t] += 1
             if not ing_t and not early and not late:
                 if nxt >= N and not resident and not waiting:
                     break
